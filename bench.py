@@ -1,0 +1,357 @@
+"""Benchmark of the staggered-grid elastic timestep loop on B200.
+
+A "step" is one full time step (velocity + stress update, source, receivers)
+of one model.  Default workload: the random-medium cube, 344^3 interior +
+20-cell split PML (384^3 computed cells, 394^3 GRID), dt 1 ms, 64x64
+receivers recording vx, vy, vz, FP32.  Metric: Gcell-updates/s (computed
+cells x steps / device seconds), whole job over all ranks.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl sgfd|reference]
+
+With N > 1 (torchrun) every rank advances its own independent replica of the
+model on its own GPU ("replicas only": the path has no exchange step), so
+scaling is weak.  `--impl reference` times the reference algorithm's CPU
+implementation (this project's oracle port, all host threads) on rank 0 and
+also reports the reference's own GPU program (compiled from its sources under
+oracle/_ref/) timed on this GPU.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "staggered-grid_b200"))
+
+# Algorithmic bytes per computed cell and kernel launch (FP32): every field
+# value read or written once per kernel.  velocity: interior reads 6 stresses
+# + 3 velocities + buoyancy and writes 3 velocities; PML reads 6 stresses + 9
+# velocity splits + buoyancy and writes 9 splits + 3 velocities.  stress:
+# interior reads 3 velocities + 6 stresses + lambda + mu, writes 6 stresses;
+# PML reads 3 velocities + 15 stress splits + lambda + mu, writes 15 splits +
+# 6 stresses.  Sum per step: 120 B interior, 276 B PML.
+BYTES = {"velocity": (52, 112), "stress": (68, 164)}
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=100)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", choices=["sgfd", "reference"], default="sgfd")
+    p.add_argument("--workload", choices=["random344", "plain100", "reference_main"], default="random344")
+    p.add_argument("--kernel", choices=["auto", "simple", "zmarch"], default="auto")
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--cpu-steps", type=int, default=6, help="steps of the CPU sample")
+    return p.parse_args()
+
+
+def build_workload(name):
+    import sgfd.workloads as wl
+    if name == "random344":
+        return wl.random_cube(n_interior=344, pml=20, nt=2000)
+    if name == "plain100":
+        return wl.plain_cube(n_interior=100, pml=20, nt=500)
+    return wl.reference_case(nt=1500)
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason sampling during the timed region."""
+    FIELDS = ("pci.bus_id,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, bus_id: str | None):
+        self.bus_id = (bus_id or "").lower()
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "20"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return None
+        time.sleep(0.05)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = [l.split(", ") for l in self.lines if l.count(",") >= 8]
+        if self.bus_id:
+            mine = [r for r in rows if self.bus_id.endswith(r[0].lower()[-12:]) or r[0].lower().endswith(self.bus_id[-12:])]
+            rows = mine or rows
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for k, n in enumerate(names):
+                if r[5 + k].strip().lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(args):
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def cpu_oracle_rate(w, steps: int, warm: int = 1):
+    """Time the oracle port (FP32, flush-to-zero on, all host threads) on the full
+    workload grid for `steps` steps after `warm` untimed steps.  Returns
+    (Gcell/s, threads, seconds)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle_py
+    threads = oracle_py.set_threads(os.cpu_count() or 1)
+    o = oracle_py.Oracle(w.cfg, fp64=False, ftz=True)
+    o.set_medium(w.b, w.lam, w.mu)
+    o.set_source(*w.src)
+    o.set_receivers(w.rec_xyz, w.rec_comp, w.nt)
+    wav = w.wavelet.astype(np.float64)
+    o.run(wav, 0, warm)
+    t0 = time.perf_counter()
+    o.run(wav, warm, steps)
+    dt = time.perf_counter() - t0
+    o.close()
+    return w.computed_cells() * steps / dt / 1e9, threads, dt
+
+
+def run_reference_arm(args, w, world, rank):
+    """CPU implementation of the reference algorithm on rank 0 (+ the reference's
+    own GPU program, if built)."""
+    if rank != 0:
+        return
+    steps = max(1, min(args.steps, args.cpu_steps))
+    rate, threads, secs = cpu_oracle_rate(w, steps, warm=min(args.warmup, 1))
+    line = {
+        "impl": "reference", "metric": "Gcell-updates/s", "value": rate, "unit": "Gcell/s",
+        "n_gpus": args.gpus, "steps": steps, "warmup": min(args.warmup, 1),
+        "ms_per_step": secs / steps * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": w.name, "grid": [w.cfg["nx"], w.cfg["ny"], w.cfg["nz"]], "pml": w.cfg["pml"],
+                   "computed_cells": w.computed_cells()},
+        "cpu_baseline": {"value": rate, "unit": "Gcell/s", "cores": threads, "kind": "port",
+                         "sample": f"{steps} full time steps of the {w.name} grid after 1 untimed step; "
+                                   f"C++ oracle restating the reference kernels, FP32, OpenMP {threads} threads, "
+                                   f"flush-to-zero on (the reference's own CPU program implements another PML "
+                                   f"and does not build unmodified)"},
+        "e2e": {"value": rate, "unit": "Gcell/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    ref_bin = os.path.join(ROOT, "oracle", "_ref", "ref_opt")
+    if os.path.exists(ref_bin):
+        line["gpu_reference"] = reference_gpu_program(ref_bin, w, steps=min(max(args.steps, 20), 200))
+    print(json.dumps(line), flush=True)
+
+
+def write_case(path, w, nt):
+    c = w.cfg
+    with open(path, "wb") as f:
+        hdr = np.array([0x43464753, 1, c["nx"], c["ny"], c["nz"], c["pml"], nt, *w.src, *w.src, 0], np.int32)
+        f.write(hdr.tobytes())
+        fl = np.array([c["dt"], c["dx"], c["dy"], c["dz"], 20.0, *c["coef"]], np.float32)
+        f.write(fl.tobytes())
+        for a in (w.b, w.lam, w.mu):
+            f.write(np.ascontiguousarray(a, np.float32).tobytes())
+
+
+def reference_gpu_program(ref_bin, w, steps):
+    """The reference's own single-GPU PML program (OPT/ElasticWaveEquation.cu),
+    built unmodified from its sources, timed with CUDA events over `steps`
+    calls of its propagate() on this workload's grid and medium."""
+    with tempfile.TemporaryDirectory() as d:
+        case, out = os.path.join(d, "case.bin"), os.path.join(d, "out.bin")
+        write_case(case, w, steps)
+        r = subprocess.run([ref_bin, case, out], capture_output=True, text=True, timeout=600)
+    if r.returncode != 0:
+        return {"error": r.stderr[-300:]}
+    tok = dict(t.split("=") for t in r.stdout.split()[1:])
+    ms = float(tok["ms"])
+    return {"value": w.computed_cells() * steps / (ms / 1e3) / 1e9, "unit": "Gcell/s", "steps": steps,
+            "ms_per_step": ms / steps,
+            "note": "reference OPT program (velocityUpdate/stressUpdate as shipped, 4 launches + device sync per "
+                    "step), built for sm_100a from its own sources, CUDA events around its propagate() loop"}
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_setup(args)
+    w = build_workload(args.workload)
+    if args.impl == "reference":
+        run_reference_arm(args, w, world, rank)
+        return
+    import torch
+    import sgfd
+    torch.cuda.set_device(local)
+    kernel = {"auto": sgfd.KERNEL_AUTO, "simple": sgfd.KERNEL_SIMPLE, "zmarch": sgfd.KERNEL_ZMARCH}[args.kernel]
+    cfg = sgfd.default_config(**{**w.cfg, "device": local, "kernel": kernel})
+    K, W = args.steps, args.warmup
+    nt = max(w.nt, W + K + 64)
+    wav = np.resize(w.wavelet, nt).astype(np.float32)
+    stream = torch.cuda.current_stream()
+    s = sgfd.Solver(cfg)
+    s.set_stream(stream.cuda_stream)
+    s.set_medium(w.b, w.lam, w.mu)
+    s.set_source(*w.src)
+    s.set_receivers(w.rec_xyz, w.rec_comp, nt)
+    s.set_wavelet(wav)
+    cells = w.computed_cells()
+    n_int, n_pml = s.cell_counts()
+
+    # ---- device-resident timing: exactly K steps ----
+    s.run(0, W)
+    torch.cuda.synchronize()
+    bus = getattr(torch.cuda.get_device_properties(local), "pci_bus_id", None)
+    clocks = ClockSampler(bus)
+    clocks.start()
+    time.sleep(0.1)
+    barrier(world)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    s.run(W, K)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    clk = clocks.stop()
+    ms = max_over_ranks(e0.elapsed_time(e1), world)
+    value = world * cells * K / (ms / 1e3) / 1e9
+
+    # ---- roofline of the dominant kernel (events around each kernel) ----
+    P = max(3, min(K, 20))
+    tv, ts = s.profile(W + K, P)
+    per = {"velocity": tv / P, "stress": ts / P}
+    dom = max(per, key=per.get)
+    alg = BYTES[dom][0] * n_int + BYTES[dom][1] * n_pml
+    peak, peak_kind = measured_peak()
+    achieved = alg / (per[dom] / 1e3) / 1e9
+    traffic = None
+    roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
+            "alg_bytes_per_launch": alg, "avg_launch_ms": per[dom],
+            "step_frac": (120 * n_int + 276 * n_pml) / (ms / K / 1e3) / 1e9 / peak,
+            "kernel_ms": per}
+
+    # ---- end to end through the C ABI with host buffers ----
+    e2e = None
+    if not args.no_e2e:
+        e2e = end_to_end(s, w, K, world, stream, wav)
+
+    kernel_name, launches = s.kernel_name(), K * s.launches_per_step()
+    s.close()
+    result = {
+        "metric": "Gcell-updates/s", "value": value, "unit": "Gcell/s", "n_gpus": world, "steps": K,
+        "warmup": W, "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": w.name, "grid": [w.cfg["nx"], w.cfg["ny"], w.cfg["nz"]], "pml": w.cfg["pml"],
+                   "computed_cells": cells, "interior_cells": n_int, "pml_cells": n_pml,
+                   "receivers": len(w.rec_comp), "kernel": None, "parallelism": f"replicas{world}",
+                   "l2": "inputs larger than L2 (9 wavefields of %.0f MB each)" % (w.cfg["nx"] * w.cfg["ny"] * w.cfg["nz"] * 4 / 1e6)},
+        "roofline": roof, "clocks": clk,
+        "gpu_launches": None, "e2e": e2e,
+    }
+    result["config"]["kernel"] = kernel_name
+    result["gpu_launches"] = launches
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, threads, secs = cpu_oracle_rate(w, args.cpu_steps)
+        result["cpu_baseline"] = {
+            "value": rate, "unit": "Gcell/s", "cores": threads, "kind": "port",
+            "sample": f"{args.cpu_steps} full time steps of {w.name} ({secs:.1f} s) after 1 untimed step; "
+                      f"C++ oracle of the reference kernels, FP32, flush-to-zero, OpenMP {threads} threads"}
+    if rank == 0:
+        print(json.dumps(result), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def end_to_end(s, w, K, world, stream, wav):
+    """The reference usage pattern through the C ABI (run(): medium upload,
+    per-step propagate with a host-supplied source value, per-step readback of
+    the receivers' samples), host buffers, timed on the host after a sync."""
+    import torch
+    n = w.b.size
+    pinned = [torch.empty(n, dtype=torch.float32, pin_memory=True) for _ in range(3)]
+    for t, a in zip(pinned, (w.b, w.lam, w.mu)):
+        t.numpy()[:] = a.reshape(-1)
+    nrec = len(w.rec_comp)
+    out = torch.empty(nrec, dtype=torch.float32, pin_memory=True).numpy()
+    s.reset()
+    s.synchronize()
+    barrier(world)
+    t0 = time.perf_counter()
+    s.set_medium(*[t.numpy() for t in pinned])
+    for it in range(K):
+        s.step(it, float(wav[it]))
+        s.trace_step(it, out)
+    s.synchronize()
+    secs = time.perf_counter() - t0
+    secs = max_over_ranks(secs, world)
+    h2d = (3 * n * 4) / K + 4
+    return {"value": world * w.computed_cells() * K / secs / 1e9, "unit": "Gcell/s",
+            "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": nrec * 4, "steps": K,
+            "note": "medium upload (3 x GRID floats, pinned) + K x (sgfd_step with host source value + "
+                    "sgfd_get_trace_step of all receivers), wall clock"}
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,212 @@
+/*
+ * sgfd.h — C ABI of the B200 staggered-grid elastic solver (libsgfd.so).
+ *
+ * One handle = one 3-D velocity–stress model on one GPU: 9 wavefields
+ * (vx, vy, vz, txx, tyy, tzz, txy, txz, tyz), the medium (buoyancy, lambda,
+ * mu), the split-field PML state, one explosive point source and a list of
+ * receivers.  The time step is 10th-order staggered differences in space and
+ * leapfrog in time, the scheme of the reference's single-GPU PML program
+ * (3DGPUwithPML_1DArraySingleGPU_optimization/, cited as OPT/ below).
+ *
+ * Geometry follows the reference GRID convention: nx, ny, nz count every
+ * allocated cell, including a 5-cell frame on each side that is never
+ * updated (OPT/ElasticMacro.h:30-39).  Cells [5, n-5) are computed; the outer
+ * `pml` cells of that range form the absorbing layer.  Host arrays are
+ * x-fastest, index = ix + iy*nx + iz*nx*ny (OPT/ElasticMacro.h:22).
+ *
+ * Every call returns an sgfd_status; nothing exits the process.  The last
+ * error message of a handle is returned by sgfd_last_error().  A handle is
+ * not thread-safe; distinct handles are independent.
+ *
+ * Reference interfaces replaced (file:line in the reference project):
+ *   sgfd_create          ElasticWaveEquation::ElasticWaveEquation  OPT/ElasticWaveEquation.cu:8-45
+ *                        + calStartEndPoint / vsPMLCPUTovsPML      OPT/ElasticWaveEquation.cu:47-113
+ *   sgfd_set_medium      the medium upload in run()               OPT/ElasticWaveEquation.cu:143-147
+ *   sgfd_set_source      sourceLocationCPUTosourceLocationGPU     OPT/ElasticWaveEquation.cu:115-118
+ *   sgfd_set_receivers   stationLocationCPUTostationLocationGPU   OPT/ElasticWaveEquation.cu:120-123
+ *   sgfd_ricker_ref      ElasticWaveEquation::sourceFunction      OPT/ElasticWaveEquation.cu:184-189
+ *   sgfd_step            ElasticWaveEquation::propagate           OPT/ElasticWaveEquation.cu:191-204
+ *                        (locateSource, velocityUpdate, stressUpdate, recordStationData:
+ *                         OPT/ElasticWaveEquation.cu:206-841)
+ *   sgfd_run             the time loop of run()                   OPT/ElasticWaveEquation.cu:153-172
+ *   sgfd_get_traces      station D2H copy                         OPT/ElasticWaveEquation.cu:174
+ *   sgfd_get_field       snapshot D2H copy                        OPT/ElasticWaveEquation.cu:162
+ *   sgfd_destroy         ElasticWaveEquation::~ElasticWaveEquation OPT/ElasticWaveEquation.cu:125-138
+ */
+#ifndef SGFD_H
+#define SGFD_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SGFD_ABI_VERSION 1
+
+typedef enum sgfd_status {
+    SGFD_OK = 0,
+    SGFD_ERR_INVALID = 1,      /* bad argument or configuration */
+    SGFD_ERR_ALLOC = 2,        /* device or host allocation failed */
+    SGFD_ERR_CUDA = 3,         /* a CUDA runtime call failed */
+    SGFD_ERR_STATE = 4,        /* call out of order (e.g. step before set_medium) */
+    SGFD_ERR_UNSUPPORTED = 5,  /* option not built into this library */
+    SGFD_ERR_NO_DEVICE = 6,    /* no usable CUDA device */
+    SGFD_ERR_NONFINITE = 7     /* a NaN/Inf was found in the wavefield */
+} sgfd_status;
+
+/* Wavefield ids (also receiver components). */
+typedef enum sgfd_field {
+    SGFD_VX = 0, SGFD_VY = 1, SGFD_VZ = 2,
+    SGFD_TXX = 3, SGFD_TYY = 4, SGFD_TZZ = 5,
+    SGFD_TXY = 6, SGFD_TXZ = 7, SGFD_TYZ = 8,
+    SGFD_NFIELDS = 9
+} sgfd_field;
+
+/* Medium ids for sgfd_get_medium. */
+typedef enum sgfd_medium_id {
+    SGFD_BUOYANCY = 0, SGFD_LAMBDA = 1, SGFD_MU = 2
+} sgfd_medium_id;
+
+/* Damping profiles of the split-field PML.
+ *  REFGPU: d = tau*Vs/dx*(8/15 - 0.03 p + p^2/1500)*(k/p)^2, tau=4.3, Vs local
+ *          shear velocity sqrt(mu*b), k = 1..p from the inner edge
+ *          (OPT/ElasticMacro.h:26-27, OPT/ElasticWaveEquation.cu:282-288).
+ *  LOGR:   d = d0*(k/p)^2, d0 = 3*Vp*ln(1/R)/(2*p*dx), Vp local P velocity
+ *          sqrt((lambda+2mu)*b); the classic quadratic profile.
+ *  REFCPU: d = log10(1/R)*3.4*Vconst/(p*dx)*(k/p)^2 with a constant velocity
+ *          (3DCPUwithPML_3DArray_GridIncludePMLandOrder/ElasticMacro.h:18-23). */
+typedef enum sgfd_damping {
+    SGFD_DAMP_REFGPU = 0,
+    SGFD_DAMP_LOGR = 1,
+    SGFD_DAMP_REFCPU = 2
+} sgfd_damping;
+
+/* Medium averaging.  REF keeps the reference's two index quirks:
+ *  - the PML velocity split update uses the x-averaged buoyancy for all three
+ *    components (OPT/ElasticMacro.h:424-456);
+ *  - the harmonic mu average for txz takes mu[ix+1,iy+1,iz] as its fourth
+ *    point (OPT/ElasticMacro.h:116-117).
+ * FIXED uses the staggered-grid averages for every component. */
+typedef enum sgfd_quirks {
+    SGFD_QUIRKS_REF = 0,
+    SGFD_QUIRKS_FIXED = 1
+} sgfd_quirks;
+
+/* Wavefield storage type in HBM (arithmetic is always FP32). */
+typedef enum sgfd_storage {
+    SGFD_STORE_F32 = 0,
+    SGFD_STORE_BF16 = 1,
+    SGFD_STORE_F16 = 2
+} sgfd_storage;
+
+/* Kernel family.  AUTO picks the fastest built variant for the storage type. */
+typedef enum sgfd_kernel {
+    SGFD_KERNEL_AUTO = 0,
+    SGFD_KERNEL_SIMPLE = 1,   /* one thread per cell, global loads */
+    SGFD_KERNEL_ZMARCH = 2    /* 2.5-D z-marching, TMA-staged xy planes */
+} sgfd_kernel;
+
+typedef struct sgfd_config {
+    int32_t nx, ny, nz;       /* GRID incl. the 5-cell frame (reference GRID) */
+    int32_t pml;              /* PML width in cells (reference `pml`) */
+    float dt, dx, dy, dz;     /* reference Delta {t, x, y, z} */
+    float coef[5];            /* staggered difference coefficients (reference diff_coef) */
+    int32_t damping;          /* sgfd_damping */
+    float damping_R;          /* reflection coefficient for LOGR / REFCPU (reference R = 0.001) */
+    float damping_vconst;     /* constant velocity for REFCPU (reference 2000) */
+    int32_t quirks;           /* sgfd_quirks */
+    int32_t storage;          /* sgfd_storage */
+    int32_t kernel;           /* sgfd_kernel */
+    int32_t device;           /* CUDA device ordinal */
+    int32_t reserved[8];      /* must be zero */
+} sgfd_config;
+
+typedef struct sgfd_solver sgfd_solver;
+
+/* Fill *cfg with the reference defaults: coefficients of the reference
+ * main.cu (CON/main.cu:40-44), REFGPU damping, REF quirks, FP32, AUTO. */
+void sgfd_config_default(sgfd_config *cfg);
+
+int sgfd_abi_version(void);
+
+/* Create a solver and allocate its device state (fields zeroed). */
+int sgfd_create(const sgfd_config *cfg, sgfd_solver **out);
+void sgfd_destroy(sgfd_solver *h);
+const char *sgfd_last_error(const sgfd_solver *h);
+/* Message for errors where no handle exists (e.g. sgfd_create failures). */
+const char *sgfd_global_error(void);
+
+/* Use this CUDA stream (a cudaStream_t passed as void*) for all device work
+ * of the handle; NULL selects the handle's own stream. */
+int sgfd_set_stream(sgfd_solver *h, void *stream);
+
+/* Upload the medium from HOST arrays of nx*ny*nz floats (x fastest). */
+int sgfd_set_medium(sgfd_solver *h, const float *buoyancy, const float *lambda,
+                    const float *mu);
+/* Same from DEVICE arrays with the same dense layout. */
+int sgfd_set_medium_device(sgfd_solver *h, const float *buoyancy,
+                           const float *lambda, const float *mu);
+
+/* Explosive point source added to txx, tyy, tzz as dt*dt*s(it) before the
+ * velocity update of step it (OPT/ElasticWaveEquation.cu:206-221). */
+int sgfd_set_source(sgfd_solver *h, int32_t x, int32_t y, int32_t z);
+
+/* Receivers: n points (xyz[3*i..3*i+2]) each recording component comp[i]
+ * (sgfd_field) into a trace of nt samples.  Velocity components are sampled
+ * after the velocity update of step it, stresses after the stress update
+ * (OPT/ElasticWaveEquation.cu:223-232).  Replaces any earlier receiver set
+ * and zeroes the traces. */
+int sgfd_set_receivers(sgfd_solver *h, int32_t n, const int32_t *xyz,
+                       const int32_t *comp, int32_t nt);
+
+/* Source wavelet for sgfd_run: values[it] for it in [0, nt). */
+int sgfd_set_wavelet(sgfd_solver *h, int32_t nt, const float *values);
+
+/* One time step with a host-supplied source value (reference propagate()). */
+int sgfd_step(sgfd_solver *h, int32_t it, float source_value);
+
+/* Steps it0 .. it0+nsteps-1 with the wavelet of sgfd_set_wavelet; launched
+ * as a captured CUDA graph when use_graph != 0.  Asynchronous on the
+ * handle's stream. */
+int sgfd_run(sgfd_solver *h, int32_t it0, int32_t nsteps, int32_t use_graph);
+
+int sgfd_synchronize(sgfd_solver *h);
+
+/* Zero all wavefields, PML state and traces (medium, source, receivers kept). */
+int sgfd_reset(sgfd_solver *h);
+
+/* Copy traces to host: out[r*nt + it] (receiver-major). */
+int sgfd_get_traces(sgfd_solver *h, float *out);
+/* Copy the n receiver samples of one step `it` to out[0..n) (blocking);
+ * the per-step readback of a drop-in loop (OPT/ElasticWaveEquation.cu:153-174). */
+int sgfd_get_trace_step(sgfd_solver *h, int32_t it, float *out);
+/* Copy one wavefield (sgfd_field) to a host array of nx*ny*nz floats. */
+int sgfd_get_field(sgfd_solver *h, int32_t field, float *out);
+/* Copy one medium array (sgfd_medium_id) back to host (nx*ny*nz floats). */
+int sgfd_get_medium(sgfd_solver *h, int32_t which, float *out);
+
+/* Reference Ricker wavelet value of step it (OPT/ElasticWaveEquation.cu:184-189):
+ * t0 = ceil(1/(f0*dt)); a = pi*f0*((it - t0)*dt - 1/f0); (1 - 2a^2)*exp(-a^2). */
+float sgfd_ricker_ref(float f0, float dt, int32_t it);
+/* Ricker wavelet with an explicit delay t0 (seconds): a = pi*f0*(it*dt - t0). */
+float sgfd_ricker_t0(float f0, float dt, float t0, int32_t it);
+
+/* Steps it0 .. it0+nsteps-1 (wavelet source) with CUDA events around each
+ * kernel; returns the summed device time of the velocity-update and the
+ * stress-update kernels in milliseconds.  Blocking.  For roofline accounting. */
+int sgfd_profile(sgfd_solver *h, int32_t it0, int32_t nsteps, float *ms_velocity, float *ms_stress);
+
+/* Counts for roofline accounting: computed cells that are interior / PML. */
+int sgfd_cell_counts(const sgfd_solver *h, int64_t *n_interior, int64_t *n_pml);
+/* Number of kernel launches issued by one sgfd_step / one step of sgfd_run. */
+int sgfd_launches_per_step(const sgfd_solver *h);
+/* Name of the kernel family in use ("simple", "zmarch"). */
+const char *sgfd_kernel_name(const sgfd_solver *h);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SGFD_H */

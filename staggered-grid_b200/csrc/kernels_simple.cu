@@ -1,0 +1,208 @@
+// kernels_simple.cu — the "simple" kernel family: one thread per computed
+// cell, neighbours read straight from global memory (L1/L2 cached).
+//
+// It is the plain restatement of the reference's per-cell kernels
+// (3DGPUwithPML_1DArraySingleGPU_optimization/ElasticWaveEquation.cu:206-841)
+// with the 26-way region `else if` chain replaced by a per-axis band test and
+// the 26 region split arrays replaced by the compact PML array.  It serves as
+// the correctness baseline for the z-marching family and as the fallback for
+// grids the z-marching kernels do not tile.
+#include "cell_math.cuh"
+
+namespace sgfd {
+
+namespace {
+
+constexpr int kBX = 32, kBY = 8;
+
+// txx, tyy, tzz at the source cell += dt*dt*s(it)   (ElasticWaveEquation.cu:206-221)
+__global__ void k_inject(Model m, Physics ph, SourceRec sr, int it, float value, int use_wavelet) {
+    if (threadIdx.x != 0 || sr.src < 0) return;
+    const float s = use_wavelet ? sr.wavelet[it] : value;
+    const float v = ph.inj_dt2 * s;
+    m.f[3][sr.src] = m.f[3][sr.src] + v;
+    m.f[4][sr.src] = m.f[4][sr.src] + v;
+    m.f[5][sr.src] = m.f[5][sr.src] + v;
+}
+
+// Velocity update of one cell (ElasticWaveEquation.cu:234-526, ElasticMacro.h:409-458).
+__global__ void __launch_bounds__(kBX * kBY) k_velocity(Model m, Physics ph) {
+    const int cx = blockIdx.x * kBX + threadIdx.x;
+    const int cy = blockIdx.y * kBY + threadIdx.y;
+    const int cz = blockIdx.z;
+    if (cx >= m.nxc || cy >= m.nyc) return;
+    const int x = cx + kHalo, y = cy + kHalo, z = cz + kHalo;
+    const int64_t ci = pidx(m, x, y, z);
+    const int64_t SY = m.px, SZ = m.plane;
+    const float *sxx = m.f[3] + ci, *syy = m.f[4] + ci, *szz = m.f[5] + ci;
+    const float *sxy = m.f[6] + ci, *sxz = m.f[7] + ci, *syz = m.f[8] + ci;
+    const float *bb = m.b + ci;
+
+    const float bx = (bb[0] + bb[1]) / 2.0f;
+    const float by = (bb[0] + bb[SY]) / 2.0f;
+    const float bz = (bb[0] + bb[SZ]) / 2.0f;
+    const float xX = dfwd(ph.c, [&](int o) { return __ldg(sxx + o); }) / ph.dx;
+    const float xY = dbwd(ph.c, [&](int o) { return __ldg(sxy + o * SY); }) / ph.dy;
+    const float xZ = dbwd(ph.c, [&](int o) { return __ldg(sxz + o * SZ); }) / ph.dz;
+    const float yX = dbwd(ph.c, [&](int o) { return __ldg(sxy + o); }) / ph.dx;
+    const float yY = dfwd(ph.c, [&](int o) { return __ldg(syy + o * SY); }) / ph.dy;
+    const float yZ = dbwd(ph.c, [&](int o) { return __ldg(syz + o * SZ); }) / ph.dz;
+    const float zX = dbwd(ph.c, [&](int o) { return __ldg(sxz + o); }) / ph.dx;
+    const float zY = dbwd(ph.c, [&](int o) { return __ldg(syz + o * SY); }) / ph.dy;
+    const float zZ = dfwd(ph.c, [&](int o) { return __ldg(szz + o * SZ); }) / ph.dz;
+
+    const int kx = band(x, m.nx, m.pml), ky = band(y, m.ny, m.pml), kz = band(z, m.nz, m.pml);
+    if (!(kx | ky | kz)) {
+        m.f[0][ci] = __fmaf_rn(ph.dt * bx, (xX + xY) + xZ, m.f[0][ci]);
+        m.f[1][ci] = __fmaf_rn(ph.dt * by, (yX + yY) + yZ, m.f[1][ci]);
+        m.f[2][ci] = __fmaf_rn(ph.dt * bz, (zX + zY) + zZ, m.f[2][ci]);
+        return;
+    }
+    float mx = 1.f, px = 1.f, my = 1.f, py = 1.f, mz = 1.f, pz = 1.f;
+    {
+        const float mu0 = m.mu[ci], b0 = bb[0], l0 = m.lam[ci];
+        if (kx) damp_factors(ph, 0, ph.dx, kx, m.pml, mu0, b0, l0, mx, px);
+        if (ky) damp_factors(ph, 1, ph.dy, ky, m.pml, mu0, b0, l0, my, py);
+        if (kz) damp_factors(ph, 2, ph.dz, kz, m.pml, mu0, b0, l0, mz, pz);
+    }
+    const bool ref = ph.quirks == 0;   // REF: x-averaged buoyancy for all components
+    const float ax = ph.dt * bx, ay = ph.dt * (ref ? bx : by), az = ph.dt * (ref ? bx : bz);
+    const int64_t pi = pml_index(m, cx, cy, cz);
+    float *sp = m.split + pi;
+    const int64_t N = m.npml;
+    float a0, a1, a2;
+    a0 = sp[S_VXX * N] = split_update(sp[S_VXX * N], ax, xX, kx, mx, px);
+    a1 = sp[S_VXY * N] = split_update(sp[S_VXY * N], ax, xY, ky, my, py);
+    a2 = sp[S_VXZ * N] = split_update(sp[S_VXZ * N], ax, xZ, kz, mz, pz);
+    m.f[0][ci] = (a0 + a1) + a2;
+    a0 = sp[S_VYX * N] = split_update(sp[S_VYX * N], ay, yX, kx, mx, px);
+    a1 = sp[S_VYY * N] = split_update(sp[S_VYY * N], ay, yY, ky, my, py);
+    a2 = sp[S_VYZ * N] = split_update(sp[S_VYZ * N], ay, yZ, kz, mz, pz);
+    m.f[1][ci] = (a0 + a1) + a2;
+    a0 = sp[S_VZX * N] = split_update(sp[S_VZX * N], az, zX, kx, mx, px);
+    a1 = sp[S_VZY * N] = split_update(sp[S_VZY * N], az, zY, ky, my, py);
+    a2 = sp[S_VZZ * N] = split_update(sp[S_VZZ * N], az, zZ, kz, mz, pz);
+    m.f[2][ci] = (a0 + a1) + a2;
+}
+
+// Stress update of one cell (ElasticWaveEquation.cu:528-841, ElasticMacro.h:460-531).
+__global__ void __launch_bounds__(kBX * kBY) k_stress(Model m, Physics ph) {
+    const int cx = blockIdx.x * kBX + threadIdx.x;
+    const int cy = blockIdx.y * kBY + threadIdx.y;
+    const int cz = blockIdx.z;
+    if (cx >= m.nxc || cy >= m.nyc) return;
+    const int x = cx + kHalo, y = cy + kHalo, z = cz + kHalo;
+    const int64_t ci = pidx(m, x, y, z);
+    const int64_t SY = m.px, SZ = m.plane;
+    const float *vx = m.f[0] + ci, *vy = m.f[1] + ci, *vz = m.f[2] + ci;
+    const float *r = m.rmu + ci;
+
+    const float dXx = dbwd(ph.c, [&](int o) { return __ldg(vx + o); }) / ph.dx;
+    const float dYy = dbwd(ph.c, [&](int o) { return __ldg(vy + o * SY); }) / ph.dy;
+    const float dZz = dbwd(ph.c, [&](int o) { return __ldg(vz + o * SZ); }) / ph.dz;
+    const float xyY = dfwd(ph.c, [&](int o) { return __ldg(vx + o * SY); }) / ph.dy;
+    const float xyX = dfwd(ph.c, [&](int o) { return __ldg(vy + o); }) / ph.dx;
+    const float xzZ = dfwd(ph.c, [&](int o) { return __ldg(vx + o * SZ); }) / ph.dz;
+    const float xzX = dfwd(ph.c, [&](int o) { return __ldg(vz + o); }) / ph.dx;
+    const float yzZ = dfwd(ph.c, [&](int o) { return __ldg(vy + o * SZ); }) / ph.dz;
+    const float yzY = dfwd(ph.c, [&](int o) { return __ldg(vz + o * SY); }) / ph.dy;
+
+    const float l = m.lam[ci];
+    const float mu0 = m.mu[ci];
+    const float l2m = __fmaf_rn(2.0f, mu0, l);
+    const bool ref = ph.quirks == 0;   // REF: fourth txz point is mu[x+1, y+1, z]
+    const float mxy = 4.0f / (((r[0] + r[1]) + r[SY]) + r[1 + SY]);
+    const float mxz = 4.0f / (((r[0] + r[1]) + r[SZ]) + (ref ? r[1 + SY] : r[1 + SZ]));
+    const float myz = 4.0f / (((r[0] + r[SY]) + r[SZ]) + r[SY + SZ]);
+
+    const int kx = band(x, m.nx, m.pml), ky = band(y, m.ny, m.pml), kz = band(z, m.nz, m.pml);
+    if (!(kx | ky | kz)) {
+        m.f[3][ci] = __fmaf_rn(ph.dt, __fmaf_rn(l2m, dXx, l * (dYy + dZz)), m.f[3][ci]);
+        m.f[4][ci] = __fmaf_rn(ph.dt, __fmaf_rn(l2m, dYy, l * (dXx + dZz)), m.f[4][ci]);
+        m.f[5][ci] = __fmaf_rn(ph.dt, __fmaf_rn(l2m, dZz, l * (dXx + dYy)), m.f[5][ci]);
+        m.f[6][ci] = __fmaf_rn(ph.dt * mxy, xyY + xyX, m.f[6][ci]);
+        m.f[7][ci] = __fmaf_rn(ph.dt * mxz, xzZ + xzX, m.f[7][ci]);
+        m.f[8][ci] = __fmaf_rn(ph.dt * myz, yzZ + yzY, m.f[8][ci]);
+        return;
+    }
+    float mx = 1.f, px = 1.f, my = 1.f, py = 1.f, mz = 1.f, pz = 1.f;
+    {
+        const float b0 = m.b[ci];
+        if (kx) damp_factors(ph, 0, ph.dx, kx, m.pml, mu0, b0, l, mx, px);
+        if (ky) damp_factors(ph, 1, ph.dy, ky, m.pml, mu0, b0, l, my, py);
+        if (kz) damp_factors(ph, 2, ph.dz, kz, m.pml, mu0, b0, l, mz, pz);
+    }
+    const int64_t pi = pml_index(m, cx, cy, cz);
+    float *sp = m.split + pi;
+    const int64_t N = m.npml;
+    const float dl = ph.dt * l2m, dt = ph.dt;
+    float a0, a1, a2;
+    a0 = sp[S_XXX * N] = split_update(sp[S_XXX * N], dl, dXx, kx, mx, px);
+    a1 = sp[S_XXY * N] = split_update(sp[S_XXY * N], dt, l * dYy, ky, my, py);
+    a2 = sp[S_XXZ * N] = split_update(sp[S_XXZ * N], dt, l * dZz, kz, mz, pz);
+    m.f[3][ci] = (a0 + a1) + a2;
+    a0 = sp[S_YYX * N] = split_update(sp[S_YYX * N], dt, l * dXx, kx, mx, px);
+    a1 = sp[S_YYY * N] = split_update(sp[S_YYY * N], dl, dYy, ky, my, py);
+    a2 = sp[S_YYZ * N] = split_update(sp[S_YYZ * N], dt, l * dZz, kz, mz, pz);
+    m.f[4][ci] = (a0 + a1) + a2;
+    a0 = sp[S_ZZX * N] = split_update(sp[S_ZZX * N], dt, l * dXx, kx, mx, px);
+    a1 = sp[S_ZZY * N] = split_update(sp[S_ZZY * N], dt, l * dYy, ky, my, py);
+    a2 = sp[S_ZZZ * N] = split_update(sp[S_ZZZ * N], dl, dZz, kz, mz, pz);
+    m.f[5][ci] = (a0 + a1) + a2;
+    const float axy = dt * mxy, axz = dt * mxz, ayz = dt * myz;
+    a0 = sp[S_XYX * N] = split_update(sp[S_XYX * N], axy, xyX, kx, mx, px);
+    a1 = sp[S_XYY * N] = split_update(sp[S_XYY * N], axy, xyY, ky, my, py);
+    m.f[6][ci] = a0 + a1;
+    a0 = sp[S_XZX * N] = split_update(sp[S_XZX * N], axz, xzX, kx, mx, px);
+    a1 = sp[S_XZZ * N] = split_update(sp[S_XZZ * N], axz, xzZ, kz, mz, pz);
+    m.f[7][ci] = a0 + a1;
+    a0 = sp[S_YZY * N] = split_update(sp[S_YZY * N], ayz, yzY, ky, my, py);
+    a1 = sp[S_YZZ * N] = split_update(sp[S_YZZ * N], ayz, yzZ, kz, mz, pz);
+    m.f[8][ci] = a0 + a1;
+}
+
+// Receivers of one phase sample their component (ElasticWaveEquation.cu:223-232).
+__global__ void k_record(Model m, SourceRec sr, int it, int velocity_phase) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= sr.nrec || it < 0 || it >= sr.nt) return;
+    const int4 q = sr.rec[r];
+    if ((q.w <= 2) != (velocity_phase != 0)) return;
+    sr.traces[(int64_t)it * sr.nrec + r] = m.f[q.w][pidx(m, q.x, q.y, q.z)];
+}
+
+__global__ void k_reciprocal(float *rmu, const float *mu, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        rmu[i] = 1.0f / mu[i];   // 1 / mu (ElasticMacro.h:112)
+}
+
+}  // namespace
+
+int simple_launches_per_step(const SourceRec &sr) {
+    int n = 2;
+    if (sr.src >= 0) n += 1;
+    if (sr.nrec > 0) n += 2;
+    return n;
+}
+
+cudaError_t simple_step(const Model &m, const Physics &ph, const SourceRec &sr,
+                        int it, float src_value, bool use_wavelet, cudaStream_t s, cudaEvent_t *ev) {
+    if (sr.src >= 0) k_inject<<<1, 32, 0, s>>>(m, ph, sr, it, src_value, use_wavelet ? 1 : 0);
+    const dim3 block(kBX, kBY);
+    const dim3 grid((m.nxc + kBX - 1) / kBX, (m.nyc + kBY - 1) / kBY, m.nzc);
+    if (ev) cudaEventRecord(ev[0], s);
+    k_velocity<<<grid, block, 0, s>>>(m, ph);
+    if (ev) cudaEventRecord(ev[1], s);
+    if (sr.nrec > 0) k_record<<<(sr.nrec + 127) / 128, 128, 0, s>>>(m, sr, it, 1);
+    if (ev) cudaEventRecord(ev[2], s);
+    k_stress<<<grid, block, 0, s>>>(m, ph);
+    if (ev) cudaEventRecord(ev[3], s);
+    if (sr.nrec > 0) k_record<<<(sr.nrec + 127) / 128, 128, 0, s>>>(m, sr, it, 0);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_reciprocal(float *rmu, const float *mu, int64_t n, cudaStream_t s) {
+    k_reciprocal<<<1184, 256, 0, s>>>(rmu, mu, n);
+    return cudaGetLastError();
+}
+
+}  // namespace sgfd

@@ -1,0 +1,500 @@
+// sgfd_api.cu — the C ABI of include/sgfd.h: handle lifetime, device memory,
+// uploads/downloads and the time loop.  Kernels live in kernels_*.cu.
+//
+// Reference counterparts (3DGPUwithPML_1DArraySingleGPU_optimization/):
+//   sgfd_create    ElasticWaveEquation.cu:8-45 (ctor), :47-108 (region table)
+//   sgfd_set_medium ElasticWaveEquation.cu:143-147
+//   sgfd_step      ElasticWaveEquation.cu:191-204 (propagate)
+//   sgfd_run       ElasticWaveEquation.cu:153-172 (time loop of run())
+//   sgfd_get_traces ElasticWaveEquation.cu:174
+//   sgfd_destroy   ElasticWaveEquation.cu:125-138
+// Differences by design: status codes instead of exit(1) (OPT/common.h:6-16),
+// 64-bit sizes (the reference's int memsize overflows past 2^29 cells,
+// OPT/ElasticWaveEquation.cu:20), one stream per handle instead of a device
+// synchronisation per step (OPT/ElasticWaveEquation.cu:201).
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/sgfd.h"
+#include "sgfd_internal.h"
+
+using namespace sgfd;
+
+struct sgfd_solver {
+    sgfd_config cfg{};
+    Model m{};
+    Physics ph{};
+    SourceRec sr{};
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaStream_t own_stream = nullptr;
+    char *field_pool = nullptr;   // 9 fields + b, lambda, mu, 1/mu
+    float *split = nullptr;
+    int4 *rec = nullptr;
+    float *traces = nullptr;
+    float *wavelet = nullptr;
+    int wavelet_nt = 0;
+    bool medium_set = false;
+    int kernel = SGFD_KERNEL_SIMPLE;
+    std::string err;
+};
+
+namespace {
+
+thread_local std::string g_error;
+
+int fail(sgfd_solver *h, int code, const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    std::vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    if (h) h->err = buf; else g_error = buf;
+    return code;
+}
+
+int cuda_fail(sgfd_solver *h, cudaError_t e, const char *what) {
+    return fail(h, SGFD_ERR_CUDA, "%s: %s (%s)", what, cudaGetErrorName(e), cudaGetErrorString(e));
+}
+
+#define SG_CUDA(h, call, what)                          \
+    do {                                                \
+        cudaError_t e_ = (call);                        \
+        if (e_ != cudaSuccess) return cuda_fail(h, e_, what); \
+    } while (0)
+
+inline size_t round_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+bool finite_pos(float v) { return std::isfinite(v) && v > 0.0f; }
+
+void set_physics(sgfd_solver *h) {
+    const sgfd_config &c = h->cfg;
+    Physics &ph = h->ph;
+    for (int i = 0; i < 5; ++i) ph.c[i] = c.coef[i];
+    ph.dt = c.dt; ph.dx = c.dx; ph.dy = c.dy; ph.dz = c.dz;
+    ph.inj_dt2 = c.dt * c.dt;
+    ph.damping = c.damping;
+    ph.quirks = c.quirks;
+    const int p = c.pml;
+    ph.q_refgpu = 0.5f * c.dt * kTau;
+    ph.poly = (8.0f / 15.0f - 0.03f * (float)p) + (1.0f / 1500.0f) * (float)(p * p);
+    const double R = c.damping_R > 0 ? (double)c.damping_R : 1e-3;
+    ph.q_logr = (float)(0.5 * (double)c.dt * 3.0 * std::log(1.0 / R) / (2.0 * (double)p));
+    const double dd[3] = {c.dx, c.dy, c.dz};
+    for (int a = 0; a < 3; ++a)
+        ph.q_refcpu[a] = (float)(0.5 * (double)c.dt * std::log10(1.0 / R) * 3.4 *
+                                 (double)c.damping_vconst / ((double)p * dd[a]));
+    ph.inv_pml = 1.0f / (float)p;
+}
+
+int check_handle(sgfd_solver *h) {
+    if (!h) return fail(nullptr, SGFD_ERR_INVALID, "null handle");
+    cudaError_t e = cudaSetDevice(h->device);
+    if (e != cudaSuccess) return cuda_fail(h, e, "cudaSetDevice");
+    return SGFD_OK;
+}
+
+int launch_step(sgfd_solver *h, int it, float value, bool use_wavelet) {
+    cudaError_t e = simple_step(h->m, h->ph, h->sr, it, value, use_wavelet, h->stream);
+    if (e != cudaSuccess) return cuda_fail(h, e, "step launch");
+    return SGFD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sgfd_abi_version(void) { return SGFD_ABI_VERSION; }
+
+void sgfd_config_default(sgfd_config *cfg) {
+    if (!cfg) return;
+    std::memset(cfg, 0, sizeof *cfg);
+    cfg->nx = cfg->ny = cfg->nz = 64;
+    cfg->pml = 10;
+    cfg->dt = 0.0005f; cfg->dx = cfg->dy = cfg->dz = 10.0f;
+    // Coefficients of the reference driver (CON/main.cu:40-44).
+    const float c[5] = {1.21124f, -8.97217e-2f, 1.38428e-2f, -1.76566e-3f, 1.18680e-4f};
+    std::memcpy(cfg->coef, c, sizeof c);
+    cfg->damping = SGFD_DAMP_REFGPU;
+    cfg->damping_R = 0.001f;        // reference R (OPT/ElasticMacro.h:20)
+    cfg->damping_vconst = 2000.0f;  // reference CPU constant Vs
+    cfg->quirks = SGFD_QUIRKS_REF;
+    cfg->storage = SGFD_STORE_F32;
+    cfg->kernel = SGFD_KERNEL_AUTO;
+    cfg->device = 0;
+}
+
+const char *sgfd_global_error(void) { return g_error.c_str(); }
+
+const char *sgfd_last_error(const sgfd_solver *h) { return h ? h->err.c_str() : g_error.c_str(); }
+
+int sgfd_create(const sgfd_config *cfg, sgfd_solver **out) {
+    if (!cfg || !out) return fail(nullptr, SGFD_ERR_INVALID, "null config or output pointer");
+    *out = nullptr;
+    const sgfd_config &c = *cfg;
+    for (int i = 0; i < 8; ++i)
+        if (c.reserved[i] != 0) return fail(nullptr, SGFD_ERR_INVALID, "reserved config fields must be zero");
+    if (c.pml < 1) return fail(nullptr, SGFD_ERR_INVALID, "pml must be >= 1 (got %d)", c.pml);
+    const int need = 2 * (kHalo + c.pml) + 1;
+    if (c.nx < need || c.ny < need || c.nz < need)
+        return fail(nullptr, SGFD_ERR_INVALID, "grid %dx%dx%d too small for pml %d (each axis needs >= %d)",
+                    c.nx, c.ny, c.nz, c.pml, need);
+    if (!finite_pos(c.dt) || !finite_pos(c.dx) || !finite_pos(c.dy) || !finite_pos(c.dz))
+        return fail(nullptr, SGFD_ERR_INVALID, "dt, dx, dy, dz must be finite and positive");
+    for (int i = 0; i < 5; ++i)
+        if (!std::isfinite(c.coef[i])) return fail(nullptr, SGFD_ERR_INVALID, "non-finite coefficient %d", i);
+    if (c.damping < SGFD_DAMP_REFGPU || c.damping > SGFD_DAMP_REFCPU)
+        return fail(nullptr, SGFD_ERR_INVALID, "unknown damping profile %d", c.damping);
+    if ((c.damping != SGFD_DAMP_REFGPU) && !(c.damping_R > 0.0f && c.damping_R < 1.0f))
+        return fail(nullptr, SGFD_ERR_INVALID, "damping_R must be in (0, 1)");
+    if (c.quirks != SGFD_QUIRKS_REF && c.quirks != SGFD_QUIRKS_FIXED)
+        return fail(nullptr, SGFD_ERR_INVALID, "unknown quirks mode %d", c.quirks);
+    if (c.storage != SGFD_STORE_F32)
+        return fail(nullptr, SGFD_ERR_UNSUPPORTED, "storage type %d is not built into this library", c.storage);
+    if (c.kernel != SGFD_KERNEL_AUTO && c.kernel != SGFD_KERNEL_SIMPLE)
+        return fail(nullptr, SGFD_ERR_UNSUPPORTED, "kernel family %d is not built into this library", c.kernel);
+    const int64_t cells = (int64_t)c.nx * c.ny * c.nz;
+    if (cells > ((int64_t)1 << 36)) return fail(nullptr, SGFD_ERR_INVALID, "grid has too many cells");
+
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(nullptr, SGFD_ERR_NO_DEVICE, "no CUDA device available");
+    }
+    if (c.device < 0 || c.device >= ndev) return fail(nullptr, SGFD_ERR_INVALID, "device %d out of range", c.device);
+
+    sgfd_solver *h = new (std::nothrow) sgfd_solver();
+    if (!h) return fail(nullptr, SGFD_ERR_ALLOC, "host allocation failed");
+    h->cfg = c;
+    h->device = c.device;
+    h->kernel = SGFD_KERNEL_SIMPLE;
+    cudaError_t e = cudaSetDevice(h->device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&h->own_stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        int r = cuda_fail(nullptr, e, "device setup");
+        delete h;
+        return r;
+    }
+    h->stream = h->own_stream;
+
+    Model &m = h->m;
+    m.nx = c.nx; m.ny = c.ny; m.nz = c.nz;
+    m.px = (int)round_up((size_t)c.nx, 32);
+    m.pml = c.pml;
+    m.nxc = c.nx - 2 * kHalo; m.nyc = c.ny - 2 * kHalo; m.nzc = c.nz - 2 * kHalo;
+    m.plane = (int64_t)m.px * m.ny;
+    m.npml = pml_count(m.nxc, m.nyc, m.nzc, m.pml);
+    const size_t arr_bytes = round_up((size_t)m.plane * m.nz * sizeof(float), 256);
+    const size_t pool_bytes = arr_bytes * 13;
+    e = cudaMalloc(&h->field_pool, pool_bytes);
+    if (e == cudaSuccess) e = cudaMalloc(&h->split, (size_t)kNumSplit * m.npml * sizeof(float));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        int r = fail(nullptr, SGFD_ERR_ALLOC, "device allocation of %.2f GB failed",
+                     (pool_bytes + (double)kNumSplit * m.npml * 4) / 1e9);
+        sgfd_destroy(h);
+        return r;
+    }
+    for (int k = 0; k < 9; ++k) m.f[k] = reinterpret_cast<float *>(h->field_pool + k * arr_bytes);
+    m.b = reinterpret_cast<float *>(h->field_pool + 9 * arr_bytes);
+    m.lam = reinterpret_cast<float *>(h->field_pool + 10 * arr_bytes);
+    m.mu = reinterpret_cast<float *>(h->field_pool + 11 * arr_bytes);
+    m.rmu = reinterpret_cast<float *>(h->field_pool + 12 * arr_bytes);
+    m.split = h->split;
+    e = cudaMemsetAsync(h->field_pool, 0, pool_bytes, h->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(h->split, 0, (size_t)kNumSplit * m.npml * sizeof(float), h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) {
+        int r = cuda_fail(nullptr, e, "zeroing device state");
+        sgfd_destroy(h);
+        return r;
+    }
+    set_physics(h);
+    h->sr.src = -1;
+    h->sr.nrec = 0;
+    *out = h;
+    return SGFD_OK;
+}
+
+void sgfd_destroy(sgfd_solver *h) {
+    if (!h) return;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    cudaFree(h->field_pool);
+    cudaFree(h->split);
+    cudaFree(h->rec);
+    cudaFree(h->traces);
+    cudaFree(h->wavelet);
+    if (h->own_stream) cudaStreamDestroy(h->own_stream);
+    delete h;
+}
+
+int sgfd_set_stream(sgfd_solver *h, void *stream) {
+    int r = check_handle(h);
+    if (r) return r;
+    SG_CUDA(h, cudaStreamSynchronize(h->stream), "synchronising previous stream");
+    h->stream = stream ? static_cast<cudaStream_t>(stream) : h->own_stream;
+    return SGFD_OK;
+}
+
+static int upload_medium(sgfd_solver *h, const float *b, const float *l, const float *mu, cudaMemcpyKind kind) {
+    int r = check_handle(h);
+    if (r) return r;
+    if (!b || !l || !mu) return fail(h, SGFD_ERR_INVALID, "null medium array");
+    const Model &m = h->m;
+    const size_t row = (size_t)m.nx * sizeof(float);
+    const size_t rows = (size_t)m.ny * m.nz;
+    const float *src[3] = {b, l, mu};
+    float *dst[3] = {const_cast<float *>(m.b), const_cast<float *>(m.lam), const_cast<float *>(m.mu)};
+    for (int k = 0; k < 3; ++k)
+        SG_CUDA(h, cudaMemcpy2DAsync(dst[k], (size_t)m.px * sizeof(float), src[k], row, row, rows, kind, h->stream),
+                "medium upload");
+    cudaError_t e = launch_reciprocal(const_cast<float *>(m.rmu), m.mu, m.plane * m.nz, h->stream);
+    if (e != cudaSuccess) return cuda_fail(h, e, "reciprocal kernel");
+    SG_CUDA(h, cudaStreamSynchronize(h->stream), "medium upload");
+    h->medium_set = true;
+    return SGFD_OK;
+}
+
+int sgfd_set_medium(sgfd_solver *h, const float *b, const float *l, const float *mu) {
+    return upload_medium(h, b, l, mu, cudaMemcpyHostToDevice);
+}
+
+int sgfd_set_medium_device(sgfd_solver *h, const float *b, const float *l, const float *mu) {
+    return upload_medium(h, b, l, mu, cudaMemcpyDeviceToDevice);
+}
+
+int sgfd_set_source(sgfd_solver *h, int32_t x, int32_t y, int32_t z) {
+    int r = check_handle(h);
+    if (r) return r;
+    const Model &m = h->m;
+    if (x < kHalo || y < kHalo || z < kHalo || x >= m.nx - kHalo || y >= m.ny - kHalo || z >= m.nz - kHalo)
+        return fail(h, SGFD_ERR_INVALID, "source (%d,%d,%d) outside the computed region [5, n-5)", x, y, z);
+    h->sr.src = pidx(m, x, y, z);
+    return SGFD_OK;
+}
+
+int sgfd_set_receivers(sgfd_solver *h, int32_t n, const int32_t *xyz, const int32_t *comp, int32_t nt) {
+    int r = check_handle(h);
+    if (r) return r;
+    if (n < 0 || (n > 0 && (!xyz || !comp || nt < 1)))
+        return fail(h, SGFD_ERR_INVALID, "bad receiver arguments (n=%d, nt=%d)", n, nt);
+    const Model &m = h->m;
+    std::vector<int4> host(n);
+    for (int i = 0; i < n; ++i) {
+        const int x = xyz[3 * i], y = xyz[3 * i + 1], z = xyz[3 * i + 2], c = comp[i];
+        if (x < 0 || y < 0 || z < 0 || x >= m.nx || y >= m.ny || z >= m.nz)
+            return fail(h, SGFD_ERR_INVALID, "receiver %d at (%d,%d,%d) outside the grid", i, x, y, z);
+        if (c < 0 || c >= SGFD_NFIELDS) return fail(h, SGFD_ERR_INVALID, "receiver %d: bad component %d", i, c);
+        host[i] = make_int4(x, y, z, c);
+    }
+    SG_CUDA(h, cudaStreamSynchronize(h->stream), "synchronise before receiver update");
+    cudaFree(h->rec);
+    cudaFree(h->traces);
+    h->rec = nullptr;
+    h->traces = nullptr;
+    h->sr.nrec = 0;
+    h->sr.nt = 0;
+    if (n > 0) {
+        const size_t tbytes = (size_t)n * nt * sizeof(float);
+        cudaError_t e = cudaMalloc(&h->rec, n * sizeof(int4));
+        if (e == cudaSuccess) e = cudaMalloc(&h->traces, tbytes);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return fail(h, SGFD_ERR_ALLOC, "receiver buffers (%zu bytes)", tbytes);
+        }
+        SG_CUDA(h, cudaMemcpy(h->rec, host.data(), n * sizeof(int4), cudaMemcpyHostToDevice), "receiver upload");
+        SG_CUDA(h, cudaMemset(h->traces, 0, tbytes), "trace clear");
+    }
+    h->sr.nrec = n;
+    h->sr.nt = n > 0 ? nt : 0;
+    h->sr.rec = h->rec;
+    h->sr.traces = h->traces;
+    return SGFD_OK;
+}
+
+int sgfd_set_wavelet(sgfd_solver *h, int32_t nt, const float *values) {
+    int r = check_handle(h);
+    if (r) return r;
+    if (nt < 1 || !values) return fail(h, SGFD_ERR_INVALID, "bad wavelet");
+    SG_CUDA(h, cudaStreamSynchronize(h->stream), "synchronise before wavelet update");
+    if (nt > h->wavelet_nt) {
+        cudaFree(h->wavelet);
+        h->wavelet = nullptr;
+        cudaError_t e = cudaMalloc(&h->wavelet, (size_t)nt * sizeof(float));
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            h->wavelet_nt = 0;
+            return fail(h, SGFD_ERR_ALLOC, "wavelet buffer");
+        }
+    }
+    h->wavelet_nt = nt;
+    SG_CUDA(h, cudaMemcpy(h->wavelet, values, (size_t)nt * sizeof(float), cudaMemcpyHostToDevice), "wavelet upload");
+    h->sr.wavelet = h->wavelet;
+    return SGFD_OK;
+}
+
+int sgfd_step(sgfd_solver *h, int32_t it, float source_value) {
+    int r = check_handle(h);
+    if (r) return r;
+    if (!h->medium_set) return fail(h, SGFD_ERR_STATE, "sgfd_set_medium must come before stepping");
+    return launch_step(h, it, source_value, false);
+}
+
+int sgfd_run(sgfd_solver *h, int32_t it0, int32_t nsteps, int32_t use_graph) {
+    (void)use_graph;
+    int r = check_handle(h);
+    if (r) return r;
+    if (!h->medium_set) return fail(h, SGFD_ERR_STATE, "sgfd_set_medium must come before stepping");
+    if (nsteps < 0 || it0 < 0) return fail(h, SGFD_ERR_INVALID, "bad step range");
+    if (h->sr.src >= 0 && (int64_t)it0 + nsteps > h->wavelet_nt)
+        return fail(h, SGFD_ERR_STATE, "wavelet covers %d steps, run needs %d", h->wavelet_nt, it0 + nsteps);
+    for (int it = it0; it < it0 + nsteps; ++it) {
+        r = launch_step(h, it, 0.0f, true);
+        if (r) return r;
+    }
+    return SGFD_OK;
+}
+
+int sgfd_synchronize(sgfd_solver *h) {
+    int r = check_handle(h);
+    if (r) return r;
+    SG_CUDA(h, cudaStreamSynchronize(h->stream), "synchronize");
+    return SGFD_OK;
+}
+
+int sgfd_reset(sgfd_solver *h) {
+    int r = check_handle(h);
+    if (r) return r;
+    const Model &m = h->m;
+    const size_t arr_bytes = round_up((size_t)m.plane * m.nz * sizeof(float), 256);
+    SG_CUDA(h, cudaMemsetAsync(h->field_pool, 0, arr_bytes * 9, h->stream), "reset fields");
+    SG_CUDA(h, cudaMemsetAsync(h->split, 0, (size_t)kNumSplit * m.npml * sizeof(float), h->stream), "reset splits");
+    if (h->traces)
+        SG_CUDA(h, cudaMemsetAsync(h->traces, 0, (size_t)h->sr.nrec * h->sr.nt * sizeof(float), h->stream), "reset traces");
+    SG_CUDA(h, cudaStreamSynchronize(h->stream), "reset");
+    return SGFD_OK;
+}
+
+int sgfd_get_traces(sgfd_solver *h, float *out) {
+    int r = check_handle(h);
+    if (r) return r;
+    if (!out) return fail(h, SGFD_ERR_INVALID, "null output");
+    const int n = h->sr.nrec, nt = h->sr.nt;
+    if (n == 0) return SGFD_OK;
+    // device traces are time-major [it][r]; the ABI returns receiver-major [r][it]
+    std::vector<float> tm((size_t)n * nt);
+    SG_CUDA(h, cudaMemcpyAsync(tm.data(), h->traces, tm.size() * sizeof(float), cudaMemcpyDeviceToHost, h->stream),
+            "trace download");
+    SG_CUDA(h, cudaStreamSynchronize(h->stream), "trace download");
+    for (int it = 0; it < nt; ++it)
+        for (int q = 0; q < n; ++q) out[(size_t)q * nt + it] = tm[(size_t)it * n + q];
+    return SGFD_OK;
+}
+
+int sgfd_get_trace_step(sgfd_solver *h, int32_t it, float *out) {
+    int r = check_handle(h);
+    if (r) return r;
+    if (!out) return fail(h, SGFD_ERR_INVALID, "null output");
+    if (it < 0 || it >= h->sr.nt) return fail(h, SGFD_ERR_INVALID, "step %d outside the trace length %d", it, h->sr.nt);
+    SG_CUDA(h, cudaMemcpyAsync(out, h->traces + (size_t)it * h->sr.nrec, (size_t)h->sr.nrec * sizeof(float),
+                               cudaMemcpyDeviceToHost, h->stream), "trace step download");
+    SG_CUDA(h, cudaStreamSynchronize(h->stream), "trace step download");
+    return SGFD_OK;
+}
+
+int sgfd_profile(sgfd_solver *h, int32_t it0, int32_t nsteps, float *ms_velocity, float *ms_stress) {
+    int r = check_handle(h);
+    if (r) return r;
+    if (!h->medium_set) return fail(h, SGFD_ERR_STATE, "sgfd_set_medium must come before stepping");
+    if (nsteps < 1 || it0 < 0) return fail(h, SGFD_ERR_INVALID, "bad step range");
+    if (h->sr.src >= 0 && (int64_t)it0 + nsteps > h->wavelet_nt)
+        return fail(h, SGFD_ERR_STATE, "wavelet covers %d steps, profile needs %d", h->wavelet_nt, it0 + nsteps);
+    cudaEvent_t ev[4];
+    for (int k = 0; k < 4; ++k) SG_CUDA(h, cudaEventCreate(&ev[k]), "event create");
+    double tv = 0, ts = 0;
+    int rc = SGFD_OK;
+    for (int it = it0; it < it0 + nsteps && rc == SGFD_OK; ++it) {
+        cudaError_t e = simple_step(h->m, h->ph, h->sr, it, 0.0f, true, h->stream, ev);
+        if (e == cudaSuccess) e = cudaEventSynchronize(ev[3]);
+        float a = 0, b = 0;
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&a, ev[0], ev[1]);
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&b, ev[2], ev[3]);
+        if (e != cudaSuccess) rc = cuda_fail(h, e, "profiled step");
+        tv += a; ts += b;
+    }
+    for (int k = 0; k < 4; ++k) cudaEventDestroy(ev[k]);
+    if (ms_velocity) *ms_velocity = (float)tv;
+    if (ms_stress) *ms_stress = (float)ts;
+    return rc;
+}
+
+static int download(sgfd_solver *h, const float *src, float *out) {
+    const Model &m = h->m;
+    const size_t row = (size_t)m.nx * sizeof(float);
+    SG_CUDA(h, cudaMemcpy2DAsync(out, row, src, (size_t)m.px * sizeof(float), row, (size_t)m.ny * m.nz,
+                                 cudaMemcpyDeviceToHost, h->stream), "field download");
+    SG_CUDA(h, cudaStreamSynchronize(h->stream), "field download");
+    return SGFD_OK;
+}
+
+int sgfd_get_field(sgfd_solver *h, int32_t field, float *out) {
+    int r = check_handle(h);
+    if (r) return r;
+    if (!out) return fail(h, SGFD_ERR_INVALID, "null output");
+    if (field < 0 || field >= SGFD_NFIELDS) return fail(h, SGFD_ERR_INVALID, "bad field id %d", field);
+    return download(h, h->m.f[field], out);
+}
+
+int sgfd_get_medium(sgfd_solver *h, int32_t which, float *out) {
+    int r = check_handle(h);
+    if (r) return r;
+    if (!out) return fail(h, SGFD_ERR_INVALID, "null output");
+    const float *src = which == SGFD_BUOYANCY ? h->m.b : which == SGFD_LAMBDA ? h->m.lam
+                     : which == SGFD_MU ? h->m.mu : nullptr;
+    if (!src) return fail(h, SGFD_ERR_INVALID, "bad medium id %d", which);
+    return download(h, src, out);
+}
+
+// Ricker wavelet of the reference (OPT/ElasticWaveEquation.cu:184-189): the
+// reference squares with pow(float, 2) in double precision and rounds to
+// float, which equals the float product a*a.
+float sgfd_ricker_ref(float f0, float dt, int32_t it) {
+    const float pi = 3.1415926f;   // reference PI (OPT/ElasticMacro.h:19)
+    const float t0 = std::ceil(1.0f / (f0 * dt));
+    const float a = pi * f0 * (((float)it - t0) * dt - 1.0f / f0);
+    const float a2 = (float)((double)a * (double)a);
+    return (1.0f - 2.0f * a2) * std::exp(-a2);
+}
+
+float sgfd_ricker_t0(float f0, float dt, float t0, int32_t it) {
+    const double a = 3.14159265358979323846 * (double)f0 * ((double)it * (double)dt - (double)t0);
+    const double a2 = a * a;
+    return (float)((1.0 - 2.0 * a2) * std::exp(-a2));
+}
+
+int sgfd_cell_counts(const sgfd_solver *h, int64_t *n_interior, int64_t *n_pml) {
+    if (!h) return SGFD_ERR_INVALID;
+    const Model &m = h->m;
+    const int64_t total = (int64_t)m.nxc * m.nyc * m.nzc;
+    if (n_pml) *n_pml = m.npml;
+    if (n_interior) *n_interior = total - m.npml;
+    return SGFD_OK;
+}
+
+int sgfd_launches_per_step(const sgfd_solver *h) {
+    if (!h) return -1;
+    return simple_launches_per_step(h->sr);
+}
+
+const char *sgfd_kernel_name(const sgfd_solver *h) {
+    if (!h) return "";
+    return h->kernel == SGFD_KERNEL_ZMARCH ? "zmarch" : "simple";
+}
+
+}  // extern "C"

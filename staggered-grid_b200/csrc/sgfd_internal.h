@@ -1,0 +1,123 @@
+// sgfd_internal.h — device data layout and launch parameters shared by the
+// host API (sgfd_api.cu) and the kernel families (kernels_*.cu).
+//
+// HBM layout of one model
+//   * 9 wavefields + buoyancy, lambda, mu: one array each, x fastest, the
+//     reference GRID (5-cell frame included), rows padded to a pitch `px`
+//     that is a multiple of 32 floats so every row starts on a 128-byte
+//     boundary (coalescing, and the 16-byte rule of TMA tensor maps).
+//     index(ix, iy, iz) = ix + iy*px + iz*px*ny.
+//   * PML split fields: a compact array of the PML cells only, 24 splits as
+//     structure-of-arrays, split k of PML cell c at split[k*npml + c].  PML
+//     cells are enumerated plane by plane (z slowest), and within a plane row
+//     by row, x fastest, so a warp reading consecutive x reads consecutive
+//     addresses (pml_index()).  The reference keeps 26 region arrays of
+//     (len+1)^3 each (OPT/ElasticWaveEquation.cu:34-41).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace sgfd {
+
+constexpr int kHalo = 5;            // reference `order` (OPT/ElasticMacro.h:24)
+constexpr int kNumSplit = 24;
+constexpr int kNumVelSplit = 9;     // velocity splits come first
+constexpr float kTau = 4.3f;        // reference `tau` (OPT/ElasticMacro.h:21)
+
+// Split ids (velocity q,axis then stress), same order as the oracle.
+enum SplitId {
+    S_VXX, S_VXY, S_VXZ, S_VYX, S_VYY, S_VYZ, S_VZX, S_VZY, S_VZZ,
+    S_XXX, S_XXY, S_XXZ, S_YYX, S_YYY, S_YYZ, S_ZZX, S_ZZY, S_ZZZ,
+    S_XYX, S_XYY, S_XZX, S_XZZ, S_YZY, S_YZZ
+};
+
+// Per-step physics constants (all FP32, computed once on the host).
+struct Physics {
+    float c[5];          // staggered coefficients
+    float dt, dx, dy, dz;
+    float inj_dt2;       // dt*dt (source scale, OPT/ElasticWaveEquation.cu:213)
+    int damping;         // sgfd_damping
+    int quirks;          // sgfd_quirks
+    float q_refgpu;      // (0.5*dt)*tau
+    float poly;          // 8/15 - 0.03 p + p^2/1500
+    float q_logr;        // 0.5*dt*3*ln(1/R)/(2p)
+    float q_refcpu[3];   // 0.5*dt*log10(1/R)*3.4*V/(p*d)
+    float inv_pml;       // unused by the arithmetic; kept for diagnostics
+};
+
+// Geometry and device pointers of one model.
+struct Model {
+    int nx, ny, nz;      // GRID (frame included)
+    int px;              // row pitch in floats
+    int pml;
+    int nxc, nyc, nzc;   // computed extents (n - 10)
+    int64_t plane;       // px * ny
+    int64_t npml;        // number of PML cells
+    float *f[9];         // vx vy vz txx tyy tzz txy txz tyz
+    const float *b, *lam, *mu, *rmu;   // rmu = 1/mu
+    float *split;        // kNumSplit * npml
+};
+
+// Source (one explosive point) and receivers.
+struct SourceRec {
+    int64_t src;         // padded index of the source cell, -1 if none
+    const float *wavelet;// device wavelet (sgfd_run) or nullptr
+    int nrec;
+    const int4 *rec;     // x, y, z, comp
+    float *traces;       // time-major: traces[it * nrec + r]
+    int nt;
+};
+
+__host__ __device__ inline int64_t pidx(const Model &m, int x, int y, int z) {
+    return (int64_t)x + (int64_t)y * m.px + (int64_t)z * m.plane;
+}
+
+// Band distance along one axis: 0 outside the PML band, else 1..pml counted
+// from the inner edge (OPT/ElasticWaveEquation.cu:283-285 `end - i`,
+// :297 `i - start + 1`).
+__host__ __device__ inline int band(int i, int n, int pml) {
+    if (i < kHalo + pml) return kHalo + pml - i;
+    if (i >= n - kHalo - pml) return i - (n - kHalo - pml) + 1;
+    return 0;
+}
+
+// Compact index of a PML cell given computed coordinates (cx, cy, cz).
+__host__ __device__ inline int64_t pml_index(const Model &m, int cx, int cy, int cz) {
+    const int p = m.pml;
+    const int64_t full = (int64_t)m.nxc * m.nyc;
+    const int64_t ring = (int64_t)2 * p * m.nxc + (int64_t)(m.nyc - 2 * p) * 2 * p;
+    int64_t base;
+    bool full_plane;
+    if (cz < p) { base = cz * full; full_plane = true; }
+    else if (cz < m.nzc - p) { base = p * full + (int64_t)(cz - p) * ring; full_plane = false; }
+    else { base = p * full + (int64_t)(m.nzc - 2 * p) * ring + (int64_t)(cz - (m.nzc - p)) * full; full_plane = true; }
+    if (full_plane) return base + (int64_t)cy * m.nxc + cx;
+    if (cy < p) return base + (int64_t)cy * m.nxc + cx;
+    if (cy < m.nyc - p) {
+        const int off = cx < p ? cx : cx - (m.nxc - 2 * p);
+        return base + (int64_t)p * m.nxc + (int64_t)(cy - p) * 2 * p + off;
+    }
+    return base + (int64_t)p * m.nxc + (int64_t)(m.nyc - 2 * p) * 2 * p + (int64_t)(cy - (m.nyc - p)) * m.nxc + cx;
+}
+
+__host__ inline int64_t pml_count(int nxc, int nyc, int nzc, int p) {
+    const int64_t full = (int64_t)nxc * nyc;
+    const int64_t ring = (int64_t)2 * p * nxc + (int64_t)(nyc - 2 * p) * 2 * p;
+    return 2 * p * full + (int64_t)(nzc - 2 * p) * ring;
+}
+
+// ---- kernel family entry points (host side) -------------------------------
+
+// "simple": one thread per computed cell.
+// ev (optional, 4 events): recorded before/after the velocity kernel and
+// before/after the stress kernel.
+cudaError_t simple_step(const Model &m, const Physics &ph, const SourceRec &sr,
+                        int it, float src_value, bool use_wavelet, cudaStream_t s,
+                        cudaEvent_t *ev = nullptr);
+int simple_launches_per_step(const SourceRec &sr);
+
+// medium post-processing: rmu = 1/mu over the padded arrays.
+cudaError_t launch_reciprocal(float *rmu, const float *mu, int64_t n, cudaStream_t s);
+
+}  // namespace sgfd

@@ -1,0 +1,260 @@
+"""Python binding of libsgfd.so (include/sgfd.h) for tests, benchmarks and scripting.
+
+The product is the C ABI and its CUDA kernels; this module is a thin ctypes
+layer over it.  There is no CPU code path: if the shared library is missing
+or no CUDA device is present, creating a Solver raises.
+
+Typical use (mirrors the reference driver 3DGPUwithPML_1DArraySingleGPU_concise/main.cu:11-79):
+
+    cfg = sgfd.default_config(nx=300, ny=200, nz=100, pml=10, dt=5e-4)
+    s = sgfd.Solver(cfg)
+    s.set_medium(b, lam, mu)               # float32 arrays of nx*ny*nz, x fastest
+    s.set_source(150, 100, 50)
+    s.set_receivers([[160, 110, 60]], [sgfd.TXX], nt=1500)
+    s.set_wavelet(sgfd.ricker_ref(20.0, 5e-4, 1500))
+    s.run(0, 1500); s.synchronize()
+    trace = s.traces()[0]
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(_PKG), "lib", "libsgfd.so")
+
+VX, VY, VZ, TXX, TYY, TZZ, TXY, TXZ, TYZ = range(9)
+FIELD_NAMES = ["vx", "vy", "vz", "txx", "tyy", "tzz", "txy", "txz", "tyz"]
+BUOYANCY, LAMBDA, MU = range(3)
+DAMP_REFGPU, DAMP_LOGR, DAMP_REFCPU = range(3)
+QUIRKS_REF, QUIRKS_FIXED = range(2)
+STORE_F32, STORE_BF16, STORE_F16 = range(3)
+KERNEL_AUTO, KERNEL_SIMPLE, KERNEL_ZMARCH = range(3)
+
+# sgfd_status
+OK, ERR_INVALID, ERR_ALLOC, ERR_CUDA, ERR_STATE, ERR_UNSUPPORTED, ERR_NO_DEVICE, ERR_NONFINITE = range(8)
+
+REF_COEF = (1.21124, -8.97217e-2, 1.38428e-2, -1.76566e-3, 1.18680e-4)
+
+
+class Config(ctypes.Structure):
+    """sgfd_config (include/sgfd.h)."""
+    _fields_ = [
+        ("nx", ctypes.c_int32), ("ny", ctypes.c_int32), ("nz", ctypes.c_int32),
+        ("pml", ctypes.c_int32),
+        ("dt", ctypes.c_float), ("dx", ctypes.c_float), ("dy", ctypes.c_float), ("dz", ctypes.c_float),
+        ("coef", ctypes.c_float * 5),
+        ("damping", ctypes.c_int32), ("damping_R", ctypes.c_float), ("damping_vconst", ctypes.c_float),
+        ("quirks", ctypes.c_int32), ("storage", ctypes.c_int32), ("kernel", ctypes.c_int32),
+        ("device", ctypes.c_int32), ("reserved", ctypes.c_int32 * 8),
+    ]
+
+
+class SgfdError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"sgfd error {code}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    """Load libsgfd.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with `make -C staggered-grid_b200` "
+                          "or __graft_entry__.build()")
+    L = ctypes.CDLL(LIB_PATH)
+    vp, fp, ip = ctypes.c_void_p, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_int32)
+    i32 = ctypes.c_int32
+    sigs = {
+        "sgfd_abi_version": (ctypes.c_int, []),
+        "sgfd_config_default": (None, [ctypes.POINTER(Config)]),
+        "sgfd_create": (ctypes.c_int, [ctypes.POINTER(Config), ctypes.POINTER(vp)]),
+        "sgfd_destroy": (None, [vp]),
+        "sgfd_last_error": (ctypes.c_char_p, [vp]),
+        "sgfd_global_error": (ctypes.c_char_p, []),
+        "sgfd_set_stream": (ctypes.c_int, [vp, vp]),
+        "sgfd_set_medium": (ctypes.c_int, [vp, fp, fp, fp]),
+        "sgfd_set_medium_device": (ctypes.c_int, [vp, vp, vp, vp]),
+        "sgfd_set_source": (ctypes.c_int, [vp, i32, i32, i32]),
+        "sgfd_set_receivers": (ctypes.c_int, [vp, i32, ip, ip, i32]),
+        "sgfd_set_wavelet": (ctypes.c_int, [vp, i32, fp]),
+        "sgfd_step": (ctypes.c_int, [vp, i32, ctypes.c_float]),
+        "sgfd_run": (ctypes.c_int, [vp, i32, i32, i32]),
+        "sgfd_synchronize": (ctypes.c_int, [vp]),
+        "sgfd_reset": (ctypes.c_int, [vp]),
+        "sgfd_get_traces": (ctypes.c_int, [vp, fp]),
+        "sgfd_get_trace_step": (ctypes.c_int, [vp, i32, fp]),
+        "sgfd_profile": (ctypes.c_int, [vp, i32, i32, fp, fp]),
+        "sgfd_get_field": (ctypes.c_int, [vp, i32, fp]),
+        "sgfd_get_medium": (ctypes.c_int, [vp, i32, fp]),
+        "sgfd_ricker_ref": (ctypes.c_float, [ctypes.c_float, ctypes.c_float, i32]),
+        "sgfd_ricker_t0": (ctypes.c_float, [ctypes.c_float, ctypes.c_float, ctypes.c_float, i32]),
+        "sgfd_cell_counts": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)]),
+        "sgfd_launches_per_step": (ctypes.c_int, [vp]),
+        "sgfd_kernel_name": (ctypes.c_char_p, [vp]),
+    }
+    for name, (res, args) in sigs.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def _fptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+
+
+def default_config(**kw) -> Config:
+    c = Config()
+    lib().sgfd_config_default(ctypes.byref(c))
+    for k, v in kw.items():
+        if k == "coef":
+            for i in range(5):
+                c.coef[i] = float(v[i])
+        elif not hasattr(c, k):
+            raise KeyError(k)
+        else:
+            setattr(c, k, v)
+    return c
+
+
+def config_dict(c: Config) -> dict:
+    d = {k: getattr(c, k) for k, _ in Config._fields_ if k not in ("coef", "reserved")}
+    d["coef"] = [c.coef[i] for i in range(5)]
+    return d
+
+
+def ricker_ref(f0: float, dt: float, nt: int) -> np.ndarray:
+    """Reference Ricker values s(it), it = 0..nt-1 (OPT/ElasticWaveEquation.cu:184-189)."""
+    L = lib()
+    return np.array([L.sgfd_ricker_ref(f0, dt, i) for i in range(nt)], dtype=np.float32)
+
+
+def ricker_t0(f0: float, dt: float, t0: float, nt: int) -> np.ndarray:
+    L = lib()
+    return np.array([L.sgfd_ricker_t0(f0, dt, t0, i) for i in range(nt)], dtype=np.float32)
+
+
+class Solver:
+    """One model on one GPU (an sgfd_solver handle)."""
+
+    def __init__(self, cfg: Config):
+        self.cfg = cfg
+        self.shape = (cfg.nz, cfg.ny, cfg.nx)
+        h = ctypes.c_void_p()
+        rc = lib().sgfd_create(ctypes.byref(cfg), ctypes.byref(h))
+        if rc != OK:
+            raise SgfdError(rc, lib().sgfd_global_error().decode())
+        self.h = h
+        self.nrec = 0
+        self.nt = 0
+
+    def _check(self, rc: int):
+        if rc != OK:
+            raise SgfdError(rc, lib().sgfd_last_error(self.h).decode())
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().sgfd_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def set_stream(self, stream_ptr: int | None):
+        self._check(lib().sgfd_set_stream(self.h, stream_ptr))
+
+    def set_medium(self, b, lam, mu):
+        arrs = [np.ascontiguousarray(a, dtype=np.float32).reshape(-1) for a in (b, lam, mu)]
+        n = int(np.prod(self.shape))
+        if any(a.size != n for a in arrs):
+            raise ValueError(f"medium arrays must have {n} cells")
+        self._check(lib().sgfd_set_medium(self.h, *[_fptr(a) for a in arrs]))
+
+    def set_medium_device(self, b_ptr: int, lam_ptr: int, mu_ptr: int):
+        self._check(lib().sgfd_set_medium_device(self.h, b_ptr, lam_ptr, mu_ptr))
+
+    def set_source(self, x: int, y: int, z: int):
+        self._check(lib().sgfd_set_source(self.h, x, y, z))
+
+    def set_receivers(self, xyz, comp, nt: int):
+        xyz = np.ascontiguousarray(np.asarray(xyz, dtype=np.int32).reshape(-1, 3))
+        comp = np.ascontiguousarray(np.asarray(comp, dtype=np.int32).reshape(-1))
+        if len(xyz) != len(comp):
+            raise ValueError("one component per receiver")
+        self._check(lib().sgfd_set_receivers(
+            self.h, len(comp), xyz.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+            comp.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), nt))
+        self.nrec, self.nt = len(comp), nt
+
+    def set_wavelet(self, w):
+        w = np.ascontiguousarray(w, dtype=np.float32)
+        self._check(lib().sgfd_set_wavelet(self.h, len(w), _fptr(w)))
+
+    def step(self, it: int, value: float):
+        self._check(lib().sgfd_step(self.h, it, value))
+
+    def run(self, it0: int, nsteps: int, graph: bool = True):
+        self._check(lib().sgfd_run(self.h, it0, nsteps, 1 if graph else 0))
+
+    def synchronize(self):
+        self._check(lib().sgfd_synchronize(self.h))
+
+    def reset(self):
+        self._check(lib().sgfd_reset(self.h))
+
+    def traces(self) -> np.ndarray:
+        out = np.zeros((self.nrec, self.nt), dtype=np.float32)
+        if self.nrec:
+            self._check(lib().sgfd_get_traces(self.h, _fptr(out)))
+        return out
+
+    def trace_step(self, it: int, out: np.ndarray | None = None) -> np.ndarray:
+        if out is None:
+            out = np.zeros(self.nrec, dtype=np.float32)
+        self._check(lib().sgfd_get_trace_step(self.h, it, _fptr(out)))
+        return out
+
+    def profile(self, it0: int, nsteps: int) -> tuple[float, float]:
+        """(ms in velocity kernels, ms in stress kernels) over nsteps steps."""
+        a, b = ctypes.c_float(), ctypes.c_float()
+        self._check(lib().sgfd_profile(self.h, it0, nsteps, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+    def field(self, fid: int) -> np.ndarray:
+        out = np.zeros(self.shape, dtype=np.float32)
+        self._check(lib().sgfd_get_field(self.h, fid, _fptr(out)))
+        return out
+
+    def medium(self, which: int) -> np.ndarray:
+        out = np.zeros(self.shape, dtype=np.float32)
+        self._check(lib().sgfd_get_medium(self.h, which, _fptr(out)))
+        return out
+
+    def cell_counts(self) -> tuple[int, int]:
+        a, b = ctypes.c_int64(), ctypes.c_int64()
+        self._check(lib().sgfd_cell_counts(self.h, ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
+
+    def launches_per_step(self) -> int:
+        return lib().sgfd_launches_per_step(self.h)
+
+    def kernel_name(self) -> str:
+        return lib().sgfd_kernel_name(self.h).decode()

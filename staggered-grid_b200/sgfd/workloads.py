@@ -1,0 +1,175 @@
+"""Workload builders: grids, media, sources, receivers and wavelets.
+
+Each builder returns a `Workload` holding everything a Solver (or the CPU
+oracle) needs.  Sizes follow the reference GRID convention (5-cell frame
+included on every side).
+
+* `reference_case()` — the reference driver's configuration
+  (3DGPUwithPML_1DArraySingleGPU_concise/main.cu:11-56), whose station trace
+  ships as CON/stationData.txt.
+* `plain_cube()` — homogeneous cube, interior n^3 + PML (configuration
+  "plain method, CPU-runnable": 100^3 + 20-cell PML, 101 vx/vz receivers).
+* `random_cube()` — random-medium cube (configuration "plain method on GPU":
+  344^3 + 20-cell PML, 64x64 receivers recording vx, vy, vz).
+* `gaussian_random_field()` — seeded Gaussian-correlated perturbation used
+  for the random media; it stands in for the reference's MATLAB generator
+  randomMedium/RandomMedia_3_d.m:1-103, which uses another spectrum.
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+
+import numpy as np
+
+from . import (DAMP_LOGR, DAMP_REFGPU, QUIRKS_FIXED, QUIRKS_REF, REF_COEF, TXX, VX, VY, VZ)
+
+HALO = 5
+
+
+@dataclasses.dataclass
+class Workload:
+    name: str
+    cfg: dict                      # sgfd_config fields
+    b: np.ndarray                  # float32, (nz, ny, nx)
+    lam: np.ndarray
+    mu: np.ndarray
+    src: tuple
+    rec_xyz: np.ndarray            # (n, 3) int32
+    rec_comp: np.ndarray           # (n,) int32
+    nt: int
+    wavelet: np.ndarray            # float32 (nt,)
+    wavelet64: np.ndarray          # float64 (nt,) for FP64 oracle runs
+
+    @property
+    def shape(self):
+        return (self.cfg["nz"], self.cfg["ny"], self.cfg["nx"])
+
+    def computed_cells(self) -> int:
+        c = self.cfg
+        return (c["nx"] - 2 * HALO) * (c["ny"] - 2 * HALO) * (c["nz"] - 2 * HALO)
+
+
+def medium_from_velocity(vp, vs, rho):
+    """b = 1/rho, mu = rho vs^2, lambda = rho (vp^2 - 2 vs^2), computed in float64, stored float32."""
+    vp = np.asarray(vp, dtype=np.float64)
+    vs = np.asarray(vs, dtype=np.float64)
+    rho = np.asarray(rho, dtype=np.float64)
+    mu = rho * vs * vs
+    lam = rho * (vp * vp - 2.0 * vs * vs)
+    return (1.0 / rho).astype(np.float32), lam.astype(np.float32), mu.astype(np.float32)
+
+
+def gaussian_random_field(shape, std, corr_cells, seed):
+    """Zero-mean field with autocorrelation ~ exp(-r^2/a^2), a = corr_cells, rescaled to `std`.
+
+    White N(0,1) noise from numpy's PCG64(seed), smoothed by a separable
+    Gaussian of sigma = a/2 cells (the convolution of two such Gaussians has
+    the requested exp(-r^2/a^2) correlation), then normalised to the sample std.
+    """
+    from scipy.ndimage import gaussian_filter
+    rng = np.random.Generator(np.random.PCG64(seed))
+    w = rng.standard_normal(size=shape, dtype=np.float32)
+    f = gaussian_filter(w, sigma=corr_cells / 2.0, mode="wrap", truncate=4.0)
+    f = f.astype(np.float64)
+    f -= f.mean()
+    f *= std / f.std()
+    return f
+
+
+def _cfg(n3, pml, dt, d, damping, quirks, **kw):
+    nx, ny, nz = n3
+    c = dict(nx=nx, ny=ny, nz=nz, pml=pml, dt=dt, dx=d, dy=d, dz=d, coef=list(REF_COEF),
+             damping=damping, damping_R=0.001, damping_vconst=2000.0, quirks=quirks)
+    c.update(kw)
+    return c
+
+
+def reference_case(nt: int = 1500) -> Workload:
+    """The reference driver's run (CON/main.cu:11-56): GRID 300x200x100, pml 10,
+    dt 0.5 ms, 10 m cells, rho 2600, lambda = rho*5000^2, mu = lambda/3,
+    source at the grid centre, one txx station 10 cells further along each axis."""
+    nx, ny, nz, pml = 300, 200, 100, 10
+    shape = (nz, ny, nx)
+    # main.cu:53-55 evaluates these in double (pow) and stores float.
+    b = np.full(shape, np.float32(1.0) / np.float32(2600.0), np.float32)
+    lam = np.full(shape, np.float32(2600.0 * 5000.0 ** 2), np.float32)
+    mu = np.full(shape, np.float32(2600.0 * 5000.0 ** 2 / 3.0), np.float32)
+    from . import ricker_ref
+    w = ricker_ref(20.0, 0.0005, nt)
+    return Workload("reference_main_300x200x100", _cfg((nx, ny, nz), pml, 0.0005, 10.0, DAMP_REFGPU, QUIRKS_REF),
+                    b, lam, mu, (nx // 2, ny // 2, nz // 2),
+                    np.array([[nx // 2 + pml, ny // 2 + pml, nz // 2 + pml]], np.int32),
+                    np.array([TXX], np.int32), nt, w, w.astype(np.float64))
+
+
+def _ricker_t0_64(f0, dt, t0, nt):
+    t = np.arange(nt, dtype=np.float64) * dt
+    a = math.pi * f0 * (t - t0)
+    return (1.0 - 2.0 * a * a) * np.exp(-a * a)
+
+
+def plain_cube(n_interior: int = 100, pml: int = 20, nt: int = 500, dt: float = 0.001, d: float = 10.0,
+               quirks: int = QUIRKS_FIXED, damping: int = DAMP_LOGR) -> Workload:
+    """Homogeneous vp 3000, vs 1732, rho 2000; explosive Ricker f0 25 Hz, t0 = 1.2/f0,
+    at the centre computed cell; 101 receivers recording vx and vz along x on the
+    line 5 cells below the top interior face (the last one is the first PML cell)."""
+    n = n_interior + 2 * pml + 2 * HALO
+    shape = (n, n, n)
+    b, lam, mu = medium_from_velocity(np.full(shape, 3000.0), np.full(shape, 1732.0), np.full(shape, 2000.0))
+    c0 = HALO + (n - 2 * HALO) // 2
+    z = HALO + pml + 5
+    xs = HALO + pml + np.arange(101)
+    xs = np.minimum(xs, n - HALO - 1)
+    xyz = np.array([[x, c0, z] for x in xs for _ in (0, 1)], np.int32)
+    comp = np.array([VX, VZ] * len(xs), np.int32)
+    f0 = 25.0
+    w64 = _ricker_t0_64(f0, dt, 1.2 / f0, nt)
+    return Workload(f"plain_{n_interior}^3+pml{pml}", _cfg((n, n, n), pml, dt, d, damping, quirks),
+                    b, lam, mu, (c0, c0, c0), xyz, comp, nt, w64.astype(np.float32), w64)
+
+
+def random_cube(n_interior: int = 344, pml: int = 20, nt: int = 2000, dt: float = 0.001, d: float = 10.0,
+                std: float = 0.05, corr_m: float = 50.0, seed: int = 2, nrec_side: int = 64,
+                src_computed=(192, 192, 40), quirks: int = QUIRKS_FIXED, damping: int = DAMP_LOGR) -> Workload:
+    """Background vp 3000, vs 1732, rho 2000 scaled by (1 + delta), delta a seeded
+    Gaussian-correlated field (std, correlation length corr_m); Ricker 20 Hz
+    explosive source; nrec_side^2 receivers on the first interior z-plane
+    recording vx, vy, vz."""
+    n = n_interior + 2 * pml + 2 * HALO
+    shape = (n, n, n)
+    delta = gaussian_random_field(shape, std, corr_m / d, seed)
+    s = 1.0 + delta
+    b, lam, mu = medium_from_velocity(3000.0 * s, 1732.0 * s, 2000.0 * s)
+    del delta, s
+    i0 = HALO + pml
+    ks = i0 + (np.arange(nrec_side) * n_interior) // nrec_side
+    z = i0
+    pts = [(x, y, z) for y in ks for x in ks]
+    xyz = np.array([p for p in pts for _ in range(3)], np.int32)
+    comp = np.array([VX, VY, VZ] * len(pts), np.int32)
+    src = tuple(int(v) + HALO for v in src_computed)
+    f0 = 20.0
+    w64 = _ricker_t0_64(f0, dt, 1.2 / f0, nt)
+    return Workload(f"random_{n_interior}^3+pml{pml}", _cfg((n, n, n), pml, dt, d, damping, quirks),
+                    b, lam, mu, src, xyz, comp, nt, w64.astype(np.float32), w64)
+
+
+def small_random_case(nx=37, ny=41, nz=45, pml=6, nt=60, seed=7, quirks=QUIRKS_REF, damping=DAMP_REFGPU,
+                      std=0.15, dt=0.0005, d=10.0, nrec=24) -> Workload:
+    """A small uneven-size heterogeneous case for bit-exact parity tests: strong
+    random perturbation (so the reference's index quirks matter), source and
+    receivers anywhere in the computed region, including inside the PML."""
+    shape = (nz, ny, nx)
+    delta = gaussian_random_field(shape, std, 3.0, seed)
+    s = 1.0 + delta
+    b, lam, mu = medium_from_velocity(3000.0 * s, 1732.0 * s * (1.0 + 0.3 * delta), 2000.0 * s)
+    rng = np.random.Generator(np.random.PCG64(seed + 1))
+    src = (nx // 2 + 1, ny // 2 - 2, nz // 2 + 3)
+    xyz = np.stack([rng.integers(HALO, nx - HALO, nrec), rng.integers(HALO, ny - HALO, nrec),
+                    rng.integers(HALO, nz - HALO, nrec)], axis=1).astype(np.int32)
+    comp = (np.arange(nrec) % 9).astype(np.int32)
+    f0 = 25.0
+    w64 = _ricker_t0_64(f0, dt, 1.2 / f0, nt)
+    return Workload(f"small_{nx}x{ny}x{nz}_pml{pml}", _cfg((nx, ny, nz), pml, dt, d, damping, quirks),
+                    b, lam, mu, src, xyz, comp, nt, w64.astype(np.float32), w64)

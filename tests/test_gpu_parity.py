@@ -1,0 +1,67 @@
+"""GPU vs CPU oracle on the same seeded inputs, through the C ABI.
+
+FP32 contract: the kernels and the oracle perform the same rounded operations
+(explicit FMAs, IEEE division and square root, no flush-to-zero), so traces and
+final wavefields must agree BIT FOR BIT.  The FP64 oracle gives each case's
+error against exact arithmetic (reported, bounded at 1e-4 relative L2)."""
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+from helpers import make_solver, run_oracle
+import sgfd
+import sgfd.workloads as wl
+
+pytestmark = pytest.mark.gpu
+
+CASES = [
+    dict(quirks=sgfd.QUIRKS_REF, damping=sgfd.DAMP_REFGPU),
+    dict(quirks=sgfd.QUIRKS_FIXED, damping=sgfd.DAMP_LOGR),
+    dict(quirks=sgfd.QUIRKS_FIXED, damping=sgfd.DAMP_REFCPU, nx=31, ny=29, nz=27, pml=3),
+    dict(quirks=sgfd.QUIRKS_REF, damping=sgfd.DAMP_LOGR, nx=23, ny=22, nz=21, pml=1, nt=40),
+    dict(quirks=sgfd.QUIRKS_REF, damping=sgfd.DAMP_REFGPU, nx=70, ny=36, nz=33, pml=8, nt=50),
+]
+
+
+def _ids(c):
+    return "_".join(f"{k}{v}" for k, v in c.items())
+
+
+@pytest.mark.parametrize("case", CASES, ids=[_ids(c) for c in CASES])
+def test_bit_exact_vs_oracle(case):
+    w = wl.small_random_case(**case)
+    o = run_oracle(w)
+    with make_solver(w) as s:
+        s.run(0, w.nt)
+        s.synchronize()
+        tr = s.traces()
+        np.testing.assert_array_equal(tr, o.traces().astype(np.float32))
+        for fid in range(9):
+            g = s.field(fid)
+            np.testing.assert_array_equal(g, o.field(fid).astype(np.float32), err_msg=sgfd.FIELD_NAMES[fid])
+    # error of the FP32 path against FP64 arithmetic
+    o64 = run_oracle(w, fp64=True)
+    err = rel_l2(tr, o64.traces())
+    assert err < 1e-4, err
+
+
+def test_step_api_equals_run_api():
+    w = wl.small_random_case(nt=30)
+    with make_solver(w) as a, make_solver(w) as b:
+        a.run(0, w.nt)
+        for it in range(w.nt):
+            b.step(it, float(w.wavelet[it]))
+        a.synchronize(); b.synchronize()
+        np.testing.assert_array_equal(a.traces(), b.traces())
+        np.testing.assert_array_equal(a.field(sgfd.TXX), b.field(sgfd.TXX))
+
+
+def test_source_inside_pml_matches_oracle():
+    """A source in the PML is overwritten by the split sum at the next stress
+    update, as in the reference (splits are the state there)."""
+    w = wl.small_random_case(nt=25)
+    w.src = (6, 7, 8)
+    o = run_oracle(w)
+    with make_solver(w) as s:
+        s.run(0, w.nt)
+        np.testing.assert_array_equal(s.traces(), o.traces().astype(np.float32))
