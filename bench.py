@@ -51,6 +51,7 @@ def parse():
     p.add_argument("--impl", choices=["sgfd", "reference"], default="sgfd")
     p.add_argument("--workload", choices=["random344", "plain100", "reference_main"], default="random344")
     p.add_argument("--kernel", choices=["auto", "simple", "zmarch"], default="auto")
+    p.add_argument("--arith", choices=["ref", "fast"], default="fast")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-steps", type=int, default=6, help="steps of the CPU sample")
@@ -112,7 +113,7 @@ class ClockSampler:
             self.proc.kill()
         rows = [l.split(", ") for l in self.lines if l.count(",") >= 8]
         if self.bus_id:
-            mine = [r for r in rows if self.bus_id.endswith(r[0].lower()[-12:]) or r[0].lower().endswith(self.bus_id[-12:])]
+            mine = [r for r in rows if r[0].lower()[-7:] == self.bus_id[-7:]]
             rows = mine or rows
         sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
         mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
@@ -243,11 +244,13 @@ def main():
     import sgfd
     torch.cuda.set_device(local)
     kernel = {"auto": sgfd.KERNEL_AUTO, "simple": sgfd.KERNEL_SIMPLE, "zmarch": sgfd.KERNEL_ZMARCH}[args.kernel]
-    cfg = sgfd.default_config(**{**w.cfg, "device": local, "kernel": kernel})
+    arith = sgfd.ARITH_FAST if args.arith == "fast" else sgfd.ARITH_REF
+    cfg = sgfd.default_config(**{**w.cfg, "device": local, "kernel": kernel, "arith": arith})
     K, W = args.steps, args.warmup
     nt = max(w.nt, W + K + 64)
     wav = np.resize(w.wavelet, nt).astype(np.float32)
-    stream = torch.cuda.current_stream()
+    stream = torch.cuda.Stream()          # a real stream: events below see the solver's work
+    torch.cuda.set_stream(stream)
     s = sgfd.Solver(cfg)
     s.set_stream(stream.cuda_stream)
     s.set_medium(w.b, w.lam, w.mu)
@@ -260,7 +263,11 @@ def main():
     # ---- device-resident timing: exactly K steps ----
     s.run(0, W)
     torch.cuda.synchronize()
-    bus = getattr(torch.cuda.get_device_properties(local), "pci_bus_id", None)
+    props = torch.cuda.get_device_properties(local)
+    try:
+        bus = "%08X:%02X:%02X.0" % (props.pci_domain_id, props.pci_bus_id, props.pci_device_id)
+    except AttributeError:
+        bus = None
     clocks = ClockSampler(bus)
     clocks.start()
     time.sleep(0.1)
@@ -304,7 +311,8 @@ def main():
         "dtype": "f32", "data": "synthetic",
         "config": {"workload": w.name, "grid": [w.cfg["nx"], w.cfg["ny"], w.cfg["nz"]], "pml": w.cfg["pml"],
                    "computed_cells": cells, "interior_cells": n_int, "pml_cells": n_pml,
-                   "receivers": len(w.rec_comp), "kernel": None, "parallelism": f"replicas{world}",
+                   "receivers": len(w.rec_comp), "kernel": None, "arith": args.arith,
+                   "parallelism": f"replicas{world}",
                    "l2": "inputs larger than L2 (9 wavefields of %.0f MB each)" % (w.cfg["nx"] * w.cfg["ny"] * w.cfg["nz"] * 4 / 1e6)},
         "roofline": roof, "clocks": clk,
         "gpu_launches": None, "e2e": e2e,

@@ -101,6 +101,17 @@ typedef enum sgfd_storage {
     SGFD_STORE_F16 = 2
 } sgfd_storage;
 
+/* Rounding of the staggered differences.
+ *  REF:  sum_i c_i (f[+] - f[-]), then divided by the cell size — the
+ *        reference's expression (OPT/ElasticWaveEquation.cu:244-250).
+ *  FAST: sum_i (c_i / d) (f[+] - f[-]) with the coefficients divided by the
+ *        cell size once on the host, so no division per cell.  Differs from
+ *        REF by rounding only (relative L2 of traces well below 1e-5). */
+typedef enum sgfd_arith {
+    SGFD_ARITH_REF = 0,
+    SGFD_ARITH_FAST = 1
+} sgfd_arith;
+
 /* Kernel family.  AUTO picks the fastest built variant for the storage type. */
 typedef enum sgfd_kernel {
     SGFD_KERNEL_AUTO = 0,
@@ -120,7 +131,8 @@ typedef struct sgfd_config {
     int32_t storage;          /* sgfd_storage */
     int32_t kernel;           /* sgfd_kernel */
     int32_t device;           /* CUDA device ordinal */
-    int32_t reserved[8];      /* must be zero */
+    int32_t arith;            /* sgfd_arith */
+    int32_t reserved[7];      /* must be zero */
 } sgfd_config;
 
 typedef struct sgfd_solver sgfd_solver;
@@ -197,6 +209,15 @@ float sgfd_ricker_t0(float f0, float dt, float t0, int32_t it);
  * kernel; returns the summed device time of the velocity-update and the
  * stress-update kernels in milliseconds.  Blocking.  For roofline accounting. */
 int sgfd_profile(sgfd_solver *h, int32_t it0, int32_t nsteps, float *ms_velocity, float *ms_stress);
+
+/* z-marching kernels: planes per z chunk (0 = automatic).  Larger chunks
+ * re-read fewer warm-up planes; smaller ones give more CTAs to balance. */
+int sgfd_set_zchunk(sgfd_solver *h, int32_t planes);
+
+/* z-marching kernels: tile height in cells (8 or 16; one or two cells per
+ * thread) and planes per z chunk (0 = automatic).  No effect on the simple
+ * family.  Results do not depend on the tiling. */
+int sgfd_set_tiling(sgfd_solver *h, int32_t tile_rows, int32_t zchunk);
 
 /* Counts for roofline accounting: computed cells that are interior / PML. */
 int sgfd_cell_counts(const sgfd_solver *h, int64_t *n_interior, int64_t *n_pml);

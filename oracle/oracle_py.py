@@ -29,7 +29,7 @@ class OracleConfig(ctypes.Structure):
         ("coef", ctypes.c_float * 5),
         ("damping", ctypes.c_int32), ("damping_R", ctypes.c_float), ("damping_vconst", ctypes.c_float),
         ("quirks", ctypes.c_int32), ("storage", ctypes.c_int32), ("kernel", ctypes.c_int32),
-        ("device", ctypes.c_int32), ("reserved", ctypes.c_int32 * 8),
+        ("device", ctypes.c_int32), ("arith", ctypes.c_int32), ("reserved", ctypes.c_int32 * 7),
     ]
 
 

@@ -83,6 +83,8 @@ struct Oracle {
     std::vector<T> b, lam, mu, rmu;   // rmu = 1/mu per cell
     std::vector<T> split[N_SPLIT];
     T c[5];
+    T cs[3][5];      // FAST arithmetic: c_i / d_axis, rounded once
+    bool fast = false;
     T dt, dx, dy, dz;
     int src_x = -1, src_y = -1, src_z = -1;
     std::vector<Receiver> rec;
@@ -94,6 +96,7 @@ struct Oracle {
     T poly;          // 8/15 - 0.03 p + p^2/1500
     T q_logr;        // 0.5*dt*3*ln(1/R)/(2p)
     T q_refcpu[3];   // 0.5*dt*log10(1/R)*3.4*V/(p*d_axis)
+    T qf[3];         // FAST: q constant pre-divided by the cell size
 
     explicit Oracle(const sgfd_config &c_) : cfg(c_) {
         nx = cfg.nx; ny = cfg.ny; nz = cfg.nz;
@@ -103,6 +106,8 @@ struct Oracle {
         for (auto &v : split) v.assign(n, T(0));
         for (int i = 0; i < 5; ++i) c[i] = (T)cfg.coef[i];
         dt = (T)cfg.dt; dx = (T)cfg.dx; dy = (T)cfg.dy; dz = (T)cfg.dz;
+        fast = cfg.arith == SGFD_ARITH_FAST;
+        for (int i = 0; i < 5; ++i) { cs[0][i] = c[i] / dx; cs[1][i] = c[i] / dy; cs[2][i] = c[i] / dz; }
         const int p = cfg.pml;
         // (0.5f * delta.t) * tau  (OPT/ElasticMacro.h:26 in 1 - 0.5*dt*DAMPING)
         T h = (T)0.5f * dt * (T)kTau;
@@ -115,21 +120,34 @@ struct Oracle {
         for (int a = 0; a < 3; ++a)
             q_refcpu[a] = (T)(0.5 * (double)cfg.dt * std::log10(1.0 / R) * 3.4 *
                               (double)cfg.damping_vconst / ((double)p * dd[a]));
+        const T d3[3] = {dx, dy, dz};
+        for (int a = 0; a < 3; ++a)
+            qf[a] = cfg.damping == SGFD_DAMP_LOGR ? q_logr / d3[a] : (h / d3[a]) * poly;
     }
 
     int64_t idx(int x, int y, int z) const { return x + (int64_t)y * sy + (int64_t)z * sz; }
 
-    // Forward staggered difference: sum c_i (f[+1+i] - f[-i])   (e.g. OPT/ElasticWaveEquation.cu:246)
-    inline T dfwd(const T *g, int64_t s) const {
+    // Forward staggered difference along `axis` (0,1,2 = x,y,z), stride s:
+    // sum c_i (f[+1+i] - f[-i]) / d   (e.g. OPT/ElasticWaveEquation.cu:246, 250).
+    // FAST arithmetic uses c_i/d and no division.
+    inline T dfwd(const T *g, int64_t s, int axis) const {
+        const T *k = fast ? cs[axis] : c;
         T d = 0;
-        for (int i = 0; i < 5; ++i) d = fma_(c[i], g[(1 + i) * s] - g[-i * s], d);
-        return d;
+        for (int i = 0; i < 5; ++i) d = fma_(k[i], g[(1 + i) * s] - g[-i * s], d);
+        return fast ? d : d / (axis == 0 ? dx : axis == 1 ? dy : dz);
     }
-    // Backward staggered difference: sum c_i (f[+i] - f[-1-i])  (e.g. OPT/ElasticWaveEquation.cu:247)
-    inline T dbwd(const T *g, int64_t s) const {
+    // Backward staggered difference: sum c_i (f[+i] - f[-1-i]) / d  (e.g. OPT/ElasticWaveEquation.cu:247)
+    inline T dbwd(const T *g, int64_t s, int axis) const {
+        const T *k = fast ? cs[axis] : c;
         T d = 0;
-        for (int i = 0; i < 5; ++i) d = fma_(c[i], g[i * s] - g[(-1 - i) * s], d);
-        return d;
+        for (int i = 0; i < 5; ++i) d = fma_(k[i], g[i * s] - g[(-1 - i) * s], d);
+        return fast ? d : d / (axis == 0 ? dx : axis == 1 ? dy : dz);
+    }
+    // Harmonic average 4 / (r0 + r1 + r2 + r3) of four reciprocals; FAST takes
+    // 4 * RN(1/s), which equals RN(4/s) exactly (a power-of-two scaling).
+    inline T hmean(T r0, T r1, T r2, T r3) const {
+        const T s = ((r0 + r1) + r2) + r3;
+        return fast ? (T)4 * ((T)1 / s) : (T)4 / s;
     }
 
     // Damping band of coordinate i along an axis of length N: 0 if not in a
@@ -141,17 +159,18 @@ struct Oracle {
         return 0;
     }
 
-    // (m, p) = (1 - q*r^2, 1 + q*r^2) for one damped axis.
+    // (m, p) = (1 - q*r^2, 1 + q*r^2) for one damped axis; FAST returns
+    // (m, RN(1/p)) and takes q from a constant pre-divided by the cell size.
     inline void damp(int axis, int k, int64_t ci, T &m, T &pp) const {
         const T d[3] = {dx, dy, dz};
         T q;
         if (cfg.damping == SGFD_DAMP_REFGPU) {
             // Vs = sqrt(mu*b) (OPT/ElasticWaveEquation.cu:282)
             T vs = std::sqrt(mu[ci] * b[ci]);
-            q = ((q_refgpu[axis] * vs) / d[axis]) * poly;
+            q = fast ? vs * qf[axis] : ((q_refgpu[axis] * vs) / d[axis]) * poly;
         } else if (cfg.damping == SGFD_DAMP_LOGR) {
             T vp = std::sqrt(fma_((T)2, mu[ci], lam[ci]) * b[ci]);
-            q = (q_logr * vp) / d[axis];
+            q = fast ? vp * qf[axis] : (q_logr * vp) / d[axis];
         } else {
             q = q_refcpu[axis];
         }
@@ -159,6 +178,7 @@ struct Oracle {
         T pw = r * r;
         m = fma_(-q, pw, (T)1);
         pp = fma_(q, pw, (T)1);
+        if (fast) pp = (T)1 / pp;
     }
 
     void inject(T s) {
@@ -170,9 +190,10 @@ struct Oracle {
         f[TZZ][ci] = f[TZZ][ci] + v;
     }
 
-    // One split update: damped -> (m*s + A*B)/p ; undamped -> s + A*B.
-    static inline T upd(T s, T A, T B, bool damped, T m, T p) {
-        return damped ? fma_(m, s, A * B) / p : fma_(A, B, s);
+    // One split update: damped -> (m*s + A*B)/p (FAST: times RN(1/p)); undamped -> s + A*B.
+    inline T upd(T s, T A, T B, bool damped, T m, T p) const {
+        if (!damped) return fma_(A, B, s);
+        return fast ? fma_(m, s, A * B) * p : fma_(m, s, A * B) / p;
     }
 
     void velocity_cell(int x, int y, int z, int kx, int ky, int kz) {
@@ -185,9 +206,9 @@ struct Oracle {
         T by = (bb[0] + bb[sy]) / (T)2;
         T bz = (bb[0] + bb[sz]) / (T)2;
         // derivatives (OPT/ElasticWaveEquation.cu:244-276)
-        T xX = dfwd(sxx, 1) / dx, xY = dbwd(sxy, sy) / dy, xZ = dbwd(sxz, sz) / dz;
-        T yX = dbwd(sxy, 1) / dx, yY = dfwd(syy, sy) / dy, yZ = dbwd(syz, sz) / dz;
-        T zX = dbwd(sxz, 1) / dx, zY = dbwd(syz, sy) / dy, zZ = dfwd(szz, sz) / dz;
+        T xX = dfwd(sxx, 1, 0), xY = dbwd(sxy, sy, 1), xZ = dbwd(sxz, sz, 2);
+        T yX = dbwd(sxy, 1, 0), yY = dfwd(syy, sy, 1), yZ = dbwd(syz, sz, 2);
+        T zX = dbwd(sxz, 1, 0), zY = dbwd(syz, sy, 1), zZ = dfwd(szz, sz, 2);
         if (!(kx | ky | kz)) {
             // interior (OPT/ElasticWaveEquation.cu:253,265,277)
             f[VX][ci] = fma_(dt * bx, (xX + xY) + xZ, f[VX][ci]);
@@ -224,18 +245,18 @@ struct Oracle {
         const T *vx = f[VX].data() + ci, *vy = f[VY].data() + ci, *vz = f[VZ].data() + ci;
         const T *r = rmu.data() + ci;
         // normal-stress derivatives (OPT/ElasticWaveEquation.cu:541-549)
-        T dXx = dbwd(vx, 1) / dx, dYy = dbwd(vy, sy) / dy, dZz = dbwd(vz, sz) / dz;
+        T dXx = dbwd(vx, 1, 0), dYy = dbwd(vy, sy, 1), dZz = dbwd(vz, sz, 2);
         // shear derivatives (OPT/ElasticWaveEquation.cu:565-591)
-        T xyY = dfwd(vx, sy) / dy, xyX = dfwd(vy, 1) / dx;
-        T xzZ = dfwd(vx, sz) / dz, xzX = dfwd(vz, 1) / dx;
-        T yzZ = dfwd(vy, sz) / dz, yzY = dfwd(vz, sy) / dy;
+        T xyY = dfwd(vx, sy, 1), xyX = dfwd(vy, 1, 0);
+        T xzZ = dfwd(vx, sz, 2), xzX = dfwd(vz, 1, 0);
+        T yzZ = dfwd(vy, sz, 2), yzY = dfwd(vz, sy, 1);
         const T l = lam[ci];
         const T l2m = fma_((T)2, mu[ci], l);
         // harmonic mu averages (OPT/ElasticMacro.h:111-119); REF quirk in xz.
         const bool ref = cfg.quirks == SGFD_QUIRKS_REF;
-        T mxy = (T)4 / (((r[0] + r[1]) + r[sy]) + r[1 + sy]);
-        T mxz = (T)4 / (((r[0] + r[1]) + r[sz]) + (ref ? r[1 + sy] : r[1 + sz]));
-        T myz = (T)4 / (((r[0] + r[sy]) + r[sz]) + r[sy + sz]);
+        T mxy = hmean(r[0], r[1], r[sy], r[1 + sy]);
+        T mxz = hmean(r[0], r[1], r[sz], ref ? r[1 + sy] : r[1 + sz]);
+        T myz = hmean(r[0], r[sy], r[sz], r[sy + sz]);
         if (!(kx | ky | kz)) {
             // interior (OPT/ElasticWaveEquation.cu:550-592)
             f[TXX][ci] = fma_(dt, fma_(l2m, dXx, l * (dYy + dZz)), f[TXX][ci]);
@@ -288,21 +309,24 @@ struct Oracle {
         const T *__restrict bb = b.data() + r0;
         T *__restrict vx = f[VX].data() + r0, *__restrict vy = f[VY].data() + r0, *__restrict vz = f[VZ].data() + r0;
         const int64_t Y = sy, Z = sz;
+        const T *kx = fast ? cs[0] : c, *ky = fast ? cs[1] : c, *kz = fast ? cs[2] : c;
+        const T qx = fast ? (T)1 : dx, qy = fast ? (T)1 : dy, qz = fast ? (T)1 : dz;
         for (int x = x0; x < x1; ++x) {
             T xX = 0, xY = 0, xZ = 0, yX = 0, yY = 0, yZ = 0, zX = 0, zY = 0, zZ = 0;
 #pragma GCC unroll 5
             for (int i = 0; i < 5; ++i) {
-                xX = fma_(c[i], sxx[x + 1 + i] - sxx[x - i], xX);
-                xY = fma_(c[i], sxy[x + i * Y] - sxy[x - (1 + i) * Y], xY);
-                xZ = fma_(c[i], sxz[x + i * Z] - sxz[x - (1 + i) * Z], xZ);
-                yX = fma_(c[i], sxy[x + i] - sxy[x - 1 - i], yX);
-                yY = fma_(c[i], syy[x + (1 + i) * Y] - syy[x - i * Y], yY);
-                yZ = fma_(c[i], syz[x + i * Z] - syz[x - (1 + i) * Z], yZ);
-                zX = fma_(c[i], sxz[x + i] - sxz[x - 1 - i], zX);
-                zY = fma_(c[i], syz[x + i * Y] - syz[x - (1 + i) * Y], zY);
-                zZ = fma_(c[i], szz[x + (1 + i) * Z] - szz[x - i * Z], zZ);
+                xX = fma_(kx[i], sxx[x + 1 + i] - sxx[x - i], xX);
+                xY = fma_(ky[i], sxy[x + i * Y] - sxy[x - (1 + i) * Y], xY);
+                xZ = fma_(kz[i], sxz[x + i * Z] - sxz[x - (1 + i) * Z], xZ);
+                yX = fma_(kx[i], sxy[x + i] - sxy[x - 1 - i], yX);
+                yY = fma_(ky[i], syy[x + (1 + i) * Y] - syy[x - i * Y], yY);
+                yZ = fma_(kz[i], syz[x + i * Z] - syz[x - (1 + i) * Z], yZ);
+                zX = fma_(kx[i], sxz[x + i] - sxz[x - 1 - i], zX);
+                zY = fma_(ky[i], syz[x + i * Y] - syz[x - (1 + i) * Y], zY);
+                zZ = fma_(kz[i], szz[x + (1 + i) * Z] - szz[x - i * Z], zZ);
             }
-            xX /= dx; xY /= dy; xZ /= dz; yX /= dx; yY /= dy; yZ /= dz; zX /= dx; zY /= dy; zZ /= dz;
+            // x / 1 is exact, so FAST takes the same code path
+            xX /= qx; xY /= qy; xZ /= qz; yX /= qx; yY /= qy; yZ /= qz; zX /= qx; zY /= qy; zZ /= qz;
             const T bx = (bb[x] + bb[x + 1]) / (T)2, by = (bb[x] + bb[x + Y]) / (T)2, bz = (bb[x] + bb[x + Z]) / (T)2;
             vx[x] = fma_(dt * bx, (xX + xY) + xZ, vx[x]);
             vy[x] = fma_(dt * by, (yX + yY) + yZ, vy[x]);
@@ -320,28 +344,30 @@ struct Oracle {
         T *__restrict sxy = f[TXY].data() + r0, *__restrict sxz = f[TXZ].data() + r0, *__restrict syz = f[TYZ].data() + r0;
         const int64_t Y = sy, Z = sz;
         const int64_t q4 = cfg.quirks == SGFD_QUIRKS_REF ? 1 + Y : 1 + Z;
+        const T *kx = fast ? cs[0] : c, *ky = fast ? cs[1] : c, *kz = fast ? cs[2] : c;
+        const T qx = fast ? (T)1 : dx, qy = fast ? (T)1 : dy, qz = fast ? (T)1 : dz;
         for (int x = x0; x < x1; ++x) {
             T dXx = 0, dYy = 0, dZz = 0, xyY = 0, xyX = 0, xzZ = 0, xzX = 0, yzZ = 0, yzY = 0;
 #pragma GCC unroll 5
             for (int i = 0; i < 5; ++i) {
-                dXx = fma_(c[i], vx[x + i] - vx[x - 1 - i], dXx);
-                dYy = fma_(c[i], vy[x + i * Y] - vy[x - (1 + i) * Y], dYy);
-                dZz = fma_(c[i], vz[x + i * Z] - vz[x - (1 + i) * Z], dZz);
-                xyY = fma_(c[i], vx[x + (1 + i) * Y] - vx[x - i * Y], xyY);
-                xyX = fma_(c[i], vy[x + 1 + i] - vy[x - i], xyX);
-                xzZ = fma_(c[i], vx[x + (1 + i) * Z] - vx[x - i * Z], xzZ);
-                xzX = fma_(c[i], vz[x + 1 + i] - vz[x - i], xzX);
-                yzZ = fma_(c[i], vy[x + (1 + i) * Z] - vy[x - i * Z], yzZ);
-                yzY = fma_(c[i], vz[x + (1 + i) * Y] - vz[x - i * Y], yzY);
+                dXx = fma_(kx[i], vx[x + i] - vx[x - 1 - i], dXx);
+                dYy = fma_(ky[i], vy[x + i * Y] - vy[x - (1 + i) * Y], dYy);
+                dZz = fma_(kz[i], vz[x + i * Z] - vz[x - (1 + i) * Z], dZz);
+                xyY = fma_(ky[i], vx[x + (1 + i) * Y] - vx[x - i * Y], xyY);
+                xyX = fma_(kx[i], vy[x + 1 + i] - vy[x - i], xyX);
+                xzZ = fma_(kz[i], vx[x + (1 + i) * Z] - vx[x - i * Z], xzZ);
+                xzX = fma_(kx[i], vz[x + 1 + i] - vz[x - i], xzX);
+                yzZ = fma_(kz[i], vy[x + (1 + i) * Z] - vy[x - i * Z], yzZ);
+                yzY = fma_(ky[i], vz[x + (1 + i) * Y] - vz[x - i * Y], yzY);
             }
-            dXx /= dx; dYy /= dy; dZz /= dz; xyY /= dy; xyX /= dx; xzZ /= dz; xzX /= dx; yzZ /= dz; yzY /= dy;
+            dXx /= qx; dYy /= qy; dZz /= qz; xyY /= qy; xyX /= qx; xzZ /= qz; xzX /= qx; yzZ /= qz; yzY /= qy;
             const T l = la[x], l2m = fma_((T)2, m[x], l);
             sxx[x] = fma_(dt, fma_(l2m, dXx, l * (dYy + dZz)), sxx[x]);
             syy[x] = fma_(dt, fma_(l2m, dYy, l * (dXx + dZz)), syy[x]);
             szz[x] = fma_(dt, fma_(l2m, dZz, l * (dXx + dYy)), szz[x]);
-            const T mxy = (T)4 / (((r[x] + r[x + 1]) + r[x + Y]) + r[x + 1 + Y]);
-            const T mxz = (T)4 / (((r[x] + r[x + 1]) + r[x + Z]) + r[x + q4]);
-            const T myz = (T)4 / (((r[x] + r[x + Y]) + r[x + Z]) + r[x + Y + Z]);
+            const T mxy = hmean(r[x], r[x + 1], r[x + Y], r[x + 1 + Y]);
+            const T mxz = hmean(r[x], r[x + 1], r[x + Z], r[x + q4]);
+            const T myz = hmean(r[x], r[x + Y], r[x + Z], r[x + Y + Z]);
             sxy[x] = fma_(dt * mxy, xyY + xyX, sxy[x]);
             sxz[x] = fma_(dt * mxz, xzZ + xzX, sxz[x]);
             syz[x] = fma_(dt * myz, yzZ + yzY, syz[x]);

@@ -35,30 +35,73 @@ __device__ __forceinline__ float dbwd(const float (&c)[5], G g) {
     return d;
 }
 
-// Damping factors m = 1 - q r^2, p = 1 + q r^2 of one damped axis at band
-// distance k (1..pml).  d_axis is dx, dy or dz.
-__device__ __forceinline__ void damp_factors(const Physics &ph, int axis, float d_axis, int k,
-                                             int pml, float mu, float b, float lam,
+// Staggered difference along AXIS (0, 1, 2 = x, y, z) divided by the cell
+// size: REF divides the sum (reference expression), FAST uses the
+// pre-divided coefficients c_i / d.
+template <bool FAST, int AXIS, class G>
+__device__ __forceinline__ float dF(const Physics &ph, G g) {
+    if (FAST) return dfwd(ph.cs[AXIS], g);
+    return dfwd(ph.c, g) / (AXIS == 0 ? ph.dx : AXIS == 1 ? ph.dy : ph.dz);
+}
+template <bool FAST, int AXIS, class G>
+__device__ __forceinline__ float dB(const Physics &ph, G g) {
+    if (FAST) return dbwd(ph.cs[AXIS], g);
+    return dbwd(ph.c, g) / (AXIS == 0 ? ph.dx : AXIS == 1 ? ph.dy : ph.dz);
+}
+
+// Harmonic mean 4 / (r0 + r1 + r2 + r3) of four reciprocals of mu
+// (ElasticMacro.h:111-112).  FAST computes 4 * RN(1/s), equal to RN(4/s)
+// because scaling by 4 is exact.
+template <bool FAST>
+__device__ __forceinline__ float hmean(float r0, float r1, float r2, float r3) {
+    const float s = ((r0 + r1) + r2) + r3;
+    return FAST ? 4.0f * __frcp_rn(s) : 4.0f / s;
+}
+
+// Wave speed the damping profile scales with, computed once per cell:
+// REFGPU the local shear speed sqrt(mu*b) (OPT/ElasticWaveEquation.cu:282),
+// LOGR the local P speed sqrt((lambda+2mu)*b), REFCPU unused.
+__device__ __forceinline__ float damp_speed(const Physics &ph, float mu, float b, float lam) {
+    if (ph.damping == 0) return sqrtf(mu * b);
+    if (ph.damping == 1) return sqrtf(__fmaf_rn(2.0f, mu, lam) * b);
+    return 0.0f;
+}
+
+// Damping factors of one damped axis at band distance k (1..pml):
+// m = 1 - q r^2 and p = 1 + q r^2 (ElasticMacro.h:26-27 inside
+// 1 -/+ 0.5*dt*DAMPING).  REF returns p; FAST returns RN(1/p) so the split
+// updates multiply instead of divide.  d_axis is dx, dy or dz; v is
+// damp_speed() of the cell.
+template <bool FAST>
+__device__ __forceinline__ void damp_factors(const Physics &ph, int axis, float d_axis, int k, int pml, float v,
                                              float &m, float &p) {
     float q;
-    if (ph.damping == 0) {                    // SGFD_DAMP_REFGPU: Vs = sqrt(mu*b)
-        const float vs = sqrtf(mu * b);
-        q = ((ph.q_refgpu * vs) / d_axis) * ph.poly;
-    } else if (ph.damping == 1) {             // SGFD_DAMP_LOGR: Vp = sqrt((lambda+2mu)*b)
-        const float vp = sqrtf(__fmaf_rn(2.0f, mu, lam) * b);
-        q = (ph.q_logr * vp) / d_axis;
+    if (ph.damping == 0) {                    // SGFD_DAMP_REFGPU
+        q = FAST ? v * ph.qf[axis] : ((ph.q_refgpu * v) / d_axis) * ph.poly;
+    } else if (ph.damping == 1) {             // SGFD_DAMP_LOGR
+        q = FAST ? v * ph.qf[axis] : (ph.q_logr * v) / d_axis;
     } else {                                  // SGFD_DAMP_REFCPU: constant velocity
         q = ph.q_refcpu[axis];
     }
-    const float r = (float)k / (float)pml;
-    const float pw = r * r;
+    float pw;
+    if (k < kPwTable) {
+        pw = ph.pw[k];
+    } else {
+        const float r = (float)k / (float)pml;
+        pw = r * r;
+    }
     m = __fmaf_rn(-q, pw, 1.0f);
     p = __fmaf_rn(q, pw, 1.0f);
+    if (FAST) p = __frcp_rn(p);
 }
 
-// One split-field update: (m*s + A*B)/p on a damped axis, s + A*B otherwise.
+// One split-field update: (m*s + A*B)/p on a damped axis (FAST: times RN(1/p)),
+// s + A*B otherwise.
+template <bool FAST>
 __device__ __forceinline__ float split_update(float s, float A, float B, bool damped, float m, float p) {
-    return damped ? __fmaf_rn(m, s, A * B) / p : __fmaf_rn(A, B, s);
+    if (!damped) return __fmaf_rn(A, B, s);
+    const float num = __fmaf_rn(m, s, A * B);
+    return FAST ? num * p : num / p;
 }
 
 }  // namespace sgfd

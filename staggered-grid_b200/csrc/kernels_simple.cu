@@ -26,6 +26,7 @@ __global__ void k_inject(Model m, Physics ph, SourceRec sr, int it, float value,
 }
 
 // Velocity update of one cell (ElasticWaveEquation.cu:234-526, ElasticMacro.h:409-458).
+template <bool FAST>
 __global__ void __launch_bounds__(kBX * kBY) k_velocity(Model m, Physics ph) {
     const int cx = blockIdx.x * kBX + threadIdx.x;
     const int cy = blockIdx.y * kBY + threadIdx.y;
@@ -41,15 +42,15 @@ __global__ void __launch_bounds__(kBX * kBY) k_velocity(Model m, Physics ph) {
     const float bx = (bb[0] + bb[1]) / 2.0f;
     const float by = (bb[0] + bb[SY]) / 2.0f;
     const float bz = (bb[0] + bb[SZ]) / 2.0f;
-    const float xX = dfwd(ph.c, [&](int o) { return __ldg(sxx + o); }) / ph.dx;
-    const float xY = dbwd(ph.c, [&](int o) { return __ldg(sxy + o * SY); }) / ph.dy;
-    const float xZ = dbwd(ph.c, [&](int o) { return __ldg(sxz + o * SZ); }) / ph.dz;
-    const float yX = dbwd(ph.c, [&](int o) { return __ldg(sxy + o); }) / ph.dx;
-    const float yY = dfwd(ph.c, [&](int o) { return __ldg(syy + o * SY); }) / ph.dy;
-    const float yZ = dbwd(ph.c, [&](int o) { return __ldg(syz + o * SZ); }) / ph.dz;
-    const float zX = dbwd(ph.c, [&](int o) { return __ldg(sxz + o); }) / ph.dx;
-    const float zY = dbwd(ph.c, [&](int o) { return __ldg(syz + o * SY); }) / ph.dy;
-    const float zZ = dfwd(ph.c, [&](int o) { return __ldg(szz + o * SZ); }) / ph.dz;
+    const float xX = dF<FAST, 0>(ph, [&](int o) { return __ldg(sxx + o); });
+    const float xY = dB<FAST, 1>(ph, [&](int o) { return __ldg(sxy + o * SY); });
+    const float xZ = dB<FAST, 2>(ph, [&](int o) { return __ldg(sxz + o * SZ); });
+    const float yX = dB<FAST, 0>(ph, [&](int o) { return __ldg(sxy + o); });
+    const float yY = dF<FAST, 1>(ph, [&](int o) { return __ldg(syy + o * SY); });
+    const float yZ = dB<FAST, 2>(ph, [&](int o) { return __ldg(syz + o * SZ); });
+    const float zX = dB<FAST, 0>(ph, [&](int o) { return __ldg(sxz + o); });
+    const float zY = dB<FAST, 1>(ph, [&](int o) { return __ldg(syz + o * SY); });
+    const float zZ = dF<FAST, 2>(ph, [&](int o) { return __ldg(szz + o * SZ); });
 
     const int kx = band(x, m.nx, m.pml), ky = band(y, m.ny, m.pml), kz = band(z, m.nz, m.pml);
     if (!(kx | ky | kz)) {
@@ -60,10 +61,10 @@ __global__ void __launch_bounds__(kBX * kBY) k_velocity(Model m, Physics ph) {
     }
     float mx = 1.f, px = 1.f, my = 1.f, py = 1.f, mz = 1.f, pz = 1.f;
     {
-        const float mu0 = m.mu[ci], b0 = bb[0], l0 = m.lam[ci];
-        if (kx) damp_factors(ph, 0, ph.dx, kx, m.pml, mu0, b0, l0, mx, px);
-        if (ky) damp_factors(ph, 1, ph.dy, ky, m.pml, mu0, b0, l0, my, py);
-        if (kz) damp_factors(ph, 2, ph.dz, kz, m.pml, mu0, b0, l0, mz, pz);
+        const float v = damp_speed(ph, m.mu[ci], bb[0], m.lam[ci]);
+        if (kx) damp_factors<FAST>(ph, 0, ph.dx, kx, m.pml, v, mx, px);
+        if (ky) damp_factors<FAST>(ph, 1, ph.dy, ky, m.pml, v, my, py);
+        if (kz) damp_factors<FAST>(ph, 2, ph.dz, kz, m.pml, v, mz, pz);
     }
     const bool ref = ph.quirks == 0;   // REF: x-averaged buoyancy for all components
     const float ax = ph.dt * bx, ay = ph.dt * (ref ? bx : by), az = ph.dt * (ref ? bx : bz);
@@ -71,21 +72,22 @@ __global__ void __launch_bounds__(kBX * kBY) k_velocity(Model m, Physics ph) {
     float *sp = m.split + pi;
     const int64_t N = m.npml;
     float a0, a1, a2;
-    a0 = sp[S_VXX * N] = split_update(sp[S_VXX * N], ax, xX, kx, mx, px);
-    a1 = sp[S_VXY * N] = split_update(sp[S_VXY * N], ax, xY, ky, my, py);
-    a2 = sp[S_VXZ * N] = split_update(sp[S_VXZ * N], ax, xZ, kz, mz, pz);
+    a0 = sp[S_VXX * N] = split_update<FAST>(sp[S_VXX * N], ax, xX, kx, mx, px);
+    a1 = sp[S_VXY * N] = split_update<FAST>(sp[S_VXY * N], ax, xY, ky, my, py);
+    a2 = sp[S_VXZ * N] = split_update<FAST>(sp[S_VXZ * N], ax, xZ, kz, mz, pz);
     m.f[0][ci] = (a0 + a1) + a2;
-    a0 = sp[S_VYX * N] = split_update(sp[S_VYX * N], ay, yX, kx, mx, px);
-    a1 = sp[S_VYY * N] = split_update(sp[S_VYY * N], ay, yY, ky, my, py);
-    a2 = sp[S_VYZ * N] = split_update(sp[S_VYZ * N], ay, yZ, kz, mz, pz);
+    a0 = sp[S_VYX * N] = split_update<FAST>(sp[S_VYX * N], ay, yX, kx, mx, px);
+    a1 = sp[S_VYY * N] = split_update<FAST>(sp[S_VYY * N], ay, yY, ky, my, py);
+    a2 = sp[S_VYZ * N] = split_update<FAST>(sp[S_VYZ * N], ay, yZ, kz, mz, pz);
     m.f[1][ci] = (a0 + a1) + a2;
-    a0 = sp[S_VZX * N] = split_update(sp[S_VZX * N], az, zX, kx, mx, px);
-    a1 = sp[S_VZY * N] = split_update(sp[S_VZY * N], az, zY, ky, my, py);
-    a2 = sp[S_VZZ * N] = split_update(sp[S_VZZ * N], az, zZ, kz, mz, pz);
+    a0 = sp[S_VZX * N] = split_update<FAST>(sp[S_VZX * N], az, zX, kx, mx, px);
+    a1 = sp[S_VZY * N] = split_update<FAST>(sp[S_VZY * N], az, zY, ky, my, py);
+    a2 = sp[S_VZZ * N] = split_update<FAST>(sp[S_VZZ * N], az, zZ, kz, mz, pz);
     m.f[2][ci] = (a0 + a1) + a2;
 }
 
 // Stress update of one cell (ElasticWaveEquation.cu:528-841, ElasticMacro.h:460-531).
+template <bool FAST>
 __global__ void __launch_bounds__(kBX * kBY) k_stress(Model m, Physics ph) {
     const int cx = blockIdx.x * kBX + threadIdx.x;
     const int cy = blockIdx.y * kBY + threadIdx.y;
@@ -97,23 +99,23 @@ __global__ void __launch_bounds__(kBX * kBY) k_stress(Model m, Physics ph) {
     const float *vx = m.f[0] + ci, *vy = m.f[1] + ci, *vz = m.f[2] + ci;
     const float *r = m.rmu + ci;
 
-    const float dXx = dbwd(ph.c, [&](int o) { return __ldg(vx + o); }) / ph.dx;
-    const float dYy = dbwd(ph.c, [&](int o) { return __ldg(vy + o * SY); }) / ph.dy;
-    const float dZz = dbwd(ph.c, [&](int o) { return __ldg(vz + o * SZ); }) / ph.dz;
-    const float xyY = dfwd(ph.c, [&](int o) { return __ldg(vx + o * SY); }) / ph.dy;
-    const float xyX = dfwd(ph.c, [&](int o) { return __ldg(vy + o); }) / ph.dx;
-    const float xzZ = dfwd(ph.c, [&](int o) { return __ldg(vx + o * SZ); }) / ph.dz;
-    const float xzX = dfwd(ph.c, [&](int o) { return __ldg(vz + o); }) / ph.dx;
-    const float yzZ = dfwd(ph.c, [&](int o) { return __ldg(vy + o * SZ); }) / ph.dz;
-    const float yzY = dfwd(ph.c, [&](int o) { return __ldg(vz + o * SY); }) / ph.dy;
+    const float dXx = dB<FAST, 0>(ph, [&](int o) { return __ldg(vx + o); });
+    const float dYy = dB<FAST, 1>(ph, [&](int o) { return __ldg(vy + o * SY); });
+    const float dZz = dB<FAST, 2>(ph, [&](int o) { return __ldg(vz + o * SZ); });
+    const float xyY = dF<FAST, 1>(ph, [&](int o) { return __ldg(vx + o * SY); });
+    const float xyX = dF<FAST, 0>(ph, [&](int o) { return __ldg(vy + o); });
+    const float xzZ = dF<FAST, 2>(ph, [&](int o) { return __ldg(vx + o * SZ); });
+    const float xzX = dF<FAST, 0>(ph, [&](int o) { return __ldg(vz + o); });
+    const float yzZ = dF<FAST, 2>(ph, [&](int o) { return __ldg(vy + o * SZ); });
+    const float yzY = dF<FAST, 1>(ph, [&](int o) { return __ldg(vz + o * SY); });
 
     const float l = m.lam[ci];
     const float mu0 = m.mu[ci];
     const float l2m = __fmaf_rn(2.0f, mu0, l);
     const bool ref = ph.quirks == 0;   // REF: fourth txz point is mu[x+1, y+1, z]
-    const float mxy = 4.0f / (((r[0] + r[1]) + r[SY]) + r[1 + SY]);
-    const float mxz = 4.0f / (((r[0] + r[1]) + r[SZ]) + (ref ? r[1 + SY] : r[1 + SZ]));
-    const float myz = 4.0f / (((r[0] + r[SY]) + r[SZ]) + r[SY + SZ]);
+    const float mxy = hmean<FAST>(r[0], r[1], r[SY], r[1 + SY]);
+    const float mxz = hmean<FAST>(r[0], r[1], r[SZ], ref ? r[1 + SY] : r[1 + SZ]);
+    const float myz = hmean<FAST>(r[0], r[SY], r[SZ], r[SY + SZ]);
 
     const int kx = band(x, m.nx, m.pml), ky = band(y, m.ny, m.pml), kz = band(z, m.nz, m.pml);
     if (!(kx | ky | kz)) {
@@ -127,37 +129,37 @@ __global__ void __launch_bounds__(kBX * kBY) k_stress(Model m, Physics ph) {
     }
     float mx = 1.f, px = 1.f, my = 1.f, py = 1.f, mz = 1.f, pz = 1.f;
     {
-        const float b0 = m.b[ci];
-        if (kx) damp_factors(ph, 0, ph.dx, kx, m.pml, mu0, b0, l, mx, px);
-        if (ky) damp_factors(ph, 1, ph.dy, ky, m.pml, mu0, b0, l, my, py);
-        if (kz) damp_factors(ph, 2, ph.dz, kz, m.pml, mu0, b0, l, mz, pz);
+        const float v = damp_speed(ph, mu0, m.b[ci], l);
+        if (kx) damp_factors<FAST>(ph, 0, ph.dx, kx, m.pml, v, mx, px);
+        if (ky) damp_factors<FAST>(ph, 1, ph.dy, ky, m.pml, v, my, py);
+        if (kz) damp_factors<FAST>(ph, 2, ph.dz, kz, m.pml, v, mz, pz);
     }
     const int64_t pi = pml_index(m, cx, cy, cz);
     float *sp = m.split + pi;
     const int64_t N = m.npml;
     const float dl = ph.dt * l2m, dt = ph.dt;
     float a0, a1, a2;
-    a0 = sp[S_XXX * N] = split_update(sp[S_XXX * N], dl, dXx, kx, mx, px);
-    a1 = sp[S_XXY * N] = split_update(sp[S_XXY * N], dt, l * dYy, ky, my, py);
-    a2 = sp[S_XXZ * N] = split_update(sp[S_XXZ * N], dt, l * dZz, kz, mz, pz);
+    a0 = sp[S_XXX * N] = split_update<FAST>(sp[S_XXX * N], dl, dXx, kx, mx, px);
+    a1 = sp[S_XXY * N] = split_update<FAST>(sp[S_XXY * N], dt, l * dYy, ky, my, py);
+    a2 = sp[S_XXZ * N] = split_update<FAST>(sp[S_XXZ * N], dt, l * dZz, kz, mz, pz);
     m.f[3][ci] = (a0 + a1) + a2;
-    a0 = sp[S_YYX * N] = split_update(sp[S_YYX * N], dt, l * dXx, kx, mx, px);
-    a1 = sp[S_YYY * N] = split_update(sp[S_YYY * N], dl, dYy, ky, my, py);
-    a2 = sp[S_YYZ * N] = split_update(sp[S_YYZ * N], dt, l * dZz, kz, mz, pz);
+    a0 = sp[S_YYX * N] = split_update<FAST>(sp[S_YYX * N], dt, l * dXx, kx, mx, px);
+    a1 = sp[S_YYY * N] = split_update<FAST>(sp[S_YYY * N], dl, dYy, ky, my, py);
+    a2 = sp[S_YYZ * N] = split_update<FAST>(sp[S_YYZ * N], dt, l * dZz, kz, mz, pz);
     m.f[4][ci] = (a0 + a1) + a2;
-    a0 = sp[S_ZZX * N] = split_update(sp[S_ZZX * N], dt, l * dXx, kx, mx, px);
-    a1 = sp[S_ZZY * N] = split_update(sp[S_ZZY * N], dt, l * dYy, ky, my, py);
-    a2 = sp[S_ZZZ * N] = split_update(sp[S_ZZZ * N], dl, dZz, kz, mz, pz);
+    a0 = sp[S_ZZX * N] = split_update<FAST>(sp[S_ZZX * N], dt, l * dXx, kx, mx, px);
+    a1 = sp[S_ZZY * N] = split_update<FAST>(sp[S_ZZY * N], dt, l * dYy, ky, my, py);
+    a2 = sp[S_ZZZ * N] = split_update<FAST>(sp[S_ZZZ * N], dl, dZz, kz, mz, pz);
     m.f[5][ci] = (a0 + a1) + a2;
     const float axy = dt * mxy, axz = dt * mxz, ayz = dt * myz;
-    a0 = sp[S_XYX * N] = split_update(sp[S_XYX * N], axy, xyX, kx, mx, px);
-    a1 = sp[S_XYY * N] = split_update(sp[S_XYY * N], axy, xyY, ky, my, py);
+    a0 = sp[S_XYX * N] = split_update<FAST>(sp[S_XYX * N], axy, xyX, kx, mx, px);
+    a1 = sp[S_XYY * N] = split_update<FAST>(sp[S_XYY * N], axy, xyY, ky, my, py);
     m.f[6][ci] = a0 + a1;
-    a0 = sp[S_XZX * N] = split_update(sp[S_XZX * N], axz, xzX, kx, mx, px);
-    a1 = sp[S_XZZ * N] = split_update(sp[S_XZZ * N], axz, xzZ, kz, mz, pz);
+    a0 = sp[S_XZX * N] = split_update<FAST>(sp[S_XZX * N], axz, xzX, kx, mx, px);
+    a1 = sp[S_XZZ * N] = split_update<FAST>(sp[S_XZZ * N], axz, xzZ, kz, mz, pz);
     m.f[7][ci] = a0 + a1;
-    a0 = sp[S_YZY * N] = split_update(sp[S_YZY * N], ayz, yzY, ky, my, py);
-    a1 = sp[S_YZZ * N] = split_update(sp[S_YZZ * N], ayz, yzZ, kz, mz, pz);
+    a0 = sp[S_YZY * N] = split_update<FAST>(sp[S_YZY * N], ayz, yzY, ky, my, py);
+    a1 = sp[S_YZZ * N] = split_update<FAST>(sp[S_YZZ * N], ayz, yzZ, kz, mz, pz);
     m.f[8][ci] = a0 + a1;
 }
 
@@ -172,7 +174,7 @@ __global__ void k_record(Model m, SourceRec sr, int it, int velocity_phase) {
 
 __global__ void k_reciprocal(float *rmu, const float *mu, int64_t n) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        rmu[i] = 1.0f / mu[i];   // 1 / mu (ElasticMacro.h:112)
+        rmu[i] = __frcp_rn(mu[i]);   // 1 / mu, IEEE round-to-nearest (ElasticMacro.h:112)
 }
 
 }  // namespace
@@ -190,11 +192,13 @@ cudaError_t simple_step(const Model &m, const Physics &ph, const SourceRec &sr,
     const dim3 block(kBX, kBY);
     const dim3 grid((m.nxc + kBX - 1) / kBX, (m.nyc + kBY - 1) / kBY, m.nzc);
     if (ev) cudaEventRecord(ev[0], s);
-    k_velocity<<<grid, block, 0, s>>>(m, ph);
+    if (ph.fast) k_velocity<true><<<grid, block, 0, s>>>(m, ph);
+    else k_velocity<false><<<grid, block, 0, s>>>(m, ph);
     if (ev) cudaEventRecord(ev[1], s);
     if (sr.nrec > 0) k_record<<<(sr.nrec + 127) / 128, 128, 0, s>>>(m, sr, it, 1);
     if (ev) cudaEventRecord(ev[2], s);
-    k_stress<<<grid, block, 0, s>>>(m, ph);
+    if (ph.fast) k_stress<true><<<grid, block, 0, s>>>(m, ph);
+    else k_stress<false><<<grid, block, 0, s>>>(m, ph);
     if (ev) cudaEventRecord(ev[3], s);
     if (sr.nrec > 0) k_record<<<(sr.nrec + 127) / 128, 128, 0, s>>>(m, sr, it, 0);
     return cudaGetLastError();

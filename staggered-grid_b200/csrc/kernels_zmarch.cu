@@ -1,0 +1,827 @@
+// kernels_zmarch.cu — the "zmarch" kernel family: 2.5-D z-marching velocity
+// and stress updates for sm_100a.
+//
+// Work decomposition.  A CTA of 256 threads owns a 32 x TY tile of computed
+// cells in the xy plane (TY = 8 * CELLS, each thread owning CELLS cells in
+// rows ty, ty + 8, ...) and marches along z over a chunk of planes.
+//
+// Data movement per plane z (all HBM traffic is TMA or coalesced 128-byte rows):
+//   * TMA (cp.async.bulk.tensor.3d, one elected thread, no multicast) stages
+//     the xy boxes the x/y derivatives need — tile plus its 5-cell halo on the
+//     sides a field is differentiated along — and the "lead" planes that feed
+//     the z register queues, into a 3-stage shared-memory ring guarded by one
+//     mbarrier per stage (expect-tx bytes, parity wait with an iteration cap).
+//     A stage is refilled with plane z + 3 as soon as plane z is done, so
+//     every load has two plane-iterations to land.
+//   * Each thread keeps the 10 z-taps of the fields it differentiates along z
+//     in a register queue (sigma_xz, sigma_yz, sigma_zz for the velocity
+//     update; vx, vy, vz for the stress update), shifted by one per plane.
+//   * Own-cell read-modify-write data (velocities, or stresses and the
+//     medium) are loaded one plane ahead into registers with plain coalesced
+//     loads; PML split fields are loaded before the plane's TMA wait.
+// Every row starts at a 128-byte boundary (the device arrays are shifted by
+// kXOff), so x-halo boxes start 8 cells left of the tile (48 wide), centre
+// boxes are exactly 32 wide, and every TMA x coordinate is a multiple of 4.
+// One block barrier per plane separates the reads of a stage from its refill
+// and carries the abort vote of the bounded waits.
+//
+// PML cells take the split-field path (cell_math.cuh), interior cells the
+// plain update; a tile-plane with no PML cell never enters the PML code.
+// The source (dt*dt*s(it) on txx, tyy, tzz, OPT/ElasticWaveEquation.cu:206-221)
+// is applied to the staged copies the velocity update reads and to the old
+// value the stress update accumulates onto, which reproduces the reference's
+// store-then-read order exactly; receivers are written from registers.
+// Arithmetic per cell is the same sequence as kernels_simple.cu and the oracle.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <type_traits>
+
+#include "cell_math.cuh"
+#include "zmarch.h"
+
+namespace sgfd {
+
+namespace {
+
+constexpr int TX = kZTileX, NT = 256, S = 3;
+constexpr int W48 = 48, W32 = 32, W36 = 36, RW = 33;
+
+constexpr int al128(int b) { return (b + 127) / 128 * 128; }
+
+// Shared-memory stage layout of the velocity update (bytes, 128-aligned boxes).
+template <int TY>
+struct VelL {
+    static constexpr int SXX = 0;                                  // 48 x TY       sigma_xx (x halo)
+    static constexpr int SYY = SXX + al128(W48 * TY * 4);          // 32 x (TY+10)  sigma_yy (y halo)
+    static constexpr int SXY = SYY + al128(W32 * (TY + 10) * 4);   // 48 x (TY+10)  sigma_xy (x, y halo)
+    static constexpr int SXZ = SXY + al128(W48 * (TY + 10) * 4);   // 48 x TY       sigma_xz (x halo)
+    static constexpr int SYZ = SXZ + al128(W48 * TY * 4);          // 32 x (TY+10)  sigma_yz (y halo)
+    static constexpr int B = SYZ + al128(W32 * (TY + 10) * 4);     // 36 x (TY+1)   buoyancy (x+1, y+1)
+    static constexpr int LXZ = B + al128(W36 * (TY + 1) * 4);      // 32 x TY       sigma_xz at z+4
+    static constexpr int LYZ = LXZ + al128(W32 * TY * 4);          // 32 x TY       sigma_yz at z+4
+    static constexpr int LZZ = LYZ + al128(W32 * TY * 4);          // 32 x TY       sigma_zz at z+5
+    static constexpr int LB = LZZ + al128(W32 * TY * 4);           // 32 x TY       buoyancy at z+1
+    static constexpr int STAGE = LB + al128(W32 * TY * 4);
+    static constexpr uint32_t TXB = 4 * (2 * W48 * TY + 2 * W32 * (TY + 10) + W48 * (TY + 10) +
+                                         W36 * (TY + 1) + 4 * W32 * TY);
+};
+// Shared-memory stage layout of the stress update.
+template <int TY>
+struct StrL {
+    static constexpr int VX = 0;                                   // 48 x (TY+10)  vx (x, y halo)
+    static constexpr int VY = VX + al128(W48 * (TY + 10) * 4);     // 48 x (TY+10)  vy
+    static constexpr int VZ = VY + al128(W48 * (TY + 10) * 4);     // 48 x (TY+10)  vz
+    static constexpr int MU = VZ + al128(W48 * (TY + 10) * 4);     // 36 x (TY+1)   mu at z+2
+    static constexpr int LX = MU + al128(W36 * (TY + 1) * 4);      // 32 x TY       vx at z+5
+    static constexpr int LY = LX + al128(W32 * TY * 4);            // 32 x TY       vy at z+5
+    static constexpr int LZ = LY + al128(W32 * TY * 4);            // 32 x TY       vz at z+4
+    static constexpr int STAGE = LZ + al128(W32 * TY * 4);
+    static constexpr uint32_t TXB = 4 * (3 * W48 * (TY + 10) + W36 * (TY + 1) + 3 * W32 * TY);
+};
+
+constexpr uint32_t kWaitCap = 2000;
+constexpr uint32_t kSuspendNs = 1000000;
+
+__device__ __forceinline__ uint32_t sptr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(sptr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(sptr(bar)), "r"(bytes) : "memory");
+}
+// One poll of the phase; the thread may sleep in the poll for up to
+// kSuspendNs (it wakes as soon as the phase completes).
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok) : "r"(sptr(bar)), "r"(parity), "n"(kSuspendNs) : "memory");
+    return ok != 0;
+}
+// Bounded wait: false after kWaitCap polls (about kWaitCap * kSuspendNs at most).
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+    for (uint32_t i = 0; i < kWaitCap; ++i)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+__device__ __forceinline__ void fence_barrier_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__device__ __forceinline__ void tma3(void *dst, const CUtensorMap *map, int x, int y, int z, uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+        ::"r"(sptr(dst)), "l"(map), "r"(x), "r"(y), "r"(z), "r"(sptr(bar))
+        : "memory");
+}
+
+struct Tile {
+    int cx0, cy0;    // computed coordinates of the tile origin
+    int xd;          // device x of the tile origin (128-byte aligned)
+    int gx0, gy0;    // GRID coordinates of the tile origin
+    int zs, ze;      // computed z range of this CTA
+    bool xy_pml;     // the tile touches the x or y PML band
+};
+
+template <int TY>
+__device__ __forceinline__ Tile make_tile(const Model &m, const ZGeom &g) {
+    Tile t;
+    const int tile = blockIdx.x;
+    t.cx0 = (tile % g.ntx) * TX;
+    t.cy0 = (tile / g.ntx) * TY;
+    t.gx0 = t.cx0 + kHalo;
+    t.gy0 = t.cy0 + kHalo;
+    t.xd = t.gx0 + kXOff;
+    t.zs = blockIdx.y * g.zc;
+    t.ze = min(t.zs + g.zc, m.nzc);
+    t.xy_pml = t.cx0 < m.pml || t.cx0 + TX > m.nxc - m.pml || t.cy0 < m.pml || t.cy0 + TY > m.nyc - m.pml;
+    return t;
+}
+
+// Wait (bounded) for the stages still in flight before an early exit.
+__device__ void drain(uint64_t *bar, int issued_end, int from, int zs) {
+    for (int j = from; j < issued_end; ++j) mbar_wait(&bar[(j - zs) % S], (uint32_t)(((j - zs) / S) & 1));
+}
+
+// 128-byte aligned start inside the dynamic shared array.  The offset is
+// computed on the shared-window address so the result stays a pointer into
+// __shared__ memory (the compiler then emits shared loads for every box read).
+__device__ __forceinline__ unsigned char *align_smem(unsigned char *p) {
+    return p + ((128u - (sptr(p) & 127u)) & 127u);
+}
+
+// ---------------------------------------------------------------------------
+// velocity update
+// ---------------------------------------------------------------------------
+
+template <int TY>
+__device__ __forceinline__ void vel_issue(const VelMaps &mp, unsigned char *st, uint64_t *bar, const Tile &t, int cz) {
+    using L = VelL<TY>;
+    const int gz = cz + kHalo;
+    mbar_expect_tx(bar, L::TXB);
+    tma3(st + L::SXX, &mp.sxx, t.xd - 8, t.gy0, gz, bar);
+    tma3(st + L::SYY, &mp.syy, t.xd, t.gy0 - 5, gz, bar);
+    tma3(st + L::SXY, &mp.sxy, t.xd - 8, t.gy0 - 5, gz, bar);
+    tma3(st + L::SXZ, &mp.sxz, t.xd - 8, t.gy0, gz, bar);
+    tma3(st + L::SYZ, &mp.syz, t.xd, t.gy0 - 5, gz, bar);
+    tma3(st + L::B, &mp.b, t.xd, t.gy0, gz, bar);
+    tma3(st + L::LXZ, &mp.sxz_c, t.xd, t.gy0, gz + 4, bar);
+    tma3(st + L::LYZ, &mp.syz_c, t.xd, t.gy0, gz + 4, bar);
+    tma3(st + L::LZZ, &mp.szz_c, t.xd, t.gy0, gz + 5, bar);
+    tma3(st + L::LB, &mp.b_c, t.xd, t.gy0, gz + 1, bar);
+}
+
+template <bool FAST, int CELLS>
+__global__ void __launch_bounds__(NT, 2)
+k_velocity_zmarch(const __grid_constant__ VelMaps mp, const __grid_constant__ Model m, const __grid_constant__ Physics ph,
+                  const __grid_constant__ ZGeom g, const __grid_constant__ SourceRec sr, int it,
+                  float src_value, int use_wavelet) {
+    constexpr int TY = 8 * CELLS;
+    using L = VelL<TY>;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    unsigned char *smem = align_smem(smem_raw);
+    __shared__ __align__(8) uint64_t bar[S];
+    const Tile t = make_tile<TY>(m, g);
+    const int tid = threadIdx.x, lx = tid & 31, ty = tid >> 5;
+    if (tid == 0) {
+        for (int s = 0; s < S; ++s) mbar_init(&bar[s], 1);
+        fence_barrier_init();
+    }
+    __syncthreads();
+    int issued_end = t.zs;   // planes [zs, issued_end) issued (meaningful in thread 0)
+    if (tid == 0) {
+        for (int s = 0; s < S && t.zs + s < t.ze; ++s) vel_issue<TY>(mp, smem + s * L::STAGE, &bar[s], t, t.zs + s);
+        issued_end = min(t.zs + S, t.ze);
+    }
+
+    const float inj = ph.inj_dt2 * ((use_wavelet && sr.wavelet) ? sr.wavelet[it] : src_value);
+    int sx = -1, sy = -1, sz = -1;
+    if (sr.src >= 0) {
+        const int64_t r = sr.src;
+        sz = (int)(r / m.plane);
+        sy = (int)((r - (int64_t)sz * m.plane) / m.px);
+        sx = (int)(r - (int64_t)sz * m.plane - (int64_t)sy * m.px);
+    }
+
+    const int gx = t.gx0 + lx;
+    const int kx = band(gx, m.nx, m.pml);
+    int lyc[CELLS], gyc[CELLS], kyc[CELLS];
+    bool act[CELLS];
+    uint32_t col[CELLS];          // element offset of the thread's column at z = 0
+    PmlColumn pcol[CELLS];
+    const uint32_t PL = (uint32_t)m.plane;
+#pragma unroll
+    for (int c = 0; c < CELLS; ++c) {
+        lyc[c] = ty + 8 * c;
+        gyc[c] = t.gy0 + lyc[c];
+        act[c] = (t.cx0 + lx < m.nxc) && (t.cy0 + lyc[c] < m.nyc);
+        kyc[c] = band(gyc[c], m.ny, m.pml);
+        // inactive threads of edge tiles address a valid cell (results discarded)
+        col[c] = (uint32_t)pidx(m, min(gx, m.nx - 1), min(gyc[c], m.ny - 1), 0);
+        pcol[c] = pml_column(m, min(t.cx0 + lx, m.nxc - 1), min(t.cy0 + lyc[c], m.nyc - 1));
+    }
+
+    // z queues: qxz, qyz hold z-5..z+4, qzz holds z-4..z+5 (filled 9 deep here)
+    float qxz[CELLS][10], qyz[CELLS][10], qzz[CELLS][10];
+    const int gz0 = t.zs + kHalo;
+#pragma unroll
+    for (int c = 0; c < CELLS; ++c) {
+#pragma unroll
+        for (int k = 0; k < 9; ++k) {
+            qxz[c][k + 1] = m.f[7][col[c] + (uint32_t)(gz0 - 5 + k) * PL];
+            qyz[c][k + 1] = m.f[8][col[c] + (uint32_t)(gz0 - 5 + k) * PL];
+            float zz = m.f[5][col[c] + (uint32_t)(gz0 - 4 + k) * PL];
+            if (gx == sx && gyc[c] == sy && gz0 - 4 + k == sz) zz = zz + inj;
+            qzz[c][k + 1] = zz;
+        }
+    }
+    // own-cell velocities of the first plane (interior cells only need them)
+    float vcur[CELLS][3];
+    {
+#pragma unroll
+        for (int c = 0; c < CELLS; ++c) {
+            const uint32_t ci = col[c] + (uint32_t)gz0 * PL;
+#pragma unroll
+            for (int q = 0; q < 3; ++q) vcur[c][q] = m.f[q][ci];
+        }
+    }
+
+    // receivers of this tile, sorted by z: skip those below the chunk
+    int rp = g.rec_off[blockIdx.x];
+    const int rend = g.rec_off[blockIdx.x + 1];
+    while (rp < rend && g.rec_list[rp].z < gz0) ++rp;
+    int rz = rp < rend ? g.rec_list[rp].z : 0x7fffffff;   // z of the next receiver
+
+    bool failed = false, abort = false;
+    int cz = t.zs;
+    const bool src_near = sr.src >= 0 && sy >= t.gy0 - 5 && sy < t.gy0 + TY + 5 && sx >= t.gx0 - 8 &&
+                          sx < t.gx0 + TX + 8;
+    // One plane.  GEN selects the general path (PML cells, source, receivers);
+    // the interior-only path is used for every other tile-plane.  Returns
+    // false when the block votes to abort.
+    auto plane = [&](auto gen_tag) -> bool {
+        constexpr bool GEN = decltype(gen_tag)::value;
+        const int k = cz - t.zs;
+        const int s = k % S;
+        unsigned char *st = smem + s * L::STAGE;
+        const int gz = cz + kHalo;
+        const int kz = band(gz, m.nz, m.pml);
+        const bool plane_pml = GEN && (t.xy_pml || kz != 0);
+
+        // own-cell velocities of the next plane (plane gz+1 <= nz-5 is always inside the grid)
+        float vnxt[CELLS][3];
+#pragma unroll
+        for (int c = 0; c < CELLS; ++c) {
+            const uint32_t ci = col[c] + (uint32_t)(gz + 1) * PL;
+#pragma unroll
+            for (int q = 0; q < 3; ++q) vnxt[c][q] = m.f[q][ci];
+        }
+
+        if (!mbar_wait(&bar[s], (uint32_t)((k / S) & 1))) failed = true;
+
+        // source patch of the staged copies (uniform branch)
+        if (GEN && src_near && (gz == sz || gz + 5 == sz)) {
+            if (tid == 0) {
+                const int ox = sx - t.gx0, oy = sy - t.gy0;
+                if (gz == sz) {
+                    float *sxx = reinterpret_cast<float *>(st + L::SXX);
+                    float *syy = reinterpret_cast<float *>(st + L::SYY);
+                    if (oy >= 0 && oy < TY && ox + 8 >= 0 && ox + 8 < W48) sxx[oy * W48 + ox + 8] += inj;
+                    if (oy + 5 >= 0 && oy + 5 < TY + 10 && ox >= 0 && ox < W32) syy[(oy + 5) * W32 + ox] += inj;
+                }
+                if (gz + 5 == sz) {
+                    float *szz = reinterpret_cast<float *>(st + L::LZZ);
+                    if (oy >= 0 && oy < TY && ox >= 0 && ox < W32) szz[oy * W32 + ox] += inj;
+                }
+            }
+            __syncthreads();
+        }
+
+        const float *sxx = reinterpret_cast<const float *>(st + L::SXX);
+        const float *syy = reinterpret_cast<const float *>(st + L::SYY);
+        const float *sxy = reinterpret_cast<const float *>(st + L::SXY);
+        const float *sxz = reinterpret_cast<const float *>(st + L::SXZ);
+        const float *syz = reinterpret_cast<const float *>(st + L::SYZ);
+        const float *bb = reinterpret_cast<const float *>(st + L::B);
+        const float *lxz = reinterpret_cast<const float *>(st + L::LXZ);
+        const float *lyz = reinterpret_cast<const float *>(st + L::LYZ);
+        const float *lzz = reinterpret_cast<const float *>(st + L::LZZ);
+        const float *lb = reinterpret_cast<const float *>(st + L::LB);
+
+#pragma unroll
+        for (int c = 0; c < CELLS; ++c) {
+            const int ly = lyc[c];
+            // advance the z queues
+#pragma unroll
+            for (int j = 0; j < 9; ++j) {
+                qxz[c][j] = qxz[c][j + 1];
+                qyz[c][j] = qyz[c][j + 1];
+                qzz[c][j] = qzz[c][j + 1];
+            }
+            qxz[c][9] = lxz[ly * W32 + lx];
+            qyz[c][9] = lyz[ly * W32 + lx];
+            qzz[c][9] = lzz[ly * W32 + lx];
+            if (!act[c]) continue;
+
+            const float *rxx = sxx + ly * W48 + lx + 8;
+            const float *cxy = sxy + (ly + 5) * W48 + lx + 8;
+            const float *rxz = sxz + ly * W48 + lx + 8;
+            const float *cyy = syy + (ly + 5) * W32 + lx;
+            const float *cyz = syz + (ly + 5) * W32 + lx;
+            const float xX = dF<FAST, 0>(ph, [&](int o) { return rxx[o]; });
+            const float xY = dB<FAST, 1>(ph, [&](int o) { return cxy[o * W48]; });
+            const float xZ = dB<FAST, 2>(ph, [&](int o) { return qxz[c][5 + o]; });
+            const float yX = dB<FAST, 0>(ph, [&](int o) { return cxy[o]; });
+            const float yY = dF<FAST, 1>(ph, [&](int o) { return cyy[o * W32]; });
+            const float yZ = dB<FAST, 2>(ph, [&](int o) { return qyz[c][5 + o]; });
+            const float zX = dB<FAST, 0>(ph, [&](int o) { return rxz[o]; });
+            const float zY = dB<FAST, 1>(ph, [&](int o) { return cyz[o * W32]; });
+            const float zZ = dF<FAST, 2>(ph, [&](int o) { return qzz[c][4 + o]; });
+            const float b0 = bb[ly * W36 + lx];
+            const float bx = (b0 + bb[ly * W36 + lx + 1]) / 2.0f;
+            const float by = (b0 + bb[(ly + 1) * W36 + lx]) / 2.0f;
+            const float bz = (b0 + lb[ly * W32 + lx]) / 2.0f;
+
+            const uint32_t ci = col[c] + (uint32_t)gz * PL;
+            float vnew[3];
+            const int ky = kyc[c];
+            if (!(plane_pml && (kx | ky | kz))) {
+                vnew[0] = __fmaf_rn(ph.dt * bx, (xX + xY) + xZ, vcur[c][0]);
+                vnew[1] = __fmaf_rn(ph.dt * by, (yX + yY) + yZ, vcur[c][1]);
+                vnew[2] = __fmaf_rn(ph.dt * bz, (zX + zY) + zZ, vcur[c][2]);
+            } else {
+                float mx = 1.f, px = 1.f, my = 1.f, py = 1.f, mz = 1.f, pz = 1.f;
+                {
+                    const float v = damp_speed(ph, m.mu[ci], b0, ph.damping == 1 ? m.lam[ci] : 0.f);
+                    if (kx) damp_factors<FAST>(ph, 0, ph.dx, kx, m.pml, v, mx, px);
+                    if (ky) damp_factors<FAST>(ph, 1, ph.dy, ky, m.pml, v, my, py);
+                    if (kz) damp_factors<FAST>(ph, 2, ph.dz, kz, m.pml, v, mz, pz);
+                }
+                const bool ref = ph.quirks == 0;
+                const float ax = ph.dt * bx, ay = ph.dt * (ref ? bx : by), az = ph.dt * (ref ? bx : bz);
+                float *sp = m.split + pml_plane_index(m, pcol[c], cz);
+                const uint32_t N = (uint32_t)m.npml;
+                float o[9];
+#pragma unroll
+                for (int q = 0; q < 9; ++q) o[q] = sp[q * N];
+                float a0, a1, a2;
+                a0 = split_update<FAST>(o[S_VXX], ax, xX, kx, mx, px);
+                a1 = split_update<FAST>(o[S_VXY], ax, xY, ky, my, py);
+                a2 = split_update<FAST>(o[S_VXZ], ax, xZ, kz, mz, pz);
+                sp[S_VXX * N] = a0; sp[S_VXY * N] = a1; sp[S_VXZ * N] = a2;
+                vnew[0] = (a0 + a1) + a2;
+                a0 = split_update<FAST>(o[S_VYX], ay, yX, kx, mx, px);
+                a1 = split_update<FAST>(o[S_VYY], ay, yY, ky, my, py);
+                a2 = split_update<FAST>(o[S_VYZ], ay, yZ, kz, mz, pz);
+                sp[S_VYX * N] = a0; sp[S_VYY * N] = a1; sp[S_VYZ * N] = a2;
+                vnew[1] = (a0 + a1) + a2;
+                a0 = split_update<FAST>(o[S_VZX], az, zX, kx, mx, px);
+                a1 = split_update<FAST>(o[S_VZY], az, zY, ky, my, py);
+                a2 = split_update<FAST>(o[S_VZZ], az, zZ, kz, mz, pz);
+                sp[S_VZX * N] = a0; sp[S_VZY * N] = a1; sp[S_VZZ * N] = a2;
+                vnew[2] = (a0 + a1) + a2;
+            }
+            m.f[0][ci] = vnew[0];
+            m.f[1][ci] = vnew[1];
+            m.f[2][ci] = vnew[2];
+            // receivers of velocity components at this cell (list sorted by z)
+            if (GEN && gz == rz && it >= 0 && it < sr.nt) {
+                for (int r = rp; r < rend && g.rec_list[r].z == gz; ++r) {
+                    const int4 q = g.rec_list[r];
+                    if (q.x == gx && q.y == gyc[c] && q.w <= 2)
+                        sr.traces[(int64_t)it * sr.nrec + g.rec_idx[r]] =
+                            q.w == 0 ? vnew[0] : q.w == 1 ? vnew[1] : vnew[2];
+                }
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < CELLS; ++c)
+#pragma unroll
+            for (int q = 0; q < 3; ++q) vcur[c][q] = vnxt[c][q];
+        if (GEN && gz == rz) {
+            while (rp < rend && g.rec_list[rp].z == gz) ++rp;
+            rz = rp < rend ? g.rec_list[rp].z : 0x7fffffff;
+        }
+
+        // every thread is done with this stage: vote on aborts, then refill it
+        if (__syncthreads_or(failed)) return false;
+        if (tid == 0 && cz + S < t.ze) {
+            fence_proxy_async();
+            vel_issue<TY>(mp, st, &bar[s], t, cz + S);
+            issued_end = cz + S + 1;
+        }
+        return true;
+    };
+    for (; cz < t.ze; ++cz) {
+        const int gzp = cz + kHalo;
+        const bool gen = t.xy_pml || band(gzp, m.nz, m.pml) != 0 || (src_near && (gzp == sz || gzp + 5 == sz)) || gzp == rz;
+        if (!(gen ? plane(std::true_type{}) : plane(std::false_type{}))) {
+            abort = true;
+            break;
+        }
+    }
+    if (abort && tid == 0) {
+        atomicExch(g.err, 1);
+        drain(bar, issued_end, cz, t.zs);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// stress update
+// ---------------------------------------------------------------------------
+
+template <int TY>
+__device__ __forceinline__ void str_issue(const StrMaps &mp, unsigned char *st, uint64_t *bar, const Tile &t, int cz) {
+    using L = StrL<TY>;
+    const int gz = cz + kHalo;
+    mbar_expect_tx(bar, L::TXB);
+    tma3(st + L::VX, &mp.vx, t.xd - 8, t.gy0 - 5, gz, bar);
+    tma3(st + L::VY, &mp.vy, t.xd - 8, t.gy0 - 5, gz, bar);
+    tma3(st + L::VZ, &mp.vz, t.xd - 8, t.gy0 - 5, gz, bar);
+    tma3(st + L::MU, &mp.mu, t.xd, t.gy0, gz + 2, bar);
+    tma3(st + L::LX, &mp.vx_c, t.xd, t.gy0, gz + 5, bar);
+    tma3(st + L::LY, &mp.vy_c, t.xd, t.gy0, gz + 5, bar);
+    tma3(st + L::LZ, &mp.vz_c, t.xd, t.gy0, gz + 4, bar);
+}
+
+template <bool FAST, int CELLS>
+__global__ void __launch_bounds__(NT, 2)
+k_stress_zmarch(const __grid_constant__ StrMaps mp, const __grid_constant__ Model m, const __grid_constant__ Physics ph,
+                  const __grid_constant__ ZGeom g, const __grid_constant__ SourceRec sr, int it,
+                float src_value, int use_wavelet) {
+    constexpr int TY = 8 * CELLS;
+    constexpr int RH = TY + 1;       // 1/mu tile: (x0..x0+32) x (y0..y0+TY)
+    using L = StrL<TY>;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    unsigned char *smem = align_smem(smem_raw);
+    __shared__ __align__(8) uint64_t bar[S];
+    __shared__ float rmu[3][RH * RW];    // ring: 1/mu of planes z, z+1, z+2
+    const Tile t = make_tile<TY>(m, g);
+    const int tid = threadIdx.x, lx = tid & 31, ty = tid >> 5;
+    if (tid == 0) {
+        for (int s = 0; s < S; ++s) mbar_init(&bar[s], 1);
+        fence_barrier_init();
+    }
+    __syncthreads();
+    int issued_end = t.zs;
+    if (tid == 0) {
+        for (int s = 0; s < S && t.zs + s < t.ze; ++s) str_issue<TY>(mp, smem + s * L::STAGE, &bar[s], t, t.zs + s);
+        issued_end = min(t.zs + S, t.ze);
+    }
+
+    const float inj = ph.inj_dt2 * ((use_wavelet && sr.wavelet) ? sr.wavelet[it] : src_value);
+    const int64_t src = sr.src;
+
+    const int gx = t.gx0 + lx;
+    const int kx = band(gx, m.nx, m.pml);
+    int lyc[CELLS], gyc[CELLS], kyc[CELLS];
+    bool act[CELLS];
+    uint32_t col[CELLS];          // element offset of the thread's column at z = 0
+    PmlColumn pcol[CELLS];
+    const uint32_t PL = (uint32_t)m.plane;
+#pragma unroll
+    for (int c = 0; c < CELLS; ++c) {
+        lyc[c] = ty + 8 * c;
+        gyc[c] = t.gy0 + lyc[c];
+        act[c] = (t.cx0 + lx < m.nxc) && (t.cy0 + lyc[c] < m.nyc);
+        kyc[c] = band(gyc[c], m.ny, m.pml);
+        // inactive threads of edge tiles address a valid cell (results discarded)
+        col[c] = (uint32_t)pidx(m, min(gx, m.nx - 1), min(gyc[c], m.ny - 1), 0);
+        pcol[c] = pml_column(m, min(t.cx0 + lx, m.nxc - 1), min(t.cy0 + lyc[c], m.nyc - 1));
+    }
+
+    // z queues: qx, qy hold z-4..z+5 (vx, vy); qz holds z-5..z+4 (vz)
+    float qx[CELLS][10], qy[CELLS][10], qz[CELLS][10];
+    const int gz0 = t.zs + kHalo;
+#pragma unroll
+    for (int c = 0; c < CELLS; ++c) {
+#pragma unroll
+        for (int k = 0; k < 9; ++k) {
+            qx[c][k + 1] = m.f[0][col[c] + (uint32_t)(gz0 - 4 + k) * PL];
+            qy[c][k + 1] = m.f[1][col[c] + (uint32_t)(gz0 - 4 + k) * PL];
+            qz[c][k + 1] = m.f[2][col[c] + (uint32_t)(gz0 - 5 + k) * PL];
+        }
+    }
+    // 1/mu of the first two planes
+    for (int e = tid; e < 2 * RH * RW; e += NT) {
+        const int p = e / (RH * RW), r = e % (RH * RW);
+        const int ex = r % RW, ey = r / RW;
+        const int gxe = min(t.gx0 + ex, m.nx - 1), gye = min(t.gy0 + ey, m.ny - 1);
+        rmu[p][r] = __frcp_rn(m.mu[pidx(m, gxe, gye, gz0 + p)]);
+    }
+    // own-cell stresses (interior cells) and medium of the first plane
+    float scur[CELLS][6], lcur[CELLS], mcur[CELLS];
+#pragma unroll
+    for (int c = 0; c < CELLS; ++c) {
+        const uint32_t ci = col[c] + (uint32_t)gz0 * PL;
+#pragma unroll
+        for (int q = 0; q < 6; ++q) scur[c][q] = m.f[3 + q][ci];
+        lcur[c] = m.lam[ci];
+        mcur[c] = m.mu[ci];
+    }
+
+    int rp = g.rec_off[blockIdx.x];
+    const int rend = g.rec_off[blockIdx.x + 1];
+    while (rp < rend && g.rec_list[rp].z < gz0) ++rp;
+    int rz = rp < rend ? g.rec_list[rp].z : 0x7fffffff;
+    __syncthreads();   // rmu warm-up visible
+
+    bool failed = false, abort = false;
+    int cz = t.zs;
+    int sz = -1;
+    if (src >= 0) sz = (int)(src / m.plane);
+    // One plane.  GEN selects the general path (PML cells, source, receivers);
+    // the interior-only path is used for every other tile-plane.  Returns
+    // false when the block votes to abort.
+    auto plane = [&](auto gen_tag) -> bool {
+        constexpr bool GEN = decltype(gen_tag)::value;
+        const int k = cz - t.zs;
+        const int s = k % S;
+        unsigned char *st = smem + s * L::STAGE;
+        const int gz = cz + kHalo;
+        const int kz = band(gz, m.nz, m.pml);
+        const bool plane_pml = GEN && (t.xy_pml || kz != 0);
+
+        // own-cell data of the next plane (plane gz+1 <= nz-5 is always inside the grid)
+        float snxt[CELLS][6], lnxt[CELLS], mnxt[CELLS];
+#pragma unroll
+        for (int c = 0; c < CELLS; ++c) {
+            const uint32_t ci = col[c] + (uint32_t)(gz + 1) * PL;
+#pragma unroll
+            for (int q = 0; q < 6; ++q) snxt[c][q] = m.f[3 + q][ci];
+            lnxt[c] = m.lam[ci];
+            mnxt[c] = m.mu[ci];
+        }
+
+        if (!mbar_wait(&bar[s], (uint32_t)((k / S) & 1))) failed = true;
+
+        // 1/mu of plane z+2 into the ring (read from iteration k+1 on)
+        {
+            const float *mub = reinterpret_cast<const float *>(st + L::MU);
+            float *rn = rmu[(k + 2) % 3];
+            for (int e = tid; e < RH * RW; e += NT) {
+                const int ex = e % RW, ey = e / RW;
+                rn[e] = __frcp_rn(mub[ey * W36 + ex]);
+            }
+        }
+        const float *r0 = rmu[k % 3];
+        const float *r1 = rmu[(k + 1) % 3];
+
+        const float *svx = reinterpret_cast<const float *>(st + L::VX);
+        const float *svy = reinterpret_cast<const float *>(st + L::VY);
+        const float *svz = reinterpret_cast<const float *>(st + L::VZ);
+        const float *llx = reinterpret_cast<const float *>(st + L::LX);
+        const float *lly = reinterpret_cast<const float *>(st + L::LY);
+        const float *llz = reinterpret_cast<const float *>(st + L::LZ);
+
+#pragma unroll
+        for (int c = 0; c < CELLS; ++c) {
+            const int ly = lyc[c];
+#pragma unroll
+            for (int j = 0; j < 9; ++j) {
+                qx[c][j] = qx[c][j + 1];
+                qy[c][j] = qy[c][j + 1];
+                qz[c][j] = qz[c][j + 1];
+            }
+            qx[c][9] = llx[ly * W32 + lx];
+            qy[c][9] = lly[ly * W32 + lx];
+            qz[c][9] = llz[ly * W32 + lx];
+            if (!act[c]) continue;
+
+            const float *cx_ = svx + (ly + 5) * W48 + lx + 8;
+            const float *cy_ = svy + (ly + 5) * W48 + lx + 8;
+            const float *cz_ = svz + (ly + 5) * W48 + lx + 8;
+            const float dXx = dB<FAST, 0>(ph, [&](int o) { return cx_[o]; });
+            const float dYy = dB<FAST, 1>(ph, [&](int o) { return cy_[o * W48]; });
+            const float dZz = dB<FAST, 2>(ph, [&](int o) { return qz[c][5 + o]; });
+            const float xyY = dF<FAST, 1>(ph, [&](int o) { return cx_[o * W48]; });
+            const float xyX = dF<FAST, 0>(ph, [&](int o) { return cy_[o]; });
+            const float xzZ = dF<FAST, 2>(ph, [&](int o) { return qx[c][4 + o]; });
+            const float xzX = dF<FAST, 0>(ph, [&](int o) { return cz_[o]; });
+            const float yzZ = dF<FAST, 2>(ph, [&](int o) { return qy[c][4 + o]; });
+            const float yzY = dF<FAST, 1>(ph, [&](int o) { return cz_[o * W48]; });
+
+            const float l = lcur[c];
+            const float l2m = __fmaf_rn(2.0f, mcur[c], l);
+            const bool ref = ph.quirks == 0;
+            const int e0 = ly * RW + lx;
+            const float mxy = hmean<FAST>(r0[e0], r0[e0 + 1], r0[e0 + RW], r0[e0 + 1 + RW]);
+            const float mxz = hmean<FAST>(r0[e0], r0[e0 + 1], r1[e0], ref ? r0[e0 + 1 + RW] : r1[e0 + 1]);
+            const float myz = hmean<FAST>(r0[e0], r0[e0 + RW], r1[e0], r1[e0 + RW]);
+
+            const uint32_t ci = col[c] + (uint32_t)gz * PL;
+            const int ky = kyc[c];
+            float snew[6];
+            if (!(plane_pml && (kx | ky | kz))) {
+                float o0 = scur[c][0], o1 = scur[c][1], o2 = scur[c][2];
+                if (GEN && (int64_t)ci == src) { o0 = o0 + inj; o1 = o1 + inj; o2 = o2 + inj; }
+                snew[0] = __fmaf_rn(ph.dt, __fmaf_rn(l2m, dXx, l * (dYy + dZz)), o0);
+                snew[1] = __fmaf_rn(ph.dt, __fmaf_rn(l2m, dYy, l * (dXx + dZz)), o1);
+                snew[2] = __fmaf_rn(ph.dt, __fmaf_rn(l2m, dZz, l * (dXx + dYy)), o2);
+                snew[3] = __fmaf_rn(ph.dt * mxy, xyY + xyX, scur[c][3]);
+                snew[4] = __fmaf_rn(ph.dt * mxz, xzZ + xzX, scur[c][4]);
+                snew[5] = __fmaf_rn(ph.dt * myz, yzZ + yzY, scur[c][5]);
+            } else {
+                float *sp = m.split + pml_plane_index(m, pcol[c], cz);
+                const uint32_t N = (uint32_t)m.npml;
+                float o[15];
+#pragma unroll
+                for (int q = 0; q < 15; ++q) o[q] = sp[(S_XXX + q) * N];
+                float mx = 1.f, px = 1.f, my = 1.f, py = 1.f, mz = 1.f, pz = 1.f;
+                {
+                    const float v = damp_speed(ph, mcur[c], m.b[ci], l);
+                    if (kx) damp_factors<FAST>(ph, 0, ph.dx, kx, m.pml, v, mx, px);
+                    if (ky) damp_factors<FAST>(ph, 1, ph.dy, ky, m.pml, v, my, py);
+                    if (kz) damp_factors<FAST>(ph, 2, ph.dz, kz, m.pml, v, mz, pz);
+                }
+                const float dl = ph.dt * l2m, dt = ph.dt;
+                float a0, a1, a2;
+                a0 = split_update<FAST>(o[S_XXX - S_XXX], dl, dXx, kx, mx, px);
+                a1 = split_update<FAST>(o[S_XXY - S_XXX], dt, l * dYy, ky, my, py);
+                a2 = split_update<FAST>(o[S_XXZ - S_XXX], dt, l * dZz, kz, mz, pz);
+                sp[S_XXX * N] = a0; sp[S_XXY * N] = a1; sp[S_XXZ * N] = a2;
+                snew[0] = (a0 + a1) + a2;
+                a0 = split_update<FAST>(o[S_YYX - S_XXX], dt, l * dXx, kx, mx, px);
+                a1 = split_update<FAST>(o[S_YYY - S_XXX], dl, dYy, ky, my, py);
+                a2 = split_update<FAST>(o[S_YYZ - S_XXX], dt, l * dZz, kz, mz, pz);
+                sp[S_YYX * N] = a0; sp[S_YYY * N] = a1; sp[S_YYZ * N] = a2;
+                snew[1] = (a0 + a1) + a2;
+                a0 = split_update<FAST>(o[S_ZZX - S_XXX], dt, l * dXx, kx, mx, px);
+                a1 = split_update<FAST>(o[S_ZZY - S_XXX], dt, l * dYy, ky, my, py);
+                a2 = split_update<FAST>(o[S_ZZZ - S_XXX], dl, dZz, kz, mz, pz);
+                sp[S_ZZX * N] = a0; sp[S_ZZY * N] = a1; sp[S_ZZZ * N] = a2;
+                snew[2] = (a0 + a1) + a2;
+                const float axy = dt * mxy, axz = dt * mxz, ayz = dt * myz;
+                a0 = split_update<FAST>(o[S_XYX - S_XXX], axy, xyX, kx, mx, px);
+                a1 = split_update<FAST>(o[S_XYY - S_XXX], axy, xyY, ky, my, py);
+                sp[S_XYX * N] = a0; sp[S_XYY * N] = a1;
+                snew[3] = a0 + a1;
+                a0 = split_update<FAST>(o[S_XZX - S_XXX], axz, xzX, kx, mx, px);
+                a1 = split_update<FAST>(o[S_XZZ - S_XXX], axz, xzZ, kz, mz, pz);
+                sp[S_XZX * N] = a0; sp[S_XZZ * N] = a1;
+                snew[4] = a0 + a1;
+                a0 = split_update<FAST>(o[S_YZY - S_XXX], ayz, yzY, ky, my, py);
+                a1 = split_update<FAST>(o[S_YZZ - S_XXX], ayz, yzZ, kz, mz, pz);
+                sp[S_YZY * N] = a0; sp[S_YZZ * N] = a1;
+                snew[5] = a0 + a1;
+            }
+#pragma unroll
+            for (int q = 0; q < 6; ++q) m.f[3 + q][ci] = snew[q];
+            if (GEN && gz == rz && it >= 0 && it < sr.nt) {
+                for (int r = rp; r < rend && g.rec_list[r].z == gz; ++r) {
+                    const int4 q = g.rec_list[r];
+                    if (q.x == gx && q.y == gyc[c] && q.w >= 3)
+                        sr.traces[(int64_t)it * sr.nrec + g.rec_idx[r]] =
+                            q.w == 3 ? snew[0] : q.w == 4 ? snew[1] : q.w == 5 ? snew[2]
+                          : q.w == 6 ? snew[3] : q.w == 7 ? snew[4] : snew[5];
+                }
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < CELLS; ++c) {
+#pragma unroll
+            for (int q = 0; q < 6; ++q) scur[c][q] = snxt[c][q];
+            lcur[c] = lnxt[c];
+            mcur[c] = mnxt[c];
+        }
+        if (GEN && gz == rz) {
+            while (rp < rend && g.rec_list[rp].z == gz) ++rp;
+            rz = rp < rend ? g.rec_list[rp].z : 0x7fffffff;
+        }
+
+        if (__syncthreads_or(failed)) return false;
+        if (tid == 0 && cz + S < t.ze) {
+            fence_proxy_async();
+            str_issue<TY>(mp, st, &bar[s], t, cz + S);
+            issued_end = cz + S + 1;
+        }
+        return true;
+    };
+    for (; cz < t.ze; ++cz) {
+        const int gzp = cz + kHalo;
+        const bool gen = t.xy_pml || band(gzp, m.nz, m.pml) != 0 || gzp == sz || gzp == rz;
+        if (!(gen ? plane(std::true_type{}) : plane(std::false_type{}))) {
+            abort = true;
+            break;
+        }
+    }
+    if (abort && tid == 0) {
+        atomicExch(g.err, 1);
+        drain(bar, issued_end, cz, t.zs);
+    }
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 get_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
+// 3-D FP32 tensor map over one padded array (base = allocation start).
+bool make_map(CUtensorMap *map, const float *grid_origin, const Model &m, int bx, int by) {
+    auto enc = get_encoder();
+    if (!enc) return false;
+    void *base = const_cast<float *>(grid_origin - kXOff);
+    cuuint64_t dims[3] = {(cuuint64_t)(m.nx + kXOff), (cuuint64_t)m.ny, (cuuint64_t)m.nz};
+    cuuint64_t strides[2] = {(cuuint64_t)m.px * 4, (cuuint64_t)m.plane * 4};
+    cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, 1};
+    cuuint32_t es[3] = {1, 1, 1};
+    CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, dims, strides, box, es,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
+template <int CELLS>
+int vel_smem() { return S * VelL<8 * CELLS>::STAGE + 128; }
+template <int CELLS>
+int str_smem() { return S * StrL<8 * CELLS>::STAGE + 128; }
+
+template <bool FAST, int CELLS>
+cudaError_t set_attrs() {
+    cudaError_t e = cudaFuncSetAttribute(k_velocity_zmarch<FAST, CELLS>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, vel_smem<CELLS>());
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_stress_zmarch<FAST, CELLS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 str_smem<CELLS>());
+    return e;
+}
+
+template <bool FAST, int CELLS>
+void launch(const Model &m, const Physics &ph, const SourceRec &sr, const ZGeom &g, const VelMaps &vm,
+            const StrMaps &sm, int it, float src_value, int uw, cudaStream_t s, cudaEvent_t *ev) {
+    const dim3 grid(g.ntx * g.nty, g.nchunks);
+    if (ev) cudaEventRecord(ev[0], s);
+    k_velocity_zmarch<FAST, CELLS><<<grid, NT, vel_smem<CELLS>(), s>>>(vm, m, ph, g, sr, it, src_value, uw);
+    if (ev) cudaEventRecord(ev[1], s);
+    if (ev) cudaEventRecord(ev[2], s);
+    k_stress_zmarch<FAST, CELLS><<<grid, NT, str_smem<CELLS>(), s>>>(sm, m, ph, g, sr, it, src_value, uw);
+    if (ev) cudaEventRecord(ev[3], s);
+}
+
+}  // namespace
+
+bool zmarch_supported(const Model &m) {
+    // Halo boxes start 8 cells left of the tile and 5 rows above: always inside
+    // the padded array because the frame is 5 cells and kXOff is 27.  The
+    // kernels address cells and PML cells with 32-bit offsets
+    const bool small = m.plane * (int64_t)m.nz < ((int64_t)1 << 31) && m.npml < ((int64_t)1 << 31);
+    return small && m.nxc >= 1 && m.nyc >= 1 && m.nzc >= 1 && get_encoder() != nullptr;
+}
+
+cudaError_t zmarch_prepare(const Model &m, int cells, VelMaps *vm, StrMaps *sm) {
+    if (cells != 1 && cells != 2) return cudaErrorInvalidValue;
+    const int ty = 8 * cells;
+    bool ok = true;
+    ok &= make_map(&vm->sxx, m.f[3], m, W48, ty);
+    ok &= make_map(&vm->syy, m.f[4], m, W32, ty + 10);
+    ok &= make_map(&vm->sxy, m.f[6], m, W48, ty + 10);
+    ok &= make_map(&vm->sxz, m.f[7], m, W48, ty);
+    ok &= make_map(&vm->syz, m.f[8], m, W32, ty + 10);
+    ok &= make_map(&vm->b, m.b, m, W36, ty + 1);
+    ok &= make_map(&vm->sxz_c, m.f[7], m, W32, ty);
+    ok &= make_map(&vm->syz_c, m.f[8], m, W32, ty);
+    ok &= make_map(&vm->szz_c, m.f[5], m, W32, ty);
+    ok &= make_map(&vm->b_c, m.b, m, W32, ty);
+    ok &= make_map(&sm->vx, m.f[0], m, W48, ty + 10);
+    ok &= make_map(&sm->vy, m.f[1], m, W48, ty + 10);
+    ok &= make_map(&sm->vz, m.f[2], m, W48, ty + 10);
+    ok &= make_map(&sm->mu, m.mu, m, W36, ty + 1);
+    ok &= make_map(&sm->vx_c, m.f[0], m, W32, ty);
+    ok &= make_map(&sm->vy_c, m.f[1], m, W32, ty);
+    ok &= make_map(&sm->vz_c, m.f[2], m, W32, ty);
+    if (!ok) return cudaErrorInvalidValue;
+    cudaError_t e = cells == 1 ? set_attrs<false, 1>() : set_attrs<false, 2>();
+    if (e == cudaSuccess) e = cells == 1 ? set_attrs<true, 1>() : set_attrs<true, 2>();
+    return e;
+}
+
+void zmarch_tiles(const Model &m, int cells, int *ntx, int *nty) {
+    *ntx = (m.nxc + TX - 1) / TX;
+    *nty = (m.nyc + 8 * cells - 1) / (8 * cells);
+}
+
+cudaError_t zmarch_step(const Model &m, const Physics &ph, const SourceRec &sr, const ZGeom &g,
+                        const VelMaps &vm, const StrMaps &sm, int it, float src_value, bool use_wavelet,
+                        cudaStream_t s, cudaEvent_t *ev) {
+    const int uw = use_wavelet ? 1 : 0;
+    if (ph.fast) {
+        if (g.cells == 1) launch<true, 1>(m, ph, sr, g, vm, sm, it, src_value, uw, s, ev);
+        else launch<true, 2>(m, ph, sr, g, vm, sm, it, src_value, uw, s, ev);
+    } else {
+        if (g.cells == 1) launch<false, 1>(m, ph, sr, g, vm, sm, it, src_value, uw, s, ev);
+        else launch<false, 2>(m, ph, sr, g, vm, sm, it, src_value, uw, s, ev);
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace sgfd

@@ -16,12 +16,14 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <algorithm>
 #include <new>
 #include <string>
 #include <vector>
 
 #include "../../include/sgfd.h"
 #include "sgfd_internal.h"
+#include "zmarch.h"
 
 using namespace sgfd;
 
@@ -41,6 +43,16 @@ struct sgfd_solver {
     int wavelet_nt = 0;
     bool medium_set = false;
     int kernel = SGFD_KERNEL_SIMPLE;
+    // z-marching family
+    VelMaps vm{};
+    StrMaps sm{};
+    ZGeom zg{};
+    int zchunk_req = 0;
+    std::vector<int4> rec_host;   // receivers, for re-bucketing when the tiling changes
+    int *zrec_off = nullptr;
+    int4 *zrec_list = nullptr;
+    int *zrec_idx = nullptr;
+    int *dev_err = nullptr;
     std::string err;
 };
 
@@ -77,6 +89,12 @@ void set_physics(sgfd_solver *h) {
     Physics &ph = h->ph;
     for (int i = 0; i < 5; ++i) ph.c[i] = c.coef[i];
     ph.dt = c.dt; ph.dx = c.dx; ph.dy = c.dy; ph.dz = c.dz;
+    for (int i = 0; i < 5; ++i) {
+        ph.cs[0][i] = c.coef[i] / c.dx;
+        ph.cs[1][i] = c.coef[i] / c.dy;
+        ph.cs[2][i] = c.coef[i] / c.dz;
+    }
+    ph.fast = c.arith == SGFD_ARITH_FAST;
     ph.inj_dt2 = c.dt * c.dt;
     ph.damping = c.damping;
     ph.quirks = c.quirks;
@@ -89,7 +107,13 @@ void set_physics(sgfd_solver *h) {
     for (int a = 0; a < 3; ++a)
         ph.q_refcpu[a] = (float)(0.5 * (double)c.dt * std::log10(1.0 / R) * 3.4 *
                                  (double)c.damping_vconst / ((double)p * dd[a]));
-    ph.inv_pml = 1.0f / (float)p;
+    const float d3[3] = {c.dx, c.dy, c.dz};
+    for (int a = 0; a < 3; ++a)
+        ph.qf[a] = c.damping == SGFD_DAMP_LOGR ? ph.q_logr / d3[a] : (ph.q_refgpu / d3[a]) * ph.poly;
+    for (int k = 0; k < kPwTable; ++k) {
+        const float r = (float)k / (float)p;
+        ph.pw[k] = r * r;
+    }
 }
 
 int check_handle(sgfd_solver *h) {
@@ -99,9 +123,85 @@ int check_handle(sgfd_solver *h) {
     return SGFD_OK;
 }
 
+cudaError_t dispatch_step(sgfd_solver *h, int it, float value, bool use_wavelet, cudaEvent_t *ev) {
+    if (h->kernel == SGFD_KERNEL_ZMARCH)
+        return zmarch_step(h->m, h->ph, h->sr, h->zg, h->vm, h->sm, it, value, use_wavelet, h->stream, ev);
+    return simple_step(h->m, h->ph, h->sr, it, value, use_wavelet, h->stream, ev);
+}
+
 int launch_step(sgfd_solver *h, int it, float value, bool use_wavelet) {
-    cudaError_t e = simple_step(h->m, h->ph, h->sr, it, value, use_wavelet, h->stream);
+    cudaError_t e = dispatch_step(h, it, value, use_wavelet, nullptr);
     if (e != cudaSuccess) return cuda_fail(h, e, "step launch");
+    return SGFD_OK;
+}
+
+// z chunking: enough CTAs for ~8 waves of two CTAs per SM, chunks >= 16 planes.
+void set_zchunks(sgfd_solver *h) {
+    ZGeom &g = h->zg;
+    const int tiles = g.ntx * g.nty;
+    int zc = h->zchunk_req;
+    if (zc <= 0) {
+        int sms = 148;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device);
+        const int target = 8 * 2 * sms;
+        int nch = (target + tiles - 1) / tiles;
+        nch = std::max(1, std::min(nch, (h->m.nzc + 15) / 16));
+        zc = (h->m.nzc + nch - 1) / nch;
+    }
+    zc = std::max(1, std::min(zc, h->m.nzc));
+    g.zc = zc;
+    g.nchunks = (h->m.nzc + zc - 1) / zc;
+}
+
+// Receivers bucketed per z-march tile, sorted by z (device arrays).
+int upload_zrec(sgfd_solver *h, const std::vector<int4> &rec) {
+    const Model &m = h->m;
+    const int tiles = h->zg.ntx * h->zg.nty;
+    std::vector<std::vector<std::pair<int4, int>>> buckets(tiles);
+    for (int i = 0; i < (int)rec.size(); ++i) {
+        const int4 q = rec[i];
+        const int cx = q.x - kHalo, cy = q.y - kHalo, cz = q.z - kHalo;
+        if (cx < 0 || cy < 0 || cz < 0 || cx >= m.nxc || cy >= m.nyc || cz >= m.nzc) continue;  // frame: stays 0
+        buckets[(cy / (8 * h->zg.cells)) * h->zg.ntx + cx / kZTileX].push_back({q, i});
+    }
+    std::vector<int> off(tiles + 1, 0);
+    std::vector<int4> list;
+    std::vector<int> idx;
+    for (int t = 0; t < tiles; ++t) {
+        auto &b = buckets[t];
+        std::stable_sort(b.begin(), b.end(), [](const std::pair<int4, int> &a, const std::pair<int4, int> &c) {
+            return a.first.z < c.first.z;
+        });
+        for (auto &e : b) { list.push_back(e.first); idx.push_back(e.second); }
+        off[t + 1] = (int)list.size();
+    }
+    cudaFree(h->zrec_off); cudaFree(h->zrec_list); cudaFree(h->zrec_idx);
+    h->zrec_off = nullptr; h->zrec_list = nullptr; h->zrec_idx = nullptr;
+    const size_t nl = std::max<size_t>(list.size(), 1);
+    cudaError_t e = cudaMalloc(&h->zrec_off, off.size() * sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc(&h->zrec_list, nl * sizeof(int4));
+    if (e == cudaSuccess) e = cudaMalloc(&h->zrec_idx, nl * sizeof(int));
+    if (e != cudaSuccess) { cudaGetLastError(); return fail(h, SGFD_ERR_ALLOC, "receiver lists"); }
+    SG_CUDA(h, cudaMemcpy(h->zrec_off, off.data(), off.size() * sizeof(int), cudaMemcpyHostToDevice), "receiver lists");
+    if (!list.empty()) {
+        SG_CUDA(h, cudaMemcpy(h->zrec_list, list.data(), list.size() * sizeof(int4), cudaMemcpyHostToDevice), "receiver lists");
+        SG_CUDA(h, cudaMemcpy(h->zrec_idx, idx.data(), idx.size() * sizeof(int), cudaMemcpyHostToDevice), "receiver lists");
+    }
+    h->zg.rec_off = h->zrec_off;
+    h->zg.rec_list = h->zrec_list;
+    h->zg.rec_idx = h->zrec_idx;
+    return SGFD_OK;
+}
+
+int check_device_error(sgfd_solver *h) {
+    if (!h->dev_err) return SGFD_OK;
+    int flag = 0;
+    SG_CUDA(h, cudaMemcpyAsync(&flag, h->dev_err, sizeof(int), cudaMemcpyDeviceToHost, h->stream), "error flag");
+    SG_CUDA(h, cudaStreamSynchronize(h->stream), "error flag");
+    if (flag) {
+        cudaMemsetAsync(h->dev_err, 0, sizeof(int), h->stream);
+        return fail(h, SGFD_ERR_CUDA, "a kernel's bounded wait for its TMA copies gave up (flag %d)", flag);
+    }
     return SGFD_OK;
 }
 
@@ -127,6 +227,7 @@ void sgfd_config_default(sgfd_config *cfg) {
     cfg->storage = SGFD_STORE_F32;
     cfg->kernel = SGFD_KERNEL_AUTO;
     cfg->device = 0;
+    cfg->arith = SGFD_ARITH_REF;
 }
 
 const char *sgfd_global_error(void) { return g_error.c_str(); }
@@ -137,8 +238,10 @@ int sgfd_create(const sgfd_config *cfg, sgfd_solver **out) {
     if (!cfg || !out) return fail(nullptr, SGFD_ERR_INVALID, "null config or output pointer");
     *out = nullptr;
     const sgfd_config &c = *cfg;
-    for (int i = 0; i < 8; ++i)
+    for (int i = 0; i < 7; ++i)
         if (c.reserved[i] != 0) return fail(nullptr, SGFD_ERR_INVALID, "reserved config fields must be zero");
+    if (c.arith != SGFD_ARITH_REF && c.arith != SGFD_ARITH_FAST)
+        return fail(nullptr, SGFD_ERR_INVALID, "unknown arithmetic mode %d", c.arith);
     if (c.pml < 1) return fail(nullptr, SGFD_ERR_INVALID, "pml must be >= 1 (got %d)", c.pml);
     const int need = 2 * (kHalo + c.pml) + 1;
     if (c.nx < need || c.ny < need || c.nz < need)
@@ -156,7 +259,7 @@ int sgfd_create(const sgfd_config *cfg, sgfd_solver **out) {
         return fail(nullptr, SGFD_ERR_INVALID, "unknown quirks mode %d", c.quirks);
     if (c.storage != SGFD_STORE_F32)
         return fail(nullptr, SGFD_ERR_UNSUPPORTED, "storage type %d is not built into this library", c.storage);
-    if (c.kernel != SGFD_KERNEL_AUTO && c.kernel != SGFD_KERNEL_SIMPLE)
+    if (c.kernel != SGFD_KERNEL_AUTO && c.kernel != SGFD_KERNEL_SIMPLE && c.kernel != SGFD_KERNEL_ZMARCH)
         return fail(nullptr, SGFD_ERR_UNSUPPORTED, "kernel family %d is not built into this library", c.kernel);
     const int64_t cells = (int64_t)c.nx * c.ny * c.nz;
     if (cells > ((int64_t)1 << 36)) return fail(nullptr, SGFD_ERR_INVALID, "grid has too many cells");
@@ -184,7 +287,7 @@ int sgfd_create(const sgfd_config *cfg, sgfd_solver **out) {
 
     Model &m = h->m;
     m.nx = c.nx; m.ny = c.ny; m.nz = c.nz;
-    m.px = (int)round_up((size_t)c.nx, 32);
+    m.px = (int)round_up((size_t)c.nx + kXOff, 32);
     m.pml = c.pml;
     m.nxc = c.nx - 2 * kHalo; m.nyc = c.ny - 2 * kHalo; m.nzc = c.nz - 2 * kHalo;
     m.plane = (int64_t)m.px * m.ny;
@@ -200,11 +303,12 @@ int sgfd_create(const sgfd_config *cfg, sgfd_solver **out) {
         sgfd_destroy(h);
         return r;
     }
-    for (int k = 0; k < 9; ++k) m.f[k] = reinterpret_cast<float *>(h->field_pool + k * arr_bytes);
-    m.b = reinterpret_cast<float *>(h->field_pool + 9 * arr_bytes);
-    m.lam = reinterpret_cast<float *>(h->field_pool + 10 * arr_bytes);
-    m.mu = reinterpret_cast<float *>(h->field_pool + 11 * arr_bytes);
-    m.rmu = reinterpret_cast<float *>(h->field_pool + 12 * arr_bytes);
+    auto arr = [&](int k) { return reinterpret_cast<float *>(h->field_pool + k * arr_bytes) + kXOff; };
+    for (int k = 0; k < 9; ++k) m.f[k] = arr(k);
+    m.b = arr(9);
+    m.lam = arr(10);
+    m.mu = arr(11);
+    m.rmu = arr(12);
     m.split = h->split;
     e = cudaMemsetAsync(h->field_pool, 0, pool_bytes, h->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(h->split, 0, (size_t)kNumSplit * m.npml * sizeof(float), h->stream);
@@ -217,6 +321,28 @@ int sgfd_create(const sgfd_config *cfg, sgfd_solver **out) {
     set_physics(h);
     h->sr.src = -1;
     h->sr.nrec = 0;
+
+    // kernel family
+    if (c.kernel != SGFD_KERNEL_SIMPLE && zmarch_supported(m)) {
+        h->zg.cells = 1;
+        e = zmarch_prepare(m, h->zg.cells, &h->vm, &h->sm);
+        if (e == cudaSuccess) e = cudaMalloc(&h->dev_err, sizeof(int));
+        if (e == cudaSuccess) e = cudaMemset(h->dev_err, 0, sizeof(int));
+        if (e != cudaSuccess) {
+            int r = cuda_fail(nullptr, e, "z-march set-up");
+            sgfd_destroy(h);
+            return r;
+        }
+        h->kernel = SGFD_KERNEL_ZMARCH;
+        zmarch_tiles(m, h->zg.cells, &h->zg.ntx, &h->zg.nty);
+        h->zg.err = h->dev_err;
+        set_zchunks(h);
+        int r = upload_zrec(h, {});
+        if (r) { g_error = h->err; sgfd_destroy(h); return r; }
+    } else if (c.kernel == SGFD_KERNEL_ZMARCH) {
+        sgfd_destroy(h);
+        return fail(nullptr, SGFD_ERR_UNSUPPORTED, "z-marching kernels unavailable (no TMA encoder in the driver)");
+    }
     *out = h;
     return SGFD_OK;
 }
@@ -230,6 +356,10 @@ void sgfd_destroy(sgfd_solver *h) {
     cudaFree(h->rec);
     cudaFree(h->traces);
     cudaFree(h->wavelet);
+    cudaFree(h->zrec_off);
+    cudaFree(h->zrec_list);
+    cudaFree(h->zrec_idx);
+    cudaFree(h->dev_err);
     if (h->own_stream) cudaStreamDestroy(h->own_stream);
     delete h;
 }
@@ -254,7 +384,7 @@ static int upload_medium(sgfd_solver *h, const float *b, const float *l, const f
     for (int k = 0; k < 3; ++k)
         SG_CUDA(h, cudaMemcpy2DAsync(dst[k], (size_t)m.px * sizeof(float), src[k], row, row, rows, kind, h->stream),
                 "medium upload");
-    cudaError_t e = launch_reciprocal(const_cast<float *>(m.rmu), m.mu, m.plane * m.nz, h->stream);
+    cudaError_t e = launch_reciprocal(const_cast<float *>(m.rmu) - kXOff, m.mu - kXOff, m.plane * m.nz, h->stream);
     if (e != cudaSuccess) return cuda_fail(h, e, "reciprocal kernel");
     SG_CUDA(h, cudaStreamSynchronize(h->stream), "medium upload");
     h->medium_set = true;
@@ -315,6 +445,8 @@ int sgfd_set_receivers(sgfd_solver *h, int32_t n, const int32_t *xyz, const int3
     h->sr.nt = n > 0 ? nt : 0;
     h->sr.rec = h->rec;
     h->sr.traces = h->traces;
+    h->rec_host = host;
+    if (h->kernel == SGFD_KERNEL_ZMARCH) return upload_zrec(h, host);
     return SGFD_OK;
 }
 
@@ -365,6 +497,36 @@ int sgfd_synchronize(sgfd_solver *h) {
     int r = check_handle(h);
     if (r) return r;
     SG_CUDA(h, cudaStreamSynchronize(h->stream), "synchronize");
+    return check_device_error(h);
+}
+
+int sgfd_set_zchunk(sgfd_solver *h, int32_t planes) {
+    int r = check_handle(h);
+    if (r) return r;
+    if (planes < 0) return fail(h, SGFD_ERR_INVALID, "negative chunk");
+    h->zchunk_req = planes;
+    if (h->kernel == SGFD_KERNEL_ZMARCH) set_zchunks(h);
+    return SGFD_OK;
+}
+
+int sgfd_set_tiling(sgfd_solver *h, int32_t tile_rows, int32_t zchunk) {
+    int r = check_handle(h);
+    if (r) return r;
+    if (tile_rows != 8 && tile_rows != 16) return fail(h, SGFD_ERR_INVALID, "tile rows must be 8 or 16");
+    if (zchunk < 0) return fail(h, SGFD_ERR_INVALID, "negative chunk");
+    if (h->kernel != SGFD_KERNEL_ZMARCH) return SGFD_OK;   // the simple family has no tiling
+    SG_CUDA(h, cudaStreamSynchronize(h->stream), "synchronise before re-tiling");
+    const int cells = tile_rows / 8;
+    if (cells != h->zg.cells) {
+        cudaError_t e = zmarch_prepare(h->m, cells, &h->vm, &h->sm);
+        if (e != cudaSuccess) return cuda_fail(h, e, "z-march re-tiling");
+        h->zg.cells = cells;
+        zmarch_tiles(h->m, cells, &h->zg.ntx, &h->zg.nty);
+        r = upload_zrec(h, h->rec_host);
+        if (r) return r;
+    }
+    h->zchunk_req = zchunk;
+    set_zchunks(h);
     return SGFD_OK;
 }
 
@@ -392,6 +554,8 @@ int sgfd_get_traces(sgfd_solver *h, float *out) {
     SG_CUDA(h, cudaMemcpyAsync(tm.data(), h->traces, tm.size() * sizeof(float), cudaMemcpyDeviceToHost, h->stream),
             "trace download");
     SG_CUDA(h, cudaStreamSynchronize(h->stream), "trace download");
+    r = check_device_error(h);
+    if (r) return r;
     for (int it = 0; it < nt; ++it)
         for (int q = 0; q < n; ++q) out[(size_t)q * nt + it] = tm[(size_t)it * n + q];
     return SGFD_OK;
@@ -420,7 +584,7 @@ int sgfd_profile(sgfd_solver *h, int32_t it0, int32_t nsteps, float *ms_velocity
     double tv = 0, ts = 0;
     int rc = SGFD_OK;
     for (int it = it0; it < it0 + nsteps && rc == SGFD_OK; ++it) {
-        cudaError_t e = simple_step(h->m, h->ph, h->sr, it, 0.0f, true, h->stream, ev);
+        cudaError_t e = dispatch_step(h, it, 0.0f, true, ev);
         if (e == cudaSuccess) e = cudaEventSynchronize(ev[3]);
         float a = 0, b = 0;
         if (e == cudaSuccess) e = cudaEventElapsedTime(&a, ev[0], ev[1]);
@@ -489,6 +653,7 @@ int sgfd_cell_counts(const sgfd_solver *h, int64_t *n_interior, int64_t *n_pml) 
 
 int sgfd_launches_per_step(const sgfd_solver *h) {
     if (!h) return -1;
+    if (h->kernel == SGFD_KERNEL_ZMARCH) return 2;
     return simple_launches_per_step(h->sr);
 }
 

@@ -5,8 +5,11 @@
 //   * 9 wavefields + buoyancy, lambda, mu: one array each, x fastest, the
 //     reference GRID (5-cell frame included), rows padded to a pitch `px`
 //     that is a multiple of 32 floats so every row starts on a 128-byte
-//     boundary (coalescing, and the 16-byte rule of TMA tensor maps).
-//     index(ix, iy, iz) = ix + iy*px + iz*px*ny.
+//     boundary (coalescing, and the 16-byte rule of TMA tensor maps).  Each
+//     row is shifted right by kXOff floats inside its pitch so that the
+//     computed cells of every 32-wide tile start on a 128-byte boundary.
+//     Model::f[k] etc. point at GRID (0,0,0); the allocation starts kXOff
+//     floats earlier.  index(ix, iy, iz) = ix + iy*px + iz*px*ny.
 //   * PML split fields: a compact array of the PML cells only, 24 splits as
 //     structure-of-arrays, split k of PML cell c at split[k*npml + c].  PML
 //     cells are enumerated plane by plane (z slowest), and within a plane row
@@ -21,9 +24,13 @@
 namespace sgfd {
 
 constexpr int kHalo = 5;            // reference `order` (OPT/ElasticMacro.h:24)
+// Device arrays store GRID x at offset kXOff so that the first computed cell
+// (x = 5) sits at a 32-float (128-byte) boundary: 5 + 27 = 32.
+constexpr int kXOff = 27;
 constexpr int kNumSplit = 24;
 constexpr int kNumVelSplit = 9;     // velocity splits come first
 constexpr float kTau = 4.3f;        // reference `tau` (OPT/ElasticMacro.h:21)
+constexpr int kPwTable = 129;       // damping-profile table covers pml <= 128
 
 // Split ids (velocity q,axis then stress), same order as the oracle.
 enum SplitId {
@@ -35,6 +42,8 @@ enum SplitId {
 // Per-step physics constants (all FP32, computed once on the host).
 struct Physics {
     float c[5];          // staggered coefficients
+    float cs[3][5];      // c_i / dx, c_i / dy, c_i / dz (FAST arithmetic)
+    int fast;            // sgfd_arith == FAST
     float dt, dx, dy, dz;
     float inj_dt2;       // dt*dt (source scale, OPT/ElasticWaveEquation.cu:213)
     int damping;         // sgfd_damping
@@ -43,7 +52,8 @@ struct Physics {
     float poly;          // 8/15 - 0.03 p + p^2/1500
     float q_logr;        // 0.5*dt*3*ln(1/R)/(2p)
     float q_refcpu[3];   // 0.5*dt*log10(1/R)*3.4*V/(p*d)
-    float inv_pml;       // unused by the arithmetic; kept for diagnostics
+    float qf[3];         // FAST: ((0.5*dt*tau)/d)*poly (REFGPU) or (0.5*dt*3*ln(1/R)/(2p))/d (LOGR)
+    float pw[kPwTable];  // (k/pml)^2 for k = 0..kPwTable-1 (rounded as (k/p)*(k/p))
 };
 
 // Geometry and device pointers of one model.
@@ -99,6 +109,34 @@ __host__ __device__ inline int64_t pml_index(const Model &m, int cx, int cy, int
         return base + (int64_t)p * m.nxc + (int64_t)(cy - p) * 2 * p + off;
     }
     return base + (int64_t)p * m.nxc + (int64_t)(m.nyc - 2 * p) * 2 * p + (int64_t)(cy - (m.nyc - p)) * m.nxc + cx;
+}
+
+// pml_index() split in two for kernels that march along z: a per-column
+// offset (in full PML planes and in ring planes) and a per-plane base.  32-bit
+// arithmetic: the z-marching family requires npml < 2^31.
+struct PmlColumn {
+    uint32_t full_off;   // offset inside a full PML plane
+    uint32_t ring_off;   // offset inside a ring plane (valid for x/y-band columns)
+};
+__host__ __device__ inline PmlColumn pml_column(const Model &m, int cx, int cy) {
+    const int p = m.pml;
+    PmlColumn c;
+    c.full_off = (uint32_t)(cy * m.nxc + cx);
+    if (cy < p) c.ring_off = (uint32_t)(cy * m.nxc + cx);
+    else if (cy < m.nyc - p)
+        c.ring_off = (uint32_t)(p * m.nxc + (cy - p) * 2 * p + (cx < p ? cx : cx - (m.nxc - 2 * p)));
+    else c.ring_off = (uint32_t)(p * m.nxc + (m.nyc - 2 * p) * 2 * p + (cy - (m.nyc - p)) * m.nxc + cx);
+    return c;
+}
+// Index of the PML cell of column c in computed plane cz.
+__host__ __device__ inline uint32_t pml_plane_index(const Model &m, const PmlColumn &c, int cz) {
+    const uint32_t p = (uint32_t)m.pml;
+    const uint32_t full = (uint32_t)m.nxc * (uint32_t)m.nyc;
+    const uint32_t ring = 2u * p * (uint32_t)m.nxc + (uint32_t)(m.nyc - 2 * m.pml) * 2u * p;
+    const uint32_t z = (uint32_t)cz;
+    if (cz < m.pml) return z * full + c.full_off;
+    if (cz < m.nzc - m.pml) return p * full + (z - p) * ring + c.ring_off;
+    return p * full + (uint32_t)(m.nzc - 2 * m.pml) * ring + (z - (uint32_t)(m.nzc - m.pml)) * full + c.full_off;
 }
 
 __host__ inline int64_t pml_count(int nxc, int nyc, int nzc, int p) {

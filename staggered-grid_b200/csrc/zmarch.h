@@ -1,0 +1,44 @@
+// zmarch.h — host interface of the z-marching kernel family (kernels_zmarch.cu).
+#pragma once
+
+#include <cuda.h>
+
+#include "sgfd_internal.h"
+
+namespace sgfd {
+
+// Tiles are 32 computed cells wide and 8 * cells high (cells = 1 or 2 per thread).
+constexpr int kZTileX = 32;
+
+// TMA descriptors of the velocity update: x/y-halo boxes of the current plane
+// and 32 x 16 centre boxes of the planes that feed the z register queues.
+struct VelMaps {
+    CUtensorMap sxx, syy, sxy, sxz, syz, b;      // current plane
+    CUtensorMap sxz_c, syz_c, szz_c, b_c;        // lead planes (centre boxes)
+};
+// TMA descriptors of the stress update.
+struct StrMaps {
+    CUtensorMap vx, vy, vz, mu;                  // current plane (mu: plane z+1)
+    CUtensorMap vx_c, vy_c, vz_c;                // lead planes
+};
+
+// Launch geometry: tiles of kZTileX x (8 * cells) computed cells, z chunks of
+// zc planes; receivers bucketed per tile and sorted by z.
+struct ZGeom {
+    int cells;
+    int ntx, nty;
+    int zc, nchunks;
+    const int *rec_off;     // ntx*nty + 1 offsets into rec_list / rec_idx
+    const int4 *rec_list;   // GRID x, y, z, component
+    const int *rec_idx;     // receiver index (trace column)
+    int *err;               // device error flag (1: a bounded wait gave up)
+};
+
+bool zmarch_supported(const Model &m);
+cudaError_t zmarch_prepare(const Model &m, int cells, VelMaps *vm, StrMaps *sm);
+void zmarch_tiles(const Model &m, int cells, int *ntx, int *nty);
+cudaError_t zmarch_step(const Model &m, const Physics &ph, const SourceRec &sr, const ZGeom &g,
+                        const VelMaps &vm, const StrMaps &sm, int it, float src_value, bool use_wavelet,
+                        cudaStream_t s, cudaEvent_t *ev = nullptr);
+
+}  // namespace sgfd

@@ -32,6 +32,7 @@ DAMP_REFGPU, DAMP_LOGR, DAMP_REFCPU = range(3)
 QUIRKS_REF, QUIRKS_FIXED = range(2)
 STORE_F32, STORE_BF16, STORE_F16 = range(3)
 KERNEL_AUTO, KERNEL_SIMPLE, KERNEL_ZMARCH = range(3)
+ARITH_REF, ARITH_FAST = range(2)
 
 # sgfd_status
 OK, ERR_INVALID, ERR_ALLOC, ERR_CUDA, ERR_STATE, ERR_UNSUPPORTED, ERR_NO_DEVICE, ERR_NONFINITE = range(8)
@@ -48,7 +49,7 @@ class Config(ctypes.Structure):
         ("coef", ctypes.c_float * 5),
         ("damping", ctypes.c_int32), ("damping_R", ctypes.c_float), ("damping_vconst", ctypes.c_float),
         ("quirks", ctypes.c_int32), ("storage", ctypes.c_int32), ("kernel", ctypes.c_int32),
-        ("device", ctypes.c_int32), ("reserved", ctypes.c_int32 * 8),
+        ("device", ctypes.c_int32), ("arith", ctypes.c_int32), ("reserved", ctypes.c_int32 * 7),
     ]
 
 
@@ -96,6 +97,8 @@ def lib() -> ctypes.CDLL:
         "sgfd_get_medium": (ctypes.c_int, [vp, i32, fp]),
         "sgfd_ricker_ref": (ctypes.c_float, [ctypes.c_float, ctypes.c_float, i32]),
         "sgfd_ricker_t0": (ctypes.c_float, [ctypes.c_float, ctypes.c_float, ctypes.c_float, i32]),
+        "sgfd_set_zchunk": (ctypes.c_int, [vp, i32]),
+        "sgfd_set_tiling": (ctypes.c_int, [vp, i32, i32]),
         "sgfd_cell_counts": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)]),
         "sgfd_launches_per_step": (ctypes.c_int, [vp]),
         "sgfd_kernel_name": (ctypes.c_char_p, [vp]),
@@ -247,6 +250,12 @@ class Solver:
         out = np.zeros(self.shape, dtype=np.float32)
         self._check(lib().sgfd_get_medium(self.h, which, _fptr(out)))
         return out
+
+    def set_zchunk(self, planes: int):
+        self._check(lib().sgfd_set_zchunk(self.h, planes))
+
+    def set_tiling(self, tile_rows: int, zchunk: int = 0):
+        self._check(lib().sgfd_set_tiling(self.h, tile_rows, zchunk))
 
     def cell_counts(self) -> tuple[int, int]:
         a, b = ctypes.c_int64(), ctypes.c_int64()

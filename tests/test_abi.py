@@ -36,8 +36,8 @@ def test_library_exports_every_declared_function():
 
 def test_abi_version_and_struct_size():
     assert sgfd.lib().sgfd_abi_version() == 1
-    # int32 x4, float x4, float coef[5], int32, float, float, int32 x4, int32[8]
-    assert ctypes.sizeof(sgfd.Config) == 4 * (4 + 4 + 5 + 3 + 4 + 8)
+    # int32 x4, float x4, float coef[5], int32, float, float, int32 x5, int32[7]
+    assert ctypes.sizeof(sgfd.Config) == 4 * (4 + 4 + 5 + 3 + 5 + 7)
 
 
 @pytest.mark.parametrize("kw,code", [
@@ -49,6 +49,7 @@ def test_abi_version_and_struct_size():
     (dict(quirks=3), sgfd.ERR_INVALID),
     (dict(damping=sgfd.DAMP_LOGR, damping_R=0.0), sgfd.ERR_INVALID),
     (dict(storage=9), sgfd.ERR_UNSUPPORTED),
+    (dict(arith=5), sgfd.ERR_INVALID),
 ])
 def test_create_rejects_bad_config(kw, code):
     cfg = sgfd.default_config(**kw)
@@ -79,7 +80,9 @@ def test_ricker_matches_oracle_bitwise():
 
 def test_pml_index_is_a_bijection(tmp_path):
     """Host-compiles the device layout helpers of csrc/sgfd_internal.h and checks
-    that pml_index() maps the PML cells one-to-one onto [0, npml) for uneven sizes."""
+    that pml_index() maps the PML cells one-to-one onto [0, npml) for uneven
+    sizes, and that the per-column/per-plane split the z-marching kernels use
+    gives the same index."""
     src = tmp_path / "t.cpp"
     src.write_text(r'''
 #include "sgfd_internal.h"
@@ -99,6 +102,8 @@ int main() {
       if (kx<0||kx>m.pml||ky<0||ky>m.pml||kz<0||kz>m.pml) { std::printf("bad band\n"); return 1; }
       int64_t i = pml_index(m, x-5, y-5, z-5);
       if (i < 0 || i >= m.npml) { std::printf("out of range %lld\n", (long long)i); return 1; }
+      PmlColumn pc = pml_column(m, x-5, y-5);
+      if (pml_plane_index(m, pc, z-5) != i) { std::printf("column/plane split differs\n"); return 1; }
       hit[i]++; cnt++;
     }
     if (cnt != m.npml) { std::printf("count %lld vs %lld\n", (long long)cnt, (long long)m.npml); return 1; }

@@ -20,18 +20,30 @@ CASES = [
     dict(quirks=sgfd.QUIRKS_FIXED, damping=sgfd.DAMP_REFCPU, nx=31, ny=29, nz=27, pml=3),
     dict(quirks=sgfd.QUIRKS_REF, damping=sgfd.DAMP_LOGR, nx=23, ny=22, nz=21, pml=1, nt=40),
     dict(quirks=sgfd.QUIRKS_REF, damping=sgfd.DAMP_REFGPU, nx=70, ny=36, nz=33, pml=8, nt=50),
+    # full 32x16 tiles with interior-only tile-planes, several z chunks
+    dict(quirks=sgfd.QUIRKS_FIXED, damping=sgfd.DAMP_LOGR, nx=90, ny=60, nz=50, pml=6, nt=45, nrec=60),
 ]
+# (id, kernel family, tile rows, z chunk)
+KERNELS = [("simple", sgfd.KERNEL_SIMPLE, 0, 0), ("zmarch", sgfd.KERNEL_ZMARCH, 8, 0),
+           ("zmarch_chunk7", sgfd.KERNEL_ZMARCH, 8, 7), ("zmarch_rows16", sgfd.KERNEL_ZMARCH, 16, 0),
+           ("zmarch_rows16_chunk5", sgfd.KERNEL_ZMARCH, 16, 5)]
 
 
 def _ids(c):
     return "_".join(f"{k}{v}" for k, v in c.items())
 
 
+@pytest.mark.parametrize("arith", [sgfd.ARITH_REF, sgfd.ARITH_FAST], ids=["ref", "fast"])
+@pytest.mark.parametrize("kernel", KERNELS, ids=[k[0] for k in KERNELS])
 @pytest.mark.parametrize("case", CASES, ids=[_ids(c) for c in CASES])
-def test_bit_exact_vs_oracle(case):
+def test_bit_exact_vs_oracle(case, kernel, arith):
     w = wl.small_random_case(**case)
+    w.cfg["arith"] = arith
     o = run_oracle(w)
-    with make_solver(w) as s:
+    with make_solver(w, kernel=kernel[1]) as s:
+        assert s.kernel_name() == kernel[0].split("_")[0]
+        if kernel[2]:
+            s.set_tiling(kernel[2], kernel[3])
         s.run(0, w.nt)
         s.synchronize()
         tr = s.traces()
@@ -43,6 +55,13 @@ def test_bit_exact_vs_oracle(case):
     o64 = run_oracle(w, fp64=True)
     err = rel_l2(tr, o64.traces())
     assert err < 1e-4, err
+
+
+def test_default_kernel_is_zmarch():
+    w = wl.small_random_case(nt=2)
+    with make_solver(w) as s:
+        assert s.kernel_name() == "zmarch"
+        assert s.launches_per_step() == 2
 
 
 def test_step_api_equals_run_api():
@@ -62,6 +81,21 @@ def test_source_inside_pml_matches_oracle():
     w = wl.small_random_case(nt=25)
     w.src = (6, 7, 8)
     o = run_oracle(w)
+    for kern in (sgfd.KERNEL_SIMPLE, sgfd.KERNEL_ZMARCH):
+        with make_solver(w, kernel=kern) as s:
+            s.run(0, w.nt)
+            np.testing.assert_array_equal(s.traces(), o.traces().astype(np.float32))
+
+
+def test_fast_arithmetic_within_tolerance_of_reference_rounding():
+    """FAST (coefficients pre-divided by the cell size) against the reference's
+    rounding (REF) on the same inputs: relative L2 of traces and final fields
+    below 1e-5, the north-star parity tolerance."""
+    w = wl.small_random_case(nx=60, ny=56, nz=52, pml=8, nt=200, nrec=40)
+    o = run_oracle(w)          # REF rounding
+    w.cfg["arith"] = sgfd.ARITH_FAST
     with make_solver(w) as s:
         s.run(0, w.nt)
-        np.testing.assert_array_equal(s.traces(), o.traces().astype(np.float32))
+        assert rel_l2(s.traces(), o.traces()) < 1e-5
+        for fid in (sgfd.VX, sgfd.TXX, sgfd.TYZ):
+            assert rel_l2(s.field(fid), o.field(fid)) < 1e-5

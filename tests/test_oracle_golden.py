@@ -61,3 +61,12 @@ def test_oracle_golden_main_arrival(golden_trace):
     err = rel_l2(tr, g)
     assert err < 1e-5, err
     assert abs(np.argmax(tr) - np.argmax(g)) == 0
+
+
+def test_fp64_fixture_against_reference_trace(golden_trace):
+    """The committed FP64 oracle trace (tests/golden/make_fp64_trace.py) sits
+    within FP32 rounding of the reference's own trace: 8.2e-6 relative L2."""
+    d64 = np.load(os.path.join(ROOT, "tests", "golden", "fp64_trace_reference_main.npy"))
+    assert d64.shape == golden_trace.shape
+    assert rel_l2(golden_trace, d64) < 1e-5
+    assert np.argmax(d64) == np.argmax(golden_trace)
