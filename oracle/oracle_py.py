@@ -144,3 +144,39 @@ class Oracle:
         out = np.zeros(self.shape, dtype=np.float64)
         lib().sgo_get_field(self.h, int(fid), _ptr(out, ctypes.c_double))
         return out
+
+
+# ---------------------------------------------------------------------------
+# The reference's own GPU program (oracle/_ref/ref_opt, built by oracle/Makefile
+# from 3DGPUwithPML_1DArraySingleGPU_optimization/ElasticWaveEquation.cu).
+# ---------------------------------------------------------------------------
+
+REF_OPT = os.path.join(_HERE, "_ref", "ref_opt")
+DROPIN_MAIN = os.path.join(_HERE, "_ref", "dropin_main")
+
+
+def write_ref_case(path, cfg: dict, b, lam, mu, src, station, nt: int, f0: float):
+    """Case file for ref_opt (format documented in oracle/ref_harness.cu)."""
+    with open(path, "wb") as f:
+        hdr = np.array([0x43464753, 1, cfg["nx"], cfg["ny"], cfg["nz"], cfg["pml"], nt, *src, *station, 0], np.int32)
+        f.write(hdr.tobytes())
+        fl = np.array([cfg["dt"], cfg["dx"], cfg["dy"], cfg["dz"], f0, *cfg["coef"]], np.float32)
+        f.write(fl.tobytes())
+        for a in (b, lam, mu):
+            f.write(np.ascontiguousarray(a, np.float32).tobytes())
+
+
+def run_ref_opt(workdir, cfg: dict, b, lam, mu, src, station, nt: int, f0: float):
+    """Run the reference program; returns (station trace [nt], fields [9, nz, ny, nx], device ms)."""
+    case = os.path.join(workdir, "case.bin")
+    out = os.path.join(workdir, "out.bin")
+    write_ref_case(case, cfg, b, lam, mu, src, station, nt, f0)
+    r = subprocess.run([REF_OPT, case, out], capture_output=True, text=True, timeout=900)
+    if r.returncode != 0:
+        raise RuntimeError(f"ref_opt failed: {r.stderr[-500:]}")
+    ms = float(r.stdout.split("ms=")[1].split()[0])
+    data = np.fromfile(out, dtype=np.float32)
+    n = cfg["nx"] * cfg["ny"] * cfg["nz"]
+    trace = data[:nt]
+    fields = data[nt:].reshape(9, cfg["nz"], cfg["ny"], cfg["nx"])
+    return trace, fields, ms
