@@ -142,13 +142,20 @@ def dist_setup(args):
 
 
 def max_over_ranks(x: float, world: int) -> float:
+    """Largest value over the ranks (the job's time is its slowest rank's)."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cpu" if dist.get_backend() == "gloo" else "cuda"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def job_rate(cells_per_rank: int, steps: int, ms_max: float, world: int) -> float:
+    """Whole-job Gcell-updates/s: every rank advances its own replica."""
+    return world * cells_per_rank * steps / (ms_max / 1e3) / 1e9
 
 
 def barrier(world):
@@ -235,11 +242,14 @@ def reference_gpu_program(ref_bin, w, steps):
 
 def main():
     args = parse()
+    if args.impl == "reference":
+        # CPU arm: rank 0 alone runs it, no process group is needed
+        rank = int(os.environ.get("RANK", "0"))
+        if rank == 0:
+            run_reference_arm(args, build_workload(args.workload), 1, 0)
+        return
     world, rank, local = dist_setup(args)
     w = build_workload(args.workload)
-    if args.impl == "reference":
-        run_reference_arm(args, w, world, rank)
-        return
     import torch
     import sgfd
     torch.cuda.set_device(local)
@@ -281,7 +291,7 @@ def main():
     barrier(world)
     clk = clocks.stop()
     ms = max_over_ranks(e0.elapsed_time(e1), world)
-    value = world * cells * K / (ms / 1e3) / 1e9
+    value = job_rate(cells, K, ms, world)
 
     # ---- roofline of the dominant kernel (events around each kernel) ----
     P = max(3, min(K, 20))

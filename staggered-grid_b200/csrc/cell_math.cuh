@@ -49,6 +49,27 @@ __device__ __forceinline__ float dB(const Physics &ph, G g) {
     return dbwd(ph.c, g) / (AXIS == 0 ? ph.dx : AXIS == 1 ? ph.dy : ph.dz);
 }
 
+// The same differences for two vertically adjacent cells (rows r and r+1)
+// that share one 11-value window, g(o) being the value o rows from row r:
+// forward windows span rows r-4 .. r+6, backward windows r-5 .. r+5.  Each
+// cell's sum is rounded exactly as dF / dB round it.
+template <bool FAST, int AXIS, class G>
+__device__ __forceinline__ void dF2(const Physics &ph, G g, float &d0, float &d1) {
+    float v[11];
+#pragma unroll
+    for (int j = 0; j < 11; ++j) v[j] = g(j - 4);
+    d0 = dF<FAST, AXIS>(ph, [&](int o) { return v[o + 4]; });
+    d1 = dF<FAST, AXIS>(ph, [&](int o) { return v[o + 5]; });
+}
+template <bool FAST, int AXIS, class G>
+__device__ __forceinline__ void dB2(const Physics &ph, G g, float &d0, float &d1) {
+    float v[11];
+#pragma unroll
+    for (int j = 0; j < 11; ++j) v[j] = g(j - 5);
+    d0 = dB<FAST, AXIS>(ph, [&](int o) { return v[o + 5]; });
+    d1 = dB<FAST, AXIS>(ph, [&](int o) { return v[o + 6]; });
+}
+
 // Harmonic mean 4 / (r0 + r1 + r2 + r3) of four reciprocals of mu
 // (ElasticMacro.h:111-112).  FAST computes 4 * RN(1/s), equal to RN(4/s)
 // because scaling by 4 is exact.

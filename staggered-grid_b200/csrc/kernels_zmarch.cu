@@ -2,8 +2,9 @@
 // and stress updates for sm_100a.
 //
 // Work decomposition.  A CTA of 256 threads owns a 32 x TY tile of computed
-// cells in the xy plane (TY = 8 * CELLS, each thread owning CELLS cells in
-// rows ty, ty + 8, ...) and marches along z over a chunk of planes.
+// cells in the xy plane (TY = 8 * CELLS, each thread owning CELLS vertically
+// adjacent cells, whose y differences share one window of staged values) and
+// marches along z over a chunk of planes.
 //
 // Data movement per plane z (all HBM traffic is TMA or coalesced 128-byte rows):
 //   * TMA (cp.async.bulk.tensor.3d, one elected thread, no multicast) stages
@@ -215,7 +216,7 @@ k_velocity_zmarch(const __grid_constant__ VelMaps mp, const __grid_constant__ Mo
     const uint32_t PL = (uint32_t)m.plane;
 #pragma unroll
     for (int c = 0; c < CELLS; ++c) {
-        lyc[c] = ty + 8 * c;
+        lyc[c] = CELLS * ty + c;   // a thread's cells are vertically adjacent
         gyc[c] = t.gy0 + lyc[c];
         act[c] = (t.cx0 + lx < m.nxc) && (t.cy0 + lyc[c] < m.nyc);
         kyc[c] = band(gyc[c], m.ny, m.pml);
@@ -311,6 +312,16 @@ k_velocity_zmarch(const __grid_constant__ VelMaps mp, const __grid_constant__ Mo
         const float *lzz = reinterpret_cast<const float *>(st + L::LZZ);
         const float *lb = reinterpret_cast<const float *>(st + L::LB);
 
+        // y differences of vertically adjacent cells share their windows
+        float xY2[2] = {0.f, 0.f}, yY2[2] = {0.f, 0.f}, zY2[2] = {0.f, 0.f};
+        if constexpr (CELLS == 2) {
+            const float *cxy0 = sxy + (lyc[0] + 5) * W48 + lx + 8;
+            const float *cyy0 = syy + (lyc[0] + 5) * W32 + lx;
+            const float *cyz0 = syz + (lyc[0] + 5) * W32 + lx;
+            dB2<FAST, 1>(ph, [&](int o) { return cxy0[o * W48]; }, xY2[0], xY2[1]);
+            dF2<FAST, 1>(ph, [&](int o) { return cyy0[o * W32]; }, yY2[0], yY2[1]);
+            dB2<FAST, 1>(ph, [&](int o) { return cyz0[o * W32]; }, zY2[0], zY2[1]);
+        }
 #pragma unroll
         for (int c = 0; c < CELLS; ++c) {
             const int ly = lyc[c];
@@ -332,13 +343,13 @@ k_velocity_zmarch(const __grid_constant__ VelMaps mp, const __grid_constant__ Mo
             const float *cyy = syy + (ly + 5) * W32 + lx;
             const float *cyz = syz + (ly + 5) * W32 + lx;
             const float xX = dF<FAST, 0>(ph, [&](int o) { return rxx[o]; });
-            const float xY = dB<FAST, 1>(ph, [&](int o) { return cxy[o * W48]; });
+            const float xY = CELLS == 2 ? xY2[c] : dB<FAST, 1>(ph, [&](int o) { return cxy[o * W48]; });
             const float xZ = dB<FAST, 2>(ph, [&](int o) { return qxz[c][5 + o]; });
             const float yX = dB<FAST, 0>(ph, [&](int o) { return cxy[o]; });
-            const float yY = dF<FAST, 1>(ph, [&](int o) { return cyy[o * W32]; });
+            const float yY = CELLS == 2 ? yY2[c] : dF<FAST, 1>(ph, [&](int o) { return cyy[o * W32]; });
             const float yZ = dB<FAST, 2>(ph, [&](int o) { return qyz[c][5 + o]; });
             const float zX = dB<FAST, 0>(ph, [&](int o) { return rxz[o]; });
-            const float zY = dB<FAST, 1>(ph, [&](int o) { return cyz[o * W32]; });
+            const float zY = CELLS == 2 ? zY2[c] : dB<FAST, 1>(ph, [&](int o) { return cyz[o * W32]; });
             const float zZ = dF<FAST, 2>(ph, [&](int o) { return qzz[c][4 + o]; });
             const float b0 = bb[ly * W36 + lx];
             const float bx = (b0 + bb[ly * W36 + lx + 1]) / 2.0f;
@@ -484,7 +495,7 @@ k_stress_zmarch(const __grid_constant__ StrMaps mp, const __grid_constant__ Mode
     const uint32_t PL = (uint32_t)m.plane;
 #pragma unroll
     for (int c = 0; c < CELLS; ++c) {
-        lyc[c] = ty + 8 * c;
+        lyc[c] = CELLS * ty + c;   // a thread's cells are vertically adjacent
         gyc[c] = t.gy0 + lyc[c];
         act[c] = (t.cx0 + lx < m.nxc) && (t.cy0 + lyc[c] < m.nyc);
         kyc[c] = band(gyc[c], m.ny, m.pml);
@@ -577,6 +588,15 @@ k_stress_zmarch(const __grid_constant__ StrMaps mp, const __grid_constant__ Mode
         const float *lly = reinterpret_cast<const float *>(st + L::LY);
         const float *llz = reinterpret_cast<const float *>(st + L::LZ);
 
+        float dYy2[2] = {0.f, 0.f}, xyY2[2] = {0.f, 0.f}, yzY2[2] = {0.f, 0.f};
+        if constexpr (CELLS == 2) {
+            const float *cx0 = svx + (lyc[0] + 5) * W48 + lx + 8;
+            const float *cy0 = svy + (lyc[0] + 5) * W48 + lx + 8;
+            const float *cz0 = svz + (lyc[0] + 5) * W48 + lx + 8;
+            dB2<FAST, 1>(ph, [&](int o) { return cy0[o * W48]; }, dYy2[0], dYy2[1]);
+            dF2<FAST, 1>(ph, [&](int o) { return cx0[o * W48]; }, xyY2[0], xyY2[1]);
+            dF2<FAST, 1>(ph, [&](int o) { return cz0[o * W48]; }, yzY2[0], yzY2[1]);
+        }
 #pragma unroll
         for (int c = 0; c < CELLS; ++c) {
             const int ly = lyc[c];
@@ -595,14 +615,14 @@ k_stress_zmarch(const __grid_constant__ StrMaps mp, const __grid_constant__ Mode
             const float *cy_ = svy + (ly + 5) * W48 + lx + 8;
             const float *cz_ = svz + (ly + 5) * W48 + lx + 8;
             const float dXx = dB<FAST, 0>(ph, [&](int o) { return cx_[o]; });
-            const float dYy = dB<FAST, 1>(ph, [&](int o) { return cy_[o * W48]; });
+            const float dYy = CELLS == 2 ? dYy2[c] : dB<FAST, 1>(ph, [&](int o) { return cy_[o * W48]; });
             const float dZz = dB<FAST, 2>(ph, [&](int o) { return qz[c][5 + o]; });
-            const float xyY = dF<FAST, 1>(ph, [&](int o) { return cx_[o * W48]; });
+            const float xyY = CELLS == 2 ? xyY2[c] : dF<FAST, 1>(ph, [&](int o) { return cx_[o * W48]; });
             const float xyX = dF<FAST, 0>(ph, [&](int o) { return cy_[o]; });
             const float xzZ = dF<FAST, 2>(ph, [&](int o) { return qx[c][4 + o]; });
             const float xzX = dF<FAST, 0>(ph, [&](int o) { return cz_[o]; });
             const float yzZ = dF<FAST, 2>(ph, [&](int o) { return qy[c][4 + o]; });
-            const float yzY = dF<FAST, 1>(ph, [&](int o) { return cz_[o * W48]; });
+            const float yzY = CELLS == 2 ? yzY2[c] : dF<FAST, 1>(ph, [&](int o) { return cz_[o * W48]; });
 
             const float l = lcur[c];
             const float l2m = __fmaf_rn(2.0f, mcur[c], l);
