@@ -179,10 +179,16 @@ int sgfd_set_wavelet(sgfd_solver *h, int32_t nt, const float *values);
 /* One time step with a host-supplied source value (reference propagate()). */
 int sgfd_step(sgfd_solver *h, int32_t it, float source_value);
 
-/* Steps it0 .. it0+nsteps-1 with the wavelet of sgfd_set_wavelet; launched
- * as a captured CUDA graph when use_graph != 0.  Asynchronous on the
- * handle's stream. */
+/* Steps it0 .. it0+nsteps-1 with the wavelet of sgfd_set_wavelet.
+ * Asynchronous on the handle's stream.  With use_graph != 0, runs of 16
+ * steps replay one captured CUDA graph whose kernels take the step index
+ * from a device counter; the graph is captured on first use and again after
+ * any setter changes what the kernels are given.  Results are identical to
+ * sgfd_step with the wavelet's values. */
 int sgfd_run(sgfd_solver *h, int32_t it0, int32_t nsteps, int32_t use_graph);
+/* Capture (if out of date) and upload the graph of sgfd_run now, so that the
+ * next sgfd_run with use_graph != 0 starts replaying at once. */
+int sgfd_prepare_run(sgfd_solver *h);
 
 int sgfd_synchronize(sgfd_solver *h);
 
@@ -223,6 +229,8 @@ int sgfd_set_tiling(sgfd_solver *h, int32_t tile_rows, int32_t zchunk);
 int sgfd_cell_counts(const sgfd_solver *h, int64_t *n_interior, int64_t *n_pml);
 /* Number of kernel launches issued by one sgfd_step / one step of sgfd_run. */
 int sgfd_launches_per_step(const sgfd_solver *h);
+/* Number of kernel launches sgfd_run(h, *, nsteps, use_graph) issues. */
+int sgfd_run_launches(const sgfd_solver *h, int32_t nsteps, int32_t use_graph);
 /* Name of the kernel family in use ("simple", "zmarch"). */
 const char *sgfd_kernel_name(const sgfd_solver *h);
 

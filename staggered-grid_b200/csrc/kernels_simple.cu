@@ -16,8 +16,9 @@ namespace {
 constexpr int kBX = 32, kBY = 8;
 
 // txx, tyy, tzz at the source cell += dt*dt*s(it)   (ElasticWaveEquation.cu:206-221)
-__global__ void k_inject(Model m, Physics ph, SourceRec sr, int it, float value, int use_wavelet) {
+__global__ void k_inject(Model m, Physics ph, SourceRec sr, int it_arg, float value, int use_wavelet) {
     if (threadIdx.x != 0 || sr.src < 0) return;
+    const int it = step_index(sr, it_arg);
     const float s = use_wavelet ? sr.wavelet[it] : value;
     const float v = ph.inj_dt2 * s;
     m.f[3][sr.src] = m.f[3][sr.src] + v;
@@ -164,12 +165,19 @@ __global__ void __launch_bounds__(kBX * kBY) k_stress(Model m, Physics ph) {
 }
 
 // Receivers of one phase sample their component (ElasticWaveEquation.cu:223-232).
-__global__ void k_record(Model m, SourceRec sr, int it, int velocity_phase) {
+__global__ void k_record(Model m, SourceRec sr, int it_arg, int velocity_phase) {
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    const int it = step_index(sr, it_arg);
     if (r >= sr.nrec || it < 0 || it >= sr.nt) return;
     const int4 q = sr.rec[r];
     if ((q.w <= 2) != (velocity_phase != 0)) return;
     sr.traces[(int64_t)it * sr.nrec + r] = m.f[q.w][pidx(m, q.x, q.y, q.z)];
+}
+
+// Device step counter of a replayed CUDA graph: set before the first replay,
+// advanced by the last node of each replay.
+__global__ void k_counter(int *ctr, int value, int add) {
+    if (threadIdx.x == 0) *ctr = add ? *ctr + value : value;
 }
 
 __global__ void k_reciprocal(float *rmu, const float *mu, int64_t n) {
@@ -201,6 +209,11 @@ cudaError_t simple_step(const Model &m, const Physics &ph, const SourceRec &sr,
     else k_stress<false><<<grid, block, 0, s>>>(m, ph);
     if (ev) cudaEventRecord(ev[3], s);
     if (sr.nrec > 0) k_record<<<(sr.nrec + 127) / 128, 128, 0, s>>>(m, sr, it, 0);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_counter(int *ctr, int value, bool add, cudaStream_t s) {
+    k_counter<<<1, 32, 0, s>>>(ctr, value, add ? 1 : 0);
     return cudaGetLastError();
 }
 

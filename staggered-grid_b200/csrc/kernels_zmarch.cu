@@ -178,7 +178,7 @@ __device__ __forceinline__ void vel_issue(const VelMaps &mp, unsigned char *st, 
 template <bool FAST, int CELLS>
 __global__ void __launch_bounds__(NT, 2)
 k_velocity_zmarch(const __grid_constant__ VelMaps mp, const __grid_constant__ Model m, const __grid_constant__ Physics ph,
-                  const __grid_constant__ ZGeom g, const __grid_constant__ SourceRec sr, int it,
+                  const __grid_constant__ ZGeom g, const __grid_constant__ SourceRec sr, int it_arg,
                   float src_value, int use_wavelet) {
     constexpr int TY = 8 * CELLS;
     using L = VelL<TY>;
@@ -198,6 +198,7 @@ k_velocity_zmarch(const __grid_constant__ VelMaps mp, const __grid_constant__ Mo
         issued_end = min(t.zs + S, t.ze);
     }
 
+    const int it = step_index(sr, it_arg);
     const float inj = ph.inj_dt2 * ((use_wavelet && sr.wavelet) ? sr.wavelet[it] : src_value);
     int sx = -1, sy = -1, sz = -1;
     if (sr.src >= 0) {
@@ -461,7 +462,7 @@ __device__ __forceinline__ void str_issue(const StrMaps &mp, unsigned char *st, 
 template <bool FAST, int CELLS>
 __global__ void __launch_bounds__(NT, 2)
 k_stress_zmarch(const __grid_constant__ StrMaps mp, const __grid_constant__ Model m, const __grid_constant__ Physics ph,
-                  const __grid_constant__ ZGeom g, const __grid_constant__ SourceRec sr, int it,
+                  const __grid_constant__ ZGeom g, const __grid_constant__ SourceRec sr, int it_arg,
                 float src_value, int use_wavelet) {
     constexpr int TY = 8 * CELLS;
     constexpr int RH = TY + 1;       // 1/mu tile: (x0..x0+32) x (y0..y0+TY)
@@ -483,6 +484,7 @@ k_stress_zmarch(const __grid_constant__ StrMaps mp, const __grid_constant__ Mode
         issued_end = min(t.zs + S, t.ze);
     }
 
+    const int it = step_index(sr, it_arg);
     const float inj = ph.inj_dt2 * ((use_wavelet && sr.wavelet) ? sr.wavelet[it] : src_value);
     const int64_t src = sr.src;
 

@@ -21,44 +21,15 @@
 #include <string>
 #include <vector>
 
-#include "../../include/sgfd.h"
-#include "sgfd_internal.h"
-#include "zmarch.h"
+#include "solver.h"
 
 using namespace sgfd;
 
-struct sgfd_solver {
-    sgfd_config cfg{};
-    Model m{};
-    Physics ph{};
-    SourceRec sr{};
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    cudaStream_t own_stream = nullptr;
-    char *field_pool = nullptr;   // 9 fields + b, lambda, mu, 1/mu
-    float *split = nullptr;
-    int4 *rec = nullptr;
-    float *traces = nullptr;
-    float *wavelet = nullptr;
-    int wavelet_nt = 0;
-    bool medium_set = false;
-    int kernel = SGFD_KERNEL_SIMPLE;
-    // z-marching family
-    VelMaps vm{};
-    StrMaps sm{};
-    ZGeom zg{};
-    int zchunk_req = 0;
-    std::vector<int4> rec_host;   // receivers, for re-bucketing when the tiling changes
-    int *zrec_off = nullptr;
-    int4 *zrec_list = nullptr;
-    int *zrec_idx = nullptr;
-    int *dev_err = nullptr;
-    std::string err;
-};
-
 namespace {
-
 thread_local std::string g_error;
+}  // namespace
+
+namespace sgfd {
 
 int fail(sgfd_solver *h, int code, const char *fmt, ...) {
     char buf[512];
@@ -74,13 +45,28 @@ int cuda_fail(sgfd_solver *h, cudaError_t e, const char *what) {
     return fail(h, SGFD_ERR_CUDA, "%s: %s (%s)", what, cudaGetErrorName(e), cudaGetErrorString(e));
 }
 
-#define SG_CUDA(h, call, what)                          \
-    do {                                                \
-        cudaError_t e_ = (call);                        \
-        if (e_ != cudaSuccess) return cuda_fail(h, e_, what); \
-    } while (0)
+int check_handle(sgfd_solver *h) {
+    if (!h) return fail(nullptr, SGFD_ERR_INVALID, "null handle");
+    cudaError_t e = cudaSetDevice(h->device);
+    if (e != cudaSuccess) return cuda_fail(h, e, "cudaSetDevice");
+    return SGFD_OK;
+}
 
-inline size_t round_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+int check_device_error(sgfd_solver *h) {
+    if (!h->dev_err) return SGFD_OK;
+    int flag = 0;
+    SG_CUDA(h, cudaMemcpyAsync(&flag, h->dev_err, sizeof(int), cudaMemcpyDeviceToHost, h->stream), "error flag");
+    SG_CUDA(h, cudaStreamSynchronize(h->stream), "error flag");
+    if (flag) {
+        cudaMemsetAsync(h->dev_err, 0, sizeof(int), h->stream);
+        return fail(h, SGFD_ERR_CUDA, "a kernel's bounded wait for its TMA copies gave up (flag %d)", flag);
+    }
+    return SGFD_OK;
+}
+
+}  // namespace sgfd
+
+namespace {
 
 bool finite_pos(float v) { return std::isfinite(v) && v > 0.0f; }
 
@@ -116,17 +102,70 @@ void set_physics(sgfd_solver *h) {
     }
 }
 
-int check_handle(sgfd_solver *h) {
-    if (!h) return fail(nullptr, SGFD_ERR_INVALID, "null handle");
-    cudaError_t e = cudaSetDevice(h->device);
-    if (e != cudaSuccess) return cuda_fail(h, e, "cudaSetDevice");
-    return SGFD_OK;
+cudaError_t dispatch_on(sgfd_solver *h, const SourceRec &sr, cudaStream_t s, int it, float value,
+                        bool use_wavelet, cudaEvent_t *ev) {
+    if (h->kernel == SGFD_KERNEL_ZMARCH)
+        return zmarch_step(h->m, h->ph, sr, h->zg, h->vm, h->sm, it, value, use_wavelet, s, ev);
+    return simple_step(h->m, h->ph, sr, it, value, use_wavelet, s, ev);
 }
 
 cudaError_t dispatch_step(sgfd_solver *h, int it, float value, bool use_wavelet, cudaEvent_t *ev) {
-    if (h->kernel == SGFD_KERNEL_ZMARCH)
-        return zmarch_step(h->m, h->ph, h->sr, h->zg, h->vm, h->sm, it, value, use_wavelet, h->stream, ev);
-    return simple_step(h->m, h->ph, h->sr, it, value, use_wavelet, h->stream, ev);
+    return dispatch_on(h, h->sr, h->stream, it, value, use_wavelet, ev);
+}
+
+void graph_key(const sgfd_solver *h, GraphKey *k) {
+    std::memset(static_cast<void *>(k), 0, sizeof *k);
+    std::memcpy(static_cast<void *>(&k->m), &h->m, sizeof h->m);
+    std::memcpy(static_cast<void *>(&k->ph), &h->ph, sizeof h->ph);
+    std::memcpy(static_cast<void *>(&k->sr), &h->sr, sizeof h->sr);
+    std::memcpy(static_cast<void *>(&k->zg), &h->zg, sizeof h->zg);
+    std::memcpy(static_cast<void *>(&k->vm), &h->vm, sizeof h->vm);
+    std::memcpy(static_cast<void *>(&k->sm), &h->sm, sizeof h->sm);
+    k->kernel = h->kernel;
+}
+
+void release_graph(sgfd_solver *h) {
+    if (h->graph) cudaGraphExecDestroy(h->graph);
+    h->graph = nullptr;
+}
+
+// Capture kGraphSteps steps on a private stream.  Step k of the graph runs
+// step *step_ctr + k; the last node adds kGraphSteps to the counter, so
+// consecutive replays walk through consecutive steps.
+int capture_graph(sgfd_solver *h) {
+    release_graph(h);
+    if (!h->cap_stream)
+        SG_CUDA(h, cudaStreamCreateWithFlags(&h->cap_stream, cudaStreamNonBlocking), "capture stream");
+    if (!h->step_ctr) {
+        SG_CUDA(h, cudaMalloc(&h->step_ctr, sizeof(int)), "step counter");
+        SG_CUDA(h, cudaMemset(h->step_ctr, 0, sizeof(int)), "step counter");
+    }
+    SourceRec sr = h->sr;
+    sr.it_dev = h->step_ctr;
+    SG_CUDA(h, cudaStreamBeginCapture(h->cap_stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+    cudaError_t e = cudaSuccess;
+    for (int k = 0; k < kGraphSteps && e == cudaSuccess; ++k)
+        e = dispatch_on(h, sr, h->cap_stream, k, 0.0f, true, nullptr);
+    if (e == cudaSuccess) e = launch_counter(h->step_ctr, kGraphSteps, true, h->cap_stream);
+    cudaGraph_t g = nullptr;
+    const cudaError_t e_end = cudaStreamEndCapture(h->cap_stream, &g);
+    if (e == cudaSuccess) e = e_end;
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&h->graph, g, 0);
+    if (g) cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        h->graph = nullptr;
+        cudaGetLastError();
+        return cuda_fail(h, e, "graph capture");
+    }
+    graph_key(h, &h->graph_key);
+    return SGFD_OK;
+}
+
+bool graph_current(const sgfd_solver *h) {
+    if (!h->graph) return false;
+    GraphKey k;
+    graph_key(h, &k);
+    return std::memcmp(&k, &h->graph_key, sizeof k) == 0;
 }
 
 int launch_step(sgfd_solver *h, int it, float value, bool use_wavelet) {
@@ -190,18 +229,6 @@ int upload_zrec(sgfd_solver *h, const std::vector<int4> &rec) {
     h->zg.rec_off = h->zrec_off;
     h->zg.rec_list = h->zrec_list;
     h->zg.rec_idx = h->zrec_idx;
-    return SGFD_OK;
-}
-
-int check_device_error(sgfd_solver *h) {
-    if (!h->dev_err) return SGFD_OK;
-    int flag = 0;
-    SG_CUDA(h, cudaMemcpyAsync(&flag, h->dev_err, sizeof(int), cudaMemcpyDeviceToHost, h->stream), "error flag");
-    SG_CUDA(h, cudaStreamSynchronize(h->stream), "error flag");
-    if (flag) {
-        cudaMemsetAsync(h->dev_err, 0, sizeof(int), h->stream);
-        return fail(h, SGFD_ERR_CUDA, "a kernel's bounded wait for its TMA copies gave up (flag %d)", flag);
-    }
     return SGFD_OK;
 }
 
@@ -292,7 +319,7 @@ int sgfd_create(const sgfd_config *cfg, sgfd_solver **out) {
     m.nxc = c.nx - 2 * kHalo; m.nyc = c.ny - 2 * kHalo; m.nzc = c.nz - 2 * kHalo;
     m.plane = (int64_t)m.px * m.ny;
     m.npml = pml_count(m.nxc, m.nyc, m.nzc, m.pml);
-    const size_t arr_bytes = round_up((size_t)m.plane * m.nz * sizeof(float), 256);
+    const size_t arr_bytes = array_bytes(m);
     const size_t pool_bytes = arr_bytes * 13;
     e = cudaMalloc(&h->field_pool, pool_bytes);
     if (e == cudaSuccess) e = cudaMalloc(&h->split, (size_t)kNumSplit * m.npml * sizeof(float));
@@ -360,6 +387,9 @@ void sgfd_destroy(sgfd_solver *h) {
     cudaFree(h->zrec_list);
     cudaFree(h->zrec_idx);
     cudaFree(h->dev_err);
+    release_graph(h);
+    cudaFree(h->step_ctr);
+    if (h->cap_stream) cudaStreamDestroy(h->cap_stream);
     if (h->own_stream) cudaStreamDestroy(h->own_stream);
     delete h;
 }
@@ -479,18 +509,47 @@ int sgfd_step(sgfd_solver *h, int32_t it, float source_value) {
 }
 
 int sgfd_run(sgfd_solver *h, int32_t it0, int32_t nsteps, int32_t use_graph) {
-    (void)use_graph;
     int r = check_handle(h);
     if (r) return r;
     if (!h->medium_set) return fail(h, SGFD_ERR_STATE, "sgfd_set_medium must come before stepping");
     if (nsteps < 0 || it0 < 0) return fail(h, SGFD_ERR_INVALID, "bad step range");
+    if ((int64_t)it0 + nsteps > INT32_MAX) return fail(h, SGFD_ERR_INVALID, "step range overflows int32");
     if (h->sr.src >= 0 && (int64_t)it0 + nsteps > h->wavelet_nt)
         return fail(h, SGFD_ERR_STATE, "wavelet covers %d steps, run needs %d", h->wavelet_nt, it0 + nsteps);
-    for (int it = it0; it < it0 + nsteps; ++it) {
+    int it = it0, left = nsteps;
+    if (use_graph && left >= kGraphSteps) {
+        if (!graph_current(h)) {
+            r = capture_graph(h);
+            if (r) return r;
+        }
+        SG_CUDA(h, launch_counter(h->step_ctr, it, false, h->stream), "step counter");
+        for (; left >= kGraphSteps; left -= kGraphSteps, it += kGraphSteps)
+            SG_CUDA(h, cudaGraphLaunch(h->graph, h->stream), "graph launch");
+    }
+    for (; left > 0; --left, ++it) {
         r = launch_step(h, it, 0.0f, true);
         if (r) return r;
     }
     return SGFD_OK;
+}
+
+int sgfd_prepare_run(sgfd_solver *h) {
+    int r = check_handle(h);
+    if (r) return r;
+    if (!h->medium_set) return fail(h, SGFD_ERR_STATE, "sgfd_set_medium must come before stepping");
+    if (!graph_current(h)) {
+        r = capture_graph(h);
+        if (r) return r;
+    }
+    SG_CUDA(h, cudaGraphUpload(h->graph, h->stream), "graph upload");
+    return SGFD_OK;
+}
+
+int sgfd_run_launches(const sgfd_solver *h, int32_t nsteps, int32_t use_graph) {
+    if (!h || nsteps < 0) return -1;
+    const int per = sgfd_launches_per_step(h);
+    const int replays = use_graph && nsteps >= kGraphSteps ? nsteps / kGraphSteps : 0;
+    return nsteps * per + (replays ? 1 + replays : 0);   // counter set + one advance per replay
 }
 
 int sgfd_synchronize(sgfd_solver *h) {
@@ -534,7 +593,7 @@ int sgfd_reset(sgfd_solver *h) {
     int r = check_handle(h);
     if (r) return r;
     const Model &m = h->m;
-    const size_t arr_bytes = round_up((size_t)m.plane * m.nz * sizeof(float), 256);
+    const size_t arr_bytes = array_bytes(m);
     SG_CUDA(h, cudaMemsetAsync(h->field_pool, 0, arr_bytes * 9, h->stream), "reset fields");
     SG_CUDA(h, cudaMemsetAsync(h->split, 0, (size_t)kNumSplit * m.npml * sizeof(float), h->stream), "reset splits");
     if (h->traces)

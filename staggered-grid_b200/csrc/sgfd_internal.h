@@ -77,7 +77,16 @@ struct SourceRec {
     const int4 *rec;     // x, y, z, comp
     float *traces;       // time-major: traces[it * nrec + r]
     int nt;
+    const int *it_dev;   // graph replay: step index = *it_dev + the launch's offset; nullptr otherwise
 };
+
+#ifdef __CUDACC__
+// Step index a kernel works on: the launch argument, plus the device step
+// counter when the launch belongs to a replayed CUDA graph.
+__device__ __forceinline__ int step_index(const SourceRec &sr, int it_arg) {
+    return sr.it_dev ? it_arg + *sr.it_dev : it_arg;
+}
+#endif
 
 __host__ __device__ inline int64_t pidx(const Model &m, int x, int y, int z) {
     return (int64_t)x + (int64_t)y * m.px + (int64_t)z * m.plane;
@@ -157,5 +166,7 @@ int simple_launches_per_step(const SourceRec &sr);
 
 // medium post-processing: rmu = 1/mu over the padded arrays.
 cudaError_t launch_reciprocal(float *rmu, const float *mu, int64_t n, cudaStream_t s);
+// *ctr = value, or *ctr += value when add is set.
+cudaError_t launch_counter(int *ctr, int value, bool add, cudaStream_t s);
 
 }  // namespace sgfd

@@ -1,0 +1,85 @@
+// solver.h — the handle behind sgfd_solver* and the error helpers shared by
+// the translation units of the C ABI (sgfd_api.cu, checkpoint.cu).
+#pragma once
+
+#include <string>
+#include <vector>
+
+#include "../../include/sgfd.h"
+#include "sgfd_internal.h"
+#include "zmarch.h"
+
+namespace sgfd {
+// Every value a captured step passes to its kernels.  A graph is replayed
+// only while a fresh copy compares equal byte for byte; any setter that
+// changes a pointer, a size or a tiling therefore forces a new capture.
+struct GraphKey {
+    Model m;
+    Physics ph;
+    SourceRec sr;
+    ZGeom zg;
+    VelMaps vm;
+    StrMaps sm;
+    int kernel;
+};
+// Steps per captured graph; sgfd_run launches the remainder directly.
+constexpr int kGraphSteps = 16;
+}  // namespace sgfd
+
+struct sgfd_solver {
+    sgfd_config cfg{};
+    sgfd::Model m{};
+    sgfd::Physics ph{};
+    sgfd::SourceRec sr{};
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaStream_t own_stream = nullptr;
+    char *field_pool = nullptr;   // 9 fields + b, lambda, mu, 1/mu
+    float *split = nullptr;
+    int4 *rec = nullptr;
+    float *traces = nullptr;
+    float *wavelet = nullptr;
+    int wavelet_nt = 0;
+    bool medium_set = false;
+    int kernel = SGFD_KERNEL_SIMPLE;
+    // z-marching family
+    sgfd::VelMaps vm{};
+    sgfd::StrMaps sm{};
+    sgfd::ZGeom zg{};
+    int zchunk_req = 0;
+    std::vector<int4> rec_host;   // receivers, for re-bucketing when the tiling changes
+    int *zrec_off = nullptr;
+    int4 *zrec_list = nullptr;
+    int *zrec_idx = nullptr;
+    int *dev_err = nullptr;
+    // CUDA-graph replay of sgfd_run
+    cudaStream_t cap_stream = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    int *step_ctr = nullptr;      // device step counter read by the replayed kernels
+    sgfd::GraphKey graph_key{};   // launch parameters the graph was captured with
+    std::string err;
+};
+
+namespace sgfd {
+
+// Record an error message on the handle (or, with h == nullptr, in the
+// thread's global slot read by sgfd_global_error) and return code.
+int fail(sgfd_solver *h, int code, const char *fmt, ...);
+int cuda_fail(sgfd_solver *h, cudaError_t e, const char *what);
+// Null check and cudaSetDevice of the handle's device.
+int check_handle(sgfd_solver *h);
+// Read and clear the kernels' device error flag.
+int check_device_error(sgfd_solver *h);
+
+inline size_t round_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+// Bytes of one padded device array (fields and medium share this size).
+inline size_t array_bytes(const Model &m) { return round_up((size_t)m.plane * m.nz * sizeof(float), 256); }
+
+}  // namespace sgfd
+
+#define SG_CUDA(h, call, what)                                        \
+    do {                                                              \
+        cudaError_t e_ = (call);                                      \
+        if (e_ != cudaSuccess) return sgfd::cuda_fail(h, e_, what);   \
+    } while (0)

@@ -101,6 +101,8 @@ def lib() -> ctypes.CDLL:
         "sgfd_set_tiling": (ctypes.c_int, [vp, i32, i32]),
         "sgfd_cell_counts": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)]),
         "sgfd_launches_per_step": (ctypes.c_int, [vp]),
+        "sgfd_run_launches": (ctypes.c_int, [vp, ctypes.c_int32, ctypes.c_int32]),
+        "sgfd_prepare_run": (ctypes.c_int, [vp]),
         "sgfd_kernel_name": (ctypes.c_char_p, [vp]),
     }
     for name, (res, args) in sigs.items():
@@ -217,6 +219,9 @@ class Solver:
     def run(self, it0: int, nsteps: int, graph: bool = True):
         self._check(lib().sgfd_run(self.h, it0, nsteps, 1 if graph else 0))
 
+    def prepare_run(self):
+        self._check(lib().sgfd_prepare_run(self.h))
+
     def synchronize(self):
         self._check(lib().sgfd_synchronize(self.h))
 
@@ -264,6 +269,9 @@ class Solver:
 
     def launches_per_step(self) -> int:
         return lib().sgfd_launches_per_step(self.h)
+
+    def run_launches(self, nsteps: int, graph: bool = True) -> int:
+        return lib().sgfd_run_launches(self.h, nsteps, 1 if graph else 0)
 
     def kernel_name(self) -> str:
         return lib().sgfd_kernel_name(self.h).decode()

@@ -22,6 +22,8 @@ CASES = [
     dict(quirks=sgfd.QUIRKS_REF, damping=sgfd.DAMP_REFGPU, nx=70, ny=36, nz=33, pml=8, nt=50),
     # full 32x16 tiles with interior-only tile-planes, several z chunks
     dict(quirks=sgfd.QUIRKS_FIXED, damping=sgfd.DAMP_LOGR, nx=90, ny=60, nz=50, pml=6, nt=45, nrec=60),
+    # a tall interior core: most tile-planes take the interior-only path
+    dict(quirks=sgfd.QUIRKS_REF, damping=sgfd.DAMP_REFGPU, nx=100, ny=58, nz=64, pml=4, nt=30, nrec=6),
 ]
 # (id, kernel family, tile rows, z chunk)
 KERNELS = [("simple", sgfd.KERNEL_SIMPLE, 0, 0), ("zmarch", sgfd.KERNEL_ZMARCH, 8, 0),
@@ -73,6 +75,38 @@ def test_step_api_equals_run_api():
         a.synchronize(); b.synchronize()
         np.testing.assert_array_equal(a.traces(), b.traces())
         np.testing.assert_array_equal(a.field(sgfd.TXX), b.field(sgfd.TXX))
+
+
+@pytest.mark.parametrize("kern", [sgfd.KERNEL_SIMPLE, sgfd.KERNEL_ZMARCH], ids=["simple", "zmarch"])
+def test_graph_replay_equals_direct_launches(kern):
+    """sgfd_run with CUDA graphs (16-step replays driven by a device step
+    counter, remainder launched directly) against direct launches: bit-equal
+    traces and fields, for one long run, for runs split at arbitrary steps, and
+    after a receiver change that forces a new capture."""
+    w = wl.small_random_case(nt=77, nrec=24)
+    with make_solver(w, kernel=kern) as a, make_solver(w, kernel=kern) as b, make_solver(w, kernel=kern) as c:
+        a.run(0, w.nt, graph=False)
+        b.prepare_run()
+        b.run(0, w.nt, graph=True)
+        for it0, n in ((0, 17), (17, 3), (20, 32), (52, 25)):
+            c.run(it0, n, graph=True)
+        for s in (a, b, c):
+            s.synchronize()
+        np.testing.assert_array_equal(b.traces(), a.traces())
+        np.testing.assert_array_equal(c.traces(), a.traces())
+        for fid in range(9):
+            np.testing.assert_array_equal(b.field(fid), a.field(fid))
+            np.testing.assert_array_equal(c.field(fid), a.field(fid))
+        assert b.run_launches(w.nt, True) == w.nt * b.launches_per_step() + 1 + w.nt // 16
+        assert b.run_launches(w.nt, False) == w.nt * b.launches_per_step()
+        # new receivers: the captured graph no longer matches and is re-captured
+        xyz = w.rec_xyz[::-1].copy()
+        for s in (a, b):
+            s.reset()
+            s.set_receivers(xyz, w.rec_comp, w.nt)
+        a.run(0, w.nt, graph=False)
+        b.run(0, w.nt, graph=True)
+        np.testing.assert_array_equal(b.traces(), a.traces())
 
 
 def test_source_inside_pml_matches_oracle():
