@@ -49,7 +49,10 @@ def parse():
     p.add_argument("--steps", type=int, default=100)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", choices=["sgfd", "reference"], default="sgfd")
-    p.add_argument("--workload", choices=["random344", "plain100", "reference_main"], default="random344")
+    p.add_argument("--workload", choices=["random344", "random472", "random216", "plain100", "reference_main",
+                                               "batch32"],
+                   default="random344")
+    p.add_argument("--no-autotune", action="store_true", help="batch32: keep the default launch shapes")
     p.add_argument("--kernel", choices=["auto", "simple", "zmarch"], default="auto")
     p.add_argument("--arith", choices=["ref", "fast"], default="fast")
     p.add_argument("--no-e2e", action="store_true")
@@ -62,6 +65,11 @@ def build_workload(name):
     import sgfd.workloads as wl
     if name == "random344":
         return wl.random_cube(n_interior=344, pml=20, nt=2000)
+    if name == "random472":
+        return wl.random_cube(n_interior=472, pml=20, nt=3000, dt=0.0008, std=0.08, corr_m=80.0, seed=4,
+                              src_computed=(256, 256, 40))
+    if name == "random216":            # a smaller cube of the same kind, for ncu captures
+        return wl.random_cube(n_interior=216, pml=20, nt=2000, src_computed=(128, 128, 40))
     if name == "plain100":
         return wl.plain_cube(n_interior=100, pml=20, nt=500)
     return wl.reference_case(nt=1500)
@@ -246,9 +254,18 @@ def main():
         # CPU arm: rank 0 alone runs it, no process group is needed
         rank = int(os.environ.get("RANK", "0"))
         if rank == 0:
-            run_reference_arm(args, build_workload(args.workload), 1, 0)
+            if args.workload == "batch32":
+                import sgfd.workloads as wl
+                w = wl.layered_model(wl.batch_specs()[0])
+                w.name = "batch32 (sample: model 0, %s)" % w.name
+                run_reference_arm(args, w, 1, 0)
+            else:
+                run_reference_arm(args, build_workload(args.workload), 1, 0)
         return
     world, rank, local = dist_setup(args)
+    if args.workload == "batch32":
+        main_batch(args, world, rank, local)
+        return
     w = build_workload(args.workload)
     import torch
     import sgfd
@@ -336,6 +353,122 @@ def main():
             "value": rate, "unit": "Gcell/s", "cores": threads, "kind": "port",
             "sample": f"{args.cpu_steps} full time steps of {w.name} ({secs:.1f} s) after 1 untimed step; "
                       f"C++ oracle of the reference kernels, FP32, flush-to-zero, OpenMP {threads} threads"}
+    if rank == 0:
+        print(json.dumps(result), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def main_batch(args, world, rank, local):
+    """The batched configuration: 32 layered models of uneven size (359 M
+    computed cells in all), each with its own source and 128 receivers,
+    advanced together by sgfd_batch_run (16-step graphs, one branch per
+    model).  With N ranks the models are dealt out by computed cells (greedy,
+    largest first); value = all ranks' cells x steps / slowest rank's time."""
+    import torch
+    import sgfd
+    import sgfd.workloads as wl
+    torch.cuda.set_device(local)
+    K, W = args.steps, args.warmup
+    specs = wl.batch_specs()
+    cells_all = [sp.computed_cells() for sp in specs]
+    mine = wl.balance(cells_all, world)[rank]
+    models, media, tunings = [], [], []
+    n_int = n_pml = 0
+    for i in mine:
+        w = wl.layered_model(specs[i])
+        nt = max(w.nt, W + K + 16)
+        wav = np.resize(w.wavelet, nt).astype(np.float32)
+        s = sgfd.Solver(sgfd.default_config(**{**w.cfg, "device": local, "arith": sgfd.ARITH_FAST}))
+        s.set_medium(w.b, w.lam, w.mu)
+        s.set_source(*w.src)
+        s.set_receivers(w.rec_xyz, w.rec_comp, nt)
+        s.set_wavelet(wav)
+        if not args.no_autotune:
+            t = s.autotune(3)
+            tunings.append({"model": i, "kernel": "zmarch" if t.kernel == sgfd.KERNEL_ZMARCH else "simple",
+                            "tile_rows": t.tile_rows, "zchunk": t.zchunk, "ms": round(t.ms_per_step, 4)})
+        a, b = s.cell_counts()
+        n_int += a
+        n_pml += b
+        models.append(s)
+        media.append((w.b, w.lam, w.mu, len(w.rec_comp)))
+    batch = sgfd.Batch(models)
+    stream = torch.cuda.ExternalStream(batch.stream())
+    batch.run(0, W)
+    batch.synchronize()
+    props = torch.cuda.get_device_properties(local)
+    try:
+        bus = "%08X:%02X:%02X.0" % (props.pci_domain_id, props.pci_bus_id, props.pci_device_id)
+    except AttributeError:
+        bus = None
+    clocks = ClockSampler(bus)
+    clocks.start()
+    time.sleep(0.1)
+    barrier(world)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    batch.run(W, K)
+    e1.record(stream)
+    e1.synchronize()
+    batch.synchronize()
+    barrier(world)
+    clk = clocks.stop()
+    ms = max_over_ranks(e0.elapsed_time(e1), world)
+    total_cells = sum(cells_all)
+    value = total_cells * K / (ms / 1e3) / 1e9
+    peak, peak_kind = measured_peak()
+    alg = 120 * n_int + 276 * n_pml                 # this rank's bytes per step
+    achieved = alg / (ms / K / 1e3) / 1e9
+    roof = {"bound": "hbm", "kernel": "batch step (all models' velocity + stress kernels, overlapped)",
+            "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
+            "traffic": None, "alg_bytes_per_launch": alg, "avg_launch_ms": ms / K}
+    launches = batch.run_launches(K)
+
+    # end to end: media upload from host arrays, K batched steps, all traces read back
+    e2e = None
+    if not args.no_e2e:
+        for s in models:
+            s.reset()
+        torch.cuda.synchronize()
+        barrier(world)
+        t0 = time.perf_counter()
+        for s, (b, lam, mu, _) in zip(models, media):
+            s.set_medium(b, lam, mu)
+        batch.run(0, K)
+        batch.synchronize()
+        for s in models:
+            s.traces()
+        secs = max_over_ranks(time.perf_counter() - t0, world)
+        h2d = sum(3 * m[0].size * 4 for m in media) / K
+        d2h = sum(m[3] * s.nt * 4 for m, s in zip(media, models)) / K
+        e2e = {"value": total_cells * K / secs / 1e9, "unit": "Gcell/s", "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": d2h, "steps": K,
+               "note": "per model: sgfd_set_medium from host arrays; sgfd_batch_run of K steps; sgfd_get_traces "
+                       "of every model; wall clock, max over ranks"}
+    batch.close()
+    for s in models:
+        s.close()
+    result = {
+        "metric": "Gcell-updates/s", "value": value, "unit": "Gcell/s", "n_gpus": world, "steps": K,
+        "warmup": W, "ms_per_step": ms / K, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "batch32", "models": len(specs), "computed_cells": total_cells,
+                   "models_this_rank": len(mine), "interior_cells_rank0": n_int, "pml_cells_rank0": n_pml,
+                   "arith": "fast", "parallelism": f"replicas{world} (models dealt by cells)",
+                   "autotune": tunings or "off",
+                   "l2": "inputs larger than L2 (%.1f GB of wavefields)" % (sum(cells_all) * 36 / 1e9)},
+        "roofline": roof, "clocks": clk, "gpu_launches": launches, "e2e": e2e,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        w0 = wl.layered_model(specs[0])
+        rate, threads, secs = cpu_oracle_rate(w0, args.cpu_steps)
+        result["cpu_baseline"] = {
+            "value": rate, "unit": "Gcell/s", "cores": threads, "kind": "port",
+            "sample": f"{args.cpu_steps} time steps of batch model 0 ({w0.name}, {secs:.1f} s) after 1 untimed "
+                      f"step; C++ oracle of the reference kernels, FP32, flush-to-zero, OpenMP {threads} threads"}
     if rank == 0:
         print(json.dumps(result), flush=True)
     if world > 1:

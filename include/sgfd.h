@@ -77,6 +77,13 @@ typedef enum sgfd_medium_id {
  *          sqrt((lambda+2mu)*b); the classic quadratic profile.
  *  REFCPU: d = log10(1/R)*3.4*Vconst/(p*dx)*(k/p)^2 with a constant velocity
  *          (3DCPUwithPML_3DArray_GridIncludePMLandOrder/ElasticMacro.h:18-23). */
+/* Regions summed by sgfd_energy. */
+typedef enum sgfd_region {
+    SGFD_REGION_COMPUTED = 0,   /* interior + PML shell */
+    SGFD_REGION_INTERIOR = 1,
+    SGFD_REGION_PML = 2
+} sgfd_region;
+
 typedef enum sgfd_damping {
     SGFD_DAMP_REFGPU = 0,
     SGFD_DAMP_LOGR = 1,
@@ -220,10 +227,98 @@ int sgfd_profile(sgfd_solver *h, int32_t it0, int32_t nsteps, float *ms_velocity
  * re-read fewer warm-up planes; smaller ones give more CTAs to balance. */
 int sgfd_set_zchunk(sgfd_solver *h, int32_t planes);
 
+/* Switch the kernel family of an existing handle (SGFD_KERNEL_AUTO means
+ * z-marching).  z-marching is available when the handle was created with
+ * AUTO or ZMARCH on a supported grid; otherwise SGFD_ERR_UNSUPPORTED.
+ * Results are bit-identical across families. */
+int sgfd_set_kernel(sgfd_solver *h, int32_t kernel);
+
 /* z-marching kernels: tile height in cells (8 or 16; one or two cells per
  * thread) and planes per z chunk (0 = automatic).  No effect on the simple
  * family.  Results do not depend on the tiling. */
 int sgfd_set_tiling(sgfd_solver *h, int32_t tile_rows, int32_t zchunk);
+
+/* ---- autotuning and batches (no counterpart in the reference, which runs
+ * one model with a fixed launch shape: OPT/main.cu's GPUDim) ---- */
+
+/* Result of sgfd_autotune: the fastest candidate and its measured time. */
+typedef struct sgfd_tuning {
+    int32_t kernel;       /* SGFD_KERNEL_SIMPLE or SGFD_KERNEL_ZMARCH */
+    int32_t tile_rows;    /* z-marching tile height: 8 or 16 */
+    int32_t zchunk;       /* planes per z chunk; 0 = automatic */
+    int32_t candidates;   /* candidates timed */
+    float ms_per_step;    /* mean step time of the chosen candidate */
+    int32_t reserved[3];
+} sgfd_tuning;
+
+/* Time the launch-shape candidates (kernel family = halo staging through
+ * TMA + shared memory or through the caches; tile height 8/16; z chunk of
+ * automatic, 16, 32, 64 planes) over probe_steps steps each (0 = 4), keep the
+ * fastest, then zero the wavefields, splits and traces (as sgfd_reset), since
+ * timing steps the model.  Call it after sgfd_set_medium and before the run.
+ * Results never depend on the choice (bit-identical). */
+int sgfd_autotune(sgfd_solver *h, int32_t probe_steps, sgfd_tuning *out);
+
+/* A batch advances several independent models (uneven sizes allowed, all on
+ * one device) together: one CUDA graph per 16 steps holds every model's
+ * kernels in parallel branches, so small models fill the GPU side by side.
+ * Each model keeps its own medium, source, receivers and wavelet (set through
+ * its handle before the run); the batch only launches.  The models stay
+ * owned by the caller and must outlive the batch. */
+typedef struct sgfd_batch sgfd_batch;
+int sgfd_batch_create(sgfd_solver *const *models, int32_t n, sgfd_batch **out);
+void sgfd_batch_destroy(sgfd_batch *b);
+const char *sgfd_batch_last_error(const sgfd_batch *b);
+/* Steps it0 .. it0+nsteps-1 of every model, from each model's wavelet.
+ * Ordered after work already queued on the models' streams, and work queued
+ * on them afterwards waits for it; asynchronous otherwise. */
+int sgfd_batch_run(sgfd_batch *b, int32_t it0, int32_t nsteps);
+int sgfd_batch_synchronize(sgfd_batch *b);
+/* The batch's launch stream (a cudaStream_t), for timing with events. */
+void *sgfd_batch_stream(sgfd_batch *b);
+/* Kernel launches one sgfd_batch_run(b, *, nsteps) issues. */
+int sgfd_batch_run_launches(const sgfd_batch *b, int32_t nsteps);
+
+/* FP64 energy audit (no counterpart in the reference): kinetic
+ * 1/2 rho |v|^2 and strain energy (s:s - lambda/(3 lambda + 2 mu) tr(s)^2) /
+ * (4 mu) of the current wavefield, fields and medium taken at the same cell,
+ * summed in FP64 on the GPU over the computed cells of `region` and
+ * multiplied by dx*dy*dz.  Waits for the handle's queued steps.  Energy left
+ * in SGFD_REGION_INTERIOR after the direct wave has left the interior is what
+ * the absorbing boundary reflected. */
+int sgfd_energy(sgfd_solver *h, int32_t region, double *kinetic, double *strain);
+
+/* ---- checkpoint / resume (no counterpart in the reference, which writes
+ * only text slices: OPT/ElasticWaveEquation.cu:843-948) ----
+ * A checkpoint holds the dynamic state: the 9 wavefields, the 24 PML split
+ * fields, the traces and the caller's next step index it_next.  The static
+ * inputs (medium, source, receivers, wavelet) are not in it: a resuming
+ * handle is created with the same configuration, given the same inputs, then
+ * loads the checkpoint and continues with step it_next.  Layout: a 128-byte
+ * header (magic "SGFDCKP1", version 1, grid, pml, receivers x steps, it_next,
+ * physics, payload size, 64-bit checksum), then the payload: 9 x nx*ny*nz
+ * float32 fields (x fastest), 24 x npml float32 splits, nt x nrec float32
+ * traces (time-major).  Loading checks the grid, physics and checksum; a
+ * checksum or length failure zeroes the state (as sgfd_reset) and returns
+ * SGFD_ERR_INVALID.  All four wait for the handle's queued steps. */
+int sgfd_checkpoint_bytes(sgfd_solver *h, int64_t *bytes);
+int sgfd_checkpoint_save(sgfd_solver *h, int32_t it_next, void *buf, int64_t bytes);
+int sgfd_checkpoint_load(sgfd_solver *h, const void *buf, int64_t bytes, int32_t *it_next);
+int sgfd_checkpoint_write(sgfd_solver *h, int32_t it_next, const char *path);
+int sgfd_checkpoint_read(sgfd_solver *h, const char *path, int32_t *it_next);
+
+/* Multi-component station files, extending the reference's single txx
+ * stationData.txt (OPT/ElasticWaveEquation.cu:950-960):
+ *   <prefix>_receivers.txt   one line per receiver: index x y z component column
+ *   <prefix>_<comp>.txt      for each recorded component (vx vy vz txx tyy tzz
+ *                            txy txz tyz): nsteps lines, one column per
+ *                            receiver of that component in receiver order,
+ *                            values printed as %g (the reference's ofstream
+ *                            format)
+ *   <prefix>_<comp>.bin      with binary != 0: int32 nsteps, int32 ncols, then
+ *                            float32 [nsteps][ncols]
+ * nsteps = 0 writes all nt steps of sgfd_set_receivers. */
+int sgfd_write_stations(sgfd_solver *h, const char *prefix, int32_t nsteps, int32_t binary);
 
 /* Counts for roofline accounting: computed cells that are interior / PML. */
 int sgfd_cell_counts(const sgfd_solver *h, int64_t *n_interior, int64_t *n_pml);

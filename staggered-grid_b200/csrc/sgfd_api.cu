@@ -64,6 +64,24 @@ int check_device_error(sgfd_solver *h) {
     return SGFD_OK;
 }
 
+cudaError_t dispatch_on(sgfd_solver *h, const SourceRec &sr, cudaStream_t s, int it, float value,
+                        bool use_wavelet, cudaEvent_t *ev) {
+    if (h->kernel == SGFD_KERNEL_ZMARCH)
+        return zmarch_step(h->m, h->ph, sr, h->zg, h->vm, h->sm, it, value, use_wavelet, s, ev);
+    return simple_step(h->m, h->ph, sr, it, value, use_wavelet, s, ev);
+}
+
+void graph_key(const sgfd_solver *h, GraphKey *k) {
+    std::memset(static_cast<void *>(k), 0, sizeof *k);
+    std::memcpy(static_cast<void *>(&k->m), &h->m, sizeof h->m);
+    std::memcpy(static_cast<void *>(&k->ph), &h->ph, sizeof h->ph);
+    std::memcpy(static_cast<void *>(&k->sr), &h->sr, sizeof h->sr);
+    std::memcpy(static_cast<void *>(&k->zg), &h->zg, sizeof h->zg);
+    std::memcpy(static_cast<void *>(&k->vm), &h->vm, sizeof h->vm);
+    std::memcpy(static_cast<void *>(&k->sm), &h->sm, sizeof h->sm);
+    k->kernel = h->kernel;
+}
+
 }  // namespace sgfd
 
 namespace {
@@ -102,26 +120,8 @@ void set_physics(sgfd_solver *h) {
     }
 }
 
-cudaError_t dispatch_on(sgfd_solver *h, const SourceRec &sr, cudaStream_t s, int it, float value,
-                        bool use_wavelet, cudaEvent_t *ev) {
-    if (h->kernel == SGFD_KERNEL_ZMARCH)
-        return zmarch_step(h->m, h->ph, sr, h->zg, h->vm, h->sm, it, value, use_wavelet, s, ev);
-    return simple_step(h->m, h->ph, sr, it, value, use_wavelet, s, ev);
-}
-
 cudaError_t dispatch_step(sgfd_solver *h, int it, float value, bool use_wavelet, cudaEvent_t *ev) {
     return dispatch_on(h, h->sr, h->stream, it, value, use_wavelet, ev);
-}
-
-void graph_key(const sgfd_solver *h, GraphKey *k) {
-    std::memset(static_cast<void *>(k), 0, sizeof *k);
-    std::memcpy(static_cast<void *>(&k->m), &h->m, sizeof h->m);
-    std::memcpy(static_cast<void *>(&k->ph), &h->ph, sizeof h->ph);
-    std::memcpy(static_cast<void *>(&k->sr), &h->sr, sizeof h->sr);
-    std::memcpy(static_cast<void *>(&k->zg), &h->zg, sizeof h->zg);
-    std::memcpy(static_cast<void *>(&k->vm), &h->vm, sizeof h->vm);
-    std::memcpy(static_cast<void *>(&k->sm), &h->sm, sizeof h->sm);
-    k->kernel = h->kernel;
 }
 
 void release_graph(sgfd_solver *h) {
@@ -387,6 +387,7 @@ void sgfd_destroy(sgfd_solver *h) {
     cudaFree(h->zrec_list);
     cudaFree(h->zrec_idx);
     cudaFree(h->dev_err);
+    cudaFree(h->audit);
     release_graph(h);
     cudaFree(h->step_ctr);
     if (h->cap_stream) cudaStreamDestroy(h->cap_stream);
@@ -476,7 +477,7 @@ int sgfd_set_receivers(sgfd_solver *h, int32_t n, const int32_t *xyz, const int3
     h->sr.rec = h->rec;
     h->sr.traces = h->traces;
     h->rec_host = host;
-    if (h->kernel == SGFD_KERNEL_ZMARCH) return upload_zrec(h, host);
+    if (h->dev_err) return upload_zrec(h, host);   // z-march receiver lists, kept current while prepared
     return SGFD_OK;
 }
 
@@ -564,7 +565,21 @@ int sgfd_set_zchunk(sgfd_solver *h, int32_t planes) {
     if (r) return r;
     if (planes < 0) return fail(h, SGFD_ERR_INVALID, "negative chunk");
     h->zchunk_req = planes;
-    if (h->kernel == SGFD_KERNEL_ZMARCH) set_zchunks(h);
+    if (h->dev_err) set_zchunks(h);
+    return SGFD_OK;
+}
+
+int sgfd_set_kernel(sgfd_solver *h, int32_t kernel) {
+    int r = check_handle(h);
+    if (r) return r;
+    if (kernel != SGFD_KERNEL_AUTO && kernel != SGFD_KERNEL_SIMPLE && kernel != SGFD_KERNEL_ZMARCH)
+        return fail(h, SGFD_ERR_INVALID, "bad kernel family %d", kernel);
+    const int want = kernel == SGFD_KERNEL_SIMPLE ? SGFD_KERNEL_SIMPLE : SGFD_KERNEL_ZMARCH;
+    if (want == SGFD_KERNEL_ZMARCH && !h->dev_err)
+        return fail(h, SGFD_ERR_UNSUPPORTED, "z-marching kernels are not prepared for this handle "
+                                             "(created with SGFD_KERNEL_SIMPLE, or the grid is not supported)");
+    SG_CUDA(h, cudaStreamSynchronize(h->stream), "synchronise before switching kernels");
+    h->kernel = want;
     return SGFD_OK;
 }
 
@@ -573,7 +588,7 @@ int sgfd_set_tiling(sgfd_solver *h, int32_t tile_rows, int32_t zchunk) {
     if (r) return r;
     if (tile_rows != 8 && tile_rows != 16) return fail(h, SGFD_ERR_INVALID, "tile rows must be 8 or 16");
     if (zchunk < 0) return fail(h, SGFD_ERR_INVALID, "negative chunk");
-    if (h->kernel != SGFD_KERNEL_ZMARCH) return SGFD_OK;   // the simple family has no tiling
+    if (!h->dev_err) return SGFD_OK;   // no z-marching kernels prepared: nothing to tile
     SG_CUDA(h, cudaStreamSynchronize(h->stream), "synchronise before re-tiling");
     const int cells = tile_rows / 8;
     if (cells != h->zg.cells) {
@@ -682,6 +697,29 @@ int sgfd_get_medium(sgfd_solver *h, int32_t which, float *out) {
                      : which == SGFD_MU ? h->m.mu : nullptr;
     if (!src) return fail(h, SGFD_ERR_INVALID, "bad medium id %d", which);
     return download(h, src, out);
+}
+
+int sgfd_energy(sgfd_solver *h, int32_t region, double *kinetic, double *strain) {
+    int r = check_handle(h);
+    if (r) return r;
+    if (region < SGFD_REGION_COMPUTED || region > SGFD_REGION_PML)
+        return fail(h, SGFD_ERR_INVALID, "bad region %d", region);
+    if (!h->audit) {
+        int sms = 0;
+        SG_CUDA(h, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device), "SM count");
+        h->audit_blocks = energy_blocks(sms);
+        SG_CUDA(h, cudaMalloc(&h->audit, (size_t)(2 * h->audit_blocks + 2) * sizeof(double)), "audit scratch");
+    }
+    double *out = h->audit + 2 * h->audit_blocks;
+    SG_CUDA(h, launch_energy(h->m, h->ph, region, h->audit, h->audit_blocks, out, h->stream), "energy audit");
+    double res[2];
+    SG_CUDA(h, cudaMemcpyAsync(res, out, sizeof res, cudaMemcpyDeviceToHost, h->stream), "energy download");
+    SG_CUDA(h, cudaStreamSynchronize(h->stream), "energy download");
+    r = check_device_error(h);
+    if (r) return r;
+    if (kinetic) *kinetic = res[0];
+    if (strain) *strain = res[1];
+    return SGFD_OK;
 }
 
 // Ricker wavelet of the reference (OPT/ElasticWaveEquation.cu:184-189): the

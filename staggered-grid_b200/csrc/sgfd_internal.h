@@ -166,6 +166,11 @@ int simple_launches_per_step(const SourceRec &sr);
 
 // medium post-processing: rmu = 1/mu over the padded arrays.
 cudaError_t launch_reciprocal(float *rmu, const float *mu, int64_t n, cudaStream_t s);
+// FP64 energy audit (kernels_audit.cu): partials holds 2 doubles per block,
+// out 2 doubles (kinetic, strain).
+int energy_blocks(int num_sms);
+cudaError_t launch_energy(const Model &m, const Physics &ph, int region, double *partials, int nblocks,
+                          double *out, cudaStream_t s);
 // *ctr = value, or *ctr += value when add is set.
 cudaError_t launch_counter(int *ctr, int value, bool add, cudaStream_t s);
 

@@ -57,6 +57,9 @@ struct sgfd_solver {
     cudaGraphExec_t graph = nullptr;
     int *step_ctr = nullptr;      // device step counter read by the replayed kernels
     sgfd::GraphKey graph_key{};   // launch parameters the graph was captured with
+    // energy audit scratch: 2 doubles per partial block, then the 2 results
+    double *audit = nullptr;
+    int audit_blocks = 0;
     std::string err;
 };
 
@@ -70,6 +73,13 @@ int cuda_fail(sgfd_solver *h, cudaError_t e, const char *what);
 int check_handle(sgfd_solver *h);
 // Read and clear the kernels' device error flag.
 int check_device_error(sgfd_solver *h);
+
+// Launch one step of h's kernels on stream s with the given receiver /
+// source record (h->sr, or a copy whose it_dev points at a step counter).
+cudaError_t dispatch_on(sgfd_solver *h, const SourceRec &sr, cudaStream_t s, int it, float value,
+                        bool use_wavelet, cudaEvent_t *ev);
+// Byte image of everything a captured step passes to h's kernels.
+void graph_key(const sgfd_solver *h, GraphKey *k);
 
 inline size_t round_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 

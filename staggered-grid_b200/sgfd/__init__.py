@@ -18,6 +18,7 @@ Typical use (mirrors the reference driver 3DGPUwithPML_1DArraySingleGPU_concise/
 from __future__ import annotations
 
 import ctypes
+import struct
 import os
 
 import numpy as np
@@ -33,6 +34,7 @@ QUIRKS_REF, QUIRKS_FIXED = range(2)
 STORE_F32, STORE_BF16, STORE_F16 = range(3)
 KERNEL_AUTO, KERNEL_SIMPLE, KERNEL_ZMARCH = range(3)
 ARITH_REF, ARITH_FAST = range(2)
+REGION_COMPUTED, REGION_INTERIOR, REGION_PML = range(3)
 
 # sgfd_status
 OK, ERR_INVALID, ERR_ALLOC, ERR_CUDA, ERR_STATE, ERR_UNSUPPORTED, ERR_NO_DEVICE, ERR_NONFINITE = range(8)
@@ -57,6 +59,12 @@ class SgfdError(RuntimeError):
     def __init__(self, code: int, msg: str):
         super().__init__(f"sgfd error {code}: {msg}")
         self.code = code
+
+
+class Tuning(ctypes.Structure):
+    """sgfd_tuning: the launch shape sgfd_autotune picked."""
+    _fields_ = [("kernel", ctypes.c_int32), ("tile_rows", ctypes.c_int32), ("zchunk", ctypes.c_int32),
+                ("candidates", ctypes.c_int32), ("ms_per_step", ctypes.c_float), ("reserved", ctypes.c_int32 * 3)]
 
 
 _lib = None
@@ -104,6 +112,22 @@ def lib() -> ctypes.CDLL:
         "sgfd_run_launches": (ctypes.c_int, [vp, ctypes.c_int32, ctypes.c_int32]),
         "sgfd_prepare_run": (ctypes.c_int, [vp]),
         "sgfd_kernel_name": (ctypes.c_char_p, [vp]),
+        "sgfd_checkpoint_bytes": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_int64)]),
+        "sgfd_checkpoint_save": (ctypes.c_int, [vp, i32, vp, ctypes.c_int64]),
+        "sgfd_checkpoint_load": (ctypes.c_int, [vp, vp, ctypes.c_int64, ip]),
+        "sgfd_checkpoint_write": (ctypes.c_int, [vp, i32, ctypes.c_char_p]),
+        "sgfd_checkpoint_read": (ctypes.c_int, [vp, ctypes.c_char_p, ip]),
+        "sgfd_write_stations": (ctypes.c_int, [vp, ctypes.c_char_p, i32, i32]),
+        "sgfd_set_kernel": (ctypes.c_int, [vp, i32]),
+        "sgfd_autotune": (ctypes.c_int, [vp, i32, ctypes.POINTER(Tuning)]),
+        "sgfd_batch_create": (ctypes.c_int, [ctypes.POINTER(vp), i32, ctypes.POINTER(vp)]),
+        "sgfd_batch_destroy": (None, [vp]),
+        "sgfd_batch_last_error": (ctypes.c_char_p, [vp]),
+        "sgfd_batch_run": (ctypes.c_int, [vp, i32, i32]),
+        "sgfd_batch_synchronize": (ctypes.c_int, [vp]),
+        "sgfd_batch_stream": (vp, [vp]),
+        "sgfd_batch_run_launches": (ctypes.c_int, [vp, i32]),
+        "sgfd_energy": (ctypes.c_int, [vp, i32, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
     }
     for name, (res, args) in sigs.items():
         fn = getattr(L, name)
@@ -275,3 +299,126 @@ class Solver:
 
     def kernel_name(self) -> str:
         return lib().sgfd_kernel_name(self.h).decode()
+
+    def set_kernel(self, kernel: int):
+        self._check(lib().sgfd_set_kernel(self.h, kernel))
+
+    def autotune(self, probe_steps: int = 0) -> Tuning:
+        t = Tuning()
+        self._check(lib().sgfd_autotune(self.h, probe_steps, ctypes.byref(t)))
+        return t
+
+    def energy(self, region: int = 0) -> tuple[float, float]:
+        """(kinetic, strain) energy of the current wavefield over a region, FP64 on the GPU."""
+        k, e = ctypes.c_double(), ctypes.c_double()
+        self._check(lib().sgfd_energy(self.h, region, ctypes.byref(k), ctypes.byref(e)))
+        return k.value, e.value
+
+    # ---- checkpoint / resume and station files ----
+    def checkpoint_bytes(self) -> int:
+        n = ctypes.c_int64()
+        self._check(lib().sgfd_checkpoint_bytes(self.h, ctypes.byref(n)))
+        return n.value
+
+    def checkpoint(self, it_next: int, path: str | None = None) -> bytes | None:
+        """Save the dynamic state; to `path` when given, else return it as bytes."""
+        if path is not None:
+            self._check(lib().sgfd_checkpoint_write(self.h, it_next, os.fsencode(path)))
+            return None
+        buf = ctypes.create_string_buffer(self.checkpoint_bytes())
+        self._check(lib().sgfd_checkpoint_save(self.h, it_next, buf, len(buf)))
+        return buf.raw
+
+    def restore(self, src: str | bytes) -> int:
+        """Load a checkpoint (a path or the bytes of checkpoint()); returns it_next."""
+        it = ctypes.c_int32()
+        if isinstance(src, (bytes, bytearray)):
+            buf = ctypes.create_string_buffer(bytes(src), len(src))
+            self._check(lib().sgfd_checkpoint_load(self.h, buf, len(src), ctypes.byref(it)))
+        else:
+            self._check(lib().sgfd_checkpoint_read(self.h, os.fsencode(src), ctypes.byref(it)))
+        return it.value
+
+    def write_stations(self, prefix: str, nsteps: int = 0, binary: bool = True):
+        self._check(lib().sgfd_write_stations(self.h, os.fsencode(prefix), nsteps, 1 if binary else 0))
+
+
+CHECKPOINT_MAGIC = b"SGFDCKP1"
+_CKPT_HEADER = struct.Struct("<8sII4i3i3i4fqQQ32x")
+
+
+def checkpoint_header(data: bytes) -> dict:
+    """Decode the 128-byte header of a checkpoint written by Solver.checkpoint."""
+    if len(data) < _CKPT_HEADER.size:
+        raise ValueError("shorter than a checkpoint header")
+    v = _CKPT_HEADER.unpack_from(data)
+    if v[0] != CHECKPOINT_MAGIC:
+        raise ValueError("not an sgfd checkpoint")
+    keys = ("magic", "version", "header_bytes", "nx", "ny", "nz", "pml", "nrec", "nt", "it_next",
+            "quirks", "damping", "arith", "dt", "dx", "dy", "dz", "npml", "payload_bytes", "checksum")
+    return dict(zip(keys, v))
+
+
+def checkpoint_checksum(payload: bytes) -> int:
+    """The header's payload checksum: 4 FNV-1a lanes over 64-bit words, a
+    byte-wise tail folded into lane 0, then lanes 1..3 folded in."""
+    P, M = 0x100000001B3, (1 << 64) - 1
+    lanes = [0xCBF29CE484222325, 0x84222325CBF29CE4, 0x9CE484222325CBF2, 0x2325CBF29CE48422]
+    whole = len(payload) // 32 * 32
+    w = np.frombuffer(payload[:whole], dtype="<u8").reshape(-1, 4)
+    for row in w.tolist():
+        for k in range(4):
+            lanes[k] = ((lanes[k] ^ row[k]) * P) & M
+    h = lanes[0]
+    for c in payload[whole:]:
+        h = ((h ^ c) * P) & M
+    for k in range(1, 4):
+        h = ((h ^ lanes[k]) * P) & M
+    return h
+
+
+class Batch:
+    """Several Solver models advanced together (sgfd_batch_*): one CUDA graph per
+    16 steps with every model's kernels in parallel branches."""
+
+    def __init__(self, models):
+        self.models = list(models)
+        arr = (ctypes.c_void_p * len(self.models))(*[m.h for m in self.models])
+        h = ctypes.c_void_p()
+        rc = lib().sgfd_batch_create(arr, len(self.models), ctypes.byref(h))
+        if rc != OK:
+            raise SgfdError(rc, lib().sgfd_global_error().decode())
+        self.h = h
+
+    def _check(self, rc: int):
+        if rc != OK:
+            raise SgfdError(rc, lib().sgfd_batch_last_error(self.h).decode())
+
+    def run(self, it0: int, nsteps: int):
+        self._check(lib().sgfd_batch_run(self.h, it0, nsteps))
+
+    def synchronize(self):
+        self._check(lib().sgfd_batch_synchronize(self.h))
+
+    def stream(self) -> int:
+        return lib().sgfd_batch_stream(self.h) or 0
+
+    def run_launches(self, nsteps: int) -> int:
+        return lib().sgfd_batch_run_launches(self.h, nsteps)
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().sgfd_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()

@@ -11,6 +11,10 @@ included on every side).
   "plain method, CPU-runnable": 100^3 + 20-cell PML, 101 vx/vz receivers).
 * `random_cube()` — random-medium cube (configuration "plain method on GPU":
   344^3 + 20-cell PML, 64x64 receivers recording vx, vy, vz).
+* `batch_specs()` / `layered_model()` — the batched configuration: 32
+  models of uneven cubic interiors (96^3 .. 256^3, seeded), 20-cell PML,
+  3-6 horizontal layers each, one Ricker source and 128 receivers per model.
+* `balance()` — greedy assignment of models to ranks by computed cells.
 * `gaussian_random_field()` — seeded Gaussian-correlated perturbation used
   for the random media; it stands in for the reference's MATLAB generator
   randomMedium/RandomMedia_3_d.m:1-103, which uses another spectrum.
@@ -173,3 +177,96 @@ def small_random_case(nx=37, ny=41, nz=45, pml=6, nt=60, seed=7, quirks=QUIRKS_R
     w64 = _ricker_t0_64(f0, dt, 1.2 / f0, nt)
     return Workload(f"small_{nx}x{ny}x{nz}_pml{pml}", _cfg((nx, ny, nz), pml, dt, d, damping, quirks),
                     b, lam, mu, src, xyz, comp, nt, w64.astype(np.float32), w64)
+
+
+# Largest layer vp kept stable at dt = 1 ms, dx = 10 m: the Courant number
+# vp dt / dx * sqrt(3) * sum|c_i| (sum|c_i| = 1.316689 for the 10th-order
+# coefficients) must stay below 1, i.e. vp < 4385 m/s.  The batched
+# configuration draws layer vp up to 4500 m/s, which would blow up; draws
+# above the cap are clipped to it.
+VP_CFL_CAP = 4380.0
+
+
+@dataclasses.dataclass
+class LayeredSpec:
+    """One model of the batched configuration, before its arrays are built."""
+    index: int
+    n_interior: int
+    pml: int
+    layer_tops: list           # GRID z index where each layer starts (first is 0)
+    vp: list                   # per layer, m/s (after the CFL cap)
+    src: tuple                 # GRID coordinates
+    f0: float
+    nt: int
+    dt: float
+    d: float
+    nrec: int
+
+    @property
+    def n(self) -> int:
+        return self.n_interior + 2 * self.pml + 2 * HALO
+
+    def computed_cells(self) -> int:
+        return (self.n - 2 * HALO) ** 3
+
+
+def batch_specs(n_models: int = 32, seed: int = 3, nt: int = 1000, dt: float = 0.001, d: float = 10.0,
+                pml: int = 20, nrec: int = 128, n_range=(96, 256), vp_range=(1800.0, 4500.0),
+                vp_cap: float = VP_CFL_CAP) -> list:
+    """Seeded specs of the batched configuration: interior edge ~ U{96..256},
+    3-6 horizontal layers with vp ~ U(1800, 4500) clipped at vp_cap, one
+    Ricker (f0 ~ U(10, 30) Hz, t0 = 1.2/f0) at a random interior cell."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    specs = []
+    for i in range(n_models):
+        ni = int(rng.integers(n_range[0], n_range[1] + 1))
+        n = ni + 2 * pml + 2 * HALO
+        nl = int(rng.integers(3, 7))
+        tops = [0] + sorted(int(t) for t in rng.choice(np.arange(HALO + pml + 1, n - HALO - pml), nl - 1,
+                                                        replace=False))
+        vp = [float(min(v, vp_cap)) for v in rng.uniform(vp_range[0], vp_range[1], nl)]
+        lo, hi = HALO + pml, n - HALO - pml
+        src = tuple(int(v) for v in rng.integers(lo, hi, 3))
+        f0 = float(rng.uniform(10.0, 30.0))
+        specs.append(LayeredSpec(i, ni, pml, tops, vp, src, f0, nt, dt, d, nrec))
+    return specs
+
+
+def layered_model(spec: LayeredSpec, quirks: int = QUIRKS_FIXED, damping: int = DAMP_LOGR) -> Workload:
+    """Arrays of one batched model: horizontal layers (vs = vp/sqrt(3),
+    rho = 310 vp^0.25, Gardner), receivers on a 16x8 grid of the plane 5 cells
+    below the top interior face recording vz."""
+    n = spec.n
+    vp_z = np.empty(n)
+    for k, top in enumerate(spec.layer_tops):
+        vp_z[top:] = spec.vp[k]
+    vs_z = vp_z / math.sqrt(3.0)
+    rho_z = 310.0 * vp_z ** 0.25
+    b_z, lam_z, mu_z = medium_from_velocity(vp_z, vs_z, rho_z)
+    shape = (n, n, n)
+    b, lam, mu = (np.ascontiguousarray(np.broadcast_to(a[:, None, None], shape)) for a in (b_z, lam_z, mu_z))
+    i0, span = HALO + spec.pml, spec.n_interior
+    nxr = 16
+    nyr = max(1, spec.nrec // nxr)
+    xs = i0 + (np.arange(nxr) * span) // nxr
+    ys = i0 + (np.arange(nyr) * span) // nyr
+    z = i0 + 5
+    xyz = np.array([(x, y, z) for y in ys for x in xs], np.int32)[:spec.nrec]
+    comp = np.full(len(xyz), VZ, np.int32)
+    w64 = _ricker_t0_64(spec.f0, spec.dt, 1.2 / spec.f0, spec.nt)
+    return Workload(f"layered{spec.index}_{spec.n_interior}^3+pml{spec.pml}",
+                    _cfg((n, n, n), spec.pml, spec.dt, spec.d, damping, quirks),
+                    b, lam, mu, spec.src, xyz, comp, spec.nt, w64.astype(np.float32), w64)
+
+
+def balance(cells, nranks: int) -> list:
+    """Greedy longest-first assignment of models to ranks: each model, largest
+    first, goes to the rank with the fewest cells so far (ties: lowest rank).
+    Returns one list of model indices per rank, each in ascending order."""
+    load = [0] * nranks
+    out = [[] for _ in range(nranks)]
+    for i in sorted(range(len(cells)), key=lambda k: (-cells[k], k)):
+        r = min(range(nranks), key=lambda q: (load[q], q))
+        out[r].append(i)
+        load[r] += cells[i]
+    return [sorted(o) for o in out]

@@ -1,0 +1,88 @@
+"""Batches of uneven models (sgfd_batch_*) and the launch-shape autotuner,
+through the C ABI: every model of a batch ends bit for bit where the same
+model run alone ends."""
+import numpy as np
+import pytest
+
+from helpers import make_solver
+import sgfd
+import sgfd.workloads as wl
+
+pytestmark = pytest.mark.gpu
+
+
+def _models():
+    return [wl.small_random_case(nx=37, ny=41, nz=45, pml=6, nt=45, seed=7),
+            wl.small_random_case(nx=52, ny=33, nz=40, pml=4, nt=45, seed=8, quirks=sgfd.QUIRKS_FIXED,
+                                 damping=sgfd.DAMP_LOGR),
+            wl.small_random_case(nx=29, ny=30, nz=31, pml=3, nt=45, seed=9, damping=sgfd.DAMP_REFCPU)]
+
+
+@pytest.mark.parametrize("split", [False, True], ids=["one_run", "split_runs"])
+def test_batch_equals_solo_runs(split):
+    ws = _models()
+    solo, members = [], []
+    try:
+        for i, w in enumerate(ws):
+            s = make_solver(w)
+            s.run(0, w.nt)
+            s.synchronize()
+            solo.append((s.traces(), [s.field(k) for k in range(9)]))
+            s.close()
+            # one member on the simple family: batches mix families
+            members.append(make_solver(w, kernel=sgfd.KERNEL_SIMPLE if i == 2 else sgfd.KERNEL_AUTO))
+        with sgfd.Batch(members) as b:
+            if split:
+                for it0, n in ((0, 20), (20, 1), (21, 24)):
+                    b.run(it0, n)
+            else:
+                b.run(0, 45)
+                assert b.run_launches(45) == 45 * sum(m.launches_per_step() for m in members) + 1 + 2
+            b.synchronize()
+            for m, (tr, fields) in zip(members, solo):
+                np.testing.assert_array_equal(m.traces(), tr)
+                for k in range(9):
+                    np.testing.assert_array_equal(m.field(k), fields[k], err_msg=sgfd.FIELD_NAMES[k])
+    finally:
+        for m in members:
+            m.close()
+
+
+def test_batch_rejects_bad_input():
+    w = _models()[0]
+    with make_solver(w) as s:
+        with pytest.raises(sgfd.SgfdError):
+            sgfd.Batch([s, s])
+        with pytest.raises(sgfd.SgfdError):
+            sgfd.Batch([])
+        with sgfd.Batch([s]) as b:
+            with pytest.raises(sgfd.SgfdError) as e:
+                b.run(0, w.nt + 5)          # beyond the wavelet
+            assert "wavelet" in str(e.value)
+
+
+def test_autotune_picks_a_candidate_and_keeps_results():
+    w = wl.small_random_case(nx=70, ny=36, nz=50, pml=8, nt=40)
+    with make_solver(w) as ref:
+        ref.run(0, w.nt)
+        ref.synchronize()
+        tr = ref.traces()
+    with make_solver(w) as s:
+        t = s.autotune(3)
+        assert t.candidates >= 2 and t.ms_per_step > 0
+        assert t.kernel in (sgfd.KERNEL_SIMPLE, sgfd.KERNEL_ZMARCH) and t.tile_rows in (8, 16)
+        assert s.kernel_name() == ("zmarch" if t.kernel == sgfd.KERNEL_ZMARCH else "simple")
+        for k in range(9):                      # timing steps were wiped
+            assert not s.field(k).any()
+        s.run(0, w.nt)
+        np.testing.assert_array_equal(s.traces(), tr)
+        # switching families by hand is also bit-identical
+        s.reset()
+        s.set_kernel(sgfd.KERNEL_SIMPLE if t.kernel == sgfd.KERNEL_ZMARCH else sgfd.KERNEL_ZMARCH)
+        s.run(0, w.nt)
+        np.testing.assert_array_equal(s.traces(), tr)
+    with make_solver(w, kernel=sgfd.KERNEL_SIMPLE) as s:
+        with pytest.raises(sgfd.SgfdError) as e:
+            s.set_kernel(sgfd.KERNEL_ZMARCH)
+        assert e.value.code == sgfd.ERR_UNSUPPORTED
+        assert s.autotune(2).kernel == sgfd.KERNEL_SIMPLE
