@@ -288,6 +288,16 @@ int sgfd_batch_run_launches(const sgfd_batch *b, int32_t nsteps);
  * the absorbing boundary reflected. */
 int sgfd_energy(sgfd_solver *h, int32_t region, double *kinetic, double *strain);
 
+/* Per-step FP64 energy audit.  With every > 0, after the stress update of
+ * each step it with it % every == 0 and it / every < nsamples, the kinetic
+ * and strain energy of `region` (as sgfd_energy) are recorded on the GPU as
+ * sample it / every; the history is zeroed here and by sgfd_reset.  Works in
+ * sgfd_step, sgfd_run (graphs included) and batches; adds two launches per
+ * step.  every = 0 switches it off. */
+int sgfd_set_audit(sgfd_solver *h, int32_t every, int32_t region, int32_t nsamples);
+/* Copy the history: out[2k] kinetic, out[2k+1] strain energy of sample k. */
+int sgfd_get_audit(sgfd_solver *h, double *out);
+
 /* ---- checkpoint / resume (no counterpart in the reference, which writes
  * only text slices: OPT/ElasticWaveEquation.cu:843-948) ----
  * A checkpoint holds the dynamic state: the 9 wavefields, the 24 PML split

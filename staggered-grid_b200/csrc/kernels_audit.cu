@@ -12,7 +12,9 @@
 //             for mu = 0, tr(s)^2 / (18 lambda)
 // both times the cell volume dx*dy*dz.  Sums run in FP64: one partial per
 // block, then one block adds the partials in a fixed order, so the result is
-// deterministic for a given launch shape.
+// deterministic for a given launch shape.  The per-step form
+// (launch_energy_step) runs after the stress update of every step and
+// records steps 0, every, 2*every, ... into a history buffer.
 #include "../../include/sgfd.h"
 #include "sgfd_internal.h"
 
@@ -43,8 +45,20 @@ __device__ __forceinline__ void block_sum2(double &a, double &b) {
     }
 }
 
-// One warp per (y, z) row of computed cells, lanes across x.
-__global__ void __launch_bounds__(kAuditThreads) k_energy_partial(Model m, int region, double *partials) {
+// Step index of a gated (per-step) audit launch, or -1 when this step is not
+// sampled.
+__device__ __forceinline__ int audit_sample(const AuditGate &gt) {
+    const int it = gt.it_dev ? gt.it_arg + *gt.it_dev : gt.it_arg;
+    if (it < 0 || it % gt.every != 0 || it / gt.every >= gt.count) return -1;
+    return it / gt.every;
+}
+
+// One warp per (y, z) row of computed cells, lanes across x.  GATED: a
+// per-step audit launch that returns at once on steps it does not sample.
+template <bool GATED>
+__global__ void __launch_bounds__(kAuditThreads) k_energy_partial(Model m, int region, double *partials,
+                                                                 AuditGate gt) {
+    if (GATED && audit_sample(gt) < 0) return;
     double ek = 0.0, es = 0.0;
     const int lane = threadIdx.x & 31;
     const int warps = gridDim.x * (kAuditThreads / 32);
@@ -76,8 +90,15 @@ __global__ void __launch_bounds__(kAuditThreads) k_energy_partial(Model m, int r
     }
 }
 
+template <bool GATED>
 __global__ void __launch_bounds__(kAuditThreads) k_energy_final(const double *partials, int nblocks, double volume,
-                                                               double *out) {
+                                                               double *out, AuditGate gt) {
+    int sample = 0;
+    if (GATED) {
+        sample = audit_sample(gt);
+        if (sample < 0) return;
+        out = gt.hist + 2 * (size_t)sample;
+    }
     double ek = 0.0, es = 0.0;
     for (int i = threadIdx.x; i < nblocks; i += kAuditThreads) {
         ek += partials[2 * i];
@@ -96,9 +117,18 @@ int energy_blocks(int num_sms) { return 8 * num_sms; }
 
 cudaError_t launch_energy(const Model &m, const Physics &ph, int region, double *partials, int nblocks,
                           double *out, cudaStream_t s) {
-    k_energy_partial<<<nblocks, kAuditThreads, 0, s>>>(m, region, partials);
+    const AuditGate none{};
+    k_energy_partial<false><<<nblocks, kAuditThreads, 0, s>>>(m, region, partials, none);
     const double volume = (double)ph.dx * (double)ph.dy * (double)ph.dz;
-    k_energy_final<<<1, kAuditThreads, 0, s>>>(partials, nblocks, volume, out);
+    k_energy_final<false><<<1, kAuditThreads, 0, s>>>(partials, nblocks, volume, out, none);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_energy_step(const Model &m, const Physics &ph, int region, double *partials, int nblocks,
+                               const AuditGate &gt, cudaStream_t s) {
+    k_energy_partial<true><<<nblocks, kAuditThreads, 0, s>>>(m, region, partials, gt);
+    const double volume = (double)ph.dx * (double)ph.dy * (double)ph.dz;
+    k_energy_final<true><<<1, kAuditThreads, 0, s>>>(partials, nblocks, volume, nullptr, gt);
     return cudaGetLastError();
 }
 

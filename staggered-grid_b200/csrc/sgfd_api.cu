@@ -66,9 +66,23 @@ int check_device_error(sgfd_solver *h) {
 
 cudaError_t dispatch_on(sgfd_solver *h, const SourceRec &sr, cudaStream_t s, int it, float value,
                         bool use_wavelet, cudaEvent_t *ev) {
-    if (h->kernel == SGFD_KERNEL_ZMARCH)
-        return zmarch_step(h->m, h->ph, sr, h->zg, h->vm, h->sm, it, value, use_wavelet, s, ev);
-    return simple_step(h->m, h->ph, sr, it, value, use_wavelet, s, ev);
+    cudaError_t e = h->kernel == SGFD_KERNEL_ZMARCH
+                        ? zmarch_step(h->m, h->ph, sr, h->zg, h->vm, h->sm, it, value, use_wavelet, s, ev)
+                        : simple_step(h->m, h->ph, sr, it, value, use_wavelet, s, ev);
+    if (e == cudaSuccess && h->audit_every > 0) {
+        const AuditGate gt{sr.it_dev, it, h->audit_every, h->audit_count, h->audit_hist};
+        e = launch_energy_step(h->m, h->ph, h->audit_region, h->audit, h->audit_blocks, gt, s);
+    }
+    return e;
+}
+
+int ensure_audit_scratch(sgfd_solver *h) {
+    if (h->audit) return SGFD_OK;
+    int sms = 0;
+    SG_CUDA(h, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device), "SM count");
+    h->audit_blocks = energy_blocks(sms);
+    SG_CUDA(h, cudaMalloc(&h->audit, (size_t)(2 * h->audit_blocks + 2) * sizeof(double)), "audit scratch");
+    return SGFD_OK;
 }
 
 void graph_key(const sgfd_solver *h, GraphKey *k) {
@@ -80,6 +94,11 @@ void graph_key(const sgfd_solver *h, GraphKey *k) {
     std::memcpy(static_cast<void *>(&k->vm), &h->vm, sizeof h->vm);
     std::memcpy(static_cast<void *>(&k->sm), &h->sm, sizeof h->sm);
     k->kernel = h->kernel;
+    k->audit_every = h->audit_every;
+    k->audit_region = h->audit_region;
+    k->audit_count = h->audit_count;
+    k->audit_hist = h->audit_hist;
+    k->audit = h->audit;
 }
 
 }  // namespace sgfd
@@ -388,6 +407,7 @@ void sgfd_destroy(sgfd_solver *h) {
     cudaFree(h->zrec_idx);
     cudaFree(h->dev_err);
     cudaFree(h->audit);
+    cudaFree(h->audit_hist);
     release_graph(h);
     cudaFree(h->step_ctr);
     if (h->cap_stream) cudaStreamDestroy(h->cap_stream);
@@ -613,6 +633,9 @@ int sgfd_reset(sgfd_solver *h) {
     SG_CUDA(h, cudaMemsetAsync(h->split, 0, (size_t)kNumSplit * m.npml * sizeof(float), h->stream), "reset splits");
     if (h->traces)
         SG_CUDA(h, cudaMemsetAsync(h->traces, 0, (size_t)h->sr.nrec * h->sr.nt * sizeof(float), h->stream), "reset traces");
+    if (h->audit_hist)
+        SG_CUDA(h, cudaMemsetAsync(h->audit_hist, 0, (size_t)h->audit_count * 2 * sizeof(double), h->stream),
+                "reset audit history");
     SG_CUDA(h, cudaStreamSynchronize(h->stream), "reset");
     return SGFD_OK;
 }
@@ -704,12 +727,8 @@ int sgfd_energy(sgfd_solver *h, int32_t region, double *kinetic, double *strain)
     if (r) return r;
     if (region < SGFD_REGION_COMPUTED || region > SGFD_REGION_PML)
         return fail(h, SGFD_ERR_INVALID, "bad region %d", region);
-    if (!h->audit) {
-        int sms = 0;
-        SG_CUDA(h, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device), "SM count");
-        h->audit_blocks = energy_blocks(sms);
-        SG_CUDA(h, cudaMalloc(&h->audit, (size_t)(2 * h->audit_blocks + 2) * sizeof(double)), "audit scratch");
-    }
+    r = ensure_audit_scratch(h);
+    if (r) return r;
     double *out = h->audit + 2 * h->audit_blocks;
     SG_CUDA(h, launch_energy(h->m, h->ph, region, h->audit, h->audit_blocks, out, h->stream), "energy audit");
     double res[2];
@@ -720,6 +739,44 @@ int sgfd_energy(sgfd_solver *h, int32_t region, double *kinetic, double *strain)
     if (kinetic) *kinetic = res[0];
     if (strain) *strain = res[1];
     return SGFD_OK;
+}
+
+int sgfd_set_audit(sgfd_solver *h, int32_t every, int32_t region, int32_t nsamples) {
+    int r = check_handle(h);
+    if (r) return r;
+    if (every < 0 || nsamples < 0) return fail(h, SGFD_ERR_INVALID, "negative audit interval or length");
+    if (region < SGFD_REGION_COMPUTED || region > SGFD_REGION_PML)
+        return fail(h, SGFD_ERR_INVALID, "bad region %d", region);
+    if (every > 0 && nsamples == 0) return fail(h, SGFD_ERR_INVALID, "an audit needs at least one sample");
+    SG_CUDA(h, cudaStreamSynchronize(h->stream), "synchronise before changing the audit");
+    if (every == 0) {
+        h->audit_every = 0;
+        return SGFD_OK;
+    }
+    r = ensure_audit_scratch(h);
+    if (r) return r;
+    if (nsamples != h->audit_count) {
+        cudaFree(h->audit_hist);
+        h->audit_hist = nullptr;
+        h->audit_count = 0;
+        SG_CUDA(h, cudaMalloc(&h->audit_hist, (size_t)nsamples * 2 * sizeof(double)), "audit history");
+        h->audit_count = nsamples;
+    }
+    SG_CUDA(h, cudaMemsetAsync(h->audit_hist, 0, (size_t)nsamples * 2 * sizeof(double), h->stream), "audit history");
+    h->audit_every = every;
+    h->audit_region = region;
+    return SGFD_OK;
+}
+
+int sgfd_get_audit(sgfd_solver *h, double *out) {
+    int r = check_handle(h);
+    if (r) return r;
+    if (!out) return fail(h, SGFD_ERR_INVALID, "null output");
+    if (h->audit_every == 0 || !h->audit_hist) return fail(h, SGFD_ERR_STATE, "no audit set (sgfd_set_audit)");
+    SG_CUDA(h, cudaMemcpyAsync(out, h->audit_hist, (size_t)h->audit_count * 2 * sizeof(double),
+                               cudaMemcpyDeviceToHost, h->stream), "audit download");
+    SG_CUDA(h, cudaStreamSynchronize(h->stream), "audit download");
+    return check_device_error(h);
 }
 
 // Ricker wavelet of the reference (OPT/ElasticWaveEquation.cu:184-189): the
@@ -750,8 +807,9 @@ int sgfd_cell_counts(const sgfd_solver *h, int64_t *n_interior, int64_t *n_pml) 
 
 int sgfd_launches_per_step(const sgfd_solver *h) {
     if (!h) return -1;
-    if (h->kernel == SGFD_KERNEL_ZMARCH) return 2;
-    return simple_launches_per_step(h->sr);
+    const int audit = h->audit_every > 0 ? 2 : 0;
+    if (h->kernel == SGFD_KERNEL_ZMARCH) return 2 + audit;
+    return simple_launches_per_step(h->sr) + audit;
 }
 
 const char *sgfd_kernel_name(const sgfd_solver *h) {

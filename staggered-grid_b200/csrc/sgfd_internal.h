@@ -171,6 +171,17 @@ cudaError_t launch_reciprocal(float *rmu, const float *mu, int64_t n, cudaStream
 int energy_blocks(int num_sms);
 cudaError_t launch_energy(const Model &m, const Physics &ph, int region, double *partials, int nblocks,
                           double *out, cudaStream_t s);
+// Per-step audit: step it = it_arg (+ *it_dev under graph replay) is sampled
+// when it % every == 0 and it / every < count; sample k goes to hist[2k..2k+1].
+struct AuditGate {
+    const int *it_dev;
+    int it_arg;
+    int every;
+    int count;
+    double *hist;
+};
+cudaError_t launch_energy_step(const Model &m, const Physics &ph, int region, double *partials, int nblocks,
+                               const AuditGate &gt, cudaStream_t s);
 // *ctr = value, or *ctr += value when add is set.
 cudaError_t launch_counter(int *ctr, int value, bool add, cudaStream_t s);
 

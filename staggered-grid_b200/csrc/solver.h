@@ -21,6 +21,8 @@ struct GraphKey {
     VelMaps vm;
     StrMaps sm;
     int kernel;
+    int audit_every, audit_region, audit_count;
+    double *audit_hist, *audit;
 };
 // Steps per captured graph; sgfd_run launches the remainder directly.
 constexpr int kGraphSteps = 16;
@@ -60,6 +62,9 @@ struct sgfd_solver {
     // energy audit scratch: 2 doubles per partial block, then the 2 results
     double *audit = nullptr;
     int audit_blocks = 0;
+    // per-step audit (sgfd_set_audit): sample k = energy after step k*every
+    int audit_every = 0, audit_region = 0, audit_count = 0;
+    double *audit_hist = nullptr;
     std::string err;
 };
 

@@ -127,6 +127,8 @@ def lib() -> ctypes.CDLL:
         "sgfd_batch_synchronize": (ctypes.c_int, [vp]),
         "sgfd_batch_stream": (vp, [vp]),
         "sgfd_batch_run_launches": (ctypes.c_int, [vp, i32]),
+        "sgfd_set_audit": (ctypes.c_int, [vp, i32, i32, i32]),
+        "sgfd_get_audit": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_double)]),
         "sgfd_energy": (ctypes.c_int, [vp, i32, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
     }
     for name, (res, args) in sigs.items():
@@ -299,6 +301,17 @@ class Solver:
 
     def kernel_name(self) -> str:
         return lib().sgfd_kernel_name(self.h).decode()
+
+    def set_audit(self, every: int, region: int = 0, nsamples: int = 0):
+        """Record the FP64 energy of `region` after every `every`-th step (0 = off)."""
+        self._check(lib().sgfd_set_audit(self.h, every, region, nsamples))
+        self.audit_samples = nsamples if every else 0
+
+    def audit(self) -> np.ndarray:
+        """(nsamples, 2) array of (kinetic, strain) energy, sample k after step k*every."""
+        out = np.zeros((self.audit_samples, 2), dtype=np.float64)
+        self._check(lib().sgfd_get_audit(self.h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double))))
+        return out
 
     def set_kernel(self, kernel: int):
         self._check(lib().sgfd_set_kernel(self.h, kernel))

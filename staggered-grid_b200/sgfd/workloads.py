@@ -15,6 +15,7 @@ included on every side).
   models of uneven cubic interiors (96^3 .. 256^3, seeded), 20-cell PML,
   3-6 horizontal layers each, one Ricker source and 128 receivers per model.
 * `balance()` — greedy assignment of models to ranks by computed cells.
+* `von_karman_random_field()` — seeded von Karman-spectrum perturbation.
 * `gaussian_random_field()` — seeded Gaussian-correlated perturbation used
   for the random media; it stands in for the reference's MATLAB generator
   randomMedium/RandomMedia_3_d.m:1-103, which uses another spectrum.
@@ -81,6 +82,30 @@ def gaussian_random_field(shape, std, corr_cells, seed):
     return f
 
 
+def von_karman_random_field(shape, std, corr_cells, hurst, seed):
+    """Zero-mean field with a von Karman spectrum, rescaled to `std`.
+
+    The 3-D von Karman power spectrum with correlation length a (cells) and
+    Hurst exponent H is P(k) ~ (1 + k^2 a^2)^-(H + 3/2) (k in radians per
+    cell).  White N(0,1) noise from numpy's PCG64(seed) is filtered in the
+    Fourier domain by sqrt(P) (periodic boundaries), then normalised to the
+    sample std.  H -> 0.5 is the exponential medium, smaller H is rougher.
+    The reference generates its media with a MATLAB script
+    (randomMedium/RandomMedia_3_d.m) that cannot run here; this is a seeded
+    restatement of the same family of spectra.
+    """
+    rng = np.random.Generator(np.random.PCG64(seed))
+    w = rng.standard_normal(size=shape)
+    spec = np.fft.rfftn(w)
+    ks = [2.0 * np.pi * np.fft.fftfreq(n) for n in shape[:-1]] + [2.0 * np.pi * np.fft.rfftfreq(shape[-1])]
+    k2 = ks[0][:, None, None] ** 2 + ks[1][None, :, None] ** 2 + ks[2][None, None, :] ** 2
+    spec *= (1.0 + k2 * corr_cells * corr_cells) ** (-(hurst + 1.5) / 2.0)
+    f = np.fft.irfftn(spec, s=shape, axes=(0, 1, 2))
+    f -= f.mean()
+    f *= std / f.std()
+    return f
+
+
 def _cfg(n3, pml, dt, d, damping, quirks, **kw):
     nx, ny, nz = n3
     c = dict(nx=nx, ny=ny, nz=nz, pml=pml, dt=dt, dx=d, dy=d, dz=d, coef=list(REF_COEF),
@@ -135,14 +160,21 @@ def plain_cube(n_interior: int = 100, pml: int = 20, nt: int = 500, dt: float = 
 
 def random_cube(n_interior: int = 344, pml: int = 20, nt: int = 2000, dt: float = 0.001, d: float = 10.0,
                 std: float = 0.05, corr_m: float = 50.0, seed: int = 2, nrec_side: int = 64,
-                src_computed=(192, 192, 40), quirks: int = QUIRKS_FIXED, damping: int = DAMP_LOGR) -> Workload:
+                src_computed=(192, 192, 40), quirks: int = QUIRKS_FIXED, damping: int = DAMP_LOGR,
+                spectrum: str = "gaussian", hurst: float = 0.3) -> Workload:
     """Background vp 3000, vs 1732, rho 2000 scaled by (1 + delta), delta a seeded
     Gaussian-correlated field (std, correlation length corr_m); Ricker 20 Hz
     explosive source; nrec_side^2 receivers on the first interior z-plane
-    recording vx, vy, vz."""
+    recording vx, vy, vz.  spectrum="von_karman" draws delta from a von Karman
+    spectrum (Hurst exponent `hurst`) instead of the Gaussian one."""
     n = n_interior + 2 * pml + 2 * HALO
     shape = (n, n, n)
-    delta = gaussian_random_field(shape, std, corr_m / d, seed)
+    if spectrum == "gaussian":
+        delta = gaussian_random_field(shape, std, corr_m / d, seed)
+    elif spectrum == "von_karman":
+        delta = von_karman_random_field(shape, std, corr_m / d, hurst, seed)
+    else:
+        raise ValueError(f"unknown spectrum {spectrum!r}")
     s = 1.0 + delta
     b, lam, mu = medium_from_velocity(3000.0 * s, 1732.0 * s, 2000.0 * s)
     del delta, s

@@ -90,3 +90,26 @@ def test_energy_conservation_and_boundary_reflection(damping):
     print(f"damping {damping}: reflected energy fraction pml10 {refl10:.3e}, pml3 {refl3:.3e}")
     assert refl10 < 2e-2
     assert refl3 > refl10
+
+
+@pytest.mark.parametrize("kern", [sgfd.KERNEL_SIMPLE, sgfd.KERNEL_ZMARCH], ids=["simple", "zmarch"])
+def test_per_step_audit_matches_on_demand_energy(kern):
+    """sgfd_set_audit records, inside sgfd_run (graph replays and direct
+    launches alike), exactly what sgfd_energy returns after the same step."""
+    w = wl.small_random_case(nt=60)
+    every, ns = 7, 9                        # samples after steps 0, 7, ..., 56
+    with make_solver(w, kernel=kern) as a:
+        a.set_audit(every, sgfd.REGION_INTERIOR, ns)
+        assert a.launches_per_step() == (2 if kern == sgfd.KERNEL_ZMARCH else 5) + 2
+        a.run(0, w.nt)
+        hist = a.audit()
+        with make_solver(w, kernel=kern) as b:
+            done = 0
+            for k in range(ns):
+                b.run(done, k * every + 1 - done, graph=False)
+                done = k * every + 1
+                assert tuple(hist[k]) == b.energy(sgfd.REGION_INTERIOR), k
+        a.reset()
+        assert not a.audit().any()
+        a.set_audit(0)
+        assert a.launches_per_step() == (2 if kern == sgfd.KERNEL_ZMARCH else 5)

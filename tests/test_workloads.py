@@ -50,3 +50,21 @@ def test_balance_is_a_partition_within_one_model_of_even():
         loads = [sum(cells[i] for i in p) for p in parts]
         assert max(loads) - min(loads) <= max(cells)
     assert wl.balance([5, 5], 4) == [[0], [1], [], []]
+
+
+def test_random_fields_are_seeded_normalised_and_ordered_by_roughness():
+    shape = (32, 40, 48)
+    g = wl.gaussian_random_field(shape, 0.05, 5.0, 2)
+    assert np.array_equal(g, wl.gaussian_random_field(shape, 0.05, 5.0, 2))
+    rough = wl.von_karman_random_field(shape, 0.05, 5.0, 0.1, 2)
+    smooth = wl.von_karman_random_field(shape, 0.05, 5.0, 1.0, 2)
+    for f in (g, rough, smooth):
+        assert abs(f.mean()) < 1e-12 and abs(f.std() - 0.05) < 1e-12 and f.shape == shape
+    assert np.array_equal(rough, wl.von_karman_random_field(shape, 0.05, 5.0, 0.1, 2))
+    grad = lambda f: float(np.mean(np.diff(f, axis=2) ** 2))
+    assert grad(rough) > grad(smooth)
+    # a longer correlation length gives a smoother field
+    assert grad(wl.von_karman_random_field(shape, 0.05, 10.0, 0.5, 3)) < grad(
+        wl.von_karman_random_field(shape, 0.05, 2.0, 0.5, 3))
+    w = wl.random_cube(n_interior=20, pml=4, nt=10, spectrum="von_karman", nrec_side=4)
+    assert w.b.shape == (38, 38, 38)
