@@ -288,6 +288,17 @@ int sgfd_batch_run_launches(const sgfd_batch *b, int32_t nsteps);
  * the absorbing boundary reflected. */
 int sgfd_energy(sgfd_solver *h, int32_t region, double *kinetic, double *strain);
 
+/* sgfd_energy without any allocation; no counterpart in the reference.
+ * For callers that cannot let the library call cudaMalloc once they are
+ * running (device memory held by another allocator such as PyTorch's caching
+ * allocator, or a footprint fixed when the handles were created): the
+ * partial sums go to a 32 KiB device array compiled into the library, at
+ * most 2047 partial-sum blocks; nblocks = 0 uses sgfd_energy's launch shape,
+ * a larger nblocks than 2047 is rejected (SGFD_ERR_INVALID).  The first call
+ * on a device looks up that array's address; make it before any stream
+ * capture.  All calls share the array: calls that overlap on one GPU race. */
+int sgfd_energy_noalloc(sgfd_solver *h, int32_t region, int32_t nblocks, double *kinetic, double *strain);
+
 /* Per-step FP64 energy audit.  With every > 0, after the stress update of
  * each step it with it % every == 0 and it / every < nsamples, the kinetic
  * and strain energy of `region` (as sgfd_energy) are recorded on the GPU as

@@ -129,6 +129,8 @@ def lib() -> ctypes.CDLL:
         "sgfd_batch_run_launches": (ctypes.c_int, [vp, i32]),
         "sgfd_set_audit": (ctypes.c_int, [vp, i32, i32, i32]),
         "sgfd_get_audit": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_double)]),
+        "sgfd_energy_noalloc": (ctypes.c_int, [vp, i32, i32, ctypes.POINTER(ctypes.c_double),
+                                                ctypes.POINTER(ctypes.c_double)]),
         "sgfd_energy": (ctypes.c_int, [vp, i32, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
     }
     for name, (res, args) in sigs.items():
@@ -301,6 +303,14 @@ class Solver:
 
     def kernel_name(self) -> str:
         return lib().sgfd_kernel_name(self.h).decode()
+
+    def energy_noalloc(self, region: int = 0, nblocks: int = 0) -> tuple[float, float]:
+        """energy() for callers that cannot have the library allocate device
+        memory: the scratch is a fixed array inside libsgfd.so (at most 2047
+        partial-sum blocks).  Calls that overlap on one GPU race on it."""
+        k, e = ctypes.c_double(), ctypes.c_double()
+        self._check(lib().sgfd_energy_noalloc(self.h, region, nblocks, ctypes.byref(k), ctypes.byref(e)))
+        return k.value, e.value
 
     def set_audit(self, every: int, region: int = 0, nsamples: int = 0):
         """Record the FP64 energy of `region` after every `every`-th step (0 = off)."""
