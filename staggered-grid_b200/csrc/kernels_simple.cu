@@ -174,6 +174,25 @@ __global__ void k_record(Model m, SourceRec sr, int it_arg, int velocity_phase) 
     sr.traces[(int64_t)it * sr.nrec + r] = m.f[q.w][pidx(m, q.x, q.y, q.z)];
 }
 
+// Staggered shear moduli of one computed cell from the reciprocals rmu = 1/mu,
+// in the operand order of the stress update (ElasticMacro.h:110-119):
+// mxy over (x,y), (x+1,y), (x,y+1), (x+1,y+1) at z; myz over (x,y), (x,y+1)
+// at z and z+1; mxz over (x,y,z), (x+1,y,z), (x,y,z+1) and, with the
+// reference's index quirk, (x+1,y+1,z) instead of (x+1,y,z+1).
+template <bool FAST>
+__global__ void k_shear_means(Model m, int quirks, float *mxy, float *mxz, float *myz) {
+    const int cx = blockIdx.x * kBX + threadIdx.x;
+    const int cy = blockIdx.y * kBY + threadIdx.y;
+    const int cz = blockIdx.z;
+    if (cx >= m.nxc || cy >= m.nyc) return;
+    const int64_t c = pidx(m, cx + kHalo, cy + kHalo, cz + kHalo);
+    const int64_t X = 1, Y = m.px, Z = m.plane;
+    const float *r = m.rmu;
+    mxy[c] = hmean<FAST>(r[c], r[c + X], r[c + Y], r[c + X + Y]);
+    mxz[c] = hmean<FAST>(r[c], r[c + X], r[c + Z], quirks == 0 ? r[c + X + Y] : r[c + X + Z]);
+    myz[c] = hmean<FAST>(r[c], r[c + Y], r[c + Z], r[c + Y + Z]);
+}
+
 // Device step counter of a replayed CUDA graph: set before the first replay,
 // advanced by the last node of each replay.
 __global__ void k_counter(int *ctr, int value, int add) {
@@ -209,6 +228,15 @@ cudaError_t simple_step(const Model &m, const Physics &ph, const SourceRec &sr,
     else k_stress<false><<<grid, block, 0, s>>>(m, ph);
     if (ev) cudaEventRecord(ev[3], s);
     if (sr.nrec > 0) k_record<<<(sr.nrec + 127) / 128, 128, 0, s>>>(m, sr, it, 0);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_shear_means(const Model &m, const Physics &ph, float *mxy, float *mxz, float *myz,
+                               cudaStream_t s) {
+    const dim3 block(kBX, kBY);
+    const dim3 grid((m.nxc + kBX - 1) / kBX, (m.nyc + kBY - 1) / kBY, m.nzc);
+    if (ph.fast) k_shear_means<true><<<grid, block, 0, s>>>(m, ph.quirks, mxy, mxz, myz);
+    else k_shear_means<false><<<grid, block, 0, s>>>(m, ph.quirks, mxy, mxz, myz);
     return cudaGetLastError();
 }
 

@@ -46,7 +46,7 @@ namespace sgfd {
 namespace {
 
 constexpr int TX = kZTileX, NT = 256, S = 3;
-constexpr int W48 = 48, W32 = 32, W36 = 36, RW = 33;
+constexpr int W48 = 48, W32 = 32, W36 = 36;
 
 constexpr int al128(int b) { return (b + 127) / 128 * 128; }
 
@@ -73,12 +73,11 @@ struct StrL {
     static constexpr int VX = 0;                                   // 48 x (TY+10)  vx (x, y halo)
     static constexpr int VY = VX + al128(W48 * (TY + 10) * 4);     // 48 x (TY+10)  vy
     static constexpr int VZ = VY + al128(W48 * (TY + 10) * 4);     // 48 x (TY+10)  vz
-    static constexpr int MU = VZ + al128(W48 * (TY + 10) * 4);     // 36 x (TY+1)   mu at z+2
-    static constexpr int LX = MU + al128(W36 * (TY + 1) * 4);      // 32 x TY       vx at z+5
+    static constexpr int LX = VZ + al128(W48 * (TY + 10) * 4);     // 32 x TY       vx at z+5
     static constexpr int LY = LX + al128(W32 * TY * 4);            // 32 x TY       vy at z+5
     static constexpr int LZ = LY + al128(W32 * TY * 4);            // 32 x TY       vz at z+4
     static constexpr int STAGE = LZ + al128(W32 * TY * 4);
-    static constexpr uint32_t TXB = 4 * (3 * W48 * (TY + 10) + W36 * (TY + 1) + 3 * W32 * TY);
+    static constexpr uint32_t TXB = 4 * (3 * W48 * (TY + 10) + 3 * W32 * TY);
 };
 
 constexpr uint32_t kWaitCap = 2000;
@@ -282,6 +281,24 @@ k_velocity_zmarch(const __grid_constant__ VelMaps mp, const __grid_constant__ Mo
             for (int q = 0; q < 3; ++q) vnxt[c][q] = m.f[q][ci];
         }
 
+        // PML cells: splits and the medium of the damping, loaded before the
+        // stage wait so that their latency overlaps the wait and the stencil
+        float opre[CELLS][9], mupre[CELLS], lampre[CELLS];
+        if (plane_pml) {
+            const uint32_t N = (uint32_t)m.npml;
+#pragma unroll
+            for (int c = 0; c < CELLS; ++c) {
+                if (act[c] && (kx | kyc[c] | kz)) {
+                    const uint32_t ci = col[c] + (uint32_t)gz * PL;
+                    const float *sp = m.split + pml_plane_index(m, pcol[c], cz);
+#pragma unroll
+                    for (int q = 0; q < 9; ++q) opre[c][q] = sp[q * N];
+                    mupre[c] = m.mu[ci];
+                    lampre[c] = ph.damping == 1 ? m.lam[ci] : 0.f;
+                }
+            }
+        }
+
         if (!mbar_wait(&bar[s], (uint32_t)((k / S) & 1))) failed = true;
 
         // source patch of the staged copies (uniform branch)
@@ -367,7 +384,7 @@ k_velocity_zmarch(const __grid_constant__ VelMaps mp, const __grid_constant__ Mo
             } else {
                 float mx = 1.f, px = 1.f, my = 1.f, py = 1.f, mz = 1.f, pz = 1.f;
                 {
-                    const float v = damp_speed(ph, m.mu[ci], b0, ph.damping == 1 ? m.lam[ci] : 0.f);
+                    const float v = damp_speed(ph, mupre[c], b0, lampre[c]);
                     if (kx) damp_factors<FAST>(ph, 0, ph.dx, kx, m.pml, v, mx, px);
                     if (ky) damp_factors<FAST>(ph, 1, ph.dy, ky, m.pml, v, my, py);
                     if (kz) damp_factors<FAST>(ph, 2, ph.dz, kz, m.pml, v, mz, pz);
@@ -376,9 +393,7 @@ k_velocity_zmarch(const __grid_constant__ VelMaps mp, const __grid_constant__ Mo
                 const float ax = ph.dt * bx, ay = ph.dt * (ref ? bx : by), az = ph.dt * (ref ? bx : bz);
                 float *sp = m.split + pml_plane_index(m, pcol[c], cz);
                 const uint32_t N = (uint32_t)m.npml;
-                float o[9];
-#pragma unroll
-                for (int q = 0; q < 9; ++q) o[q] = sp[q * N];
+                const float *o = opre[c];
                 float a0, a1, a2;
                 a0 = split_update<FAST>(o[S_VXX], ax, xX, kx, mx, px);
                 a1 = split_update<FAST>(o[S_VXY], ax, xY, ky, my, py);
@@ -453,7 +468,6 @@ __device__ __forceinline__ void str_issue(const StrMaps &mp, unsigned char *st, 
     tma3(st + L::VX, &mp.vx, t.xd - 8, t.gy0 - 5, gz, bar);
     tma3(st + L::VY, &mp.vy, t.xd - 8, t.gy0 - 5, gz, bar);
     tma3(st + L::VZ, &mp.vz, t.xd - 8, t.gy0 - 5, gz, bar);
-    tma3(st + L::MU, &mp.mu, t.xd, t.gy0, gz + 2, bar);
     tma3(st + L::LX, &mp.vx_c, t.xd, t.gy0, gz + 5, bar);
     tma3(st + L::LY, &mp.vy_c, t.xd, t.gy0, gz + 5, bar);
     tma3(st + L::LZ, &mp.vz_c, t.xd, t.gy0, gz + 4, bar);
@@ -465,12 +479,10 @@ k_stress_zmarch(const __grid_constant__ StrMaps mp, const __grid_constant__ Mode
                   const __grid_constant__ ZGeom g, const __grid_constant__ SourceRec sr, int it_arg,
                 float src_value, int use_wavelet) {
     constexpr int TY = 8 * CELLS;
-    constexpr int RH = TY + 1;       // 1/mu tile: (x0..x0+32) x (y0..y0+TY)
     using L = StrL<TY>;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     unsigned char *smem = align_smem(smem_raw);
     __shared__ __align__(8) uint64_t bar[S];
-    __shared__ float rmu[3][RH * RW];    // ring: 1/mu of planes z, z+1, z+2
     const Tile t = make_tile<TY>(m, g);
     const int tid = threadIdx.x, lx = tid & 31, ty = tid >> 5;
     if (tid == 0) {
@@ -518,15 +530,9 @@ k_stress_zmarch(const __grid_constant__ StrMaps mp, const __grid_constant__ Mode
             qz[c][k + 1] = m.f[2][col[c] + (uint32_t)(gz0 - 5 + k) * PL];
         }
     }
-    // 1/mu of the first two planes
-    for (int e = tid; e < 2 * RH * RW; e += NT) {
-        const int p = e / (RH * RW), r = e % (RH * RW);
-        const int ex = r % RW, ey = r / RW;
-        const int gxe = min(t.gx0 + ex, m.nx - 1), gye = min(t.gy0 + ey, m.ny - 1);
-        rmu[p][r] = __frcp_rn(m.mu[pidx(m, gxe, gye, gz0 + p)]);
-    }
-    // own-cell stresses (interior cells) and medium of the first plane
-    float scur[CELLS][6], lcur[CELLS], mcur[CELLS];
+    // own-cell stresses (interior cells) and medium of the first plane; the
+    // staggered shear moduli were averaged once when the medium was set
+    float scur[CELLS][6], lcur[CELLS], mcur[CELLS], gcur[CELLS][3];
 #pragma unroll
     for (int c = 0; c < CELLS; ++c) {
         const uint32_t ci = col[c] + (uint32_t)gz0 * PL;
@@ -534,13 +540,15 @@ k_stress_zmarch(const __grid_constant__ StrMaps mp, const __grid_constant__ Mode
         for (int q = 0; q < 6; ++q) scur[c][q] = m.f[3 + q][ci];
         lcur[c] = m.lam[ci];
         mcur[c] = m.mu[ci];
+        gcur[c][0] = m.mxy[ci];
+        gcur[c][1] = m.mxz[ci];
+        gcur[c][2] = m.myz[ci];
     }
 
     int rp = g.rec_off[blockIdx.x];
     const int rend = g.rec_off[blockIdx.x + 1];
     while (rp < rend && g.rec_list[rp].z < gz0) ++rp;
     int rz = rp < rend ? g.rec_list[rp].z : 0x7fffffff;
-    __syncthreads();   // rmu warm-up visible
 
     bool failed = false, abort = false;
     int cz = t.zs;
@@ -559,7 +567,7 @@ k_stress_zmarch(const __grid_constant__ StrMaps mp, const __grid_constant__ Mode
         const bool plane_pml = GEN && (t.xy_pml || kz != 0);
 
         // own-cell data of the next plane (plane gz+1 <= nz-5 is always inside the grid)
-        float snxt[CELLS][6], lnxt[CELLS], mnxt[CELLS];
+        float snxt[CELLS][6], lnxt[CELLS], mnxt[CELLS], gnxt[CELLS][3];
 #pragma unroll
         for (int c = 0; c < CELLS; ++c) {
             const uint32_t ci = col[c] + (uint32_t)(gz + 1) * PL;
@@ -567,21 +575,29 @@ k_stress_zmarch(const __grid_constant__ StrMaps mp, const __grid_constant__ Mode
             for (int q = 0; q < 6; ++q) snxt[c][q] = m.f[3 + q][ci];
             lnxt[c] = m.lam[ci];
             mnxt[c] = m.mu[ci];
+            gnxt[c][0] = m.mxy[ci];
+            gnxt[c][1] = m.mxz[ci];
+            gnxt[c][2] = m.myz[ci];
+        }
+
+        // PML cells: splits and the buoyancy of the damping, loaded before the
+        // stage wait so that their latency overlaps the wait and the stencil
+        float opre[CELLS][15], bpre[CELLS];
+        if (plane_pml) {
+            const uint32_t N = (uint32_t)m.npml;
+#pragma unroll
+            for (int c = 0; c < CELLS; ++c) {
+                if (act[c] && (kx | kyc[c] | kz)) {
+                    const uint32_t ci = col[c] + (uint32_t)gz * PL;
+                    const float *sp = m.split + pml_plane_index(m, pcol[c], cz);
+#pragma unroll
+                    for (int q = 0; q < 15; ++q) opre[c][q] = sp[(S_XXX + q) * N];
+                    bpre[c] = m.b[ci];
+                }
+            }
         }
 
         if (!mbar_wait(&bar[s], (uint32_t)((k / S) & 1))) failed = true;
-
-        // 1/mu of plane z+2 into the ring (read from iteration k+1 on)
-        {
-            const float *mub = reinterpret_cast<const float *>(st + L::MU);
-            float *rn = rmu[(k + 2) % 3];
-            for (int e = tid; e < RH * RW; e += NT) {
-                const int ex = e % RW, ey = e / RW;
-                rn[e] = __frcp_rn(mub[ey * W36 + ex]);
-            }
-        }
-        const float *r0 = rmu[k % 3];
-        const float *r1 = rmu[(k + 1) % 3];
 
         const float *svx = reinterpret_cast<const float *>(st + L::VX);
         const float *svy = reinterpret_cast<const float *>(st + L::VY);
@@ -628,11 +644,7 @@ k_stress_zmarch(const __grid_constant__ StrMaps mp, const __grid_constant__ Mode
 
             const float l = lcur[c];
             const float l2m = __fmaf_rn(2.0f, mcur[c], l);
-            const bool ref = ph.quirks == 0;
-            const int e0 = ly * RW + lx;
-            const float mxy = hmean<FAST>(r0[e0], r0[e0 + 1], r0[e0 + RW], r0[e0 + 1 + RW]);
-            const float mxz = hmean<FAST>(r0[e0], r0[e0 + 1], r1[e0], ref ? r0[e0 + 1 + RW] : r1[e0 + 1]);
-            const float myz = hmean<FAST>(r0[e0], r0[e0 + RW], r1[e0], r1[e0 + RW]);
+            const float mxy = gcur[c][0], mxz = gcur[c][1], myz = gcur[c][2];
 
             const uint32_t ci = col[c] + (uint32_t)gz * PL;
             const int ky = kyc[c];
@@ -649,12 +661,10 @@ k_stress_zmarch(const __grid_constant__ StrMaps mp, const __grid_constant__ Mode
             } else {
                 float *sp = m.split + pml_plane_index(m, pcol[c], cz);
                 const uint32_t N = (uint32_t)m.npml;
-                float o[15];
-#pragma unroll
-                for (int q = 0; q < 15; ++q) o[q] = sp[(S_XXX + q) * N];
+                const float *o = opre[c];
                 float mx = 1.f, px = 1.f, my = 1.f, py = 1.f, mz = 1.f, pz = 1.f;
                 {
-                    const float v = damp_speed(ph, mcur[c], m.b[ci], l);
+                    const float v = damp_speed(ph, mcur[c], bpre[c], l);
                     if (kx) damp_factors<FAST>(ph, 0, ph.dx, kx, m.pml, v, mx, px);
                     if (ky) damp_factors<FAST>(ph, 1, ph.dy, ky, m.pml, v, my, py);
                     if (kz) damp_factors<FAST>(ph, 2, ph.dz, kz, m.pml, v, mz, pz);
@@ -708,6 +718,8 @@ k_stress_zmarch(const __grid_constant__ StrMaps mp, const __grid_constant__ Mode
             for (int q = 0; q < 6; ++q) scur[c][q] = snxt[c][q];
             lcur[c] = lnxt[c];
             mcur[c] = mnxt[c];
+#pragma unroll
+            for (int q = 0; q < 3; ++q) gcur[c][q] = gnxt[c][q];
         }
         if (GEN && gz == rz) {
             while (rp < rend && g.rec_list[rp].z == gz) ++rp;
@@ -817,7 +829,6 @@ cudaError_t zmarch_prepare(const Model &m, int cells, VelMaps *vm, StrMaps *sm) 
     ok &= make_map(&sm->vx, m.f[0], m, W48, ty + 10);
     ok &= make_map(&sm->vy, m.f[1], m, W48, ty + 10);
     ok &= make_map(&sm->vz, m.f[2], m, W48, ty + 10);
-    ok &= make_map(&sm->mu, m.mu, m, W36, ty + 1);
     ok &= make_map(&sm->vx_c, m.f[0], m, W32, ty);
     ok &= make_map(&sm->vy_c, m.f[1], m, W32, ty);
     ok &= make_map(&sm->vz_c, m.f[2], m, W32, ty);

@@ -339,7 +339,7 @@ int sgfd_create(const sgfd_config *cfg, sgfd_solver **out) {
     m.plane = (int64_t)m.px * m.ny;
     m.npml = pml_count(m.nxc, m.nyc, m.nzc, m.pml);
     const size_t arr_bytes = array_bytes(m);
-    const size_t pool_bytes = arr_bytes * 13;
+    const size_t pool_bytes = arr_bytes * 16;
     e = cudaMalloc(&h->field_pool, pool_bytes);
     if (e == cudaSuccess) e = cudaMalloc(&h->split, (size_t)kNumSplit * m.npml * sizeof(float));
     if (e != cudaSuccess) {
@@ -355,6 +355,9 @@ int sgfd_create(const sgfd_config *cfg, sgfd_solver **out) {
     m.lam = arr(10);
     m.mu = arr(11);
     m.rmu = arr(12);
+    m.mxy = arr(13);
+    m.mxz = arr(14);
+    m.myz = arr(15);
     m.split = h->split;
     e = cudaMemsetAsync(h->field_pool, 0, pool_bytes, h->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(h->split, 0, (size_t)kNumSplit * m.npml * sizeof(float), h->stream);
@@ -436,7 +439,10 @@ static int upload_medium(sgfd_solver *h, const float *b, const float *l, const f
         SG_CUDA(h, cudaMemcpy2DAsync(dst[k], (size_t)m.px * sizeof(float), src[k], row, row, rows, kind, h->stream),
                 "medium upload");
     cudaError_t e = launch_reciprocal(const_cast<float *>(m.rmu) - kXOff, m.mu - kXOff, m.plane * m.nz, h->stream);
-    if (e != cudaSuccess) return cuda_fail(h, e, "reciprocal kernel");
+    if (e == cudaSuccess)
+        e = launch_shear_means(m, h->ph, const_cast<float *>(m.mxy), const_cast<float *>(m.mxz),
+                               const_cast<float *>(m.myz), h->stream);
+    if (e != cudaSuccess) return cuda_fail(h, e, "medium set-up kernels");
     SG_CUDA(h, cudaStreamSynchronize(h->stream), "medium upload");
     h->medium_set = true;
     return SGFD_OK;

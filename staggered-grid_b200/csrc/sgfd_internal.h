@@ -66,6 +66,9 @@ struct Model {
     int64_t npml;        // number of PML cells
     float *f[9];         // vx vy vz txx tyy tzz txy txz tyz
     const float *b, *lam, *mu, *rmu;   // rmu = 1/mu
+    // staggered shear moduli of the txy, txz, tyz updates: harmonic means of
+    // four mu (ElasticMacro.h:110-119), computed once per medium upload
+    const float *mxy, *mxz, *myz;
     float *split;        // kNumSplit * npml
 };
 
@@ -164,8 +167,11 @@ cudaError_t simple_step(const Model &m, const Physics &ph, const SourceRec &sr,
                         cudaEvent_t *ev = nullptr);
 int simple_launches_per_step(const SourceRec &sr);
 
-// medium post-processing: rmu = 1/mu over the padded arrays.
+// medium post-processing: rmu = 1/mu over the padded arrays, then the three
+// staggered shear moduli of every computed cell from rmu.
 cudaError_t launch_reciprocal(float *rmu, const float *mu, int64_t n, cudaStream_t s);
+cudaError_t launch_shear_means(const Model &m, const Physics &ph, float *mxy, float *mxz, float *myz,
+                               cudaStream_t s);
 // FP64 energy audit (kernels_audit.cu): partials holds 2 doubles per block,
 // out 2 doubles (kinetic, strain).
 int energy_blocks(int num_sms);

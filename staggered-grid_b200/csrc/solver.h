@@ -36,7 +36,7 @@ struct sgfd_solver {
     int device = 0;
     cudaStream_t stream = nullptr;
     cudaStream_t own_stream = nullptr;
-    char *field_pool = nullptr;   // 9 fields + b, lambda, mu, 1/mu
+    char *field_pool = nullptr;   // 9 fields + b, lambda, mu, 1/mu, 3 shear moduli
     float *split = nullptr;
     int4 *rec = nullptr;
     float *traces = nullptr;

@@ -18,7 +18,7 @@ struct VelMaps {
 };
 // TMA descriptors of the stress update.
 struct StrMaps {
-    CUtensorMap vx, vy, vz, mu;                  // current plane (mu: plane z+1)
+    CUtensorMap vx, vy, vz;                      // current plane
     CUtensorMap vx_c, vy_c, vz_c;                // lead planes
 };
 
