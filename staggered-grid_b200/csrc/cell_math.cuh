@@ -49,6 +49,21 @@ __device__ __forceinline__ float dB(const Physics &ph, G g) {
     return dbwd(ph.c, g) / (AXIS == 0 ? ph.dx : AXIS == 1 ? ph.dy : ph.dz);
 }
 
+// Two staggered differences at once on packed FP32x2 (sm_100 fma.rn.f32x2):
+// lane 0 of every operand belongs to the first difference, lane 1 to the
+// second; plus(i) and minus(i) give term i's taps of both (forward g(1+i),
+// g(-i); backward g(i), g(-1-i)) and c their coefficients.  Each lane does
+// exactly what dfwd / dbwd do: the tap difference a - b is computed as
+// fma(b, -1, a), which rounds to the same value.
+template <class P, class M>
+__device__ __forceinline__ float2 dpair(const float2 (&c)[5], P plus, M minus) {
+    const float2 neg1 = make_float2(-1.0f, -1.0f);
+    float2 d = make_float2(0.0f, 0.0f);
+#pragma unroll
+    for (int i = 0; i < 5; ++i) d = __ffma2_rn(c[i], __ffma2_rn(minus(i), neg1, plus(i)), d);
+    return d;
+}
+
 // The same differences for two vertically adjacent cells (rows r and r+1)
 // that share one 11-value window, g(o) being the value o rows from row r:
 // forward windows span rows r-4 .. r+6, backward windows r-5 .. r+5.  Each

@@ -331,7 +331,7 @@ k_velocity_zmarch(const __grid_constant__ VelMaps mp, const __grid_constant__ Mo
         const float *lb = reinterpret_cast<const float *>(st + L::LB);
 
         // y differences of vertically adjacent cells share their windows
-        float xY2[2] = {0.f, 0.f}, yY2[2] = {0.f, 0.f}, zY2[2] = {0.f, 0.f};
+        [[maybe_unused]] float xY2[2] = {0.f, 0.f}, yY2[2] = {0.f, 0.f}, zY2[2] = {0.f, 0.f};
         if constexpr (CELLS == 2) {
             const float *cxy0 = sxy + (lyc[0] + 5) * W48 + lx + 8;
             const float *cyy0 = syy + (lyc[0] + 5) * W32 + lx;
@@ -360,15 +360,32 @@ k_velocity_zmarch(const __grid_constant__ VelMaps mp, const __grid_constant__ Mo
             const float *rxz = sxz + ly * W48 + lx + 8;
             const float *cyy = syy + (ly + 5) * W32 + lx;
             const float *cyz = syz + (ly + 5) * W32 + lx;
-            const float xX = dF<FAST, 0>(ph, [&](int o) { return rxx[o]; });
-            const float xY = CELLS == 2 ? xY2[c] : dB<FAST, 1>(ph, [&](int o) { return cxy[o * W48]; });
-            const float xZ = dB<FAST, 2>(ph, [&](int o) { return qxz[c][5 + o]; });
-            const float yX = dB<FAST, 0>(ph, [&](int o) { return cxy[o]; });
-            const float yY = CELLS == 2 ? yY2[c] : dF<FAST, 1>(ph, [&](int o) { return cyy[o * W32]; });
-            const float yZ = dB<FAST, 2>(ph, [&](int o) { return qyz[c][5 + o]; });
-            const float zX = dB<FAST, 0>(ph, [&](int o) { return rxz[o]; });
-            const float zY = CELLS == 2 ? zY2[c] : dB<FAST, 1>(ph, [&](int o) { return cyz[o * W32]; });
-            const float zZ = dF<FAST, 2>(ph, [&](int o) { return qzz[c][4 + o]; });
+            float xX, xY, xZ, yX, yY, yZ, zX, zY, zZ;
+            if constexpr (FAST && CELLS == 1) {
+                // eight of the nine differences in pairs on FP32x2, same roundings
+                const float2 yzX = dpair(ph.cp[0], [&](int i) { return make_float2(cxy[i], rxz[i]); },
+                                         [&](int i) { return make_float2(cxy[-1 - i], rxz[-1 - i]); });
+                const float2 xzY = dpair(ph.cp[1], [&](int i) { return make_float2(cxy[i * W48], cyz[i * W32]); },
+                                         [&](int i) { return make_float2(cxy[(-1 - i) * W48], cyz[(-1 - i) * W32]); });
+                const float2 xyZ = dpair(ph.cp[2], [&](int i) { return make_float2(qxz[c][5 + i], qyz[c][5 + i]); },
+                                         [&](int i) { return make_float2(qxz[c][4 - i], qyz[c][4 - i]); });
+                const float2 xXyY = dpair(ph.cp[3], [&](int i) { return make_float2(rxx[1 + i], cyy[(1 + i) * W32]); },
+                                          [&](int i) { return make_float2(rxx[-i], cyy[-i * W32]); });
+                xX = xXyY.x; yY = xXyY.y;
+                yX = yzX.x; zX = yzX.y;
+                xY = xzY.x; zY = xzY.y;
+                xZ = xyZ.x; yZ = xyZ.y;
+            } else {
+                xX = dF<FAST, 0>(ph, [&](int o) { return rxx[o]; });
+                xY = CELLS == 2 ? xY2[c] : dB<FAST, 1>(ph, [&](int o) { return cxy[o * W48]; });
+                xZ = dB<FAST, 2>(ph, [&](int o) { return qxz[c][5 + o]; });
+                yX = dB<FAST, 0>(ph, [&](int o) { return cxy[o]; });
+                yY = CELLS == 2 ? yY2[c] : dF<FAST, 1>(ph, [&](int o) { return cyy[o * W32]; });
+                yZ = dB<FAST, 2>(ph, [&](int o) { return qyz[c][5 + o]; });
+                zX = dB<FAST, 0>(ph, [&](int o) { return rxz[o]; });
+                zY = CELLS == 2 ? zY2[c] : dB<FAST, 1>(ph, [&](int o) { return cyz[o * W32]; });
+            }
+            zZ = dF<FAST, 2>(ph, [&](int o) { return qzz[c][4 + o]; });
             const float b0 = bb[ly * W36 + lx];
             const float bx = (b0 + bb[ly * W36 + lx + 1]) / 2.0f;
             const float by = (b0 + bb[(ly + 1) * W36 + lx]) / 2.0f;
@@ -606,7 +623,7 @@ k_stress_zmarch(const __grid_constant__ StrMaps mp, const __grid_constant__ Mode
         const float *lly = reinterpret_cast<const float *>(st + L::LY);
         const float *llz = reinterpret_cast<const float *>(st + L::LZ);
 
-        float dYy2[2] = {0.f, 0.f}, xyY2[2] = {0.f, 0.f}, yzY2[2] = {0.f, 0.f};
+        [[maybe_unused]] float dYy2[2] = {0.f, 0.f}, xyY2[2] = {0.f, 0.f}, yzY2[2] = {0.f, 0.f};
         if constexpr (CELLS == 2) {
             const float *cx0 = svx + (lyc[0] + 5) * W48 + lx + 8;
             const float *cy0 = svy + (lyc[0] + 5) * W48 + lx + 8;
@@ -632,15 +649,33 @@ k_stress_zmarch(const __grid_constant__ StrMaps mp, const __grid_constant__ Mode
             const float *cx_ = svx + (ly + 5) * W48 + lx + 8;
             const float *cy_ = svy + (ly + 5) * W48 + lx + 8;
             const float *cz_ = svz + (ly + 5) * W48 + lx + 8;
-            const float dXx = dB<FAST, 0>(ph, [&](int o) { return cx_[o]; });
-            const float dYy = CELLS == 2 ? dYy2[c] : dB<FAST, 1>(ph, [&](int o) { return cy_[o * W48]; });
-            const float dZz = dB<FAST, 2>(ph, [&](int o) { return qz[c][5 + o]; });
-            const float xyY = CELLS == 2 ? xyY2[c] : dF<FAST, 1>(ph, [&](int o) { return cx_[o * W48]; });
-            const float xyX = dF<FAST, 0>(ph, [&](int o) { return cy_[o]; });
-            const float xzZ = dF<FAST, 2>(ph, [&](int o) { return qx[c][4 + o]; });
-            const float xzX = dF<FAST, 0>(ph, [&](int o) { return cz_[o]; });
-            const float yzZ = dF<FAST, 2>(ph, [&](int o) { return qy[c][4 + o]; });
-            const float yzY = CELLS == 2 ? yzY2[c] : dF<FAST, 1>(ph, [&](int o) { return cz_[o * W48]; });
+            float dXx, dYy, dZz, xyY, xyX, xzZ, xzX, yzZ, yzY;
+            if constexpr (FAST && CELLS == 1) {
+                // eight of the nine differences in pairs on FP32x2, same roundings
+                const float2 pX = dpair(ph.cp[0], [&](int i) { return make_float2(cy_[1 + i], cz_[1 + i]); },
+                                        [&](int i) { return make_float2(cy_[-i], cz_[-i]); });
+                const float2 pY = dpair(ph.cp[1],
+                                        [&](int i) { return make_float2(cx_[(1 + i) * W48], cz_[(1 + i) * W48]); },
+                                        [&](int i) { return make_float2(cx_[-i * W48], cz_[-i * W48]); });
+                const float2 pZ = dpair(ph.cp[2], [&](int i) { return make_float2(qx[c][5 + i], qy[c][5 + i]); },
+                                        [&](int i) { return make_float2(qx[c][4 - i], qy[c][4 - i]); });
+                const float2 pN = dpair(ph.cp[3], [&](int i) { return make_float2(cx_[i], cy_[i * W48]); },
+                                        [&](int i) { return make_float2(cx_[-1 - i], cy_[(-1 - i) * W48]); });
+                xyX = pX.x; xzX = pX.y;
+                xyY = pY.x; yzY = pY.y;
+                xzZ = pZ.x; yzZ = pZ.y;
+                dXx = pN.x; dYy = pN.y;
+            } else {
+                dXx = dB<FAST, 0>(ph, [&](int o) { return cx_[o]; });
+                dYy = CELLS == 2 ? dYy2[c] : dB<FAST, 1>(ph, [&](int o) { return cy_[o * W48]; });
+                xyY = CELLS == 2 ? xyY2[c] : dF<FAST, 1>(ph, [&](int o) { return cx_[o * W48]; });
+                xyX = dF<FAST, 0>(ph, [&](int o) { return cy_[o]; });
+                xzZ = dF<FAST, 2>(ph, [&](int o) { return qx[c][4 + o]; });
+                xzX = dF<FAST, 0>(ph, [&](int o) { return cz_[o]; });
+                yzZ = dF<FAST, 2>(ph, [&](int o) { return qy[c][4 + o]; });
+                yzY = CELLS == 2 ? yzY2[c] : dF<FAST, 1>(ph, [&](int o) { return cz_[o * W48]; });
+            }
+            dZz = dB<FAST, 2>(ph, [&](int o) { return qz[c][5 + o]; });
 
             const float l = lcur[c];
             const float l2m = __fmaf_rn(2.0f, mcur[c], l);

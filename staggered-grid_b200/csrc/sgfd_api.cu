@@ -117,6 +117,10 @@ void set_physics(sgfd_solver *h) {
         ph.cs[1][i] = c.coef[i] / c.dy;
         ph.cs[2][i] = c.coef[i] / c.dz;
     }
+    for (int i = 0; i < 5; ++i) {
+        for (int a = 0; a < 3; ++a) ph.cp[a][i] = make_float2(ph.cs[a][i], ph.cs[a][i]);
+        ph.cp[3][i] = make_float2(ph.cs[0][i], ph.cs[1][i]);
+    }
     ph.fast = c.arith == SGFD_ARITH_FAST;
     ph.inj_dt2 = c.dt * c.dt;
     ph.damping = c.damping;

@@ -43,6 +43,7 @@ enum SplitId {
 struct Physics {
     float c[5];          // staggered coefficients
     float cs[3][5];      // c_i / dx, c_i / dy, c_i / dz (FAST arithmetic)
+    float2 cp[4][5];     // FAST pairs for FP32x2: (cs_x, cs_x), (cs_y, cs_y), (cs_z, cs_z), (cs_x, cs_y)
     int fast;            // sgfd_arith == FAST
     float dt, dx, dy, dz;
     float inj_dt2;       // dt*dt (source scale, OPT/ElasticWaveEquation.cu:213)
