@@ -7,19 +7,19 @@
 // marches along z over a chunk of planes.
 //
 // Data movement per plane z (all HBM traffic is TMA or coalesced 128-byte rows):
-//   * TMA (cp.async.bulk.tensor.3d, one elected thread, no multicast) stages
+//   * TMA (cp.async.bulk.tensor.3d, no multicast) stages
 //     the xy boxes the x/y derivatives need — tile plus its 5-cell halo on the
 //     sides a field is differentiated along — and the "lead" planes that feed
-//     the z register queues, into a 3-stage shared-memory ring guarded by one
-//     mbarrier per stage (expect-tx bytes, parity wait with an iteration cap).
+//     the z register queues, and the cell's own read-modify-write data, into
+//     a 3-stage shared-memory ring guarded by one mbarrier per stage (expect-tx
+//     bytes, parity wait with an iteration cap); lane 0 of each warp issues a
+//     share of a stage's boxes so that no warp carries the issue alone.
 //     A stage is refilled with plane z + 3 as soon as plane z is done, so
 //     every load has two plane-iterations to land.
 //   * Each thread keeps the 10 z-taps of the fields it differentiates along z
 //     in a register queue (sigma_xz, sigma_yz, sigma_zz for the velocity
 //     update; vx, vy, vz for the stress update), shifted by one per plane.
-//   * Own-cell read-modify-write data (velocities, or stresses and the
-//     medium) are loaded one plane ahead into registers with plain coalesced
-//     loads; PML split fields are loaded before the plane's TMA wait.
+//   * PML split fields are loaded into registers before the plane's TMA wait.
 // Every row starts at a 128-byte boundary (the device arrays are shifted by
 // kXOff), so x-halo boxes start 8 cells left of the tile (48 wide), centre
 // boxes are exactly 32 wide, and every TMA x coordinate is a multiple of 4.
@@ -63,9 +63,10 @@ struct VelL {
     static constexpr int LYZ = LXZ + al128(W32 * TY * 4);          // 32 x TY       sigma_yz at z+4
     static constexpr int LZZ = LYZ + al128(W32 * TY * 4);          // 32 x TY       sigma_zz at z+5
     static constexpr int LB = LZZ + al128(W32 * TY * 4);           // 32 x TY       buoyancy at z+1
-    static constexpr int STAGE = LB + al128(W32 * TY * 4);
+    static constexpr int OV = LB + al128(W32 * TY * 4);            // 3 x 32 x TY   own vx, vy, vz at z
+    static constexpr int STAGE = OV + 3 * al128(W32 * TY * 4);
     static constexpr uint32_t TXB = 4 * (2 * W48 * TY + 2 * W32 * (TY + 10) + W48 * (TY + 10) +
-                                         W36 * (TY + 1) + 4 * W32 * TY);
+                                         W36 * (TY + 1) + 7 * W32 * TY);
 };
 // Shared-memory stage layout of the stress update.
 template <int TY>
@@ -76,8 +77,12 @@ struct StrL {
     static constexpr int LX = VZ + al128(W48 * (TY + 10) * 4);     // 32 x TY       vx at z+5
     static constexpr int LY = LX + al128(W32 * TY * 4);            // 32 x TY       vy at z+5
     static constexpr int LZ = LY + al128(W32 * TY * 4);            // 32 x TY       vz at z+4
-    static constexpr int STAGE = LZ + al128(W32 * TY * 4);
-    static constexpr uint32_t TXB = 4 * (3 * W48 * (TY + 10) + 3 * W32 * TY);
+    // own-cell data at z, 32 x TY each: txx tyy tzz txy txz tyz, lambda, mu,
+    // the shear moduli of txy, txz, tyz
+    static constexpr int OWN = LZ + al128(W32 * TY * 4);
+    static constexpr int NOWN = 11;
+    static constexpr int STAGE = OWN + NOWN * al128(W32 * TY * 4);
+    static constexpr uint32_t TXB = 4 * (3 * W48 * (TY + 10) + (3 + NOWN) * W32 * TY);
 };
 
 constexpr uint32_t kWaitCap = 2000;
@@ -157,21 +162,45 @@ __device__ __forceinline__ unsigned char *align_smem(unsigned char *p) {
 // velocity update
 // ---------------------------------------------------------------------------
 
+constexpr int kWarps = NT / 32;
+constexpr int kVelBoxes = 13;
+constexpr int kStrBoxes = 17;
+
+// Box q of the velocity stage of GRID plane gz.
 template <int TY>
-__device__ __forceinline__ void vel_issue(const VelMaps &mp, unsigned char *st, uint64_t *bar, const Tile &t, int cz) {
+__device__ __forceinline__ void vel_box(const VelMaps &mp, unsigned char *st, uint64_t *bar, const Tile &t, int gz,
+                                        int q) {
+    using L = VelL<TY>;
+    constexpr int OB = al128(W32 * TY * 4);
+    switch (q) {
+    case 0: tma3(st + L::SXX, &mp.sxx, t.xd - 8, t.gy0, gz, bar); break;
+    case 1: tma3(st + L::SYY, &mp.syy, t.xd, t.gy0 - 5, gz, bar); break;
+    case 2: tma3(st + L::SXY, &mp.sxy, t.xd - 8, t.gy0 - 5, gz, bar); break;
+    case 3: tma3(st + L::SXZ, &mp.sxz, t.xd - 8, t.gy0, gz, bar); break;
+    case 4: tma3(st + L::SYZ, &mp.syz, t.xd, t.gy0 - 5, gz, bar); break;
+    case 5: tma3(st + L::B, &mp.b, t.xd, t.gy0, gz, bar); break;
+    case 6: tma3(st + L::LXZ, &mp.sxz_c, t.xd, t.gy0, gz + 4, bar); break;
+    case 7: tma3(st + L::LYZ, &mp.syz_c, t.xd, t.gy0, gz + 4, bar); break;
+    case 8: tma3(st + L::LZZ, &mp.szz_c, t.xd, t.gy0, gz + 5, bar); break;
+    case 9: tma3(st + L::LB, &mp.b_c, t.xd, t.gy0, gz + 1, bar); break;
+    case 10: tma3(st + L::OV, &mp.own[0], t.xd, t.gy0, gz, bar); break;
+    case 11: tma3(st + L::OV + OB, &mp.own[1], t.xd, t.gy0, gz, bar); break;
+    default: tma3(st + L::OV + 2 * OB, &mp.own[2], t.xd, t.gy0, gz, bar); break;
+    }
+}
+
+// Stage the velocity inputs of computed plane cz.  The issue is shared so
+// that no warp falls behind the others: lane 0 of warp w issues boxes w,
+// w + 8, ..., and thread 0 also arms the stage's barrier with its bytes (the
+// barrier's phase cannot complete before that arrival, whichever copy lands
+// first).  Called by lane 0 of every warp.
+template <int TY>
+__device__ __forceinline__ void vel_issue(const VelMaps &mp, unsigned char *st, uint64_t *bar, const Tile &t, int cz,
+                                          int warp) {
     using L = VelL<TY>;
     const int gz = cz + kHalo;
-    mbar_expect_tx(bar, L::TXB);
-    tma3(st + L::SXX, &mp.sxx, t.xd - 8, t.gy0, gz, bar);
-    tma3(st + L::SYY, &mp.syy, t.xd, t.gy0 - 5, gz, bar);
-    tma3(st + L::SXY, &mp.sxy, t.xd - 8, t.gy0 - 5, gz, bar);
-    tma3(st + L::SXZ, &mp.sxz, t.xd - 8, t.gy0, gz, bar);
-    tma3(st + L::SYZ, &mp.syz, t.xd, t.gy0 - 5, gz, bar);
-    tma3(st + L::B, &mp.b, t.xd, t.gy0, gz, bar);
-    tma3(st + L::LXZ, &mp.sxz_c, t.xd, t.gy0, gz + 4, bar);
-    tma3(st + L::LYZ, &mp.syz_c, t.xd, t.gy0, gz + 4, bar);
-    tma3(st + L::LZZ, &mp.szz_c, t.xd, t.gy0, gz + 5, bar);
-    tma3(st + L::LB, &mp.b_c, t.xd, t.gy0, gz + 1, bar);
+    if (warp == 0) mbar_expect_tx(bar, L::TXB);
+    for (int q = warp; q < kVelBoxes; q += kWarps) vel_box<TY>(mp, st, bar, t, gz, q);
 }
 
 template <bool FAST, int CELLS>
@@ -191,11 +220,10 @@ k_velocity_zmarch(const __grid_constant__ VelMaps mp, const __grid_constant__ Mo
         fence_barrier_init();
     }
     __syncthreads();
-    int issued_end = t.zs;   // planes [zs, issued_end) issued (meaningful in thread 0)
-    if (tid == 0) {
-        for (int s = 0; s < S && t.zs + s < t.ze; ++s) vel_issue<TY>(mp, smem + s * L::STAGE, &bar[s], t, t.zs + s);
-        issued_end = min(t.zs + S, t.ze);
-    }
+    const int warp = tid >> 5;
+    if (lx == 0)
+        for (int s = 0; s < S && t.zs + s < t.ze; ++s) vel_issue<TY>(mp, smem + s * L::STAGE, &bar[s], t, t.zs + s, warp);
+    int issued_end = min(t.zs + S, t.ze);   // planes [zs, issued_end) issued
 
     const int it = step_index(sr, it_arg);
     const float inj = ph.inj_dt2 * ((use_wavelet && sr.wavelet) ? sr.wavelet[it] : src_value);
@@ -239,16 +267,6 @@ k_velocity_zmarch(const __grid_constant__ VelMaps mp, const __grid_constant__ Mo
             qzz[c][k + 1] = zz;
         }
     }
-    // own-cell velocities of the first plane (interior cells only need them)
-    float vcur[CELLS][3];
-    {
-#pragma unroll
-        for (int c = 0; c < CELLS; ++c) {
-            const uint32_t ci = col[c] + (uint32_t)gz0 * PL;
-#pragma unroll
-            for (int q = 0; q < 3; ++q) vcur[c][q] = m.f[q][ci];
-        }
-    }
 
     // receivers of this tile, sorted by z: skip those below the chunk
     int rp = g.rec_off[blockIdx.x];
@@ -272,14 +290,6 @@ k_velocity_zmarch(const __grid_constant__ VelMaps mp, const __grid_constant__ Mo
         const int kz = band(gz, m.nz, m.pml);
         const bool plane_pml = GEN && (t.xy_pml || kz != 0);
 
-        // own-cell velocities of the next plane (plane gz+1 <= nz-5 is always inside the grid)
-        float vnxt[CELLS][3];
-#pragma unroll
-        for (int c = 0; c < CELLS; ++c) {
-            const uint32_t ci = col[c] + (uint32_t)(gz + 1) * PL;
-#pragma unroll
-            for (int q = 0; q < 3; ++q) vnxt[c][q] = m.f[q][ci];
-        }
 
         // PML cells: splits and the medium of the damping, loaded before the
         // stage wait so that their latency overlaps the wait and the stencil
@@ -329,6 +339,8 @@ k_velocity_zmarch(const __grid_constant__ VelMaps mp, const __grid_constant__ Mo
         const float *lyz = reinterpret_cast<const float *>(st + L::LYZ);
         const float *lzz = reinterpret_cast<const float *>(st + L::LZZ);
         const float *lb = reinterpret_cast<const float *>(st + L::LB);
+        const float *ov = reinterpret_cast<const float *>(st + L::OV);
+        constexpr int OVS = al128(W32 * TY * 4) / 4;   // floats between the own-velocity boxes
 
         // y differences of vertically adjacent cells share their windows
         [[maybe_unused]] float xY2[2] = {0.f, 0.f}, yY2[2] = {0.f, 0.f}, zY2[2] = {0.f, 0.f};
@@ -395,9 +407,10 @@ k_velocity_zmarch(const __grid_constant__ VelMaps mp, const __grid_constant__ Mo
             float vnew[3];
             const int ky = kyc[c];
             if (!(plane_pml && (kx | ky | kz))) {
-                vnew[0] = __fmaf_rn(ph.dt * bx, (xX + xY) + xZ, vcur[c][0]);
-                vnew[1] = __fmaf_rn(ph.dt * by, (yX + yY) + yZ, vcur[c][1]);
-                vnew[2] = __fmaf_rn(ph.dt * bz, (zX + zY) + zZ, vcur[c][2]);
+                const int e = ly * W32 + lx;
+                vnew[0] = __fmaf_rn(ph.dt * bx, (xX + xY) + xZ, ov[e]);
+                vnew[1] = __fmaf_rn(ph.dt * by, (yX + yY) + yZ, ov[OVS + e]);
+                vnew[2] = __fmaf_rn(ph.dt * bz, (zX + zY) + zZ, ov[2 * OVS + e]);
             } else {
                 float mx = 1.f, px = 1.f, my = 1.f, py = 1.f, mz = 1.f, pz = 1.f;
                 {
@@ -441,10 +454,6 @@ k_velocity_zmarch(const __grid_constant__ VelMaps mp, const __grid_constant__ Mo
                 }
             }
         }
-#pragma unroll
-        for (int c = 0; c < CELLS; ++c)
-#pragma unroll
-            for (int q = 0; q < 3; ++q) vcur[c][q] = vnxt[c][q];
         if (GEN && gz == rz) {
             while (rp < rend && g.rec_list[rp].z == gz) ++rp;
             rz = rp < rend ? g.rec_list[rp].z : 0x7fffffff;
@@ -452,9 +461,11 @@ k_velocity_zmarch(const __grid_constant__ VelMaps mp, const __grid_constant__ Mo
 
         // every thread is done with this stage: vote on aborts, then refill it
         if (__syncthreads_or(failed)) return false;
-        if (tid == 0 && cz + S < t.ze) {
-            fence_proxy_async();
-            vel_issue<TY>(mp, st, &bar[s], t, cz + S);
+        if (cz + S < t.ze) {
+            if (lx == 0) {
+                fence_proxy_async();
+                vel_issue<TY>(mp, st, &bar[s], t, cz + S, warp);
+            }
             issued_end = cz + S + 1;
         }
         return true;
@@ -477,17 +488,41 @@ k_velocity_zmarch(const __grid_constant__ VelMaps mp, const __grid_constant__ Mo
 // stress update
 // ---------------------------------------------------------------------------
 
+// Box q of the stress stage of GRID plane gz.
 template <int TY>
-__device__ __forceinline__ void str_issue(const StrMaps &mp, unsigned char *st, uint64_t *bar, const Tile &t, int cz) {
+__device__ __forceinline__ void str_box(const StrMaps &mp, unsigned char *st, uint64_t *bar, const Tile &t, int gz,
+                                        int q) {
+    using L = StrL<TY>;
+    constexpr int OB = al128(W32 * TY * 4);
+    switch (q) {
+    case 0: tma3(st + L::VX, &mp.vx, t.xd - 8, t.gy0 - 5, gz, bar); break;
+    case 1: tma3(st + L::VY, &mp.vy, t.xd - 8, t.gy0 - 5, gz, bar); break;
+    case 2: tma3(st + L::VZ, &mp.vz, t.xd - 8, t.gy0 - 5, gz, bar); break;
+    case 3: tma3(st + L::LX, &mp.vx_c, t.xd, t.gy0, gz + 5, bar); break;
+    case 4: tma3(st + L::LY, &mp.vy_c, t.xd, t.gy0, gz + 5, bar); break;
+    case 5: tma3(st + L::LZ, &mp.vz_c, t.xd, t.gy0, gz + 4, bar); break;
+    case 6: tma3(st + L::OWN, &mp.own[0], t.xd, t.gy0, gz, bar); break;
+    case 7: tma3(st + L::OWN + OB, &mp.own[1], t.xd, t.gy0, gz, bar); break;
+    case 8: tma3(st + L::OWN + 2 * OB, &mp.own[2], t.xd, t.gy0, gz, bar); break;
+    case 9: tma3(st + L::OWN + 3 * OB, &mp.own[3], t.xd, t.gy0, gz, bar); break;
+    case 10: tma3(st + L::OWN + 4 * OB, &mp.own[4], t.xd, t.gy0, gz, bar); break;
+    case 11: tma3(st + L::OWN + 5 * OB, &mp.own[5], t.xd, t.gy0, gz, bar); break;
+    case 12: tma3(st + L::OWN + 6 * OB, &mp.own[6], t.xd, t.gy0, gz, bar); break;
+    case 13: tma3(st + L::OWN + 7 * OB, &mp.own[7], t.xd, t.gy0, gz, bar); break;
+    case 14: tma3(st + L::OWN + 8 * OB, &mp.own[8], t.xd, t.gy0, gz, bar); break;
+    case 15: tma3(st + L::OWN + 9 * OB, &mp.own[9], t.xd, t.gy0, gz, bar); break;
+    default: tma3(st + L::OWN + 10 * OB, &mp.own[10], t.xd, t.gy0, gz, bar); break;
+    }
+}
+
+// Stage the stress inputs of computed plane cz, issue shared as in vel_issue.
+template <int TY>
+__device__ __forceinline__ void str_issue(const StrMaps &mp, unsigned char *st, uint64_t *bar, const Tile &t, int cz,
+                                          int warp) {
     using L = StrL<TY>;
     const int gz = cz + kHalo;
-    mbar_expect_tx(bar, L::TXB);
-    tma3(st + L::VX, &mp.vx, t.xd - 8, t.gy0 - 5, gz, bar);
-    tma3(st + L::VY, &mp.vy, t.xd - 8, t.gy0 - 5, gz, bar);
-    tma3(st + L::VZ, &mp.vz, t.xd - 8, t.gy0 - 5, gz, bar);
-    tma3(st + L::LX, &mp.vx_c, t.xd, t.gy0, gz + 5, bar);
-    tma3(st + L::LY, &mp.vy_c, t.xd, t.gy0, gz + 5, bar);
-    tma3(st + L::LZ, &mp.vz_c, t.xd, t.gy0, gz + 4, bar);
+    if (warp == 0) mbar_expect_tx(bar, L::TXB);
+    for (int q = warp; q < kStrBoxes; q += kWarps) str_box<TY>(mp, st, bar, t, gz, q);
 }
 
 template <bool FAST, int CELLS>
@@ -507,11 +542,10 @@ k_stress_zmarch(const __grid_constant__ StrMaps mp, const __grid_constant__ Mode
         fence_barrier_init();
     }
     __syncthreads();
-    int issued_end = t.zs;
-    if (tid == 0) {
-        for (int s = 0; s < S && t.zs + s < t.ze; ++s) str_issue<TY>(mp, smem + s * L::STAGE, &bar[s], t, t.zs + s);
-        issued_end = min(t.zs + S, t.ze);
-    }
+    const int warp = tid >> 5;
+    if (lx == 0)
+        for (int s = 0; s < S && t.zs + s < t.ze; ++s) str_issue<TY>(mp, smem + s * L::STAGE, &bar[s], t, t.zs + s, warp);
+    int issued_end = min(t.zs + S, t.ze);   // planes [zs, issued_end) issued
 
     const int it = step_index(sr, it_arg);
     const float inj = ph.inj_dt2 * ((use_wavelet && sr.wavelet) ? sr.wavelet[it] : src_value);
@@ -547,20 +581,6 @@ k_stress_zmarch(const __grid_constant__ StrMaps mp, const __grid_constant__ Mode
             qz[c][k + 1] = m.f[2][col[c] + (uint32_t)(gz0 - 5 + k) * PL];
         }
     }
-    // own-cell stresses (interior cells) and medium of the first plane; the
-    // staggered shear moduli were averaged once when the medium was set
-    float scur[CELLS][6], lcur[CELLS], mcur[CELLS], gcur[CELLS][3];
-#pragma unroll
-    for (int c = 0; c < CELLS; ++c) {
-        const uint32_t ci = col[c] + (uint32_t)gz0 * PL;
-#pragma unroll
-        for (int q = 0; q < 6; ++q) scur[c][q] = m.f[3 + q][ci];
-        lcur[c] = m.lam[ci];
-        mcur[c] = m.mu[ci];
-        gcur[c][0] = m.mxy[ci];
-        gcur[c][1] = m.mxz[ci];
-        gcur[c][2] = m.myz[ci];
-    }
 
     int rp = g.rec_off[blockIdx.x];
     const int rend = g.rec_off[blockIdx.x + 1];
@@ -583,19 +603,6 @@ k_stress_zmarch(const __grid_constant__ StrMaps mp, const __grid_constant__ Mode
         const int kz = band(gz, m.nz, m.pml);
         const bool plane_pml = GEN && (t.xy_pml || kz != 0);
 
-        // own-cell data of the next plane (plane gz+1 <= nz-5 is always inside the grid)
-        float snxt[CELLS][6], lnxt[CELLS], mnxt[CELLS], gnxt[CELLS][3];
-#pragma unroll
-        for (int c = 0; c < CELLS; ++c) {
-            const uint32_t ci = col[c] + (uint32_t)(gz + 1) * PL;
-#pragma unroll
-            for (int q = 0; q < 6; ++q) snxt[c][q] = m.f[3 + q][ci];
-            lnxt[c] = m.lam[ci];
-            mnxt[c] = m.mu[ci];
-            gnxt[c][0] = m.mxy[ci];
-            gnxt[c][1] = m.mxz[ci];
-            gnxt[c][2] = m.myz[ci];
-        }
 
         // PML cells: splits and the buoyancy of the damping, loaded before the
         // stage wait so that their latency overlaps the wait and the stencil
@@ -622,6 +629,9 @@ k_stress_zmarch(const __grid_constant__ StrMaps mp, const __grid_constant__ Mode
         const float *llx = reinterpret_cast<const float *>(st + L::LX);
         const float *lly = reinterpret_cast<const float *>(st + L::LY);
         const float *llz = reinterpret_cast<const float *>(st + L::LZ);
+        // own-cell boxes: txx..tyz at q = 0..5, lambda 6, mu 7, shear moduli 8..10
+        const float *own = reinterpret_cast<const float *>(st + L::OWN);
+        constexpr int OS = al128(W32 * TY * 4) / 4;
 
         [[maybe_unused]] float dYy2[2] = {0.f, 0.f}, xyY2[2] = {0.f, 0.f}, yzY2[2] = {0.f, 0.f};
         if constexpr (CELLS == 2) {
@@ -677,29 +687,30 @@ k_stress_zmarch(const __grid_constant__ StrMaps mp, const __grid_constant__ Mode
             }
             dZz = dB<FAST, 2>(ph, [&](int o) { return qz[c][5 + o]; });
 
-            const float l = lcur[c];
-            const float l2m = __fmaf_rn(2.0f, mcur[c], l);
-            const float mxy = gcur[c][0], mxz = gcur[c][1], myz = gcur[c][2];
+            const int e = ly * W32 + lx;
+            const float l = own[6 * OS + e], mu_c = own[7 * OS + e];
+            const float l2m = __fmaf_rn(2.0f, mu_c, l);
+            const float mxy = own[8 * OS + e], mxz = own[9 * OS + e], myz = own[10 * OS + e];
 
             const uint32_t ci = col[c] + (uint32_t)gz * PL;
             const int ky = kyc[c];
             float snew[6];
             if (!(plane_pml && (kx | ky | kz))) {
-                float o0 = scur[c][0], o1 = scur[c][1], o2 = scur[c][2];
+                float o0 = own[e], o1 = own[OS + e], o2 = own[2 * OS + e];
                 if (GEN && (int64_t)ci == src) { o0 = o0 + inj; o1 = o1 + inj; o2 = o2 + inj; }
                 snew[0] = __fmaf_rn(ph.dt, __fmaf_rn(l2m, dXx, l * (dYy + dZz)), o0);
                 snew[1] = __fmaf_rn(ph.dt, __fmaf_rn(l2m, dYy, l * (dXx + dZz)), o1);
                 snew[2] = __fmaf_rn(ph.dt, __fmaf_rn(l2m, dZz, l * (dXx + dYy)), o2);
-                snew[3] = __fmaf_rn(ph.dt * mxy, xyY + xyX, scur[c][3]);
-                snew[4] = __fmaf_rn(ph.dt * mxz, xzZ + xzX, scur[c][4]);
-                snew[5] = __fmaf_rn(ph.dt * myz, yzZ + yzY, scur[c][5]);
+                snew[3] = __fmaf_rn(ph.dt * mxy, xyY + xyX, own[3 * OS + e]);
+                snew[4] = __fmaf_rn(ph.dt * mxz, xzZ + xzX, own[4 * OS + e]);
+                snew[5] = __fmaf_rn(ph.dt * myz, yzZ + yzY, own[5 * OS + e]);
             } else {
                 float *sp = m.split + pml_plane_index(m, pcol[c], cz);
                 const uint32_t N = (uint32_t)m.npml;
                 const float *o = opre[c];
                 float mx = 1.f, px = 1.f, my = 1.f, py = 1.f, mz = 1.f, pz = 1.f;
                 {
-                    const float v = damp_speed(ph, mcur[c], bpre[c], l);
+                    const float v = damp_speed(ph, mu_c, bpre[c], l);
                     if (kx) damp_factors<FAST>(ph, 0, ph.dx, kx, m.pml, v, mx, px);
                     if (ky) damp_factors<FAST>(ph, 1, ph.dy, ky, m.pml, v, my, py);
                     if (kz) damp_factors<FAST>(ph, 2, ph.dz, kz, m.pml, v, mz, pz);
@@ -747,24 +758,17 @@ k_stress_zmarch(const __grid_constant__ StrMaps mp, const __grid_constant__ Mode
                 }
             }
         }
-#pragma unroll
-        for (int c = 0; c < CELLS; ++c) {
-#pragma unroll
-            for (int q = 0; q < 6; ++q) scur[c][q] = snxt[c][q];
-            lcur[c] = lnxt[c];
-            mcur[c] = mnxt[c];
-#pragma unroll
-            for (int q = 0; q < 3; ++q) gcur[c][q] = gnxt[c][q];
-        }
         if (GEN && gz == rz) {
             while (rp < rend && g.rec_list[rp].z == gz) ++rp;
             rz = rp < rend ? g.rec_list[rp].z : 0x7fffffff;
         }
 
         if (__syncthreads_or(failed)) return false;
-        if (tid == 0 && cz + S < t.ze) {
-            fence_proxy_async();
-            str_issue<TY>(mp, st, &bar[s], t, cz + S);
+        if (cz + S < t.ze) {
+            if (lx == 0) {
+                fence_proxy_async();
+                str_issue<TY>(mp, st, &bar[s], t, cz + S, warp);
+            }
             issued_end = cz + S + 1;
         }
         return true;
@@ -861,12 +865,16 @@ cudaError_t zmarch_prepare(const Model &m, int cells, VelMaps *vm, StrMaps *sm) 
     ok &= make_map(&vm->syz_c, m.f[8], m, W32, ty);
     ok &= make_map(&vm->szz_c, m.f[5], m, W32, ty);
     ok &= make_map(&vm->b_c, m.b, m, W32, ty);
+    for (int q = 0; q < 3; ++q) ok &= make_map(&vm->own[q], m.f[q], m, W32, ty);
     ok &= make_map(&sm->vx, m.f[0], m, W48, ty + 10);
     ok &= make_map(&sm->vy, m.f[1], m, W48, ty + 10);
     ok &= make_map(&sm->vz, m.f[2], m, W48, ty + 10);
     ok &= make_map(&sm->vx_c, m.f[0], m, W32, ty);
     ok &= make_map(&sm->vy_c, m.f[1], m, W32, ty);
     ok &= make_map(&sm->vz_c, m.f[2], m, W32, ty);
+    const float *own[StrMaps::kOwn] = {m.f[3], m.f[4], m.f[5], m.f[6], m.f[7], m.f[8], m.lam, m.mu,
+                                       m.mxy, m.mxz, m.myz};
+    for (int q = 0; q < StrMaps::kOwn; ++q) ok &= make_map(&sm->own[q], own[q], m, W32, ty);
     if (!ok) return cudaErrorInvalidValue;
     cudaError_t e = cells == 1 ? set_attrs<false, 1>() : set_attrs<false, 2>();
     if (e == cudaSuccess) e = cells == 1 ? set_attrs<true, 1>() : set_attrs<true, 2>();

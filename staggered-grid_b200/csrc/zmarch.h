@@ -15,11 +15,14 @@ constexpr int kZTileX = 32;
 struct VelMaps {
     CUtensorMap sxx, syy, sxy, sxz, syz, b;      // current plane
     CUtensorMap sxz_c, syz_c, szz_c, b_c;        // lead planes (centre boxes)
+    CUtensorMap own[3];                          // own-cell vx, vy, vz (centre boxes)
 };
 // TMA descriptors of the stress update.
 struct StrMaps {
     CUtensorMap vx, vy, vz;                      // current plane
     CUtensorMap vx_c, vy_c, vz_c;                // lead planes
+    static constexpr int kOwn = 11;
+    CUtensorMap own[kOwn];                       // own-cell txx..tyz, lambda, mu, mxy, mxz, myz
 };
 
 // Launch geometry: tiles of kZTileX x (8 * cells) computed cells, z chunks of
