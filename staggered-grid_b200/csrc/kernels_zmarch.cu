@@ -19,7 +19,10 @@
 //   * Each thread keeps the 10 z-taps of the fields it differentiates along z
 //     in a register queue (sigma_xz, sigma_yz, sigma_zz for the velocity
 //     update; vx, vy, vz for the stress update), shifted by one per plane.
-//   * PML split fields are loaded into registers before the plane's TMA wait.
+//   * The velocity update loads the PML split fields of its cell into
+//     registers before the plane's TMA wait; the stress update, which needs
+//     15 of them, loads them where they are used, so that it fits the 80
+//     registers per thread of three resident CTAs per SM.
 // Every row starts at a 128-byte boundary (the device arrays are shifted by
 // kXOff), so x-halo boxes start 8 cells left of the tile (48 wide), centre
 // boxes are exactly 32 wide, and every TMA x coordinate is a multiple of 4.
@@ -204,7 +207,7 @@ __device__ __forceinline__ void vel_issue(const VelMaps &mp, unsigned char *st, 
 }
 
 template <bool FAST, int CELLS>
-__global__ void __launch_bounds__(NT, 2)
+__global__ void __launch_bounds__(NT, 3)
 k_velocity_zmarch(const __grid_constant__ VelMaps mp, const __grid_constant__ Model m, const __grid_constant__ Physics ph,
                   const __grid_constant__ ZGeom g, const __grid_constant__ SourceRec sr, int it_arg,
                   float src_value, int use_wavelet) {
@@ -526,7 +529,7 @@ __device__ __forceinline__ void str_issue(const StrMaps &mp, unsigned char *st, 
 }
 
 template <bool FAST, int CELLS>
-__global__ void __launch_bounds__(NT, 2)
+__global__ void __launch_bounds__(NT, 3)
 k_stress_zmarch(const __grid_constant__ StrMaps mp, const __grid_constant__ Model m, const __grid_constant__ Physics ph,
                   const __grid_constant__ ZGeom g, const __grid_constant__ SourceRec sr, int it_arg,
                 float src_value, int use_wavelet) {
@@ -606,20 +609,6 @@ k_stress_zmarch(const __grid_constant__ StrMaps mp, const __grid_constant__ Mode
 
         // PML cells: splits and the buoyancy of the damping, loaded before the
         // stage wait so that their latency overlaps the wait and the stencil
-        float opre[CELLS][15], bpre[CELLS];
-        if (plane_pml) {
-            const uint32_t N = (uint32_t)m.npml;
-#pragma unroll
-            for (int c = 0; c < CELLS; ++c) {
-                if (act[c] && (kx | kyc[c] | kz)) {
-                    const uint32_t ci = col[c] + (uint32_t)gz * PL;
-                    const float *sp = m.split + pml_plane_index(m, pcol[c], cz);
-#pragma unroll
-                    for (int q = 0; q < 15; ++q) opre[c][q] = sp[(S_XXX + q) * N];
-                    bpre[c] = m.b[ci];
-                }
-            }
-        }
 
         if (!mbar_wait(&bar[s], (uint32_t)((k / S) & 1))) failed = true;
 
@@ -707,10 +696,12 @@ k_stress_zmarch(const __grid_constant__ StrMaps mp, const __grid_constant__ Mode
             } else {
                 float *sp = m.split + pml_plane_index(m, pcol[c], cz);
                 const uint32_t N = (uint32_t)m.npml;
-                const float *o = opre[c];
+                float o[15];
+#pragma unroll
+                for (int q = 0; q < 15; ++q) o[q] = sp[(S_XXX + q) * N];
                 float mx = 1.f, px = 1.f, my = 1.f, py = 1.f, mz = 1.f, pz = 1.f;
                 {
-                    const float v = damp_speed(ph, mu_c, bpre[c], l);
+                    const float v = damp_speed(ph, mu_c, m.b[ci], l);
                     if (kx) damp_factors<FAST>(ph, 0, ph.dx, kx, m.pml, v, mx, px);
                     if (ky) damp_factors<FAST>(ph, 1, ph.dy, ky, m.pml, v, my, py);
                     if (kz) damp_factors<FAST>(ph, 2, ph.dz, kz, m.pml, v, mz, pz);

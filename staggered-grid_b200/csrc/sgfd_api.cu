@@ -197,7 +197,10 @@ int launch_step(sgfd_solver *h, int it, float value, bool use_wavelet) {
     return SGFD_OK;
 }
 
-// z chunking: enough CTAs for ~8 waves of two CTAs per SM, chunks >= 16 planes.
+// z chunking: chunks of at most 24 planes (measured best on B200 for large
+// grids: shorter marches keep the resident CTAs on nearby planes), shorter,
+// down to 16 planes, when the grid has too few tiles for ~16 waves of three
+// CTAs per SM.
 void set_zchunks(sgfd_solver *h) {
     ZGeom &g = h->zg;
     const int tiles = g.ntx * g.nty;
@@ -205,10 +208,10 @@ void set_zchunks(sgfd_solver *h) {
     if (zc <= 0) {
         int sms = 148;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device);
-        const int target = 8 * 2 * sms;
+        const int target = 16 * 3 * sms;
         int nch = (target + tiles - 1) / tiles;
         nch = std::max(1, std::min(nch, (h->m.nzc + 15) / 16));
-        zc = (h->m.nzc + nch - 1) / nch;
+        zc = std::min(24, (h->m.nzc + nch - 1) / nch);
     }
     zc = std::max(1, std::min(zc, h->m.nzc));
     g.zc = zc;
