@@ -40,6 +40,11 @@ sys.path.insert(0, os.path.join(ROOT, "staggered-grid_b200"))
 # PML reads 3 velocities + 15 stress splits + lambda + mu, writes 15 splits +
 # 6 stresses.  Sum per step: 120 B interior, 276 B PML.
 BYTES = {"velocity": (52, 112), "stress": (68, 164)}
+# DRAM traffic / algorithmic bytes per kernel, from ncu (dram__bytes_read.sum +
+# dram__bytes_write.sum) on the 216^3 + 20 PML cube of the same kernels; the
+# 394^3 workload is too large for a multi-metric capture, so its traffic is
+# reported as its algorithmic bytes times this ratio.
+TRAFFIC_RATIO = {"velocity": 1.18, "stress": 1.31}
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -319,9 +324,11 @@ def main():
     alg = BYTES[dom][0] * n_int + BYTES[dom][1] * n_pml
     peak, peak_kind = measured_peak()
     achieved = alg / (per[dom] / 1e3) / 1e9
-    traffic = None
+    traffic = alg * TRAFFIC_RATIO[dom] if kernel == sgfd.KERNEL_AUTO or args.kernel == "zmarch" else None
     roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
+            "traffic_source": "ncu dram bytes / algorithmic bytes of the z-march kernels on the 216^3 + 20 PML "
+                              "cube, times this launch's algorithmic bytes" if traffic else None,
             "alg_bytes_per_launch": alg, "avg_launch_ms": per[dom],
             "step_frac": (120 * n_int + 276 * n_pml) / (ms / K / 1e3) / 1e9 / peak,
             "kernel_ms": per}
