@@ -101,7 +101,14 @@ typedef enum sgfd_quirks {
     SGFD_QUIRKS_FIXED = 1
 } sgfd_quirks;
 
-/* Wavefield storage type in HBM (arithmetic is always FP32). */
+/* Wavefield storage type in HBM (arithmetic is always FP32).  BF16 / F16
+ * store every wavefield and its PML splits as 16-bit values with a per-field
+ * power-of-two scale 2^e (value = float(stored) * 2^e; binary16 saturates at
+ * +-65504), halving the wavefield bytes.  The scales are re-chosen after steps
+ * 0, 1, 3, 7, 15, 31, 49 and then every 50 steps from the largest magnitude
+ * each field wrote in that step, so that it is stored near 2^7.  16-bit storage
+ * runs on the per-cell kernel family (SGFD_KERNEL_ZMARCH is rejected), and
+ * the per-step audit (sgfd_set_audit) is not available with it. */
 typedef enum sgfd_storage {
     SGFD_STORE_F32 = 0,
     SGFD_STORE_BF16 = 1,
@@ -317,7 +324,8 @@ int sgfd_get_audit(sgfd_solver *h, double *out);
  * handle is created with the same configuration, given the same inputs, then
  * loads the checkpoint and continues with step it_next.  Layout: a 128-byte
  * header (magic "SGFDCKP1", version 1, grid, pml, receivers x steps, it_next,
- * physics, payload size, 64-bit checksum), then the payload: 9 x nx*ny*nz
+ * physics, payload size, 64-bit checksum, storage type and the 16-bit field
+ * scales), then the payload: 9 x nx*ny*nz
  * float32 fields (x fastest), 24 x npml float32 splits, nt x nrec float32
  * traces (time-major).  Loading checks the grid, physics and checksum; a
  * checksum or length failure zeroes the state (as sgfd_reset) and returns

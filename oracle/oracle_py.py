@@ -58,6 +58,8 @@ def lib():
         L.sgo_run.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, dp]
         L.sgo_get_traces.argtypes = [ctypes.c_void_p, dp]
         L.sgo_get_field.argtypes = [ctypes.c_void_p, ctypes.c_int, dp]
+        L.sgo_round16.argtypes = [ctypes.c_int, fp, fp, ctypes.c_int64]
+        L.sgo_scale_exponents.argtypes = [ctypes.c_void_p, ip]
         L.sgo_ricker_ref.restype = ctypes.c_float
         L.sgo_ricker_ref.argtypes = [ctypes.c_float, ctypes.c_float, ctypes.c_int]
         _lib = L
@@ -70,6 +72,14 @@ def _ptr(a, ctype):
 
 def set_threads(n: int) -> int:
     return lib().sgo_set_threads(int(n))
+
+
+def round16(storage: int, x) -> np.ndarray:
+    """The oracle's 16-bit rounding (storage 1 = bfloat16, 2 = binary16), as float32."""
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    out = np.empty_like(x)
+    lib().sgo_round16(int(storage), _ptr(x, ctypes.c_float), _ptr(out, ctypes.c_float), x.size)
+    return out
 
 
 def ricker_ref(f0: float, dt: float, nt: int) -> np.ndarray:
@@ -138,6 +148,12 @@ class Oracle:
     def traces(self) -> np.ndarray:
         out = np.zeros((self.nrec, self.nt), dtype=np.float64)
         lib().sgo_get_traces(self.h, _ptr(out, ctypes.c_double))
+        return out
+
+    def scale_exponents(self) -> np.ndarray:
+        """Per-field scale exponents of the 16-bit storage emulation."""
+        out = np.zeros(9, dtype=np.int32)
+        lib().sgo_scale_exponents(self.h, _ptr(out, ctypes.c_int32))
         return out
 
     def field(self, fid: int) -> np.ndarray:

@@ -72,6 +72,56 @@ enum {
 
 template <typename T> inline T fma_(T a, T b, T c) { return std::fma(a, b, c); }
 
+// ---- 16-bit wavefield storage (sgfd_config.storage BF16 / F16) -------------
+// The product stores each wavefield (and its PML splits) as 16-bit values h
+// with a per-field power-of-two scale 2^e: stored = RN16(v * 2^-e), read back
+// as float(h) * 2^e.  Arithmetic stays FP32.  These helpers restate that
+// rounding on the CPU: round to nearest, ties to even, binary16 with
+// subnormals and overflow to infinity, bfloat16 as the upper half of an
+// FP32 word.
+
+// v rounded to the nearest binary16 value, returned as float (IEEE: values
+// from 65520 up overflow to infinity).
+inline float rn_f16(float v) {
+    if (!std::isfinite(v) || v == 0.0f) return v;
+    const float av = std::fabs(v);
+    if (av >= 65520.0f) return std::copysign(INFINITY, v);   // past the midpoint 65504 .. 2^16
+    int e;
+    std::frexp(av, &e);                       // av = m 2^e, m in [0.5, 1)
+    const int ex = std::max(e - 1, -14);      // binade (subnormals share 2^-14's quantum)
+    const float ulp = std::ldexp(1.0f, ex - 10);
+    const float r = std::nearbyint(av / ulp) * ulp;   // av / ulp is exact; ties to even
+    return std::copysign(r, v);
+}
+// v rounded to the nearest bfloat16 value (ties to even), returned as float.
+inline float rn_bf16(float v) {
+    if (!std::isfinite(v)) return v;
+    uint32_t u;
+    std::memcpy(&u, &v, 4);
+    u = (u + 0x7FFFu + ((u >> 16) & 1u)) & 0xFFFF0000u;
+    float r;
+    std::memcpy(&r, &u, 4);
+    return r;
+}
+// The storage rounding: binary16 saturates at +-65504 (a field outgrowing its
+// scale between two rescales is clipped, not turned into infinity).
+inline float store16(int storage, float w) {
+    if (storage == SGFD_STORE_F16) return rn_f16(std::fmin(std::fmax(w, -65504.0f), 65504.0f));
+    return rn_bf16(w);
+}
+// Steps after which the scales are re-chosen: it + 1 a power of two up to
+// kRescaleEvery (the first steps of a run grow fast from zero), then every
+// kRescaleEvery steps.  kScaleHead: the largest stored magnitude is put in
+// [2^(kScaleHead-1), 2^kScaleHead), 256x below the binary16 maximum (room
+// for growth until the next rescale) and 2^22 above its smallest normal.
+constexpr int kRescaleEvery = 50;
+constexpr int kScaleHead = 8;
+inline bool rescale_step(int it) {
+    const int n = it + 1;
+    if (n <= 0) return false;
+    return (n <= kRescaleEvery && (n & (n - 1)) == 0) || n % kRescaleEvery == 0;
+}
+
 struct Receiver { int x, y, z, comp; };
 
 template <typename T>
@@ -97,6 +147,10 @@ struct Oracle {
     T q_logr;        // 0.5*dt*3*ln(1/R)/(2p)
     T q_refcpu[3];   // 0.5*dt*log10(1/R)*3.4*V/(p*d_axis)
     T qf[3];         // FAST: q constant pre-divided by the cell size
+    // 16-bit storage emulation (FP32 oracle only): per-field scale exponents
+    int storage = SGFD_STORE_F32;
+    int scale_e[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    T pending_max[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};   // largest value written before rounding
 
     explicit Oracle(const sgfd_config &c_) : cfg(c_) {
         nx = cfg.nx; ny = cfg.ny; nz = cfg.nz;
@@ -126,6 +180,61 @@ struct Oracle {
     }
 
     int64_t idx(int x, int y, int z) const { return x + (int64_t)y * sy + (int64_t)z * sz; }
+
+    // Field each split belongs to (its scale group).
+    static int split_field(int k) {
+        static const int g[N_SPLIT] = {VX, VX, VX, VY, VY, VY, VZ, VZ, VZ, TXX, TXX, TXX, TYY, TYY, TYY,
+                                       TZZ, TZZ, TZZ, TXY, TXY, TXZ, TXZ, TYZ, TYZ};
+        return g[k];
+    }
+    // Stored value of v under field g's scale.
+    T quant(T v, int g) const {
+        const float sc = std::ldexp(1.0f, scale_e[g]), inv = std::ldexp(1.0f, -scale_e[g]);
+        return (T)(store16(storage, (float)v * inv) * sc);
+    }
+    // Round fields [f0, f1] and their splits, just written by an update, to
+    // the stored values.  On rescale steps first note each field's largest
+    // written magnitude before rounding (a field whose values underflow the
+    // current scale still gets a scale that fits them; the source injection
+    // counts too, so that a run starting from zero fields gets going).
+    void quantize_fields(int f0, int f1, bool track) {
+        if (storage == SGFD_STORE_F32) return;
+        if (track) {
+            for (int g = f0; g <= f1; ++g) {
+                T mx = 0;
+                for (int64_t i = 0; i < n; ++i) mx = std::max(mx, (T)std::fabs(f[g][i]));
+                for (int k = 0; k < N_SPLIT; ++k)
+                    if (split_field(k) == g)
+                        for (int64_t i = 0; i < n; ++i) mx = std::max(mx, (T)std::fabs(split[k][i]));
+                pending_max[g] = std::max(pending_max[g], mx);
+            }
+        }
+        for (int g = f0; g <= f1; ++g) {
+#pragma omp parallel for schedule(static)
+            for (int64_t i = 0; i < n; ++i) f[g][i] = quant(f[g][i], g);
+        }
+        for (int k = 0; k < N_SPLIT; ++k) {
+            const int g = split_field(k);
+            if (g < f0 || g > f1) continue;
+#pragma omp parallel for schedule(static)
+            for (int64_t i = 0; i < n; ++i) split[k][i] = quant(split[k][i], g);
+        }
+    }
+    // Re-choose every field's scale so that the largest magnitude written in
+    // this step lands in [2^(kScaleHead-1), 2^kScaleHead), then re-round the
+    // stored values to the new scales.  Fields that wrote only zeros keep
+    // their scale.
+    void rescale() {
+        for (int g = 0; g < 9; ++g) {
+            const T mx = pending_max[g];
+            pending_max[g] = 0;
+            if (!(mx > 0) || !std::isfinite((float)mx)) continue;
+            int e;
+            std::frexp((float)mx, &e);            // mx in [2^(e-1), 2^e)
+            scale_e[g] = std::min(100, std::max(-100, e - kScaleHead));
+        }
+        quantize_fields(0, 8, false);
+    }
 
     // Forward staggered difference along `axis` (0,1,2 = x,y,z), stride s:
     // sum c_i (f[+1+i] - f[-i]) / d   (e.g. OPT/ElasticWaveEquation.cu:246, 250).
@@ -181,13 +290,18 @@ struct Oracle {
         if (fast) pp = (T)1 / pp;
     }
 
-    void inject(T s) {
+    void inject(T s, bool track) {
         if (src_x < 0) return;
         int64_t ci = idx(src_x, src_y, src_z);
         T v = (dt * dt) * s;   // deltaT * deltaT * sourceValue (OPT/ElasticWaveEquation.cu:213)
         f[TXX][ci] = f[TXX][ci] + v;
         f[TYY][ci] = f[TYY][ci] + v;
         f[TZZ][ci] = f[TZZ][ci] + v;
+        if (storage != SGFD_STORE_F32)
+            for (int g = TXX; g <= TZZ; ++g) {
+                if (track) pending_max[g] = std::max(pending_max[g], (T)std::fabs(f[g][ci]));
+                f[g][ci] = quant(f[g][ci], g);
+            }
     }
 
     // One split update: damped -> (m*s + A*B)/p (FAST: times RN(1/p)); undamped -> s + A*B.
@@ -410,13 +524,17 @@ struct Oracle {
     }
 
     void step(int it, T s) {
-        inject(s);
+        const bool rs = storage != SGFD_STORE_F32 && rescale_step(it);
+        inject(s, rs);
         sweep([this](int x, int y, int z, int kx, int ky, int kz) { velocity_cell(x, y, z, kx, ky, kz); },
               [this](int y, int z, int x0, int x1) { velocity_row(y, z, x0, x1); });
+        quantize_fields(VX, VZ, rs);
         record(true, it);
         sweep([this](int x, int y, int z, int kx, int ky, int kz) { stress_cell(x, y, z, kx, ky, kz); },
               [this](int y, int z, int x0, int x1) { stress_row(y, z, x0, x1); });
+        quantize_fields(TXX, TYZ, rs);
         record(false, it);
+        if (rs) rescale();
     }
 };
 
@@ -444,7 +562,10 @@ void *sgo_create(const sgfd_config *cfg, int fp64) {
     auto *h = new Handle();
     h->fp64 = fp64;
     if (fp64) h->f64.reset(new Oracle<double>(*cfg));
-    else h->f32.reset(new Oracle<float>(*cfg));
+    else {
+        h->f32.reset(new Oracle<float>(*cfg));
+        h->f32->storage = cfg->storage;   // 16-bit storage emulated in FP32 runs only
+    }
     return h;
 }
 
@@ -521,6 +642,19 @@ int sgo_get_field(void *p, int field, double *out) {
         for (int64_t i = 0; i < o.n; ++i) out[i] = (double)o.f[field][i];
         return 0;
     });
+}
+
+// The 16-bit roundings of the storage emulation, for checking against numpy.
+void sgo_round16(int storage, const float *in, float *out, int64_t n) {
+    for (int64_t i = 0; i < n; ++i) out[i] = storage == SGFD_STORE_F16 ? rn_f16(in[i]) : rn_bf16(in[i]);
+}
+
+// Scale exponents of the 9 fields (16-bit storage emulation).
+int sgo_scale_exponents(void *p, int *out) {
+    auto *h = static_cast<Handle *>(p);
+    if (!h || h->fp64) return SGFD_ERR_INVALID;
+    for (int g = 0; g < 9; ++g) out[g] = h->f32->scale_e[g];
+    return 0;
 }
 
 // Reference Ricker wavelet (OPT/ElasticWaveEquation.cu:184-189), evaluated in

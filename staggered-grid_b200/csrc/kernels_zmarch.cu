@@ -166,44 +166,55 @@ __device__ __forceinline__ unsigned char *align_smem(unsigned char *p) {
 // ---------------------------------------------------------------------------
 
 constexpr int kWarps = NT / 32;
+
+// One TMA box of a stage: tensor map, destination offset in the stage, x and
+// y of its origin and its plane relative to the staged plane.  Each warp's
+// boxes are worked out once per CTA and kept in shared memory, so that the
+// per-plane issue is a few loads and the copies themselves.
+struct TmaBox {
+    const CUtensorMap *map;
+    uint32_t off;
+    int x, y, dz;
+};
+constexpr int kMaxBoxesPerWarp = 3;
+
+__device__ __forceinline__ void issue_boxes(const TmaBox *b, int n, unsigned char *st, uint64_t *bar, int gz) {
+    for (int j = 0; j < n; ++j) tma3(st + b[j].off, b[j].map, b[j].x, b[j].y, gz + b[j].dz, bar);
+}
 constexpr int kVelBoxes = 13;
 constexpr int kStrBoxes = 17;
 
-// Box q of the velocity stage of GRID plane gz.
+// Box q of the velocity stage.
 template <int TY>
-__device__ __forceinline__ void vel_box(const VelMaps &mp, unsigned char *st, uint64_t *bar, const Tile &t, int gz,
-                                        int q) {
+__device__ __forceinline__ TmaBox vel_box(const VelMaps &mp, const Tile &t, int q) {
     using L = VelL<TY>;
-    constexpr int OB = al128(W32 * TY * 4);
+    constexpr uint32_t OB = al128(W32 * TY * 4);
     switch (q) {
-    case 0: tma3(st + L::SXX, &mp.sxx, t.xd - 8, t.gy0, gz, bar); break;
-    case 1: tma3(st + L::SYY, &mp.syy, t.xd, t.gy0 - 5, gz, bar); break;
-    case 2: tma3(st + L::SXY, &mp.sxy, t.xd - 8, t.gy0 - 5, gz, bar); break;
-    case 3: tma3(st + L::SXZ, &mp.sxz, t.xd - 8, t.gy0, gz, bar); break;
-    case 4: tma3(st + L::SYZ, &mp.syz, t.xd, t.gy0 - 5, gz, bar); break;
-    case 5: tma3(st + L::B, &mp.b, t.xd, t.gy0, gz, bar); break;
-    case 6: tma3(st + L::LXZ, &mp.sxz_c, t.xd, t.gy0, gz + 4, bar); break;
-    case 7: tma3(st + L::LYZ, &mp.syz_c, t.xd, t.gy0, gz + 4, bar); break;
-    case 8: tma3(st + L::LZZ, &mp.szz_c, t.xd, t.gy0, gz + 5, bar); break;
-    case 9: tma3(st + L::LB, &mp.b_c, t.xd, t.gy0, gz + 1, bar); break;
-    case 10: tma3(st + L::OV, &mp.own[0], t.xd, t.gy0, gz, bar); break;
-    case 11: tma3(st + L::OV + OB, &mp.own[1], t.xd, t.gy0, gz, bar); break;
-    default: tma3(st + L::OV + 2 * OB, &mp.own[2], t.xd, t.gy0, gz, bar); break;
+    case 0: return {&mp.sxx, L::SXX, t.xd - 8, t.gy0, 0};
+    case 1: return {&mp.syy, L::SYY, t.xd, t.gy0 - 5, 0};
+    case 2: return {&mp.sxy, L::SXY, t.xd - 8, t.gy0 - 5, 0};
+    case 3: return {&mp.sxz, L::SXZ, t.xd - 8, t.gy0, 0};
+    case 4: return {&mp.syz, L::SYZ, t.xd, t.gy0 - 5, 0};
+    case 5: return {&mp.b, L::B, t.xd, t.gy0, 0};
+    case 6: return {&mp.sxz_c, L::LXZ, t.xd, t.gy0, 4};
+    case 7: return {&mp.syz_c, L::LYZ, t.xd, t.gy0, 4};
+    case 8: return {&mp.szz_c, L::LZZ, t.xd, t.gy0, 5};
+    case 9: return {&mp.b_c, L::LB, t.xd, t.gy0, 1};
+    case 10: return {&mp.own[0], L::OV, t.xd, t.gy0, 0};
+    case 11: return {&mp.own[1], L::OV + OB, t.xd, t.gy0, 0};
+    default: return {&mp.own[2], L::OV + 2 * OB, t.xd, t.gy0, 0};
     }
 }
 
-// Stage the velocity inputs of computed plane cz.  The issue is shared so
-// that no warp falls behind the others: lane 0 of warp w issues boxes w,
-// w + 8, ..., and thread 0 also arms the stage's barrier with its bytes (the
-// barrier's phase cannot complete before that arrival, whichever copy lands
-// first).  Called by lane 0 of every warp.
+// Stage the velocity inputs of computed plane cz from this warp's boxes
+// (boxes w, w + 8, ... of the stage for warp w; called by lane 0 of every
+// warp).  Thread 0 also arms the stage's barrier with all of the stage's
+// bytes; the barrier's phase cannot complete before that arrival, whichever
+// copy lands first.
 template <int TY>
-__device__ __forceinline__ void vel_issue(const VelMaps &mp, unsigned char *st, uint64_t *bar, const Tile &t, int cz,
-                                          int warp) {
-    using L = VelL<TY>;
-    const int gz = cz + kHalo;
-    if (warp == 0) mbar_expect_tx(bar, L::TXB);
-    for (int q = warp; q < kVelBoxes; q += kWarps) vel_box<TY>(mp, st, bar, t, gz, q);
+__device__ __forceinline__ void vel_issue(const TmaBox *b, int n, unsigned char *st, uint64_t *bar, int cz, int warp) {
+    if (warp == 0) mbar_expect_tx(bar, VelL<TY>::TXB);
+    issue_boxes(b, n, st, bar, cz + kHalo);
 }
 
 template <bool FAST, int CELLS>
@@ -224,9 +235,17 @@ k_velocity_zmarch(const __grid_constant__ VelMaps mp, const __grid_constant__ Mo
     }
     __syncthreads();
     const int warp = tid >> 5;
-    if (lx == 0)
-        for (int s = 0; s < S && t.zs + s < t.ze; ++s) vel_issue<TY>(mp, smem + s * L::STAGE, &bar[s], t, t.zs + s, warp);
+    __shared__ TmaBox boxes[kWarps][kMaxBoxesPerWarp];
+    const TmaBox *mybox = boxes[warp];
+    const int nbox = (kVelBoxes - warp + kWarps - 1) / kWarps;
+    if (lx == 0) {
+        for (int j = 0; j < nbox; ++j) boxes[warp][j] = vel_box<TY>(mp, t, warp + j * kWarps);
+        for (int s = 0; s < S && t.zs + s < t.ze; ++s)
+            vel_issue<TY>(mybox, nbox, smem + s * L::STAGE, &bar[s], t.zs + s, warp);
+    }
     int issued_end = min(t.zs + S, t.ze);   // planes [zs, issued_end) issued
+    int stage = 0;                          // stage of plane cz, and the parity of its barrier
+    uint32_t parity = 0;
 
     const int it = step_index(sr, it_arg);
     const float inj = ph.inj_dt2 * ((use_wavelet && sr.wavelet) ? sr.wavelet[it] : src_value);
@@ -286,8 +305,7 @@ k_velocity_zmarch(const __grid_constant__ VelMaps mp, const __grid_constant__ Mo
     // false when the block votes to abort.
     auto plane = [&](auto gen_tag) -> bool {
         constexpr bool GEN = decltype(gen_tag)::value;
-        const int k = cz - t.zs;
-        const int s = k % S;
+        const int s = stage;
         unsigned char *st = smem + s * L::STAGE;
         const int gz = cz + kHalo;
         const int kz = band(gz, m.nz, m.pml);
@@ -312,7 +330,7 @@ k_velocity_zmarch(const __grid_constant__ VelMaps mp, const __grid_constant__ Mo
             }
         }
 
-        if (!mbar_wait(&bar[s], (uint32_t)((k / S) & 1))) failed = true;
+        if (!mbar_wait(&bar[s], parity)) failed = true;
 
         // source patch of the staged copies (uniform branch)
         if (GEN && src_near && (gz == sz || gz + 5 == sz)) {
@@ -467,9 +485,13 @@ k_velocity_zmarch(const __grid_constant__ VelMaps mp, const __grid_constant__ Mo
         if (cz + S < t.ze) {
             if (lx == 0) {
                 fence_proxy_async();
-                vel_issue<TY>(mp, st, &bar[s], t, cz + S, warp);
+                vel_issue<TY>(mybox, nbox, st, &bar[s], cz + S, warp);
             }
             issued_end = cz + S + 1;
+        }
+        if (++stage == S) {
+            stage = 0;
+            parity ^= 1u;
         }
         return true;
     };
@@ -491,41 +513,27 @@ k_velocity_zmarch(const __grid_constant__ VelMaps mp, const __grid_constant__ Mo
 // stress update
 // ---------------------------------------------------------------------------
 
-// Box q of the stress stage of GRID plane gz.
+// Box q of the stress stage.
 template <int TY>
-__device__ __forceinline__ void str_box(const StrMaps &mp, unsigned char *st, uint64_t *bar, const Tile &t, int gz,
-                                        int q) {
+__device__ __forceinline__ TmaBox str_box(const StrMaps &mp, const Tile &t, int q) {
     using L = StrL<TY>;
-    constexpr int OB = al128(W32 * TY * 4);
+    constexpr uint32_t OB = al128(W32 * TY * 4);
     switch (q) {
-    case 0: tma3(st + L::VX, &mp.vx, t.xd - 8, t.gy0 - 5, gz, bar); break;
-    case 1: tma3(st + L::VY, &mp.vy, t.xd - 8, t.gy0 - 5, gz, bar); break;
-    case 2: tma3(st + L::VZ, &mp.vz, t.xd - 8, t.gy0 - 5, gz, bar); break;
-    case 3: tma3(st + L::LX, &mp.vx_c, t.xd, t.gy0, gz + 5, bar); break;
-    case 4: tma3(st + L::LY, &mp.vy_c, t.xd, t.gy0, gz + 5, bar); break;
-    case 5: tma3(st + L::LZ, &mp.vz_c, t.xd, t.gy0, gz + 4, bar); break;
-    case 6: tma3(st + L::OWN, &mp.own[0], t.xd, t.gy0, gz, bar); break;
-    case 7: tma3(st + L::OWN + OB, &mp.own[1], t.xd, t.gy0, gz, bar); break;
-    case 8: tma3(st + L::OWN + 2 * OB, &mp.own[2], t.xd, t.gy0, gz, bar); break;
-    case 9: tma3(st + L::OWN + 3 * OB, &mp.own[3], t.xd, t.gy0, gz, bar); break;
-    case 10: tma3(st + L::OWN + 4 * OB, &mp.own[4], t.xd, t.gy0, gz, bar); break;
-    case 11: tma3(st + L::OWN + 5 * OB, &mp.own[5], t.xd, t.gy0, gz, bar); break;
-    case 12: tma3(st + L::OWN + 6 * OB, &mp.own[6], t.xd, t.gy0, gz, bar); break;
-    case 13: tma3(st + L::OWN + 7 * OB, &mp.own[7], t.xd, t.gy0, gz, bar); break;
-    case 14: tma3(st + L::OWN + 8 * OB, &mp.own[8], t.xd, t.gy0, gz, bar); break;
-    case 15: tma3(st + L::OWN + 9 * OB, &mp.own[9], t.xd, t.gy0, gz, bar); break;
-    default: tma3(st + L::OWN + 10 * OB, &mp.own[10], t.xd, t.gy0, gz, bar); break;
+    case 0: return {&mp.vx, L::VX, t.xd - 8, t.gy0 - 5, 0};
+    case 1: return {&mp.vy, L::VY, t.xd - 8, t.gy0 - 5, 0};
+    case 2: return {&mp.vz, L::VZ, t.xd - 8, t.gy0 - 5, 0};
+    case 3: return {&mp.vx_c, L::LX, t.xd, t.gy0, 5};
+    case 4: return {&mp.vy_c, L::LY, t.xd, t.gy0, 5};
+    case 5: return {&mp.vz_c, L::LZ, t.xd, t.gy0, 4};
+    default: return {&mp.own[q - 6], L::OWN + (uint32_t)(q - 6) * OB, t.xd, t.gy0, 0};
     }
 }
 
-// Stage the stress inputs of computed plane cz, issue shared as in vel_issue.
+// Stage the stress inputs of computed plane cz, as vel_issue.
 template <int TY>
-__device__ __forceinline__ void str_issue(const StrMaps &mp, unsigned char *st, uint64_t *bar, const Tile &t, int cz,
-                                          int warp) {
-    using L = StrL<TY>;
-    const int gz = cz + kHalo;
-    if (warp == 0) mbar_expect_tx(bar, L::TXB);
-    for (int q = warp; q < kStrBoxes; q += kWarps) str_box<TY>(mp, st, bar, t, gz, q);
+__device__ __forceinline__ void str_issue(const TmaBox *b, int n, unsigned char *st, uint64_t *bar, int cz, int warp) {
+    if (warp == 0) mbar_expect_tx(bar, StrL<TY>::TXB);
+    issue_boxes(b, n, st, bar, cz + kHalo);
 }
 
 template <bool FAST, int CELLS>
@@ -546,9 +554,17 @@ k_stress_zmarch(const __grid_constant__ StrMaps mp, const __grid_constant__ Mode
     }
     __syncthreads();
     const int warp = tid >> 5;
-    if (lx == 0)
-        for (int s = 0; s < S && t.zs + s < t.ze; ++s) str_issue<TY>(mp, smem + s * L::STAGE, &bar[s], t, t.zs + s, warp);
+    __shared__ TmaBox boxes[kWarps][kMaxBoxesPerWarp];
+    const TmaBox *mybox = boxes[warp];
+    const int nbox = (kStrBoxes - warp + kWarps - 1) / kWarps;
+    if (lx == 0) {
+        for (int j = 0; j < nbox; ++j) boxes[warp][j] = str_box<TY>(mp, t, warp + j * kWarps);
+        for (int s = 0; s < S && t.zs + s < t.ze; ++s)
+            str_issue<TY>(mybox, nbox, smem + s * L::STAGE, &bar[s], t.zs + s, warp);
+    }
     int issued_end = min(t.zs + S, t.ze);   // planes [zs, issued_end) issued
+    int stage = 0;                          // stage of plane cz, and the parity of its barrier
+    uint32_t parity = 0;
 
     const int it = step_index(sr, it_arg);
     const float inj = ph.inj_dt2 * ((use_wavelet && sr.wavelet) ? sr.wavelet[it] : src_value);
@@ -599,8 +615,7 @@ k_stress_zmarch(const __grid_constant__ StrMaps mp, const __grid_constant__ Mode
     // false when the block votes to abort.
     auto plane = [&](auto gen_tag) -> bool {
         constexpr bool GEN = decltype(gen_tag)::value;
-        const int k = cz - t.zs;
-        const int s = k % S;
+        const int s = stage;
         unsigned char *st = smem + s * L::STAGE;
         const int gz = cz + kHalo;
         const int kz = band(gz, m.nz, m.pml);
@@ -610,7 +625,7 @@ k_stress_zmarch(const __grid_constant__ StrMaps mp, const __grid_constant__ Mode
         // PML cells: splits and the buoyancy of the damping, loaded before the
         // stage wait so that their latency overlaps the wait and the stencil
 
-        if (!mbar_wait(&bar[s], (uint32_t)((k / S) & 1))) failed = true;
+        if (!mbar_wait(&bar[s], parity)) failed = true;
 
         const float *svx = reinterpret_cast<const float *>(st + L::VX);
         const float *svy = reinterpret_cast<const float *>(st + L::VY);
@@ -758,9 +773,13 @@ k_stress_zmarch(const __grid_constant__ StrMaps mp, const __grid_constant__ Mode
         if (cz + S < t.ze) {
             if (lx == 0) {
                 fence_proxy_async();
-                str_issue<TY>(mp, st, &bar[s], t, cz + S, warp);
+                str_issue<TY>(mybox, nbox, st, &bar[s], cz + S, warp);
             }
             issued_end = cz + S + 1;
+        }
+        if (++stage == S) {
+            stage = 0;
+            parity ^= 1u;
         }
         return true;
     };

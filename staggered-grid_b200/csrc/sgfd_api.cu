@@ -64,9 +64,51 @@ int check_device_error(sgfd_solver *h) {
     return SGFD_OK;
 }
 
+int sync_views(sgfd_solver *h) {
+    if (h->storage == SGFD_STORE_F32) return SGFD_OK;
+    SG_CUDA(h, half_to_views(h->m, h->hs, h->stream), "16-bit fields to FP32");
+    return SGFD_OK;
+}
+
+int sync_from_views(sgfd_solver *h) {
+    if (h->storage == SGFD_STORE_F32) return SGFD_OK;
+    SG_CUDA(h, half_from_views(h->m, h->hs, h->stream), "FP32 fields to 16-bit");
+    return SGFD_OK;
+}
+
+int set_scale_exponents(sgfd_solver *h, const int *e) {
+    if (h->storage == SGFD_STORE_F32) return SGFD_OK;
+    struct { int e[9], e_new[9]; float sc[9], inv[9]; unsigned amax[9]; } st{};
+    for (int g = 0; g < 9; ++g) {
+        st.e[g] = st.e_new[g] = e[g];
+        st.sc[g] = std::ldexp(1.0f, e[g]);
+        st.inv[g] = std::ldexp(1.0f, -e[g]);
+    }
+    SG_CUDA(h, cudaMemcpyAsync(h->hstate, &st, sizeof st, cudaMemcpyHostToDevice, h->stream), "scale state");
+    SG_CUDA(h, cudaStreamSynchronize(h->stream), "scale state");
+    return SGFD_OK;
+}
+
+int reset_scales(sgfd_solver *h) {
+    const int zero[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    return set_scale_exponents(h, zero);
+}
+
+int get_scale_exponents(sgfd_solver *h, int *e) {
+    if (h->storage == SGFD_STORE_F32) {
+        for (int g = 0; g < 9; ++g) e[g] = 0;
+        return SGFD_OK;
+    }
+    SG_CUDA(h, cudaMemcpyAsync(e, h->hs.e, 9 * sizeof(int), cudaMemcpyDeviceToHost, h->stream), "scale state");
+    SG_CUDA(h, cudaStreamSynchronize(h->stream), "scale state");
+    return SGFD_OK;
+}
+
 cudaError_t dispatch_on(sgfd_solver *h, const SourceRec &sr, cudaStream_t s, int it, float value,
                         bool use_wavelet, cudaEvent_t *ev) {
-    cudaError_t e = h->kernel == SGFD_KERNEL_ZMARCH
+    cudaError_t e = h->storage != SGFD_STORE_F32
+                        ? half_step(h->m, h->ph, sr, h->hs, it, value, use_wavelet, s, ev)
+                    : h->kernel == SGFD_KERNEL_ZMARCH
                         ? zmarch_step(h->m, h->ph, sr, h->zg, h->vm, h->sm, it, value, use_wavelet, s, ev)
                         : simple_step(h->m, h->ph, sr, it, value, use_wavelet, s, ev);
     if (e == cudaSuccess && h->audit_every > 0) {
@@ -310,8 +352,10 @@ int sgfd_create(const sgfd_config *cfg, sgfd_solver **out) {
         return fail(nullptr, SGFD_ERR_INVALID, "damping_R must be in (0, 1)");
     if (c.quirks != SGFD_QUIRKS_REF && c.quirks != SGFD_QUIRKS_FIXED)
         return fail(nullptr, SGFD_ERR_INVALID, "unknown quirks mode %d", c.quirks);
-    if (c.storage != SGFD_STORE_F32)
+    if (c.storage != SGFD_STORE_F32 && c.storage != SGFD_STORE_BF16 && c.storage != SGFD_STORE_F16)
         return fail(nullptr, SGFD_ERR_UNSUPPORTED, "storage type %d is not built into this library", c.storage);
+    if (c.storage != SGFD_STORE_F32 && c.kernel == SGFD_KERNEL_ZMARCH)
+        return fail(nullptr, SGFD_ERR_UNSUPPORTED, "16-bit storage runs on the per-cell kernels only");
     if (c.kernel != SGFD_KERNEL_AUTO && c.kernel != SGFD_KERNEL_SIMPLE && c.kernel != SGFD_KERNEL_ZMARCH)
         return fail(nullptr, SGFD_ERR_UNSUPPORTED, "kernel family %d is not built into this library", c.kernel);
     const int64_t cells = (int64_t)c.nx * c.ny * c.nz;
@@ -379,7 +423,35 @@ int sgfd_create(const sgfd_config *cfg, sgfd_solver **out) {
     h->sr.nrec = 0;
 
     // kernel family
-    if (c.kernel != SGFD_KERNEL_SIMPLE && zmarch_supported(m)) {
+    // 16-bit storage: the stored fields and splits and their scale state
+    if (c.storage != SGFD_STORE_F32) {
+        h->storage = c.storage;
+        const size_t a16 = round_up((size_t)m.plane * m.nz * 2, 256);
+        const size_t s16 = round_up((size_t)kNumSplit * m.npml * 2, 256);
+        e = cudaMalloc(&h->h16_pool, a16 * 9 + s16);
+        if (e == cudaSuccess) e = cudaMalloc(&h->hstate, 64 * sizeof(int));
+        if (e == cudaSuccess) e = cudaMemsetAsync(h->h16_pool, 0, a16 * 9 + s16, h->stream);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            int r = fail(nullptr, SGFD_ERR_ALLOC, "16-bit storage allocation failed");
+            sgfd_destroy(h);
+            return r;
+        }
+        HalfState &hs = h->hs;
+        for (int k = 0; k < 9; ++k) hs.f[k] = reinterpret_cast<uint16_t *>(h->h16_pool + k * a16) + kXOff;
+        hs.split = reinterpret_cast<uint16_t *>(h->h16_pool + 9 * a16);
+        int *hst = static_cast<int *>(h->hstate);
+        hs.e = hst;
+        hs.e_new = hst + 9;
+        hs.sc = reinterpret_cast<float *>(hst + 18);
+        hs.inv = reinterpret_cast<float *>(hst + 27);
+        hs.amax = reinterpret_cast<unsigned *>(hst + 36);
+        hs.storage = c.storage;
+        int r = reset_scales(h);
+        if (r) { g_error = h->err; sgfd_destroy(h); return r; }
+    }
+
+    if (c.kernel != SGFD_KERNEL_SIMPLE && c.storage == SGFD_STORE_F32 && zmarch_supported(m)) {
         h->zg.cells = 1;
         e = zmarch_prepare(m, h->zg.cells, &h->vm, &h->sm);
         if (e == cudaSuccess) e = cudaMalloc(&h->dev_err, sizeof(int));
@@ -416,6 +488,8 @@ void sgfd_destroy(sgfd_solver *h) {
     cudaFree(h->zrec_list);
     cudaFree(h->zrec_idx);
     cudaFree(h->dev_err);
+    cudaFree(h->h16_pool);
+    cudaFree(h->hstate);
     cudaFree(h->audit);
     cudaFree(h->audit_hist);
     release_graph(h);
@@ -649,6 +723,13 @@ int sgfd_reset(sgfd_solver *h) {
     if (h->audit_hist)
         SG_CUDA(h, cudaMemsetAsync(h->audit_hist, 0, (size_t)h->audit_count * 2 * sizeof(double), h->stream),
                 "reset audit history");
+    if (h->h16_pool) {
+        const size_t a16 = round_up((size_t)m.plane * m.nz * 2, 256);
+        const size_t s16 = round_up((size_t)kNumSplit * m.npml * 2, 256);
+        SG_CUDA(h, cudaMemsetAsync(h->h16_pool, 0, a16 * 9 + s16, h->stream), "reset 16-bit fields");
+        const int r = reset_scales(h);
+        if (r) return r;
+    }
     SG_CUDA(h, cudaStreamSynchronize(h->stream), "reset");
     return SGFD_OK;
 }
@@ -722,6 +803,8 @@ int sgfd_get_field(sgfd_solver *h, int32_t field, float *out) {
     if (r) return r;
     if (!out) return fail(h, SGFD_ERR_INVALID, "null output");
     if (field < 0 || field >= SGFD_NFIELDS) return fail(h, SGFD_ERR_INVALID, "bad field id %d", field);
+    r = sync_views(h);
+    if (r) return r;
     return download(h, h->m.f[field], out);
 }
 
@@ -741,6 +824,7 @@ int sgfd_energy(sgfd_solver *h, int32_t region, double *kinetic, double *strain)
     if (region < SGFD_REGION_COMPUTED || region > SGFD_REGION_PML)
         return fail(h, SGFD_ERR_INVALID, "bad region %d", region);
     r = ensure_audit_scratch(h);
+    if (r == SGFD_OK) r = sync_views(h);
     if (r) return r;
     double *out = h->audit + 2 * h->audit_blocks;
     SG_CUDA(h, launch_energy(h->m, h->ph, region, h->audit, h->audit_blocks, out, h->stream), "energy audit");
@@ -761,6 +845,8 @@ int sgfd_set_audit(sgfd_solver *h, int32_t every, int32_t region, int32_t nsampl
     if (region < SGFD_REGION_COMPUTED || region > SGFD_REGION_PML)
         return fail(h, SGFD_ERR_INVALID, "bad region %d", region);
     if (every > 0 && nsamples == 0) return fail(h, SGFD_ERR_INVALID, "an audit needs at least one sample");
+    if (every > 0 && h->storage != SGFD_STORE_F32)
+        return fail(h, SGFD_ERR_UNSUPPORTED, "the per-step audit needs FP32 storage (use sgfd_energy)");
     SG_CUDA(h, cudaStreamSynchronize(h->stream), "synchronise before changing the audit");
     if (every == 0) {
         h->audit_every = 0;
@@ -821,6 +907,7 @@ int sgfd_cell_counts(const sgfd_solver *h, int64_t *n_interior, int64_t *n_pml) 
 int sgfd_launches_per_step(const sgfd_solver *h) {
     if (!h) return -1;
     const int audit = h->audit_every > 0 ? 2 : 0;
+    if (h->storage != SGFD_STORE_F32) return half_launches_per_step(h->sr) + audit;
     if (h->kernel == SGFD_KERNEL_ZMARCH) return 2 + audit;
     return simple_launches_per_step(h->sr) + audit;
 }

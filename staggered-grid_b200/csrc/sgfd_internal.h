@@ -73,6 +73,20 @@ struct Model {
     float *split;        // kNumSplit * npml
 };
 
+// 16-bit wavefield storage (kernels_half.cu): fields and splits as 16-bit
+// values with per-field power-of-two scales; scale state in device memory so
+// that replayed graphs see its updates.
+constexpr int kRescaleEvery = 50;   // scales re-chosen every 50 steps (after steps 0, 1, 3, 7, ... first)
+constexpr int kScaleHead = 8;       // largest stored magnitude put in [2^7, 2^8)
+struct HalfState {
+    uint16_t *f[9];      // same layout (pitch, offset) as Model::f
+    uint16_t *split;     // kNumSplit * npml
+    int *e, *e_new;      // scale exponents (9 each)
+    float *sc, *inv;     // 2^e, 2^-e
+    unsigned *amax;      // largest |value| written on a rescale step (float bits)
+    int storage;         // SGFD_STORE_BF16 or SGFD_STORE_F16
+};
+
 // Source (one explosive point) and receivers.
 struct SourceRec {
     int64_t src;         // padded index of the source cell, -1 if none
@@ -189,6 +203,13 @@ struct AuditGate {
 };
 cudaError_t launch_energy_step(const Model &m, const Physics &ph, int region, double *partials, int nblocks,
                                const AuditGate &gt, cudaStream_t s);
+// 16-bit storage: one step, launches per step, and the FP32 copies of the
+// stored fields and splits (Model::f, Model::split) in both directions.
+cudaError_t half_step(const Model &m, const Physics &ph, const SourceRec &sr, const HalfState &hs, int it,
+                      float src_value, bool use_wavelet, cudaStream_t s, cudaEvent_t *ev = nullptr);
+int half_launches_per_step(const SourceRec &sr);
+cudaError_t half_to_views(const Model &m, const HalfState &hs, cudaStream_t s);
+cudaError_t half_from_views(const Model &m, const HalfState &hs, cudaStream_t s);
 // *ctr = value, or *ctr += value when add is set.
 cudaError_t launch_counter(int *ctr, int value, bool add, cudaStream_t s);
 

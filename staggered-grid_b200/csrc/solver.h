@@ -59,6 +59,13 @@ struct sgfd_solver {
     cudaGraphExec_t graph = nullptr;
     int *step_ctr = nullptr;      // device step counter read by the replayed kernels
     sgfd::GraphKey graph_key{};   // launch parameters the graph was captured with
+    // 16-bit wavefield storage (storage != SGFD_STORE_F32): the stored
+    // fields and splits and their scale state; Model::f / Model::split then
+    // hold FP32 copies made for the read-out paths (sync_views)
+    int storage = SGFD_STORE_F32;
+    char *h16_pool = nullptr;
+    void *hstate = nullptr;
+    sgfd::HalfState hs{};
     // energy audit scratch: 2 doubles per partial block, then the 2 results
     double *audit = nullptr;
     int audit_blocks = 0;
@@ -78,6 +85,15 @@ int cuda_fail(sgfd_solver *h, cudaError_t e, const char *what);
 int check_handle(sgfd_solver *h);
 // Read and clear the kernels' device error flag.
 int check_device_error(sgfd_solver *h);
+// 16-bit storage: refresh the FP32 copies Model::f / Model::split from the
+// stored values (no-op for FP32 storage), or the stored values from them.
+int sync_views(sgfd_solver *h);
+int sync_from_views(sgfd_solver *h);
+// 16-bit storage: reset the scale state (exponents 0, maxima 0).
+int reset_scales(sgfd_solver *h);
+// 16-bit storage: exponents of the 9 field scales, to the host / from the host.
+int get_scale_exponents(sgfd_solver *h, int *e);
+int set_scale_exponents(sgfd_solver *h, const int *e);
 
 // Launch one step of h's kernels on stream s with the given receiver /
 // source record (h->sr, or a copy whose it_dev points at a step counter).

@@ -43,7 +43,9 @@ struct CkptHeader {
     int64_t npml;
     uint64_t payload_bytes;
     uint64_t checksum;
-    uint8_t pad[128 - 8 - 8 - 16 - 12 - 12 - 16 - 24];
+    int8_t scale_e[9];   // 16-bit storage: exponents of the field scales (0 for FP32)
+    uint8_t storage;     // sgfd_storage of the payload's values
+    uint8_t pad[128 - 8 - 8 - 16 - 12 - 12 - 16 - 24 - 10];
 };
 static_assert(sizeof(CkptHeader) == 128, "checkpoint header is 128 bytes");
 
@@ -149,6 +151,7 @@ void fill_header(sgfd_solver *h, int32_t it_next, CkptHeader *hd) {
     hd->dt = c.dt; hd->dx = c.dx; hd->dy = c.dy; hd->dz = c.dz;
     hd->npml = h->m.npml;
     hd->payload_bytes = payload_bytes(h);
+    hd->storage = (uint8_t)h->storage;
 }
 
 // Regions move through the staging chunk as whole rows where a row fits
@@ -161,6 +164,11 @@ int save_state(sgfd_solver *h, int32_t it_next, Stream &out) {
     if (it_next < 0) return fail(h, SGFD_ERR_INVALID, "negative step index");
     CkptHeader hd;
     fill_header(h, it_next, &hd);
+    int e[9];
+    r = get_scale_exponents(h, e);
+    if (r == SGFD_OK) r = sync_views(h);   // 16-bit storage: the payload holds the read-back values
+    if (r) return r;
+    for (int g = 0; g < 9; ++g) hd.scale_e[g] = (int8_t)e[g];
     const long hdr_pos = out.fp ? std::ftell(out.fp) : (long)out.pos;
     if (!out.write(&hd, sizeof hd)) return fail(h, SGFD_ERR_INVALID, "checkpoint buffer too small or write failed");
     void *raw = nullptr;
@@ -218,6 +226,9 @@ int load_state(sgfd_solver *h, Stream &in, int32_t *it_next) {
         hd.dy != want.dy || hd.dz != want.dz)
         return fail(h, SGFD_ERR_INVALID, "checkpoint physics (dt, cell sizes, damping, quirks) differ from the solver's");
     if (hd.payload_bytes != want.payload_bytes) return fail(h, SGFD_ERR_INVALID, "checkpoint payload size mismatch");
+    if (hd.storage != want.storage)
+        return fail(h, SGFD_ERR_INVALID, "checkpoint storage type %d differs from the solver's %d", hd.storage,
+                    want.storage);
     void *raw = nullptr;
     SG_CUDA(h, cudaMallocHost(&raw, kStage), "checkpoint staging buffer");
     std::unique_ptr<void, PinnedDeleter> stage(raw);
@@ -245,6 +256,14 @@ int load_state(sgfd_solver *h, Stream &in, int32_t *it_next) {
         sgfd_reset(h);   // do not leave a half-loaded state behind
         return fail(h, SGFD_ERR_INVALID, short_read ? "checkpoint truncated; state reset to zero"
                                                     : "checkpoint checksum mismatch; state reset to zero");
+    }
+    if (h->storage != SGFD_STORE_F32) {   // back to 16-bit values under the saved scales
+        int e[9];
+        for (int g = 0; g < 9; ++g) e[g] = hd.scale_e[g];
+        r = set_scale_exponents(h, e);
+        if (r == SGFD_OK) r = sync_from_views(h);
+        if (r) return r;
+        SG_CUDA(h, cudaStreamSynchronize(h->stream), "checkpoint: 16-bit values");
     }
     if (it_next) *it_next = hd.it_next;
     return SGFD_OK;

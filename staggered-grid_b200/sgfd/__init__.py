@@ -367,7 +367,7 @@ class Solver:
 
 
 CHECKPOINT_MAGIC = b"SGFDCKP1"
-_CKPT_HEADER = struct.Struct("<8sII4i3i3i4fqQQ32x")
+_CKPT_HEADER = struct.Struct("<8sII4i3i3i4fqQQ9bB22x")
 
 
 def checkpoint_header(data: bytes) -> dict:
@@ -379,7 +379,10 @@ def checkpoint_header(data: bytes) -> dict:
         raise ValueError("not an sgfd checkpoint")
     keys = ("magic", "version", "header_bytes", "nx", "ny", "nz", "pml", "nrec", "nt", "it_next",
             "quirks", "damping", "arith", "dt", "dx", "dy", "dz", "npml", "payload_bytes", "checksum")
-    return dict(zip(keys, v))
+    d = dict(zip(keys, v[:20]))
+    d["scale_exponents"] = list(v[20:29])
+    d["storage"] = v[29]
+    return d
 
 
 def checkpoint_checksum(payload: bytes) -> int:
