@@ -45,6 +45,9 @@ BYTES = {"velocity": (52, 112), "stress": (68, 164)}
 # 394^3 workload is too large for a multi-metric capture, so its traffic is
 # reported as its algorithmic bytes times this ratio.
 TRAFFIC_RATIO = {"velocity": 1.18, "stress": 1.31}
+# 16-bit storage: fields and splits 2 B, medium 4 B (per step 66 B interior, 144 B PML).
+BYTES16 = {"velocity": (28, 58), "stress": (38, 86)}
+STORAGE = {"f32": 0, "bf16": 1, "f16": 2}
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -60,6 +63,9 @@ def parse():
     p.add_argument("--no-autotune", action="store_true", help="batch32: keep the default launch shapes")
     p.add_argument("--kernel", choices=["auto", "simple", "zmarch"], default="auto")
     p.add_argument("--arith", choices=["ref", "fast"], default="fast")
+    p.add_argument("--storage", choices=["f32", "bf16", "f16"], default="f32",
+                   help="wavefield storage; 16-bit also reports errors on a 128^3 crop")
+    p.add_argument("--no-accuracy", action="store_true", help="skip the 16-bit accuracy leg")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-steps", type=int, default=6, help="steps of the CPU sample")
@@ -277,7 +283,8 @@ def main():
     torch.cuda.set_device(local)
     kernel = {"auto": sgfd.KERNEL_AUTO, "simple": sgfd.KERNEL_SIMPLE, "zmarch": sgfd.KERNEL_ZMARCH}[args.kernel]
     arith = sgfd.ARITH_FAST if args.arith == "fast" else sgfd.ARITH_REF
-    cfg = sgfd.default_config(**{**w.cfg, "device": local, "kernel": kernel, "arith": arith})
+    cfg = sgfd.default_config(**{**w.cfg, "device": local, "kernel": kernel, "arith": arith,
+                                 "storage": STORAGE[args.storage]})
     K, W = args.steps, args.warmup
     nt = max(w.nt, W + K + 64)
     wav = np.resize(w.wavelet, nt).astype(np.float32)
@@ -321,16 +328,18 @@ def main():
     tv, ts = s.profile(W + K, P)
     per = {"velocity": tv / P, "stress": ts / P}
     dom = max(per, key=per.get)
-    alg = BYTES[dom][0] * n_int + BYTES[dom][1] * n_pml
+    bpc = BYTES if args.storage == "f32" else BYTES16
+    alg = bpc[dom][0] * n_int + bpc[dom][1] * n_pml
     peak, peak_kind = measured_peak()
     achieved = alg / (per[dom] / 1e3) / 1e9
-    traffic = alg * TRAFFIC_RATIO[dom] if kernel == sgfd.KERNEL_AUTO or args.kernel == "zmarch" else None
+    traffic = alg * TRAFFIC_RATIO[dom] if s.kernel_name() == "zmarch" else None
     roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
             "traffic_source": "ncu dram bytes / algorithmic bytes of the z-march kernels on the 216^3 + 20 PML "
                               "cube, times this launch's algorithmic bytes" if traffic else None,
             "alg_bytes_per_launch": alg, "avg_launch_ms": per[dom],
-            "step_frac": (120 * n_int + 276 * n_pml) / (ms / K / 1e3) / 1e9 / peak,
+            "step_frac": (sum(v[0] for v in bpc.values()) * n_int + sum(v[1] for v in bpc.values()) * n_pml)
+                         / (ms / K / 1e3) / 1e9 / peak,
             "kernel_ms": per}
 
     # ---- end to end through the C ABI with host buffers ----
@@ -343,10 +352,10 @@ def main():
     result = {
         "metric": "Gcell-updates/s", "value": value, "unit": "Gcell/s", "n_gpus": world, "steps": K,
         "warmup": W, "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32", "data": "synthetic",
+        "dtype": "f32" if args.storage == "f32" else f"f32 arithmetic, {args.storage} storage", "data": "synthetic",
         "config": {"workload": w.name, "grid": [w.cfg["nx"], w.cfg["ny"], w.cfg["nz"]], "pml": w.cfg["pml"],
                    "computed_cells": cells, "interior_cells": n_int, "pml_cells": n_pml,
-                   "receivers": len(w.rec_comp), "kernel": None, "arith": args.arith,
+                   "receivers": len(w.rec_comp), "kernel": None, "arith": args.arith, "storage": args.storage,
                    "parallelism": f"replicas{world}",
                    "l2": "inputs larger than L2 (9 wavefields of %.0f MB each)" % (w.cfg["nx"] * w.cfg["ny"] * w.cfg["nz"] * 4 / 1e6)},
         "roofline": roof, "clocks": clk,
@@ -360,11 +369,77 @@ def main():
             "value": rate, "unit": "Gcell/s", "cores": threads, "kind": "port",
             "sample": f"{args.cpu_steps} full time steps of {w.name} ({secs:.1f} s) after 1 untimed step; "
                       f"C++ oracle of the reference kernels, FP32, flush-to-zero, OpenMP {threads} threads"}
+    if rank == 0 and world == 1 and args.storage != "f32" and not args.no_accuracy:
+        result["accuracy"] = storage_accuracy(w, args, local)
     if rank == 0:
         print(json.dumps(result), flush=True)
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+def crop_workload(w, n_grid=138, pml=20, nt=300):
+    """The centre n_grid^3 window of w's medium as a model of its own (128^3
+    computed cells with pml 20): source at its centre, Ricker 20 Hz, 16x16
+    receivers 5 cells below the top interior face recording vz and txx."""
+    import sgfd
+    import sgfd.workloads as wl
+    nz, ny, nx = w.b.shape
+    z0, y0, x0 = (nz - n_grid) // 2, (ny - n_grid) // 2, (nx - n_grid) // 2
+    sl = (slice(z0, z0 + n_grid), slice(y0, y0 + n_grid), slice(x0, x0 + n_grid))
+    b, lam, mu = (np.ascontiguousarray(a[sl]) for a in (w.b, w.lam, w.mu))
+    c = n_grid // 2
+    i0, span = wl.HALO + pml, n_grid - 2 * (wl.HALO + pml)
+    ks = i0 + (np.arange(16) * span) // 16
+    pts = [(x, y, i0 + 5) for y in ks for x in ks]
+    xyz = np.array([p for p in pts for _ in (0, 1)], np.int32)
+    comp = np.array([sgfd.VZ, sgfd.TXX] * len(pts), np.int32)
+    cfg = {**w.cfg, "nx": n_grid, "ny": n_grid, "nz": n_grid, "pml": pml}
+    w64 = wl._ricker_t0_64(20.0, w.cfg["dt"], 1.2 / 20.0, nt)
+    return wl.Workload(f"crop{n_grid - 10}^3 of {w.name}", cfg, b, lam, mu, (c, c, c), xyz, comp, nt,
+                       w64.astype(np.float32), w64)
+
+
+def storage_accuracy(w, args, local):
+    """Relative L2 errors of 16-bit storage on a 128^3 crop of the workload's
+    medium: traces and final vx / txx snapshots, against the FP32 GPU path and
+    against the FP64 CPU oracle (the same crop run in double precision)."""
+    import sgfd
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle_py
+    cw = crop_workload(w)
+    arith = sgfd.ARITH_FAST if args.arith == "fast" else sgfd.ARITH_REF
+
+    def gpu(storage):
+        s = sgfd.Solver(sgfd.default_config(**{**cw.cfg, "device": local, "arith": arith, "storage": storage}))
+        s.set_medium(cw.b, cw.lam, cw.mu)
+        s.set_source(*cw.src)
+        s.set_receivers(cw.rec_xyz, cw.rec_comp, cw.nt)
+        s.set_wavelet(cw.wavelet)
+        s.run(0, cw.nt)
+        out = (s.traces(), s.field(sgfd.VX), s.field(sgfd.TXX))
+        s.close()
+        return out
+
+    oracle_py.set_threads(os.cpu_count() or 1)
+    o = oracle_py.Oracle(cw.cfg, fp64=True)
+    o.set_medium(cw.b, cw.lam, cw.mu)
+    o.set_source(*cw.src)
+    o.set_receivers(cw.rec_xyz, cw.rec_comp, cw.nt)
+    o.run(cw.wavelet64, 0, cw.nt)
+    ref64 = (o.traces(), o.field(sgfd.VX), o.field(sgfd.TXX))
+    o.close()
+    r16, r32 = gpu(STORAGE[args.storage]), gpu(0)
+
+    def rel(a, b):
+        b = np.asarray(b, np.float64)
+        return float(np.linalg.norm(np.asarray(a, np.float64) - b) / np.linalg.norm(b))
+
+    names = ("traces", "vx", "txx")
+    return {"workload": cw.name, "steps": cw.nt, "storage": args.storage,
+            "vs_fp64": {n: rel(a, b) for n, a, b in zip(names, r16, ref64)},
+            "vs_fp32": {n: rel(a, b) for n, a, b in zip(names, r16, r32)},
+            "fp32_vs_fp64": {n: rel(a, b) for n, a, b in zip(names, r32, ref64)}}
 
 
 def main_batch(args, world, rank, local):
