@@ -86,3 +86,36 @@ def test_autotune_picks_a_candidate_and_keeps_results():
             s.set_kernel(sgfd.KERNEL_ZMARCH)
         assert e.value.code == sgfd.ERR_UNSUPPORTED
         assert s.autotune(2).kernel == sgfd.KERNEL_SIMPLE
+
+
+def test_batch_mixes_storage_audit_and_families():
+    """One batch holding a 16-bit model, an FP32 model with a per-step energy
+    audit and an FP32 model on the per-cell kernels: each ends bit-identical
+    to the same model run alone, audit history included."""
+    ws = _models()
+    ws[0].cfg["storage"] = sgfd.STORE_F16
+    solo = []
+    for i, w in enumerate(ws):
+        with make_solver(w, kernel=sgfd.KERNEL_SIMPLE if i == 2 else sgfd.KERNEL_AUTO) as s:
+            if i == 1:
+                s.set_audit(9, sgfd.REGION_INTERIOR, 5)
+            s.run(0, w.nt)
+            solo.append((s.traces(), s.field(sgfd.TXX), s.audit() if i == 1 else None))
+    members = []
+    try:
+        for i, w in enumerate(ws):
+            m = make_solver(w, kernel=sgfd.KERNEL_SIMPLE if i == 2 else sgfd.KERNEL_AUTO)
+            if i == 1:
+                m.set_audit(9, sgfd.REGION_INTERIOR, 5)
+            members.append(m)
+        with sgfd.Batch(members) as b:
+            b.run(0, 45)
+            b.synchronize()
+        for i, (m, (tr, txx, hist)) in enumerate(zip(members, solo)):
+            np.testing.assert_array_equal(m.traces(), tr)
+            np.testing.assert_array_equal(m.field(sgfd.TXX), txx)
+            if hist is not None:
+                np.testing.assert_array_equal(m.audit(), hist)
+    finally:
+        for m in members:
+            m.close()

@@ -105,3 +105,18 @@ def test_station_files(tmp_path):
         c0 = int(w.rec_comp[0])
         assert np.loadtxt(prefix + f"_short_{names[c0]}.txt", ndmin=2).shape[0] == 10
         assert not os.path.exists(prefix + f"_short_{names[c0]}.bin")
+
+
+def test_checkpoint_moves_between_kernel_families():
+    """The checkpoint layout does not depend on the kernel family: a state saved
+    by the z-marching kernels resumes on the per-cell kernels bit for bit."""
+    w = wl.small_random_case(nt=50)
+    with make_solver(w) as full:
+        full.run(0, w.nt)
+        tr = full.traces()
+    with make_solver(w, kernel=sgfd.KERNEL_ZMARCH) as a:
+        a.run(0, 23)
+        blob = a.checkpoint(23)
+    with make_solver(w, kernel=sgfd.KERNEL_SIMPLE) as b:
+        b.run(b.restore(blob), w.nt - 23)
+        np.testing.assert_array_equal(b.traces(), tr)
