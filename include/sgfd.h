@@ -209,6 +209,11 @@ int sgfd_synchronize(sgfd_solver *h);
 /* Zero all wavefields, PML state and traces (medium, source, receivers kept). */
 int sgfd_reset(sgfd_solver *h);
 
+/* Overwrite one wavefield from a host array (nx*ny*nz, x fastest): initial
+ * conditions, or a state taken from another run.  The 5-cell frame should
+ * hold zeros, as the reference's does. */
+int sgfd_set_field(sgfd_solver *h, int32_t field, const float *src);
+
 /* Copy traces to host: out[r*nt + it] (receiver-major). */
 int sgfd_get_traces(sgfd_solver *h, float *out);
 /* Copy the n receiver samples of one step `it` to out[0..n) (blocking);
@@ -285,6 +290,33 @@ int sgfd_batch_synchronize(sgfd_batch *b);
 void *sgfd_batch_stream(sgfd_batch *b);
 /* Kernel launches one sgfd_batch_run(b, *, nsteps) issues. */
 int sgfd_batch_run_launches(const sgfd_batch *b, int32_t nsteps);
+
+/* ---- learned absorbing strip (no counterpart in the reference) ----
+ * A model created with pml = 0 ends at the zero frame.  sgfd_set_learned_strip
+ * makes its outer `width` computed cells a learned absorbing strip: after
+ * every step each strip cell's 9 fields get a correction predicted by an MLP
+ * (252 inputs: the 9 fields of the cell's 3x3x3 neighbourhood, velocities times
+ * rho*vp, over their RMS s; vp/3000, vs/1732, rho/2000; per axis the depth into
+ * the strip over width and the side; 64 and 64 GELU units; 9 outputs times s,
+ * velocities divided back by rho*vp).  params: sgfd_mlp_param_count() floats,
+ * W1[252][64], b1[64], W2[64][64], b2[64], W3[64][9], b3[9].  width 0 removes
+ * the strip.  FP32 storage only. */
+int sgfd_set_learned_strip(sgfd_solver *h, int32_t width, const float *params);
+/* The 252 MLP inputs of n strip cells (computed coordinates cx, cy, cz per
+ * cell) from the current state, with each cell's s and rho*vp (training data). */
+int sgfd_strip_features(sgfd_solver *h, int32_t width, int32_t n, const int32_t *cells, float *X, float *scale,
+                        float *zimp);
+/* The MLP on the GPU of `device`, host arrays in and out: parameter count,
+ * forward pass of n input rows, loss (mean squared error over the 9 outputs)
+ * and its gradient for n rows, and minibatch Adam training (lr, betas 0.9 and
+ * 0.999) over `epochs` passes of the n rows in order, params updated in place
+ * and the mean minibatch loss of every epoch in epoch_loss. */
+int sgfd_mlp_param_count(void);
+int sgfd_mlp_forward(int32_t device, const float *params, const float *X, int64_t n, float *out);
+int sgfd_mlp_gradient(int32_t device, const float *params, const float *X, const float *Y, int32_t n, float *loss,
+                      float *grad);
+int sgfd_mlp_train(int32_t device, float *params, const float *X, const float *Y, int64_t n, int32_t epochs,
+                   int32_t batch, float lr, float *epoch_loss);
 
 /* FP64 energy audit (no counterpart in the reference): kinetic
  * 1/2 rho |v|^2 and strain energy (s:s - lambda/(3 lambda + 2 mu) tr(s)^2) /

@@ -557,7 +557,7 @@ int dispatch(Handle *h, Fn &&fn) {
 extern "C" {
 
 void *sgo_create(const sgfd_config *cfg, int fp64) {
-    if (!cfg || cfg->nx < 11 || cfg->ny < 11 || cfg->nz < 11 || cfg->pml < 1) return nullptr;
+    if (!cfg || cfg->nx < 11 || cfg->ny < 11 || cfg->nz < 11 || cfg->pml < 0) return nullptr;
     if (2 * (cfg->pml + kHalo) > std::min({cfg->nx, cfg->ny, cfg->nz})) return nullptr;
     auto *h = new Handle();
     h->fp64 = fp64;

@@ -111,6 +111,9 @@ cudaError_t dispatch_on(sgfd_solver *h, const SourceRec &sr, cudaStream_t s, int
                     : h->kernel == SGFD_KERNEL_ZMARCH
                         ? zmarch_step(h->m, h->ph, sr, h->zg, h->vm, h->sm, it, value, use_wavelet, s, ev)
                         : simple_step(h->m, h->ph, sr, it, value, use_wavelet, s, ev);
+    if (e == cudaSuccess && h->strip_n > 0)
+        e = launch_strip(h->m, h->strip_w, h->strip_cells, h->strip_n, h->strip_buf,
+                         h->strip_buf + mlp_params(), s);
     if (e == cudaSuccess && h->audit_every > 0) {
         const AuditGate gt{sr.it_dev, it, h->audit_every, h->audit_count, h->audit_hist};
         e = launch_energy_step(h->m, h->ph, h->audit_region, h->audit, h->audit_blocks, gt, s);
@@ -141,6 +144,10 @@ void graph_key(const sgfd_solver *h, GraphKey *k) {
     k->audit_count = h->audit_count;
     k->audit_hist = h->audit_hist;
     k->audit = h->audit;
+    k->strip_w = h->strip_w;
+    k->strip_n = h->strip_n;
+    k->strip_cells = h->strip_cells;
+    k->strip_buf = h->strip_buf;
 }
 
 }  // namespace sgfd
@@ -167,7 +174,7 @@ void set_physics(sgfd_solver *h) {
     ph.inj_dt2 = c.dt * c.dt;
     ph.damping = c.damping;
     ph.quirks = c.quirks;
-    const int p = c.pml;
+    const int p = std::max(c.pml, 1);   // pml = 0: no PML cell uses the damping constants
     ph.q_refgpu = 0.5f * c.dt * kTau;
     ph.poly = (8.0f / 15.0f - 0.03f * (float)p) + (1.0f / 1500.0f) * (float)(p * p);
     const double R = c.damping_R > 0 ? (double)c.damping_R : 1e-3;
@@ -337,7 +344,7 @@ int sgfd_create(const sgfd_config *cfg, sgfd_solver **out) {
         if (c.reserved[i] != 0) return fail(nullptr, SGFD_ERR_INVALID, "reserved config fields must be zero");
     if (c.arith != SGFD_ARITH_REF && c.arith != SGFD_ARITH_FAST)
         return fail(nullptr, SGFD_ERR_INVALID, "unknown arithmetic mode %d", c.arith);
-    if (c.pml < 1) return fail(nullptr, SGFD_ERR_INVALID, "pml must be >= 1 (got %d)", c.pml);
+    if (c.pml < 0) return fail(nullptr, SGFD_ERR_INVALID, "pml must be >= 0 (got %d)", c.pml);
     const int need = 2 * (kHalo + c.pml) + 1;
     if (c.nx < need || c.ny < need || c.nz < need)
         return fail(nullptr, SGFD_ERR_INVALID, "grid %dx%dx%d too small for pml %d (each axis needs >= %d)",
@@ -492,6 +499,8 @@ void sgfd_destroy(sgfd_solver *h) {
     cudaFree(h->hstate);
     cudaFree(h->audit);
     cudaFree(h->audit_hist);
+    cudaFree(h->strip_cells);
+    cudaFree(h->strip_buf);
     release_graph(h);
     cudaFree(h->step_ctr);
     if (h->cap_stream) cudaStreamDestroy(h->cap_stream);
@@ -798,6 +807,23 @@ static int download(sgfd_solver *h, const float *src, float *out) {
     return SGFD_OK;
 }
 
+int sgfd_set_field(sgfd_solver *h, int32_t field, const float *src) {
+    int r = check_handle(h);
+    if (r) return r;
+    if (!src) return fail(h, SGFD_ERR_INVALID, "null input");
+    if (field < 0 || field >= SGFD_NFIELDS) return fail(h, SGFD_ERR_INVALID, "bad field id %d", field);
+    r = sync_views(h);   // 16-bit storage: every FP32 copy current before re-storing them
+    if (r) return r;
+    const Model &m = h->m;
+    const size_t row = (size_t)m.nx * sizeof(float);
+    SG_CUDA(h, cudaMemcpy2DAsync(m.f[field], (size_t)m.px * sizeof(float), src, row, row, (size_t)m.ny * m.nz,
+                                 cudaMemcpyHostToDevice, h->stream), "field upload");
+    r = sync_from_views(h);
+    if (r) return r;
+    SG_CUDA(h, cudaStreamSynchronize(h->stream), "field upload");
+    return SGFD_OK;
+}
+
 int sgfd_get_field(sgfd_solver *h, int32_t field, float *out) {
     int r = check_handle(h);
     if (r) return r;
@@ -906,7 +932,7 @@ int sgfd_cell_counts(const sgfd_solver *h, int64_t *n_interior, int64_t *n_pml) 
 
 int sgfd_launches_per_step(const sgfd_solver *h) {
     if (!h) return -1;
-    const int audit = h->audit_every > 0 ? 2 : 0;
+    const int audit = (h->audit_every > 0 ? 2 : 0) + (h->strip_n > 0 ? 2 : 0);
     if (h->storage != SGFD_STORE_F32) return half_launches_per_step(h->sr) + audit;
     if (h->kernel == SGFD_KERNEL_ZMARCH) return 2 + audit;
     return simple_launches_per_step(h->sr) + audit;

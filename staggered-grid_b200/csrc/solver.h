@@ -23,6 +23,9 @@ struct GraphKey {
     int kernel;
     int audit_every, audit_region, audit_count;
     double *audit_hist, *audit;
+    int strip_w, strip_n;
+    int4 *strip_cells;
+    float *strip_buf;
 };
 // Steps per captured graph; sgfd_run launches the remainder directly.
 constexpr int kGraphSteps = 16;
@@ -66,6 +69,11 @@ struct sgfd_solver {
     char *h16_pool = nullptr;
     void *hstate = nullptr;
     sgfd::HalfState hs{};
+    // learned absorbing strip (pml = 0 models): cells of the strip, then the
+    // MLP parameters followed by one correction per cell and field
+    int strip_w = 0, strip_n = 0;
+    int4 *strip_cells = nullptr;
+    float *strip_buf = nullptr;
     // energy audit scratch: 2 doubles per partial block, then the 2 results
     double *audit = nullptr;
     int audit_blocks = 0;
@@ -101,6 +109,14 @@ cudaError_t dispatch_on(sgfd_solver *h, const SourceRec &sr, cudaStream_t s, int
                         bool use_wavelet, cudaEvent_t *ev);
 // Byte image of everything a captured step passes to h's kernels.
 void graph_key(const sgfd_solver *h, GraphKey *k);
+
+// Learned strip (learned.cu): the strip's cells (computed coordinates), the
+// kernel set-up, and one correction pass (MLP then apply).
+int strip_cell_list(const Model &m, int w, std::vector<int4> &cells);
+cudaError_t strip_prepare();
+cudaError_t launch_strip(const Model &m, int w, const int4 *cells, int n, const float *params, float *delta,
+                         cudaStream_t s);
+int mlp_params();
 
 inline size_t round_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 

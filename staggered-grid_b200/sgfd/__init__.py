@@ -102,6 +102,7 @@ def lib() -> ctypes.CDLL:
         "sgfd_get_trace_step": (ctypes.c_int, [vp, i32, fp]),
         "sgfd_profile": (ctypes.c_int, [vp, i32, i32, fp, fp]),
         "sgfd_get_field": (ctypes.c_int, [vp, i32, fp]),
+        "sgfd_set_field": (ctypes.c_int, [vp, i32, fp]),
         "sgfd_get_medium": (ctypes.c_int, [vp, i32, fp]),
         "sgfd_ricker_ref": (ctypes.c_float, [ctypes.c_float, ctypes.c_float, i32]),
         "sgfd_ricker_t0": (ctypes.c_float, [ctypes.c_float, ctypes.c_float, ctypes.c_float, i32]),
@@ -131,6 +132,12 @@ def lib() -> ctypes.CDLL:
         "sgfd_get_audit": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_double)]),
         "sgfd_energy_noalloc": (ctypes.c_int, [vp, i32, i32, ctypes.POINTER(ctypes.c_double),
                                                 ctypes.POINTER(ctypes.c_double)]),
+        "sgfd_set_learned_strip": (ctypes.c_int, [vp, i32, fp]),
+        "sgfd_strip_features": (ctypes.c_int, [vp, i32, i32, ip, fp, fp, fp]),
+        "sgfd_mlp_param_count": (ctypes.c_int, []),
+        "sgfd_mlp_forward": (ctypes.c_int, [i32, fp, fp, ctypes.c_int64, fp]),
+        "sgfd_mlp_gradient": (ctypes.c_int, [i32, fp, fp, fp, i32, fp, fp]),
+        "sgfd_mlp_train": (ctypes.c_int, [i32, fp, fp, fp, ctypes.c_int64, i32, i32, ctypes.c_float, fp]),
         "sgfd_energy": (ctypes.c_int, [vp, i32, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
     }
     for name, (res, args) in sigs.items():
@@ -279,6 +286,12 @@ class Solver:
         self._check(lib().sgfd_get_field(self.h, fid, _fptr(out)))
         return out
 
+    def set_field(self, fid: int, values):
+        a = np.ascontiguousarray(values, dtype=np.float32).reshape(-1)
+        if a.size != int(np.prod(self.shape)):
+            raise ValueError("field arrays must have nx*ny*nz cells")
+        self._check(lib().sgfd_set_field(self.h, fid, _fptr(a)))
+
     def medium(self, which: int) -> np.ndarray:
         out = np.zeros(self.shape, dtype=np.float32)
         self._check(lib().sgfd_get_medium(self.h, which, _fptr(out)))
@@ -303,6 +316,22 @@ class Solver:
 
     def kernel_name(self) -> str:
         return lib().sgfd_kernel_name(self.h).decode()
+
+    def set_learned_strip(self, width: int, params=None):
+        """Make the outer `width` computed cells a learned absorbing strip (pml = 0 models)."""
+        p = None if params is None else np.ascontiguousarray(params, dtype=np.float32)
+        self._check(lib().sgfd_set_learned_strip(self.h, width, _fptr(p) if p is not None else None))
+
+    def strip_features(self, width: int, cells):
+        """(X [n][252], s [n], rho*vp [n]) of the listed strip cells (computed coordinates)."""
+        c = np.ascontiguousarray(np.asarray(cells, dtype=np.int32).reshape(-1, 3))
+        n = len(c)
+        X = np.zeros((n, 252), np.float32)
+        sc = np.zeros(n, np.float32)
+        zi = np.zeros(n, np.float32)
+        self._check(lib().sgfd_strip_features(self.h, width, n, c.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+                                              _fptr(X), _fptr(sc), _fptr(zi)))
+        return X, sc, zi
 
     def energy_noalloc(self, region: int = 0, nblocks: int = 0) -> tuple[float, float]:
         """energy() for callers that cannot have the library allocate device
@@ -448,3 +477,43 @@ class Batch:
 
     def __exit__(self, *a):
         self.close()
+
+
+# ---- the strip MLP on the GPU (host arrays in and out) ----
+MLP_PARAMS = 20937
+
+
+def _check_global(rc: int):
+    if rc != OK:
+        raise SgfdError(rc, lib().sgfd_global_error().decode())
+
+
+def mlp_forward(params, X, device: int = 0) -> np.ndarray:
+    p = np.ascontiguousarray(params, np.float32)
+    X = np.ascontiguousarray(X, np.float32)
+    out = np.zeros((len(X), 9), np.float32)
+    _check_global(lib().sgfd_mlp_forward(device, _fptr(p), _fptr(X), len(X), _fptr(out)))
+    return out
+
+
+def mlp_gradient(params, X, Y, device: int = 0):
+    """(loss, gradient) of the mean squared error of the MLP on rows X against Y."""
+    p = np.ascontiguousarray(params, np.float32)
+    X = np.ascontiguousarray(X, np.float32)
+    Y = np.ascontiguousarray(Y, np.float32)
+    g = np.zeros(MLP_PARAMS, np.float32)
+    loss = ctypes.c_float()
+    _check_global(lib().sgfd_mlp_gradient(device, _fptr(p), _fptr(X), _fptr(Y), len(X),
+                                          ctypes.pointer(loss), _fptr(g)))
+    return loss.value, g
+
+
+def mlp_train(params, X, Y, epochs: int, batch: int = 4096, lr: float = 1e-3, device: int = 0):
+    """Minibatch Adam on the GPU; returns (params, per-epoch mean loss)."""
+    p = np.ascontiguousarray(params, np.float32).copy()
+    X = np.ascontiguousarray(X, np.float32)
+    Y = np.ascontiguousarray(Y, np.float32)
+    hist = np.zeros(epochs, np.float32)
+    _check_global(lib().sgfd_mlp_train(device, _fptr(p), _fptr(X), _fptr(Y), len(X), epochs, batch, lr,
+                                       _fptr(hist)))
+    return p, hist

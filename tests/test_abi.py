@@ -41,7 +41,7 @@ def test_abi_version_and_struct_size():
 
 
 @pytest.mark.parametrize("kw,code", [
-    (dict(pml=0), sgfd.ERR_INVALID),
+    (dict(pml=-1), sgfd.ERR_INVALID),
     (dict(nx=20, pml=10), sgfd.ERR_INVALID),
     (dict(dt=0.0), sgfd.ERR_INVALID),
     (dict(dx=-1.0), sgfd.ERR_INVALID),

@@ -1,0 +1,129 @@
+"""The learned absorbing strip on the GPU: the MLP's forward pass and gradients
+against the CPU oracle (FP64 numpy), training, the strip's inputs against
+their definition, the fused correction against the oracle's network, and what
+the trained network gains over the same strip without it."""
+import os
+
+import numpy as np
+import pytest
+
+import mlp_oracle as mo
+import sgfd
+import sgfd.learned as L
+import sgfd.workloads as wl
+
+pytestmark = pytest.mark.gpu
+
+
+def _rel(a, b):
+    return np.linalg.norm(np.asarray(a, np.float64) - b) / max(np.linalg.norm(b), 1e-30)
+
+
+def test_forward_and_gradient_match_cpu_oracle():
+    rng = np.random.default_rng(3)
+    p = (rng.standard_normal(mo.N_PARAMS) * 0.2).astype(np.float32)
+    X = rng.standard_normal((96, mo.N_IN)).astype(np.float32)
+    Y = rng.standard_normal((96, mo.N_OUT)).astype(np.float32)
+    out, _ = mo.forward(p, X)
+    assert _rel(sgfd.mlp_forward(p, X), out) < 1e-5
+    loss, g = sgfd.mlp_gradient(p, X, Y)
+    loss_ref, g_ref = mo.loss_and_gradient(p, X, Y)
+    assert abs(loss - loss_ref) <= 1e-5 * loss_ref
+    o = 0
+    for name, shape in mo.SHAPES:           # every parameter block separately
+        n = int(np.prod(shape))
+        assert _rel(g[o:o + n], g_ref[o:o + n]) < 1e-4, name
+        o += n
+
+
+def test_training_fits_a_smooth_target():
+    rng = np.random.default_rng(4)
+    X = rng.standard_normal((16384, mo.N_IN)).astype(np.float32)
+    A = rng.standard_normal((mo.N_IN, mo.N_OUT)) / np.sqrt(mo.N_IN)
+    Y = (np.tanh(X @ A) * 0.5).astype(np.float32)
+    p, hist = sgfd.mlp_train(L.init_params(1), X, Y, epochs=25, batch=1024, lr=2e-3)
+    assert hist[-1] < 0.1 * hist[0], hist
+    pred = sgfd.mlp_forward(p, X[:512])
+    assert np.mean((pred - Y[:512]) ** 2) < 0.1 * np.mean(Y[:512] ** 2)
+
+
+def _strip_model(n=30, seed=5):
+    w = wl.small_random_case(nx=n, ny=n, nz=n, pml=0, nt=10, seed=seed)
+    s = sgfd.Solver(sgfd.default_config(**{**w.cfg, "arith": sgfd.ARITH_FAST}))
+    s.set_medium(w.b, w.lam, w.mu)
+    rng = np.random.default_rng(seed)
+    for f in range(9):
+        a = np.zeros(w.b.shape, np.float32)
+        inner = (slice(5, n - 5),) * 3
+        a[inner] = rng.standard_normal(a[inner].shape) * (1e-6 if f < 3 else 1e2)
+        s.set_field(f, a)
+    return w, s
+
+
+def _features_numpy(fields, w, cells, width):
+    b, lam, mu = (a.astype(np.float32) for a in (w.b, w.lam, w.mu))
+    nc = w.b.shape[0] - 10
+    X = np.zeros((len(cells), 252))
+    for i, (cx, cy, cz) in enumerate(cells):
+        x, y, z = cx + 5, cy + 5, cz + 5
+        rho, vp = 1.0 / b[z, y, x], np.sqrt((lam[z, y, x] + 2 * mu[z, y, x]) * b[z, y, x])
+        vs = np.sqrt(mu[z, y, x] * b[z, y, x])
+        u = np.array([[fields[k][z + dz, y + dy, x + dx] * (rho * vp if k < 3 else 1.0) for k in range(9)]
+                      for dz in (-1, 0, 1) for dy in (-1, 0, 1) for dx in (-1, 0, 1)], np.float64).ravel()
+        s = np.sqrt(np.mean(u * u))
+        X[i, :243] = u / s
+        X[i, 243:246] = vp / 3000.0, vs / 1732.0, rho / 2000.0
+        for a, c in enumerate((cx, cy, cz)):
+            if c < width:
+                X[i, 246 + a], X[i, 249 + a] = (width - c) / width, -1
+            elif c >= nc - width:
+                X[i, 246 + a], X[i, 249 + a] = (c - (nc - width) + 1) / width, 1
+    return X
+
+
+def test_strip_inputs_follow_their_definition():
+    w, s = _strip_model()
+    cells = np.array([[0, 0, 0], [3, 10, 19], [19, 5, 2], [10, 19, 10], [5, 0, 12]], np.int32)
+    X, sc, z = s.strip_features(6, cells)
+    fields = [s.field(k) for k in range(9)]
+    np.testing.assert_allclose(X, _features_numpy(fields, w, cells, 6), rtol=2e-5, atol=2e-6)
+    s.close()
+
+
+def test_fused_strip_correction_is_the_network_output():
+    rng = np.random.default_rng(6)
+    p = (rng.standard_normal(mo.N_PARAMS) * 0.05).astype(np.float32)
+    w, plain = _strip_model(seed=7)
+    _, strip = _strip_model(seed=7)
+    strip.set_learned_strip(6, p)
+    assert strip.launches_per_step() == plain.launches_per_step() + 2
+    plain.step(0, 0.0)
+    strip.step(0, 0.0)
+    cells = L.strip_cells(20, 6)
+    X, sc, z = plain.strip_features(6, cells)
+    out, _ = mo.forward(p, X)
+    delta = out * sc[:, None]
+    delta[:, :3] /= z[:, None]
+    gx, gy, gz = (cells + 5).T
+    for k in range(9):
+        a, b = plain.field(k), strip.field(k)
+        d = (b - a)[gz, gy, gx]
+        np.testing.assert_allclose(d, delta[:, k], rtol=2e-3, atol=1e-3 * np.abs(delta[:, k]).max())
+        mask = np.ones(a.shape, bool)
+        mask[gz, gy, gx] = False
+        np.testing.assert_array_equal(a[mask], b[mask])     # interior untouched
+    with pytest.raises(sgfd.SgfdError):
+        sgfd.Solver(sgfd.default_config(**{**w.cfg, "pml": 4})).set_learned_strip(6, p)
+    plain.close()
+    strip.close()
+
+
+@pytest.mark.skipif(not os.path.exists(L.PARAMS_PATH), reason="no trained strip parameters in the package")
+def test_trained_strip_reflects_less_than_the_bare_strip():
+    """Held-out medium: energy left in the interior after the direct wave has
+    gone, relative to its peak, with the trained 6-cell strip, the same strip
+    without the network, and a 20-cell split-field PML."""
+    r = L.reflection(L.load_params(), seed=999)
+    learned, bare, pml = (r[k]["final_over_peak"] for k in ("learned_strip", "bare_strip", "pml20"))
+    print(f"reflected energy / peak: learned strip {learned:.3e}, bare strip {bare:.3e}, 20-cell PML {pml:.3e}")
+    assert np.isfinite(learned) and learned < 0.8 * bare
