@@ -58,7 +58,7 @@ def parse():
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", choices=["sgfd", "reference"], default="sgfd")
     p.add_argument("--workload", choices=["random344", "random472", "random216", "plain100", "reference_main",
-                                               "batch32"],
+                                               "batch32", "learned256"],
                    default="random344")
     p.add_argument("--no-autotune", action="store_true", help="batch32: keep the default launch shapes")
     p.add_argument("--kernel", choices=["auto", "simple", "zmarch"], default="auto")
@@ -277,6 +277,9 @@ def main():
     if args.workload == "batch32":
         main_batch(args, world, rank, local)
         return
+    if args.workload == "learned256":
+        main_learned(args, world, rank, local)
+        return
     w = build_workload(args.workload)
     import torch
     import sgfd
@@ -440,6 +443,69 @@ def storage_accuracy(w, args, local):
             "vs_fp64": {n: rel(a, b) for n, a, b in zip(names, r16, ref64)},
             "vs_fp32": {n: rel(a, b) for n, a, b in zip(names, r16, r32)},
             "fp32_vs_fp64": {n: rel(a, b) for n, a, b in zip(names, r32, ref64)}}
+
+
+def main_learned(args, world, rank, local):
+    """The learned-boundary configuration: 256^3 interior with a 6-cell
+    learned strip (268^3 computed cells, pml = 0, the trained network in the
+    package) against the same interior with a 20-cell split-field PML (296^3
+    computed), random medium (std 5 %, 50 m), Ricker 20 Hz at the centre.
+    value: computed-cell updates per second of the strip model; the line
+    also gives interior-cell updates per second of both, the quantity the two
+    boundaries compete on."""
+    import torch
+    import sgfd
+    import sgfd.learned as L
+    import sgfd.workloads as wl
+    torch.cuda.set_device(local)
+    K, W = args.steps, args.warmup
+    n_int, pml20 = 256, 20
+    big = wl.random_cube(n_interior=n_int, pml=pml20, nt=W + K + 16, seed=5)
+    params = L.load_params()
+    out = {}
+    for name, width, pml in (("learned_strip", L.WIDTH, 0), ("pml20", pml20, pml20)):
+        n = n_int + 2 * width + 2 * wl.HALO
+        off = pml20 - width
+        cut = slice(off, off + n)
+        mb, ml, mm = (np.ascontiguousarray(a[cut, cut, cut]) for a in (big.b, big.lam, big.mu))
+        cfg = sgfd.default_config(**{**big.cfg, "nx": n, "ny": n, "nz": n, "pml": pml, "device": local,
+                                     "arith": sgfd.ARITH_FAST})
+        s = sgfd.Solver(cfg)
+        s.set_medium(mb, ml, mm)
+        s.set_source(n // 2, n // 2, n // 2)
+        s.set_wavelet(np.resize(big.wavelet, W + K + 16))
+        if pml == 0:
+            s.set_learned_strip(L.WIDTH, params)
+        s.run(0, W)
+        s.prepare_run()
+        s.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        st = torch.cuda.Stream()
+        s.set_stream(st.cuda_stream)
+        e0.record(st)
+        s.run(W, K)
+        e1.record(st)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        out[name] = {"ms_per_step": ms / K, "computed_cells": (n - 10) ** 3,
+                     "gcell_per_s": (n - 10) ** 3 * K / ms / 1e6, "interior_gcell_per_s": n_int ** 3 * K / ms / 1e6,
+                     "launches_per_step": s.launches_per_step()}
+        s.close()
+    ls = out["learned_strip"]
+    refl = L.reflection(params, seed=999) if not args.no_accuracy else None
+    result = {
+        "metric": "Gcell-updates/s", "value": ls["gcell_per_s"], "unit": "Gcell/s", "n_gpus": 1, "steps": K,
+        "warmup": W, "ms_per_step": ls["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "learned256", "interior": n_int, "strip_width": L.WIDTH, "pml_compared": pml20,
+                   "computed_cells": ls["computed_cells"], "parallelism": "replicas1"},
+        "comparison": out,
+        "reflected_energy_over_peak": None if refl is None else
+            {k: v["final_over_peak"] for k, v in refl.items()},
+        "gpu_launches": ls["launches_per_step"] * K,
+    }
+    if rank == 0:
+        print(json.dumps(result), flush=True)
 
 
 def main_batch(args, world, rank, local):

@@ -14,7 +14,9 @@
 //     +1 high, 0 off the band);
 //   network: 252 -> 64 -> 64 -> 9, GELU after both hidden layers;
 //   output: 9 corrections in units of s (velocities divided back by rho*vp),
-//     so that the correction scales with the wavefield, as the physics does.
+//     so that the correction scales with the wavefield, as the physics does,
+//     scaled down where needed so that no correction raises its cell's
+//     energy (k_strip_mlp).
 // Parameters, 20 937 floats: W1 [252][64], b1, W2 [64][64], b2, W3 [64][9], b3.
 //
 // Training (sgfd_mlp_train) runs minibatch Adam with hand-written kernels:
@@ -127,8 +129,31 @@ __global__ void __launch_bounds__(128) k_strip_mlp(Model m, int w, const int4 *c
 #pragma unroll
         for (int k = 0; k < kOut; ++k) out[k] = fmaf(a, wsm[oW3 + j2 * kOut + k], out[k]);
     }
+    // Energy limit: the correction d may not raise the cell's energy
+    // E(f) = rho/2 |v|^2 + (s:s - c tr(s)^2) / (4 mu), c = lambda / (3 lambda + 2 mu)
+    // (the energy audit's density).  E(f + a d) = E(f) + 2 a B + a^2 Q, so the
+    // largest admissible a in [0, 1] is -2B/Q when B < 0, else 0.  A network
+    // trained on one-step targets is otherwise free to feed energy back into
+    // the strip and grow over long runs.
+    const int64_t c = pidx(m, q.x + kHalo, q.y + kHalo, q.z + kHalo);
+    float f[kOut], d[kOut];
 #pragma unroll
-    for (int k = 0; k < kOut; ++k) delta[(int64_t)i * kOut + k] = out[k] * s / (k < 3 ? z : 1.0f);
+    for (int k = 0; k < kOut; ++k) {
+        f[k] = m.f[k][c];
+        d[k] = out[k] * s / (k < 3 ? z : 1.0f);
+    }
+    const float rho = 1.0f / m.b[c], lam = m.lam[c], mu = m.mu[c];
+    const float cc = lam / (3.0f * lam + 2.0f * mu), i4m = 0.25f / mu;
+    const float trf = f[3] + f[4] + f[5], trd = d[3] + d[4] + d[5];
+    const float B = 0.5f * rho * (f[0] * d[0] + f[1] * d[1] + f[2] * d[2]) +
+                    i4m * (f[3] * d[3] + f[4] * d[4] + f[5] * d[5] + 2.0f * (f[6] * d[6] + f[7] * d[7] + f[8] * d[8]) -
+                           cc * trf * trd);
+    const float Q = 0.5f * rho * (d[0] * d[0] + d[1] * d[1] + d[2] * d[2]) +
+                    i4m * (d[3] * d[3] + d[4] * d[4] + d[5] * d[5] + 2.0f * (d[6] * d[6] + d[7] * d[7] + d[8] * d[8]) -
+                           cc * trd * trd);
+    const float a = (Q > 0.0f && B < 0.0f) ? fminf(1.0f, -2.0f * B / Q) : 0.0f;
+#pragma unroll
+    for (int k = 0; k < kOut; ++k) delta[(int64_t)i * kOut + k] = a * d[k];
 }
 
 __global__ void k_strip_apply(Model m, const int4 *cells, int n, const float *delta) {

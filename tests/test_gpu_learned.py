@@ -1,7 +1,8 @@
 """The learned absorbing strip on the GPU: the MLP's forward pass and gradients
 against the CPU oracle (FP64 numpy), training, the strip's inputs against
-their definition, the fused correction against the oracle's network, and what
-the trained network gains over the same strip without it."""
+their definition, the fused correction against the oracle's network (with the
+energy limit), and what the trained network gains over the same strip
+without it, over a short and a long run."""
 import os
 
 import numpy as np
@@ -105,6 +106,18 @@ def test_fused_strip_correction_is_the_network_output():
     delta = out * sc[:, None]
     delta[:, :3] /= z[:, None]
     gx, gy, gz = (cells + 5).T
+    # energy limit: scale each cell's correction so that it does not raise the cell's energy
+    f = np.stack([plain.field(k)[gz, gy, gx] for k in range(9)], axis=1).astype(np.float64)
+    b, lam, mu = (a[gz, gy, gx].astype(np.float64) for a in (w.b, w.lam, w.mu))
+    rho, cc, i4m = 1 / b, lam / (3 * lam + 2 * mu), 0.25 / mu
+
+    def bil(u, v):
+        return (0.5 * rho * (u[:, :3] * v[:, :3]).sum(1) + i4m * ((u[:, 3:6] * v[:, 3:6]).sum(1)
+                + 2 * (u[:, 6:] * v[:, 6:]).sum(1) - cc * u[:, 3:6].sum(1) * v[:, 3:6].sum(1)))
+    B, Q = bil(f, delta), bil(delta, delta)
+    alpha = np.where((Q > 0) & (B < 0), np.minimum(1.0, -2 * B / np.where(Q > 0, Q, 1)), 0.0)
+    delta *= alpha[:, None]
+    assert (alpha > 0).any() and (alpha < 1).any()
     for k in range(9):
         a, b = plain.field(k), strip.field(k)
         d = (b - a)[gz, gy, gx]
@@ -123,7 +136,11 @@ def test_trained_strip_reflects_less_than_the_bare_strip():
     """Held-out medium: energy left in the interior after the direct wave has
     gone, relative to its peak, with the trained 6-cell strip, the same strip
     without the network, and a 20-cell split-field PML."""
-    r = L.reflection(L.load_params(), seed=999)
-    learned, bare, pml = (r[k]["final_over_peak"] for k in ("learned_strip", "bare_strip", "pml20"))
-    print(f"reflected energy / peak: learned strip {learned:.3e}, bare strip {bare:.3e}, 20-cell PML {pml:.3e}")
-    assert np.isfinite(learned) and learned < 0.8 * bare
+    for nt in (400, 1500):
+        r = L.reflection(L.load_params(), seed=999, nt=nt, sample_every=50)
+        learned, bare, pml = (r[k]["final_over_peak"] for k in ("learned_strip", "bare_strip", "pml20"))
+        print(f"{nt} steps, reflected energy / peak: learned strip {learned:.3e}, bare strip {bare:.3e}, "
+              f"20-cell PML {pml:.3e}")
+        assert np.isfinite(learned) and learned < 0.8 * bare
+        hist = np.array(r["learned_strip"]["history"])
+        assert hist[-1] <= 1.5 * hist[len(hist) // 2]   # no growth over the second half: the strip is stable
