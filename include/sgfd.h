@@ -324,7 +324,8 @@ int sgfd_mlp_train(int32_t device, float *params, const float *X, const float *Y
  * summed in FP64 on the GPU over the computed cells of `region` and
  * multiplied by dx*dy*dz.  Waits for the handle's queued steps.  Energy left
  * in SGFD_REGION_INTERIOR after the direct wave has left the interior is what
- * the absorbing boundary reflected. */
+ * the absorbing boundary reflected.  In a model with a learned strip
+ * (pml = 0) the strip takes the PML's place in the regions. */
 int sgfd_energy(sgfd_solver *h, int32_t region, double *kinetic, double *strain);
 
 /* sgfd_energy without any allocation; no counterpart in the reference.

@@ -72,7 +72,7 @@ extern "C" int sgfd_energy_noalloc(sgfd_solver *h, int32_t region, int32_t nbloc
     r = sync_views(h);   // 16-bit storage: FP32 copies of the stored fields (no allocation)
     if (r) return r;
     double *out = scratch + 2 * nblocks;
-    SG_CUDA(h, launch_energy(h->m, h->ph, region, scratch, nblocks, out, h->stream), "energy audit");
+    SG_CUDA(h, launch_energy(audit_model(h), h->ph, region, scratch, nblocks, out, h->stream), "energy audit");
     double res[2];
     SG_CUDA(h, cudaMemcpyAsync(res, out, sizeof res, cudaMemcpyDeviceToHost, h->stream), "energy download");
     SG_CUDA(h, cudaStreamSynchronize(h->stream), "energy download");

@@ -116,7 +116,7 @@ cudaError_t dispatch_on(sgfd_solver *h, const SourceRec &sr, cudaStream_t s, int
                          h->strip_buf + mlp_params(), s);
     if (e == cudaSuccess && h->audit_every > 0) {
         const AuditGate gt{sr.it_dev, it, h->audit_every, h->audit_count, h->audit_hist};
-        e = launch_energy_step(h->m, h->ph, h->audit_region, h->audit, h->audit_blocks, gt, s);
+        e = launch_energy_step(audit_model(h), h->ph, h->audit_region, h->audit, h->audit_blocks, gt, s);
     }
     return e;
 }
@@ -853,7 +853,7 @@ int sgfd_energy(sgfd_solver *h, int32_t region, double *kinetic, double *strain)
     if (r == SGFD_OK) r = sync_views(h);
     if (r) return r;
     double *out = h->audit + 2 * h->audit_blocks;
-    SG_CUDA(h, launch_energy(h->m, h->ph, region, h->audit, h->audit_blocks, out, h->stream), "energy audit");
+    SG_CUDA(h, launch_energy(audit_model(h), h->ph, region, h->audit, h->audit_blocks, out, h->stream), "energy audit");
     double res[2];
     SG_CUDA(h, cudaMemcpyAsync(res, out, sizeof res, cudaMemcpyDeviceToHost, h->stream), "energy download");
     SG_CUDA(h, cudaStreamSynchronize(h->stream), "energy download");

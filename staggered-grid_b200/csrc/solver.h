@@ -120,6 +120,14 @@ int mlp_params();
 
 inline size_t round_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
+// The model as the energy audit sees it: for a model with a learned strip
+// (pml = 0) the strip plays the PML's part in the audit's regions.
+inline sgfd::Model audit_model(const sgfd_solver *h) {
+    sgfd::Model m = h->m;
+    if (m.pml == 0) m.pml = h->strip_w;
+    return m;
+}
+
 // Bytes of one padded device array (fields and medium share this size).
 inline size_t array_bytes(const Model &m) { return round_up((size_t)m.plane * m.nz * sizeof(float), 256); }
 

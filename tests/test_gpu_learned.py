@@ -144,3 +144,20 @@ def test_trained_strip_reflects_less_than_the_bare_strip():
         assert np.isfinite(learned) and learned < 0.8 * bare
         hist = np.array(r["learned_strip"]["history"])
         assert hist[-1] <= 1.5 * hist[len(hist) // 2]   # no growth over the second half: the strip is stable
+
+
+def test_energy_audit_regions_follow_the_strip():
+    """With a learned strip the audit's interior is the cells inside the strip."""
+    rng = np.random.default_rng(8)
+    p = (rng.standard_normal(mo.N_PARAMS) * 0.05).astype(np.float32)
+    w, s = _strip_model(seed=9)
+    s.set_learned_strip(6, p)
+    s.step(0, 0.0)
+    fields = [s.field(k) for k in range(9)]
+    inner = (slice(11, 19),) * 3              # GRID 30: frame 5 + strip 6
+    k, e = s.energy(sgfd.REGION_INTERIOR)
+    np.testing.assert_allclose(k + e, L.energy(fields, w.b, w.lam, w.mu, inner) * 1000.0, rtol=1e-9)
+    kt, et = s.energy(sgfd.REGION_COMPUTED)
+    ks, es = s.energy(sgfd.REGION_PML)
+    np.testing.assert_allclose(kt + et, k + e + ks + es, rtol=1e-12)
+    s.close()
