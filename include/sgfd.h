@@ -300,7 +300,8 @@ int sgfd_batch_run_launches(const sgfd_batch *b, int32_t nsteps);
  * the strip over width and the side; 64 and 64 GELU units; 9 outputs times s,
  * velocities divided back by rho*vp).  params: sgfd_mlp_param_count() floats,
  * W1[252][64], b1[64], W2[64][64], b2[64], W3[64][9], b3[9].  width 0 removes
- * the strip.  FP32 storage only. */
+ * the strip.  FP32 storage only.  The network runs on the tensor cores with
+ * FP16 operands and FP32 accumulation (see sgfd_mlp_infer). */
 int sgfd_set_learned_strip(sgfd_solver *h, int32_t width, const float *params);
 /* The 252 MLP inputs of n strip cells (computed coordinates cx, cy, cz per
  * cell) from the current state, with each cell's s and rho*vp (training data). */
@@ -313,6 +314,12 @@ int sgfd_strip_features(sgfd_solver *h, int32_t width, int32_t n, const int32_t 
  * and the mean minibatch loss of every epoch in epoch_loss. */
 int sgfd_mlp_param_count(void);
 int sgfd_mlp_forward(int32_t device, const float *params, const float *X, int64_t n, float *out);
+/* The strip's inference path on n given input rows: the three layers on the
+ * tensor cores with FP16 operands (inputs, weights and hidden activations
+ * rounded to binary16) and FP32 accumulation, outputs before the energy limit
+ * and the scale s.  Checks the tensor-core path on inputs of the caller's
+ * choosing; n <= 2^30. */
+int sgfd_mlp_infer(int32_t device, const float *params, const float *X, int64_t n, float *out);
 int sgfd_mlp_gradient(int32_t device, const float *params, const float *X, const float *Y, int32_t n, float *loss,
                       float *grad);
 int sgfd_mlp_train(int32_t device, float *params, const float *X, const float *Y, int64_t n, int32_t epochs,

@@ -7,6 +7,11 @@ as W1[252][64], b1[64], W2[64][64], b2[64], W3[64][9], b3[9]; loss the mean
 of the squared errors over all rows and the 9 outputs.  Only tests/ use it,
 to check the GPU's forward pass and gradients.  The reference has no such
 network; the restatement follows the definition written in learned.cu.
+
+`forward_f16` is the same network with the operand rounding of the GPU's
+tensor-core inference (k_strip_tc): inputs, weights and both hidden
+activations rounded to IEEE binary16 (round to nearest even), biases and all
+sums exact (FP64 here, FP32 accumulators on the GPU).
 """
 import math
 
@@ -47,6 +52,18 @@ def forward(p, X):
     z2 = a1 @ w["W2"] + w["b2"]
     a2 = gelu(z2)
     return a2 @ w["W3"] + w["b3"], (X, z1, a1, z2, a2)
+
+
+def f16(a):
+    """Round to IEEE binary16 (nearest even) and back."""
+    return np.asarray(a, np.float64).astype(np.float16).astype(np.float64)
+
+
+def forward_f16(p, X):
+    w = unpack(p)
+    a1 = f16(gelu(f16(X) @ f16(w["W1"]) + w["b1"]))
+    a2 = f16(gelu(a1 @ f16(w["W2"]) + w["b2"]))
+    return a2 @ f16(w["W3"]) + w["b3"]
 
 
 def loss_and_gradient(p, X, Y):

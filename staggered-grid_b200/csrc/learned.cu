@@ -16,16 +16,30 @@
 //   output: 9 corrections in units of s (velocities divided back by rho*vp),
 //     so that the correction scales with the wavefield, as the physics does,
 //     scaled down where needed so that no correction raises its cell's
-//     energy (k_strip_mlp).
+//     energy (k_strip_tc).
 // Parameters, 20 937 floats: W1 [252][64], b1, W2 [64][64], b2, W3 [64][9], b3.
+//
+// Inference (k_strip_tc) runs the three layers on the tensor cores
+// (tcgen05.mma kind::f16: FP16 operands in shared memory, FP32 accumulators
+// in tensor memory), 128 strip cells per tile.  The strip is cut into boxes
+// of at most 128 cells (32 x 4 x 1 on the z faces, 32 x 2 x 2 on the y faces,
+// width x 4 x 5 on the x faces for width 6); a box's fields and their one-cell
+// halo are staged in shared memory with coalesced loads, and each thread
+// builds its cell's 252 inputs from there into row t of the A operand.
+// Each CTA (one per SM) holds the weights once and runs two warpgroups that
+// work on alternate tiles, so one warpgroup's loads overlap the other's
+// tensor-core and epilogue work.
 //
 // Training (sgfd_mlp_train) runs minibatch Adam with hand-written kernels:
 // a tiled FP32 GEMM, bias + GELU, the output loss (mean squared error over the
 // 9 outputs), the GELU backward, column sums and the Adam update.  The
 // gradients are checked against a CPU restatement in the tests.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
+
+#include <cuda_fp16.h>
 
 #include "solver.h"
 
@@ -96,73 +110,383 @@ __global__ void k_strip_features(Model m, int w, const int4 *cells, int n, float
     zimp[i] = z;
 }
 
-// Corrections of all strip cells from the current state (one thread per
-// cell, the parameters in shared memory).  Written to delta first and added
-// by k_strip_apply, so that every correction sees the uncorrected state.
-__global__ void __launch_bounds__(128) k_strip_mlp(Model m, int w, const int4 *cells, int n, const float *params,
-                                                   float *delta) {
-    extern __shared__ float wsm[];
-    for (int i = threadIdx.x; i < kParams; i += blockDim.x) wsm[i] = params[i];
-    __syncthreads();
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const int4 q = cells[i];
-    float h1[kH];
-#pragma unroll
-    for (int j = 0; j < kH; ++j) h1[j] = wsm[oB1 + j];
-    float z;
-    const float s = strip_inputs(m, w, q.x, q.y, q.z, z, [&](int f, float v) {
-        const float *row = wsm + oW1 + f * kH;
-#pragma unroll
-        for (int j = 0; j < kH; ++j) h1[j] = fmaf(v, row[j], h1[j]);
-    });
-#pragma unroll
-    for (int j = 0; j < kH; ++j) h1[j] = gelu(h1[j]);
-    float out[kOut];
-#pragma unroll
-    for (int k = 0; k < kOut; ++k) out[k] = wsm[oB3 + k];
-    for (int j2 = 0; j2 < kH; ++j2) {
-        float a = wsm[oB2 + j2];
-#pragma unroll
-        for (int j = 0; j < kH; ++j) a = fmaf(h1[j], wsm[oW2 + j * kH + j2], a);
-        a = gelu(a);
-#pragma unroll
-        for (int k = 0; k < kOut; ++k) out[k] = fmaf(a, wsm[oW3 + j2 * kOut + k], out[k]);
-    }
-    // Energy limit: the correction d may not raise the cell's energy
-    // E(f) = rho/2 |v|^2 + (s:s - c tr(s)^2) / (4 mu), c = lambda / (3 lambda + 2 mu)
-    // (the energy audit's density).  E(f + a d) = E(f) + 2 a B + a^2 Q, so the
-    // largest admissible a in [0, 1] is -2B/Q when B < 0, else 0.  A network
-    // trained on one-step targets is otherwise free to feed energy back into
-    // the strip and grow over long runs.
-    const int64_t c = pidx(m, q.x + kHalo, q.y + kHalo, q.z + kHalo);
-    float f[kOut], d[kOut];
-#pragma unroll
-    for (int k = 0; k < kOut; ++k) {
-        f[k] = m.f[k][c];
-        d[k] = out[k] * s / (k < 3 ? z : 1.0f);
-    }
-    const float rho = 1.0f / m.b[c], lam = m.lam[c], mu = m.mu[c];
-    const float cc = lam / (3.0f * lam + 2.0f * mu), i4m = 0.25f / mu;
-    const float trf = f[3] + f[4] + f[5], trd = d[3] + d[4] + d[5];
-    const float B = 0.5f * rho * (f[0] * d[0] + f[1] * d[1] + f[2] * d[2]) +
-                    i4m * (f[3] * d[3] + f[4] * d[4] + f[5] * d[5] + 2.0f * (f[6] * d[6] + f[7] * d[7] + f[8] * d[8]) -
-                           cc * trf * trd);
-    const float Q = 0.5f * rho * (d[0] * d[0] + d[1] * d[1] + d[2] * d[2]) +
-                    i4m * (d[3] * d[3] + d[4] * d[4] + d[5] * d[5] + 2.0f * (d[6] * d[6] + d[7] * d[7] + d[8] * d[8]) -
-                           cc * trd * trd);
-    const float a = (Q > 0.0f && B < 0.0f) ? fminf(1.0f, -2.0f * B / Q) : 0.0f;
-#pragma unroll
-    for (int k = 0; k < kOut; ++k) delta[(int64_t)i * kOut + k] = a * d[k];
+// ---- tensor-core inference --------------------------------------------------
+
+constexpr int kRows = 128;                 // cells per tile = MMA M
+constexpr int kK1 = 256;                   // layer-1 K: the 252 inputs and 4 zeros
+constexpr int kN3 = 16;                    // layer-3 N: the 9 outputs and 7 zeros
+constexpr int kStage = 612;                // staged cells per box, (32+2)(4+2)(1+2) at most
+// Weight image (bytes): W1, W2, W3 transposed to N x K, FP16, in the K-major
+// core-matrix order of kmaj, then the biases b1, b2, b3 (b3 padded to 16) in FP32.
+constexpr int kImgW1 = 0, kImgW2 = kImgW1 + kH * kK1 * 2, kImgW3 = kImgW2 + kH * kH * 2,
+              kImgB = kImgW3 + kN3 * kH * 2, kImg = kImgB + (2 * kH + kN3) * 4;
+constexpr int kImgPad = (kImg + 1023) / 1024 * 1024;
+constexpr int kAOp = kRows * kK1 * 2;                        // A operand of one warpgroup
+constexpr int kStg = 9 * kStage * 4;                         // staged fields of one warpgroup
+constexpr int kWgBytes = kAOp + (kStg + 1023) / 1024 * 1024;
+constexpr int kTcSmem = 1024 + kImgPad + 2 * kWgBytes + 64;  // + alignment, barriers, TMEM address
+static_assert(kImg % 16 == 0, "weight image is copied in 16-byte pieces");
+static_assert(kTcSmem <= 232448, "shared memory of one CTA");
+constexpr uint32_t kTmemCols = 256;                          // 128 per warpgroup: D1/D3 at +0, D2 at +64
+
+// Byte offset of element (row, k) of a K-major operand with KT columns: 8x8
+// core matrices of 128 contiguous bytes (8 rows of 16 bytes), the K-adjacent
+// core matrices 128 bytes apart (LBO), the next 8 rows KT*16 bytes on (SBO).
+__host__ __device__ constexpr uint32_t kmaj(int row, int k, int KT) {
+    return (uint32_t)((row >> 3) * (KT * 16) + (k >> 3) * 128 + (row & 7) * 16 + (k & 7) * 2);
 }
 
-__global__ void k_strip_apply(Model m, const int4 *cells, int n, const float *delta) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const int4 q = cells[i];
-    const int64_t c = pidx(m, q.x + kHalo, q.y + kHalo, q.z + kHalo);
+// Shared-memory matrix descriptor: start address, LBO 128 B, SBO KT*16 B,
+// descriptor version 1, no swizzle.
+__device__ __forceinline__ uint64_t smem_desc(uint32_t saddr, int KT) {
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)(128 >> 4) << 16) | ((uint64_t)((KT * 16) >> 4) << 32) |
+           (1ull << 46);
+}
+// Instruction descriptor of kind::f16: FP32 accumulator, A and B FP16 and
+// K-major, M = 128, N = n.
+__host__ __device__ constexpr uint32_t instr_desc(int n) {
+    return (1u << 4) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(kRows >> 4) << 24);
+}
+
+__device__ __forceinline__ uint32_t saddr_of(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init1(uint64_t *bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(saddr_of(bar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+// Bounded wait for the phase of the given parity: false after about 2 s.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity) {
+    for (int i = 0; i < 2000; ++i) {
+        uint32_t ok;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, 1000000;\n"
+            " selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(ok) : "r"(saddr_of(bar)), "r"(parity) : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void tc_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+// Barrier of one warpgroup (named barrier 1 + wg) that also ORs a flag over it.
+__device__ __forceinline__ bool wg_sync_or(int wg, bool flag) {
+    uint32_t r;
+    asm volatile(
+        "{\n .reg .pred p, q;\n setp.ne.u32 p, %1, 0;\n bar.red.or.pred q, %2, 128, p;\n selp.u32 %0, 1, 0, q;\n}\n"
+        : "=r"(r) : "r"((uint32_t)flag), "r"(wg + 1) : "memory");
+    return r != 0;
+}
+__device__ __forceinline__ void wg_sync(int wg) { asm volatile("bar.sync %0, 128;" ::"r"(wg + 1) : "memory"); }
+
+// D[tmem] (+)= A[a] * B[b]^T over KT columns, M = 128, N = n, K = 16 per instruction.
+__device__ __forceinline__ void mma_chain(uint32_t tmem_d, uint32_t a, uint32_t b, int KT, int n) {
+    const uint32_t id = instr_desc(n);
+    for (int kk = 0; kk < KT / 16; ++kk) {
+        const uint64_t ad = smem_desc(a + kk * 256, KT), bd = smem_desc(b + kk * 256, KT);
+        asm volatile(
+            "{\n .reg .pred p;\n setp.ne.u32 p, %4, 0;\n"
+            " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n"
+            ::"r"(tmem_d), "l"(ad), "l"(bd), "r"(id), "r"((uint32_t)(kk > 0)) : "memory");
+    }
+}
+__device__ __forceinline__ void mma_commit(uint64_t *bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(saddr_of(bar))
+                 : "memory");
+}
+// 16 consecutive FP32 columns of this thread's TMEM lane; the wait is inside
+// the same statement so no use of the registers can move above it.
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];\n"
+        "tcgen05.wait::ld.sync.aligned;\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr) : "memory");
 #pragma unroll
-    for (int k = 0; k < kOut; ++k) m.f[k][c] += delta[(int64_t)i * kOut + k];
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+__device__ __forceinline__ uint32_t pack_half2(float a, float b) {
+    const __half2 h = __floats2half2_rn(a, b);
+    return *reinterpret_cast<const uint32_t *>(&h);
+}
+__device__ __forceinline__ void store_chunk(unsigned char *p, const float (&v)[8]) {
+    *reinterpret_cast<uint4 *>(p) = make_uint4(pack_half2(v[0], v[1]), pack_half2(v[2], v[3]),
+                                               pack_half2(v[4], v[5]), pack_half2(v[6], v[7]));
+}
+
+// Hidden layer: 64 accumulator columns of this thread's row, + bias, GELU,
+// FP16 into row t of the next A operand (K = 64).
+__device__ __forceinline__ void hidden_layer(uint32_t taddr, const float *bias, unsigned char *a_op, int t) {
+#pragma unroll
+    for (int c = 0; c < kH / 16; ++c) {
+        float v[16];
+        tmem_ld16(taddr + c * 16, v);
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            float g[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) g[q] = gelu(v[8 * h + q] + bias[16 * c + 8 * h + q]);
+            store_chunk(a_op + kmaj(t, 16 * c + 8 * h, kH), g);
+        }
+    }
+}
+
+// Weight image from the FP32 parameters (once per sgfd_set_learned_strip).
+__global__ void k_weight_image(const float *p, unsigned char *img) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kH * kK1; i += gridDim.x * blockDim.x) {
+        const int j = i / kK1, k = i % kK1;   // output j, input k
+        *reinterpret_cast<__half *>(img + kImgW1 + kmaj(j, k, kK1)) =
+            __float2half_rn(k < kIn ? p[oW1 + k * kH + j] : 0.0f);
+        if (k < kH) {
+            *reinterpret_cast<__half *>(img + kImgW2 + kmaj(j, k, kH)) = __float2half_rn(p[oW2 + k * kH + j]);
+            if (j < kN3)
+                *reinterpret_cast<__half *>(img + kImgW3 + kmaj(j, k, kH)) =
+                    __float2half_rn(j < kOut ? p[oW3 + k * kOut + j] : 0.0f);
+        }
+        if (i < kH) {
+            float *bias = reinterpret_cast<float *>(img + kImgB);
+            bias[i] = p[oB1 + i];
+            bias[kH + i] = p[oB2 + i];
+            if (i < kN3) bias[2 * kH + i] = i < kOut ? p[oB3 + i] : 0.0f;
+        }
+    }
+}
+
+// Strip box of tile `td`: origin (computed coordinates) and extents.
+struct Box {
+    int x, y, z, ex, ey, ez;
+};
+__device__ __forceinline__ Box box_of(int4 td) { return {td.x, td.y, td.z, td.w & 255, (td.w >> 8) & 255, (td.w >> 16) & 255}; }
+
+// Network of every strip cell (ROWS = false), or of n input rows X (ROWS =
+// true: the tensor-core path checked on given inputs, raw outputs to out).
+// One CTA per SM, two warpgroups; warpgroup wg takes tiles 2*blockIdx.x + wg,
+// then every 2*gridDim.x-th.  Thread t of a warpgroup owns row t of its tiles
+// (TMEM lane t).  delta[tile][k][128] receives the energy-limited corrections.
+template <bool ROWS>
+__global__ void __launch_bounds__(256, 1)
+k_strip_tc(Model m, int w, const int4 *tiles, int ntiles, const unsigned char *wimg, float *delta, const float *X,
+           int64_t nrows, float *out, int *err) {
+    extern __shared__ unsigned char smem_raw[];
+    unsigned char *sm = smem_raw + ((1024 - (saddr_of(smem_raw) & 1023)) & 1023);
+    const int tid = threadIdx.x, wg = tid >> 7, t = tid & 127, warp = tid >> 5;
+    unsigned char *a_op = sm + kImgPad + wg * kWgBytes;
+    float *stg = reinterpret_cast<float *>(a_op + kAOp);
+    uint64_t *bar = reinterpret_cast<uint64_t *>(sm + kImgPad + 2 * kWgBytes);
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bar + 2);
+
+    for (int i = tid; i < kImg / 16; i += blockDim.x)
+        reinterpret_cast<uint4 *>(sm)[i] = reinterpret_cast<const uint4 *>(wimg)[i];
+    if (tid == 0) { mbar_init1(&bar[0]); mbar_init1(&bar[1]); }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(saddr_of(tmem_slot)),
+                     "r"(kTmemCols) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    fence_async_smem();   // the weight image is read by the tensor cores
+    tc_before();
+    __syncthreads();
+    tc_after();
+    const uint32_t tmem_base = *tmem_slot;
+    const uint32_t tmem = tmem_base + (uint32_t)(wg * 128) + ((uint32_t)((warp & 3) * 32) << 16);
+    const uint32_t a_s = saddr_of(a_op), w1_s = saddr_of(sm + kImgW1), w2_s = saddr_of(sm + kImgW2),
+                   w3_s = saddr_of(sm + kImgW3);
+    const float *b1 = reinterpret_cast<const float *>(sm + kImgB), *b2 = b1 + kH, *b3 = b2 + kH;
+    uint64_t *mybar = &bar[wg];
+    uint32_t parity = 0;
+    bool failed = false;
+
+    const int nt = ROWS ? (int)((nrows + kRows - 1) / kRows) : ntiles;
+    for (int tile = 2 * blockIdx.x + wg; tile < nt; tile += 2 * gridDim.x) {
+        // ---- inputs: row t of the A operand ----
+        float s = 0.0f, zimp = 1.0f, fc[kOut];
+        int count;
+        int64_t gc = 0;
+        if (ROWS) {
+            const int64_t first = (int64_t)tile * kRows, row = first + t;
+            count = (int)(nrows - first < kRows ? nrows - first : kRows);
+            const float *x = X + row * kIn;
+#pragma unroll 4
+            for (int j = 0; j < kK1 / 8; ++j) {
+                float v[8];
+#pragma unroll
+                for (int q = 0; q < 8; ++q) v[q] = (t < count && 8 * j + q < kIn) ? x[8 * j + q] : 0.0f;
+                store_chunk(a_op + kmaj(t, 8 * j, kK1), v);
+            }
+        } else {
+            const Box bx = box_of(tiles[tile]);
+            const int sx = bx.ex + 2, sxy = sx * (bx.ey + 2), ns = sxy * (bx.ez + 2);
+            for (int r = t; r < ns; r += kRows) {
+                const int lx = r % sx, ly = (r / sx) % (bx.ey + 2), lz = r / sxy;
+                const int64_t gi = pidx(m, bx.x - 1 + lx + kHalo, bx.y - 1 + ly + kHalo, bx.z - 1 + lz + kHalo);
+#pragma unroll
+                for (int k = 0; k < 9; ++k) stg[k * kStage + r] = m.f[k][gi];
+            }
+            wg_sync(wg);
+            count = bx.ex * bx.ey * bx.ez;
+            if (t < count) {
+                const int lx = t % bx.ex, ly = (t / bx.ex) % bx.ey, lz = t / (bx.ex * bx.ey);
+                const int cx = bx.x + lx, cy = bx.y + ly, cz = bx.z + lz;
+                const int c0 = (lx + 1) + (ly + 1) * sx + (lz + 1) * sxy;
+                gc = pidx(m, cx + kHalo, cy + kHalo, cz + kHalo);
+                const float b = m.b[gc], lam = m.lam[gc], mu = m.mu[gc];
+                const float rho = 1.0f / b, vp = sqrtf((lam + 2.0f * mu) * b), vs = sqrtf(mu * b);
+                zimp = rho * vp;
+                float ss = 0.0f;
+#pragma unroll
+                for (int n = 0; n < 27; ++n) {
+                    const int o = c0 + (n % 3 - 1) + ((n / 3) % 3 - 1) * sx + (n / 9 - 1) * sxy;
+#pragma unroll
+                    for (int k = 0; k < 9; ++k) {
+                        const float u = stg[k * kStage + o] * (k < 3 ? zimp : 1.0f);
+                        ss = fmaf(u, u, ss);
+                    }
+                }
+                s = sqrtf(ss * (1.0f / 243.0f));
+                const float inv = s > 0.0f ? 1.0f / s : 0.0f;
+                float ext[9];
+                ext[0] = vp * (1.0f / 3000.0f);
+                ext[1] = vs * (1.0f / 1732.0f);
+                ext[2] = rho * (1.0f / 2000.0f);
+                band_of(cx, m.nxc, w, ext[3], ext[6]);
+                band_of(cy, m.nyc, w, ext[4], ext[7]);
+                band_of(cz, m.nzc, w, ext[5], ext[8]);
+#pragma unroll
+                for (int j = 0; j < kK1 / 8; ++j) {
+                    float v[8];
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) {
+                        const int f = 8 * j + q;
+                        if (f < 243) {
+                            const int n = f / 9, k = f % 9;
+                            const int o = c0 + (n % 3 - 1) + ((n / 3) % 3 - 1) * sx + (n / 9 - 1) * sxy;
+                            v[q] = stg[k * kStage + o] * (k < 3 ? zimp : 1.0f) * inv;
+                        } else {
+                            v[q] = f < kIn ? ext[f - 243] : 0.0f;
+                        }
+                    }
+                    store_chunk(a_op + kmaj(t, 8 * j, kK1), v);
+                }
+#pragma unroll
+                for (int k = 0; k < kOut; ++k) fc[k] = stg[k * kStage + c0];
+            } else {
+                const float zero[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll 4
+                for (int j = 0; j < kK1 / 8; ++j) store_chunk(a_op + kmaj(t, 8 * j, kK1), zero);
+            }
+        }
+
+        // ---- layer 1: D1 = A (128 x 256) W1^T ----
+        fence_async_smem();
+        tc_before();
+        wg_sync(wg);
+        if (t == 0) {
+            tc_after();
+            mma_chain(tmem_base + wg * 128, a_s, w1_s, kK1, kH);
+            mma_commit(mybar);
+        }
+        bool ok = mbar_wait_bounded(mybar, parity);
+        parity ^= 1u;
+        if (wg_sync_or(wg, !ok)) { failed = true; break; }
+        tc_after();
+        hidden_layer(tmem, b1, a_op, t);
+
+        // ---- layer 2: D2 = H1 (128 x 64) W2^T ----
+        fence_async_smem();
+        tc_before();
+        wg_sync(wg);
+        if (t == 0) {
+            tc_after();
+            mma_chain(tmem_base + wg * 128 + 64, a_s, w2_s, kH, kH);
+            mma_commit(mybar);
+        }
+        ok = mbar_wait_bounded(mybar, parity);
+        parity ^= 1u;
+        if (wg_sync_or(wg, !ok)) { failed = true; break; }
+        tc_after();
+        hidden_layer(tmem + 64, b2, a_op, t);
+
+        // ---- layer 3: D3 = H2 (128 x 64) W3^T, N = 16 ----
+        fence_async_smem();
+        tc_before();
+        wg_sync(wg);
+        if (t == 0) {
+            tc_after();
+            mma_chain(tmem_base + wg * 128, a_s, w3_s, kH, kN3);
+            mma_commit(mybar);
+        }
+        ok = mbar_wait_bounded(mybar, parity);
+        parity ^= 1u;
+        if (wg_sync_or(wg, !ok)) { failed = true; break; }
+        tc_after();
+        float o16[16];
+        tmem_ld16(tmem, o16);
+
+        // ---- epilogue ----
+        if (t < count) {
+            if (ROWS) {
+                const int64_t row = (int64_t)tile * kRows + t;
+#pragma unroll
+                for (int k = 0; k < kOut; ++k) out[row * kOut + k] = o16[k] + b3[k];
+            } else {
+                // Energy limit: the correction d may not raise the cell's energy
+                // E(f) = rho/2 |v|^2 + (s:s - c tr(s)^2) / (4 mu), c = lambda / (3 lambda + 2 mu)
+                // (the energy audit's density).  E(f + a d) = E(f) + 2 a B + a^2 Q, so the
+                // largest admissible a in [0, 1] is -2B/Q when B < 0, else 0.  A network
+                // trained on one-step targets is otherwise free to feed energy back into
+                // the strip and grow over long runs.
+                float d[kOut];
+#pragma unroll
+                for (int k = 0; k < kOut; ++k) d[k] = (o16[k] + b3[k]) * s / (k < 3 ? zimp : 1.0f);
+                const float rho = 1.0f / m.b[gc], lam = m.lam[gc], mu = m.mu[gc];
+                const float cc = lam / (3.0f * lam + 2.0f * mu), i4m = 0.25f / mu;
+                const float trf = fc[3] + fc[4] + fc[5], trd = d[3] + d[4] + d[5];
+                const float B = 0.5f * rho * (fc[0] * d[0] + fc[1] * d[1] + fc[2] * d[2]) +
+                                i4m * (fc[3] * d[3] + fc[4] * d[4] + fc[5] * d[5] +
+                                       2.0f * (fc[6] * d[6] + fc[7] * d[7] + fc[8] * d[8]) - cc * trf * trd);
+                const float Q = 0.5f * rho * (d[0] * d[0] + d[1] * d[1] + d[2] * d[2]) +
+                                i4m * (d[3] * d[3] + d[4] * d[4] + d[5] * d[5] +
+                                       2.0f * (d[6] * d[6] + d[7] * d[7] + d[8] * d[8]) - cc * trd * trd);
+                const float a = (Q > 0.0f && B < 0.0f) ? fminf(1.0f, -2.0f * B / Q) : 0.0f;
+                float *dt = delta + (int64_t)tile * (kRows * kOut);
+#pragma unroll
+                for (int k = 0; k < kOut; ++k) dt[k * kRows + t] = a * d[k];
+            }
+        }
+    }
+    if (failed) {
+        if (t == 0) atomicOr(err, 4);
+        mbar_wait_bounded(mybar, parity ^ 1u);   // the commit the failed wait was for
+    }
+    tc_before();
+    __syncthreads();
+    if (warp == 0) {
+        tc_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(kTmemCols)
+                     : "memory");
+    }
+}
+
+// One CTA per SM (fewer for small strips): each runs two warpgroups.
+int tc_grid(int ntiles) {
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return std::max(1, std::min(sms, (ntiles + 1) / 2));
+}
+
+// Adds the corrections to the strip cells (after every cell's correction has
+// been computed from the uncorrected state).  One block per tile.
+__global__ void __launch_bounds__(kRows) k_strip_apply(Model m, const int4 *tiles, const float *delta) {
+    const Box bx = box_of(tiles[blockIdx.x]);
+    const int t = threadIdx.x;
+    if (t >= bx.ex * bx.ey * bx.ez) return;
+    const int lx = t % bx.ex, ly = (t / bx.ex) % bx.ey, lz = t / (bx.ex * bx.ey);
+    const int64_t c = pidx(m, bx.x + lx + kHalo, bx.y + ly + kHalo, bx.z + lz + kHalo);
+    const float *dt = delta + (int64_t)blockIdx.x * (kRows * kOut);
+#pragma unroll
+    for (int k = 0; k < kOut; ++k) m.f[k][c] += dt[k * kRows + t];
 }
 
 // ---- training kernels ------------------------------------------------------
@@ -317,6 +641,40 @@ int sgfd_mlp_forward(int32_t device, const float *params, const float *X, int64_
     return SGFD_OK;
 }
 
+int sgfd_mlp_infer(int32_t device, const float *params, const float *X, int64_t n, float *out) {
+    if (!params || !X || !out || n <= 0 || n > ((int64_t)1 << 30))
+        return fail(nullptr, SGFD_ERR_INVALID, "bad MLP inference arguments");
+    cudaError_t e = cudaSetDevice(device);
+    unsigned char *img = nullptr;
+    float *dp = nullptr, *dX = nullptr, *dout = nullptr;
+    int *err = nullptr;
+    const int nt = (int)((n + kRows - 1) / kRows);
+    if (e == cudaSuccess) e = strip_prepare();
+    if (e == cudaSuccess) e = cudaMalloc(&img, kImgPad + 16);
+    if (e == cudaSuccess) e = cudaMalloc(&dp, kParams * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&dX, (size_t)n * kIn * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&dout, (size_t)n * kOut * sizeof(float));
+    if (e == cudaSuccess) e = cudaMemset(img, 0, kImgPad + 16);
+    if (e == cudaSuccess) e = cudaMemcpy(dp, params, kParams * sizeof(float), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(dX, X, (size_t)n * kIn * sizeof(float), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        err = reinterpret_cast<int *>(img + kImgPad);
+        k_weight_image<<<64, 256>>>(dp, img);
+        k_strip_tc<true><<<tc_grid(nt), 256, kTcSmem>>>(Model{}, 0, nullptr, 0, img, nullptr, dX, n, dout, err);
+        e = cudaGetLastError();
+    }
+    int flag = 0;
+    if (e == cudaSuccess) e = cudaMemcpy(out, dout, (size_t)n * kOut * sizeof(float), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(&flag, err, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaFree(img);
+    cudaFree(dp);
+    cudaFree(dX);
+    cudaFree(dout);
+    if (e != cudaSuccess) return mlp_fail("MLP inference", e);
+    if (flag) return fail(nullptr, SGFD_ERR_CUDA, "MLP inference: a bounded wait for tensor-core results gave up");
+    return SGFD_OK;
+}
+
 int sgfd_mlp_gradient(int32_t device, const float *params, const float *X, const float *Y, int32_t n, float *loss,
                       float *grad) {
     if (!params || !X || !Y || !grad || n <= 0) return fail(nullptr, SGFD_ERR_INVALID, "bad MLP gradient arguments");
@@ -400,15 +758,26 @@ int sgfd_set_learned_strip(sgfd_solver *h, int32_t width, const float *params) {
     const Model &m = h->m;
     if (2 * width >= std::min(m.nxc, std::min(m.nyc, m.nzc)))
         return fail(h, SGFD_ERR_INVALID, "strip width %d leaves no interior", width);
-    std::vector<int4> cells;
-    const int n = strip_cell_list(m, width, cells);
+    std::vector<int4> tiles;
+    const int nt = strip_tile_list(m, width, tiles);
+    if (nt <= 0) return fail(h, SGFD_ERR_INVALID, "strip width %d: no strip tiling", width);
     SG_CUDA(h, strip_prepare(), "strip kernel set-up");
-    SG_CUDA(h, cudaMalloc(&h->strip_cells, (size_t)n * sizeof(int4)), "strip cell list");
-    SG_CUDA(h, cudaMalloc(&h->strip_buf, ((size_t)kParams + (size_t)n * kOut) * sizeof(float)), "strip buffers");
-    SG_CUDA(h, cudaMemcpy(h->strip_cells, cells.data(), (size_t)n * sizeof(int4), cudaMemcpyHostToDevice), "strip cells");
-    SG_CUDA(h, cudaMemcpy(h->strip_buf, params, (size_t)kParams * sizeof(float), cudaMemcpyHostToDevice), "strip parameters");
+    SG_CUDA(h, cudaMalloc(&h->strip_cells, (size_t)nt * sizeof(int4)), "strip tiles");
+    SG_CUDA(h, cudaMalloc(&h->strip_buf, strip_buffer_bytes(nt)), "strip buffers");
+    SG_CUDA(h, cudaMemcpy(h->strip_cells, tiles.data(), (size_t)nt * sizeof(int4), cudaMemcpyHostToDevice), "strip tiles");
+    SG_CUDA(h, cudaMemset(h->strip_buf, 0, strip_buffer_bytes(nt)), "strip buffers");
+    float *dp = nullptr;
+    SG_CUDA(h, cudaMalloc(&dp, (size_t)kParams * sizeof(float)), "strip parameters");
+    cudaError_t e = cudaMemcpy(dp, params, (size_t)kParams * sizeof(float), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        k_weight_image<<<64, 256>>>(dp, reinterpret_cast<unsigned char *>(h->strip_buf));
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    cudaFree(dp);
+    if (e != cudaSuccess) return cuda_fail(h, e, "strip weight image");
     h->strip_w = width;
-    h->strip_n = n;
+    h->strip_n = nt;
     return SGFD_OK;
 }
 
@@ -454,25 +823,51 @@ int sgfd_strip_features(sgfd_solver *h, int32_t width, int32_t n, const int32_t 
 
 namespace sgfd {
 
-int strip_cell_list(const Model &m, int w, std::vector<int4> &cells) {
-    cells.clear();
-    for (int z = 0; z < m.nzc; ++z)
-        for (int y = 0; y < m.nyc; ++y)
-            for (int x = 0; x < m.nxc; ++x) {
-                const bool in = x < w || y < w || z < w || x >= m.nxc - w || y >= m.nyc - w || z >= m.nzc - w;
-                if (in) cells.push_back(make_int4(x, y, z, 0));
-            }
-    return (int)cells.size();
+// Boxes of at most 128 strip cells covering the strip once: the two z faces
+// in 32 x 4 x 1 boxes, the two y faces (between the z faces) in 32 x 2 x 2,
+// the two x faces (between the others) in min(w, 32) x 4 x rest.  Each tile is
+// (x, y, z, ex | ey << 8 | ez << 16) in computed coordinates; -1 if a box
+// would not fit the staging area.
+int strip_tile_list(const Model &m, int w, std::vector<int4> &tiles) {
+    tiles.clear();
+    bool fits = true;
+    auto boxes = [&](int x0, int x1, int y0, int y1, int z0, int z1, int ex, int ey, int ez) {
+        fits = fits && ex * ey * ez <= kRows && (ex + 2) * (ey + 2) * (ez + 2) <= kStage;
+        for (int z = z0; z < z1; z += ez)
+            for (int y = y0; y < y1; y += ey)
+                for (int x = x0; x < x1; x += ex)
+                    tiles.push_back(make_int4(x, y, z, std::min(ex, x1 - x) | std::min(ey, y1 - y) << 8 |
+                                                           std::min(ez, z1 - z) << 16));
+    };
+    const int X = m.nxc, Y = m.nyc, Z = m.nzc;
+    boxes(0, X, 0, Y, 0, w, 32, 4, 1);
+    boxes(0, X, 0, Y, Z - w, Z, 32, 4, 1);
+    boxes(0, X, 0, w, w, Z - w, 32, 2, 2);
+    boxes(0, X, Y - w, Y, w, Z - w, 32, 2, 2);
+    const int ex = std::min(w, 32), ey = std::min(4, kRows / ex), ez = kRows / ex / ey;
+    boxes(0, w, w, Y - w, w, Z - w, ex, ey, ez);
+    boxes(X - w, X, w, Y - w, w, Z - w, ex, ey, ez);
+    return fits ? (int)tiles.size() : -1;
+}
+
+// Strip buffer: weight image, corrections [tile][9][128], error flag.
+size_t strip_buffer_bytes(int ntiles) { return (size_t)kImgPad + (size_t)ntiles * kRows * kOut * 4 + 16; }
+int *strip_error_flag(float *buf, int ntiles) {
+    return reinterpret_cast<int *>(reinterpret_cast<unsigned char *>(buf) + strip_buffer_bytes(ntiles) - 16);
 }
 
 cudaError_t strip_prepare() {
-    return cudaFuncSetAttribute(k_strip_mlp, cudaFuncAttributeMaxDynamicSharedMemorySize, kParams * (int)sizeof(float));
+    cudaError_t e = cudaFuncSetAttribute(k_strip_tc<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_strip_tc<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem);
+    return e;
 }
 
-cudaError_t launch_strip(const Model &m, int w, const int4 *cells, int n, const float *params, float *delta,
-                         cudaStream_t s) {
-    k_strip_mlp<<<cdiv(n, 128), 128, kParams * sizeof(float), s>>>(m, w, cells, n, params, delta);
-    k_strip_apply<<<cdiv(n, 256), 256, 0, s>>>(m, cells, n, delta);
+cudaError_t launch_strip(const Model &m, int w, const int4 *tiles, int ntiles, float *buf, cudaStream_t s) {
+    const unsigned char *img = reinterpret_cast<const unsigned char *>(buf);
+    float *delta = reinterpret_cast<float *>(reinterpret_cast<unsigned char *>(buf) + kImgPad);
+    k_strip_tc<false><<<tc_grid(ntiles), 256, kTcSmem, s>>>(m, w, tiles, ntiles, img, delta, nullptr, 0, nullptr,
+                                                            strip_error_flag(buf, ntiles));
+    k_strip_apply<<<ntiles, kRows, 0, s>>>(m, tiles, delta);
     return cudaGetLastError();
 }
 

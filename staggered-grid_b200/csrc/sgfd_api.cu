@@ -53,13 +53,17 @@ int check_handle(sgfd_solver *h) {
 }
 
 int check_device_error(sgfd_solver *h) {
-    if (!h->dev_err) return SGFD_OK;
-    int flag = 0;
-    SG_CUDA(h, cudaMemcpyAsync(&flag, h->dev_err, sizeof(int), cudaMemcpyDeviceToHost, h->stream), "error flag");
-    SG_CUDA(h, cudaStreamSynchronize(h->stream), "error flag");
-    if (flag) {
-        cudaMemsetAsync(h->dev_err, 0, sizeof(int), h->stream);
-        return fail(h, SGFD_ERR_CUDA, "a kernel's bounded wait for its TMA copies gave up (flag %d)", flag);
+    int *flags[2] = {h->dev_err, h->strip_n > 0 ? strip_error_flag(h->strip_buf, h->strip_n) : nullptr};
+    for (int *f : flags) {
+        if (!f) continue;
+        int flag = 0;
+        SG_CUDA(h, cudaMemcpyAsync(&flag, f, sizeof(int), cudaMemcpyDeviceToHost, h->stream), "error flag");
+        SG_CUDA(h, cudaStreamSynchronize(h->stream), "error flag");
+        if (flag) {
+            cudaMemsetAsync(f, 0, sizeof(int), h->stream);
+            return fail(h, SGFD_ERR_CUDA, "a kernel's bounded wait for its %s gave up (flag %d)",
+                        f == h->dev_err ? "TMA copies" : "tensor-core results", flag);
+        }
     }
     return SGFD_OK;
 }
@@ -112,8 +116,7 @@ cudaError_t dispatch_on(sgfd_solver *h, const SourceRec &sr, cudaStream_t s, int
                         ? zmarch_step(h->m, h->ph, sr, h->zg, h->vm, h->sm, it, value, use_wavelet, s, ev)
                         : simple_step(h->m, h->ph, sr, it, value, use_wavelet, s, ev);
     if (e == cudaSuccess && h->strip_n > 0)
-        e = launch_strip(h->m, h->strip_w, h->strip_cells, h->strip_n, h->strip_buf,
-                         h->strip_buf + mlp_params(), s);
+        e = launch_strip(h->m, h->strip_w, h->strip_cells, h->strip_n, h->strip_buf, s);
     if (e == cudaSuccess && h->audit_every > 0) {
         const AuditGate gt{sr.it_dev, it, h->audit_every, h->audit_count, h->audit_hist};
         e = launch_energy_step(audit_model(h), h->ph, h->audit_region, h->audit, h->audit_blocks, gt, s);

@@ -24,7 +24,7 @@ struct GraphKey {
     int audit_every, audit_region, audit_count;
     double *audit_hist, *audit;
     int strip_w, strip_n;
-    int4 *strip_cells;
+    int4 *strip_cells;   // tiles
     float *strip_buf;
 };
 // Steps per captured graph; sgfd_run launches the remainder directly.
@@ -110,12 +110,15 @@ cudaError_t dispatch_on(sgfd_solver *h, const SourceRec &sr, cudaStream_t s, int
 // Byte image of everything a captured step passes to h's kernels.
 void graph_key(const sgfd_solver *h, GraphKey *k);
 
-// Learned strip (learned.cu): the strip's cells (computed coordinates), the
-// kernel set-up, and one correction pass (MLP then apply).
-int strip_cell_list(const Model &m, int w, std::vector<int4> &cells);
+// Learned strip (learned.cu): the strip's tiles (boxes of at most 128 cells),
+// the size of its device buffer (weight image, corrections, error flag), the
+// error flag inside it, the kernel set-up, and one correction pass (network
+// then apply).
+int strip_tile_list(const Model &m, int w, std::vector<int4> &tiles);
+size_t strip_buffer_bytes(int ntiles);
+int *strip_error_flag(float *buf, int ntiles);
 cudaError_t strip_prepare();
-cudaError_t launch_strip(const Model &m, int w, const int4 *cells, int n, const float *params, float *delta,
-                         cudaStream_t s);
+cudaError_t launch_strip(const Model &m, int w, const int4 *tiles, int ntiles, float *buf, cudaStream_t s);
 int mlp_params();
 
 inline size_t round_up(size_t v, size_t a) { return (v + a - 1) / a * a; }

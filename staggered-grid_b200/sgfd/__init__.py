@@ -136,6 +136,7 @@ def lib() -> ctypes.CDLL:
         "sgfd_strip_features": (ctypes.c_int, [vp, i32, i32, ip, fp, fp, fp]),
         "sgfd_mlp_param_count": (ctypes.c_int, []),
         "sgfd_mlp_forward": (ctypes.c_int, [i32, fp, fp, ctypes.c_int64, fp]),
+        "sgfd_mlp_infer": (ctypes.c_int, [i32, fp, fp, ctypes.c_int64, fp]),
         "sgfd_mlp_gradient": (ctypes.c_int, [i32, fp, fp, fp, i32, fp, fp]),
         "sgfd_mlp_train": (ctypes.c_int, [i32, fp, fp, fp, ctypes.c_int64, i32, i32, ctypes.c_float, fp]),
         "sgfd_energy": (ctypes.c_int, [vp, i32, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
@@ -493,6 +494,15 @@ def mlp_forward(params, X, device: int = 0) -> np.ndarray:
     X = np.ascontiguousarray(X, np.float32)
     out = np.zeros((len(X), 9), np.float32)
     _check_global(lib().sgfd_mlp_forward(device, _fptr(p), _fptr(X), len(X), _fptr(out)))
+    return out
+
+
+def mlp_infer(params, X, device: int = 0) -> np.ndarray:
+    """The strip's tensor-core inference (FP16 operands, FP32 accumulation) on rows X."""
+    p = np.ascontiguousarray(params, np.float32)
+    X = np.ascontiguousarray(X, np.float32)
+    out = np.zeros((len(X), 9), np.float32)
+    _check_global(lib().sgfd_mlp_infer(device, _fptr(p), _fptr(X), len(X), _fptr(out)))
     return out
 
 

@@ -21,3 +21,18 @@ def test_oracle_gradient_matches_finite_differences():
         fd = (mo.loss_and_gradient(p + e, X, Y)[0] - mo.loss_and_gradient(p - e, X, Y)[0]) / (2 * h)
         assert abs(fd - g[i]) <= 1e-6 + 1e-5 * abs(fd), (i, fd, g[i])
     assert mo.N_PARAMS == 20937
+
+
+def test_f16_forward_rounds_operands_and_stays_near_fp64():
+    """forward_f16 rounds to binary16 with ties to even, and the FP16 operand
+    rounding moves the network's outputs by well under 1e-2 of the largest."""
+    assert mo.f16(1.0 + 2.0 ** -11) == 1.0                    # tie -> even
+    assert mo.f16(1.0 + 3 * 2.0 ** -11) == 1.0 + 2.0 ** -9    # tie -> even (up)
+    assert mo.f16(65504.0) == 65504.0 and mo.f16(2.0 ** -24) == 2.0 ** -24
+    rng = np.random.default_rng(2)
+    p = rng.standard_normal(mo.N_PARAMS) * 0.1
+    X = rng.standard_normal((256, mo.N_IN))
+    exact, _ = mo.forward(p, X)
+    approx = mo.forward_f16(p, X)
+    err = np.abs(approx - exact).max() / np.abs(exact).max()
+    assert 1e-5 < err < 1e-2, err
