@@ -26,9 +26,11 @@
 // width x 4 x 5 on the x faces for width 6); a box's fields and their one-cell
 // halo are staged in shared memory with coalesced loads, and each thread
 // builds its cell's 252 inputs from there into row t of the A operand.
-// Each CTA (one per SM) holds the weights once and runs two warpgroups that
-// work on alternate tiles, so one warpgroup's loads overlap the other's
-// tensor-core and epilogue work.
+// Each CTA (one per SM) holds the weights once and runs two groups of 256
+// threads that work on alternate tiles, so one group's loads overlap the
+// other's tensor-core and epilogue work; two threads share each row.  The
+// hidden layers' GELU uses an erfc approximation (Abramowitz & Stegun 7.1.26,
+// |error| <= 1.5e-7) on the special-function unit.
 //
 // Training (sgfd_mlp_train) runs minibatch Adam with hand-written kernels:
 // a tiled FP32 GEMM, bias + GELU, the output loss (mean squared error over the
@@ -73,16 +75,18 @@ __device__ __forceinline__ float strip_inputs(const Model &m, int w, int cx, int
     const float b = m.b[c], lam = m.lam[c], mu = m.mu[c];
     const float rho = 1.0f / b, vp = sqrtf((lam + 2.0f * mu) * b), vs = sqrtf(mu * b);
     zimp = rho * vp;
-    float ss = 0.0f;
+    // sum of squares in two parts (neighbours 0..13 and 14..26), added at the
+    // end: the order in which the inference kernel's two threads of a row sum
+    float ss[2] = {0.0f, 0.0f};
     for (int n = 0; n < 27; ++n) {
         const int64_t o = c + (n % 3 - 1) + (int64_t)((n / 3) % 3 - 1) * m.px + (int64_t)(n / 9 - 1) * m.plane;
 #pragma unroll
         for (int k = 0; k < 9; ++k) {
             const float u = m.f[k][o] * (k < 3 ? zimp : 1.0f);
-            ss = fmaf(u, u, ss);
+            ss[n >= 14] = fmaf(u, u, ss[n >= 14]);
         }
     }
-    const float s = sqrtf(ss * (1.0f / 243.0f));
+    const float s = sqrtf((ss[0] + ss[1]) * (1.0f / 243.0f));
     const float inv = s > 0.0f ? 1.0f / s : 0.0f;
     for (int n = 0; n < 27; ++n) {
         const int64_t o = c + (n % 3 - 1) + (int64_t)((n / 3) % 3 - 1) * m.px + (int64_t)(n / 9 - 1) * m.plane;
@@ -123,8 +127,10 @@ constexpr int kImgW1 = 0, kImgW2 = kImgW1 + kH * kK1 * 2, kImgW3 = kImgW2 + kH *
 constexpr int kImgPad = (kImg + 1023) / 1024 * 1024;
 constexpr int kAOp = kRows * kK1 * 2;                        // A operand of one warpgroup
 constexpr int kStg = 9 * kStage * 4;                         // staged fields of one warpgroup
-constexpr int kWgBytes = kAOp + (kStg + 1023) / 1024 * 1024;
+constexpr int kRed = 2 * kRows * 4;                          // partial sums of squares of one warpgroup
+constexpr int kWgBytes = kAOp + (kStg + 1023) / 1024 * 1024 + kRed;
 constexpr int kTcSmem = 1024 + kImgPad + 2 * kWgBytes + 64;  // + alignment, barriers, TMEM address
+constexpr int kTcThreads = 512;                              // two warpgroups of 256: two threads per row
 static_assert(kImg % 16 == 0, "weight image is copied in 16-byte pieces");
 static_assert(kTcSmem <= 232448, "shared memory of one CTA");
 constexpr uint32_t kTmemCols = 256;                          // 128 per warpgroup: D1/D3 at +0, D2 at +64
@@ -169,15 +175,16 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity
 __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 __device__ __forceinline__ void tc_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-// Barrier of one warpgroup (named barrier 1 + wg) that also ORs a flag over it.
-__device__ __forceinline__ bool wg_sync_or(int wg, bool flag) {
+// Barrier of one 256-thread warpgroup pair (named barrier 1 + g) that also
+// ORs a flag over it.
+__device__ __forceinline__ bool wg_sync_or(int g, bool flag) {
     uint32_t r;
     asm volatile(
-        "{\n .reg .pred p, q;\n setp.ne.u32 p, %1, 0;\n bar.red.or.pred q, %2, 128, p;\n selp.u32 %0, 1, 0, q;\n}\n"
-        : "=r"(r) : "r"((uint32_t)flag), "r"(wg + 1) : "memory");
+        "{\n .reg .pred p, q;\n setp.ne.u32 p, %1, 0;\n bar.red.or.pred q, %2, 256, p;\n selp.u32 %0, 1, 0, q;\n}\n"
+        : "=r"(r) : "r"((uint32_t)flag), "r"(g + 1) : "memory");
     return r != 0;
 }
-__device__ __forceinline__ void wg_sync(int wg) { asm volatile("bar.sync %0, 128;" ::"r"(wg + 1) : "memory"); }
+__device__ __forceinline__ void wg_sync(int g) { asm volatile("bar.sync %0, 256;" ::"r"(g + 1) : "memory"); }
 
 // D[tmem] (+)= A[a] * B[b]^T over KT columns, M = 128, N = n, K = 16 per instruction.
 __device__ __forceinline__ void mma_chain(uint32_t tmem_d, uint32_t a, uint32_t b, int KT, int n) {
@@ -216,19 +223,45 @@ __device__ __forceinline__ void store_chunk(unsigned char *p, const float (&v)[8
                                                pack_half2(v[4], v[5]), pack_half2(v[6], v[7]));
 }
 
-// Hidden layer: 64 accumulator columns of this thread's row, + bias, GELU,
-// FP16 into row t of the next A operand (K = 64).
-__device__ __forceinline__ void hidden_layer(uint32_t taddr, const float *bias, unsigned char *a_op, int t) {
+__device__ __forceinline__ float rcp_approx(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ float ex2_approx(float x) {
+    float r;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+// GELU(x) = x Phi(x), Phi(x) = erfc(-x / sqrt 2) / 2, with erfc from
+// Abramowitz & Stegun 7.1.26 (Hastings' approximation): for z >= 0,
+// erfc(z) = t (a1 + t (a2 + t (a3 + t (a4 + t a5)))) exp(-z^2), t = 1 / (1 + p z),
+// |error| <= 1.5e-7; exp(-z^2) = 2^(-x^2 / (2 ln 2)).  Far below the half
+// ulp of the binary16 the activation is stored in (2.4e-4 relative).
+__device__ __forceinline__ float gelu_fast(float x) {
+    const float z = fabsf(x) * 0.70710678f;
+    const float t = rcp_approx(fmaf(0.3275911f, z, 1.0f));
+    float p = fmaf(t, 1.061405429f, -1.453152027f);
+    p = fmaf(t, p, 1.421413741f);
+    p = fmaf(t, p, -0.284496736f);
+    p = fmaf(t, p, 0.254829592f);
+    const float half_erfc = 0.5f * (t * p) * ex2_approx(-(x * x) * 0.72134752f);
+    return x * (x >= 0.0f ? 1.0f - half_erfc : half_erfc);
+}
+
+// Hidden layer, columns c0 .. c0+31 of this thread's row: accumulators + bias,
+// GELU, FP16 into row t of the next A operand (K = 64).
+__device__ __forceinline__ void hidden_half(uint32_t taddr, const float *bias, unsigned char *a_op, int t, int c0) {
 #pragma unroll
-    for (int c = 0; c < kH / 16; ++c) {
+    for (int c = 0; c < 2; ++c) {
         float v[16];
-        tmem_ld16(taddr + c * 16, v);
+        tmem_ld16(taddr + c0 + c * 16, v);
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
             float g[8];
 #pragma unroll
-            for (int q = 0; q < 8; ++q) g[q] = gelu(v[8 * h + q] + bias[16 * c + 8 * h + q]);
-            store_chunk(a_op + kmaj(t, 16 * c + 8 * h, kH), g);
+            for (int q = 0; q < 8; ++q) g[q] = gelu_fast(v[8 * h + q] + bias[c0 + 16 * c + 8 * h + q]);
+            store_chunk(a_op + kmaj(t, c0 + 16 * c + 8 * h, kH), g);
         }
     }
 }
@@ -260,20 +293,64 @@ struct Box {
 };
 __device__ __forceinline__ Box box_of(int4 td) { return {td.x, td.y, td.z, td.w & 255, (td.w >> 8) & 255, (td.w >> 16) & 255}; }
 
+// Sum of squares of the 9 staged fields (velocities times zimp) over the
+// neighbours n0 .. n1-1 of the staged cell c0.
+template <int N0, int N1>
+__device__ __forceinline__ float staged_squares(const float *stg, int c0, int sx, int sxy, float zimp) {
+    float ss = 0.0f;
+#pragma unroll
+    for (int n = N0; n < N1; ++n) {
+        const int o = c0 + (n % 3 - 1) + ((n / 3) % 3 - 1) * sx + (n / 9 - 1) * sxy;
+#pragma unroll
+        for (int k = 0; k < 9; ++k) {
+            const float u = stg[k * kStage + o] * (k < 3 ? zimp : 1.0f);
+            ss = fmaf(u, u, ss);
+        }
+    }
+    return ss;
+}
+
+// Inputs J0*8 .. J0*8+127 of row t (16 chunks of 8) from the staged fields.
+template <int J0>
+__device__ __forceinline__ void staged_inputs(const float *stg, int c0, int sx, int sxy, float zimp, float inv,
+                                              const float (&ext)[9], unsigned char *a_op, int t) {
+#pragma unroll
+    for (int j = J0; j < J0 + 16; ++j) {
+        float v[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int f = 8 * j + q;
+            if (f < 243) {
+                const int n = f / 9, k = f % 9;
+                const int o = c0 + (n % 3 - 1) + ((n / 3) % 3 - 1) * sx + (n / 9 - 1) * sxy;
+                v[q] = stg[k * kStage + o] * (k < 3 ? zimp : 1.0f) * inv;
+            } else {
+                v[q] = f < kIn ? ext[f - 243] : 0.0f;
+            }
+        }
+        store_chunk(a_op + kmaj(t, 8 * j, kK1), v);
+    }
+}
+
 // Network of every strip cell (ROWS = false), or of n input rows X (ROWS =
 // true: the tensor-core path checked on given inputs, raw outputs to out).
-// One CTA per SM, two warpgroups; warpgroup wg takes tiles 2*blockIdx.x + wg,
-// then every 2*gridDim.x-th.  Thread t of a warpgroup owns row t of its tiles
-// (TMEM lane t).  delta[tile][k][128] receives the energy-limited corrections.
+// One CTA per SM with 512 threads in two groups of 256; group g takes tiles
+// 2*blockIdx.x + g, then every 2*gridDim.x-th.  In a group, threads t and
+// t + 128 (warps w and w + 4, which reach the same TMEM lanes) share row t of
+// a tile: half h = 0 takes neighbours 0..13, inputs 0..127 and hidden
+// columns 0..31, half h = 1 neighbours 14..26, inputs 128..255 (with the 9
+// cell inputs) and hidden columns 32..63; half 0 runs the epilogue.
+// delta[tile][k][128] receives the energy-limited corrections.
 template <bool ROWS>
-__global__ void __launch_bounds__(256, 1)
+__global__ void __launch_bounds__(kTcThreads, 1)
 k_strip_tc(Model m, int w, const int4 *tiles, int ntiles, const unsigned char *wimg, float *delta, const float *X,
            int64_t nrows, float *out, int *err) {
     extern __shared__ unsigned char smem_raw[];
     unsigned char *sm = smem_raw + ((1024 - (saddr_of(smem_raw) & 1023)) & 1023);
-    const int tid = threadIdx.x, wg = tid >> 7, t = tid & 127, warp = tid >> 5;
-    unsigned char *a_op = sm + kImgPad + wg * kWgBytes;
+    const int tid = threadIdx.x, g = tid >> 8, u = tid & 255, h = u >> 7, t = u & 127, warp = tid >> 5;
+    unsigned char *a_op = sm + kImgPad + g * kWgBytes;
     float *stg = reinterpret_cast<float *>(a_op + kAOp);
+    float *red = reinterpret_cast<float *>(a_op + kWgBytes - kRed);
     uint64_t *bar = reinterpret_cast<uint64_t *>(sm + kImgPad + 2 * kWgBytes);
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bar + 2);
 
@@ -290,17 +367,18 @@ k_strip_tc(Model m, int w, const int4 *tiles, int ntiles, const unsigned char *w
     __syncthreads();
     tc_after();
     const uint32_t tmem_base = *tmem_slot;
-    const uint32_t tmem = tmem_base + (uint32_t)(wg * 128) + ((uint32_t)((warp & 3) * 32) << 16);
+    const uint32_t tmem_g = tmem_base + (uint32_t)(g * 128);
+    const uint32_t tmem = tmem_g + ((uint32_t)((warp & 3) * 32) << 16);
     const uint32_t a_s = saddr_of(a_op), w1_s = saddr_of(sm + kImgW1), w2_s = saddr_of(sm + kImgW2),
                    w3_s = saddr_of(sm + kImgW3);
     const float *b1 = reinterpret_cast<const float *>(sm + kImgB), *b2 = b1 + kH, *b3 = b2 + kH;
-    uint64_t *mybar = &bar[wg];
+    uint64_t *mybar = &bar[g];
     uint32_t parity = 0;
     bool failed = false;
 
     const int nt = ROWS ? (int)((nrows + kRows - 1) / kRows) : ntiles;
-    for (int tile = 2 * blockIdx.x + wg; tile < nt; tile += 2 * gridDim.x) {
-        // ---- inputs: row t of the A operand ----
+    for (int tile = 2 * blockIdx.x + g; tile < nt; tile += 2 * gridDim.x) {
+        // ---- inputs: row t of the A operand, half h ----
         float s = 0.0f, zimp = 1.0f, fc[kOut];
         int count;
         int64_t gc = 0;
@@ -309,7 +387,7 @@ k_strip_tc(Model m, int w, const int4 *tiles, int ntiles, const unsigned char *w
             count = (int)(nrows - first < kRows ? nrows - first : kRows);
             const float *x = X + row * kIn;
 #pragma unroll 4
-            for (int j = 0; j < kK1 / 8; ++j) {
+            for (int j = 16 * h; j < 16 * h + 16; ++j) {
                 float v[8];
 #pragma unroll
                 for (int q = 0; q < 8; ++q) v[q] = (t < count && 8 * j + q < kIn) ? x[8 * j + q] : 0.0f;
@@ -318,33 +396,34 @@ k_strip_tc(Model m, int w, const int4 *tiles, int ntiles, const unsigned char *w
         } else {
             const Box bx = box_of(tiles[tile]);
             const int sx = bx.ex + 2, sxy = sx * (bx.ey + 2), ns = sxy * (bx.ez + 2);
-            for (int r = t; r < ns; r += kRows) {
+            for (int r = u; r < ns; r += 2 * kRows) {
                 const int lx = r % sx, ly = (r / sx) % (bx.ey + 2), lz = r / sxy;
                 const int64_t gi = pidx(m, bx.x - 1 + lx + kHalo, bx.y - 1 + ly + kHalo, bx.z - 1 + lz + kHalo);
 #pragma unroll
                 for (int k = 0; k < 9; ++k) stg[k * kStage + r] = m.f[k][gi];
             }
-            wg_sync(wg);
+            wg_sync(g);
             count = bx.ex * bx.ey * bx.ez;
+            int c0 = 0, cx = 0, cy = 0, cz = 0;
+            float rho = 0.0f, vp = 0.0f, vs = 0.0f;
             if (t < count) {
                 const int lx = t % bx.ex, ly = (t / bx.ex) % bx.ey, lz = t / (bx.ex * bx.ey);
-                const int cx = bx.x + lx, cy = bx.y + ly, cz = bx.z + lz;
-                const int c0 = (lx + 1) + (ly + 1) * sx + (lz + 1) * sxy;
+                cx = bx.x + lx;
+                cy = bx.y + ly;
+                cz = bx.z + lz;
+                c0 = (lx + 1) + (ly + 1) * sx + (lz + 1) * sxy;
                 gc = pidx(m, cx + kHalo, cy + kHalo, cz + kHalo);
                 const float b = m.b[gc], lam = m.lam[gc], mu = m.mu[gc];
-                const float rho = 1.0f / b, vp = sqrtf((lam + 2.0f * mu) * b), vs = sqrtf(mu * b);
+                rho = 1.0f / b;
+                vp = sqrtf((lam + 2.0f * mu) * b);
+                vs = sqrtf(mu * b);
                 zimp = rho * vp;
-                float ss = 0.0f;
-#pragma unroll
-                for (int n = 0; n < 27; ++n) {
-                    const int o = c0 + (n % 3 - 1) + ((n / 3) % 3 - 1) * sx + (n / 9 - 1) * sxy;
-#pragma unroll
-                    for (int k = 0; k < 9; ++k) {
-                        const float u = stg[k * kStage + o] * (k < 3 ? zimp : 1.0f);
-                        ss = fmaf(u, u, ss);
-                    }
-                }
-                s = sqrtf(ss * (1.0f / 243.0f));
+                red[h * kRows + t] = h == 0 ? staged_squares<0, 14>(stg, c0, sx, sxy, zimp)
+                                            : staged_squares<14, 27>(stg, c0, sx, sxy, zimp);
+            }
+            wg_sync(g);
+            if (t < count) {
+                s = sqrtf((red[t] + red[kRows + t]) * (1.0f / 243.0f));
                 const float inv = s > 0.0f ? 1.0f / s : 0.0f;
                 float ext[9];
                 ext[0] = vp * (1.0f / 3000.0f);
@@ -353,111 +432,102 @@ k_strip_tc(Model m, int w, const int4 *tiles, int ntiles, const unsigned char *w
                 band_of(cx, m.nxc, w, ext[3], ext[6]);
                 band_of(cy, m.nyc, w, ext[4], ext[7]);
                 band_of(cz, m.nzc, w, ext[5], ext[8]);
+                if (h == 0) {
+                    staged_inputs<0>(stg, c0, sx, sxy, zimp, inv, ext, a_op, t);
 #pragma unroll
-                for (int j = 0; j < kK1 / 8; ++j) {
-                    float v[8];
-#pragma unroll
-                    for (int q = 0; q < 8; ++q) {
-                        const int f = 8 * j + q;
-                        if (f < 243) {
-                            const int n = f / 9, k = f % 9;
-                            const int o = c0 + (n % 3 - 1) + ((n / 3) % 3 - 1) * sx + (n / 9 - 1) * sxy;
-                            v[q] = stg[k * kStage + o] * (k < 3 ? zimp : 1.0f) * inv;
-                        } else {
-                            v[q] = f < kIn ? ext[f - 243] : 0.0f;
-                        }
-                    }
-                    store_chunk(a_op + kmaj(t, 8 * j, kK1), v);
+                    for (int k = 0; k < kOut; ++k) fc[k] = stg[k * kStage + c0];
+                } else {
+                    staged_inputs<16>(stg, c0, sx, sxy, zimp, inv, ext, a_op, t);
                 }
-#pragma unroll
-                for (int k = 0; k < kOut; ++k) fc[k] = stg[k * kStage + c0];
             } else {
                 const float zero[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 #pragma unroll 4
-                for (int j = 0; j < kK1 / 8; ++j) store_chunk(a_op + kmaj(t, 8 * j, kK1), zero);
+                for (int j = 16 * h; j < 16 * h + 16; ++j) store_chunk(a_op + kmaj(t, 8 * j, kK1), zero);
             }
         }
 
         // ---- layer 1: D1 = A (128 x 256) W1^T ----
         fence_async_smem();
         tc_before();
-        wg_sync(wg);
-        if (t == 0) {
+        wg_sync(g);
+        if (u == 0) {
             tc_after();
-            mma_chain(tmem_base + wg * 128, a_s, w1_s, kK1, kH);
+            mma_chain(tmem_g, a_s, w1_s, kK1, kH);
             mma_commit(mybar);
         }
         bool ok = mbar_wait_bounded(mybar, parity);
         parity ^= 1u;
-        if (wg_sync_or(wg, !ok)) { failed = true; break; }
+        if (wg_sync_or(g, !ok)) { failed = true; break; }
         tc_after();
-        hidden_layer(tmem, b1, a_op, t);
+        hidden_half(tmem, b1, a_op, t, 32 * h);
 
         // ---- layer 2: D2 = H1 (128 x 64) W2^T ----
         fence_async_smem();
         tc_before();
-        wg_sync(wg);
-        if (t == 0) {
+        wg_sync(g);
+        if (u == 0) {
             tc_after();
-            mma_chain(tmem_base + wg * 128 + 64, a_s, w2_s, kH, kH);
+            mma_chain(tmem_g + 64, a_s, w2_s, kH, kH);
             mma_commit(mybar);
         }
         ok = mbar_wait_bounded(mybar, parity);
         parity ^= 1u;
-        if (wg_sync_or(wg, !ok)) { failed = true; break; }
+        if (wg_sync_or(g, !ok)) { failed = true; break; }
         tc_after();
-        hidden_layer(tmem + 64, b2, a_op, t);
+        hidden_half(tmem + 64, b2, a_op, t, 32 * h);
 
         // ---- layer 3: D3 = H2 (128 x 64) W3^T, N = 16 ----
         fence_async_smem();
         tc_before();
-        wg_sync(wg);
-        if (t == 0) {
+        wg_sync(g);
+        if (u == 0) {
             tc_after();
-            mma_chain(tmem_base + wg * 128, a_s, w3_s, kH, kN3);
+            mma_chain(tmem_g, a_s, w3_s, kH, kN3);
             mma_commit(mybar);
         }
         ok = mbar_wait_bounded(mybar, parity);
         parity ^= 1u;
-        if (wg_sync_or(wg, !ok)) { failed = true; break; }
+        if (wg_sync_or(g, !ok)) { failed = true; break; }
         tc_after();
-        float o16[16];
-        tmem_ld16(tmem, o16);
 
-        // ---- epilogue ----
-        if (t < count) {
-            if (ROWS) {
-                const int64_t row = (int64_t)tile * kRows + t;
+        // ---- epilogue (half 0) ----
+        if (h == 0) {
+            float o16[16];
+            tmem_ld16(tmem, o16);
+            if (t < count) {
+                if (ROWS) {
+                    const int64_t row = (int64_t)tile * kRows + t;
 #pragma unroll
-                for (int k = 0; k < kOut; ++k) out[row * kOut + k] = o16[k] + b3[k];
-            } else {
-                // Energy limit: the correction d may not raise the cell's energy
-                // E(f) = rho/2 |v|^2 + (s:s - c tr(s)^2) / (4 mu), c = lambda / (3 lambda + 2 mu)
-                // (the energy audit's density).  E(f + a d) = E(f) + 2 a B + a^2 Q, so the
-                // largest admissible a in [0, 1] is -2B/Q when B < 0, else 0.  A network
-                // trained on one-step targets is otherwise free to feed energy back into
-                // the strip and grow over long runs.
-                float d[kOut];
+                    for (int k = 0; k < kOut; ++k) out[row * kOut + k] = o16[k] + b3[k];
+                } else {
+                    // Energy limit: the correction d may not raise the cell's energy
+                    // E(f) = rho/2 |v|^2 + (s:s - c tr(s)^2) / (4 mu), c = lambda / (3 lambda + 2 mu)
+                    // (the energy audit's density).  E(f + a d) = E(f) + 2 a B + a^2 Q, so the
+                    // largest admissible a in [0, 1] is -2B/Q when B < 0, else 0.  A network
+                    // trained on one-step targets is otherwise free to feed energy back into
+                    // the strip and grow over long runs.
+                    float d[kOut];
 #pragma unroll
-                for (int k = 0; k < kOut; ++k) d[k] = (o16[k] + b3[k]) * s / (k < 3 ? zimp : 1.0f);
-                const float rho = 1.0f / m.b[gc], lam = m.lam[gc], mu = m.mu[gc];
-                const float cc = lam / (3.0f * lam + 2.0f * mu), i4m = 0.25f / mu;
-                const float trf = fc[3] + fc[4] + fc[5], trd = d[3] + d[4] + d[5];
-                const float B = 0.5f * rho * (fc[0] * d[0] + fc[1] * d[1] + fc[2] * d[2]) +
-                                i4m * (fc[3] * d[3] + fc[4] * d[4] + fc[5] * d[5] +
-                                       2.0f * (fc[6] * d[6] + fc[7] * d[7] + fc[8] * d[8]) - cc * trf * trd);
-                const float Q = 0.5f * rho * (d[0] * d[0] + d[1] * d[1] + d[2] * d[2]) +
-                                i4m * (d[3] * d[3] + d[4] * d[4] + d[5] * d[5] +
-                                       2.0f * (d[6] * d[6] + d[7] * d[7] + d[8] * d[8]) - cc * trd * trd);
-                const float a = (Q > 0.0f && B < 0.0f) ? fminf(1.0f, -2.0f * B / Q) : 0.0f;
-                float *dt = delta + (int64_t)tile * (kRows * kOut);
+                    for (int k = 0; k < kOut; ++k) d[k] = (o16[k] + b3[k]) * s / (k < 3 ? zimp : 1.0f);
+                    const float rho = 1.0f / m.b[gc], lam = m.lam[gc], mu = m.mu[gc];
+                    const float cc = lam / (3.0f * lam + 2.0f * mu), i4m = 0.25f / mu;
+                    const float trf = fc[3] + fc[4] + fc[5], trd = d[3] + d[4] + d[5];
+                    const float B = 0.5f * rho * (fc[0] * d[0] + fc[1] * d[1] + fc[2] * d[2]) +
+                                    i4m * (fc[3] * d[3] + fc[4] * d[4] + fc[5] * d[5] +
+                                           2.0f * (fc[6] * d[6] + fc[7] * d[7] + fc[8] * d[8]) - cc * trf * trd);
+                    const float Q = 0.5f * rho * (d[0] * d[0] + d[1] * d[1] + d[2] * d[2]) +
+                                    i4m * (d[3] * d[3] + d[4] * d[4] + d[5] * d[5] +
+                                           2.0f * (d[6] * d[6] + d[7] * d[7] + d[8] * d[8]) - cc * trd * trd);
+                    const float a = (Q > 0.0f && B < 0.0f) ? fminf(1.0f, -2.0f * B / Q) : 0.0f;
+                    float *dt = delta + (int64_t)tile * (kRows * kOut);
 #pragma unroll
-                for (int k = 0; k < kOut; ++k) dt[k * kRows + t] = a * d[k];
+                    for (int k = 0; k < kOut; ++k) dt[k * kRows + t] = a * d[k];
+                }
             }
         }
     }
     if (failed) {
-        if (t == 0) atomicOr(err, 4);
+        if (u == 0) atomicOr(err, 4);
         mbar_wait_bounded(mybar, parity ^ 1u);   // the commit the failed wait was for
     }
     tc_before();
@@ -660,7 +730,7 @@ int sgfd_mlp_infer(int32_t device, const float *params, const float *X, int64_t 
     if (e == cudaSuccess) {
         err = reinterpret_cast<int *>(img + kImgPad);
         k_weight_image<<<64, 256>>>(dp, img);
-        k_strip_tc<true><<<tc_grid(nt), 256, kTcSmem>>>(Model{}, 0, nullptr, 0, img, nullptr, dX, n, dout, err);
+        k_strip_tc<true><<<tc_grid(nt), kTcThreads, kTcSmem>>>(Model{}, 0, nullptr, 0, img, nullptr, dX, n, dout, err);
         e = cudaGetLastError();
     }
     int flag = 0;
@@ -865,7 +935,7 @@ cudaError_t strip_prepare() {
 cudaError_t launch_strip(const Model &m, int w, const int4 *tiles, int ntiles, float *buf, cudaStream_t s) {
     const unsigned char *img = reinterpret_cast<const unsigned char *>(buf);
     float *delta = reinterpret_cast<float *>(reinterpret_cast<unsigned char *>(buf) + kImgPad);
-    k_strip_tc<false><<<tc_grid(ntiles), 256, kTcSmem, s>>>(m, w, tiles, ntiles, img, delta, nullptr, 0, nullptr,
+    k_strip_tc<false><<<tc_grid(ntiles), kTcThreads, kTcSmem, s>>>(m, w, tiles, ntiles, img, delta, nullptr, 0, nullptr,
                                                             strip_error_flag(buf, ntiles));
     k_strip_apply<<<ntiles, kRows, 0, s>>>(m, tiles, delta);
     return cudaGetLastError();

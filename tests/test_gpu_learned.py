@@ -76,6 +76,28 @@ def test_tensor_core_inference(n):
         assert np.abs(got - exact).max() <= 3e-3 * scale
 
 
+def test_tensor_core_gelu():
+    """The hidden layers' GELU (an erfc approximation on the special-function
+    unit) against exact erf.  With identity weights the network passes inputs
+    0..8 straight through both hidden layers, so out_k = f16(GELU(f16(GELU(
+    f16(x_k))))): every output within two binary16 ulps (plus 1e-6) of the
+    exact-erf oracle, nearly all identical, for x in [-9, 9]."""
+    p = np.zeros(mo.N_PARAMS, np.float32)
+    o_w1, o_w2, o_w3 = 0, 252 * 64 + 64, 252 * 64 + 64 + 64 * 64 + 64
+    idx = np.arange(64)
+    p[o_w1 + idx * 64 + idx] = 1.0                           # W1[k][k] = 1, k < 64
+    p[o_w2 + idx * 64 + idx] = 1.0                           # W2 = I
+    p[o_w3 + np.arange(9) * 9 + np.arange(9)] = 1.0          # W3[k][k] = 1, k < 9
+    x = np.linspace(-9.0, 9.0, 9 * 4096).astype(np.float32).reshape(4096, 9)
+    X = np.zeros((4096, mo.N_IN), np.float32)
+    X[:, :9] = x
+    got = sgfd.mlp_infer(p, X).astype(np.float64)
+    ref = mo.forward_f16(p, X)
+    assert np.all(np.abs(got - ref) <= 2.0 ** -9 * np.abs(ref) + 1e-6)
+    assert (got == ref).mean() > 0.99
+    assert np.abs(ref).max() > 8.0                           # the positive side was reached
+
+
 def test_training_fits_a_smooth_target():
     rng = np.random.default_rng(4)
     X = rng.standard_normal((16384, mo.N_IN)).astype(np.float32)
