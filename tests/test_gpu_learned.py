@@ -77,8 +77,9 @@ def test_tensor_core_inference(n):
 
 
 def test_tensor_core_gelu():
-    """The hidden layers' GELU (an erfc approximation on the special-function
-    unit) against exact erf.  With identity weights the network passes inputs
+    """The hidden layers' GELU (a Chebyshev fit of erfc with fractional error
+    below 1.2e-7, the exponential on the special-function unit) against exact
+    erf.  With identity weights the network passes inputs
     0..8 straight through both hidden layers, so out_k = f16(GELU(f16(GELU(
     f16(x_k))))): every output within two binary16 ulps (plus 1e-6) of the
     exact-erf oracle, nearly all identical, for x in [-9, 9]."""
@@ -94,7 +95,7 @@ def test_tensor_core_gelu():
     got = sgfd.mlp_infer(p, X).astype(np.float64)
     ref = mo.forward_f16(p, X)
     assert np.all(np.abs(got - ref) <= 2.0 ** -9 * np.abs(ref) + 1e-6)
-    assert (got == ref).mean() > 0.99
+    assert (got == ref).mean() > 0.995                      # 1e-4 differ in an FP32 emulation
     assert np.abs(ref).max() > 8.0                           # the positive side was reached
 
 
