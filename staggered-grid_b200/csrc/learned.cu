@@ -22,10 +22,11 @@
 // Inference (k_strip_tc) runs the three layers on the tensor cores
 // (tcgen05.mma kind::f16: FP16 operands in shared memory, FP32 accumulators
 // in tensor memory), 128 strip cells per tile.  The strip is cut into boxes
-// of at most 128 cells (32 x 4 x 1 on the z faces, 32 x 2 x 2 on the y faces,
-// width x 4 x 5 on the x faces for width 6); a box's fields and their one-cell
-// halo are staged in shared memory with coalesced loads, and each thread
-// builds its cell's 252 inputs from there into row t of the A operand.
+// of at most 128 cells (32 x 2 x 2 on the z and y faces, width x 4 x 5 on the
+// x faces for width 6); a box's fields and their one-cell halo are staged in
+// shared memory with coalesced loads, with each staged cell's sums of squares,
+// and two threads build a cell's 252 inputs from there into row t of the A
+// operand.
 // Each CTA (one per SM) holds the weights once and runs two groups of 256
 // threads that work on alternate tiles, so one group's loads overlap the
 // other's tensor-core and epilogue work; two threads share each row.  The
@@ -67,6 +68,22 @@ __device__ __forceinline__ void band_of(int c, int nc, int w, float &depth, floa
     else { depth = 0.0f; side = 0.0f; }
 }
 
+// Per-cell sums of squares of the velocities and of the stresses, and the
+// RMS scale s of a neighbourhood from their sums over its 27 cells (two
+// partial sums each, neighbours 0..13 and 14..26, added at the end): the
+// velocities enter times rho*vp, s = sqrt((zimp^2 SV + SS) / 243).  The same
+// operations, in the same order, in the training inputs and the inference
+// kernel, so both see the same s.
+__device__ __forceinline__ float sq_velocity(const float (&f)[9]) {
+    return fmaf(f[2], f[2], fmaf(f[1], f[1], f[0] * f[0]));
+}
+__device__ __forceinline__ float sq_stress(const float (&f)[9]) {
+    return fmaf(f[8], f[8], fmaf(f[7], f[7], fmaf(f[6], f[6], fmaf(f[5], f[5], fmaf(f[4], f[4], f[3] * f[3])))));
+}
+__device__ __forceinline__ float rms_scale(float sv, float ss, float zimp) {
+    return sqrtf(fmaf(zimp * zimp, sv, ss) * (1.0f / 243.0f));
+}
+
 // The 252 inputs of computed cell (cx, cy, cz), passed one by one to emit(i,
 // value); returns the RMS scale s and sets zimp = rho * vp.
 template <class F>
@@ -75,23 +92,21 @@ __device__ __forceinline__ float strip_inputs(const Model &m, int w, int cx, int
     const float b = m.b[c], lam = m.lam[c], mu = m.mu[c];
     const float rho = 1.0f / b, vp = sqrtf((lam + 2.0f * mu) * b), vs = sqrtf(mu * b);
     zimp = rho * vp;
-    // sum of squares in two parts (neighbours 0..13 and 14..26), added at the
-    // end: the order in which the inference kernel's two threads of a row sum
-    float ss[2] = {0.0f, 0.0f};
+    float sv[2] = {0.0f, 0.0f}, ss[2] = {0.0f, 0.0f};
     for (int n = 0; n < 27; ++n) {
         const int64_t o = c + (n % 3 - 1) + (int64_t)((n / 3) % 3 - 1) * m.px + (int64_t)(n / 9 - 1) * m.plane;
+        float f[9];
 #pragma unroll
-        for (int k = 0; k < 9; ++k) {
-            const float u = m.f[k][o] * (k < 3 ? zimp : 1.0f);
-            ss[n >= 14] = fmaf(u, u, ss[n >= 14]);
-        }
+        for (int k = 0; k < 9; ++k) f[k] = m.f[k][o];
+        sv[n >= 14] += sq_velocity(f);
+        ss[n >= 14] += sq_stress(f);
     }
-    const float s = sqrtf((ss[0] + ss[1]) * (1.0f / 243.0f));
-    const float inv = s > 0.0f ? 1.0f / s : 0.0f;
+    const float s = rms_scale(sv[0] + sv[1], ss[0] + ss[1], zimp);
+    const float inv = s > 0.0f ? 1.0f / s : 0.0f, zinv = zimp * inv;
     for (int n = 0; n < 27; ++n) {
         const int64_t o = c + (n % 3 - 1) + (int64_t)((n / 3) % 3 - 1) * m.px + (int64_t)(n / 9 - 1) * m.plane;
 #pragma unroll
-        for (int k = 0; k < 9; ++k) emit(n * 9 + k, m.f[k][o] * (k < 3 ? zimp : 1.0f) * inv);
+        for (int k = 0; k < 9; ++k) emit(n * 9 + k, m.f[k][o] * (k < 3 ? zinv : inv));
     }
     emit(243, vp * (1.0f / 3000.0f));
     emit(244, vs * (1.0f / 1732.0f));
@@ -119,15 +134,15 @@ __global__ void k_strip_features(Model m, int w, const int4 *cells, int n, float
 constexpr int kRows = 128;                 // cells per tile = MMA M
 constexpr int kK1 = 256;                   // layer-1 K: the 252 inputs and 4 zeros
 constexpr int kN3 = 16;                    // layer-3 N: the 9 outputs and 7 zeros
-constexpr int kStage = 612;                // staged cells per box, (32+2)(4+2)(1+2) at most
+constexpr int kStage = 544;                // staged cells per box, (32+2)(2+2)(2+2) at most
 // Weight image (bytes): W1, W2, W3 transposed to N x K, FP16, in the K-major
 // core-matrix order of kmaj, then the biases b1, b2, b3 (b3 padded to 16) in FP32.
 constexpr int kImgW1 = 0, kImgW2 = kImgW1 + kH * kK1 * 2, kImgW3 = kImgW2 + kH * kH * 2,
               kImgB = kImgW3 + kN3 * kH * 2, kImg = kImgB + (2 * kH + kN3) * 4;
 constexpr int kImgPad = (kImg + 1023) / 1024 * 1024;
 constexpr int kAOp = kRows * kK1 * 2;                        // A operand of one warpgroup
-constexpr int kStg = 9 * kStage * 4;                         // staged fields of one warpgroup
-constexpr int kRed = 2 * kRows * 4;                          // partial sums of squares of one warpgroup
+constexpr int kStg = 11 * kStage * 4;                        // staged fields and sums of squares of one warpgroup
+constexpr int kRed = 4 * kRows * 4;                          // partial sums of squares of one warpgroup
 constexpr int kWgBytes = kAOp + (kStg + 1023) / 1024 * 1024 + kRed;
 constexpr int kTcSmem = 1024 + kImgPad + 2 * kWgBytes + 64;  // + alignment, barriers, TMEM address
 constexpr int kTcThreads = 512;                              // two warpgroups of 256: two threads per row
@@ -239,20 +254,25 @@ __device__ __forceinline__ float ex2_approx(float x) {
 // degree 9, fractional error below 1.2e-7 for every z, the small negative
 // tail included -- far below the half ulp of the binary16 the activation is
 // stored in (2.4e-4 relative).  The exponential is 2^((P - z^2) log2 e).
-__device__ __forceinline__ float gelu_fast(float x) {
-    const float z = fabsf(x) * 0.70710678f;
-    const float t = rcp_approx(fmaf(0.5f, z, 1.0f));
-    float p = fmaf(t, 0.17087277f, -0.82215223f);
-    p = fmaf(t, p, 1.48851587f);
-    p = fmaf(t, p, -1.13520398f);
-    p = fmaf(t, p, 0.27886807f);
-    p = fmaf(t, p, -0.18628806f);
-    p = fmaf(t, p, 0.09678418f);
-    p = fmaf(t, p, 0.37409196f);
-    p = fmaf(t, p, 1.00002368f);
-    p = fmaf(t, p, -1.26551223f);
-    const float half_erfc = 0.5f * t * ex2_approx((p - z * z) * 1.44269504f);
-    return x * (x >= 0.0f ? 1.0f - half_erfc : half_erfc);
+// Two values at a time with packed FP32x2 arithmetic.
+__device__ __forceinline__ float2 f2(float v) { return make_float2(v, v); }
+__device__ __forceinline__ float2 gelu_fast2(float2 x) {
+    const float2 z = __fmul2_rn(make_float2(fabsf(x.x), fabsf(x.y)), f2(0.70710678f));
+    const float2 d = __ffma2_rn(f2(0.5f), z, f2(1.0f));
+    const float2 t = make_float2(rcp_approx(d.x), rcp_approx(d.y));
+    float2 p = __ffma2_rn(t, f2(0.17087277f), f2(-0.82215223f));
+    p = __ffma2_rn(t, p, f2(1.48851587f));
+    p = __ffma2_rn(t, p, f2(-1.13520398f));
+    p = __ffma2_rn(t, p, f2(0.27886807f));
+    p = __ffma2_rn(t, p, f2(-0.18628806f));
+    p = __ffma2_rn(t, p, f2(0.09678418f));
+    p = __ffma2_rn(t, p, f2(0.37409196f));
+    p = __ffma2_rn(t, p, f2(1.00002368f));
+    p = __ffma2_rn(t, p, f2(-1.26551223f));
+    const float2 q = __fmul2_rn(__ffma2_rn(make_float2(-z.x, -z.y), z, p), f2(1.44269504f));
+    const float2 he = __fmul2_rn(__fmul2_rn(f2(0.5f), t), make_float2(ex2_approx(q.x), ex2_approx(q.y)));
+    const float2 phi = make_float2(x.x >= 0.0f ? 1.0f - he.x : he.x, x.y >= 0.0f ? 1.0f - he.y : he.y);
+    return __fmul2_rn(x, phi);
 }
 
 // Hidden layer, columns c0 .. c0+31 of this thread's row: accumulators + bias,
@@ -266,7 +286,13 @@ __device__ __forceinline__ void hidden_half(uint32_t taddr, const float *bias, u
         for (int h = 0; h < 2; ++h) {
             float g[8];
 #pragma unroll
-            for (int q = 0; q < 8; ++q) g[q] = gelu_fast(v[8 * h + q] + bias[c0 + 16 * c + 8 * h + q]);
+            for (int q = 0; q < 8; q += 2) {
+                const float2 r = gelu_fast2(__fadd2_rn(make_float2(v[8 * h + q], v[8 * h + q + 1]),
+                                                       make_float2(bias[c0 + 16 * c + 8 * h + q],
+                                                                   bias[c0 + 16 * c + 8 * h + q + 1])));
+                g[q] = r.x;
+                g[q + 1] = r.y;
+            }
             store_chunk(a_op + kmaj(t, c0 + 16 * c + 8 * h, kH), g);
         }
     }
@@ -299,26 +325,23 @@ struct Box {
 };
 __device__ __forceinline__ Box box_of(int4 td) { return {td.x, td.y, td.z, td.w & 255, (td.w >> 8) & 255, (td.w >> 16) & 255}; }
 
-// Sum of squares of the 9 staged fields (velocities times zimp) over the
-// neighbours n0 .. n1-1 of the staged cell c0.
+// Sums over the neighbours N0 .. N1-1 of staged cell c0 of the staged
+// per-cell sums of squares: velocities (sv) and stresses (ss).
 template <int N0, int N1>
-__device__ __forceinline__ float staged_squares(const float *stg, int c0, int sx, int sxy, float zimp) {
-    float ss = 0.0f;
+__device__ __forceinline__ void staged_sums(const float *stg, int c0, int sx, int sxy, float &sv, float &ss) {
+    sv = 0.0f;
+    ss = 0.0f;
 #pragma unroll
     for (int n = N0; n < N1; ++n) {
         const int o = c0 + (n % 3 - 1) + ((n / 3) % 3 - 1) * sx + (n / 9 - 1) * sxy;
-#pragma unroll
-        for (int k = 0; k < 9; ++k) {
-            const float u = stg[k * kStage + o] * (k < 3 ? zimp : 1.0f);
-            ss = fmaf(u, u, ss);
-        }
+        sv += stg[9 * kStage + o];
+        ss += stg[10 * kStage + o];
     }
-    return ss;
 }
 
 // Inputs J0*8 .. J0*8+127 of row t (16 chunks of 8) from the staged fields.
 template <int J0>
-__device__ __forceinline__ void staged_inputs(const float *stg, int c0, int sx, int sxy, float zimp, float inv,
+__device__ __forceinline__ void staged_inputs(const float *stg, int c0, int sx, int sxy, float zinv, float inv,
                                               const float (&ext)[9], unsigned char *a_op, int t) {
 #pragma unroll
     for (int j = J0; j < J0 + 16; ++j) {
@@ -329,7 +352,7 @@ __device__ __forceinline__ void staged_inputs(const float *stg, int c0, int sx, 
             if (f < 243) {
                 const int n = f / 9, k = f % 9;
                 const int o = c0 + (n % 3 - 1) + ((n / 3) % 3 - 1) * sx + (n / 9 - 1) * sxy;
-                v[q] = stg[k * kStage + o] * (k < 3 ? zimp : 1.0f) * inv;
+                v[q] = stg[k * kStage + o] * (k < 3 ? zinv : inv);
             } else {
                 v[q] = f < kIn ? ext[f - 243] : 0.0f;
             }
@@ -402,11 +425,21 @@ k_strip_tc(Model m, int w, const int4 *tiles, int ntiles, const unsigned char *w
         } else {
             const Box bx = box_of(tiles[tile]);
             const int sx = bx.ex + 2, sxy = sx * (bx.ey + 2), ns = sxy * (bx.ez + 2);
+            // staged cell r = lx + ly sx + lz sxy; the quotients through a float
+            // reciprocal, exact here: (r + 1/2) / d stays 1/(2d) > 9e-4 away from
+            // an integer and the product errs by < 2e-4 for r < 544
+            const float inv_sx = 1.0f / (float)sx, inv_sxy = 1.0f / (float)sxy;
             for (int r = u; r < ns; r += 2 * kRows) {
-                const int lx = r % sx, ly = (r / sx) % (bx.ey + 2), lz = r / sxy;
+                const int lz = __float2int_rz(((float)r + 0.5f) * inv_sxy), rr = r - lz * sxy;
+                const int ly = __float2int_rz(((float)rr + 0.5f) * inv_sx), lx = rr - ly * sx;
                 const int64_t gi = pidx(m, bx.x - 1 + lx + kHalo, bx.y - 1 + ly + kHalo, bx.z - 1 + lz + kHalo);
+                float f[9];
 #pragma unroll
-                for (int k = 0; k < 9; ++k) stg[k * kStage + r] = m.f[k][gi];
+                for (int k = 0; k < 9; ++k) f[k] = m.f[k][gi];
+#pragma unroll
+                for (int k = 0; k < 9; ++k) stg[k * kStage + r] = f[k];
+                stg[9 * kStage + r] = sq_velocity(f);
+                stg[10 * kStage + r] = sq_stress(f);
             }
             wg_sync(g);
             count = bx.ex * bx.ey * bx.ez;
@@ -424,13 +457,16 @@ k_strip_tc(Model m, int w, const int4 *tiles, int ntiles, const unsigned char *w
                 vp = sqrtf((lam + 2.0f * mu) * b);
                 vs = sqrtf(mu * b);
                 zimp = rho * vp;
-                red[h * kRows + t] = h == 0 ? staged_squares<0, 14>(stg, c0, sx, sxy, zimp)
-                                            : staged_squares<14, 27>(stg, c0, sx, sxy, zimp);
+                float sv, ss;
+                if (h == 0) staged_sums<0, 14>(stg, c0, sx, sxy, sv, ss);
+                else staged_sums<14, 27>(stg, c0, sx, sxy, sv, ss);
+                red[(2 * h) * kRows + t] = sv;
+                red[(2 * h + 1) * kRows + t] = ss;
             }
             wg_sync(g);
             if (t < count) {
-                s = sqrtf((red[t] + red[kRows + t]) * (1.0f / 243.0f));
-                const float inv = s > 0.0f ? 1.0f / s : 0.0f;
+                s = rms_scale(red[t] + red[2 * kRows + t], red[kRows + t] + red[3 * kRows + t], zimp);
+                const float inv = s > 0.0f ? 1.0f / s : 0.0f, zinv = zimp * inv;
                 float ext[9];
                 ext[0] = vp * (1.0f / 3000.0f);
                 ext[1] = vs * (1.0f / 1732.0f);
@@ -439,11 +475,11 @@ k_strip_tc(Model m, int w, const int4 *tiles, int ntiles, const unsigned char *w
                 band_of(cy, m.nyc, w, ext[4], ext[7]);
                 band_of(cz, m.nzc, w, ext[5], ext[8]);
                 if (h == 0) {
-                    staged_inputs<0>(stg, c0, sx, sxy, zimp, inv, ext, a_op, t);
+                    staged_inputs<0>(stg, c0, sx, sxy, zinv, inv, ext, a_op, t);
 #pragma unroll
                     for (int k = 0; k < kOut; ++k) fc[k] = stg[k * kStage + c0];
                 } else {
-                    staged_inputs<16>(stg, c0, sx, sxy, zimp, inv, ext, a_op, t);
+                    staged_inputs<16>(stg, c0, sx, sxy, zinv, inv, ext, a_op, t);
                 }
             } else {
                 const float zero[8] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -900,8 +936,8 @@ int sgfd_strip_features(sgfd_solver *h, int32_t width, int32_t n, const int32_t 
 namespace sgfd {
 
 // Boxes of at most 128 strip cells covering the strip once: the two z faces
-// in 32 x 4 x 1 boxes, the two y faces (between the z faces) in 32 x 2 x 2,
-// the two x faces (between the others) in min(w, 32) x 4 x rest.  Each tile is
+// and the two y faces (between the z faces) in 32 x 2 x 2 boxes, the two x
+// faces (between the others) in min(w, 32) x ey x ez (6 x 4 x 5 for w = 6).  Each tile is
 // (x, y, z, ex | ey << 8 | ez << 16) in computed coordinates; -1 if a box
 // would not fit the staging area.
 int strip_tile_list(const Model &m, int w, std::vector<int4> &tiles) {
@@ -916,11 +952,14 @@ int strip_tile_list(const Model &m, int w, std::vector<int4> &tiles) {
                                                            std::min(ez, z1 - z) << 16));
     };
     const int X = m.nxc, Y = m.nyc, Z = m.nzc;
-    boxes(0, X, 0, Y, 0, w, 32, 4, 1);
-    boxes(0, X, 0, Y, Z - w, Z, 32, 4, 1);
+    boxes(0, X, 0, Y, 0, w, 32, 2, 2);
+    boxes(0, X, 0, Y, Z - w, Z, 32, 2, 2);
     boxes(0, X, 0, w, w, Z - w, 32, 2, 2);
     boxes(0, X, Y - w, Y, w, Z - w, 32, 2, 2);
-    const int ex = std::min(w, 32), ey = std::min(4, kRows / ex), ez = kRows / ex / ey;
+    const int ex = std::min(w, 32), rest = kRows / ex;
+    int ey = 1;
+    while (4 * ey * ey <= rest) ey *= 2;        // largest power of two with ey^2 <= rest
+    const int ez = rest / ey;
     boxes(0, w, w, Y - w, w, Z - w, ex, ey, ez);
     boxes(X - w, X, w, Y - w, w, Z - w, ex, ey, ez);
     return fits ? (int)tiles.size() : -1;
