@@ -143,8 +143,9 @@ constexpr int kImgPad = (kImg + 1023) / 1024 * 1024;
 constexpr int kAOp = kRows * kK1 * 2;                        // A operand of one warpgroup
 constexpr int kStg = 11 * kStage * 4;                        // staged fields and sums of squares of one warpgroup
 constexpr int kRed = 4 * kRows * 4;                          // partial sums of squares of one warpgroup
-constexpr int kWgBytes = kAOp + (kStg + 1023) / 1024 * 1024 + kRed;
-constexpr int kTcSmem = 1024 + kImgPad + 2 * kWgBytes + 64;  // + alignment, barriers, TMEM address
+constexpr int kMed = 3 * kRows * 4;                          // b, lambda, mu of the next tile's cells
+constexpr int kWgBytes = kAOp + (kStg + 1023) / 1024 * 1024 + kRed + kMed;
+constexpr int kTcSmem = 128 + kImgPad + 2 * kWgBytes + 64;   // + alignment, barriers, TMEM address
 constexpr int kTcThreads = 512;                              // two warpgroups of 256: two threads per row
 static_assert(kImg % 16 == 0, "weight image is copied in 16-byte pieces");
 static_assert(kTcSmem <= 232448, "shared memory of one CTA");
@@ -325,6 +326,38 @@ struct Box {
 };
 __device__ __forceinline__ Box box_of(int4 td) { return {td.x, td.y, td.z, td.w & 255, (td.w >> 8) & 255, (td.w >> 16) & 255}; }
 
+__device__ __forceinline__ void cp_async4(float *dst, const float *src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(saddr_of(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// Starts the asynchronous copies of tile td's box with its one-cell halo (the
+// 9 fields, all 256 threads of a group) and of the medium of its cells
+// (thread u for row u) into the group's staging area; cp_async_wait_all
+// completes them.  Staged cell r = lx + ly sx + lz sxy; the quotients through
+// a float reciprocal, exact here: (r + 1/2) / d stays 1/(2d) > 9e-4 away from
+// an integer and the product errs by < 2e-4 for r < 544.
+__device__ __forceinline__ void stage_async(const Model &m, int4 td, float *stg, float *med, int u) {
+    const Box bx = box_of(td);
+    const int sx = bx.ex + 2, sxy = sx * (bx.ey + 2), ns = sxy * (bx.ez + 2);
+    const float inv_sx = 1.0f / (float)sx, inv_sxy = 1.0f / (float)sxy;
+    for (int r = u; r < ns; r += 2 * kRows) {
+        const int lz = __float2int_rz(((float)r + 0.5f) * inv_sxy), rr = r - lz * sxy;
+        const int ly = __float2int_rz(((float)rr + 0.5f) * inv_sx), lx = rr - ly * sx;
+        const int64_t gi = pidx(m, bx.x - 1 + lx + kHalo, bx.y - 1 + ly + kHalo, bx.z - 1 + lz + kHalo);
+#pragma unroll
+        for (int k = 0; k < 9; ++k) cp_async4(stg + k * kStage + r, m.f[k] + gi);
+    }
+    if (u < bx.ex * bx.ey * bx.ez) {
+        const int lx = u % bx.ex, ly = (u / bx.ex) % bx.ey, lz = u / (bx.ex * bx.ey);
+        const int64_t gc = pidx(m, bx.x + lx + kHalo, bx.y + ly + kHalo, bx.z + lz + kHalo);
+        cp_async4(med + u, m.b + gc);
+        cp_async4(med + kRows + u, m.lam + gc);
+        cp_async4(med + 2 * kRows + u, m.mu + gc);
+    }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+
 // Sums over the neighbours N0 .. N1-1 of staged cell c0 of the staged
 // per-cell sums of squares: velocities (sv) and stresses (ss).
 template <int N0, int N1>
@@ -375,11 +408,12 @@ __global__ void __launch_bounds__(kTcThreads, 1)
 k_strip_tc(Model m, int w, const int4 *tiles, int ntiles, const unsigned char *wimg, float *delta, const float *X,
            int64_t nrows, float *out, int *err) {
     extern __shared__ unsigned char smem_raw[];
-    unsigned char *sm = smem_raw + ((1024 - (saddr_of(smem_raw) & 1023)) & 1023);
+    unsigned char *sm = smem_raw + ((128 - (saddr_of(smem_raw) & 127)) & 127);
     const int tid = threadIdx.x, g = tid >> 8, u = tid & 255, h = u >> 7, t = u & 127, warp = tid >> 5;
     unsigned char *a_op = sm + kImgPad + g * kWgBytes;
     float *stg = reinterpret_cast<float *>(a_op + kAOp);
-    float *red = reinterpret_cast<float *>(a_op + kWgBytes - kRed);
+    float *red = reinterpret_cast<float *>(a_op + kWgBytes - kRed - kMed);
+    float *med = reinterpret_cast<float *>(a_op + kWgBytes - kMed);
     uint64_t *bar = reinterpret_cast<uint64_t *>(sm + kImgPad + 2 * kWgBytes);
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bar + 2);
 
@@ -406,11 +440,11 @@ k_strip_tc(Model m, int w, const int4 *tiles, int ntiles, const unsigned char *w
     bool failed = false;
 
     const int nt = ROWS ? (int)((nrows + kRows - 1) / kRows) : ntiles;
+    if (!ROWS && 2 * (int)blockIdx.x + g < nt) stage_async(m, tiles[2 * blockIdx.x + g], stg, med, u);
     for (int tile = 2 * blockIdx.x + g; tile < nt; tile += 2 * gridDim.x) {
         // ---- inputs: row t of the A operand, half h ----
-        float s = 0.0f, zimp = 1.0f, fc[kOut];
+        float s = 0.0f, zimp = 1.0f, fc[kOut], c_b = 1.0f, c_lam = 0.0f, c_mu = 1.0f;
         int count;
-        int64_t gc = 0;
         if (ROWS) {
             const int64_t first = (int64_t)tile * kRows, row = first + t;
             count = (int)(nrows - first < kRows ? nrows - first : kRows);
@@ -425,19 +459,11 @@ k_strip_tc(Model m, int w, const int4 *tiles, int ntiles, const unsigned char *w
         } else {
             const Box bx = box_of(tiles[tile]);
             const int sx = bx.ex + 2, sxy = sx * (bx.ey + 2), ns = sxy * (bx.ez + 2);
-            // staged cell r = lx + ly sx + lz sxy; the quotients through a float
-            // reciprocal, exact here: (r + 1/2) / d stays 1/(2d) > 9e-4 away from
-            // an integer and the product errs by < 2e-4 for r < 544
-            const float inv_sx = 1.0f / (float)sx, inv_sxy = 1.0f / (float)sxy;
+            cp_async_wait_all();   // this tile's copies, started during the previous tile
             for (int r = u; r < ns; r += 2 * kRows) {
-                const int lz = __float2int_rz(((float)r + 0.5f) * inv_sxy), rr = r - lz * sxy;
-                const int ly = __float2int_rz(((float)rr + 0.5f) * inv_sx), lx = rr - ly * sx;
-                const int64_t gi = pidx(m, bx.x - 1 + lx + kHalo, bx.y - 1 + ly + kHalo, bx.z - 1 + lz + kHalo);
                 float f[9];
 #pragma unroll
-                for (int k = 0; k < 9; ++k) f[k] = m.f[k][gi];
-#pragma unroll
-                for (int k = 0; k < 9; ++k) stg[k * kStage + r] = f[k];
+                for (int k = 0; k < 9; ++k) f[k] = stg[k * kStage + r];
                 stg[9 * kStage + r] = sq_velocity(f);
                 stg[10 * kStage + r] = sq_stress(f);
             }
@@ -451,8 +477,10 @@ k_strip_tc(Model m, int w, const int4 *tiles, int ntiles, const unsigned char *w
                 cy = bx.y + ly;
                 cz = bx.z + lz;
                 c0 = (lx + 1) + (ly + 1) * sx + (lz + 1) * sxy;
-                gc = pidx(m, cx + kHalo, cy + kHalo, cz + kHalo);
-                const float b = m.b[gc], lam = m.lam[gc], mu = m.mu[gc];
+                const float b = med[t], lam = med[kRows + t], mu = med[2 * kRows + t];
+                c_b = b;
+                c_lam = lam;
+                c_mu = mu;
                 rho = 1.0f / b;
                 vp = sqrtf((lam + 2.0f * mu) * b);
                 vs = sqrtf(mu * b);
@@ -497,6 +525,8 @@ k_strip_tc(Model m, int w, const int4 *tiles, int ntiles, const unsigned char *w
             mma_chain(tmem_g, a_s, w1_s, kK1, kH);
             mma_commit(mybar);
         }
+        // the staging area is free: the next tile's copies overlap this one's network
+        if (!ROWS && tile + 2 * (int)gridDim.x < nt) stage_async(m, tiles[tile + 2 * gridDim.x], stg, med, u);
         bool ok = mbar_wait_bounded(mybar, parity);
         parity ^= 1u;
         if (wg_sync_or(g, !ok)) { failed = true; break; }
@@ -551,7 +581,7 @@ k_strip_tc(Model m, int w, const int4 *tiles, int ntiles, const unsigned char *w
                     float d[kOut];
 #pragma unroll
                     for (int k = 0; k < kOut; ++k) d[k] = (o16[k] + b3[k]) * s / (k < 3 ? zimp : 1.0f);
-                    const float rho = 1.0f / m.b[gc], lam = m.lam[gc], mu = m.mu[gc];
+                    const float rho = 1.0f / c_b, lam = c_lam, mu = c_mu;
                     const float cc = lam / (3.0f * lam + 2.0f * mu), i4m = 0.25f / mu;
                     const float trf = fc[3] + fc[4] + fc[5], trd = d[3] + d[4] + d[5];
                     const float B = 0.5f * rho * (fc[0] * d[0] + fc[1] * d[1] + fc[2] * d[2]) +
@@ -568,6 +598,7 @@ k_strip_tc(Model m, int w, const int4 *tiles, int ntiles, const unsigned char *w
             }
         }
     }
+    cp_async_wait_all();
     if (failed) {
         if (u == 0) atomicOr(err, 4);
         mbar_wait_bounded(mybar, parity ^ 1u);   // the commit the failed wait was for
