@@ -27,10 +27,9 @@
 // shared memory with coalesced loads, with each staged cell's sums of squares,
 // and two threads build a cell's 252 inputs from there into row t of the A
 // operand.
-// Each CTA (one per SM) holds the weights once and runs two groups of 512
+// Each CTA (one per SM) holds the weights once and runs two groups of 256
 // threads that work on alternate tiles, so one group's loads overlap the
-// other's tensor-core and epilogue work; four threads share each row, and
-// the next tile's fields are copied in (cp.async) while a tile is computed.  The
+// other's tensor-core and epilogue work; two threads share each row.  The
 // hidden layers' GELU uses a Chebyshev fit of erfc (Numerical Recipes erfcc,
 // fractional error < 1.2e-7) with the exponential on the special-function unit.
 //
@@ -147,9 +146,7 @@ constexpr int kRed = 4 * kRows * 4;                          // partial sums of 
 constexpr int kMed = 3 * kRows * 4;                          // b, lambda, mu of the next tile's cells
 constexpr int kWgBytes = kAOp + (kStg + 1023) / 1024 * 1024 + kRed + kMed;
 constexpr int kTcSmem = 128 + kImgPad + 2 * kWgBytes + 64;   // + alignment, barriers, TMEM address
-constexpr int kSplit = 4;                                    // threads per row
-constexpr int kGroup = kRows * kSplit;                       // threads of one tile group
-constexpr int kTcThreads = 2 * kGroup;                       // two groups per CTA
+constexpr int kTcThreads = 512;                              // two warpgroups of 256: two threads per row
 static_assert(kImg % 16 == 0, "weight image is copied in 16-byte pieces");
 static_assert(kTcSmem <= 232448, "shared memory of one CTA");
 constexpr uint32_t kTmemCols = 256;                          // 128 per warpgroup: D1/D3 at +0, D2 at +64
@@ -194,16 +191,16 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity
 __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 __device__ __forceinline__ void tc_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-// Barrier of one tile group (named barrier 1 + g, kGroup threads) that also
+// Barrier of one 256-thread warpgroup pair (named barrier 1 + g) that also
 // ORs a flag over it.
 __device__ __forceinline__ bool wg_sync_or(int g, bool flag) {
     uint32_t r;
     asm volatile(
-        "{\n .reg .pred p, q;\n setp.ne.u32 p, %1, 0;\n bar.red.or.pred q, %2, %3, p;\n selp.u32 %0, 1, 0, q;\n}\n"
-        : "=r"(r) : "r"((uint32_t)flag), "r"(g + 1), "n"(kGroup) : "memory");
+        "{\n .reg .pred p, q;\n setp.ne.u32 p, %1, 0;\n bar.red.or.pred q, %2, 256, p;\n selp.u32 %0, 1, 0, q;\n}\n"
+        : "=r"(r) : "r"((uint32_t)flag), "r"(g + 1) : "memory");
     return r != 0;
 }
-__device__ __forceinline__ void wg_sync(int g) { asm volatile("bar.sync %0, %1;" ::"r"(g + 1), "n"(kGroup) : "memory"); }
+__device__ __forceinline__ void wg_sync(int g) { asm volatile("bar.sync %0, 256;" ::"r"(g + 1) : "memory"); }
 
 // D[tmem] (+)= A[a] * B[b]^T over KT columns, M = 128, N = n, K = 16 per instruction.
 __device__ __forceinline__ void mma_chain(uint32_t tmem_d, uint32_t a, uint32_t b, int KT, int n) {
@@ -279,22 +276,26 @@ __device__ __forceinline__ float2 gelu_fast2(float2 x) {
     return __fmul2_rn(x, phi);
 }
 
-// Hidden layer, columns c0 .. c0+15 of this thread's row: accumulators +
-// bias, GELU, FP16 into row t of the next A operand (K = 64).
-__device__ __forceinline__ void hidden_part(uint32_t taddr, const float *bias, unsigned char *a_op, int t, int c0) {
-    float v[16];
-    tmem_ld16(taddr + c0, v);
+// Hidden layer, columns c0 .. c0+31 of this thread's row: accumulators + bias,
+// GELU, FP16 into row t of the next A operand (K = 64).
+__device__ __forceinline__ void hidden_half(uint32_t taddr, const float *bias, unsigned char *a_op, int t, int c0) {
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
-        float g[8];
+    for (int c = 0; c < 2; ++c) {
+        float v[16];
+        tmem_ld16(taddr + c0 + c * 16, v);
 #pragma unroll
-        for (int q = 0; q < 8; q += 2) {
-            const float2 r = gelu_fast2(__fadd2_rn(make_float2(v[8 * h + q], v[8 * h + q + 1]),
-                                                   make_float2(bias[c0 + 8 * h + q], bias[c0 + 8 * h + q + 1])));
-            g[q] = r.x;
-            g[q + 1] = r.y;
+        for (int h = 0; h < 2; ++h) {
+            float g[8];
+#pragma unroll
+            for (int q = 0; q < 8; q += 2) {
+                const float2 r = gelu_fast2(__fadd2_rn(make_float2(v[8 * h + q], v[8 * h + q + 1]),
+                                                       make_float2(bias[c0 + 16 * c + 8 * h + q],
+                                                                   bias[c0 + 16 * c + 8 * h + q + 1])));
+                g[q] = r.x;
+                g[q + 1] = r.y;
+            }
+            store_chunk(a_op + kmaj(t, c0 + 16 * c + 8 * h, kH), g);
         }
-        store_chunk(a_op + kmaj(t, c0 + 8 * h, kH), g);
     }
 }
 
@@ -331,7 +332,7 @@ __device__ __forceinline__ void cp_async4(float *dst, const float *src) {
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 // Starts the asynchronous copies of tile td's box with its one-cell halo (the
-// 9 fields, all threads of a group) and of the medium of its cells
+// 9 fields, all 256 threads of a group) and of the medium of its cells
 // (thread u for row u) into the group's staging area; cp_async_wait_all
 // completes them.  Staged cell r = lx + ly sx + lz sxy; the quotients through
 // a float reciprocal, exact here: (r + 1/2) / d stays 1/(2d) > 9e-4 away from
@@ -340,7 +341,7 @@ __device__ __forceinline__ void stage_async(const Model &m, int4 td, float *stg,
     const Box bx = box_of(td);
     const int sx = bx.ex + 2, sxy = sx * (bx.ey + 2), ns = sxy * (bx.ez + 2);
     const float inv_sx = 1.0f / (float)sx, inv_sxy = 1.0f / (float)sxy;
-    for (int r = u; r < ns; r += kGroup) {
+    for (int r = u; r < ns; r += 2 * kRows) {
         const int lz = __float2int_rz(((float)r + 0.5f) * inv_sxy), rr = r - lz * sxy;
         const int ly = __float2int_rz(((float)rr + 0.5f) * inv_sx), lx = rr - ly * sx;
         const int64_t gi = pidx(m, bx.x - 1 + lx + kHalo, bx.y - 1 + ly + kHalo, bx.z - 1 + lz + kHalo);
@@ -371,12 +372,12 @@ __device__ __forceinline__ void staged_sums(const float *stg, int c0, int sx, in
     }
 }
 
-// Inputs J0*8 .. J0*8+63 of row t (8 chunks of 8) from the staged fields.
+// Inputs J0*8 .. J0*8+127 of row t (16 chunks of 8) from the staged fields.
 template <int J0>
 __device__ __forceinline__ void staged_inputs(const float *stg, int c0, int sx, int sxy, float zinv, float inv,
                                               const float (&ext)[9], unsigned char *a_op, int t) {
 #pragma unroll
-    for (int j = J0; j < J0 + 8; ++j) {
+    for (int j = J0; j < J0 + 16; ++j) {
         float v[8];
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
@@ -395,13 +396,12 @@ __device__ __forceinline__ void staged_inputs(const float *stg, int c0, int sx, 
 
 // Network of every strip cell (ROWS = false), or of n input rows X (ROWS =
 // true: the tensor-core path checked on given inputs, raw outputs to out).
-// One CTA per SM with 1024 threads in two groups of 512; group g takes tiles
-// 2*blockIdx.x + g, then every 2*gridDim.x-th.  In a group, threads t,
-// t + 128, t + 256 and t + 384 (warps w, w + 4, w + 8, w + 12, which reach the
-// same TMEM lanes) share row t of a tile: quarter q builds inputs 64q ..
-// 64q + 63 (quarter 3 with the 9 cell inputs) and hidden columns 16q ..
-// 16q + 15; quarters 0 and 1 sum the squares over neighbours 0..13 and
-// 14..26; quarter 0 runs the epilogue.
+// One CTA per SM with 512 threads in two groups of 256; group g takes tiles
+// 2*blockIdx.x + g, then every 2*gridDim.x-th.  In a group, threads t and
+// t + 128 (warps w and w + 4, which reach the same TMEM lanes) share row t of
+// a tile: half h = 0 takes neighbours 0..13, inputs 0..127 and hidden
+// columns 0..31, half h = 1 neighbours 14..26, inputs 128..255 (with the 9
+// cell inputs) and hidden columns 32..63; half 0 runs the epilogue.
 // delta[tile][k][128] receives the energy-limited corrections.
 template <bool ROWS>
 __global__ void __launch_bounds__(kTcThreads, 1)
@@ -409,7 +409,7 @@ k_strip_tc(Model m, int w, const int4 *tiles, int ntiles, const unsigned char *w
            int64_t nrows, float *out, int *err) {
     extern __shared__ unsigned char smem_raw[];
     unsigned char *sm = smem_raw + ((128 - (saddr_of(smem_raw) & 127)) & 127);
-    const int tid = threadIdx.x, g = tid / kGroup, u = tid % kGroup, h = u / kRows, t = u % kRows, warp = tid >> 5;
+    const int tid = threadIdx.x, g = tid >> 8, u = tid & 255, h = u >> 7, t = u & 127, warp = tid >> 5;
     unsigned char *a_op = sm + kImgPad + g * kWgBytes;
     float *stg = reinterpret_cast<float *>(a_op + kAOp);
     float *red = reinterpret_cast<float *>(a_op + kWgBytes - kRed - kMed);
@@ -450,7 +450,7 @@ k_strip_tc(Model m, int w, const int4 *tiles, int ntiles, const unsigned char *w
             count = (int)(nrows - first < kRows ? nrows - first : kRows);
             const float *x = X + row * kIn;
 #pragma unroll 4
-            for (int j = 8 * h; j < 8 * h + 8; ++j) {
+            for (int j = 16 * h; j < 16 * h + 16; ++j) {
                 float v[8];
 #pragma unroll
                 for (int q = 0; q < 8; ++q) v[q] = (t < count && 8 * j + q < kIn) ? x[8 * j + q] : 0.0f;
@@ -460,7 +460,7 @@ k_strip_tc(Model m, int w, const int4 *tiles, int ntiles, const unsigned char *w
             const Box bx = box_of(tiles[tile]);
             const int sx = bx.ex + 2, sxy = sx * (bx.ey + 2), ns = sxy * (bx.ez + 2);
             cp_async_wait_all();   // this tile's copies, started during the previous tile
-            for (int r = u; r < ns; r += kGroup) {
+            for (int r = u; r < ns; r += 2 * kRows) {
                 float f[9];
 #pragma unroll
                 for (int k = 0; k < 9; ++k) f[k] = stg[k * kStage + r];
@@ -470,7 +470,7 @@ k_strip_tc(Model m, int w, const int4 *tiles, int ntiles, const unsigned char *w
             wg_sync(g);
             count = bx.ex * bx.ey * bx.ez;
             int c0 = 0, cx = 0, cy = 0, cz = 0;
-            float rho = 0.0f, vp = 0.0f, vs = 0.0f;
+            float rho = 0.0f, vp = 0.0f;
             if (t < count) {
                 const int lx = t % bx.ex, ly = (t / bx.ex) % bx.ey, lz = t / (bx.ex * bx.ey);
                 cx = bx.x + lx;
@@ -483,42 +483,37 @@ k_strip_tc(Model m, int w, const int4 *tiles, int ntiles, const unsigned char *w
                 c_mu = mu;
                 rho = 1.0f / b;
                 vp = sqrtf((lam + 2.0f * mu) * b);
-                vs = sqrtf(mu * b);
                 zimp = rho * vp;
-                if (h < 2) {
-                    float sv, ss;
-                    if (h == 0) staged_sums<0, 14>(stg, c0, sx, sxy, sv, ss);
-                    else staged_sums<14, 27>(stg, c0, sx, sxy, sv, ss);
-                    red[(2 * h) * kRows + t] = sv;
-                    red[(2 * h + 1) * kRows + t] = ss;
-                }
+                float sv, ss;
+                if (h == 0) staged_sums<0, 14>(stg, c0, sx, sxy, sv, ss);
+                else staged_sums<14, 27>(stg, c0, sx, sxy, sv, ss);
+                red[(2 * h) * kRows + t] = sv;
+                red[(2 * h + 1) * kRows + t] = ss;
             }
             wg_sync(g);
             if (t < count) {
                 s = rms_scale(red[t] + red[2 * kRows + t], red[kRows + t] + red[3 * kRows + t], zimp);
                 const float inv = s > 0.0f ? 1.0f / s : 0.0f, zinv = zimp * inv;
-                float ext[9];
-                ext[0] = vp * (1.0f / 3000.0f);
-                ext[1] = vs * (1.0f / 1732.0f);
-                ext[2] = rho * (1.0f / 2000.0f);
-                band_of(cx, m.nxc, w, ext[3], ext[6]);
-                band_of(cy, m.nyc, w, ext[4], ext[7]);
-                band_of(cz, m.nzc, w, ext[5], ext[8]);
                 if (h == 0) {
-                    staged_inputs<0>(stg, c0, sx, sxy, zinv, inv, ext, a_op, t);
+                    const float none[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};   // inputs 0..127 hold no cell inputs
+                    staged_inputs<0>(stg, c0, sx, sxy, zinv, inv, none, a_op, t);
 #pragma unroll
                     for (int k = 0; k < kOut; ++k) fc[k] = stg[k * kStage + c0];
-                } else if (h == 1) {
-                    staged_inputs<8>(stg, c0, sx, sxy, zinv, inv, ext, a_op, t);
-                } else if (h == 2) {
-                    staged_inputs<16>(stg, c0, sx, sxy, zinv, inv, ext, a_op, t);
                 } else {
-                    staged_inputs<24>(stg, c0, sx, sxy, zinv, inv, ext, a_op, t);
+                    // the 9 cell inputs (243..251) are in this half only
+                    float ext[9];
+                    ext[0] = vp * (1.0f / 3000.0f);
+                    ext[1] = sqrtf(c_mu * c_b) * (1.0f / 1732.0f);
+                    ext[2] = rho * (1.0f / 2000.0f);
+                    band_of(cx, m.nxc, w, ext[3], ext[6]);
+                    band_of(cy, m.nyc, w, ext[4], ext[7]);
+                    band_of(cz, m.nzc, w, ext[5], ext[8]);
+                    staged_inputs<16>(stg, c0, sx, sxy, zinv, inv, ext, a_op, t);
                 }
             } else {
                 const float zero[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 #pragma unroll 4
-                for (int j = 8 * h; j < 8 * h + 8; ++j) store_chunk(a_op + kmaj(t, 8 * j, kK1), zero);
+                for (int j = 16 * h; j < 16 * h + 16; ++j) store_chunk(a_op + kmaj(t, 8 * j, kK1), zero);
             }
         }
 
@@ -537,7 +532,7 @@ k_strip_tc(Model m, int w, const int4 *tiles, int ntiles, const unsigned char *w
         parity ^= 1u;
         if (wg_sync_or(g, !ok)) { failed = true; break; }
         tc_after();
-        hidden_part(tmem, b1, a_op, t, 16 * h);
+        hidden_half(tmem, b1, a_op, t, 32 * h);
 
         // ---- layer 2: D2 = H1 (128 x 64) W2^T ----
         fence_async_smem();
@@ -552,7 +547,7 @@ k_strip_tc(Model m, int w, const int4 *tiles, int ntiles, const unsigned char *w
         parity ^= 1u;
         if (wg_sync_or(g, !ok)) { failed = true; break; }
         tc_after();
-        hidden_part(tmem + 64, b2, a_op, t, 16 * h);
+        hidden_half(tmem + 64, b2, a_op, t, 32 * h);
 
         // ---- layer 3: D3 = H2 (128 x 64) W3^T, N = 16 ----
         fence_async_smem();
@@ -568,7 +563,7 @@ k_strip_tc(Model m, int w, const int4 *tiles, int ntiles, const unsigned char *w
         if (wg_sync_or(g, !ok)) { failed = true; break; }
         tc_after();
 
-        // ---- epilogue (quarter 0) ----
+        // ---- epilogue (half 0) ----
         if (h == 0) {
             float o16[16];
             tmem_ld16(tmem, o16);
