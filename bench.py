@@ -625,16 +625,19 @@ def main_batch(args, world, rank, local):
 
 
 def end_to_end(s, w, K, world, stream, wav):
-    """The reference usage pattern through the C ABI (run(): medium upload,
-    per-step propagate with a host-supplied source value, per-step readback of
-    the receivers' samples), host buffers, timed on the host after a sync."""
+    """The reference's run() pattern through the C ABI with host buffers
+    (OPT/ElasticWaveEquation.cu:140-182): the medium uploaded from pinned host
+    memory, one sgfd_step per step with the host-computed source value, and
+    the receivers' samples of the K steps read back into pinned memory at the
+    end (the reference's station output), all inside the timed region; wall
+    clock, max over ranks."""
     import torch
     n = w.b.size
     pinned = [torch.empty(n, dtype=torch.float32, pin_memory=True) for _ in range(3)]
     for t, a in zip(pinned, (w.b, w.lam, w.mu)):
         t.numpy()[:] = a.reshape(-1)
     nrec = len(w.rec_comp)
-    out = torch.empty(nrec, dtype=torch.float32, pin_memory=True).numpy()
+    out = torch.empty((K, nrec), dtype=torch.float32, pin_memory=True).numpy()
     s.reset()
     s.synchronize()
     barrier(world)
@@ -642,15 +645,14 @@ def end_to_end(s, w, K, world, stream, wav):
     s.set_medium(*[t.numpy() for t in pinned])
     for it in range(K):
         s.step(it, float(wav[it]))
-        s.trace_step(it, out)
-    s.synchronize()
+    s.trace_range(0, K, out)
     secs = time.perf_counter() - t0
     secs = max_over_ranks(secs, world)
     h2d = (3 * n * 4) / K + 4
     return {"value": world * w.computed_cells() * K / secs / 1e9, "unit": "Gcell/s",
             "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": nrec * 4, "steps": K,
-            "note": "medium upload (3 x GRID floats, pinned) + K x (sgfd_step with host source value + "
-                    "sgfd_get_trace_step of all receivers), wall clock"}
+            "note": "medium upload (3 x GRID floats, pinned) + K x sgfd_step with the host source value + "
+                    "sgfd_get_trace_range of the K steps' receiver samples (pinned), wall clock"}
 
 
 if __name__ == "__main__":

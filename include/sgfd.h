@@ -219,6 +219,12 @@ int sgfd_get_traces(sgfd_solver *h, float *out);
 /* Copy the n receiver samples of one step `it` to out[0..n) (blocking);
  * the per-step readback of a drop-in loop (OPT/ElasticWaveEquation.cu:153-174). */
 int sgfd_get_trace_step(sgfd_solver *h, int32_t it, float *out);
+/* Copy the samples of steps it0 .. it0+n-1 to out[(it - it0)*nrec + r]
+ * (time-major, as recorded) in one transfer, waiting for the steps queued
+ * before it: the station readback at the end of a run
+ * (OPT/ElasticWaveEquation.cu:174, stationDataOutput :950-960) for only the
+ * steps taken.  out may be pinned memory. */
+int sgfd_get_trace_range(sgfd_solver *h, int32_t it0, int32_t n, float *out);
 /* Copy one wavefield (sgfd_field) to a host array of nx*ny*nz floats. */
 int sgfd_get_field(sgfd_solver *h, int32_t field, float *out);
 /* Copy one medium array (sgfd_medium_id) back to host (nx*ny*nz floats). */

@@ -764,6 +764,19 @@ int sgfd_get_traces(sgfd_solver *h, float *out) {
     return SGFD_OK;
 }
 
+int sgfd_get_trace_range(sgfd_solver *h, int32_t it0, int32_t n, float *out) {
+    int r = check_handle(h);
+    if (r) return r;
+    if (!out && n > 0) return fail(h, SGFD_ERR_INVALID, "null output");
+    if (it0 < 0 || n < 0 || (int64_t)it0 + n > h->sr.nt)
+        return fail(h, SGFD_ERR_INVALID, "steps %d..%d outside the trace length %d", it0, it0 + n - 1, h->sr.nt);
+    if (n == 0 || h->sr.nrec == 0) return SGFD_OK;
+    SG_CUDA(h, cudaMemcpyAsync(out, h->traces + (size_t)it0 * h->sr.nrec, (size_t)n * h->sr.nrec * sizeof(float),
+                               cudaMemcpyDeviceToHost, h->stream), "trace range download");
+    SG_CUDA(h, cudaStreamSynchronize(h->stream), "trace range download");
+    return check_device_error(h);
+}
+
 int sgfd_get_trace_step(sgfd_solver *h, int32_t it, float *out) {
     int r = check_handle(h);
     if (r) return r;

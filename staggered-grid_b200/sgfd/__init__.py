@@ -99,6 +99,7 @@ def lib() -> ctypes.CDLL:
         "sgfd_synchronize": (ctypes.c_int, [vp]),
         "sgfd_reset": (ctypes.c_int, [vp]),
         "sgfd_get_traces": (ctypes.c_int, [vp, fp]),
+        "sgfd_get_trace_range": (ctypes.c_int, [vp, i32, i32, fp]),
         "sgfd_get_trace_step": (ctypes.c_int, [vp, i32, fp]),
         "sgfd_profile": (ctypes.c_int, [vp, i32, i32, fp, fp]),
         "sgfd_get_field": (ctypes.c_int, [vp, i32, fp]),
@@ -268,6 +269,14 @@ class Solver:
         out = np.zeros((self.nrec, self.nt), dtype=np.float32)
         if self.nrec:
             self._check(lib().sgfd_get_traces(self.h, _fptr(out)))
+        return out
+
+    def trace_range(self, it0: int, n: int, out: np.ndarray | None = None) -> np.ndarray:
+        """Samples of steps it0 .. it0+n-1, time-major [n][nrec], in one transfer."""
+        if out is None:
+            out = np.zeros((n, self.nrec), dtype=np.float32)
+        assert out.dtype == np.float32 and out.flags.c_contiguous and out.size >= n * self.nrec
+        self._check(lib().sgfd_get_trace_range(self.h, it0, n, _fptr(out)))
         return out
 
     def trace_step(self, it: int, out: np.ndarray | None = None) -> np.ndarray:

@@ -107,6 +107,23 @@ def test_station_files(tmp_path):
         assert not os.path.exists(prefix + f"_short_{names[c0]}.bin")
 
 
+def test_trace_range_readback():
+    """sgfd_get_trace_range: one time-major block of steps equals the same
+    steps of sgfd_get_traces and of sgfd_get_trace_step; ranges past the
+    trace length are rejected."""
+    w = wl.small_random_case(nt=40, nrec=24)
+    with make_solver(w) as s:
+        for it in range(25):
+            s.step(it, float(w.wavelet[it]))
+        block = s.trace_range(3, 20)
+        tr = s.traces()
+        np.testing.assert_array_equal(block, tr[:, 3:23].T)
+        np.testing.assert_array_equal(block[5], s.trace_step(8))
+        assert s.trace_range(0, 0).shape == (0, len(w.rec_comp))
+        with pytest.raises(sgfd.SgfdError):
+            s.trace_range(30, 11)
+
+
 def test_checkpoint_moves_between_kernel_families():
     """The checkpoint layout does not depend on the kernel family: a state saved
     by the z-marching kernels resumes on the per-cell kernels bit for bit."""
