@@ -204,6 +204,13 @@ __global__ void k_reciprocal(float *rmu, const float *mu, int64_t n) {
         rmu[i] = __frcp_rn(mu[i]);   // 1 / mu, IEEE round-to-nearest (ElasticMacro.h:112)
 }
 
+// Packed rows (nx floats each, as a host array is laid out) into the padded
+// device layout (row pitch px): one block per row at a time.
+__global__ void k_pitch_rows(float *dst, int64_t px, const float *src, int nx, int64_t nrows) {
+    for (int64_t r = blockIdx.x; r < nrows; r += gridDim.x)
+        for (int x = threadIdx.x; x < nx; x += blockDim.x) dst[r * px + x] = src[r * (int64_t)nx + x];
+}
+
 }  // namespace
 
 int simple_launches_per_step(const SourceRec &sr) {
@@ -242,6 +249,11 @@ cudaError_t launch_shear_means(const Model &m, const Physics &ph, float *mxy, fl
 
 cudaError_t launch_counter(int *ctr, int value, bool add, cudaStream_t s) {
     k_counter<<<1, 32, 0, s>>>(ctr, value, add ? 1 : 0);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pitch_rows(float *dst, int64_t px, const float *src, int nx, int64_t nrows, cudaStream_t s) {
+    k_pitch_rows<<<1184, 128, 0, s>>>(dst, px, src, nx, nrows);
     return cudaGetLastError();
 }
 

@@ -528,9 +528,22 @@ static int upload_medium(sgfd_solver *h, const float *b, const float *l, const f
     const size_t rows = (size_t)m.ny * m.nz;
     const float *src[3] = {b, l, mu};
     float *dst[3] = {const_cast<float *>(m.b), const_cast<float *>(m.lam), const_cast<float *>(m.mu)};
-    for (int k = 0; k < 3; ++k)
-        SG_CUDA(h, cudaMemcpy2DAsync(dst[k], (size_t)m.px * sizeof(float), src[k], row, row, rows, kind, h->stream),
-                "medium upload");
+    if (kind == cudaMemcpyHostToDevice) {
+        // One contiguous transfer per array (short-row 2D copies from host
+        // memory run far below the link's bandwidth) into the storage of the
+        // three shear moduli, which are recomputed from b and mu below, then
+        // into the padded rows on the device.
+        float *stage[3] = {const_cast<float *>(m.mxy) - kXOff, const_cast<float *>(m.mxz) - kXOff,
+                           const_cast<float *>(m.myz) - kXOff};
+        for (int k = 0; k < 3; ++k)
+            SG_CUDA(h, cudaMemcpyAsync(stage[k], src[k], row * rows, kind, h->stream), "medium upload");
+        for (int k = 0; k < 3; ++k)
+            SG_CUDA(h, launch_pitch_rows(dst[k], m.px, stage[k], m.nx, (int64_t)rows, h->stream), "medium rows");
+    } else {
+        for (int k = 0; k < 3; ++k)
+            SG_CUDA(h, cudaMemcpy2DAsync(dst[k], (size_t)m.px * sizeof(float), src[k], row, row, rows, kind,
+                                         h->stream), "medium upload");
+    }
     cudaError_t e = launch_reciprocal(const_cast<float *>(m.rmu) - kXOff, m.mu - kXOff, m.plane * m.nz, h->stream);
     if (e == cudaSuccess)
         e = launch_shear_means(m, h->ph, const_cast<float *>(m.mxy), const_cast<float *>(m.mxz),

@@ -185,6 +185,8 @@ int simple_launches_per_step(const SourceRec &sr);
 // medium post-processing: rmu = 1/mu over the padded arrays, then the three
 // staggered shear moduli of every computed cell from rmu.
 cudaError_t launch_reciprocal(float *rmu, const float *mu, int64_t n, cudaStream_t s);
+// dst[r * px + x] = src[r * nx + x] for nrows rows of nx floats.
+cudaError_t launch_pitch_rows(float *dst, int64_t px, const float *src, int nx, int64_t nrows, cudaStream_t s);
 cudaError_t launch_shear_means(const Model &m, const Physics &ph, float *mxy, float *mxz, float *myz,
                                cudaStream_t s);
 // FP64 energy audit (kernels_audit.cu): partials holds 2 doubles per block,
