@@ -249,31 +249,32 @@ __device__ __forceinline__ float ex2_approx(float x) {
     asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
     return r;
 }
-// GELU(x) = x Phi(x), Phi(x) = erfc(-x / sqrt 2) / 2, with erfc from the
-// Chebyshev fit of Numerical Recipes (Press et al., 2nd ed., section 6.2,
-// erfcc): for z >= 0, erfc(z) = t exp(P(t) - z^2), t = 1 / (1 + z / 2), P of
-// degree 9, fractional error below 1.2e-7 for every z, the small negative
-// tail included -- far below the half ulp of the binary16 the activation is
-// stored in (2.4e-4 relative).  The exponential is 2^((P - z^2) log2 e).
-// Two values at a time with packed FP32x2 arithmetic.
+// GELU(x) = x Phi(x) = max(x, 0) - |x| erfc(|x| / sqrt 2) / 2 for either sign
+// of x, with erfc from the Chebyshev fit of Numerical Recipes (Press et al.,
+// 2nd ed., section 6.2, erfcc): erfc(z) = t exp(P(t) - z^2), t = 1 / (1 + z / 2),
+// P of degree 9, fractional error below 1.2e-7 for every z, the small
+// negative tail included -- far below the half ulp of the binary16 the
+// activation is stored in (2.4e-4 relative).  The factor 1/2 and the change
+// to base 2 are folded into P's coefficients: erfc(z) / 2 =
+// t 2^(P2(t) - x^2 log2(e) / 2) with P2 = (P - ln 2) log2(e).  Two values at a
+// time with packed FP32x2 arithmetic; the reciprocal and 2^q on the SFU.
 __device__ __forceinline__ float2 f2(float v) { return make_float2(v, v); }
 __device__ __forceinline__ float2 gelu_fast2(float2 x) {
-    const float2 z = __fmul2_rn(make_float2(fabsf(x.x), fabsf(x.y)), f2(0.70710678f));
-    const float2 d = __ffma2_rn(f2(0.5f), z, f2(1.0f));
+    const float2 nax = make_float2(-fabsf(x.x), -fabsf(x.y));
+    const float2 d = __ffma2_rn(nax, f2(-0.35355339f), f2(1.0f));
     const float2 t = make_float2(rcp_approx(d.x), rcp_approx(d.y));
-    float2 p = __ffma2_rn(t, f2(0.17087277f), f2(-0.82215223f));
-    p = __ffma2_rn(t, p, f2(1.48851587f));
-    p = __ffma2_rn(t, p, f2(-1.13520398f));
-    p = __ffma2_rn(t, p, f2(0.27886807f));
-    p = __ffma2_rn(t, p, f2(-0.18628806f));
-    p = __ffma2_rn(t, p, f2(0.09678418f));
-    p = __ffma2_rn(t, p, f2(0.37409196f));
-    p = __ffma2_rn(t, p, f2(1.00002368f));
-    p = __ffma2_rn(t, p, f2(-1.26551223f));
-    const float2 q = __fmul2_rn(__ffma2_rn(make_float2(-z.x, -z.y), z, p), f2(1.44269504f));
-    const float2 he = __fmul2_rn(__fmul2_rn(f2(0.5f), t), make_float2(ex2_approx(q.x), ex2_approx(q.y)));
-    const float2 phi = make_float2(x.x >= 0.0f ? 1.0f - he.x : he.x, x.y >= 0.0f ? 1.0f - he.y : he.y);
-    return __fmul2_rn(x, phi);
+    float2 p = __ffma2_rn(t, f2(0.2465172979f), f2(-1.186114945f));
+    p = __ffma2_rn(t, p, f2(2.147474464f));
+    p = __ffma2_rn(t, p, f2(-1.637753152f));
+    p = __ffma2_rn(t, p, f2(0.4023215817f));
+    p = __ffma2_rn(t, p, f2(-0.2687568603f));
+    p = __ffma2_rn(t, p, f2(0.1396300565f));
+    p = __ffma2_rn(t, p, f2(0.5397006155f));
+    p = __ffma2_rn(t, p, f2(1.442729204f));
+    p = __ffma2_rn(t, p, f2(-2.825748218f));
+    const float2 q = __ffma2_rn(__fmul2_rn(x, f2(-0.72134752f)), x, p);
+    const float2 e = make_float2(ex2_approx(q.x), ex2_approx(q.y));
+    return __ffma2_rn(__fmul2_rn(nax, t), e, make_float2(fmaxf(x.x, 0.0f), fmaxf(x.y, 0.0f)));
 }
 
 // Hidden layer, columns c0 .. c0+31 of this thread's row: accumulators + bias,
