@@ -27,7 +27,7 @@
 // shared memory with coalesced loads, with each staged cell's sums of squares,
 // and two threads build a cell's 252 inputs from there into row t of the A
 // operand.
-// Each CTA (one per SM) holds the weights once and runs two groups of 256
+// Each CTA (one per SM) holds the weights once and runs three groups of 256
 // threads that work on alternate tiles, so one group's loads overlap the
 // other's tensor-core and epilogue work; two threads share each row.  The
 // hidden layers' GELU uses a Chebyshev fit of erfc (Numerical Recipes erfcc,
@@ -140,16 +140,18 @@ constexpr int kStage = 544;                // staged cells per box, (32+2)(2+2)(
 constexpr int kImgW1 = 0, kImgW2 = kImgW1 + kH * kK1 * 2, kImgW3 = kImgW2 + kH * kH * 2,
               kImgB = kImgW3 + kN3 * kH * 2, kImg = kImgB + (2 * kH + kN3) * 4;
 constexpr int kImgPad = (kImg + 1023) / 1024 * 1024;
-constexpr int kAOp = kRows * kK1 * 2;                        // A operand of one warpgroup
+constexpr int kKHalf = kK1 / 2;                              // layer 1 runs in two halves of K
+constexpr int kAOp = kRows * kKHalf * 2;                     // A operand of one group (one half of K)
 constexpr int kStg = 11 * kStage * 4;                        // staged fields and sums of squares of one warpgroup
 constexpr int kRed = 4 * kRows * 4;                          // partial sums of squares of one warpgroup
 constexpr int kMed = 3 * kRows * 4;                          // b, lambda, mu of the next tile's cells
 constexpr int kWgBytes = kAOp + (kStg + 1023) / 1024 * 1024 + kRed + kMed;
-constexpr int kTcSmem = 128 + kImgPad + 2 * kWgBytes + 64;   // + alignment, barriers, TMEM address
-constexpr int kTcThreads = 512;                              // two warpgroups of 256: two threads per row
+constexpr int kGroups = 3;                                   // tile groups per CTA
+constexpr int kTcSmem = 128 + kImgPad + kGroups * kWgBytes + 64;   // + alignment, barriers, TMEM address
+constexpr int kTcThreads = kGroups * 2 * kRows;              // groups of 256 threads: two threads per row
 static_assert(kImg % 16 == 0, "weight image is copied in 16-byte pieces");
 static_assert(kTcSmem <= 232448, "shared memory of one CTA");
-constexpr uint32_t kTmemCols = 256;                          // 128 per warpgroup: D1/D3 at +0, D2 at +64
+constexpr uint32_t kTmemCols = 512;                          // 128 per group: D1/D3 at +0, D2 at +64
 
 // Byte offset of element (row, k) of a K-major operand with KT columns: 8x8
 // core matrices of 128 contiguous bytes (8 rows of 16 bytes), the K-adjacent
@@ -202,16 +204,21 @@ __device__ __forceinline__ bool wg_sync_or(int g, bool flag) {
 }
 __device__ __forceinline__ void wg_sync(int g) { asm volatile("bar.sync %0, 256;" ::"r"(g + 1) : "memory"); }
 
-// D[tmem] (+)= A[a] * B[b]^T over KT columns, M = 128, N = n, K = 16 per instruction.
-__device__ __forceinline__ void mma_chain(uint32_t tmem_d, uint32_t a, uint32_t b, int KT, int n) {
+// D[tmem] (+)= A[a] * B[b]^T over nk steps of K = 16 (M = 128, N = n); A and
+// B are K-major with kta and ktb columns; acc: add to D from the first step.
+__device__ __forceinline__ void mma_k(uint32_t tmem_d, uint32_t a, int kta, uint32_t b, int ktb, int nk, int n,
+                                      bool acc) {
     const uint32_t id = instr_desc(n);
-    for (int kk = 0; kk < KT / 16; ++kk) {
-        const uint64_t ad = smem_desc(a + kk * 256, KT), bd = smem_desc(b + kk * 256, KT);
+    for (int kk = 0; kk < nk; ++kk) {
+        const uint64_t ad = smem_desc(a + kk * 256, kta), bd = smem_desc(b + kk * 256, ktb);
         asm volatile(
             "{\n .reg .pred p;\n setp.ne.u32 p, %4, 0;\n"
             " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n"
-            ::"r"(tmem_d), "l"(ad), "l"(bd), "r"(id), "r"((uint32_t)(kk > 0)) : "memory");
+            ::"r"(tmem_d), "l"(ad), "l"(bd), "r"(id), "r"((uint32_t)(acc || kk > 0)) : "memory");
     }
+}
+__device__ __forceinline__ void mma_chain(uint32_t tmem_d, uint32_t a, uint32_t b, int KT, int n) {
+    mma_k(tmem_d, a, KT, b, KT, KT / 16, n, false);
 }
 __device__ __forceinline__ void mma_commit(uint64_t *bar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(saddr_of(bar))
@@ -373,12 +380,13 @@ __device__ __forceinline__ void staged_sums(const float *stg, int c0, int sx, in
     }
 }
 
-// Inputs J0*8 .. J0*8+127 of row t (16 chunks of 8) from the staged fields.
+// Inputs J0*8 .. J0*8+63 of row t (8 chunks of 8) from the staged fields,
+// into columns col0 .. col0+63 of the half-K A operand.
 template <int J0>
 __device__ __forceinline__ void staged_inputs(const float *stg, int c0, int sx, int sxy, float zinv, float inv,
-                                              const float (&ext)[9], unsigned char *a_op, int t) {
+                                              const float (&ext)[9], unsigned char *a_op, int t, int col0) {
 #pragma unroll
-    for (int j = J0; j < J0 + 16; ++j) {
+    for (int j = J0; j < J0 + 8; ++j) {
         float v[8];
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
@@ -391,14 +399,14 @@ __device__ __forceinline__ void staged_inputs(const float *stg, int c0, int sx, 
                 v[q] = f < kIn ? ext[f - 243] : 0.0f;
             }
         }
-        store_chunk(a_op + kmaj(t, 8 * j, kK1), v);
+        store_chunk(a_op + kmaj(t, col0 + 8 * (j - J0), kKHalf), v);
     }
 }
 
 // Network of every strip cell (ROWS = false), or of n input rows X (ROWS =
 // true: the tensor-core path checked on given inputs, raw outputs to out).
-// One CTA per SM with 512 threads in two groups of 256; group g takes tiles
-// 2*blockIdx.x + g, then every 2*gridDim.x-th.  In a group, threads t and
+// One CTA per SM with 768 threads in three groups of 256; group g takes tiles
+// 3*blockIdx.x + g, then every 3*gridDim.x-th.  In a group, threads t and
 // t + 128 (warps w and w + 4, which reach the same TMEM lanes) share row t of
 // a tile: half h = 0 takes neighbours 0..13, inputs 0..127 and hidden
 // columns 0..31, half h = 1 neighbours 14..26, inputs 128..255 (with the 9
@@ -415,12 +423,12 @@ k_strip_tc(Model m, int w, const int4 *tiles, int ntiles, const unsigned char *w
     float *stg = reinterpret_cast<float *>(a_op + kAOp);
     float *red = reinterpret_cast<float *>(a_op + kWgBytes - kRed - kMed);
     float *med = reinterpret_cast<float *>(a_op + kWgBytes - kMed);
-    uint64_t *bar = reinterpret_cast<uint64_t *>(sm + kImgPad + 2 * kWgBytes);
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bar + 2);
+    uint64_t *bar = reinterpret_cast<uint64_t *>(sm + kImgPad + kGroups * kWgBytes);
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bar + kGroups);
 
     for (int i = tid; i < kImg / 16; i += blockDim.x)
         reinterpret_cast<uint4 *>(sm)[i] = reinterpret_cast<const uint4 *>(wimg)[i];
-    if (tid == 0) { mbar_init1(&bar[0]); mbar_init1(&bar[1]); }
+    if (tid < kGroups) mbar_init1(&bar[tid]);
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(saddr_of(tmem_slot)),
                      "r"(kTmemCols) : "memory");
@@ -441,25 +449,21 @@ k_strip_tc(Model m, int w, const int4 *tiles, int ntiles, const unsigned char *w
     bool failed = false;
 
     const int nt = ROWS ? (int)((nrows + kRows - 1) / kRows) : ntiles;
-    if (!ROWS && 2 * (int)blockIdx.x + g < nt) stage_async(m, tiles[2 * blockIdx.x + g], stg, med, u);
-    for (int tile = 2 * blockIdx.x + g; tile < nt; tile += 2 * gridDim.x) {
-        // ---- inputs: row t of the A operand, half h ----
-        float s = 0.0f, zimp = 1.0f, fc[kOut], c_b = 1.0f, c_lam = 0.0f, c_mu = 1.0f;
-        int count;
+    const int first = kGroups * (int)blockIdx.x + g, stride = kGroups * (int)gridDim.x;
+    if (!ROWS && first < nt) stage_async(m, tiles[first], stg, med, u);
+    for (int tile = first; tile < nt; tile += stride) {
+        // ---- row t's set-up: scale s, cell medium ----
+        float s = 0.0f, zimp = 1.0f, inv = 0.0f, zinv = 0.0f, rho = 0.0f, vp = 0.0f, fc[kOut];
+        float c_b = 1.0f, c_lam = 0.0f, c_mu = 1.0f;
+        int count, c0 = 0, cx = 0, cy = 0, cz = 0, sx = 0, sxy = 0;
         if (ROWS) {
-            const int64_t first = (int64_t)tile * kRows, row = first + t;
-            count = (int)(nrows - first < kRows ? nrows - first : kRows);
-            const float *x = X + row * kIn;
-#pragma unroll 4
-            for (int j = 16 * h; j < 16 * h + 16; ++j) {
-                float v[8];
-#pragma unroll
-                for (int q = 0; q < 8; ++q) v[q] = (t < count && 8 * j + q < kIn) ? x[8 * j + q] : 0.0f;
-                store_chunk(a_op + kmaj(t, 8 * j, kK1), v);
-            }
+            const int64_t first_row = (int64_t)tile * kRows;
+            count = (int)(nrows - first_row < kRows ? nrows - first_row : kRows);
         } else {
             const Box bx = box_of(tiles[tile]);
-            const int sx = bx.ex + 2, sxy = sx * (bx.ey + 2), ns = sxy * (bx.ez + 2);
+            sx = bx.ex + 2;
+            sxy = sx * (bx.ey + 2);
+            const int ns = sxy * (bx.ez + 2);
             cp_async_wait_all();   // this tile's copies, started during the previous tile
             for (int r = u; r < ns; r += 2 * kRows) {
                 float f[9];
@@ -470,20 +474,17 @@ k_strip_tc(Model m, int w, const int4 *tiles, int ntiles, const unsigned char *w
             }
             wg_sync(g);
             count = bx.ex * bx.ey * bx.ez;
-            int c0 = 0, cx = 0, cy = 0, cz = 0;
-            float rho = 0.0f, vp = 0.0f;
             if (t < count) {
                 const int lx = t % bx.ex, ly = (t / bx.ex) % bx.ey, lz = t / (bx.ex * bx.ey);
                 cx = bx.x + lx;
                 cy = bx.y + ly;
                 cz = bx.z + lz;
                 c0 = (lx + 1) + (ly + 1) * sx + (lz + 1) * sxy;
-                const float b = med[t], lam = med[kRows + t], mu = med[2 * kRows + t];
-                c_b = b;
-                c_lam = lam;
-                c_mu = mu;
-                rho = 1.0f / b;
-                vp = sqrtf((lam + 2.0f * mu) * b);
+                c_b = med[t];
+                c_lam = med[kRows + t];
+                c_mu = med[2 * kRows + t];
+                rho = 1.0f / c_b;
+                vp = sqrtf((c_lam + 2.0f * c_mu) * c_b);
                 zimp = rho * vp;
                 float sv, ss;
                 if (h == 0) staged_sums<0, 14>(stg, c0, sx, sxy, sv, ss);
@@ -494,14 +495,38 @@ k_strip_tc(Model m, int w, const int4 *tiles, int ntiles, const unsigned char *w
             wg_sync(g);
             if (t < count) {
                 s = rms_scale(red[t] + red[2 * kRows + t], red[kRows + t] + red[3 * kRows + t], zimp);
-                const float inv = s > 0.0f ? 1.0f / s : 0.0f, zinv = zimp * inv;
+                inv = s > 0.0f ? 1.0f / s : 0.0f;
+                zinv = zimp * inv;
                 if (h == 0) {
-                    const float none[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};   // inputs 0..127 hold no cell inputs
-                    staged_inputs<0>(stg, c0, sx, sxy, zinv, inv, none, a_op, t);
 #pragma unroll
                     for (int k = 0; k < kOut; ++k) fc[k] = stg[k * kStage + c0];
+                }
+            }
+        }
+
+        // ---- layer 1 in two halves of K: D1 = A W1^T, the A operand holding
+        // inputs 128*half .. 128*half+127 (row t: 64 of them per thread) ----
+        bool bad = false;
+        for (int half = 0; half < 2; ++half) {
+            if (ROWS) {
+                const float *x = X + ((int64_t)tile * kRows + t) * kIn;
+#pragma unroll 2
+                for (int j = 0; j < 8; ++j) {
+                    const int k0 = kKHalf * half + 64 * h + 8 * j;
+                    float v[8];
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) v[q] = (t < count && k0 + q < kIn) ? x[k0 + q] : 0.0f;
+                    store_chunk(a_op + kmaj(t, 64 * h + 8 * j, kKHalf), v);
+                }
+            } else if (t < count) {
+                const float none[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};   // inputs 0..191 hold no cell inputs
+                if (half == 0) {
+                    if (h == 0) staged_inputs<0>(stg, c0, sx, sxy, zinv, inv, none, a_op, t, 0);
+                    else staged_inputs<8>(stg, c0, sx, sxy, zinv, inv, none, a_op, t, 64);
+                } else if (h == 0) {
+                    staged_inputs<16>(stg, c0, sx, sxy, zinv, inv, none, a_op, t, 0);
                 } else {
-                    // the 9 cell inputs (243..251) are in this half only
+                    // the 9 cell inputs (243..251) are in this quarter only
                     float ext[9];
                     ext[0] = vp * (1.0f / 3000.0f);
                     ext[1] = sqrtf(c_mu * c_b) * (1.0f / 1732.0f);
@@ -509,30 +534,31 @@ k_strip_tc(Model m, int w, const int4 *tiles, int ntiles, const unsigned char *w
                     band_of(cx, m.nxc, w, ext[3], ext[6]);
                     band_of(cy, m.nyc, w, ext[4], ext[7]);
                     band_of(cz, m.nzc, w, ext[5], ext[8]);
-                    staged_inputs<16>(stg, c0, sx, sxy, zinv, inv, ext, a_op, t);
+                    staged_inputs<24>(stg, c0, sx, sxy, zinv, inv, ext, a_op, t, 64);
                 }
             } else {
                 const float zero[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-#pragma unroll 4
-                for (int j = 16 * h; j < 16 * h + 16; ++j) store_chunk(a_op + kmaj(t, 8 * j, kK1), zero);
+#pragma unroll 2
+                for (int j = 0; j < 8; ++j) store_chunk(a_op + kmaj(t, 64 * h + 8 * j, kKHalf), zero);
             }
-        }
-
-        // ---- layer 1: D1 = A (128 x 256) W1^T ----
-        fence_async_smem();
-        tc_before();
-        wg_sync(g);
-        if (u == 0) {
+            fence_async_smem();
+            tc_before();
+            wg_sync(g);
+            if (u == 0) {
+                tc_after();
+                mma_k(tmem_g, a_s, kKHalf, w1_s + half * (kKHalf / 16) * 256, kK1, kKHalf / 16, kH, half > 0);
+                mma_commit(mybar);
+            }
+            // after the second half the staging area is free: the next tile's
+            // copies overlap this one's network
+            if (!ROWS && half == 1 && tile + stride < nt) stage_async(m, tiles[tile + stride], stg, med, u);
+            const bool ok = mbar_wait_bounded(mybar, parity);
+            parity ^= 1u;
+            bad = wg_sync_or(g, !ok);
+            if (bad) break;
             tc_after();
-            mma_chain(tmem_g, a_s, w1_s, kK1, kH);
-            mma_commit(mybar);
         }
-        // the staging area is free: the next tile's copies overlap this one's network
-        if (!ROWS && tile + 2 * (int)gridDim.x < nt) stage_async(m, tiles[tile + 2 * gridDim.x], stg, med, u);
-        bool ok = mbar_wait_bounded(mybar, parity);
-        parity ^= 1u;
-        if (wg_sync_or(g, !ok)) { failed = true; break; }
-        tc_after();
+        if (bad) { failed = true; break; }
         hidden_half(tmem, b1, a_op, t, 32 * h);
 
         // ---- layer 2: D2 = H1 (128 x 64) W2^T ----
@@ -544,7 +570,7 @@ k_strip_tc(Model m, int w, const int4 *tiles, int ntiles, const unsigned char *w
             mma_chain(tmem_g + 64, a_s, w2_s, kH, kH);
             mma_commit(mybar);
         }
-        ok = mbar_wait_bounded(mybar, parity);
+        bool ok = mbar_wait_bounded(mybar, parity);
         parity ^= 1u;
         if (wg_sync_or(g, !ok)) { failed = true; break; }
         tc_after();
@@ -614,11 +640,11 @@ k_strip_tc(Model m, int w, const int4 *tiles, int ntiles, const unsigned char *w
     }
 }
 
-// One CTA per SM (fewer for small strips): each runs two warpgroups.
+// One CTA per SM (fewer for small strips): each runs kGroups tile groups.
 int tc_grid(int ntiles) {
     int dev = 0, sms = 148;
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    return std::max(1, std::min(sms, (ntiles + 1) / 2));
+    return std::max(1, std::min(sms, (ntiles + kGroups - 1) / kGroups));
 }
 
 // Adds the corrections to the strip cells (after every cell's correction has
