@@ -656,8 +656,16 @@ __global__ void __launch_bounds__(kRows) k_strip_apply(Model m, const int4 *tile
     const int lx = t % bx.ex, ly = (t / bx.ex) % bx.ey, lz = t / (bx.ex * bx.ey);
     const int64_t c = pidx(m, bx.x + lx + kHalo, bx.y + ly + kHalo, bx.z + lz + kHalo);
     const float *dt = delta + (int64_t)blockIdx.x * (kRows * kOut);
+    // every load before the first store: the field arrays and delta could
+    // alias as far as the compiler knows, which would otherwise serialise
+    // nine load-store round trips
+    float d[kOut], f[kOut];
 #pragma unroll
-    for (int k = 0; k < kOut; ++k) m.f[k][c] += dt[k * kRows + t];
+    for (int k = 0; k < kOut; ++k) d[k] = dt[k * kRows + t];
+#pragma unroll
+    for (int k = 0; k < kOut; ++k) f[k] = m.f[k][c];
+#pragma unroll
+    for (int k = 0; k < kOut; ++k) m.f[k][c] = f[k] + d[k];
 }
 
 // ---- training kernels ------------------------------------------------------
