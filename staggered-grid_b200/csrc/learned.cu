@@ -411,7 +411,7 @@ __device__ __forceinline__ void staged_inputs(const float *stg, int c0, int sx, 
 // a tile: half h = 0 takes neighbours 0..13, inputs 0..127 and hidden
 // columns 0..31, half h = 1 neighbours 14..26, inputs 128..255 (with the 9
 // cell inputs) and hidden columns 32..63; half 0 runs the epilogue.
-// delta[tile][k][128] receives the energy-limited corrections.
+// delta[tile][k][128] receives the corrected fields f + a d (a d the energy-limited correction).
 template <bool ROWS>
 __global__ void __launch_bounds__(kTcThreads, 1)
 k_strip_tc(Model m, int w, const int4 *tiles, int ntiles, const unsigned char *wimg, float *delta, const float *X,
@@ -621,7 +621,7 @@ k_strip_tc(Model m, int w, const int4 *tiles, int ntiles, const unsigned char *w
                     const float a = (Q > 0.0f && B < 0.0f) ? fminf(1.0f, -2.0f * B / Q) : 0.0f;
                     float *dt = delta + (int64_t)tile * (kRows * kOut);
 #pragma unroll
-                    for (int k = 0; k < kOut; ++k) dt[k * kRows + t] = a * d[k];
+                    for (int k = 0; k < kOut; ++k) dt[k * kRows + t] = fc[k] + a * d[k];
                 }
             }
         }
@@ -647,8 +647,9 @@ int tc_grid(int ntiles) {
     return std::max(1, std::min(sms, (ntiles + kGroups - 1) / kGroups));
 }
 
-// Adds the corrections to the strip cells (after every cell's correction has
-// been computed from the uncorrected state).  One block per tile.
+// Writes the corrected fields into the strip cells (after every cell's
+// correction has been computed from the uncorrected state).  One block per
+// tile; k_strip_tc left f + a d for each cell in delta[tile][k][128].
 __global__ void __launch_bounds__(kRows) k_strip_apply(Model m, const int4 *tiles, const float *delta) {
     const Box bx = box_of(tiles[blockIdx.x]);
     const int t = threadIdx.x;
@@ -656,16 +657,11 @@ __global__ void __launch_bounds__(kRows) k_strip_apply(Model m, const int4 *tile
     const int lx = t % bx.ex, ly = (t / bx.ex) % bx.ey, lz = t / (bx.ex * bx.ey);
     const int64_t c = pidx(m, bx.x + lx + kHalo, bx.y + ly + kHalo, bx.z + lz + kHalo);
     const float *dt = delta + (int64_t)blockIdx.x * (kRows * kOut);
-    // every load before the first store: the field arrays and delta could
-    // alias as far as the compiler knows, which would otherwise serialise
-    // nine load-store round trips
-    float d[kOut], f[kOut];
+    float v[kOut];   // every load before the first store (the arrays could alias as far as the compiler knows)
 #pragma unroll
-    for (int k = 0; k < kOut; ++k) d[k] = dt[k * kRows + t];
+    for (int k = 0; k < kOut; ++k) v[k] = dt[k * kRows + t];
 #pragma unroll
-    for (int k = 0; k < kOut; ++k) f[k] = m.f[k][c];
-#pragma unroll
-    for (int k = 0; k < kOut; ++k) m.f[k][c] = f[k] + d[k];
+    for (int k = 0; k < kOut; ++k) m.f[k][c] = v[k];
 }
 
 // ---- training kernels ------------------------------------------------------
