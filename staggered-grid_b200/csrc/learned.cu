@@ -1028,7 +1028,7 @@ int strip_tile_list(const Model &m, int w, std::vector<int4> &tiles) {
     return fits ? (int)tiles.size() : -1;
 }
 
-// Strip buffer: weight image, corrections [tile][9][128], error flag.
+// Strip buffer: weight image, corrected fields [tile][9][128], error flag.
 size_t strip_buffer_bytes(int ntiles) { return (size_t)kImgPad + (size_t)ntiles * kRows * kOut * 4 + 16; }
 int *strip_error_flag(float *buf, int ntiles) {
     return reinterpret_cast<int *>(reinterpret_cast<unsigned char *>(buf) + strip_buffer_bytes(ntiles) - 16);
