@@ -648,24 +648,20 @@ int tc_grid(int ntiles) {
 }
 
 // Writes the corrected fields into the strip cells (after every cell's
-// correction has been computed from the uncorrected state).  Each block
-// takes two tiles at a time (128 threads each) and strides over the tiles;
-// k_strip_tc left f + a d for each cell in delta[tile][k][128].
-__global__ void __launch_bounds__(2 * kRows) k_strip_apply(Model m, const int4 *tiles, int ntiles,
-                                                           const float *delta) {
-    const int t = threadIdx.x % kRows;
-    for (int tile = 2 * blockIdx.x + threadIdx.x / kRows; tile < ntiles; tile += 2 * gridDim.x) {
-        const Box bx = box_of(tiles[tile]);
-        if (t >= bx.ex * bx.ey * bx.ez) continue;
-        const int lx = t % bx.ex, ly = (t / bx.ex) % bx.ey, lz = t / (bx.ex * bx.ey);
-        const int64_t c = pidx(m, bx.x + lx + kHalo, bx.y + ly + kHalo, bx.z + lz + kHalo);
-        const float *dt = delta + (int64_t)tile * (kRows * kOut);
-        float v[kOut];   // every load before the first store (the arrays could alias as far as the compiler knows)
+// correction has been computed from the uncorrected state).  One block per
+// tile; k_strip_tc left f + a d for each cell in delta[tile][k][128].
+__global__ void __launch_bounds__(kRows) k_strip_apply(Model m, const int4 *tiles, const float *delta) {
+    const Box bx = box_of(tiles[blockIdx.x]);
+    const int t = threadIdx.x;
+    if (t >= bx.ex * bx.ey * bx.ez) return;
+    const int lx = t % bx.ex, ly = (t / bx.ex) % bx.ey, lz = t / (bx.ex * bx.ey);
+    const int64_t c = pidx(m, bx.x + lx + kHalo, bx.y + ly + kHalo, bx.z + lz + kHalo);
+    const float *dt = delta + (int64_t)blockIdx.x * (kRows * kOut);
+    float v[kOut];   // every load before the first store (the arrays could alias as far as the compiler knows)
 #pragma unroll
-        for (int k = 0; k < kOut; ++k) v[k] = dt[k * kRows + t];
+    for (int k = 0; k < kOut; ++k) v[k] = dt[k * kRows + t];
 #pragma unroll
-        for (int k = 0; k < kOut; ++k) m.f[k][c] = v[k];
-    }
+    for (int k = 0; k < kOut; ++k) m.f[k][c] = v[k];
 }
 
 // ---- training kernels ------------------------------------------------------
@@ -1049,7 +1045,7 @@ cudaError_t launch_strip(const Model &m, int w, const int4 *tiles, int ntiles, f
     float *delta = reinterpret_cast<float *>(reinterpret_cast<unsigned char *>(buf) + kImgPad);
     k_strip_tc<false><<<tc_grid(ntiles), kTcThreads, kTcSmem, s>>>(m, w, tiles, ntiles, img, delta, nullptr, 0, nullptr,
                                                             strip_error_flag(buf, ntiles));
-    k_strip_apply<<<std::min((ntiles + 1) / 2, 8 * tc_grid(1 << 30)), 2 * kRows, 0, s>>>(m, tiles, ntiles, delta);
+    k_strip_apply<<<ntiles, kRows, 0, s>>>(m, tiles, delta);
     return cudaGetLastError();
 }
 
