@@ -119,3 +119,39 @@ def test_batch_mixes_storage_audit_and_families():
     finally:
         for m in members:
             m.close()
+
+
+def test_batch_with_learned_strips():
+    """Two models with a learned absorbing strip (pml = 0, the network on the
+    tensor cores) and one with a split-field PML in one batch: each ends bit
+    for bit where the same model run alone ends."""
+    rng = np.random.default_rng(12)
+    p = (rng.standard_normal(sgfd.MLP_PARAMS) * 0.05).astype(np.float32)
+    ws = [wl.small_random_case(nx=40, ny=44, nz=38, pml=0, nt=45, seed=11),
+          wl.small_random_case(nx=36, ny=39, nz=42, pml=0, nt=45, seed=12),
+          wl.small_random_case(nx=37, ny=41, nz=45, pml=6, nt=45, seed=7)]
+
+    def build(w):
+        s = make_solver(w)
+        if w.cfg["pml"] == 0:
+            s.set_learned_strip(6, p)
+        return s
+
+    solo, members = [], []
+    try:
+        for w in ws:
+            with build(w) as s:
+                s.run(0, w.nt)
+                solo.append((s.traces(), [s.field(k) for k in range(9)]))
+        members = [build(w) for w in ws]
+        assert members[0].launches_per_step() == members[2].launches_per_step() + 2
+        with sgfd.Batch(members) as b:
+            b.run(0, 45)
+            b.synchronize()
+        for m, (tr, fields) in zip(members, solo):
+            np.testing.assert_array_equal(m.traces(), tr)
+            for k in range(9):
+                np.testing.assert_array_equal(m.field(k), fields[k], err_msg=sgfd.FIELD_NAMES[k])
+    finally:
+        for m in members:
+            m.close()
