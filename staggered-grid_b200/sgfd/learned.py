@@ -18,7 +18,8 @@ Evaluation (`reflection`): the same interior and source run three ways — a
 split-field PML — and each reports the energy left in the interior once the
 direct wave has gone, relative to its peak (what the boundary reflected).
 
-    python -m sgfd.learned train --out strip_params.npy
+    python -m sgfd.learned train --out strip_params.npy          (200 runs, seeds 1000-1199)
+    python -m sgfd.learned evaluate --params strip_params.npy --steps 1500
 """
 from __future__ import annotations
 
@@ -88,7 +89,7 @@ def _cfg(n_grid: int, pml: int, dt: float, d: float, device: int):
 
 
 def generate(seeds, n_int: int = 32, nt: int = 220, first: int = 30, every: int = 3, per_snapshot: int = 4000,
-             dt: float = 0.001, d: float = 10.0, device: int = 0):
+             dt: float = 0.001, d: float = 10.0, device: int = 0, progress: bool = False):
     """Training rows (X [n][252], Y [n][9]) from one extended run per seed
     (seeds alternate random and layered media, Ricker f0 ~ U(15, 30) Hz at
     the centre)."""
@@ -140,6 +141,8 @@ def generate(seeds, n_int: int = 32, nt: int = 220, first: int = 30, every: int 
         finally:
             E.close()
             D.close()
+        if progress and (k + 1) % 20 == 0:
+            print(f"generated {k + 1} runs, {sum(len(x) for x in Xs)} rows", flush=True)
     return np.concatenate(Xs), np.concatenate(Ys)
 
 
@@ -205,21 +208,26 @@ def main(argv=None):
     sub = ap.add_subparsers(dest="cmd", required=True)
     t = sub.add_parser("train")
     t.add_argument("--out", default=PARAMS_PATH)
-    t.add_argument("--runs", type=int, default=12)
+    t.add_argument("--runs", type=int, default=200)
+    t.add_argument("--seed0", type=int, default=1000, help="first seed (seeds seed0 .. seed0+runs-1)")
+    t.add_argument("--per-snapshot", type=int, default=600, help="strip cells sampled per snapshot")
     t.add_argument("--epochs", type=int, default=30)
     t.add_argument("--device", type=int, default=0)
     e = sub.add_parser("evaluate")
     e.add_argument("--params", default=PARAMS_PATH)
+    e.add_argument("--steps", type=int, default=400)
     e.add_argument("--device", type=int, default=0)
     a = ap.parse_args(argv)
     if a.cmd == "train":
-        X, Y = generate(range(1, a.runs + 1), device=a.device)
+        X, Y = generate(range(a.seed0, a.seed0 + a.runs), per_snapshot=a.per_snapshot, device=a.device,
+                        progress=True)
         p, hist = train(X, Y, epochs=a.epochs, device=a.device)
         np.save(a.out, p)
-        print({"rows": len(X), "epoch_loss": [round(float(v), 6) for v in hist]})
-        print(reflection(p, device=a.device))
+        print({"rows": len(X), "epoch_loss": [round(float(v), 6) for v in hist]}, flush=True)
+        print(reflection(p, device=a.device), flush=True)
     else:
-        print(reflection(np.load(a.params), device=a.device))
+        r = reflection(np.load(a.params), nt=a.steps, sample_every=50 if a.steps > 400 else 20, device=a.device)
+        print({k: v["final_over_peak"] for k, v in r.items()}, flush=True)
 
 
 if __name__ == "__main__":
