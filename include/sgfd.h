@@ -313,6 +313,15 @@ int sgfd_set_learned_strip(sgfd_solver *h, int32_t width, const float *params);
  * cell) from the current state, with each cell's s and rho*vp (training data). */
 int sgfd_strip_features(sgfd_solver *h, int32_t width, int32_t n, const int32_t *cells, float *X, float *scale,
                         float *zimp);
+/* Training data for the strip (no counterpart in the reference).
+ * sgfd_copy_window: dst's 9 fields (its whole GRID) from the window of src
+ * whose GRID origin is (x0, y0, z0), with dst's 5-cell frame set to zero; both
+ * models FP32 on one device, dst with pml = 0; ordered after the work queued
+ * on both models' streams.  sgfd_sample_fields: the 9 fields of n cells
+ * (computed coordinates cx, cy, cz per cell) to out[i*9 + k]; waits for the
+ * queued steps. */
+int sgfd_copy_window(sgfd_solver *dst, sgfd_solver *src, int32_t x0, int32_t y0, int32_t z0);
+int sgfd_sample_fields(sgfd_solver *h, int32_t n, const int32_t *cells, float *out);
 /* The MLP on the GPU of `device`, host arrays in and out: parameter count,
  * forward pass of n input rows, loss (mean squared error over the 9 outputs)
  * and its gradient for n rows, and minibatch Adam training (lr, betas 0.9 and

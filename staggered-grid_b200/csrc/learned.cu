@@ -129,6 +129,30 @@ __global__ void k_strip_features(Model m, int w, const int4 *cells, int n, float
     zimp[i] = z;
 }
 
+// Training-data support.  dst's 9 fields (whole GRID) from the window of
+// src whose GRID origin is (x0, y0, z0), dst's 5-cell frame set to zero.
+__global__ void k_copy_window(Model dst, Model src, int x0, int y0, int z0) {
+    const int64_t n = (int64_t)dst.nx * dst.ny * dst.nz;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int x = (int)(i % dst.nx), y = (int)((i / dst.nx) % dst.ny), z = (int)(i / ((int64_t)dst.nx * dst.ny));
+        const bool frame = x < kHalo || y < kHalo || z < kHalo || x >= dst.nx - kHalo || y >= dst.ny - kHalo ||
+                           z >= dst.nz - kHalo;
+        const int64_t di = pidx(dst, x, y, z), si = pidx(src, x + x0, y + y0, z + z0);
+#pragma unroll
+        for (int k = 0; k < 9; ++k) dst.f[k][di] = frame ? 0.0f : src.f[k][si];
+    }
+}
+
+// The 9 fields of listed computed cells: out[i][k].
+__global__ void k_sample_fields(Model m, const int4 *cells, int n, float *out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int4 q = cells[i];
+    const int64_t c = pidx(m, q.x + kHalo, q.y + kHalo, q.z + kHalo);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) out[(int64_t)i * 9 + k] = m.f[k][c];
+}
+
 // ---- tensor-core inference --------------------------------------------------
 
 constexpr int kRows = 128;                 // cells per tile = MMA M
@@ -954,6 +978,64 @@ int sgfd_set_learned_strip(sgfd_solver *h, int32_t width, const float *params) {
     h->strip_w = width;
     h->strip_n = nt;
     return SGFD_OK;
+}
+
+int sgfd_copy_window(sgfd_solver *dst, sgfd_solver *src, int32_t x0, int32_t y0, int32_t z0) {
+    int r = check_handle(src);
+    if (r) return r;
+    r = check_handle(dst);
+    if (r) return r;
+    if (dst->device != src->device) return fail(dst, SGFD_ERR_INVALID, "the two models are on different devices");
+    if (dst->cfg.pml != 0) return fail(dst, SGFD_ERR_INVALID, "the destination model must have pml = 0");
+    if (dst->storage != SGFD_STORE_F32 || src->storage != SGFD_STORE_F32)
+        return fail(dst, SGFD_ERR_UNSUPPORTED, "window copies need FP32 storage");
+    const Model &d = dst->m, &s = src->m;
+    if (x0 < 0 || y0 < 0 || z0 < 0 || x0 + d.nx > s.nx || y0 + d.ny > s.ny || z0 + d.nz > s.nz)
+        return fail(dst, SGFD_ERR_INVALID, "window (%d,%d,%d)+(%d,%d,%d) outside the source grid", x0, y0, z0, d.nx,
+                    d.ny, d.nz);
+    // dst's stream waits for src's queued steps, src's for this copy
+    cudaEvent_t ev = nullptr;
+    SG_CUDA(dst, cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "window event");
+    cudaError_t e = cudaEventRecord(ev, src->stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(dst->stream, ev, 0);
+    if (e == cudaSuccess) {
+        k_copy_window<<<1184, 256, 0, dst->stream>>>(d, s, x0, y0, z0);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaEventRecord(ev, dst->stream);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(src->stream, ev, 0);
+    cudaEventDestroy(ev);
+    return e == cudaSuccess ? SGFD_OK : cuda_fail(dst, e, "window copy");
+}
+
+int sgfd_sample_fields(sgfd_solver *h, int32_t n, const int32_t *cells, float *out) {
+    int r = check_handle(h);
+    if (r) return r;
+    if (n < 0 || (n && (!cells || !out))) return fail(h, SGFD_ERR_INVALID, "bad sample arguments");
+    if (n == 0) return SGFD_OK;
+    const Model &m = h->m;
+    std::vector<int4> c(n);
+    for (int i = 0; i < n; ++i) {
+        c[i] = make_int4(cells[3 * i], cells[3 * i + 1], cells[3 * i + 2], 0);
+        if (c[i].x < 0 || c[i].y < 0 || c[i].z < 0 || c[i].x >= m.nxc || c[i].y >= m.nyc || c[i].z >= m.nzc)
+            return fail(h, SGFD_ERR_INVALID, "cell %d is outside the computed region", i);
+    }
+    r = sync_views(h);
+    if (r) return r;
+    int4 *dc = nullptr;
+    float *dout = nullptr;
+    SG_CUDA(h, cudaMalloc(&dc, (size_t)n * sizeof(int4)), "sample scratch");
+    cudaError_t e = cudaMalloc(&dout, (size_t)n * 9 * sizeof(float));
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dc, c.data(), (size_t)n * sizeof(int4), cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess) {
+        k_sample_fields<<<cdiv(n, 128), 128, 0, h->stream>>>(m, dc, n, dout);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, dout, (size_t)n * 9 * sizeof(float), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    cudaFree(dc);
+    cudaFree(dout);
+    return e == cudaSuccess ? SGFD_OK : cuda_fail(h, e, "field samples");
 }
 
 int sgfd_strip_features(sgfd_solver *h, int32_t width, int32_t n, const int32_t *cells, float *X, float *scale,

@@ -135,6 +135,8 @@ def lib() -> ctypes.CDLL:
                                                 ctypes.POINTER(ctypes.c_double)]),
         "sgfd_set_learned_strip": (ctypes.c_int, [vp, i32, fp]),
         "sgfd_strip_features": (ctypes.c_int, [vp, i32, i32, ip, fp, fp, fp]),
+        "sgfd_copy_window": (ctypes.c_int, [vp, vp, i32, i32, i32]),
+        "sgfd_sample_fields": (ctypes.c_int, [vp, i32, ip, fp]),
         "sgfd_mlp_param_count": (ctypes.c_int, []),
         "sgfd_mlp_forward": (ctypes.c_int, [i32, fp, fp, ctypes.c_int64, fp]),
         "sgfd_mlp_infer": (ctypes.c_int, [i32, fp, fp, ctypes.c_int64, fp]),
@@ -331,6 +333,19 @@ class Solver:
         """Make the outer `width` computed cells a learned absorbing strip (pml = 0 models)."""
         p = None if params is None else np.ascontiguousarray(params, dtype=np.float32)
         self._check(lib().sgfd_set_learned_strip(self.h, width, _fptr(p) if p is not None else None))
+
+    def copy_window_from(self, src: "Solver", x0: int, y0: int, z0: int):
+        """This model's 9 fields from the window of src at GRID origin (x0, y0, z0),
+        frame zeroed (this model: pml = 0)."""
+        self._check(lib().sgfd_copy_window(self.h, src.h, x0, y0, z0))
+
+    def sample_fields(self, cells) -> np.ndarray:
+        """The 9 fields [n][9] of the listed cells (computed coordinates)."""
+        c = np.ascontiguousarray(np.asarray(cells, dtype=np.int32).reshape(-1, 3))
+        out = np.zeros((len(c), 9), np.float32)
+        self._check(lib().sgfd_sample_fields(self.h, len(c), c.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+                                             _fptr(out)))
+        return out
 
     def strip_features(self, width: int, cells):
         """(X [n][252], s [n], rho*vp [n]) of the listed strip cells (computed coordinates)."""

@@ -115,22 +115,17 @@ def generate(seeds, n_int: int = 32, nt: int = 220, first: int = 30, every: int 
             while it < nt:
                 E.step(it, float(wav[it]))
                 if it >= first and (it - first) % every == 0 and it + 1 < nt:
-                    for f in range(9):
-                        a = np.array(E.field(f)[win, win, win])
-                        a[:HALO], a[-HALO:] = 0.0, 0.0          # the strip model's frame stays zero
-                        a[:, :HALO], a[:, -HALO:] = 0.0, 0.0
-                        a[:, :, :HALO], a[:, :, -HALO:] = 0.0, 0.0
-                        D.set_field(f, a)
+                    # the strip model takes the wide run's state on its window (frame zero)
+                    D.copy_window_from(E, EXT_PML, EXT_PML, EXT_PML)
                     D.step(it + 1, 0.0)                       # one plain step of the strip model
-                    tilde = [D.field(f) for f in range(9)]
-                    E.step(it + 1, float(wav[it + 1]))
-                    true = [E.field(f)[win, win, win] for f in range(9)]
                     pick = cells_all[rng.choice(len(cells_all), min(per_snapshot, len(cells_all)), replace=False)]
+                    tilde = D.sample_fields(pick)
+                    E.step(it + 1, float(wav[it + 1]))
+                    true = E.sample_fields(pick + EXT_PML)    # the same cells in the wide run
                     X, s, z = D.strip_features(WIDTH, pick)
                     keep = s > 0
                     if keep.any():
-                        gx, gy, gz = (pick[keep] + HALO).T
-                        y = np.stack([(true[f][gz, gy, gx] - tilde[f][gz, gy, gx]) for f in range(9)], axis=1)
+                        y = true[keep] - tilde[keep]
                         y[:, :3] *= z[keep, None]
                         y /= s[keep, None]
                         Xs.append(X[keep])

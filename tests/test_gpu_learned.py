@@ -230,3 +230,33 @@ def test_energy_audit_regions_follow_the_strip():
     ks, es = s.energy(sgfd.REGION_PML)
     np.testing.assert_allclose(kt + et, k + e + ks + es, rtol=1e-12)
     s.close()
+
+
+def test_window_copy_and_field_samples():
+    """Training-data support: sgfd_copy_window equals the host path (the
+    window of the wide model's fields with the frame zeroed, uploaded with
+    sgfd_set_field), and sgfd_sample_fields equals indexing the downloaded
+    fields; models with a PML and windows outside the source are rejected."""
+    big = wl.small_random_case(nx=40, ny=42, nz=44, pml=8, nt=30, seed=3)
+    with make_solver(big) as E:
+        E.run(0, 20)
+        n = 24
+        cfg = sgfd.default_config(**{**big.cfg, "nx": n, "ny": n, "nz": n, "pml": 0})
+        with sgfd.Solver(cfg) as D:
+            win = (slice(9, 9 + n), slice(7, 7 + n), slice(8, 8 + n))     # GRID z, y, x
+            D.set_medium(*(np.ascontiguousarray(a[win]) for a in (big.b, big.lam, big.mu)))
+            D.copy_window_from(E, 8, 7, 9)
+            for k in range(9):
+                want = np.array(E.field(k)[win])
+                want[:5], want[-5:], want[:, :5], want[:, -5:], want[:, :, :5], want[:, :, -5:] = 0, 0, 0, 0, 0, 0
+                np.testing.assert_array_equal(D.field(k), want)
+            rng = np.random.default_rng(4)
+            cells = rng.integers(0, n - 10, (50, 3)).astype(np.int32)
+            got = D.sample_fields(cells)
+            for k in range(9):
+                f = D.field(k)
+                np.testing.assert_array_equal(got[:, k], f[cells[:, 2] + 5, cells[:, 1] + 5, cells[:, 0] + 5])
+            with pytest.raises(sgfd.SgfdError):
+                D.copy_window_from(E, 20, 0, 0)                            # past the source's x extent
+            with pytest.raises(sgfd.SgfdError):
+                E.copy_window_from(D, 0, 0, 0)                             # destination with a PML
