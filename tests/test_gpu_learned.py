@@ -9,6 +9,7 @@ import os
 import numpy as np
 import pytest
 
+from helpers import make_solver
 import mlp_oracle as mo
 import sgfd
 import sgfd.learned as L
