@@ -35,6 +35,10 @@ from . import workloads as wl
 WIDTH = 6          # strip cells per face
 EXT_PML = 40       # PML of the extended (ground-truth) runs
 PARAMS_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "strip_params.npy")
+# the same network trained on 200 runs (seeds 1000-1199, 600 strip cells per
+# snapshot, 7.3 M rows); it leaves more energy in the interior late in a run
+# than the default parameters (12 runs, seeds 1-12, 4000 cells per snapshot)
+PARAMS_200_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "strip_params_200runs.npy")
 HALO = wl.HALO
 
 
@@ -50,8 +54,8 @@ def init_params(seed: int = 0) -> np.ndarray:
     return p.astype(np.float32)
 
 
-def load_params() -> np.ndarray:
-    return np.load(PARAMS_PATH).astype(np.float32)
+def load_params(path: str = PARAMS_PATH) -> np.ndarray:
+    return np.load(path).astype(np.float32)
 
 
 def strip_cells(nc: int, w: int = WIDTH) -> np.ndarray:

@@ -201,13 +201,15 @@ def test_fused_strip_correction_is_the_network_output():
     strip.close()
 
 
-@pytest.mark.skipif(not os.path.exists(L.PARAMS_PATH), reason="no trained strip parameters in the package")
-def test_trained_strip_reflects_less_than_the_bare_strip():
+@pytest.mark.parametrize("path", [L.PARAMS_PATH, L.PARAMS_200_PATH], ids=["12_runs", "200_runs"])
+def test_trained_strip_reflects_less_than_the_bare_strip(path):
     """Held-out medium: energy left in the interior after the direct wave has
     gone, relative to its peak, with the trained 6-cell strip, the same strip
     without the network, and a 20-cell split-field PML."""
+    if not os.path.exists(path):
+        pytest.skip("no trained strip parameters in the package")
     for nt in (400, 1500):
-        r = L.reflection(L.load_params(), seed=999, nt=nt, sample_every=50)
+        r = L.reflection(L.load_params(path), seed=999, nt=nt, sample_every=50)
         learned, bare, pml = (r[k]["final_over_peak"] for k in ("learned_strip", "bare_strip", "pml20"))
         print(f"{nt} steps, reflected energy / peak: learned strip {learned:.3e}, bare strip {bare:.3e}, "
               f"20-cell PML {pml:.3e}")
