@@ -93,10 +93,14 @@ def _cfg(n_grid: int, pml: int, dt: float, d: float, device: int):
 
 
 def generate(seeds, n_int: int = 32, nt: int = 220, first: int = 30, every: int = 3, per_snapshot: int = 4000,
-             dt: float = 0.001, d: float = 10.0, device: int = 0, progress: bool = False):
+             dt: float = 0.001, d: float = 10.0, device: int = 0, progress: bool = False, rollout=(0,),
+             policy=None):
     """Training rows (X [n][252], Y [n][9]) from one extended run per seed
     (seeds alternate random and layered media, Ricker f0 ~ U(15, 30) Hz at
-    the centre)."""
+    the centre).  With rollout lengths other than 0 and a policy network,
+    each snapshot first lets the strip model run r steps (r drawn from
+    `rollout`) with that network's corrections next to the wide run, so that
+    the rows also cover the states a learned strip drifts into."""
     nd = n_int + 2 * WIDTH + 2 * HALO            # strip model GRID
     ne = nd + 2 * EXT_PML                        # extended model GRID
     win = slice(EXT_PML, EXT_PML + nd)
@@ -119,8 +123,17 @@ def generate(seeds, n_int: int = 32, nt: int = 220, first: int = 30, every: int 
             while it < nt:
                 E.step(it, float(wav[it]))
                 if it >= first and (it - first) % every == 0 and it + 1 < nt:
+                    r = int(rng.choice(rollout)) if policy is not None and len(rollout) > 1 else 0
+                    r = min(r, nt - it - 2)
                     # the strip model takes the wide run's state on its window (frame zero)
                     D.copy_window_from(E, EXT_PML, EXT_PML, EXT_PML)
+                    if r > 0:                                 # r steps with the policy's corrections
+                        D.set_learned_strip(WIDTH, policy)
+                        for j in range(1, r + 1):
+                            D.step(it + j, 0.0)
+                            E.step(it + j, float(wav[it + j]))
+                        D.set_learned_strip(0)
+                        it += r
                     D.step(it + 1, 0.0)                       # one plain step of the strip model
                     pick = cells_all[rng.choice(len(cells_all), min(per_snapshot, len(cells_all)), replace=False)]
                     tilde = D.sample_fields(pick)
@@ -211,6 +224,9 @@ def main(argv=None):
     t.add_argument("--seed0", type=int, default=1000, help="first seed (seeds seed0 .. seed0+runs-1)")
     t.add_argument("--per-snapshot", type=int, default=600, help="strip cells sampled per snapshot")
     t.add_argument("--epochs", type=int, default=30)
+    t.add_argument("--nt", type=int, default=220, help="steps of each wide run")
+    t.add_argument("--rollout", default="0", help="comma-separated rollout lengths drawn per snapshot")
+    t.add_argument("--policy", default=PARAMS_PATH, help="network that runs the rollouts")
     t.add_argument("--device", type=int, default=0)
     e = sub.add_parser("evaluate")
     e.add_argument("--params", default=PARAMS_PATH)
@@ -218,12 +234,17 @@ def main(argv=None):
     e.add_argument("--device", type=int, default=0)
     a = ap.parse_args(argv)
     if a.cmd == "train":
-        X, Y = generate(range(a.seed0, a.seed0 + a.runs), per_snapshot=a.per_snapshot, device=a.device,
-                        progress=True)
+        roll = tuple(int(v) for v in a.rollout.split(","))
+        X, Y = generate(range(a.seed0, a.seed0 + a.runs), nt=a.nt, per_snapshot=a.per_snapshot, device=a.device,
+                        progress=True, rollout=roll, policy=load_params(a.policy) if max(roll) > 0 else None)
         p, hist = train(X, Y, epochs=a.epochs, device=a.device)
         np.save(a.out, p)
         print({"rows": len(X), "epoch_loss": [round(float(v), 6) for v in hist]}, flush=True)
-        print(reflection(p, device=a.device), flush=True)
+        for n in (400, 1500):
+            r = reflection(p, nt=n, sample_every=50, device=a.device)
+            hist_l = r["learned_strip"]["history"]
+            print(n, {k: v["final_over_peak"] for k, v in r.items()},
+                  "second-half growth", hist_l[-1] / hist_l[len(hist_l) // 2], flush=True)
     else:
         r = reflection(np.load(a.params), nt=a.steps, sample_every=50 if a.steps > 400 else 20, device=a.device)
         print({k: v["final_over_peak"] for k, v in r.items()}, flush=True)
