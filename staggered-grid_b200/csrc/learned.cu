@@ -45,6 +45,7 @@
 #include <cuda_fp16.h>
 
 #include "solver.h"
+#include "strip_tiles.h"
 
 using namespace sgfd;
 
@@ -155,10 +156,10 @@ __global__ void k_sample_fields(Model m, const int4 *cells, int n, float *out) {
 
 // ---- tensor-core inference --------------------------------------------------
 
-constexpr int kRows = 128;                 // cells per tile = MMA M
+constexpr int kRows = kStripRows;          // cells per tile = MMA M
 constexpr int kK1 = 256;                   // layer-1 K: the 252 inputs and 4 zeros
 constexpr int kN3 = 16;                    // layer-3 N: the 9 outputs and 7 zeros
-constexpr int kStage = 544;                // staged cells per box, (32+2)(2+2)(2+2) at most
+constexpr int kStage = kStripStage;        // staged cells per box, (32+2)(2+2)(2+2) at most
 // Weight image (bytes): W1, W2, W3 transposed to N x K, FP16, in the K-major
 // core-matrix order of kmaj, then the biases b1, b2, b3 (b3 padded to 16) in FP32.
 constexpr int kImgW1 = 0, kImgW2 = kImgW1 + kH * kK1 * 2, kImgW3 = kImgW2 + kH * kH * 2,
@@ -1080,35 +1081,8 @@ int sgfd_strip_features(sgfd_solver *h, int32_t width, int32_t n, const int32_t 
 
 namespace sgfd {
 
-// Boxes of at most 128 strip cells covering the strip once: the two z faces
-// and the two y faces (between the z faces) in 32 x 2 x 2 boxes, the two x
-// faces (between the others) in min(w, 32) x ey x ez (6 x 4 x 5 for w = 6).  Each tile is
-// (x, y, z, ex | ey << 8 | ez << 16) in computed coordinates; -1 if a box
-// would not fit the staging area.
-int strip_tile_list(const Model &m, int w, std::vector<int4> &tiles) {
-    tiles.clear();
-    bool fits = true;
-    auto boxes = [&](int x0, int x1, int y0, int y1, int z0, int z1, int ex, int ey, int ez) {
-        fits = fits && ex * ey * ez <= kRows && (ex + 2) * (ey + 2) * (ez + 2) <= kStage;
-        for (int z = z0; z < z1; z += ez)
-            for (int y = y0; y < y1; y += ey)
-                for (int x = x0; x < x1; x += ex)
-                    tiles.push_back(make_int4(x, y, z, std::min(ex, x1 - x) | std::min(ey, y1 - y) << 8 |
-                                                           std::min(ez, z1 - z) << 16));
-    };
-    const int X = m.nxc, Y = m.nyc, Z = m.nzc;
-    boxes(0, X, 0, Y, 0, w, 32, 2, 2);
-    boxes(0, X, 0, Y, Z - w, Z, 32, 2, 2);
-    boxes(0, X, 0, w, w, Z - w, 32, 2, 2);
-    boxes(0, X, Y - w, Y, w, Z - w, 32, 2, 2);
-    const int ex = std::min(w, 32), rest = kRows / ex;
-    int ey = 1;
-    while (4 * ey * ey <= rest) ey *= 2;        // largest power of two with ey^2 <= rest
-    const int ez = rest / ey;
-    boxes(0, w, w, Y - w, w, Z - w, ex, ey, ez);
-    boxes(X - w, X, w, Y - w, w, Z - w, ex, ey, ez);
-    return fits ? (int)tiles.size() : -1;
-}
+// The strip's tiles (strip_tiles.h) for model m.
+int strip_tile_list(const Model &m, int w, std::vector<int4> &tiles) { return strip_tiles(m.nxc, m.nyc, m.nzc, w, tiles); }
 
 // Strip buffer: weight image, corrected fields [tile][9][128], error flag.
 size_t strip_buffer_bytes(int ntiles) { return (size_t)kImgPad + (size_t)ntiles * kRows * kOut * 4 + 16; }

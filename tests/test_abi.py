@@ -120,3 +120,56 @@ int main() {
     assert r.returncode == 0, r.stderr
     r = subprocess.run([str(exe)], capture_output=True, text=True)
     assert r.returncode == 0 and r.stdout.strip() == "ok", r.stdout
+
+
+def test_strip_tiles_cover_the_strip_once(tmp_path):
+    """Host-compiles csrc/strip_tiles.h and checks the learned strip's tiling
+    for uneven sizes and widths: every strip cell in exactly one tile, no
+    interior cell in any, every box within 128 cells and its one-cell halo
+    within the 544 staged cells; and the staging index split of k_strip_tc
+    (quotients through a float reciprocal) equal to integer division for every
+    staged cell of every box."""
+    src = tmp_path / "t.cpp"
+    src.write_text(r'''
+#include "strip_tiles.h"
+#include <cstdio>
+#include <vector>
+using namespace sgfd;
+int main() {
+  const int cases[][4] = {{20,20,20,6},{268,268,268,6},{58,47,63,6},{30,31,29,1},{40,40,40,3},
+                          {100,90,80,33},{21,22,23,10},{70,70,70,2},{90,91,92,16},{200,150,120,12}};
+  for (auto &c : cases) {
+    const int X = c[0], Y = c[1], Z = c[2], w = c[3];
+    std::vector<int4> t;
+    if (strip_tiles(X, Y, Z, w, t) != (int)t.size()) { std::printf("does not fit\n"); return 1; }
+    std::vector<int> hit((size_t)X * Y * Z, 0);
+    for (auto &q : t) {
+      const int ex = q.w & 255, ey = (q.w >> 8) & 255, ez = (q.w >> 16) & 255;
+      if (ex < 1 || ey < 1 || ez < 1 || ex * ey * ez > kStripRows) { std::printf("bad extents\n"); return 1; }
+      if ((ex + 2) * (ey + 2) * (ez + 2) > kStripStage) { std::printf("halo too large\n"); return 1; }
+      if (q.x < 0 || q.y < 0 || q.z < 0 || q.x + ex > X || q.y + ey > Y || q.z + ez > Z) { std::printf("outside\n"); return 1; }
+      for (int z = q.z; z < q.z + ez; ++z) for (int y = q.y; y < q.y + ey; ++y) for (int x = q.x; x < q.x + ex; ++x)
+        hit[((size_t)z * Y + y) * X + x]++;
+      const int sx = ex + 2, sxy = sx * (ey + 2), ns = sxy * (ez + 2);
+      const float inv_sx = 1.0f / (float)sx, inv_sxy = 1.0f / (float)sxy;
+      for (int r = 0; r < ns; ++r) {
+        const int lz = (int)(((float)r + 0.5f) * inv_sxy), rr = r - lz * sxy;
+        const int ly = (int)(((float)rr + 0.5f) * inv_sx), lx = rr - ly * sx;
+        if (lz != r / sxy || ly != (r % sxy) / sx || lx != r % sx) { std::printf("staging index\n"); return 1; }
+      }
+    }
+    for (int z = 0; z < Z; ++z) for (int y = 0; y < Y; ++y) for (int x = 0; x < X; ++x) {
+      const bool strip = x < w || y < w || z < w || x >= X - w || y >= Y - w || z >= Z - w;
+      if (hit[((size_t)z * Y + y) * X + x] != (strip ? 1 : 0)) { std::printf("cover\n"); return 1; }
+    }
+  }
+  std::puts("ok"); return 0;
+}
+''')
+    exe = tmp_path / "t"
+    inc = os.path.join(ROOT, "staggered-grid_b200", "csrc")
+    r = subprocess.run(["g++", "-std=c++17", "-O1", f"-I{inc}", "-I/usr/local/cuda/include", str(src), "-o", str(exe)],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    r = subprocess.run([str(exe)], capture_output=True, text=True)
+    assert r.returncode == 0 and r.stdout.strip() == "ok", r.stdout
