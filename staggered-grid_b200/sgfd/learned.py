@@ -4,11 +4,15 @@ training on the GPU, evaluation against the split-field PML.
 Training data (`generate`).  For each seeded medium an "extended" model runs
 with a wide 40-cell PML around the region of interest; a second, strip-sized
 model (pml = 0: it ends at the zero frame) takes, every few steps, the
-extended model's state on its window, advances one plain step, and is
-compared with the extended model's next state.  In the outer cells of the
-strip the plain step misses what lies beyond the frame; the difference, in
-the MLP's output units, is the target, and the MLP's inputs are the strip
-model's state after its step (`Solver.strip_features`).
+extended model's state on its window (`Solver.copy_window_from`, on the
+device), advances one plain step, and is compared with the extended model's
+next state at sampled strip cells (`Solver.sample_fields`).  In the outer
+cells of the strip the plain step misses what lies beyond the frame; the
+difference, in the MLP's output units, is the target, and the MLP's inputs
+are the strip model's state after its step (`Solver.strip_features`).
+Optionally (`rollout`, `policy`) the strip model first runs a few steps with
+a network's corrections, so that rows also come from the states a learned
+strip drifts into.
 
 Training (`train`): minibatch Adam on the GPU (`mlp_train`, hand-written
 forward/backward/Adam kernels).
