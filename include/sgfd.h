@@ -355,10 +355,12 @@ int sgfd_energy(sgfd_solver *h, int32_t region, double *kinetic, double *strain)
  * running (device memory held by another allocator such as PyTorch's caching
  * allocator, or a footprint fixed when the handles were created): the
  * partial sums go to a 32 KiB device array compiled into the library, at
- * most 2047 partial-sum blocks; nblocks = 0 uses sgfd_energy's launch shape,
- * a larger nblocks than 2047 is rejected (SGFD_ERR_INVALID).  The first call
- * on a device looks up that array's address; make it before any stream
- * capture.  All calls share the array: calls that overlap on one GPU race. */
+ * most 2047 partial-sum blocks; nblocks = 0 uses sgfd_energy's launch shape
+ * capped at 2047 blocks, a larger nblocks than 2047 is rejected
+ * (SGFD_ERR_INVALID).  The first call on a device looks up that array's
+ * address; make it before any stream capture (a call that finds a new CUDA
+ * context on the device, e.g. after cudaDeviceReset, looks it up again).
+ * All calls share the array: calls that overlap on one GPU race. */
 int sgfd_energy_noalloc(sgfd_solver *h, int32_t region, int32_t nblocks, double *kinetic, double *strain);
 
 /* Per-step FP64 energy audit.  With every > 0, after the stress update of
@@ -406,6 +408,11 @@ int sgfd_write_stations(sgfd_solver *h, const char *prefix, int32_t nsteps, int3
 
 /* Counts for roofline accounting: computed cells that are interior / PML. */
 int sgfd_cell_counts(const sgfd_solver *h, int64_t *n_interior, int64_t *n_pml);
+/* Device allocations (cudaMalloc calls) the handle has made since
+ * sgfd_create, counting those freed since; no counterpart in the reference.
+ * A caller that must not see the library allocate once it runs can check
+ * that this count stays put across its steady-state calls. */
+int sgfd_device_allocations(const sgfd_solver *h, int64_t *count);
 /* Number of kernel launches issued by one sgfd_step / one step of sgfd_run. */
 int sgfd_launches_per_step(const sgfd_solver *h);
 /* Number of kernel launches sgfd_run(h, *, nsteps, use_graph) issues. */

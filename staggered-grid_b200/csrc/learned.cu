@@ -962,12 +962,12 @@ int sgfd_set_learned_strip(sgfd_solver *h, int32_t width, const float *params) {
     const int nt = strip_tile_list(m, width, tiles);
     if (nt <= 0) return fail(h, SGFD_ERR_INVALID, "strip width %d: no strip tiling", width);
     SG_CUDA(h, strip_prepare(), "strip kernel set-up");
-    SG_CUDA(h, cudaMalloc(&h->strip_cells, (size_t)nt * sizeof(int4)), "strip tiles");
-    SG_CUDA(h, cudaMalloc(&h->strip_buf, strip_buffer_bytes(nt)), "strip buffers");
+    SG_CUDA(h, dev_malloc(h, &h->strip_cells, (size_t)nt * sizeof(int4)), "strip tiles");
+    SG_CUDA(h, dev_malloc(h, &h->strip_buf, strip_buffer_bytes(nt)), "strip buffers");
     SG_CUDA(h, cudaMemcpy(h->strip_cells, tiles.data(), (size_t)nt * sizeof(int4), cudaMemcpyHostToDevice), "strip tiles");
     SG_CUDA(h, cudaMemset(h->strip_buf, 0, strip_buffer_bytes(nt)), "strip buffers");
     float *dp = nullptr;
-    SG_CUDA(h, cudaMalloc(&dp, (size_t)kParams * sizeof(float)), "strip parameters");
+    SG_CUDA(h, dev_malloc(h, &dp, (size_t)kParams * sizeof(float)), "strip parameters");
     cudaError_t e = cudaMemcpy(dp, params, (size_t)kParams * sizeof(float), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) {
         k_weight_image<<<64, 256>>>(dp, reinterpret_cast<unsigned char *>(h->strip_buf));
@@ -1025,8 +1025,8 @@ int sgfd_sample_fields(sgfd_solver *h, int32_t n, const int32_t *cells, float *o
     if (r) return r;
     int4 *dc = nullptr;
     float *dout = nullptr;
-    SG_CUDA(h, cudaMalloc(&dc, (size_t)n * sizeof(int4)), "sample scratch");
-    cudaError_t e = cudaMalloc(&dout, (size_t)n * 9 * sizeof(float));
+    SG_CUDA(h, dev_malloc(h, &dc, (size_t)n * sizeof(int4)), "sample scratch");
+    cudaError_t e = dev_malloc(h, &dout, (size_t)n * 9 * sizeof(float));
     if (e == cudaSuccess) e = cudaMemcpyAsync(dc, c.data(), (size_t)n * sizeof(int4), cudaMemcpyHostToDevice, h->stream);
     if (e == cudaSuccess) {
         k_sample_fields<<<cdiv(n, 128), 128, 0, h->stream>>>(m, dc, n, dout);
@@ -1057,8 +1057,8 @@ int sgfd_strip_features(sgfd_solver *h, int32_t width, int32_t n, const int32_t 
     if (r) return r;
     int4 *dc = nullptr;
     float *dX = nullptr;
-    SG_CUDA(h, cudaMalloc(&dc, (size_t)n * sizeof(int4)), "feature scratch");
-    cudaError_t e = cudaMalloc(&dX, (size_t)n * (kIn + 2) * sizeof(float));
+    SG_CUDA(h, dev_malloc(h, &dc, (size_t)n * sizeof(int4)), "feature scratch");
+    cudaError_t e = dev_malloc(h, &dX, (size_t)n * (kIn + 2) * sizeof(float));
     if (e == cudaSuccess) e = cudaMemcpyAsync(dc, c.data(), (size_t)n * sizeof(int4), cudaMemcpyHostToDevice, h->stream);
     if (e == cudaSuccess) {
         k_strip_features<<<cdiv(n, 128), 128, 0, h->stream>>>(m, width, dc, n, dX, dX + (size_t)n * kIn,

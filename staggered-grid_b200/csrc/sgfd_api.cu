@@ -129,7 +129,7 @@ int ensure_audit_scratch(sgfd_solver *h) {
     int sms = 0;
     SG_CUDA(h, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h->device), "SM count");
     h->audit_blocks = energy_blocks(sms);
-    SG_CUDA(h, cudaMalloc(&h->audit, (size_t)(2 * h->audit_blocks + 2) * sizeof(double)), "audit scratch");
+    SG_CUDA(h, dev_malloc(h, &h->audit, (size_t)(2 * h->audit_blocks + 2) * sizeof(double)), "audit scratch");
     return SGFD_OK;
 }
 
@@ -212,7 +212,7 @@ int capture_graph(sgfd_solver *h) {
     if (!h->cap_stream)
         SG_CUDA(h, cudaStreamCreateWithFlags(&h->cap_stream, cudaStreamNonBlocking), "capture stream");
     if (!h->step_ctr) {
-        SG_CUDA(h, cudaMalloc(&h->step_ctr, sizeof(int)), "step counter");
+        SG_CUDA(h, dev_malloc(h, &h->step_ctr, sizeof(int)), "step counter");
         SG_CUDA(h, cudaMemset(h->step_ctr, 0, sizeof(int)), "step counter");
     }
     SourceRec sr = h->sr;
@@ -295,9 +295,9 @@ int upload_zrec(sgfd_solver *h, const std::vector<int4> &rec) {
     cudaFree(h->zrec_off); cudaFree(h->zrec_list); cudaFree(h->zrec_idx);
     h->zrec_off = nullptr; h->zrec_list = nullptr; h->zrec_idx = nullptr;
     const size_t nl = std::max<size_t>(list.size(), 1);
-    cudaError_t e = cudaMalloc(&h->zrec_off, off.size() * sizeof(int));
-    if (e == cudaSuccess) e = cudaMalloc(&h->zrec_list, nl * sizeof(int4));
-    if (e == cudaSuccess) e = cudaMalloc(&h->zrec_idx, nl * sizeof(int));
+    cudaError_t e = dev_malloc(h, &h->zrec_off, off.size() * sizeof(int));
+    if (e == cudaSuccess) e = dev_malloc(h, &h->zrec_list, nl * sizeof(int4));
+    if (e == cudaSuccess) e = dev_malloc(h, &h->zrec_idx, nl * sizeof(int));
     if (e != cudaSuccess) { cudaGetLastError(); return fail(h, SGFD_ERR_ALLOC, "receiver lists"); }
     SG_CUDA(h, cudaMemcpy(h->zrec_off, off.data(), off.size() * sizeof(int), cudaMemcpyHostToDevice), "receiver lists");
     if (!list.empty()) {
@@ -401,8 +401,8 @@ int sgfd_create(const sgfd_config *cfg, sgfd_solver **out) {
     m.npml = pml_count(m.nxc, m.nyc, m.nzc, m.pml);
     const size_t arr_bytes = array_bytes(m);
     const size_t pool_bytes = arr_bytes * 16;
-    e = cudaMalloc(&h->field_pool, pool_bytes);
-    if (e == cudaSuccess) e = cudaMalloc(&h->split, (size_t)kNumSplit * m.npml * sizeof(float));
+    e = dev_malloc(h, &h->field_pool, pool_bytes);
+    if (e == cudaSuccess) e = dev_malloc(h, &h->split, (size_t)kNumSplit * m.npml * sizeof(float));
     if (e != cudaSuccess) {
         cudaGetLastError();
         int r = fail(nullptr, SGFD_ERR_ALLOC, "device allocation of %.2f GB failed",
@@ -438,8 +438,8 @@ int sgfd_create(const sgfd_config *cfg, sgfd_solver **out) {
         h->storage = c.storage;
         const size_t a16 = round_up((size_t)m.plane * m.nz * 2, 256);
         const size_t s16 = round_up((size_t)kNumSplit * m.npml * 2, 256);
-        e = cudaMalloc(&h->h16_pool, a16 * 9 + s16);
-        if (e == cudaSuccess) e = cudaMalloc(&h->hstate, 64 * sizeof(int));
+        e = dev_malloc(h, &h->h16_pool, a16 * 9 + s16);
+        if (e == cudaSuccess) e = dev_malloc(h, &h->hstate, 64 * sizeof(int));
         if (e == cudaSuccess) e = cudaMemsetAsync(h->h16_pool, 0, a16 * 9 + s16, h->stream);
         if (e != cudaSuccess) {
             cudaGetLastError();
@@ -464,7 +464,7 @@ int sgfd_create(const sgfd_config *cfg, sgfd_solver **out) {
     if (c.kernel != SGFD_KERNEL_SIMPLE && c.storage == SGFD_STORE_F32 && zmarch_supported(m)) {
         h->zg.cells = 1;
         e = zmarch_prepare(m, h->zg.cells, &h->vm, &h->sm);
-        if (e == cudaSuccess) e = cudaMalloc(&h->dev_err, sizeof(int));
+        if (e == cudaSuccess) e = dev_malloc(h, &h->dev_err, sizeof(int));
         if (e == cudaSuccess) e = cudaMemset(h->dev_err, 0, sizeof(int));
         if (e != cudaSuccess) {
             int r = cuda_fail(nullptr, e, "z-march set-up");
@@ -595,8 +595,8 @@ int sgfd_set_receivers(sgfd_solver *h, int32_t n, const int32_t *xyz, const int3
     h->sr.nt = 0;
     if (n > 0) {
         const size_t tbytes = (size_t)n * nt * sizeof(float);
-        cudaError_t e = cudaMalloc(&h->rec, n * sizeof(int4));
-        if (e == cudaSuccess) e = cudaMalloc(&h->traces, tbytes);
+        cudaError_t e = dev_malloc(h, &h->rec, n * sizeof(int4));
+        if (e == cudaSuccess) e = dev_malloc(h, &h->traces, tbytes);
         if (e != cudaSuccess) {
             cudaGetLastError();
             return fail(h, SGFD_ERR_ALLOC, "receiver buffers (%zu bytes)", tbytes);
@@ -621,7 +621,7 @@ int sgfd_set_wavelet(sgfd_solver *h, int32_t nt, const float *values) {
     if (nt > h->wavelet_nt) {
         cudaFree(h->wavelet);
         h->wavelet = nullptr;
-        cudaError_t e = cudaMalloc(&h->wavelet, (size_t)nt * sizeof(float));
+        cudaError_t e = dev_malloc(h, &h->wavelet, (size_t)nt * sizeof(float));
         if (e != cudaSuccess) {
             cudaGetLastError();
             h->wavelet_nt = 0;
@@ -913,7 +913,7 @@ int sgfd_set_audit(sgfd_solver *h, int32_t every, int32_t region, int32_t nsampl
         cudaFree(h->audit_hist);
         h->audit_hist = nullptr;
         h->audit_count = 0;
-        SG_CUDA(h, cudaMalloc(&h->audit_hist, (size_t)nsamples * 2 * sizeof(double)), "audit history");
+        SG_CUDA(h, dev_malloc(h, &h->audit_hist, (size_t)nsamples * 2 * sizeof(double)), "audit history");
         h->audit_count = nsamples;
     }
     SG_CUDA(h, cudaMemsetAsync(h->audit_hist, 0, (size_t)nsamples * 2 * sizeof(double), h->stream), "audit history");
@@ -956,6 +956,12 @@ int sgfd_cell_counts(const sgfd_solver *h, int64_t *n_interior, int64_t *n_pml) 
     const int64_t total = (int64_t)m.nxc * m.nyc * m.nzc;
     if (n_pml) *n_pml = m.npml;
     if (n_interior) *n_interior = total - m.npml;
+    return SGFD_OK;
+}
+
+int sgfd_device_allocations(const sgfd_solver *h, int64_t *count) {
+    if (!h || !count) return SGFD_ERR_INVALID;
+    *count = h->dev_allocs;
     return SGFD_OK;
 }
 

@@ -80,6 +80,8 @@ struct sgfd_solver {
     // per-step audit (sgfd_set_audit): sample k = energy after step k*every
     int audit_every = 0, audit_region = 0, audit_count = 0;
     double *audit_hist = nullptr;
+    // device allocations this handle has made since sgfd_create (dev_malloc)
+    int64_t dev_allocs = 0;
     std::string err;
 };
 
@@ -120,6 +122,14 @@ int *strip_error_flag(float *buf, int ntiles);
 cudaError_t strip_prepare();
 cudaError_t launch_strip(const Model &m, int w, const int4 *tiles, int ntiles, float *buf, cudaStream_t s);
 int mlp_params();
+
+// cudaMalloc on behalf of handle h, counted in h->dev_allocs.
+template <class T>
+inline cudaError_t dev_malloc(sgfd_solver *h, T **p, size_t bytes) {
+    const cudaError_t e = cudaMalloc(reinterpret_cast<void **>(p), bytes);
+    if (e == cudaSuccess) ++h->dev_allocs;
+    return e;
+}
 
 inline size_t round_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 

@@ -111,6 +111,7 @@ def lib() -> ctypes.CDLL:
         "sgfd_set_tiling": (ctypes.c_int, [vp, i32, i32]),
         "sgfd_cell_counts": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)]),
         "sgfd_launches_per_step": (ctypes.c_int, [vp]),
+        "sgfd_device_allocations": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_int64)]),
         "sgfd_run_launches": (ctypes.c_int, [vp, ctypes.c_int32, ctypes.c_int32]),
         "sgfd_prepare_run": (ctypes.c_int, [vp]),
         "sgfd_kernel_name": (ctypes.c_char_p, [vp]),
@@ -319,6 +320,12 @@ class Solver:
         a, b = ctypes.c_int64(), ctypes.c_int64()
         self._check(lib().sgfd_cell_counts(self.h, ctypes.byref(a), ctypes.byref(b)))
         return a.value, b.value
+
+    def device_allocations(self) -> int:
+        """Device allocations the handle has made since it was created."""
+        n = ctypes.c_int64()
+        self._check(lib().sgfd_device_allocations(self.h, ctypes.byref(n)))
+        return n.value
 
     def launches_per_step(self) -> int:
         return lib().sgfd_launches_per_step(self.h)

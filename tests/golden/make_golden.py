@@ -8,6 +8,7 @@ main.cu:11-56.  The reference tree is not available where GPU tests run, so a
 verbatim copy is kept here with its SHA-256.
 
 Usage: python tests/golden/make_golden.py [/path/to/reference]
+(default: $SGFD_REFERENCE_DIR, else /root/reference)
 """
 import hashlib
 import os
@@ -20,7 +21,7 @@ DST = os.path.join(HERE, "stationData_reference_main.txt")
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("SGFD_REFERENCE_DIR", "/root/reference")
     shutil.copyfile(os.path.join(ref, SRC), DST)
     digest = hashlib.sha256(open(DST, "rb").read()).hexdigest()
     with open(DST + ".sha256", "w") as f:

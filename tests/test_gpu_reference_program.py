@@ -98,6 +98,43 @@ def test_reference_main_runs_on_the_dropin_class(tmp_path, golden_trace):
             assert path.exists(), path
             vals = np.loadtxt(path)
             assert vals.shape == (lines,)
-    # the XOY slice through the source equals the field the library holds at that step
-    s1400 = np.loadtxt(tmp_path / "snapshotSliceXX_XOY_1400.txt").reshape(ny, nx)
-    assert np.abs(s1400).max() > 0
+    # slice values: the oracle's txx after steps 500 and 1400, cut along the
+    # planes and in the orders of snapShootSlice (OPT/ElasticWaveEquation.cu:
+    # 843-909) and printed as the reference prints them (ostream, 6
+    # significant digits), equals the files line for line
+    w = wl.reference_case(nt=1500)
+    o = oracle_py.Oracle(w.cfg)
+    o.set_medium(w.b, w.lam, w.mu)
+    o.set_source(*w.src)
+    o.set_receivers(w.rec_xyz, w.rec_comp, w.nt)
+    wav = w.wavelet.astype(np.float64)
+    done = 0
+    for it in (500, 1400):
+        o.run(wav, done, it + 1 - done)
+        done = it + 1
+        txx = o.field(sgfd.TXX).astype(np.float32)
+        for stem, want in _slices(txx, w.src, w.cfg["pml"]).items():
+            got = (tmp_path / f"{stem}_{it}.txt").read_text().split()
+            assert got == [_ostream(v) for v in want.reshape(-1)], (stem, it)
+        assert np.abs(txx).max() > 0
+    o.close()
+
+
+def _slices(txx, src, pml):
+    """The six txx slices of the reference's snapShootSlice, each in its file's
+    value order: YoZ through the source (iz outer, iy inner), XoZ (iz, ix),
+    XOY (iy, ix), and the same three through the first cell of the high PML
+    band (CalculateAreaEnd = n - 5 - pml).  The reference's
+    surf XOY loop reads a stale z index past the array end; the drop-in writes
+    the intended z = CalculateAreaEndZ plane, which is what is checked."""
+    nz, ny, nx = txx.shape
+    sx, sy, sz = src
+    ex, ey, ez = nx - 5 - pml, ny - 5 - pml, nz - 5 - pml
+    return {"snapshotSliceXX_YoZ": txx[:, :, sx], "surfSliceXX_YoZ": txx[:, :, ex],
+            "snapshotSliceXX_XoZ": txx[:, sy, :], "surfSliceXX_XoZ": txx[:, ey, :],
+            "snapshotSliceXX_XOY": txx[sz, :, :], "surfSliceXX_XOY": txx[ez, :, :]}
+
+
+def _ostream(v) -> str:
+    """A float as `std::cout << v` prints it (default precision 6, %g)."""
+    return "%g" % float(v)

@@ -3,8 +3,9 @@ library allocate device memory while they run (their device memory belongs
 to another allocator, or their footprint was fixed at start-up): its partial
 sums live in a fixed array inside libsgfd.so instead of a cudaMalloc'd
 buffer.  Checked through the C ABI against sgfd_energy, on two calls in a
-row with steps between them, and for its size limit.  Collected last, so a
-run that stops at the first failure has run every other test first."""
+row with steps between them, for its size limit, and on a fresh handle that
+it makes no device allocation of its own.  Collected last, so a run that
+stops at the first failure has run every other test first."""
 import numpy as np
 import pytest
 
@@ -42,3 +43,23 @@ def test_noalloc_energy_rejects_more_blocks_than_the_static_scratch_holds():
         assert e.value.code == sgfd.ERR_INVALID and "static scratch" in str(e.value)
         with pytest.raises(sgfd.SgfdError):
             s.energy_noalloc(5)
+
+
+def test_noalloc_energy_makes_no_device_allocation_on_a_fresh_handle():
+    """On a handle that never ran sgfd_energy (whose first call allocates the
+    partial sums), sgfd_energy_noalloc leaves the handle's allocation count
+    where it was, across two calls; sgfd_energy afterwards does allocate,
+    which shows that the count sees such an allocation."""
+    w = wl.small_random_case(nx=40, ny=36, nz=34, pml=5, nt=40)
+    with make_solver(w) as s:
+        s.run(0, 20)
+        s.synchronize()
+        before = s.device_allocations()
+        first = s.energy_noalloc(sgfd.REGION_COMPUTED)
+        s.run(20, 20)
+        second = s.energy_noalloc(sgfd.REGION_COMPUTED)
+        assert s.device_allocations() == before
+        assert first[0] > 0 and second[0] > 0 and first != second
+        want = s.energy(sgfd.REGION_COMPUTED)
+        assert s.device_allocations() == before + 1
+        np.testing.assert_allclose(second, want, rtol=RTOL)
