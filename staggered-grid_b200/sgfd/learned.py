@@ -20,10 +20,17 @@ forward/backward/Adam kernels).
 Evaluation (`reflection`): the same interior and source run three ways — a
 6-cell learned strip, the same strip without the network, and a 20-cell
 split-field PML — and each reports the energy left in the interior once the
-direct wave has gone, relative to its peak (what the boundary reflected).
+direct wave has gone, relative to its peak (what the boundary reflected),
+in all and per face.
+
+Gate (`gate`, `boundary`): the PML is the judge and the fallback.  A
+calibration run compares, face by face, the energy the learned strip leaves
+with the PML's; the strip is used only when no face does worse, otherwise
+the model keeps the 20-cell PML.
 
     python -m sgfd.learned train --out strip_params.npy          (200 runs, seeds 1000-1199)
     python -m sgfd.learned evaluate --params strip_params.npy --steps 1500
+    python -m sgfd.learned gate --params strip_params.npy
 """
 from __future__ import annotations
 
@@ -170,6 +177,16 @@ def train(X, Y, epochs: int = 30, batch: int = 4096, lr: float = 1e-3, seed: int
     return p, hist
 
 
+def energy_density(fields, b, lam, mu, win) -> np.ndarray:
+    """Kinetic + strain energy per cell (the sgfd_energy formulas) of a window."""
+    v = [fields[k][win].astype(np.float64) for k in range(9)]
+    bb, la, m = (a[win].astype(np.float64) for a in (b, lam, mu))
+    ek = 0.5 * (v[0] ** 2 + v[1] ** 2 + v[2] ** 2) / bb
+    tr = v[3] + v[4] + v[5]
+    ss = v[3] ** 2 + v[4] ** 2 + v[5] ** 2 + 2 * (v[6] ** 2 + v[7] ** 2 + v[8] ** 2)
+    return ek + (ss - la / (3 * la + 2 * m) * tr * tr) / (4 * m)
+
+
 def energy(fields, b, lam, mu, win) -> float:
     """Kinetic + strain energy (the sgfd_energy formulas) of a cubic window."""
     v = [fields[k][win].astype(np.float64) for k in range(9)]
@@ -181,14 +198,35 @@ def energy(fields, b, lam, mu, win) -> float:
     return float(ek.sum() + es.sum())
 
 
+FACES = ("x-", "x+", "y-", "y+", "z-", "z+")
+
+
+def face_masks(n: int) -> np.ndarray:
+    """For an n^3 interior, a boolean mask per face (FACES order) of the cells
+    nearer to that face than to any other (ties go to the first face): the
+    part of the interior whose late energy that face reflected."""
+    r = np.arange(n)
+    z, y, x = np.meshgrid(r, r, r, indexing="ij")
+    dist = np.stack([x, n - 1 - x, y, n - 1 - y, z, n - 1 - z])
+    near = np.argmin(dist, axis=0)
+    return np.stack([near == k for k in range(6)])
+
+
 def reflection(params, seed: int = 999, n_int: int = 48, nt: int = 400, sample_every: int = 20,
-               dt: float = 0.001, d: float = 10.0, device: int = 0) -> dict:
+               dt: float = 0.001, d: float = 10.0, device: int = 0, media=None) -> dict:
     """Energy left in the n_int^3 interior at the end relative to its peak, for
     the learned 6-cell strip, the bare 6-cell strip (no network) and a 20-cell
-    split-field PML, on one seeded random medium with a centred Ricker."""
+    split-field PML, on one seeded random medium (or on `media` = (b, lam, mu)
+    of (n_int + 50)^3 GRID cells) with a centred Ricker.  Also the final
+    energy of each face's part of the interior (face_masks) over the peak."""
     pml20 = 20
     n_big = n_int + 2 * pml20 + 2 * HALO
-    b, lam, mu = medium(n_big, seed, "random")
+    if media is None:
+        b, lam, mu = medium(n_big, seed, "random")
+    else:
+        b, lam, mu = (np.asarray(a, np.float32) for a in media)
+        assert b.shape == (n_big,) * 3, f"calibration media must be {n_big}^3 GRID cells"
+    masks = face_masks(n_int)
     f0 = 20.0
     t = np.arange(nt) * dt - 1.2 / f0
     wav = ((1 - 2 * (math.pi * f0 * t) ** 2) * np.exp(-(math.pi * f0 * t) ** 2)).astype(np.float32)
@@ -211,12 +249,46 @@ def reflection(params, seed: int = 999, n_int: int = 48, nt: int = 400, sample_e
                 s.run(it0, min(sample_every, nt - it0))
                 f = [s.field(k) for k in range(9)]
                 hist.append(energy(f, mb, ml, mm, (inner, inner, inner)))
+            dens = energy_density(f, mb, ml, mm, (inner, inner, inner))
         finally:
             s.close()
         hist = np.array(hist)
         out[name] = {"final_over_peak": float(hist[-1] / hist.max()), "peak": float(hist.max()),
-                     "history": hist.tolist()}
+                     "history": hist.tolist(),
+                     "face_final_over_peak": {fc: float(dens[masks[k]].sum() / hist.max())
+                                              for k, fc in enumerate(FACES)}}
     return out
+
+
+def gate(params, nt: int = 400, seed: int = 999, media=None, margin: float = 1.0, device: int = 0) -> dict:
+    """The learned strip's gate: the split-field PML is the judge and the
+    fallback.  A calibration run (reflection(): the same medium and source
+    with the learned 6-cell strip and with a 20-cell PML) measures, per face,
+    the energy that face's part of the interior still holds after nt steps.
+    A face accepts the strip when its energy is no larger than margin times
+    the PML's.  The solver runs one boundary kind on all six faces, so the
+    strip is used only if every face accepts it; otherwise the model keeps
+    the PML.  Returns the decision ("learned_strip" or "pml20"), the faces'
+    verdicts and the measured energies."""
+    r = reflection(params, seed=seed, nt=nt, sample_every=max(1, nt // 8), device=device, media=media)
+    learned, pml = r["learned_strip"], r["pml20"]
+    faces = {fc: bool(np.isfinite(learned["face_final_over_peak"][fc]) and
+                      learned["face_final_over_peak"][fc] <= margin * pml["face_final_over_peak"][fc])
+             for fc in FACES}
+    total_ok = bool(np.isfinite(learned["final_over_peak"]) and
+                    learned["final_over_peak"] <= margin * pml["final_over_peak"])
+    use = all(faces.values()) and total_ok
+    return {"boundary": "learned_strip" if use else "pml20", "faces_accept": faces, "steps": nt,
+            "learned_final_over_peak": learned["final_over_peak"], "pml_final_over_peak": pml["final_over_peak"],
+            "learned_faces": learned["face_final_over_peak"], "pml_faces": pml["face_final_over_peak"]}
+
+
+def boundary(params, decision: dict) -> dict:
+    """Solver settings for a gate decision: the learned strip (pml = 0 and the
+    strip's width and parameters for set_learned_strip) or the 20-cell PML."""
+    if decision["boundary"] == "learned_strip":
+        return {"pml": 0, "strip_width": WIDTH, "params": params}
+    return {"pml": 20, "strip_width": 0, "params": None}
 
 
 def main(argv=None):
@@ -232,6 +304,10 @@ def main(argv=None):
     t.add_argument("--rollout", default="0", help="comma-separated rollout lengths drawn per snapshot")
     t.add_argument("--policy", default=PARAMS_PATH, help="network that runs the rollouts")
     t.add_argument("--device", type=int, default=0)
+    g = sub.add_parser("gate")
+    g.add_argument("--params", default=PARAMS_PATH)
+    g.add_argument("--steps", type=int, default=400)
+    g.add_argument("--device", type=int, default=0)
     e = sub.add_parser("evaluate")
     e.add_argument("--params", default=PARAMS_PATH)
     e.add_argument("--steps", type=int, default=400)
@@ -249,6 +325,8 @@ def main(argv=None):
             hist_l = r["learned_strip"]["history"]
             print(n, {k: v["final_over_peak"] for k, v in r.items()},
                   "second-half growth", hist_l[-1] / hist_l[len(hist_l) // 2], flush=True)
+    elif a.cmd == "gate":
+        print(gate(np.load(a.params), nt=a.steps, device=a.device), flush=True)
     else:
         r = reflection(np.load(a.params), nt=a.steps, sample_every=50 if a.steps > 400 else 20, device=a.device)
         print({k: v["final_over_peak"] for k, v in r.items()}, flush=True)

@@ -263,3 +263,26 @@ def test_window_copy_and_field_samples():
                 D.copy_window_from(E, 20, 0, 0)                            # past the source's x extent
             with pytest.raises(sgfd.SgfdError):
                 E.copy_window_from(D, 0, 0, 0)                             # destination with a PML
+
+
+def test_gate_falls_back_to_the_pml_for_a_bad_network():
+    """The gate keeps the split-field PML when the network does worse: a
+    deliberately bad parameter set (large random weights, so the strip's
+    corrections are noise) leaves more energy than the 20-cell PML on every
+    face and is rejected; the shipped network is judged on the same run, and
+    its decision follows its measured energies."""
+    rng = np.random.default_rng(21)
+    bad = (rng.standard_normal(mo.N_PARAMS) * 0.5).astype(np.float32)
+    d = L.gate(bad, nt=200)
+    assert d["boundary"] == "pml20"
+    assert not any(d["faces_accept"].values())
+    assert L.boundary(bad, d) == {"pml": 20, "strip_width": 0, "params": None}
+    good = L.load_params()
+    g = L.gate(good, nt=200)
+    expect = all(g["learned_faces"][f] <= g["pml_faces"][f] for f in L.FACES) and \
+        g["learned_final_over_peak"] <= g["pml_final_over_peak"]
+    assert (g["boundary"] == "learned_strip") == expect
+    # a margin wide enough to accept anything finite selects the strip
+    lenient = L.gate(good, nt=200, margin=1e12)
+    assert lenient["boundary"] == "learned_strip"
+    assert L.boundary(good, lenient)["pml"] == 0 and L.boundary(good, lenient)["strip_width"] == L.WIDTH

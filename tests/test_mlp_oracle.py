@@ -36,3 +36,16 @@ def test_f16_forward_rounds_operands_and_stays_near_fp64():
     approx = mo.forward_f16(p, X)
     err = np.abs(approx - exact).max() / np.abs(exact).max()
     assert 1e-5 < err < 1e-2, err
+
+
+def test_face_masks_partition_the_interior():
+    """Every interior cell belongs to exactly one face's part, opposite faces'
+    parts are mirror images (even edge), and a cell next to a face belongs to it."""
+    import sgfd.learned as L
+    m = L.face_masks(12)
+    assert m.shape == (6, 12, 12, 12)
+    np.testing.assert_array_equal(m.sum(axis=0), 1)
+    assert m[0, 6, 6, 0] and m[1, 6, 6, 11] and m[2, 6, 0, 6] and m[3, 6, 11, 6] and m[4, 0, 6, 6] and m[5, 11, 6, 6]
+    sizes = m.reshape(6, -1).sum(axis=1)
+    assert sizes.min() > 0 and sizes[0] == sizes[1] and sizes[2] == sizes[3] and sizes[4] == sizes[5]
+    np.testing.assert_array_equal(m[0], m[1][:, :, ::-1])
