@@ -45,6 +45,8 @@ BYTES = {"velocity": (52, 112), "stress": (68, 164)}
 # 394^3 workload is too large for a multi-metric capture, so its traffic is
 # reported as its algorithmic bytes times this ratio.
 TRAFFIC_RATIO = {"velocity": 1.18, "stress": 1.31}
+TRAFFIC_SOURCE = ("ncu dram bytes / algorithmic bytes of the z-march kernels on the 216^3 + 20 PML cube, "
+                  "times this launch's algorithmic bytes")
 # 16-bit storage: fields and splits 2 B, medium 4 B (per step 66 B interior, 144 B PML).
 BYTES16 = {"velocity": (28, 58), "stress": (38, 86)}
 STORAGE = {"f32": 0, "bf16": 1, "f16": 2}
@@ -62,10 +64,13 @@ def parse():
                    default="random344")
     p.add_argument("--no-autotune", action="store_true", help="batch32: keep the default launch shapes")
     p.add_argument("--kernel", choices=["auto", "simple", "zmarch"], default="auto")
-    p.add_argument("--arith", choices=["ref", "fast"], default="fast")
+    p.add_argument("--arith", choices=["ref", "fast"], default="ref",
+                   help="ref: the reference's rounding (the drop-in's); fast: pre-divided coefficients")
     p.add_argument("--storage", choices=["f32", "bf16", "f16"], default="f32",
                    help="wavefield storage; 16-bit also reports errors on a 128^3 crop")
-    p.add_argument("--no-accuracy", action="store_true", help="skip the 16-bit accuracy leg")
+    p.add_argument("--no-accuracy", action="store_true", help="skip the accuracy leg against the FP64 oracle")
+    p.add_argument("--no-large", action="store_true", help="random344: skip the 472^3 + 20 (512^3 computed) line")
+    p.add_argument("--no-other-arith", action="store_true", help="skip timing the other rounding mode")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-steps", type=int, default=6, help="steps of the CPU sample")
@@ -284,11 +289,64 @@ def main():
     import torch
     import sgfd
     torch.cuda.set_device(local)
-    kernel = {"auto": sgfd.KERNEL_AUTO, "simple": sgfd.KERNEL_SIMPLE, "zmarch": sgfd.KERNEL_ZMARCH}[args.kernel]
-    arith = sgfd.ARITH_FAST if args.arith == "fast" else sgfd.ARITH_REF
-    cfg = sgfd.default_config(**{**w.cfg, "device": local, "kernel": kernel, "arith": arith,
-                                 "storage": STORAGE[args.storage]})
     K, W = args.steps, args.warmup
+    leg = timed_leg(w, args, local, world, args.arith, STORAGE[args.storage], K, W, e2e=not args.no_e2e)
+    result = {
+        "metric": "Gcell-updates/s", "value": leg["value"], "unit": "Gcell/s", "n_gpus": world, "steps": K,
+        "warmup": W, "ms_per_step": leg["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32" if args.storage == "f32" else f"f32 arithmetic, {args.storage} storage", "data": "synthetic",
+        "config": {"workload": w.name, "grid": [w.cfg["nx"], w.cfg["ny"], w.cfg["nz"]], "pml": w.cfg["pml"],
+                   "computed_cells": w.computed_cells(), "interior_cells": leg["n_int"], "pml_cells": leg["n_pml"],
+                   "receivers": len(w.rec_comp), "kernel": leg["kernel"], "arith": args.arith,
+                   "storage": args.storage, "parallelism": f"replicas{world}",
+                   "l2": "inputs larger than L2 (9 wavefields of %.0f MB each)"
+                         % (w.cfg["nx"] * w.cfg["ny"] * w.cfg["nz"] * 4 / 1e6)},
+        "roofline": leg["roofline"], "clocks": leg["clocks"], "gpu_launches": leg["launches"], "e2e": leg["e2e"],
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        rate, threads, secs = cpu_oracle_rate(w, args.cpu_steps)
+        result["cpu_baseline"] = {
+            "value": rate, "unit": "Gcell/s", "cores": threads, "kind": "port",
+            "sample": f"{args.cpu_steps} full time steps of {w.name} ({secs:.1f} s) after 1 untimed step; "
+                      f"C++ oracle of the reference kernels, FP32, flush-to-zero, OpenMP {threads} threads"}
+    if rank == 0 and world == 1 and not args.no_accuracy:
+        result["accuracy"] = accuracy_leg(w, args, local)
+    # the other rounding mode on the same model, for comparison
+    if not args.no_other_arith and args.storage == "f32":
+        other = "fast" if args.arith == "ref" else "ref"
+        o = timed_leg(w, args, local, world, other, STORAGE["f32"], K, W, e2e=False)
+        result[f"arith_{other}"] = {k: o[k] for k in ("value", "ms_per_step", "clocks")} | {
+            "kernel_ms": o["roofline"]["kernel_ms"], "frac": o["roofline"]["frac"]}
+    # the 512^3-computed cube on which the FP32 roofline target is stated
+    if args.workload == "random344" and not args.no_large:
+        del w
+        big = build_workload("random472")
+        b = timed_leg(big, args, local, world, args.arith, STORAGE["f32"], K, W, e2e=False)
+        result["random472"] = {
+            "workload": big.name, "grid": [big.cfg["nx"], big.cfg["ny"], big.cfg["nz"]],
+            "computed_cells": big.computed_cells(), "arith": args.arith, "value": b["value"], "unit": "Gcell/s",
+            "ms_per_step": b["ms_per_step"], "steps": K, "warmup": W, "roofline": b["roofline"],
+            "clocks": b["clocks"], "gpu_launches": b["launches"]}
+        if rank == 0 and world == 1 and not args.no_accuracy:
+            result["random472"]["accuracy"] = accuracy_leg(big, args, local)
+    if rank == 0:
+        print(json.dumps(result), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def timed_leg(w, args, local, world, arith_name, storage, K, W, e2e):
+    """W untimed steps, then exactly K steps of w timed with CUDA events on the
+    solver's stream (barrier and synchronize on both sides, max over ranks),
+    nvidia-smi clocks sampled meanwhile; then the per-kernel launch times
+    (roofline of the dominant kernel) and, with e2e, the end-to-end leg."""
+    import torch
+    import sgfd
+    kernel = {"auto": sgfd.KERNEL_AUTO, "simple": sgfd.KERNEL_SIMPLE, "zmarch": sgfd.KERNEL_ZMARCH}[args.kernel]
+    arith = sgfd.ARITH_FAST if arith_name == "fast" else sgfd.ARITH_REF
+    cfg = sgfd.default_config(**{**w.cfg, "device": local, "kernel": kernel, "arith": arith, "storage": storage})
     nt = max(w.nt, W + K + 64)
     wav = np.resize(w.wavelet, nt).astype(np.float32)
     stream = torch.cuda.Stream()          # a real stream: events below see the solver's work
@@ -302,7 +360,6 @@ def main():
     cells = w.computed_cells()
     n_int, n_pml = s.cell_counts()
 
-    # ---- device-resident timing: exactly K steps ----
     s.run(0, W)
     s.prepare_run()                       # graph captured and uploaded outside the timed region
     torch.cuda.synchronize()
@@ -326,91 +383,43 @@ def main():
     ms = max_over_ranks(e0.elapsed_time(e1), world)
     value = job_rate(cells, K, ms, world)
 
-    # ---- roofline of the dominant kernel (events around each kernel) ----
+    # roofline of the dominant kernel (events around each kernel launch)
     P = max(3, min(K, 20))
     tv, ts = s.profile(W + K, P)
     per = {"velocity": tv / P, "stress": ts / P}
     dom = max(per, key=per.get)
-    bpc = BYTES if args.storage == "f32" else BYTES16
+    bpc = BYTES if storage == STORAGE["f32"] else BYTES16
     alg = bpc[dom][0] * n_int + bpc[dom][1] * n_pml
     peak, peak_kind = measured_peak()
     achieved = alg / (per[dom] / 1e3) / 1e9
-    traffic = alg * TRAFFIC_RATIO[dom] if s.kernel_name() == "zmarch" else None
+    traffic = alg * TRAFFIC_RATIO[dom] if s.kernel_name() == "zmarch" and storage == STORAGE["f32"] else None
     roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
-            "traffic_source": "ncu dram bytes / algorithmic bytes of the z-march kernels on the 216^3 + 20 PML "
-                              "cube, times this launch's algorithmic bytes" if traffic else None,
+            "traffic_source": TRAFFIC_SOURCE if traffic else None,
             "alg_bytes_per_launch": alg, "avg_launch_ms": per[dom],
             "step_frac": (sum(v[0] for v in bpc.values()) * n_int + sum(v[1] for v in bpc.values()) * n_pml)
                          / (ms / K / 1e3) / 1e9 / peak,
             "kernel_ms": per}
-
-    # ---- end to end through the C ABI with host buffers ----
-    e2e = None
-    if not args.no_e2e:
-        e2e = end_to_end(s, w, K, world, stream, wav)
-
-    kernel_name, launches = s.kernel_name(), s.run_launches(K)
+    out = {"value": value, "ms_per_step": ms / K, "n_int": n_int, "n_pml": n_pml, "roofline": roof, "clocks": clk,
+           "kernel": s.kernel_name(), "launches": s.run_launches(K), "e2e": None}
+    if e2e:
+        out["e2e"] = end_to_end(s, w, K, world, stream, wav)
     s.close()
-    result = {
-        "metric": "Gcell-updates/s", "value": value, "unit": "Gcell/s", "n_gpus": world, "steps": K,
-        "warmup": W, "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32" if args.storage == "f32" else f"f32 arithmetic, {args.storage} storage", "data": "synthetic",
-        "config": {"workload": w.name, "grid": [w.cfg["nx"], w.cfg["ny"], w.cfg["nz"]], "pml": w.cfg["pml"],
-                   "computed_cells": cells, "interior_cells": n_int, "pml_cells": n_pml,
-                   "receivers": len(w.rec_comp), "kernel": None, "arith": args.arith, "storage": args.storage,
-                   "parallelism": f"replicas{world}",
-                   "l2": "inputs larger than L2 (9 wavefields of %.0f MB each)" % (w.cfg["nx"] * w.cfg["ny"] * w.cfg["nz"] * 4 / 1e6)},
-        "roofline": roof, "clocks": clk,
-        "gpu_launches": None, "e2e": e2e,
-    }
-    result["config"]["kernel"] = kernel_name
-    result["gpu_launches"] = launches
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        rate, threads, secs = cpu_oracle_rate(w, args.cpu_steps)
-        result["cpu_baseline"] = {
-            "value": rate, "unit": "Gcell/s", "cores": threads, "kind": "port",
-            "sample": f"{args.cpu_steps} full time steps of {w.name} ({secs:.1f} s) after 1 untimed step; "
-                      f"C++ oracle of the reference kernels, FP32, flush-to-zero, OpenMP {threads} threads"}
-    if rank == 0 and world == 1 and args.storage != "f32" and not args.no_accuracy:
-        result["accuracy"] = storage_accuracy(w, args, local)
-    if rank == 0:
-        print(json.dumps(result), flush=True)
-    if world > 1:
-        import torch.distributed as dist
-        dist.destroy_process_group()
+    torch.cuda.set_stream(torch.cuda.default_stream())
+    return out
 
 
-def crop_workload(w, n_grid=138, pml=20, nt=300):
-    """The centre n_grid^3 window of w's medium as a model of its own (128^3
-    computed cells with pml 20): source at its centre, Ricker 20 Hz, 16x16
-    receivers 5 cells below the top interior face recording vz and txx."""
-    import sgfd
-    import sgfd.workloads as wl
-    nz, ny, nx = w.b.shape
-    z0, y0, x0 = (nz - n_grid) // 2, (ny - n_grid) // 2, (nx - n_grid) // 2
-    sl = (slice(z0, z0 + n_grid), slice(y0, y0 + n_grid), slice(x0, x0 + n_grid))
-    b, lam, mu = (np.ascontiguousarray(a[sl]) for a in (w.b, w.lam, w.mu))
-    c = n_grid // 2
-    i0, span = wl.HALO + pml, n_grid - 2 * (wl.HALO + pml)
-    ks = i0 + (np.arange(16) * span) // 16
-    pts = [(x, y, i0 + 5) for y in ks for x in ks]
-    xyz = np.array([p for p in pts for _ in (0, 1)], np.int32)
-    comp = np.array([sgfd.VZ, sgfd.TXX] * len(pts), np.int32)
-    cfg = {**w.cfg, "nx": n_grid, "ny": n_grid, "nz": n_grid, "pml": pml}
-    w64 = wl._ricker_t0_64(20.0, w.cfg["dt"], 1.2 / 20.0, nt)
-    return wl.Workload(f"crop{n_grid - 10}^3 of {w.name}", cfg, b, lam, mu, (c, c, c), xyz, comp, nt,
-                       w64.astype(np.float32), w64)
-
-
-def storage_accuracy(w, args, local):
-    """Relative L2 errors of 16-bit storage on a 128^3 crop of the workload's
-    medium: traces and final vx / txx snapshots, against the FP32 GPU path and
-    against the FP64 CPU oracle (the same crop run in double precision)."""
+def accuracy_leg(w, args, local):
+    """Relative L2 errors of this configuration's arithmetic against the FP64
+    CPU oracle (exact arithmetic): traces and final vx / txx.  The CPU-sized
+    plain cube runs in full; a large cube runs on the centre 128^3 crop of its
+    medium for 300 steps.  16-bit storage also reports its error against the
+    FP32 GPU path, and the FP32 path's own error against FP64."""
     import sgfd
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle_py
-    cw = crop_workload(w)
+    import sgfd.workloads as wl
+    cw = w if w.computed_cells() <= 150 ** 3 else wl.crop_workload(w)
     arith = sgfd.ARITH_FAST if args.arith == "fast" else sgfd.ARITH_REF
 
     def gpu(storage):
@@ -432,17 +441,21 @@ def storage_accuracy(w, args, local):
     o.run(cw.wavelet64, 0, cw.nt)
     ref64 = (o.traces(), o.field(sgfd.VX), o.field(sgfd.TXX))
     o.close()
-    r16, r32 = gpu(STORAGE[args.storage]), gpu(0)
 
     def rel(a, b):
         b = np.asarray(b, np.float64)
         return float(np.linalg.norm(np.asarray(a, np.float64) - b) / np.linalg.norm(b))
 
     names = ("traces", "vx", "txx")
-    return {"workload": cw.name, "steps": cw.nt, "storage": args.storage,
-            "vs_fp64": {n: rel(a, b) for n, a, b in zip(names, r16, ref64)},
-            "vs_fp32": {n: rel(a, b) for n, a, b in zip(names, r16, r32)},
-            "fp32_vs_fp64": {n: rel(a, b) for n, a, b in zip(names, r32, ref64)}}
+    r32 = gpu(0)
+    out = {"workload": cw.name, "steps": cw.nt, "arith": args.arith, "storage": args.storage,
+           "vs_fp64": {n: rel(a, b) for n, a, b in zip(names, r32, ref64)}}
+    if args.storage != "f32":
+        r16 = gpu(STORAGE[args.storage])
+        out["vs_fp64"] = {n: rel(a, b) for n, a, b in zip(names, r16, ref64)}
+        out["vs_fp32"] = {n: rel(a, b) for n, a, b in zip(names, r16, r32)}
+        out["fp32_vs_fp64"] = {n: rel(a, b) for n, a, b in zip(names, r32, ref64)}
+    return out
 
 
 def main_learned(args, world, rank, local):
@@ -469,7 +482,7 @@ def main_learned(args, world, rank, local):
         cut = slice(off, off + n)
         mb, ml, mm = (np.ascontiguousarray(a[cut, cut, cut]) for a in (big.b, big.lam, big.mu))
         cfg = sgfd.default_config(**{**big.cfg, "nx": n, "ny": n, "nz": n, "pml": pml, "device": local,
-                                     "arith": sgfd.ARITH_FAST})
+                                     "arith": sgfd.ARITH_FAST if args.arith == "fast" else sgfd.ARITH_REF})
         s = sgfd.Solver(cfg)
         s.set_medium(mb, ml, mm)
         s.set_source(n // 2, n // 2, n // 2)
@@ -498,6 +511,7 @@ def main_learned(args, world, rank, local):
         "warmup": W, "ms_per_step": ls["ms_per_step"], "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": "learned256", "interior": n_int, "strip_width": L.WIDTH, "pml_compared": pml20,
+                   "arith": args.arith,
                    "computed_cells": ls["computed_cells"], "parallelism": "replicas1"},
         "comparison": out,
         "reflected_energy_over_peak": None if refl is None else
@@ -528,7 +542,7 @@ def main_batch(args, world, rank, local):
         w = wl.layered_model(specs[i])
         nt = max(w.nt, W + K + 16)
         wav = np.resize(w.wavelet, nt).astype(np.float32)
-        s = sgfd.Solver(sgfd.default_config(**{**w.cfg, "device": local, "arith": sgfd.ARITH_FAST}))
+        s = sgfd.Solver(sgfd.default_config(**{**w.cfg, "device": local, "arith": sgfd.ARITH_FAST if args.arith == "fast" else sgfd.ARITH_REF}))
         s.set_medium(w.b, w.lam, w.mu)
         s.set_source(*w.src)
         s.set_receivers(w.rec_xyz, w.rec_comp, nt)
@@ -605,7 +619,7 @@ def main_batch(args, world, rank, local):
         "dtype": "f32", "data": "synthetic",
         "config": {"workload": "batch32", "models": len(specs), "computed_cells": total_cells,
                    "models_this_rank": len(mine), "interior_cells_rank0": n_int, "pml_cells_rank0": n_pml,
-                   "arith": "fast", "parallelism": f"replicas{world} (models dealt by cells)",
+                   "arith": args.arith, "parallelism": f"replicas{world} (models dealt by cells)",
                    "autotune": tunings or "off",
                    "l2": "inputs larger than L2 (%.1f GB of wavefields)" % (sum(cells_all) * 36 / 1e9)},
         "roofline": roof, "clocks": clk, "gpu_launches": launches, "e2e": e2e,

@@ -35,18 +35,67 @@ __device__ __forceinline__ float dbwd(const float (&c)[5], G g) {
     return d;
 }
 
+#ifndef SGFD_REFDIV
+#define SGFD_REFDIV 2
+#endif
+
+// a / d correctly rounded (IEEE round to nearest), for d = the cell size
+// along `axis`, the divisor of every REF staggered difference.  The divisor is
+// known in advance, so no division instruction is needed:
+//   * double-precision reciprocal: q = RN32(RN64(a * RN64(1/d))).  The
+//     computed double is within 2^-52 (relative) of a/d, while a quotient of
+//     two binary32 numbers is never a binary32 midpoint and stays more than
+//     2^-50 (relative) away from every one (a - m d is a nonzero multiple of
+//     2^(e_a - 26) for a midpoint m, and |a| < 2^(e_a + 24)), so the final
+//     rounding lands on RN32(a/d): the double-rounding argument of
+//     S. A. Figueroa, "When is double rounding innocuous?", SIGNUM Newsl.
+//     30(3), 1995, for a product with a reciprocal accurate to 2^-53.
+//     Subnormal results included; zeros keep their sign.
+//   * single-precision correction step: q0 = RN(a y), y = RN(1/d);
+//     t = RN(q0 d - a) (exact); q = RN(q0 - t y) — P. Markstein's correction
+//     (IBM J. Res. Dev. 34(1), 1990) in the known-divisor form of Brisebarre,
+//     Muller and Raina (IEEE Trans. Computers 53(8), 2004).  Whether it is
+//     exact for every a depends on d; the host checks every significand of
+//     one binade (ph.mdiv), which covers all |a| in [2^-100, 2^100] by
+//     scaling, and tiny nonzero |a|, where t would lose bits, divide.
+__device__ __forceinline__ float div_cell(const Physics &ph, int axis, float a) {
+    const float d = axis == 0 ? ph.dx : axis == 1 ? ph.dy : ph.dz;
+#if SGFD_REFDIV == 2
+    (void)d;
+    return __double2float_rn(__dmul_rn((double)a, ph.rd64[axis]));
+#elif SGFD_REFDIV == 1
+    if (!((ph.mdiv >> axis) & 1)) return __fdiv_rn(a, d);
+    const float y = ph.rd[axis];
+    const float q0 = __fmul_rn(a, y);
+    const float t = __fmaf_rn(q0, d, -a);
+    float q = __fmaf_rn(-t, y, q0);
+    const float aa = fabsf(a);
+    if (!(aa >= 0x1p-100f && aa <= 0x1p100f) && aa != 0.0f) q = __fdiv_rn(a, d);
+    return q;
+#else
+    return __fdiv_rn(a, d);
+#endif
+}
+
+// A difference sum divided by the cell size of `axis` (REF), or as it is
+// (FAST sums are formed with the pre-divided coefficients).
+template <bool FAST>
+__device__ __forceinline__ float by_cell(const Physics &ph, int axis, float sum) {
+    return FAST ? sum : div_cell(ph, axis, sum);
+}
+
 // Staggered difference along AXIS (0, 1, 2 = x, y, z) divided by the cell
 // size: REF divides the sum (reference expression), FAST uses the
 // pre-divided coefficients c_i / d.
 template <bool FAST, int AXIS, class G>
 __device__ __forceinline__ float dF(const Physics &ph, G g) {
     if (FAST) return dfwd(ph.cs[AXIS], g);
-    return dfwd(ph.c, g) / (AXIS == 0 ? ph.dx : AXIS == 1 ? ph.dy : ph.dz);
+    return div_cell(ph, AXIS, dfwd(ph.c, g));
 }
 template <bool FAST, int AXIS, class G>
 __device__ __forceinline__ float dB(const Physics &ph, G g) {
     if (FAST) return dbwd(ph.cs[AXIS], g);
-    return dbwd(ph.c, g) / (AXIS == 0 ? ph.dx : AXIS == 1 ? ph.dy : ph.dz);
+    return div_cell(ph, AXIS, dbwd(ph.c, g));
 }
 
 // Two staggered differences at once on packed FP32x2 (sm_100 fma.rn.f32x2):
@@ -112,10 +161,11 @@ template <bool FAST>
 __device__ __forceinline__ void damp_factors(const Physics &ph, int axis, float d_axis, int k, int pml, float v,
                                              float &m, float &p) {
     float q;
+    (void)d_axis;
     if (ph.damping == 0) {                    // SGFD_DAMP_REFGPU
-        q = FAST ? v * ph.qf[axis] : ((ph.q_refgpu * v) / d_axis) * ph.poly;
+        q = FAST ? v * ph.qf[axis] : div_cell(ph, axis, ph.q_refgpu * v) * ph.poly;
     } else if (ph.damping == 1) {             // SGFD_DAMP_LOGR
-        q = FAST ? v * ph.qf[axis] : (ph.q_logr * v) / d_axis;
+        q = FAST ? v * ph.qf[axis] : div_cell(ph, axis, ph.q_logr * v);
     } else {                                  // SGFD_DAMP_REFCPU: constant velocity
         q = ph.q_refcpu[axis];
     }

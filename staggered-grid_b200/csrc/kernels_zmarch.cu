@@ -394,20 +394,24 @@ k_velocity_zmarch(const __grid_constant__ VelMaps mp, const __grid_constant__ Mo
             const float *cyy = syy + (ly + 5) * W32 + lx;
             const float *cyz = syz + (ly + 5) * W32 + lx;
             float xX, xY, xZ, yX, yY, yZ, zX, zY, zZ;
-            if constexpr (FAST && CELLS == 1) {
+            if constexpr (CELLS == 1) {
                 // eight of the nine differences in pairs on FP32x2, same roundings
-                const float2 yzX = dpair(ph.cp[0], [&](int i) { return make_float2(cxy[i], rxz[i]); },
+                // (REF: sums with the plain coefficients, then the divisions)
+                const float2 yzX = dpair(FAST ? ph.cp[0] : ph.cr, [&](int i) { return make_float2(cxy[i], rxz[i]); },
                                          [&](int i) { return make_float2(cxy[-1 - i], rxz[-1 - i]); });
-                const float2 xzY = dpair(ph.cp[1], [&](int i) { return make_float2(cxy[i * W48], cyz[i * W32]); },
+                const float2 xzY = dpair(FAST ? ph.cp[1] : ph.cr,
+                                         [&](int i) { return make_float2(cxy[i * W48], cyz[i * W32]); },
                                          [&](int i) { return make_float2(cxy[(-1 - i) * W48], cyz[(-1 - i) * W32]); });
-                const float2 xyZ = dpair(ph.cp[2], [&](int i) { return make_float2(qxz[c][5 + i], qyz[c][5 + i]); },
+                const float2 xyZ = dpair(FAST ? ph.cp[2] : ph.cr,
+                                         [&](int i) { return make_float2(qxz[c][5 + i], qyz[c][5 + i]); },
                                          [&](int i) { return make_float2(qxz[c][4 - i], qyz[c][4 - i]); });
-                const float2 xXyY = dpair(ph.cp[3], [&](int i) { return make_float2(rxx[1 + i], cyy[(1 + i) * W32]); },
+                const float2 xXyY = dpair(FAST ? ph.cp[3] : ph.cr,
+                                          [&](int i) { return make_float2(rxx[1 + i], cyy[(1 + i) * W32]); },
                                           [&](int i) { return make_float2(rxx[-i], cyy[-i * W32]); });
-                xX = xXyY.x; yY = xXyY.y;
-                yX = yzX.x; zX = yzX.y;
-                xY = xzY.x; zY = xzY.y;
-                xZ = xyZ.x; yZ = xyZ.y;
+                xX = by_cell<FAST>(ph, 0, xXyY.x); yY = by_cell<FAST>(ph, 1, xXyY.y);
+                yX = by_cell<FAST>(ph, 0, yzX.x); zX = by_cell<FAST>(ph, 0, yzX.y);
+                xY = by_cell<FAST>(ph, 1, xzY.x); zY = by_cell<FAST>(ph, 1, xzY.y);
+                xZ = by_cell<FAST>(ph, 2, xyZ.x); yZ = by_cell<FAST>(ph, 2, xyZ.y);
             } else {
                 xX = dF<FAST, 0>(ph, [&](int o) { return rxx[o]; });
                 xY = CELLS == 2 ? xY2[c] : dB<FAST, 1>(ph, [&](int o) { return cxy[o * W48]; });
@@ -664,21 +668,25 @@ k_stress_zmarch(const __grid_constant__ StrMaps mp, const __grid_constant__ Mode
             const float *cy_ = svy + (ly + 5) * W48 + lx + 8;
             const float *cz_ = svz + (ly + 5) * W48 + lx + 8;
             float dXx, dYy, dZz, xyY, xyX, xzZ, xzX, yzZ, yzY;
-            if constexpr (FAST && CELLS == 1) {
+            if constexpr (CELLS == 1) {
                 // eight of the nine differences in pairs on FP32x2, same roundings
-                const float2 pX = dpair(ph.cp[0], [&](int i) { return make_float2(cy_[1 + i], cz_[1 + i]); },
+                // (REF: sums with the plain coefficients, then the divisions)
+                const float2 pX = dpair(FAST ? ph.cp[0] : ph.cr,
+                                        [&](int i) { return make_float2(cy_[1 + i], cz_[1 + i]); },
                                         [&](int i) { return make_float2(cy_[-i], cz_[-i]); });
-                const float2 pY = dpair(ph.cp[1],
+                const float2 pY = dpair(FAST ? ph.cp[1] : ph.cr,
                                         [&](int i) { return make_float2(cx_[(1 + i) * W48], cz_[(1 + i) * W48]); },
                                         [&](int i) { return make_float2(cx_[-i * W48], cz_[-i * W48]); });
-                const float2 pZ = dpair(ph.cp[2], [&](int i) { return make_float2(qx[c][5 + i], qy[c][5 + i]); },
+                const float2 pZ = dpair(FAST ? ph.cp[2] : ph.cr,
+                                        [&](int i) { return make_float2(qx[c][5 + i], qy[c][5 + i]); },
                                         [&](int i) { return make_float2(qx[c][4 - i], qy[c][4 - i]); });
-                const float2 pN = dpair(ph.cp[3], [&](int i) { return make_float2(cx_[i], cy_[i * W48]); },
+                const float2 pN = dpair(FAST ? ph.cp[3] : ph.cr,
+                                        [&](int i) { return make_float2(cx_[i], cy_[i * W48]); },
                                         [&](int i) { return make_float2(cx_[-1 - i], cy_[(-1 - i) * W48]); });
-                xyX = pX.x; xzX = pX.y;
-                xyY = pY.x; yzY = pY.y;
-                xzZ = pZ.x; yzZ = pZ.y;
-                dXx = pN.x; dYy = pN.y;
+                xyX = by_cell<FAST>(ph, 0, pX.x); xzX = by_cell<FAST>(ph, 0, pX.y);
+                xyY = by_cell<FAST>(ph, 1, pY.x); yzY = by_cell<FAST>(ph, 1, pY.y);
+                xzZ = by_cell<FAST>(ph, 2, pZ.x); yzZ = by_cell<FAST>(ph, 2, pZ.y);
+                dXx = by_cell<FAST>(ph, 0, pN.x); dYy = by_cell<FAST>(ph, 1, pN.y);
             } else {
                 dXx = dB<FAST, 0>(ph, [&](int o) { return cx_[o]; });
                 dYy = CELLS == 2 ? dYy2[c] : dB<FAST, 1>(ph, [&](int o) { return cy_[o * W48]; });

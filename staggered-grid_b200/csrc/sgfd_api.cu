@@ -17,6 +17,7 @@
 #include <cstdio>
 #include <cstring>
 #include <algorithm>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -159,6 +160,37 @@ namespace {
 
 bool finite_pos(float v) { return std::isfinite(v) && v > 0.0f; }
 
+// Whether the single-precision correction step of div_cell (cell_math.cuh)
+// returns RN(a/d) for every significand of a in [1, 2), which by scaling
+// covers every |a| in [2^-100, 2^100].  Checked once per divisor value (about
+// 2^23 divisions on the host) and remembered.
+bool correction_step_exact(float d) {
+    static std::mutex mu;
+    static std::vector<std::pair<uint32_t, bool>> known;
+    uint32_t key;
+    std::memcpy(&key, &d, 4);
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        for (auto &k : known)
+            if (k.first == key) return k.second;
+    }
+    bool ok = std::isfinite(d) && std::fabs(d) >= 0x1p-20f && std::fabs(d) <= 0x1p20f;
+    const float y = 1.0f / d;
+    for (uint32_t sig = 0; ok && sig < (1u << 23); ++sig) {
+        float a;
+        const uint32_t bits = (127u << 23) | sig;
+        std::memcpy(&a, &bits, 4);
+        const volatile float want = a / d;
+        const float q0 = a * y;
+        const float t = std::fma(q0, d, -a);
+        const float q = std::fma(-t, y, q0);
+        ok = q == want;
+    }
+    std::lock_guard<std::mutex> lock(mu);
+    known.push_back({key, ok});
+    return ok;
+}
+
 void set_physics(sgfd_solver *h) {
     const sgfd_config &c = h->cfg;
     Physics &ph = h->ph;
@@ -192,6 +224,13 @@ void set_physics(sgfd_solver *h) {
     for (int k = 0; k < kPwTable; ++k) {
         const float r = (float)k / (float)p;
         ph.pw[k] = r * r;
+    }
+    for (int i = 0; i < 5; ++i) ph.cr[i] = make_float2(c.coef[i], c.coef[i]);
+    ph.mdiv = 0;
+    for (int a = 0; a < 3; ++a) {
+        ph.rd[a] = 1.0f / d3[a];
+        ph.rd64[a] = 1.0 / (double)d3[a];
+        if (correction_step_exact(d3[a])) ph.mdiv |= 1 << a;
     }
 }
 

@@ -55,6 +55,12 @@ struct Physics {
     float q_refcpu[3];   // 0.5*dt*log10(1/R)*3.4*V/(p*d)
     float qf[3];         // FAST: ((0.5*dt*tau)/d)*poly (REFGPU) or (0.5*dt*3*ln(1/R)/(2p))/d (LOGR)
     float pw[kPwTable];  // (k/pml)^2 for k = 0..kPwTable-1 (rounded as (k/p)*(k/p))
+    // REF arithmetic: the reference's divisions by the cell sizes, correctly
+    // rounded without a division instruction (cell_math.cuh, div_cell)
+    float2 cr[5];        // (c_i, c_i): REF sums of two differences on FP32x2
+    float rd[3];         // RN(1/dx), RN(1/dy), RN(1/dz)
+    int mdiv;            // bit a: the single-precision correction step is exact for axis a
+    double rd64[3];      // RN64(1/dx), RN64(1/dy), RN64(1/dz)
 };
 
 // Geometry and device pointers of one model.

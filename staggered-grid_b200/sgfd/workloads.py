@@ -191,6 +191,28 @@ def random_cube(n_interior: int = 344, pml: int = 20, nt: int = 2000, dt: float 
                     b, lam, mu, src, xyz, comp, nt, w64.astype(np.float32), w64)
 
 
+def crop_workload(w: Workload, n_grid: int = 138, pml: int = 20, nt: int = 300) -> Workload:
+    """The centre n_grid^3 window of w's medium as a model of its own (128^3
+    computed cells with pml 20): source at its centre, Ricker 20 Hz
+    (t0 = 1.2/f0), 16x16 receivers 5 cells below the top interior face
+    recording vz and txx.  A case the FP64 oracle finishes in seconds, for
+    the error of a large configuration's arithmetic against exact arithmetic."""
+    nz, ny, nx = w.b.shape
+    z0, y0, x0 = (nz - n_grid) // 2, (ny - n_grid) // 2, (nx - n_grid) // 2
+    sl = (slice(z0, z0 + n_grid), slice(y0, y0 + n_grid), slice(x0, x0 + n_grid))
+    b, lam, mu = (np.ascontiguousarray(a[sl]) for a in (w.b, w.lam, w.mu))
+    c = n_grid // 2
+    i0, span = HALO + pml, n_grid - 2 * (HALO + pml)
+    ks = i0 + (np.arange(16) * span) // 16
+    pts = [(x, y, i0 + 5) for y in ks for x in ks]
+    xyz = np.array([p for p in pts for _ in (0, 1)], np.int32)
+    comp = np.array([VZ, TXX] * len(pts), np.int32)
+    cfg = {**w.cfg, "nx": n_grid, "ny": n_grid, "nz": n_grid, "pml": pml}
+    w64 = _ricker_t0_64(20.0, w.cfg["dt"], 1.2 / 20.0, nt)
+    return Workload(f"crop{n_grid - 10}^3 of {w.name}", cfg, b, lam, mu, (c, c, c), xyz, comp, nt,
+                    w64.astype(np.float32), w64)
+
+
 def small_random_case(nx=37, ny=41, nz=45, pml=6, nt=60, seed=7, quirks=QUIRKS_REF, damping=DAMP_REFGPU,
                       std=0.15, dt=0.0005, d=10.0, nrec=24) -> Workload:
     """A small uneven-size heterogeneous case for bit-exact parity tests: strong

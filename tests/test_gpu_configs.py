@@ -1,0 +1,72 @@
+"""Parity at the benchmark configurations themselves, not only on small cases.
+
+* "Plain method, CPU-runnable": homogeneous 100^3 interior + 20-cell PML
+  (150^3 GRID), 500 steps, LOGR damping, 101 receivers recording vx and vz.
+  The whole run on the GPU equals the FP32 oracle bit for bit (traces and the
+  final vx and txx), in both rounding modes, and its error against the FP64
+  oracle (exact arithmetic) is stated and bounded.
+* "Plain method on GPU, random medium" (344^3 + 20) and "mixed-precision
+  storage at scale" (472^3 + 20): too large for the CPU oracle over many
+  steps, so their media are checked on the centre 128^3 crop over 300 steps,
+  as the benchmark's accuracy leg does: bit-exact against the FP32 oracle,
+  and within 1e-5 relative L2 of the FP64 oracle.
+"""
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+from helpers import make_solver, run_oracle
+import sgfd
+import sgfd.workloads as wl
+
+pytestmark = pytest.mark.gpu
+
+FP64_TOL = 1e-5   # relative L2 of an FP32 run against exact arithmetic
+
+
+def _gpu_run(w, arith):
+    with make_solver(w, arith=arith) as s:
+        assert s.kernel_name() == "zmarch"
+        s.run(0, w.nt)
+        s.synchronize()
+        return s.traces(), s.field(sgfd.VX), s.field(sgfd.TXX)
+
+
+def _check(w, arith):
+    tr, vx, txx = _gpu_run(w, arith)
+    w.cfg["arith"] = arith
+    o = run_oracle(w)
+    np.testing.assert_array_equal(tr, o.traces().astype(np.float32))
+    np.testing.assert_array_equal(vx, o.field(sgfd.VX).astype(np.float32))
+    np.testing.assert_array_equal(txx, o.field(sgfd.TXX).astype(np.float32))
+    o.close()
+    o64 = run_oracle(w, fp64=True)
+    errs = {"traces": rel_l2(tr, o64.traces()), "vx": rel_l2(vx, o64.field(sgfd.VX)),
+            "txx": rel_l2(txx, o64.field(sgfd.TXX))}
+    o64.close()
+    for k, e in errs.items():
+        assert e < FP64_TOL, (k, e)
+    assert np.abs(tr).max() > 0
+    return errs
+
+
+@pytest.mark.parametrize("arith", [sgfd.ARITH_REF, sgfd.ARITH_FAST], ids=["ref", "fast"])
+def test_plain_cube_config_full_run(arith):
+    w = wl.plain_cube(n_interior=100, pml=20, nt=500)
+    assert w.computed_cells() == 140 ** 3 and len(w.rec_comp) == 202
+    _check(w, arith)
+
+
+@pytest.fixture(scope="module")
+def random344():
+    return wl.random_cube(n_interior=344, pml=20, nt=300)
+
+
+def test_random_cube_config_crop(random344):
+    _check(wl.crop_workload(random344), sgfd.ARITH_REF)
+
+
+def test_storage_config_medium_crop():
+    w = wl.random_cube(n_interior=472, pml=20, nt=300, dt=0.0008, std=0.08, corr_m=80.0, seed=4,
+                       src_computed=(256, 256, 40))
+    _check(wl.crop_workload(w), sgfd.ARITH_REF)
