@@ -64,6 +64,9 @@ def parse():
                    default="random344")
     p.add_argument("--no-autotune", action="store_true", help="batch32: keep the default launch shapes")
     p.add_argument("--kernel", choices=["auto", "simple", "zmarch"], default="auto")
+    p.add_argument("--tile", choices=["default", "32x8", "32x16", "64x8"], default="default",
+                   help="z-marching tile shape (default: the library's choice)")
+    p.add_argument("--zchunk", type=int, default=0, help="z-marching planes per chunk (0: automatic)")
     p.add_argument("--arith", choices=["ref", "fast"], default="ref",
                    help="ref: the reference's rounding (the drop-in's); fast: pre-divided coefficients")
     p.add_argument("--storage", choices=["f32", "bf16", "f16"], default="f32",
@@ -298,7 +301,7 @@ def main():
         "dtype": "f32" if args.storage == "f32" else f"f32 arithmetic, {args.storage} storage", "data": "synthetic",
         "config": {"workload": w.name, "grid": [w.cfg["nx"], w.cfg["ny"], w.cfg["nz"]], "pml": w.cfg["pml"],
                    "computed_cells": w.computed_cells(), "interior_cells": leg["n_int"], "pml_cells": leg["n_pml"],
-                   "receivers": len(w.rec_comp), "kernel": leg["kernel"], "arith": args.arith,
+                   "receivers": len(w.rec_comp), "kernel": leg["kernel"], "tile": leg["tile"], "arith": args.arith,
                    "storage": args.storage, "parallelism": f"replicas{world}",
                    "l2": "inputs larger than L2 (9 wavefields of %.0f MB each)"
                          % (w.cfg["nx"] * w.cfg["ny"] * w.cfg["nz"] * 4 / 1e6)},
@@ -316,7 +319,7 @@ def main():
     if not args.no_other_arith and args.storage == "f32":
         other = "fast" if args.arith == "ref" else "ref"
         o = timed_leg(w, args, local, world, other, STORAGE["f32"], K, W, e2e=False)
-        result[f"arith_{other}"] = {k: o[k] for k in ("value", "ms_per_step", "clocks")} | {
+        result[f"arith_{other}"] = {k: o[k] for k in ("value", "ms_per_step", "clocks", "tile")} | {
             "kernel_ms": o["roofline"]["kernel_ms"], "frac": o["roofline"]["frac"]}
     # the 512^3-computed cube on which the FP32 roofline target is stated
     if args.workload == "random344" and not args.no_large:
@@ -326,7 +329,7 @@ def main():
         result["random472"] = {
             "workload": big.name, "grid": [big.cfg["nx"], big.cfg["ny"], big.cfg["nz"]],
             "computed_cells": big.computed_cells(), "arith": args.arith, "value": b["value"], "unit": "Gcell/s",
-            "ms_per_step": b["ms_per_step"], "steps": K, "warmup": W, "roofline": b["roofline"],
+            "ms_per_step": b["ms_per_step"], "steps": K, "warmup": W, "tile": b["tile"], "roofline": b["roofline"],
             "clocks": b["clocks"], "gpu_launches": b["launches"]}
         if rank == 0 and world == 1 and not args.no_accuracy:
             result["random472"]["accuracy"] = accuracy_leg(big, args, local)
@@ -357,6 +360,10 @@ def timed_leg(w, args, local, world, arith_name, storage, K, W, e2e):
     s.set_source(*w.src)
     s.set_receivers(w.rec_xyz, w.rec_comp, nt)
     s.set_wavelet(wav)
+    if s.kernel_name() == "zmarch" and (args.tile != "default" or args.zchunk):
+        cols, rows = (int(v) for v in (args.tile if args.tile != "default" else "x".join(
+            str(v) for v in s.tile()[:2])).split("x"))
+        s.set_tile(cols, rows, args.zchunk)
     cells = w.computed_cells()
     n_int, n_pml = s.cell_counts()
 
@@ -401,7 +408,8 @@ def timed_leg(w, args, local, world, arith_name, storage, K, W, e2e):
                          / (ms / K / 1e3) / 1e9 / peak,
             "kernel_ms": per}
     out = {"value": value, "ms_per_step": ms / K, "n_int": n_int, "n_pml": n_pml, "roofline": roof, "clocks": clk,
-           "kernel": s.kernel_name(), "launches": s.run_launches(K), "e2e": None}
+           "kernel": s.kernel_name(), "tile": "%dx%d, z chunk %d" % s.tile(), "launches": s.run_launches(K),
+           "e2e": None}
     if e2e:
         out["e2e"] = end_to_end(s, w, K, world, stream, wav)
     s.close()

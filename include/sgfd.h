@@ -253,8 +253,16 @@ int sgfd_set_kernel(sgfd_solver *h, int32_t kernel);
 
 /* z-marching kernels: tile height in cells (8 or 16; one or two cells per
  * thread) and planes per z chunk (0 = automatic).  No effect on the simple
- * family.  Results do not depend on the tiling. */
+ * family.  Results do not depend on the tiling.  Same as sgfd_set_tile with
+ * 32 tile columns. */
 int sgfd_set_tiling(sgfd_solver *h, int32_t tile_rows, int32_t zchunk);
+/* z-marching kernels: tile shape and planes per z chunk (0 = automatic).
+ * 32 x 8 and 32 x 16: one or two y-adjacent cells per thread; 64 x 8: two
+ * x-adjacent cells per thread, differences and updates of the pair on packed
+ * FP32x2.  Results do not depend on the tiling (bit-identical). */
+int sgfd_set_tile(sgfd_solver *h, int32_t tile_cols, int32_t tile_rows, int32_t zchunk);
+/* The z-marching tile shape and z chunk in use (zeros for the simple family). */
+int sgfd_get_tile(const sgfd_solver *h, int32_t *tile_cols, int32_t *tile_rows, int32_t *zchunk);
 
 /* ---- autotuning and batches (no counterpart in the reference, which runs
  * one model with a fixed launch shape: OPT/main.cu's GPUDim) ---- */
@@ -266,11 +274,12 @@ typedef struct sgfd_tuning {
     int32_t zchunk;       /* planes per z chunk; 0 = automatic */
     int32_t candidates;   /* candidates timed */
     float ms_per_step;    /* mean step time of the chosen candidate */
-    int32_t reserved[3];
+    int32_t tile_cols;    /* z-marching tile width: 32 or 64 */
+    int32_t reserved[2];
 } sgfd_tuning;
 
 /* Time the launch-shape candidates (kernel family = halo staging through
- * TMA + shared memory or through the caches; tile height 8/16; z chunk of
+ * TMA + shared memory or through the caches; tiles 32 x 8, 32 x 16, 64 x 8; z chunk of
  * automatic, 16, 32, 64 planes) over probe_steps steps each (0 = 4), keep the
  * fastest, then zero the wavefields, splits and traces (as sgfd_reset), since
  * timing steps the model.  Call it after sgfd_set_medium and before the run.

@@ -113,14 +113,15 @@ int sgfd_autotune(sgfd_solver *h, int32_t probe_steps, sgfd_tuning *out) {
     if (!h->medium_set) return fail(h, SGFD_ERR_STATE, "sgfd_set_medium must come before sgfd_autotune");
     if (probe_steps < 0) return fail(h, SGFD_ERR_INVALID, "negative probe length");
     if (probe_steps == 0) probe_steps = 4;
-    struct Cand { int kernel, rows, zchunk; };
+    struct Cand { int kernel, cols, rows, zchunk; };
     std::vector<Cand> cands;
     if (h->dev_err) {
-        for (int rows : {8, 16})
+        for (int shape = 0; shape < 3; ++shape)
             for (int zc : {0, 16, 32, 64})
-                if (zc == 0 || zc < h->m.nzc) cands.push_back({SGFD_KERNEL_ZMARCH, rows, zc});
+                if (zc == 0 || zc < h->m.nzc)
+                    cands.push_back({SGFD_KERNEL_ZMARCH, shape == 2 ? kPairTileX : kZTileX, shape == 1 ? 16 : 8, zc});
     }
-    cands.push_back({SGFD_KERNEL_SIMPLE, 8, 0});
+    cands.push_back({SGFD_KERNEL_SIMPLE, 0, 8, 0});
     cudaEvent_t e0, e1;
     SG_CUDA(h, cudaEventCreate(&e0), "event");
     if (cudaEventCreate(&e1) != cudaSuccess) {
@@ -131,7 +132,8 @@ int sgfd_autotune(sgfd_solver *h, int32_t probe_steps, sgfd_tuning *out) {
     int best = -1;
     for (size_t c = 0; c < cands.size() && r == SGFD_OK; ++c) {
         r = sgfd_set_kernel(h, cands[c].kernel);
-        if (r == SGFD_OK && cands[c].kernel == SGFD_KERNEL_ZMARCH) r = sgfd_set_tiling(h, cands[c].rows, cands[c].zchunk);
+        if (r == SGFD_OK && cands[c].kernel == SGFD_KERNEL_ZMARCH)
+            r = sgfd_set_tile(h, cands[c].cols, cands[c].rows, cands[c].zchunk);
         if (r) break;
         cudaError_t e = dispatch_on(h, h->sr, h->stream, 0, 0.0f, false, nullptr);   // warm-up step
         if (e == cudaSuccess) e = cudaEventRecord(e0, h->stream);
@@ -151,13 +153,14 @@ int sgfd_autotune(sgfd_solver *h, int32_t probe_steps, sgfd_tuning *out) {
     if (r) return r;
     const Cand &w = cands[best];
     r = sgfd_set_kernel(h, w.kernel);
-    if (r == SGFD_OK && w.kernel == SGFD_KERNEL_ZMARCH) r = sgfd_set_tiling(h, w.rows, w.zchunk);
+    if (r == SGFD_OK && w.kernel == SGFD_KERNEL_ZMARCH) r = sgfd_set_tile(h, w.cols, w.rows, w.zchunk);
     if (r == SGFD_OK) r = sgfd_reset(h);
     if (r) return r;
     if (out) {
         std::memset(out, 0, sizeof *out);
         out->kernel = w.kernel;
         out->tile_rows = w.rows;
+        out->tile_cols = w.cols;
         out->zchunk = w.zchunk;
         out->candidates = (int32_t)cands.size();
         out->ms_per_step = best_ms;

@@ -43,10 +43,13 @@
 
 #include "cell_math.cuh"
 #include "zmarch.h"
+#include "zmarch_dev.cuh"
 
 namespace sgfd {
 
 namespace {
+
+using namespace zdev;
 
 constexpr int TX = kZTileX, NT = 256, S = 3;
 constexpr int W48 = 48, W32 = 32, W36 = 36;
@@ -88,44 +91,6 @@ struct StrL {
     static constexpr uint32_t TXB = 4 * (3 * W48 * (TY + 10) + (3 + NOWN) * W32 * TY);
 };
 
-constexpr uint32_t kWaitCap = 2000;
-constexpr uint32_t kSuspendNs = 1000000;
-
-__device__ __forceinline__ uint32_t sptr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(sptr(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(sptr(bar)), "r"(bytes) : "memory");
-}
-// One poll of the phase; the thread may sleep in the poll for up to
-// kSuspendNs (it wakes as soon as the phase completes).
-__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(ok) : "r"(sptr(bar)), "r"(parity), "n"(kSuspendNs) : "memory");
-    return ok != 0;
-}
-// Bounded wait: false after kWaitCap polls (about kWaitCap * kSuspendNs at most).
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
-    for (uint32_t i = 0; i < kWaitCap; ++i)
-        if (mbar_try_wait(bar, parity)) return true;
-    return false;
-}
-__device__ __forceinline__ void fence_barrier_init() {
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-}
-__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-
-__device__ __forceinline__ void tma3(void *dst, const CUtensorMap *map, int x, int y, int z, uint64_t *bar) {
-    asm volatile(
-        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
-        ::"r"(sptr(dst)), "l"(map), "r"(x), "r"(y), "r"(z), "r"(sptr(bar))
-        : "memory");
-}
-
 struct Tile {
     int cx0, cy0;    // computed coordinates of the tile origin
     int xd;          // device x of the tile origin (128-byte aligned)
@@ -147,18 +112,6 @@ __device__ __forceinline__ Tile make_tile(const Model &m, const ZGeom &g) {
     t.ze = min(t.zs + g.zc, m.nzc);
     t.xy_pml = t.cx0 < m.pml || t.cx0 + TX > m.nxc - m.pml || t.cy0 < m.pml || t.cy0 + TY > m.nyc - m.pml;
     return t;
-}
-
-// Wait (bounded) for the stages still in flight before an early exit.
-__device__ void drain(uint64_t *bar, int issued_end, int from, int zs) {
-    for (int j = from; j < issued_end; ++j) mbar_wait(&bar[(j - zs) % S], (uint32_t)(((j - zs) / S) & 1));
-}
-
-// 128-byte aligned start inside the dynamic shared array.  The offset is
-// computed on the shared-window address so the result stays a pointer into
-// __shared__ memory (the compiler then emits shared loads for every box read).
-__device__ __forceinline__ unsigned char *align_smem(unsigned char *p) {
-    return p + ((128u - (sptr(p) & 127u)) & 127u);
 }
 
 // ---------------------------------------------------------------------------
@@ -509,7 +462,7 @@ k_velocity_zmarch(const __grid_constant__ VelMaps mp, const __grid_constant__ Mo
     }
     if (abort && tid == 0) {
         atomicExch(g.err, 1);
-        drain(bar, issued_end, cz, t.zs);
+        drain<S>(bar, issued_end, cz, t.zs);
     }
 }
 
@@ -801,7 +754,7 @@ k_stress_zmarch(const __grid_constant__ StrMaps mp, const __grid_constant__ Mode
     }
     if (abort && tid == 0) {
         atomicExch(g.err, 1);
-        drain(bar, issued_end, cz, t.zs);
+        drain<S>(bar, issued_end, cz, t.zs);
     }
 }
 
@@ -815,21 +768,6 @@ PFN_cuTensorMapEncodeTiled_v12000 get_encoder() {
             fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
     }
     return fn;
-}
-
-// 3-D FP32 tensor map over one padded array (base = allocation start).
-bool make_map(CUtensorMap *map, const float *grid_origin, const Model &m, int bx, int by) {
-    auto enc = get_encoder();
-    if (!enc) return false;
-    void *base = const_cast<float *>(grid_origin - kXOff);
-    cuuint64_t dims[3] = {(cuuint64_t)(m.nx + kXOff), (cuuint64_t)m.ny, (cuuint64_t)m.nz};
-    cuuint64_t strides[2] = {(cuuint64_t)m.px * 4, (cuuint64_t)m.plane * 4};
-    cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, 1};
-    cuuint32_t es[3] = {1, 1, 1};
-    CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, dims, strides, box, es,
-                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    return r == CUDA_SUCCESS;
 }
 
 template <int CELLS>
@@ -861,6 +799,21 @@ void launch(const Model &m, const Physics &ph, const SourceRec &sr, const ZGeom 
 
 }  // namespace
 
+// 3-D FP32 tensor map over one padded array (base = allocation start).
+bool make_box_map(CUtensorMap *map, const float *grid_origin, const Model &m, int bx, int by) {
+    auto enc = get_encoder();
+    if (!enc) return false;
+    void *base = const_cast<float *>(grid_origin - kXOff);
+    cuuint64_t dims[3] = {(cuuint64_t)(m.nx + kXOff), (cuuint64_t)m.ny, (cuuint64_t)m.nz};
+    cuuint64_t strides[2] = {(cuuint64_t)m.px * 4, (cuuint64_t)m.plane * 4};
+    cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, 1};
+    cuuint32_t es[3] = {1, 1, 1};
+    CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, dims, strides, box, es,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
 bool zmarch_supported(const Model &m) {
     // Halo boxes start 8 cells left of the tile and 5 rows above: always inside
     // the padded array because the frame is 5 cells and kXOff is 27.  The
@@ -873,26 +826,26 @@ cudaError_t zmarch_prepare(const Model &m, int cells, VelMaps *vm, StrMaps *sm) 
     if (cells != 1 && cells != 2) return cudaErrorInvalidValue;
     const int ty = 8 * cells;
     bool ok = true;
-    ok &= make_map(&vm->sxx, m.f[3], m, W48, ty);
-    ok &= make_map(&vm->syy, m.f[4], m, W32, ty + 10);
-    ok &= make_map(&vm->sxy, m.f[6], m, W48, ty + 10);
-    ok &= make_map(&vm->sxz, m.f[7], m, W48, ty);
-    ok &= make_map(&vm->syz, m.f[8], m, W32, ty + 10);
-    ok &= make_map(&vm->b, m.b, m, W36, ty + 1);
-    ok &= make_map(&vm->sxz_c, m.f[7], m, W32, ty);
-    ok &= make_map(&vm->syz_c, m.f[8], m, W32, ty);
-    ok &= make_map(&vm->szz_c, m.f[5], m, W32, ty);
-    ok &= make_map(&vm->b_c, m.b, m, W32, ty);
-    for (int q = 0; q < 3; ++q) ok &= make_map(&vm->own[q], m.f[q], m, W32, ty);
-    ok &= make_map(&sm->vx, m.f[0], m, W48, ty + 10);
-    ok &= make_map(&sm->vy, m.f[1], m, W48, ty + 10);
-    ok &= make_map(&sm->vz, m.f[2], m, W48, ty + 10);
-    ok &= make_map(&sm->vx_c, m.f[0], m, W32, ty);
-    ok &= make_map(&sm->vy_c, m.f[1], m, W32, ty);
-    ok &= make_map(&sm->vz_c, m.f[2], m, W32, ty);
+    ok &= make_box_map(&vm->sxx, m.f[3], m, W48, ty);
+    ok &= make_box_map(&vm->syy, m.f[4], m, W32, ty + 10);
+    ok &= make_box_map(&vm->sxy, m.f[6], m, W48, ty + 10);
+    ok &= make_box_map(&vm->sxz, m.f[7], m, W48, ty);
+    ok &= make_box_map(&vm->syz, m.f[8], m, W32, ty + 10);
+    ok &= make_box_map(&vm->b, m.b, m, W36, ty + 1);
+    ok &= make_box_map(&vm->sxz_c, m.f[7], m, W32, ty);
+    ok &= make_box_map(&vm->syz_c, m.f[8], m, W32, ty);
+    ok &= make_box_map(&vm->szz_c, m.f[5], m, W32, ty);
+    ok &= make_box_map(&vm->b_c, m.b, m, W32, ty);
+    for (int q = 0; q < 3; ++q) ok &= make_box_map(&vm->own[q], m.f[q], m, W32, ty);
+    ok &= make_box_map(&sm->vx, m.f[0], m, W48, ty + 10);
+    ok &= make_box_map(&sm->vy, m.f[1], m, W48, ty + 10);
+    ok &= make_box_map(&sm->vz, m.f[2], m, W48, ty + 10);
+    ok &= make_box_map(&sm->vx_c, m.f[0], m, W32, ty);
+    ok &= make_box_map(&sm->vy_c, m.f[1], m, W32, ty);
+    ok &= make_box_map(&sm->vz_c, m.f[2], m, W32, ty);
     const float *own[StrMaps::kOwn] = {m.f[3], m.f[4], m.f[5], m.f[6], m.f[7], m.f[8], m.lam, m.mu,
                                        m.mxy, m.mxz, m.myz};
-    for (int q = 0; q < StrMaps::kOwn; ++q) ok &= make_map(&sm->own[q], own[q], m, W32, ty);
+    for (int q = 0; q < StrMaps::kOwn; ++q) ok &= make_box_map(&sm->own[q], own[q], m, W32, ty);
     if (!ok) return cudaErrorInvalidValue;
     cudaError_t e = cells == 1 ? set_attrs<false, 1>() : set_attrs<false, 2>();
     if (e == cudaSuccess) e = cells == 1 ? set_attrs<true, 1>() : set_attrs<true, 2>();

@@ -1,0 +1,814 @@
+// kernels_zpair.cu — the paired tiling of the z-marching family: each thread
+// owns two x-adjacent cells, so that the y and z differences, the updates and
+// the global stores of both run on packed FP32x2 (fma.rn.f32x2 and friends)
+// and every shared-memory load of a y tap or an own-cell value brings both.
+//
+// Work decomposition.  A CTA of 256 threads owns a 64 x 8 tile of computed
+// cells (warp w = tile row w, lane l = cells 2l and 2l+1 of that row) and
+// marches along z over a chunk of planes, as the single-cell tiling of
+// kernels_zmarch.cu does: per plane, TMA (cp.async.bulk.tensor.3d, no
+// multicast) stages the xy boxes with the 5-cell halos each field is
+// differentiated along (80 wide for x halos, 18 rows for y halos), the lead
+// planes of the z register queues and the cells' own read-modify-write data
+// into a ring of S stages guarded by one mbarrier each (expect-tx bytes,
+// bounded parity waits); lane 0 of every warp issues a share of a stage's
+// boxes; a stage is refilled with plane z + S as soon as plane z is done.
+//
+// Per thread and plane: x differences per cell from a 12-value window loaded
+// as six 8-byte shared loads; y differences on FP32x2 from ten 8-byte column
+// loads; z differences on FP32x2 from register queues of float2.  Each lane
+// of a packed operation rounds exactly as the scalar operation, so results
+// are bit-identical to kernels_zmarch.cu, kernels_simple.cu and the oracle.
+// Tile-planes with PML cells, the source or receivers take the general path,
+// which updates cell by cell; every other tile-plane updates the pair on
+// FP32x2 and stores it with one 8-byte store per field.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <type_traits>
+
+#include "cell_math.cuh"
+#include "zmarch.h"
+#include "zmarch_dev.cuh"
+
+namespace sgfd {
+
+namespace {
+
+using namespace zdev;
+
+constexpr int PX = kPairTileX;   // computed cells per tile row (two per thread)
+constexpr int PY = 8;            // tile rows, one warp each
+constexpr int NT = 256;
+constexpr int XW = PX + 16;      // x-halo boxes start 8 cells left: TMA x stays a multiple of 4
+constexpr int BW = PX + 4;       // buoyancy box: the tile and one cell to the right, width a multiple of 4
+constexpr int SV = 3;            // velocity ring stages
+constexpr int SS = 2;            // stress ring stages
+
+constexpr int al128(int b) { return (b + 127) / 128 * 128; }
+constexpr int OB = al128(PX * PY * 4);   // one 64 x 8 FP32 box
+
+// Shared-memory stage of the velocity update (byte offsets, 128-aligned boxes).
+struct VelP {
+    static constexpr int SXX = 0;                                  // XW x PY        sigma_xx (x halo)
+    static constexpr int SYY = SXX + al128(XW * PY * 4);           // PX x (PY+10)   sigma_yy (y halo)
+    static constexpr int SXY = SYY + al128(PX * (PY + 10) * 4);    // XW x (PY+10)   sigma_xy (x, y halo)
+    static constexpr int SXZ = SXY + al128(XW * (PY + 10) * 4);    // XW x PY        sigma_xz (x halo)
+    static constexpr int SYZ = SXZ + al128(XW * PY * 4);           // PX x (PY+10)   sigma_yz (y halo)
+    static constexpr int B = SYZ + al128(PX * (PY + 10) * 4);      // BW x (PY+1)    buoyancy (x+1, y+1)
+    static constexpr int LXZ = B + al128(BW * (PY + 1) * 4);       // sigma_xz at z+4
+    static constexpr int LYZ = LXZ + OB;                           // sigma_yz at z+4
+    static constexpr int LZZ = LYZ + OB;                           // sigma_zz at z+5
+    static constexpr int LB = LZZ + OB;                            // buoyancy at z+1
+    static constexpr int OV = LB + OB;                             // own vx, vy, vz at z
+    static constexpr int STAGE = OV + 3 * OB;
+    static constexpr uint32_t TXB = 4 * (2 * XW * PY + 2 * PX * (PY + 10) + XW * (PY + 10) + BW * (PY + 1) +
+                                         7 * PX * PY);
+};
+// Shared-memory stage of the stress update.
+struct StrP {
+    static constexpr int VX = 0;                                   // XW x (PY+10)  vx (x, y halo)
+    static constexpr int VY = VX + al128(XW * (PY + 10) * 4);
+    static constexpr int VZ = VY + al128(XW * (PY + 10) * 4);
+    static constexpr int LX = VZ + al128(XW * (PY + 10) * 4);      // vx at z+5
+    static constexpr int LY = LX + OB;                             // vy at z+5
+    static constexpr int LZ = LY + OB;                             // vz at z+4
+    static constexpr int OWN = LZ + OB;                            // txx..tyz, lambda, mu, mxy, mxz, myz at z
+    static constexpr int NOWN = 11;
+    static constexpr int STAGE = OWN + NOWN * OB;
+    static constexpr uint32_t TXB = 4 * (3 * XW * (PY + 10) + (3 + NOWN) * PX * PY);
+};
+
+struct PTile {
+    int cx0, cy0;    // computed coordinates of the tile origin
+    int xd;          // device x of the tile origin (128-byte aligned)
+    int gx0, gy0;    // GRID coordinates of the tile origin
+    int zs, ze;      // computed z range of this CTA
+    bool xy_pml;     // the tile touches the x or y PML band
+};
+
+__device__ __forceinline__ PTile make_ptile(const Model &m, const ZGeom &g) {
+    PTile t;
+    const int tile = blockIdx.x;
+    t.cx0 = (tile % g.ntx) * PX;
+    t.cy0 = (tile / g.ntx) * PY;
+    t.gx0 = t.cx0 + kHalo;
+    t.gy0 = t.cy0 + kHalo;
+    t.xd = t.gx0 + kXOff;
+    t.zs = blockIdx.y * g.zc;
+    t.ze = min(t.zs + g.zc, m.nzc);
+    t.xy_pml = t.cx0 < m.pml || t.cx0 + PX > m.nxc - m.pml || t.cy0 < m.pml || t.cy0 + PY > m.nyc - m.pml;
+    return t;
+}
+
+struct TmaBox {
+    const CUtensorMap *map;
+    uint32_t off;
+    int x, y, dz;
+};
+constexpr int kWarps = NT / 32;
+constexpr int kMaxBoxesPerWarp = 3;
+constexpr int kVelBoxes = 13;
+constexpr int kStrBoxes = 17;
+
+__device__ __forceinline__ TmaBox vel_box(const VelMaps &mp, const PTile &t, int q) {
+    using L = VelP;
+    switch (q) {
+    case 0: return {&mp.sxx, L::SXX, t.xd - 8, t.gy0, 0};
+    case 1: return {&mp.syy, L::SYY, t.xd, t.gy0 - 5, 0};
+    case 2: return {&mp.sxy, L::SXY, t.xd - 8, t.gy0 - 5, 0};
+    case 3: return {&mp.sxz, L::SXZ, t.xd - 8, t.gy0, 0};
+    case 4: return {&mp.syz, L::SYZ, t.xd, t.gy0 - 5, 0};
+    case 5: return {&mp.b, L::B, t.xd, t.gy0, 0};
+    case 6: return {&mp.sxz_c, L::LXZ, t.xd, t.gy0, 4};
+    case 7: return {&mp.syz_c, L::LYZ, t.xd, t.gy0, 4};
+    case 8: return {&mp.szz_c, L::LZZ, t.xd, t.gy0, 5};
+    case 9: return {&mp.b_c, L::LB, t.xd, t.gy0, 1};
+    case 10: return {&mp.own[0], L::OV, t.xd, t.gy0, 0};
+    case 11: return {&mp.own[1], L::OV + OB, t.xd, t.gy0, 0};
+    default: return {&mp.own[2], L::OV + 2 * OB, t.xd, t.gy0, 0};
+    }
+}
+
+__device__ __forceinline__ TmaBox str_box(const StrMaps &mp, const PTile &t, int q) {
+    using L = StrP;
+    switch (q) {
+    case 0: return {&mp.vx, L::VX, t.xd - 8, t.gy0 - 5, 0};
+    case 1: return {&mp.vy, L::VY, t.xd - 8, t.gy0 - 5, 0};
+    case 2: return {&mp.vz, L::VZ, t.xd - 8, t.gy0 - 5, 0};
+    case 3: return {&mp.vx_c, L::LX, t.xd, t.gy0, 5};
+    case 4: return {&mp.vy_c, L::LY, t.xd, t.gy0, 5};
+    case 5: return {&mp.vz_c, L::LZ, t.xd, t.gy0, 4};
+    default: return {&mp.own[q - 6], L::OWN + (uint32_t)(q - 6) * OB, t.xd, t.gy0, 0};
+    }
+}
+
+// Stage the inputs of computed plane cz from this warp's boxes (lane 0 of
+// every warp); warp 0 arms the stage's barrier with all of the stage's bytes.
+__device__ __forceinline__ void issue(const TmaBox *b, int n, unsigned char *st, uint64_t *bar, int cz, int warp,
+                                      uint32_t txb) {
+    if (warp == 0) mbar_expect_tx(bar, txb);
+    for (int j = 0; j < n; ++j) tma3(st + b[j].off, b[j].map, b[j].x, b[j].y, cz + kHalo + b[j].dz, bar);
+}
+
+__device__ __forceinline__ float2 ld2(const float *p) { return *reinterpret_cast<const float2 *>(p); }
+__device__ __forceinline__ float2 bcast(float v) { return make_float2(v, v); }
+
+// A pair's difference sums (FP32x2, lane = cell) divided by the cell size of
+// `axis` (REF) or as they are (FAST).
+template <bool FAST>
+__device__ __forceinline__ float2 by_cell2(const Physics &ph, int axis, float2 s) {
+    if (FAST) return s;
+    return make_float2(div_cell(ph, axis, s.x), div_cell(ph, axis, s.y));
+}
+// Forward / backward staggered difference of a cell pair from taps g(o)
+// (float2: both cells' values o cells, rows or planes away).
+template <bool FAST, int AXIS, class G>
+__device__ __forceinline__ float2 dF2p(const Physics &ph, G g) {
+    const float2 s = dpair(FAST ? ph.cp[AXIS] : ph.cr, [&](int i) { return g(1 + i); }, [&](int i) { return g(-i); });
+    return by_cell2<FAST>(ph, AXIS, s);
+}
+template <bool FAST, int AXIS, class G>
+__device__ __forceinline__ float2 dB2p(const Physics &ph, G g) {
+    const float2 s = dpair(FAST ? ph.cp[AXIS] : ph.cr, [&](int i) { return g(i); }, [&](int i) { return g(-1 - i); });
+    return by_cell2<FAST>(ph, AXIS, s);
+}
+// x differences of both cells of a pair from one 12-value window w (w[0]
+// at x offset `first` from cell 0): forward taps of cell c at offsets -4..5,
+// backward at -5..4.
+template <bool FAST>
+__device__ __forceinline__ float2 dFx(const Physics &ph, const float (&w)[12], int first) {
+    const float a = dF<FAST, 0>(ph, [&](int o) { return w[o - first]; });
+    const float b = dF<FAST, 0>(ph, [&](int o) { return w[o + 1 - first]; });
+    return make_float2(a, b);
+}
+template <bool FAST>
+__device__ __forceinline__ float2 dBx(const Physics &ph, const float (&w)[12], int first) {
+    const float a = dB<FAST, 0>(ph, [&](int o) { return w[o - first]; });
+    const float b = dB<FAST, 0>(ph, [&](int o) { return w[o + 1 - first]; });
+    return make_float2(a, b);
+}
+// Twelve values of one row starting at an even float index (six 8-byte loads).
+__device__ __forceinline__ void window(const float *row, float (&w)[12]) {
+#pragma unroll
+    for (int k = 0; k < 6; ++k) {
+        const float2 v = ld2(row + 2 * k);
+        w[2 * k] = v.x;
+        w[2 * k + 1] = v.y;
+    }
+}
+__device__ __forceinline__ float lane_of(float2 v, int c) { return c ? v.y : v.x; }
+// Element k of a six-value register array without indexing it at run time
+// (which would move the array to local memory).
+template <class T>
+__device__ __forceinline__ T pick6(const T (&a)[6], int k) {
+    return k == 0 ? a[0] : k == 1 ? a[1] : k == 2 ? a[2] : k == 3 ? a[3] : k == 4 ? a[4] : a[5];
+}
+
+// Common per-thread state of both updates.
+struct PairCtx {
+    int gx, gy;          // GRID coordinates of cell 0
+    bool act0, act1;     // cells inside the computed region
+    int kx0, kx1, ky;    // PML band distances
+    uint32_t col;        // element offset of the pair at z = 0 (in bounds for inactive pairs)
+    PmlColumn pc0, pc1;
+};
+
+__device__ __forceinline__ PairCtx pair_ctx(const Model &m, const PTile &t, int lx, int ly) {
+    PairCtx p;
+    p.gx = t.gx0 + 2 * lx;       // odd GRID x: the pair is 8-byte aligned in the device rows
+    p.gy = t.gy0 + ly;
+    const bool row_ok = t.cy0 + ly < m.nyc;
+    p.act0 = row_ok && t.cx0 + 2 * lx < m.nxc;
+    p.act1 = row_ok && t.cx0 + 2 * lx + 1 < m.nxc;
+    p.kx0 = band(p.gx, m.nx, m.pml);
+    p.kx1 = band(p.gx + 1, m.nx, m.pml);
+    p.ky = band(p.gy, m.ny, m.pml);
+    const int nxo = (m.nx - 2) | 1;   // largest odd x whose pair stays inside the row
+    p.col = (uint32_t)pidx(m, min(p.gx, nxo), min(p.gy, m.ny - 1), 0);
+    p.pc0 = pml_column(m, min(t.cx0 + 2 * lx, m.nxc - 1), min(t.cy0 + ly, m.nyc - 1));
+    p.pc1 = pml_column(m, min(t.cx0 + 2 * lx + 1, m.nxc - 1), min(t.cy0 + ly, m.nyc - 1));
+    return p;
+}
+
+__device__ __forceinline__ void st2(float *p, float2 v, bool both) {
+    if (both) *reinterpret_cast<float2 *>(p) = v;
+    else *p = v.x;
+}
+
+// ---------------------------------------------------------------------------
+// velocity update
+// ---------------------------------------------------------------------------
+
+template <bool FAST>
+__global__ void __launch_bounds__(NT, 2)
+k_velocity_zpair(const __grid_constant__ VelMaps mp, const __grid_constant__ Model m, const __grid_constant__ Physics ph,
+                 const __grid_constant__ ZGeom g, const __grid_constant__ SourceRec sr, int it_arg, float src_value,
+                 int use_wavelet) {
+    using L = VelP;
+    constexpr int S = SV;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    unsigned char *smem = align_smem(smem_raw);
+    __shared__ __align__(8) uint64_t bar[S];
+    __shared__ TmaBox boxes[kWarps][kMaxBoxesPerWarp];
+    const PTile t = make_ptile(m, g);
+    const int tid = threadIdx.x, lx = tid & 31, ly = tid >> 5, warp = ly;
+    if (tid == 0) {
+        for (int s = 0; s < S; ++s) mbar_init(&bar[s], 1);
+        fence_barrier_init();
+    }
+    __syncthreads();
+    const TmaBox *mybox = boxes[warp];
+    const int nbox = (kVelBoxes - warp + kWarps - 1) / kWarps;
+    if (lx == 0) {
+        for (int j = 0; j < nbox; ++j) boxes[warp][j] = vel_box(mp, t, warp + j * kWarps);
+        for (int s = 0; s < S && t.zs + s < t.ze; ++s)
+            issue(mybox, nbox, smem + s * L::STAGE, &bar[s], t.zs + s, warp, L::TXB);
+    }
+    int issued_end = min(t.zs + S, t.ze);   // planes [zs, issued_end) issued
+    int stage = 0;                          // stage of plane cz, and the parity of its barrier
+    uint32_t parity = 0;
+
+    const int it = step_index(sr, it_arg);
+    const float inj = ph.inj_dt2 * ((use_wavelet && sr.wavelet) ? sr.wavelet[it] : src_value);
+    int sx = -1, sy = -1, sz = -1;
+    if (sr.src >= 0) {
+        const int64_t r = sr.src;
+        sz = (int)(r / m.plane);
+        sy = (int)((r - (int64_t)sz * m.plane) / m.px);
+        sx = (int)(r - (int64_t)sz * m.plane - (int64_t)sy * m.px);
+    }
+    const PairCtx pc = pair_ctx(m, t, lx, ly);
+    const uint32_t PL = (uint32_t)m.plane;
+
+    // z queues (both cells): qxz, qyz hold z-5..z+4, qzz holds z-4..z+5 (filled 9 deep here)
+    float2 qxz[10], qyz[10], qzz[10];
+    const int gz0 = t.zs + kHalo;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+        qxz[k + 1] = ld2(m.f[7] + pc.col + (uint32_t)(gz0 - 5 + k) * PL);
+        qyz[k + 1] = ld2(m.f[8] + pc.col + (uint32_t)(gz0 - 5 + k) * PL);
+        float2 zz = ld2(m.f[5] + pc.col + (uint32_t)(gz0 - 4 + k) * PL);
+        if (pc.gy == sy && gz0 - 4 + k == sz) {
+            if (pc.gx == sx) zz.x = zz.x + inj;
+            if (pc.gx + 1 == sx) zz.y = zz.y + inj;
+        }
+        qzz[k + 1] = zz;
+    }
+
+    // receivers of this tile, sorted by z: skip those below the chunk
+    int rp = g.rec_off[blockIdx.x];
+    const int rend = g.rec_off[blockIdx.x + 1];
+    while (rp < rend && g.rec_list[rp].z < gz0) ++rp;
+    int rz = rp < rend ? g.rec_list[rp].z : 0x7fffffff;
+
+    bool failed = false, abort = false;
+    int cz = t.zs;
+    const bool src_near = sr.src >= 0 && sy >= t.gy0 - 5 && sy < t.gy0 + PY + 5 && sx >= t.gx0 - 8 &&
+                          sx < t.gx0 + PX + 8;
+    // One plane.  GEN selects the general path (PML cells, source, receivers);
+    // every other tile-plane takes the packed interior path.  Returns false
+    // when the block votes to abort.
+    auto plane = [&](auto gen_tag) -> bool {
+        constexpr bool GEN = decltype(gen_tag)::value;
+        const int s = stage;
+        unsigned char *st = smem + s * L::STAGE;
+        const int gz = cz + kHalo;
+        const int kz = band(gz, m.nz, m.pml);
+
+        if (!mbar_wait(&bar[s], parity)) failed = true;
+
+        // source patch of the staged copies (uniform branch)
+        if (GEN && src_near && (gz == sz || gz + 5 == sz)) {
+            if (tid == 0) {
+                const int ox = sx - t.gx0, oy = sy - t.gy0;
+                if (gz == sz) {
+                    float *sxx = reinterpret_cast<float *>(st + L::SXX);
+                    float *syy = reinterpret_cast<float *>(st + L::SYY);
+                    if (oy >= 0 && oy < PY && ox + 8 >= 0 && ox + 8 < XW) sxx[oy * XW + ox + 8] += inj;
+                    if (oy + 5 >= 0 && oy + 5 < PY + 10 && ox >= 0 && ox < PX) syy[(oy + 5) * PX + ox] += inj;
+                }
+                if (gz + 5 == sz) {
+                    float *szz = reinterpret_cast<float *>(st + L::LZZ);
+                    if (oy >= 0 && oy < PY && ox >= 0 && ox < PX) szz[oy * PX + ox] += inj;
+                }
+            }
+            __syncthreads();
+        }
+
+        const float *sxx = reinterpret_cast<const float *>(st + L::SXX);
+        const float *syy = reinterpret_cast<const float *>(st + L::SYY);
+        const float *sxy = reinterpret_cast<const float *>(st + L::SXY);
+        const float *sxz = reinterpret_cast<const float *>(st + L::SXZ);
+        const float *syz = reinterpret_cast<const float *>(st + L::SYZ);
+        const float *bb = reinterpret_cast<const float *>(st + L::B);
+        const float *ov = reinterpret_cast<const float *>(st + L::OV);
+        constexpr int OVS = OB / 4;                 // floats between the own-velocity boxes
+        const int e = ly * PX + 2 * lx;             // 64 x 8 box index of cell 0
+
+        // advance the z queues
+#pragma unroll
+        for (int j = 0; j < 9; ++j) {
+            qxz[j] = qxz[j + 1];
+            qyz[j] = qyz[j + 1];
+            qzz[j] = qzz[j + 1];
+        }
+        qxz[9] = ld2(reinterpret_cast<const float *>(st + L::LXZ) + e);
+        qyz[9] = ld2(reinterpret_cast<const float *>(st + L::LYZ) + e);
+        qzz[9] = ld2(reinterpret_cast<const float *>(st + L::LZZ) + e);
+
+        if (pc.act0) {
+            // x differences, per cell, from 12-value windows
+            float w[12];
+            window(sxx + ly * XW + 2 * lx + 4, w);              // x offsets -4 .. 7 of cell 0
+            const float2 xX = dFx<FAST>(ph, w, -4);
+            window(sxy + (ly + 5) * XW + 2 * lx + 2, w);        // -6 .. 5
+            const float2 yX = dBx<FAST>(ph, w, -6);
+            window(sxz + ly * XW + 2 * lx + 2, w);
+            const float2 zX = dBx<FAST>(ph, w, -6);
+            // y and z differences, both cells at once
+            const float *cxy = sxy + (ly + 5) * XW + 2 * lx + 8;
+            const float *cyy = syy + (ly + 5) * PX + 2 * lx;
+            const float *cyz = syz + (ly + 5) * PX + 2 * lx;
+            const float2 xY = dB2p<FAST, 1>(ph, [&](int o) { return ld2(cxy + o * XW); });
+            const float2 yY = dF2p<FAST, 1>(ph, [&](int o) { return ld2(cyy + o * PX); });
+            const float2 zY = dB2p<FAST, 1>(ph, [&](int o) { return ld2(cyz + o * PX); });
+            const float2 xZ = dB2p<FAST, 2>(ph, [&](int o) { return qxz[5 + o]; });
+            const float2 yZ = dB2p<FAST, 2>(ph, [&](int o) { return qyz[5 + o]; });
+            const float2 zZ = dF2p<FAST, 2>(ph, [&](int o) { return qzz[4 + o]; });
+
+            const float2 b0 = ld2(bb + ly * BW + 2 * lx);
+            const float2 bxp = make_float2(b0.y, bb[ly * BW + 2 * lx + 2]);
+            const float2 byp = ld2(bb + (ly + 1) * BW + 2 * lx);
+            const float2 bzp = ld2(reinterpret_cast<const float *>(st + L::LB) + e);
+            const float2 half = bcast(0.5f);            // (a + b) / 2 rounds as (a + b) * 0.5
+            const float2 bx = __fmul2_rn(__fadd2_rn(b0, bxp), half);
+            const float2 by = __fmul2_rn(__fadd2_rn(b0, byp), half);
+            const float2 bz = __fmul2_rn(__fadd2_rn(b0, bzp), half);
+            const float2 dt2 = bcast(ph.dt);
+            const uint32_t ci = pc.col + (uint32_t)gz * PL;   // cell 0
+
+            const bool pml0 = (pc.kx0 | pc.ky | kz) != 0, pml1 = (pc.kx1 | pc.ky | kz) != 0;
+            if (!(GEN && (t.xy_pml || kz != 0) && (pml0 || (pc.act1 && pml1)))) {
+                const float2 v0 = __ffma2_rn(__fmul2_rn(dt2, bx), __fadd2_rn(__fadd2_rn(xX, xY), xZ), ld2(ov + e));
+                const float2 v1 =
+                    __ffma2_rn(__fmul2_rn(dt2, by), __fadd2_rn(__fadd2_rn(yX, yY), yZ), ld2(ov + OVS + e));
+                const float2 v2 =
+                    __ffma2_rn(__fmul2_rn(dt2, bz), __fadd2_rn(__fadd2_rn(zX, zY), zZ), ld2(ov + 2 * OVS + e));
+                st2(m.f[0] + ci, v0, pc.act1);
+                st2(m.f[1] + ci, v1, pc.act1);
+                st2(m.f[2] + ci, v2, pc.act1);
+                if (GEN && gz == rz && it >= 0 && it < sr.nt) {
+                    for (int r = rp; r < rend && g.rec_list[r].z == gz; ++r) {
+                        const int4 q = g.rec_list[r];
+                        if (q.y == pc.gy && q.w <= 2 && (q.x == pc.gx || (pc.act1 && q.x == pc.gx + 1))) {
+                            const int c = q.x - pc.gx;
+                            sr.traces[(int64_t)it * sr.nrec + g.rec_idx[r]] =
+                                q.w == 0 ? lane_of(v0, c) : q.w == 1 ? lane_of(v1, c) : lane_of(v2, c);
+                        }
+                    }
+                }
+            } else {
+                // general path, cell by cell; PML cells through their split fields
+#pragma unroll
+                for (int c = 0; c < 2; ++c) {
+                    if (c == 1 && !pc.act1) break;
+                    const int kx = c ? pc.kx1 : pc.kx0, ky = pc.ky;
+                    const uint32_t cc = ci + c;
+                    float vnew[3];
+                    if (!(kx | ky | kz)) {
+                        vnew[0] = __fmaf_rn(ph.dt * lane_of(bx, c),
+                                            (lane_of(xX, c) + lane_of(xY, c)) + lane_of(xZ, c), ov[e + c]);
+                        vnew[1] = __fmaf_rn(ph.dt * lane_of(by, c),
+                                            (lane_of(yX, c) + lane_of(yY, c)) + lane_of(yZ, c), ov[OVS + e + c]);
+                        vnew[2] = __fmaf_rn(ph.dt * lane_of(bz, c),
+                                            (lane_of(zX, c) + lane_of(zY, c)) + lane_of(zZ, c), ov[2 * OVS + e + c]);
+                    } else {
+                        float mx = 1.f, px = 1.f, my = 1.f, py = 1.f, mz = 1.f, pz = 1.f;
+                        {
+                            const float v = damp_speed(ph, m.mu[cc], lane_of(b0, c),
+                                                       ph.damping == 1 ? m.lam[cc] : 0.f);
+                            if (kx) damp_factors<FAST>(ph, 0, ph.dx, kx, m.pml, v, mx, px);
+                            if (ky) damp_factors<FAST>(ph, 1, ph.dy, ky, m.pml, v, my, py);
+                            if (kz) damp_factors<FAST>(ph, 2, ph.dz, kz, m.pml, v, mz, pz);
+                        }
+                        const bool ref = ph.quirks == 0;
+                        const float bxc = lane_of(bx, c);
+                        const float ax = ph.dt * bxc, ay = ph.dt * (ref ? bxc : lane_of(by, c)),
+                                    az = ph.dt * (ref ? bxc : lane_of(bz, c));
+                        float *sp = m.split + pml_plane_index(m, c ? pc.pc1 : pc.pc0, cz);
+                        const uint32_t N = (uint32_t)m.npml;
+                        float a0, a1, a2;
+                        a0 = split_update<FAST>(sp[S_VXX * N], ax, lane_of(xX, c), kx, mx, px);
+                        a1 = split_update<FAST>(sp[S_VXY * N], ax, lane_of(xY, c), ky, my, py);
+                        a2 = split_update<FAST>(sp[S_VXZ * N], ax, lane_of(xZ, c), kz, mz, pz);
+                        sp[S_VXX * N] = a0; sp[S_VXY * N] = a1; sp[S_VXZ * N] = a2;
+                        vnew[0] = (a0 + a1) + a2;
+                        a0 = split_update<FAST>(sp[S_VYX * N], ay, lane_of(yX, c), kx, mx, px);
+                        a1 = split_update<FAST>(sp[S_VYY * N], ay, lane_of(yY, c), ky, my, py);
+                        a2 = split_update<FAST>(sp[S_VYZ * N], ay, lane_of(yZ, c), kz, mz, pz);
+                        sp[S_VYX * N] = a0; sp[S_VYY * N] = a1; sp[S_VYZ * N] = a2;
+                        vnew[1] = (a0 + a1) + a2;
+                        a0 = split_update<FAST>(sp[S_VZX * N], az, lane_of(zX, c), kx, mx, px);
+                        a1 = split_update<FAST>(sp[S_VZY * N], az, lane_of(zY, c), ky, my, py);
+                        a2 = split_update<FAST>(sp[S_VZZ * N], az, lane_of(zZ, c), kz, mz, pz);
+                        sp[S_VZX * N] = a0; sp[S_VZY * N] = a1; sp[S_VZZ * N] = a2;
+                        vnew[2] = (a0 + a1) + a2;
+                    }
+                    m.f[0][cc] = vnew[0];
+                    m.f[1][cc] = vnew[1];
+                    m.f[2][cc] = vnew[2];
+                    if (gz == rz && it >= 0 && it < sr.nt) {
+                        for (int r = rp; r < rend && g.rec_list[r].z == gz; ++r) {
+                            const int4 q = g.rec_list[r];
+                            if (q.x == pc.gx + c && q.y == pc.gy && q.w <= 2)
+                                sr.traces[(int64_t)it * sr.nrec + g.rec_idx[r]] =
+                                    q.w == 0 ? vnew[0] : q.w == 1 ? vnew[1] : vnew[2];
+                        }
+                    }
+                }
+            }
+        }
+        if (GEN && gz == rz) {
+            while (rp < rend && g.rec_list[rp].z == gz) ++rp;
+            rz = rp < rend ? g.rec_list[rp].z : 0x7fffffff;
+        }
+
+        // every thread is done with this stage: vote on aborts, then refill it
+        if (__syncthreads_or(failed)) return false;
+        if (cz + S < t.ze) {
+            if (lx == 0) {
+                fence_proxy_async();
+                issue(mybox, nbox, st, &bar[s], cz + S, warp, L::TXB);
+            }
+            issued_end = cz + S + 1;
+        }
+        if (++stage == S) {
+            stage = 0;
+            parity ^= 1u;
+        }
+        return true;
+    };
+    for (; cz < t.ze; ++cz) {
+        const int gzp = cz + kHalo;
+        const bool gen = t.xy_pml || band(gzp, m.nz, m.pml) != 0 || (src_near && (gzp == sz || gzp + 5 == sz)) ||
+                         gzp == rz;
+        if (!(gen ? plane(std::true_type{}) : plane(std::false_type{}))) {
+            abort = true;
+            break;
+        }
+    }
+    if (abort && tid == 0) {
+        atomicExch(g.err, 1);
+        drain<S>(bar, issued_end, cz, t.zs);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// stress update
+// ---------------------------------------------------------------------------
+
+template <bool FAST>
+__global__ void __launch_bounds__(NT, 2)
+k_stress_zpair(const __grid_constant__ StrMaps mp, const __grid_constant__ Model m, const __grid_constant__ Physics ph,
+               const __grid_constant__ ZGeom g, const __grid_constant__ SourceRec sr, int it_arg, float src_value,
+               int use_wavelet) {
+    using L = StrP;
+    constexpr int S = SS;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    unsigned char *smem = align_smem(smem_raw);
+    __shared__ __align__(8) uint64_t bar[S];
+    __shared__ TmaBox boxes[kWarps][kMaxBoxesPerWarp];
+    const PTile t = make_ptile(m, g);
+    const int tid = threadIdx.x, lx = tid & 31, ly = tid >> 5, warp = ly;
+    if (tid == 0) {
+        for (int s = 0; s < S; ++s) mbar_init(&bar[s], 1);
+        fence_barrier_init();
+    }
+    __syncthreads();
+    const TmaBox *mybox = boxes[warp];
+    const int nbox = (kStrBoxes - warp + kWarps - 1) / kWarps;
+    if (lx == 0) {
+        for (int j = 0; j < nbox; ++j) boxes[warp][j] = str_box(mp, t, warp + j * kWarps);
+        for (int s = 0; s < S && t.zs + s < t.ze; ++s)
+            issue(mybox, nbox, smem + s * L::STAGE, &bar[s], t.zs + s, warp, L::TXB);
+    }
+    int issued_end = min(t.zs + S, t.ze);
+    int stage = 0;
+    uint32_t parity = 0;
+
+    const int it = step_index(sr, it_arg);
+    const float inj = ph.inj_dt2 * ((use_wavelet && sr.wavelet) ? sr.wavelet[it] : src_value);
+    const int64_t src = sr.src;
+    const PairCtx pc = pair_ctx(m, t, lx, ly);
+    const uint32_t PL = (uint32_t)m.plane;
+
+    // z queues (both cells): qx, qy hold z-4..z+5 (vx, vy); qz holds z-5..z+4 (vz)
+    float2 qx[10], qy[10], qz[10];
+    const int gz0 = t.zs + kHalo;
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+        qx[k + 1] = ld2(m.f[0] + pc.col + (uint32_t)(gz0 - 4 + k) * PL);
+        qy[k + 1] = ld2(m.f[1] + pc.col + (uint32_t)(gz0 - 4 + k) * PL);
+        qz[k + 1] = ld2(m.f[2] + pc.col + (uint32_t)(gz0 - 5 + k) * PL);
+    }
+
+    int rp = g.rec_off[blockIdx.x];
+    const int rend = g.rec_off[blockIdx.x + 1];
+    while (rp < rend && g.rec_list[rp].z < gz0) ++rp;
+    int rz = rp < rend ? g.rec_list[rp].z : 0x7fffffff;
+
+    bool failed = false, abort = false;
+    int cz = t.zs;
+    const int sz = src >= 0 ? (int)(src / m.plane) : -1;
+    auto plane = [&](auto gen_tag) -> bool {
+        constexpr bool GEN = decltype(gen_tag)::value;
+        const int s = stage;
+        unsigned char *st = smem + s * L::STAGE;
+        const int gz = cz + kHalo;
+        const int kz = band(gz, m.nz, m.pml);
+
+        if (!mbar_wait(&bar[s], parity)) failed = true;
+
+        const float *svx = reinterpret_cast<const float *>(st + L::VX);
+        const float *svy = reinterpret_cast<const float *>(st + L::VY);
+        const float *svz = reinterpret_cast<const float *>(st + L::VZ);
+        // own-cell boxes: txx..tyz at q = 0..5, lambda 6, mu 7, shear moduli 8..10
+        const float *own = reinterpret_cast<const float *>(st + L::OWN);
+        constexpr int OS = OB / 4;
+        const int e = ly * PX + 2 * lx;
+
+#pragma unroll
+        for (int j = 0; j < 9; ++j) {
+            qx[j] = qx[j + 1];
+            qy[j] = qy[j + 1];
+            qz[j] = qz[j + 1];
+        }
+        qx[9] = ld2(reinterpret_cast<const float *>(st + L::LX) + e);
+        qy[9] = ld2(reinterpret_cast<const float *>(st + L::LY) + e);
+        qz[9] = ld2(reinterpret_cast<const float *>(st + L::LZ) + e);
+
+        if (pc.act0) {
+            float w[12];
+            window(svx + (ly + 5) * XW + 2 * lx + 2, w);        // x offsets -6 .. 5 of cell 0
+            const float2 dXx = dBx<FAST>(ph, w, -6);
+            window(svy + (ly + 5) * XW + 2 * lx + 4, w);        // -4 .. 7
+            const float2 xyX = dFx<FAST>(ph, w, -4);
+            window(svz + (ly + 5) * XW + 2 * lx + 4, w);
+            const float2 xzX = dFx<FAST>(ph, w, -4);
+            const float *cx_ = svx + (ly + 5) * XW + 2 * lx + 8;
+            const float *cy_ = svy + (ly + 5) * XW + 2 * lx + 8;
+            const float *cz_ = svz + (ly + 5) * XW + 2 * lx + 8;
+            const float2 dYy = dB2p<FAST, 1>(ph, [&](int o) { return ld2(cy_ + o * XW); });
+            const float2 xyY = dF2p<FAST, 1>(ph, [&](int o) { return ld2(cx_ + o * XW); });
+            const float2 yzY = dF2p<FAST, 1>(ph, [&](int o) { return ld2(cz_ + o * XW); });
+            const float2 xzZ = dF2p<FAST, 2>(ph, [&](int o) { return qx[4 + o]; });
+            const float2 yzZ = dF2p<FAST, 2>(ph, [&](int o) { return qy[4 + o]; });
+            const float2 dZz = dB2p<FAST, 2>(ph, [&](int o) { return qz[5 + o]; });
+
+            const float2 l = ld2(own + 6 * OS + e), mu2 = ld2(own + 7 * OS + e);
+            const float2 l2m = __ffma2_rn(bcast(2.0f), mu2, l);
+            const float2 mxy = ld2(own + 8 * OS + e), mxz = ld2(own + 9 * OS + e), myz = ld2(own + 10 * OS + e);
+            const uint32_t ci = pc.col + (uint32_t)gz * PL;
+            const float2 dt2 = bcast(ph.dt);
+
+            const bool pml0 = (pc.kx0 | pc.ky | kz) != 0, pml1 = (pc.kx1 | pc.ky | kz) != 0;
+            if (!(GEN && (t.xy_pml || kz != 0) && (pml0 || (pc.act1 && pml1)))) {
+                float2 o0 = ld2(own + e), o1 = ld2(own + OS + e), o2 = ld2(own + 2 * OS + e);
+                if (GEN && (int64_t)ci == src) { o0.x = o0.x + inj; o1.x = o1.x + inj; o2.x = o2.x + inj; }
+                if (GEN && (int64_t)ci + 1 == src) { o0.y = o0.y + inj; o1.y = o1.y + inj; o2.y = o2.y + inj; }
+                float2 sn[6];
+                sn[0] = __ffma2_rn(dt2, __ffma2_rn(l2m, dXx, __fmul2_rn(l, __fadd2_rn(dYy, dZz))), o0);
+                sn[1] = __ffma2_rn(dt2, __ffma2_rn(l2m, dYy, __fmul2_rn(l, __fadd2_rn(dXx, dZz))), o1);
+                sn[2] = __ffma2_rn(dt2, __ffma2_rn(l2m, dZz, __fmul2_rn(l, __fadd2_rn(dXx, dYy))), o2);
+                sn[3] = __ffma2_rn(__fmul2_rn(dt2, mxy), __fadd2_rn(xyY, xyX), ld2(own + 3 * OS + e));
+                sn[4] = __ffma2_rn(__fmul2_rn(dt2, mxz), __fadd2_rn(xzZ, xzX), ld2(own + 4 * OS + e));
+                sn[5] = __ffma2_rn(__fmul2_rn(dt2, myz), __fadd2_rn(yzZ, yzY), ld2(own + 5 * OS + e));
+#pragma unroll
+                for (int q = 0; q < 6; ++q) st2(m.f[3 + q] + ci, sn[q], pc.act1);
+                if (GEN && gz == rz && it >= 0 && it < sr.nt) {
+                    for (int r = rp; r < rend && g.rec_list[r].z == gz; ++r) {
+                        const int4 q = g.rec_list[r];
+                        if (q.y == pc.gy && q.w >= 3 && (q.x == pc.gx || (pc.act1 && q.x == pc.gx + 1)))
+                            sr.traces[(int64_t)it * sr.nrec + g.rec_idx[r]] = lane_of(pick6(sn, q.w - 3), q.x - pc.gx);
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int c = 0; c < 2; ++c) {
+                    if (c == 1 && !pc.act1) break;
+                    const int kx = c ? pc.kx1 : pc.kx0, ky = pc.ky;
+                    const uint32_t cc = ci + c;
+                    const float lc = lane_of(l, c), mu_c = lane_of(mu2, c), l2mc = lane_of(l2m, c);
+                    const float dXxc = lane_of(dXx, c), dYyc = lane_of(dYy, c), dZzc = lane_of(dZz, c);
+                    float snew[6];
+                    if (!(kx | ky | kz)) {
+                        float o0 = own[e + c], o1 = own[OS + e + c], o2 = own[2 * OS + e + c];
+                        if ((int64_t)cc == src) { o0 = o0 + inj; o1 = o1 + inj; o2 = o2 + inj; }
+                        snew[0] = __fmaf_rn(ph.dt, __fmaf_rn(l2mc, dXxc, lc * (dYyc + dZzc)), o0);
+                        snew[1] = __fmaf_rn(ph.dt, __fmaf_rn(l2mc, dYyc, lc * (dXxc + dZzc)), o1);
+                        snew[2] = __fmaf_rn(ph.dt, __fmaf_rn(l2mc, dZzc, lc * (dXxc + dYyc)), o2);
+                        snew[3] = __fmaf_rn(ph.dt * lane_of(mxy, c), lane_of(xyY, c) + lane_of(xyX, c),
+                                            own[3 * OS + e + c]);
+                        snew[4] = __fmaf_rn(ph.dt * lane_of(mxz, c), lane_of(xzZ, c) + lane_of(xzX, c),
+                                            own[4 * OS + e + c]);
+                        snew[5] = __fmaf_rn(ph.dt * lane_of(myz, c), lane_of(yzZ, c) + lane_of(yzY, c),
+                                            own[5 * OS + e + c]);
+                    } else {
+                        float *sp = m.split + pml_plane_index(m, c ? pc.pc1 : pc.pc0, cz);
+                        const uint32_t N = (uint32_t)m.npml;
+                        float mx = 1.f, px = 1.f, my = 1.f, py = 1.f, mz = 1.f, pz = 1.f;
+                        {
+                            const float v = damp_speed(ph, mu_c, m.b[cc], lc);
+                            if (kx) damp_factors<FAST>(ph, 0, ph.dx, kx, m.pml, v, mx, px);
+                            if (ky) damp_factors<FAST>(ph, 1, ph.dy, ky, m.pml, v, my, py);
+                            if (kz) damp_factors<FAST>(ph, 2, ph.dz, kz, m.pml, v, mz, pz);
+                        }
+                        const float dl = ph.dt * l2mc, dt = ph.dt;
+                        float a0, a1, a2;
+                        a0 = split_update<FAST>(sp[S_XXX * N], dl, dXxc, kx, mx, px);
+                        a1 = split_update<FAST>(sp[S_XXY * N], dt, lc * dYyc, ky, my, py);
+                        a2 = split_update<FAST>(sp[S_XXZ * N], dt, lc * dZzc, kz, mz, pz);
+                        sp[S_XXX * N] = a0; sp[S_XXY * N] = a1; sp[S_XXZ * N] = a2;
+                        snew[0] = (a0 + a1) + a2;
+                        a0 = split_update<FAST>(sp[S_YYX * N], dt, lc * dXxc, kx, mx, px);
+                        a1 = split_update<FAST>(sp[S_YYY * N], dl, dYyc, ky, my, py);
+                        a2 = split_update<FAST>(sp[S_YYZ * N], dt, lc * dZzc, kz, mz, pz);
+                        sp[S_YYX * N] = a0; sp[S_YYY * N] = a1; sp[S_YYZ * N] = a2;
+                        snew[1] = (a0 + a1) + a2;
+                        a0 = split_update<FAST>(sp[S_ZZX * N], dt, lc * dXxc, kx, mx, px);
+                        a1 = split_update<FAST>(sp[S_ZZY * N], dt, lc * dYyc, ky, my, py);
+                        a2 = split_update<FAST>(sp[S_ZZZ * N], dl, dZzc, kz, mz, pz);
+                        sp[S_ZZX * N] = a0; sp[S_ZZY * N] = a1; sp[S_ZZZ * N] = a2;
+                        snew[2] = (a0 + a1) + a2;
+                        const float axy = dt * lane_of(mxy, c), axz = dt * lane_of(mxz, c),
+                                    ayz = dt * lane_of(myz, c);
+                        a0 = split_update<FAST>(sp[S_XYX * N], axy, lane_of(xyX, c), kx, mx, px);
+                        a1 = split_update<FAST>(sp[S_XYY * N], axy, lane_of(xyY, c), ky, my, py);
+                        sp[S_XYX * N] = a0; sp[S_XYY * N] = a1;
+                        snew[3] = a0 + a1;
+                        a0 = split_update<FAST>(sp[S_XZX * N], axz, lane_of(xzX, c), kx, mx, px);
+                        a1 = split_update<FAST>(sp[S_XZZ * N], axz, lane_of(xzZ, c), kz, mz, pz);
+                        sp[S_XZX * N] = a0; sp[S_XZZ * N] = a1;
+                        snew[4] = a0 + a1;
+                        a0 = split_update<FAST>(sp[S_YZY * N], ayz, lane_of(yzY, c), ky, my, py);
+                        a1 = split_update<FAST>(sp[S_YZZ * N], ayz, lane_of(yzZ, c), kz, mz, pz);
+                        sp[S_YZY * N] = a0; sp[S_YZZ * N] = a1;
+                        snew[5] = a0 + a1;
+                    }
+#pragma unroll
+                    for (int q = 0; q < 6; ++q) m.f[3 + q][cc] = snew[q];
+                    if (gz == rz && it >= 0 && it < sr.nt) {
+                        for (int r = rp; r < rend && g.rec_list[r].z == gz; ++r) {
+                            const int4 q = g.rec_list[r];
+                            if (q.x == pc.gx + c && q.y == pc.gy && q.w >= 3)
+                                sr.traces[(int64_t)it * sr.nrec + g.rec_idx[r]] = pick6(snew, q.w - 3);
+                        }
+                    }
+                }
+            }
+        }
+        if (GEN && gz == rz) {
+            while (rp < rend && g.rec_list[rp].z == gz) ++rp;
+            rz = rp < rend ? g.rec_list[rp].z : 0x7fffffff;
+        }
+
+        if (__syncthreads_or(failed)) return false;
+        if (cz + S < t.ze) {
+            if (lx == 0) {
+                fence_proxy_async();
+                issue(mybox, nbox, st, &bar[s], cz + S, warp, L::TXB);
+            }
+            issued_end = cz + S + 1;
+        }
+        if (++stage == S) {
+            stage = 0;
+            parity ^= 1u;
+        }
+        return true;
+    };
+    for (; cz < t.ze; ++cz) {
+        const int gzp = cz + kHalo;
+        const bool gen = t.xy_pml || band(gzp, m.nz, m.pml) != 0 || gzp == sz || gzp == rz;
+        if (!(gen ? plane(std::true_type{}) : plane(std::false_type{}))) {
+            abort = true;
+            break;
+        }
+    }
+    if (abort && tid == 0) {
+        atomicExch(g.err, 1);
+        drain<S>(bar, issued_end, cz, t.zs);
+    }
+}
+
+constexpr int vel_smem() { return SV * VelP::STAGE + 128; }
+constexpr int str_smem() { return SS * StrP::STAGE + 128; }
+static_assert(vel_smem() <= 113 * 1024 && str_smem() <= 113 * 1024, "two CTAs per SM");
+
+template <bool FAST>
+cudaError_t set_attrs() {
+    cudaError_t e = cudaFuncSetAttribute(k_velocity_zpair<FAST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         vel_smem());
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_stress_zpair<FAST>, cudaFuncAttributeMaxDynamicSharedMemorySize, str_smem());
+    return e;
+}
+
+template <bool FAST>
+void launch(const Model &m, const Physics &ph, const SourceRec &sr, const ZGeom &g, const VelMaps &vm,
+            const StrMaps &sm, int it, float src_value, int uw, cudaStream_t s, cudaEvent_t *ev) {
+    const dim3 grid(g.ntx * g.nty, g.nchunks);
+    if (ev) cudaEventRecord(ev[0], s);
+    k_velocity_zpair<FAST><<<grid, NT, vel_smem(), s>>>(vm, m, ph, g, sr, it, src_value, uw);
+    if (ev) cudaEventRecord(ev[1], s);
+    if (ev) cudaEventRecord(ev[2], s);
+    k_stress_zpair<FAST><<<grid, NT, str_smem(), s>>>(sm, m, ph, g, sr, it, src_value, uw);
+    if (ev) cudaEventRecord(ev[3], s);
+}
+
+}  // namespace
+
+cudaError_t zpair_prepare(const Model &m, VelMaps *vm, StrMaps *sm) {
+    constexpr int ty = PY;
+    bool ok = true;
+    ok &= make_box_map(&vm->sxx, m.f[3], m, XW, ty);
+    ok &= make_box_map(&vm->syy, m.f[4], m, PX, ty + 10);
+    ok &= make_box_map(&vm->sxy, m.f[6], m, XW, ty + 10);
+    ok &= make_box_map(&vm->sxz, m.f[7], m, XW, ty);
+    ok &= make_box_map(&vm->syz, m.f[8], m, PX, ty + 10);
+    ok &= make_box_map(&vm->b, m.b, m, BW, ty + 1);
+    ok &= make_box_map(&vm->sxz_c, m.f[7], m, PX, ty);
+    ok &= make_box_map(&vm->syz_c, m.f[8], m, PX, ty);
+    ok &= make_box_map(&vm->szz_c, m.f[5], m, PX, ty);
+    ok &= make_box_map(&vm->b_c, m.b, m, PX, ty);
+    for (int q = 0; q < 3; ++q) ok &= make_box_map(&vm->own[q], m.f[q], m, PX, ty);
+    ok &= make_box_map(&sm->vx, m.f[0], m, XW, ty + 10);
+    ok &= make_box_map(&sm->vy, m.f[1], m, XW, ty + 10);
+    ok &= make_box_map(&sm->vz, m.f[2], m, XW, ty + 10);
+    ok &= make_box_map(&sm->vx_c, m.f[0], m, PX, ty);
+    ok &= make_box_map(&sm->vy_c, m.f[1], m, PX, ty);
+    ok &= make_box_map(&sm->vz_c, m.f[2], m, PX, ty);
+    const float *own[StrMaps::kOwn] = {m.f[3], m.f[4], m.f[5], m.f[6], m.f[7], m.f[8], m.lam, m.mu,
+                                       m.mxy, m.mxz, m.myz};
+    for (int q = 0; q < StrMaps::kOwn; ++q) ok &= make_box_map(&sm->own[q], own[q], m, PX, ty);
+    if (!ok) return cudaErrorInvalidValue;
+    cudaError_t e = set_attrs<false>();
+    if (e == cudaSuccess) e = set_attrs<true>();
+    return e;
+}
+
+void zpair_tiles(const Model &m, int *ntx, int *nty) {
+    *ntx = (m.nxc + PX - 1) / PX;
+    *nty = (m.nyc + PY - 1) / PY;
+}
+
+cudaError_t zpair_step(const Model &m, const Physics &ph, const SourceRec &sr, const ZGeom &g, const VelMaps &vm,
+                       const StrMaps &sm, int it, float src_value, bool use_wavelet, cudaStream_t s,
+                       cudaEvent_t *ev) {
+    const int uw = use_wavelet ? 1 : 0;
+    if (ph.fast) launch<true>(m, ph, sr, g, vm, sm, it, src_value, uw, s, ev);
+    else launch<false>(m, ph, sr, g, vm, sm, it, src_value, uw, s, ev);
+    return cudaGetLastError();
+}
+
+}  // namespace sgfd

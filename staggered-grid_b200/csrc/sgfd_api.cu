@@ -114,7 +114,8 @@ cudaError_t dispatch_on(sgfd_solver *h, const SourceRec &sr, cudaStream_t s, int
     cudaError_t e = h->storage != SGFD_STORE_F32
                         ? half_step(h->m, h->ph, sr, h->hs, it, value, use_wavelet, s, ev)
                     : h->kernel == SGFD_KERNEL_ZMARCH
-                        ? zmarch_step(h->m, h->ph, sr, h->zg, h->vm, h->sm, it, value, use_wavelet, s, ev)
+                        ? (h->zg.pair ? zpair_step(h->m, h->ph, sr, h->zg, h->vm, h->sm, it, value, use_wavelet, s, ev)
+                                      : zmarch_step(h->m, h->ph, sr, h->zg, h->vm, h->sm, it, value, use_wavelet, s, ev))
                         : simple_step(h->m, h->ph, sr, it, value, use_wavelet, s, ev);
     if (e == cudaSuccess && h->strip_n > 0)
         e = launch_strip(h->m, h->strip_w, h->strip_cells, h->strip_n, h->strip_buf, s);
@@ -318,7 +319,7 @@ int upload_zrec(sgfd_solver *h, const std::vector<int4> &rec) {
         const int4 q = rec[i];
         const int cx = q.x - kHalo, cy = q.y - kHalo, cz = q.z - kHalo;
         if (cx < 0 || cy < 0 || cz < 0 || cx >= m.nxc || cy >= m.nyc || cz >= m.nzc) continue;  // frame: stays 0
-        buckets[(cy / (8 * h->zg.cells)) * h->zg.ntx + cx / kZTileX].push_back({q, i});
+        buckets[(cy / (8 * h->zg.cells)) * h->zg.ntx + cx / h->zg.tw].push_back({q, i});
     }
     std::vector<int> off(tiles + 1, 0);
     std::vector<int4> list;
@@ -502,6 +503,8 @@ int sgfd_create(const sgfd_config *cfg, sgfd_solver **out) {
 
     if (c.kernel != SGFD_KERNEL_SIMPLE && c.storage == SGFD_STORE_F32 && zmarch_supported(m)) {
         h->zg.cells = 1;
+        h->zg.pair = 0;
+        h->zg.tw = kZTileX;
         e = zmarch_prepare(m, h->zg.cells, &h->vm, &h->sm);
         if (e == cudaSuccess) e = dev_malloc(h, &h->dev_err, sizeof(int));
         if (e == cudaSuccess) e = cudaMemset(h->dev_err, 0, sizeof(int));
@@ -754,24 +757,42 @@ int sgfd_set_kernel(sgfd_solver *h, int32_t kernel) {
     return SGFD_OK;
 }
 
-int sgfd_set_tiling(sgfd_solver *h, int32_t tile_rows, int32_t zchunk) {
+int sgfd_set_tile(sgfd_solver *h, int32_t tile_cols, int32_t tile_rows, int32_t zchunk) {
     int r = check_handle(h);
     if (r) return r;
-    if (tile_rows != 8 && tile_rows != 16) return fail(h, SGFD_ERR_INVALID, "tile rows must be 8 or 16");
+    const bool pair = tile_cols == kPairTileX;
+    if (tile_cols != kZTileX && !pair) return fail(h, SGFD_ERR_INVALID, "tile columns must be 32 or 64");
+    if (pair ? tile_rows != 8 : (tile_rows != 8 && tile_rows != 16))
+        return fail(h, SGFD_ERR_INVALID, "tiles are 32 x 8, 32 x 16 or 64 x 8");
     if (zchunk < 0) return fail(h, SGFD_ERR_INVALID, "negative chunk");
     if (!h->dev_err) return SGFD_OK;   // no z-marching kernels prepared: nothing to tile
     SG_CUDA(h, cudaStreamSynchronize(h->stream), "synchronise before re-tiling");
     const int cells = tile_rows / 8;
-    if (cells != h->zg.cells) {
-        cudaError_t e = zmarch_prepare(h->m, cells, &h->vm, &h->sm);
+    if (cells != h->zg.cells || (int)pair != h->zg.pair) {
+        cudaError_t e = pair ? zpair_prepare(h->m, &h->vm, &h->sm) : zmarch_prepare(h->m, cells, &h->vm, &h->sm);
         if (e != cudaSuccess) return cuda_fail(h, e, "z-march re-tiling");
         h->zg.cells = cells;
-        zmarch_tiles(h->m, cells, &h->zg.ntx, &h->zg.nty);
+        h->zg.pair = pair ? 1 : 0;
+        h->zg.tw = tile_cols;
+        if (pair) zpair_tiles(h->m, &h->zg.ntx, &h->zg.nty);
+        else zmarch_tiles(h->m, cells, &h->zg.ntx, &h->zg.nty);
         r = upload_zrec(h, h->rec_host);
         if (r) return r;
     }
     h->zchunk_req = zchunk;
     set_zchunks(h);
+    return SGFD_OK;
+}
+
+int sgfd_set_tiling(sgfd_solver *h, int32_t tile_rows, int32_t zchunk) {
+    return sgfd_set_tile(h, kZTileX, tile_rows, zchunk);
+}
+
+int sgfd_get_tile(const sgfd_solver *h, int32_t *tile_cols, int32_t *tile_rows, int32_t *zchunk) {
+    if (!h) return SGFD_ERR_INVALID;
+    if (tile_cols) *tile_cols = h->kernel == SGFD_KERNEL_ZMARCH ? h->zg.tw : 0;
+    if (tile_rows) *tile_rows = h->kernel == SGFD_KERNEL_ZMARCH ? 8 * h->zg.cells : 0;
+    if (zchunk) *zchunk = h->kernel == SGFD_KERNEL_ZMARCH ? h->zg.zc : 0;
     return SGFD_OK;
 }
 

@@ -7,8 +7,11 @@
 
 namespace sgfd {
 
-// Tiles are 32 computed cells wide and 8 * cells high (cells = 1 or 2 per thread).
+// Single-cell tiling (kernels_zmarch.cu): tiles 32 computed cells wide and
+// 8 * cells high (cells = 1 or 2 per thread, stacked along y).
 constexpr int kZTileX = 32;
+// Paired tiling (kernels_zpair.cu): tiles 64 x 8, two x-adjacent cells per thread.
+constexpr int kPairTileX = 64;
 
 // TMA descriptors of the velocity update: x/y-halo boxes of the current plane
 // and 32 x 16 centre boxes of the planes that feed the z register queues.
@@ -28,6 +31,8 @@ struct StrMaps {
 // Launch geometry: tiles of kZTileX x (8 * cells) computed cells, z chunks of
 // zc planes; receivers bucketed per tile and sorted by z.
 struct ZGeom {
+    int pair;               // 1: paired tiling (64 x 8 tiles), 0: single-cell tiling
+    int tw;                 // tile width in computed cells (kZTileX or kPairTileX)
     int cells;
     int ntx, nty;
     int zc, nchunks;
@@ -37,11 +42,20 @@ struct ZGeom {
     int *err;               // device error flag (1: a bounded wait gave up)
 };
 
+// 3-D FP32 tensor map over one padded device array with a bx x by x 1 box.
+bool make_box_map(CUtensorMap *map, const float *grid_origin, const Model &m, int bx, int by);
+
 bool zmarch_supported(const Model &m);
 cudaError_t zmarch_prepare(const Model &m, int cells, VelMaps *vm, StrMaps *sm);
 void zmarch_tiles(const Model &m, int cells, int *ntx, int *nty);
 cudaError_t zmarch_step(const Model &m, const Physics &ph, const SourceRec &sr, const ZGeom &g,
                         const VelMaps &vm, const StrMaps &sm, int it, float src_value, bool use_wavelet,
                         cudaStream_t s, cudaEvent_t *ev = nullptr);
+// Paired tiling: tensor maps, tile counts and one step (velocity + stress).
+cudaError_t zpair_prepare(const Model &m, VelMaps *vm, StrMaps *sm);
+void zpair_tiles(const Model &m, int *ntx, int *nty);
+cudaError_t zpair_step(const Model &m, const Physics &ph, const SourceRec &sr, const ZGeom &g, const VelMaps &vm,
+                       const StrMaps &sm, int it, float src_value, bool use_wavelet, cudaStream_t s,
+                       cudaEvent_t *ev = nullptr);
 
 }  // namespace sgfd

@@ -1,0 +1,66 @@
+// zmarch_dev.cuh — device helpers shared by the z-marching kernel families
+// (kernels_zmarch.cu, kernels_zpair.cu): mbarrier waits with an iteration
+// cap, TMA tiled loads (no multicast) and shared-memory alignment.
+#pragma once
+
+#include <cuda.h>
+
+#include <cstdint>
+
+namespace sgfd {
+namespace zdev {
+
+constexpr uint32_t kWaitCap = 2000;
+constexpr uint32_t kSuspendNs = 1000000;
+
+__device__ __forceinline__ uint32_t sptr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(sptr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(sptr(bar)), "r"(bytes) : "memory");
+}
+// One poll of the phase; the thread may sleep in the poll for up to
+// kSuspendNs (it wakes as soon as the phase completes).
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok) : "r"(sptr(bar)), "r"(parity), "n"(kSuspendNs) : "memory");
+    return ok != 0;
+}
+// Bounded wait: false after kWaitCap polls (about kWaitCap * kSuspendNs at most).
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+    for (uint32_t i = 0; i < kWaitCap; ++i)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+__device__ __forceinline__ void fence_barrier_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__device__ __forceinline__ void tma3(void *dst, const CUtensorMap *map, int x, int y, int z, uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+        ::"r"(sptr(dst)), "l"(map), "r"(x), "r"(y), "r"(z), "r"(sptr(bar))
+        : "memory");
+}
+
+// Wait (bounded) for the stages still in flight before an early exit:
+// planes [from, issued_end) of a ring of S stages started at plane zs.
+template <int S>
+__device__ void drain(uint64_t *bar, int issued_end, int from, int zs) {
+    for (int j = from; j < issued_end; ++j) mbar_wait(&bar[(j - zs) % S], (uint32_t)(((j - zs) / S) & 1));
+}
+
+// 128-byte aligned start inside the dynamic shared array.  The offset is
+// computed on the shared-window address so the result stays a pointer into
+// __shared__ memory (the compiler then emits shared loads for every box read).
+__device__ __forceinline__ unsigned char *align_smem(unsigned char *p) {
+    return p + ((128u - (sptr(p) & 127u)) & 127u);
+}
+
+}  // namespace zdev
+}  // namespace sgfd

@@ -64,7 +64,8 @@ class SgfdError(RuntimeError):
 class Tuning(ctypes.Structure):
     """sgfd_tuning: the launch shape sgfd_autotune picked."""
     _fields_ = [("kernel", ctypes.c_int32), ("tile_rows", ctypes.c_int32), ("zchunk", ctypes.c_int32),
-                ("candidates", ctypes.c_int32), ("ms_per_step", ctypes.c_float), ("reserved", ctypes.c_int32 * 3)]
+                ("candidates", ctypes.c_int32), ("ms_per_step", ctypes.c_float), ("tile_cols", ctypes.c_int32),
+                ("reserved", ctypes.c_int32 * 2)]
 
 
 _lib = None
@@ -111,6 +112,8 @@ def lib() -> ctypes.CDLL:
         "sgfd_set_tiling": (ctypes.c_int, [vp, i32, i32]),
         "sgfd_cell_counts": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64)]),
         "sgfd_launches_per_step": (ctypes.c_int, [vp]),
+        "sgfd_set_tile": (ctypes.c_int, [vp, i32, i32, i32]),
+        "sgfd_get_tile": (ctypes.c_int, [vp, ip, ip, ip]),
         "sgfd_device_allocations": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_int64)]),
         "sgfd_run_launches": (ctypes.c_int, [vp, ctypes.c_int32, ctypes.c_int32]),
         "sgfd_prepare_run": (ctypes.c_int, [vp]),
@@ -315,6 +318,16 @@ class Solver:
 
     def set_tiling(self, tile_rows: int, zchunk: int = 0):
         self._check(lib().sgfd_set_tiling(self.h, tile_rows, zchunk))
+
+    def set_tile(self, tile_cols: int, tile_rows: int = 8, zchunk: int = 0):
+        """z-marching tile shape: 32 x 8, 32 x 16 or 64 x 8 (cell pairs on FP32x2)."""
+        self._check(lib().sgfd_set_tile(self.h, tile_cols, tile_rows, zchunk))
+
+    def tile(self) -> tuple[int, int, int]:
+        """(tile columns, tile rows, z chunk) of the z-marching kernels in use."""
+        a, b, c = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+        self._check(lib().sgfd_get_tile(self.h, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
+        return a.value, b.value, c.value
 
     def cell_counts(self) -> tuple[int, int]:
         a, b = ctypes.c_int64(), ctypes.c_int64()

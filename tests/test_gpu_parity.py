@@ -25,10 +25,11 @@ CASES = [
     # a tall interior core: most tile-planes take the interior-only path
     dict(quirks=sgfd.QUIRKS_REF, damping=sgfd.DAMP_REFGPU, nx=100, ny=58, nz=64, pml=4, nt=30, nrec=6),
 ]
-# (id, kernel family, tile rows, z chunk)
-KERNELS = [("simple", sgfd.KERNEL_SIMPLE, 0, 0), ("zmarch", sgfd.KERNEL_ZMARCH, 8, 0),
-           ("zmarch_chunk7", sgfd.KERNEL_ZMARCH, 8, 7), ("zmarch_rows16", sgfd.KERNEL_ZMARCH, 16, 0),
-           ("zmarch_rows16_chunk5", sgfd.KERNEL_ZMARCH, 16, 5)]
+# (id, kernel family, tile rows, z chunk, tile columns)
+KERNELS = [("simple", sgfd.KERNEL_SIMPLE, 0, 0, 32), ("zmarch", sgfd.KERNEL_ZMARCH, 8, 0, 32),
+           ("zmarch_chunk7", sgfd.KERNEL_ZMARCH, 8, 7, 32), ("zmarch_rows16", sgfd.KERNEL_ZMARCH, 16, 0, 32),
+           ("zmarch_rows16_chunk5", sgfd.KERNEL_ZMARCH, 16, 5, 32),
+           ("zmarch_pairs", sgfd.KERNEL_ZMARCH, 8, 0, 64), ("zmarch_pairs_chunk6", sgfd.KERNEL_ZMARCH, 8, 6, 64)]
 
 
 def _ids(c):
@@ -45,7 +46,8 @@ def test_bit_exact_vs_oracle(case, kernel, arith):
     with make_solver(w, kernel=kernel[1]) as s:
         assert s.kernel_name() == kernel[0].split("_")[0]
         if kernel[2]:
-            s.set_tiling(kernel[2], kernel[3])
+            s.set_tile(kernel[4], kernel[2], kernel[3])
+            assert s.tile()[:2] == (kernel[4], kernel[2])
         s.run(0, w.nt)
         s.synchronize()
         tr = s.traces()
@@ -77,14 +79,18 @@ def test_step_api_equals_run_api():
         np.testing.assert_array_equal(a.field(sgfd.TXX), b.field(sgfd.TXX))
 
 
-@pytest.mark.parametrize("kern", [sgfd.KERNEL_SIMPLE, sgfd.KERNEL_ZMARCH], ids=["simple", "zmarch"])
-def test_graph_replay_equals_direct_launches(kern):
+@pytest.mark.parametrize("kern,cols", [(sgfd.KERNEL_SIMPLE, 0), (sgfd.KERNEL_ZMARCH, 32), (sgfd.KERNEL_ZMARCH, 64)],
+                         ids=["simple", "zmarch", "zmarch_pairs"])
+def test_graph_replay_equals_direct_launches(kern, cols):
     """sgfd_run with CUDA graphs (16-step replays driven by a device step
     counter, remainder launched directly) against direct launches: bit-equal
     traces and fields, for one long run, for runs split at arbitrary steps, and
     after a receiver change that forces a new capture."""
     w = wl.small_random_case(nt=77, nrec=24)
     with make_solver(w, kernel=kern) as a, make_solver(w, kernel=kern) as b, make_solver(w, kernel=kern) as c:
+        if cols:
+            for s in (a, b, c):
+                s.set_tile(cols, 8)
         a.run(0, w.nt, graph=False)
         b.prepare_run()
         b.run(0, w.nt, graph=True)
@@ -115,10 +121,13 @@ def test_source_inside_pml_matches_oracle():
     w = wl.small_random_case(nt=25)
     w.src = (6, 7, 8)
     o = run_oracle(w)
-    for kern in (sgfd.KERNEL_SIMPLE, sgfd.KERNEL_ZMARCH):
+    for kern, cols in ((sgfd.KERNEL_SIMPLE, 0), (sgfd.KERNEL_ZMARCH, 32), (sgfd.KERNEL_ZMARCH, 64)):
         with make_solver(w, kernel=kern) as s:
+            if cols:
+                s.set_tile(cols, 8)
             s.run(0, w.nt)
             np.testing.assert_array_equal(s.traces(), o.traces().astype(np.float32))
+            np.testing.assert_array_equal(s.field(sgfd.TXX), o.field(sgfd.TXX).astype(np.float32))
 
 
 def test_fast_arithmetic_within_tolerance_of_reference_rounding():
