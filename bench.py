@@ -63,6 +63,8 @@ def parse():
                                                "batch32", "learned256"],
                    default="random344")
     p.add_argument("--no-autotune", action="store_true", help="batch32: keep the default launch shapes")
+    p.add_argument("--batch-mode", choices=["persistent", "graph"], default="persistent",
+                   help="batch32: one persistent launch per run, or graph replays with one branch per model")
     p.add_argument("--kernel", choices=["auto", "simple", "zmarch"], default="auto")
     p.add_argument("--tile", choices=["default", "32x8", "32x16", "64x8"], default="default",
                    help="z-marching tile shape (default: the library's choice)")
@@ -533,8 +535,9 @@ def main_learned(args, world, rank, local):
 def main_batch(args, world, rank, local):
     """The batched configuration: 32 layered models of uneven size (359 M
     computed cells in all), each with its own source and 128 receivers,
-    advanced together by sgfd_batch_run (16-step graphs, one branch per
-    model).  With N ranks the models are dealt out by computed cells (greedy,
+    advanced together by sgfd_batch_run: by default one persistent launch per
+    run over all models' work items (--batch-mode graph: 16-step graphs, one
+    branch per model, autotuned launch shapes).  With N ranks the models are dealt out by computed cells (greedy,
     largest first); value = all ranks' cells x steps / slowest rank's time."""
     import torch
     import sgfd
@@ -555,7 +558,7 @@ def main_batch(args, world, rank, local):
         s.set_source(*w.src)
         s.set_receivers(w.rec_xyz, w.rec_comp, nt)
         s.set_wavelet(wav)
-        if not args.no_autotune:
+        if not args.no_autotune and args.batch_mode == "graph":
             t = s.autotune(3)
             tunings.append({"model": i, "kernel": "zmarch" if t.kernel == sgfd.KERNEL_ZMARCH else "simple",
                             "tile_rows": t.tile_rows, "zchunk": t.zchunk, "ms": round(t.ms_per_step, 4)})
@@ -565,6 +568,8 @@ def main_batch(args, world, rank, local):
         models.append(s)
         media.append((w.b, w.lam, w.mu, len(w.rec_comp)))
     batch = sgfd.Batch(models)
+    if args.batch_mode == "persistent":
+        batch.set_persistent(True)
     stream = torch.cuda.ExternalStream(batch.stream())
     batch.run(0, W)
     batch.synchronize()
@@ -628,6 +633,7 @@ def main_batch(args, world, rank, local):
         "config": {"workload": "batch32", "models": len(specs), "computed_cells": total_cells,
                    "models_this_rank": len(mine), "interior_cells_rank0": n_int, "pml_cells_rank0": n_pml,
                    "arith": args.arith, "parallelism": f"replicas{world} (models dealt by cells)",
+                   "batch_mode": args.batch_mode,
                    "autotune": tunings or "off",
                    "l2": "inputs larger than L2 (%.1f GB of wavefields)" % (sum(cells_all) * 36 / 1e9)},
         "roofline": roof, "clocks": clk, "gpu_launches": launches, "e2e": e2e,

@@ -8,7 +8,11 @@
 // per model (up to kMaxBranches streams, models dealt round-robin), so the
 // hardware schedules the small models' CTAs side by side; a device step
 // counter, advanced by the graph's last node, gives the kernels their step
-// index, as in sgfd_run.
+// index, as in sgfd_run.  In persistent mode (sgfd_batch_set_persistent) one
+// cooperative launch runs all steps of all models instead: its CTAs take the
+// models' (tile, z chunk) work items from a global counter, velocity phase
+// then stress phase, with a bounded grid barrier between the phases
+// (kernels_zpair.cu, k_batch_zpair).
 #include <algorithm>
 #include <cstdarg>
 #include <cstdio>
@@ -31,6 +35,17 @@ struct sgfd_batch {
     cudaGraphExec_t graph = nullptr;
     std::vector<GraphKey> keys;
     int *step_ctr = nullptr;
+    // persistent mode: one cooperative launch runs every model's work items
+    bool persistent = false;
+    bool pfast = false;
+    int barrier_ctas = 0;                 // 0: as many as launched
+    int ctas = 0;                         // CTAs that fit at once
+    PairModel *pdesc = nullptr;           // device copies of the models' descriptors
+    int *pfirst = nullptr;                // prefix sums of the models' work items
+    unsigned *pctl = nullptr;             // barrier arrivals + work counters
+    int pctl_steps = 0;
+    int *pstatus = nullptr;
+    std::vector<GraphKey> pkeys;          // model state the descriptors were built from
     std::string err;
 };
 
@@ -103,9 +118,112 @@ int capture(sgfd_batch *b) {
     return SGFD_OK;
 }
 
+// Whether a model can run in a persistent batch (paired z-march tiling).
+const char *persistent_blocker(const sgfd_solver *h) {
+    if (h->storage != SGFD_STORE_F32) return "16-bit storage";
+    if (!h->dev_err) return "no z-marching kernels on this grid";
+    if (h->strip_n > 0) return "a learned strip";
+    if (h->audit_every > 0) return "a per-step audit";
+    return nullptr;
+}
+
+// Device descriptors of the models, rebuilt when a model changed since.
+int build_descriptors(sgfd_batch *b) {
+    const int n = (int)b->models.size();
+    bool current = b->pdesc && (int)b->pkeys.size() == n;
+    for (int i = 0; i < n && current; ++i) {
+        GraphKey k;
+        graph_key(b->models[i], &k);
+        current = std::memcmp(&k, &b->pkeys[i], sizeof k) == 0;
+    }
+    if (current) return SGFD_OK;
+    std::vector<PairModel> d(n);
+    std::vector<int> first(n + 1, 0);
+    for (int i = 0; i < n; ++i) {
+        const sgfd_solver *h = b->models[i];
+        std::memset(static_cast<void *>(&d[i]), 0, sizeof d[i]);
+        d[i].vm = h->vm;
+        d[i].sm = h->sm;
+        d[i].m = h->m;
+        d[i].ph = h->ph;
+        d[i].g = h->zg;
+        d[i].sr = h->sr;
+        d[i].sr.it_dev = nullptr;
+        d[i].items = h->zg.ntx * h->zg.nty * h->zg.nchunks;
+        first[i + 1] = first[i] + d[i].items;
+    }
+    if (!b->pdesc) {
+        BATCH_CUDA(b, cudaMalloc(&b->pdesc, (size_t)n * sizeof(PairModel)), "batch descriptors");
+        BATCH_CUDA(b, cudaMalloc(&b->pfirst, (size_t)(n + 1) * sizeof(int)), "batch descriptors");
+        BATCH_CUDA(b, cudaMalloc(&b->pstatus, sizeof(int)), "batch status");
+        BATCH_CUDA(b, cudaMemset(b->pstatus, 0, sizeof(int)), "batch status");
+    }
+    BATCH_CUDA(b, cudaMemcpy(b->pdesc, d.data(), (size_t)n * sizeof(PairModel), cudaMemcpyHostToDevice),
+               "batch descriptors");
+    BATCH_CUDA(b, cudaMemcpy(b->pfirst, first.data(), (size_t)(n + 1) * sizeof(int), cudaMemcpyHostToDevice),
+               "batch descriptors");
+    b->pkeys.resize(n);
+    for (int i = 0; i < n; ++i) graph_key(b->models[i], &b->pkeys[i]);
+    return SGFD_OK;
+}
+
+int run_persistent(sgfd_batch *b, int it0, int nsteps) {
+    if (nsteps == 0) return SGFD_OK;
+    for (size_t i = 0; i < b->models.size(); ++i) {
+        const char *why = persistent_blocker(b->models[i]);
+        if (why) return bfail(b, SGFD_ERR_STATE, "model %zu cannot run persistently: %s", i, why);
+        if (b->models[i]->zg.pair != 1 || (bool)b->models[i]->ph.fast != b->pfast)
+            return bfail(b, SGFD_ERR_STATE, "model %zu changed tiling or rounding since sgfd_batch_set_persistent", i);
+    }
+    int r = build_descriptors(b);
+    if (r) return r;
+    if (nsteps > b->pctl_steps) {
+        cudaFree(b->pctl);
+        b->pctl = nullptr;
+        b->pctl_steps = 0;
+        BATCH_CUDA(b, cudaMalloc(&b->pctl, (size_t)(1 + 2 * nsteps) * sizeof(unsigned)), "batch counters");
+        b->pctl_steps = nsteps;
+    }
+    BATCH_CUDA(b, cudaMemsetAsync(b->pctl, 0, (size_t)(1 + 2 * nsteps) * sizeof(unsigned), b->stream),
+               "batch counters");
+    const int bar = b->barrier_ctas > 0 ? b->barrier_ctas : b->ctas;
+    BATCH_CUDA(b, zpair_batch_run(b->pdesc, (int)b->models.size(), b->pfirst, it0, nsteps, b->pctl, bar, b->ctas,
+                                  b->pfast, b->pstatus, b->stream),
+               "persistent batch launch");
+    return SGFD_OK;
+}
+
 }  // namespace
 
 extern "C" {
+
+int sgfd_batch_set_persistent(sgfd_batch *b, int32_t on, int32_t barrier_ctas) {
+    if (!b) return fail(nullptr, SGFD_ERR_INVALID, "null batch");
+    BATCH_CUDA(b, cudaSetDevice(b->device), "cudaSetDevice");
+    if (barrier_ctas < 0) return bfail(b, SGFD_ERR_INVALID, "negative barrier count");
+    if (!on) {
+        b->persistent = false;
+        return SGFD_OK;
+    }
+    for (size_t i = 0; i < b->models.size(); ++i) {
+        const char *why = persistent_blocker(b->models[i]);
+        if (why) return bfail(b, SGFD_ERR_UNSUPPORTED, "model %zu cannot run persistently: %s", i, why);
+        if ((bool)b->models[i]->ph.fast != (bool)b->models[0]->ph.fast)
+            return bfail(b, SGFD_ERR_UNSUPPORTED, "models %zu and 0 differ in rounding mode", i);
+    }
+    b->ctas = zpair_batch_ctas(b->device);
+    if (b->ctas <= 0) return bfail(b, SGFD_ERR_UNSUPPORTED, "the persistent batch kernel does not fit this device");
+    for (size_t i = 0; i < b->models.size(); ++i) {
+        sgfd_solver *h = b->models[i];
+        if (h->zg.pair != 1 && sgfd_set_tile(h, kPairTileX, 8, h->zchunk_req) != SGFD_OK)
+            return bfail(b, SGFD_ERR_CUDA, "model %zu: %s", i, h->err.c_str());
+    }
+    b->pfast = b->models[0]->ph.fast != 0;
+    b->barrier_ctas = barrier_ctas;
+    b->persistent = true;
+    b->pkeys.clear();
+    return SGFD_OK;
+}
 
 int sgfd_autotune(sgfd_solver *h, int32_t probe_steps, sgfd_tuning *out) {
     int r = check_handle(h);
@@ -227,6 +345,10 @@ void sgfd_batch_destroy(sgfd_batch *b) {
     if (b->cap) cudaStreamDestroy(b->cap);
     if (b->stream) cudaStreamDestroy(b->stream);
     cudaFree(b->step_ctr);
+    cudaFree(b->pdesc);
+    cudaFree(b->pfirst);
+    cudaFree(b->pctl);
+    cudaFree(b->pstatus);
     delete b;
 }
 
@@ -246,6 +368,14 @@ int sgfd_batch_run(sgfd_batch *b, int32_t it0, int32_t nsteps) {
     for (size_t i = 0; i < b->models.size(); ++i) {   // after the models' queued work
         BATCH_CUDA(b, cudaEventRecord(b->ev_in[i], b->models[i]->stream), "order after model streams");
         BATCH_CUDA(b, cudaStreamWaitEvent(b->stream, b->ev_in[i], 0), "order after model streams");
+    }
+    if (b->persistent) {
+        const int r = run_persistent(b, it0, nsteps);
+        if (r) return r;
+        BATCH_CUDA(b, cudaEventRecord(b->done, b->stream), "order model streams after the batch");
+        for (sgfd_solver *h : b->models)
+            BATCH_CUDA(b, cudaStreamWaitEvent(h->stream, b->done, 0), "order model streams after the batch");
+        return SGFD_OK;
     }
     int it = it0, left = nsteps;
     if (left >= kGraphSteps) {
@@ -270,6 +400,16 @@ int sgfd_batch_synchronize(sgfd_batch *b) {
     if (!b) return fail(nullptr, SGFD_ERR_INVALID, "null batch");
     BATCH_CUDA(b, cudaSetDevice(b->device), "cudaSetDevice");
     BATCH_CUDA(b, cudaStreamSynchronize(b->stream), "batch synchronize");
+    if (b->pstatus) {
+        int st = 0;
+        BATCH_CUDA(b, cudaMemcpy(&st, b->pstatus, sizeof st, cudaMemcpyDeviceToHost), "batch status");
+        if (st) {
+            BATCH_CUDA(b, cudaMemset(b->pstatus, 0, sizeof st), "batch status");
+            for (sgfd_solver *h : b->models) check_device_error(h);   // clear the models' flags too
+            return bfail(b, SGFD_ERR_CUDA, "persistent batch: a bounded %s wait gave up",
+                         st == kBatchWaitGrid ? "grid-barrier" : "TMA");
+        }
+    }
     for (size_t i = 0; i < b->models.size(); ++i)
         if (check_device_error(b->models[i]) != SGFD_OK)
             return bfail(b, SGFD_ERR_CUDA, "model %zu: %s", i, b->models[i]->err.c_str());
@@ -280,6 +420,7 @@ void *sgfd_batch_stream(sgfd_batch *b) { return b ? static_cast<void *>(b->strea
 
 int sgfd_batch_run_launches(const sgfd_batch *b, int32_t nsteps) {
     if (!b || nsteps < 0) return -1;
+    if (b->persistent) return nsteps > 0 ? 1 : 0;
     int per = 0;
     for (const sgfd_solver *h : b->models) per += sgfd_launches_per_step(h);
     const int replays = nsteps >= kGraphSteps ? nsteps / kGraphSteps : 0;

@@ -87,15 +87,14 @@ struct PTile {
     bool xy_pml;     // the tile touches the x or y PML band
 };
 
-__device__ __forceinline__ PTile make_ptile(const Model &m, const ZGeom &g) {
+__device__ __forceinline__ PTile make_ptile(const Model &m, const ZGeom &g, int tile, int chunk) {
     PTile t;
-    const int tile = blockIdx.x;
     t.cx0 = (tile % g.ntx) * PX;
     t.cy0 = (tile / g.ntx) * PY;
     t.gx0 = t.cx0 + kHalo;
     t.gy0 = t.cy0 + kHalo;
     t.xd = t.gx0 + kXOff;
-    t.zs = blockIdx.y * g.zc;
+    t.zs = chunk * g.zc;
     t.ze = min(t.zs + g.zc, m.nzc);
     t.xy_pml = t.cx0 < m.pml || t.cx0 + PX > m.nxc - m.pml || t.cy0 < m.pml || t.cy0 + PY > m.nyc - m.pml;
     return t;
@@ -240,34 +239,30 @@ __device__ __forceinline__ void st2(float *p, float2 v, bool both) {
 // velocity update
 // ---------------------------------------------------------------------------
 
+// One work item of the vel update: tile `tile`, z chunk `chunk`.  The
+// ring's barriers (bar, S of them) are initialised by the caller; pbits holds
+// the parity of the next wait of each stage and carries over between the
+// work items of a persistent caller.  Returns false when the block gave up
+// on a wait (after waiting, bounded, for its own copies still in flight).
 template <bool FAST>
-__global__ void __launch_bounds__(NT, 2)
-k_velocity_zpair(const __grid_constant__ VelMaps mp, const __grid_constant__ Model m, const __grid_constant__ Physics ph,
-                 const __grid_constant__ ZGeom g, const __grid_constant__ SourceRec sr, int it_arg, float src_value,
-                 int use_wavelet) {
+__device__ __forceinline__ bool vel_pair(const VelMaps &mp, const Model &m, const Physics &ph, const ZGeom &g,
+                                        const SourceRec &sr, int it_arg, float src_value, int use_wavelet, int tile,
+                                        int chunk, unsigned char *smem, uint64_t *bar,
+                                        TmaBox (*boxes)[kMaxBoxesPerWarp], uint32_t &pbits) {
     using L = VelP;
     constexpr int S = SV;
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    unsigned char *smem = align_smem(smem_raw);
-    __shared__ __align__(8) uint64_t bar[S];
-    __shared__ TmaBox boxes[kWarps][kMaxBoxesPerWarp];
-    const PTile t = make_ptile(m, g);
+    const PTile t = make_ptile(m, g, tile, chunk);
     const int tid = threadIdx.x, lx = tid & 31, ly = tid >> 5, warp = ly;
-    if (tid == 0) {
-        for (int s = 0; s < S; ++s) mbar_init(&bar[s], 1);
-        fence_barrier_init();
-    }
-    __syncthreads();
     const TmaBox *mybox = boxes[warp];
     const int nbox = (kVelBoxes - warp + kWarps - 1) / kWarps;
     if (lx == 0) {
+        fence_proxy_async();   // a persistent caller's previous item read these stages
         for (int j = 0; j < nbox; ++j) boxes[warp][j] = vel_box(mp, t, warp + j * kWarps);
         for (int s = 0; s < S && t.zs + s < t.ze; ++s)
             issue(mybox, nbox, smem + s * L::STAGE, &bar[s], t.zs + s, warp, L::TXB);
     }
     int issued_end = min(t.zs + S, t.ze);   // planes [zs, issued_end) issued
-    int stage = 0;                          // stage of plane cz, and the parity of its barrier
-    uint32_t parity = 0;
+    int stage = 0;                          // stage of plane cz
 
     const int it = step_index(sr, it_arg);
     const float inj = ph.inj_dt2 * ((use_wavelet && sr.wavelet) ? sr.wavelet[it] : src_value);
@@ -297,8 +292,8 @@ k_velocity_zpair(const __grid_constant__ VelMaps mp, const __grid_constant__ Mod
     }
 
     // receivers of this tile, sorted by z: skip those below the chunk
-    int rp = g.rec_off[blockIdx.x];
-    const int rend = g.rec_off[blockIdx.x + 1];
+    int rp = g.rec_off[tile];
+    const int rend = g.rec_off[tile + 1];
     while (rp < rend && g.rec_list[rp].z < gz0) ++rp;
     int rz = rp < rend ? g.rec_list[rp].z : 0x7fffffff;
 
@@ -316,7 +311,8 @@ k_velocity_zpair(const __grid_constant__ VelMaps mp, const __grid_constant__ Mod
         const int gz = cz + kHalo;
         const int kz = band(gz, m.nz, m.pml);
 
-        if (!mbar_wait(&bar[s], parity)) failed = true;
+        if (mbar_wait(&bar[s], (pbits >> s) & 1u)) pbits ^= 1u << s;
+        else failed = true;
 
         // source patch of the staged copies (uniform branch)
         if (GEN && src_near && (gz == sz || gz + 5 == sz)) {
@@ -483,10 +479,7 @@ k_velocity_zpair(const __grid_constant__ VelMaps mp, const __grid_constant__ Mod
             }
             issued_end = cz + S + 1;
         }
-        if (++stage == S) {
-            stage = 0;
-            parity ^= 1u;
-        }
+        if (++stage == S) stage = 0;
         return true;
     };
     for (; cz < t.ze; ++cz) {
@@ -500,42 +493,45 @@ k_velocity_zpair(const __grid_constant__ VelMaps mp, const __grid_constant__ Mod
     }
     if (abort && tid == 0) {
         atomicExch(g.err, 1);
-        drain<S>(bar, issued_end, cz, t.zs);
+        // planes still in flight: [cz, issued_end), less plane cz when this
+        // thread's own wait for it completed
+        for (int j = failed ? cz : cz + 1; j < issued_end; ++j) {
+            const int q = (j - t.zs) % S;
+            mbar_wait(&bar[q], (pbits >> q) & 1u);
+            pbits ^= 1u << q;
+        }
     }
+    return !abort;
 }
 
 // ---------------------------------------------------------------------------
 // stress update
 // ---------------------------------------------------------------------------
 
+// One work item of the str update: tile `tile`, z chunk `chunk`.  The
+// ring's barriers (bar, S of them) are initialised by the caller; pbits holds
+// the parity of the next wait of each stage and carries over between the
+// work items of a persistent caller.  Returns false when the block gave up
+// on a wait (after waiting, bounded, for its own copies still in flight).
 template <bool FAST>
-__global__ void __launch_bounds__(NT, 2)
-k_stress_zpair(const __grid_constant__ StrMaps mp, const __grid_constant__ Model m, const __grid_constant__ Physics ph,
-               const __grid_constant__ ZGeom g, const __grid_constant__ SourceRec sr, int it_arg, float src_value,
-               int use_wavelet) {
+__device__ __forceinline__ bool str_pair(const StrMaps &mp, const Model &m, const Physics &ph, const ZGeom &g,
+                                        const SourceRec &sr, int it_arg, float src_value, int use_wavelet, int tile,
+                                        int chunk, unsigned char *smem, uint64_t *bar,
+                                        TmaBox (*boxes)[kMaxBoxesPerWarp], uint32_t &pbits) {
     using L = StrP;
     constexpr int S = SS;
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    unsigned char *smem = align_smem(smem_raw);
-    __shared__ __align__(8) uint64_t bar[S];
-    __shared__ TmaBox boxes[kWarps][kMaxBoxesPerWarp];
-    const PTile t = make_ptile(m, g);
+    const PTile t = make_ptile(m, g, tile, chunk);
     const int tid = threadIdx.x, lx = tid & 31, ly = tid >> 5, warp = ly;
-    if (tid == 0) {
-        for (int s = 0; s < S; ++s) mbar_init(&bar[s], 1);
-        fence_barrier_init();
-    }
-    __syncthreads();
     const TmaBox *mybox = boxes[warp];
     const int nbox = (kStrBoxes - warp + kWarps - 1) / kWarps;
     if (lx == 0) {
+        fence_proxy_async();
         for (int j = 0; j < nbox; ++j) boxes[warp][j] = str_box(mp, t, warp + j * kWarps);
         for (int s = 0; s < S && t.zs + s < t.ze; ++s)
             issue(mybox, nbox, smem + s * L::STAGE, &bar[s], t.zs + s, warp, L::TXB);
     }
     int issued_end = min(t.zs + S, t.ze);
-    int stage = 0;
-    uint32_t parity = 0;
+    int stage = 0;                          // stage of plane cz
 
     const int it = step_index(sr, it_arg);
     const float inj = ph.inj_dt2 * ((use_wavelet && sr.wavelet) ? sr.wavelet[it] : src_value);
@@ -553,8 +549,8 @@ k_stress_zpair(const __grid_constant__ StrMaps mp, const __grid_constant__ Model
         qz[k + 1] = ld2(m.f[2] + pc.col + (uint32_t)(gz0 - 5 + k) * PL);
     }
 
-    int rp = g.rec_off[blockIdx.x];
-    const int rend = g.rec_off[blockIdx.x + 1];
+    int rp = g.rec_off[tile];
+    const int rend = g.rec_off[tile + 1];
     while (rp < rend && g.rec_list[rp].z < gz0) ++rp;
     int rz = rp < rend ? g.rec_list[rp].z : 0x7fffffff;
 
@@ -568,7 +564,8 @@ k_stress_zpair(const __grid_constant__ StrMaps mp, const __grid_constant__ Model
         const int gz = cz + kHalo;
         const int kz = band(gz, m.nz, m.pml);
 
-        if (!mbar_wait(&bar[s], parity)) failed = true;
+        if (mbar_wait(&bar[s], (pbits >> s) & 1u)) pbits ^= 1u << s;
+        else failed = true;
 
         const float *svx = reinterpret_cast<const float *>(st + L::VX);
         const float *svy = reinterpret_cast<const float *>(st + L::VY);
@@ -721,10 +718,7 @@ k_stress_zpair(const __grid_constant__ StrMaps mp, const __grid_constant__ Model
             }
             issued_end = cz + S + 1;
         }
-        if (++stage == S) {
-            stage = 0;
-            parity ^= 1u;
-        }
+        if (++stage == S) stage = 0;
         return true;
     };
     for (; cz < t.ze; ++cz) {
@@ -737,7 +731,135 @@ k_stress_zpair(const __grid_constant__ StrMaps mp, const __grid_constant__ Model
     }
     if (abort && tid == 0) {
         atomicExch(g.err, 1);
-        drain<S>(bar, issued_end, cz, t.zs);
+        // planes still in flight: [cz, issued_end), less plane cz when this
+        // thread's own wait for it completed
+        for (int j = failed ? cz : cz + 1; j < issued_end; ++j) {
+            const int q = (j - t.zs) % S;
+            mbar_wait(&bar[q], (pbits >> q) & 1u);
+            pbits ^= 1u << q;
+        }
+    }
+    return !abort;
+}
+
+// One launch per update: one CTA per (tile, z chunk).
+template <bool FAST>
+__global__ void __launch_bounds__(NT, 2)
+k_velocity_zpair(const __grid_constant__ VelMaps mp, const __grid_constant__ Model m, const __grid_constant__ Physics ph,
+                 const __grid_constant__ ZGeom g, const __grid_constant__ SourceRec sr, int it_arg, float src_value,
+                 int use_wavelet) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t bar[SV];
+    __shared__ TmaBox boxes[kWarps][kMaxBoxesPerWarp];
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < SV; ++s) mbar_init(&bar[s], 1);
+        fence_barrier_init();
+    }
+    __syncthreads();
+    uint32_t pbits = 0;
+    vel_pair<FAST>(mp, m, ph, g, sr, it_arg, src_value, use_wavelet, blockIdx.x, blockIdx.y, align_smem(smem_raw), bar,
+                   boxes, pbits);
+}
+
+template <bool FAST>
+__global__ void __launch_bounds__(NT, 2)
+k_stress_zpair(const __grid_constant__ StrMaps mp, const __grid_constant__ Model m, const __grid_constant__ Physics ph,
+               const __grid_constant__ ZGeom g, const __grid_constant__ SourceRec sr, int it_arg, float src_value,
+               int use_wavelet) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t bar[SS];
+    __shared__ TmaBox boxes[kWarps][kMaxBoxesPerWarp];
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < SS; ++s) mbar_init(&bar[s], 1);
+        fence_barrier_init();
+    }
+    __syncthreads();
+    uint32_t pbits = 0;
+    str_pair<FAST>(mp, m, ph, g, sr, it_arg, src_value, use_wavelet, blockIdx.x, blockIdx.y, align_smem(smem_raw), bar,
+                   boxes, pbits);
+}
+
+// ---------------------------------------------------------------------------
+// persistent batch: every model's work items, both updates, nsteps steps
+// ---------------------------------------------------------------------------
+
+constexpr uint32_t kGridWaitCap = 1u << 20;   // polls of about 1 us: a grid barrier gives up after ~1 s
+
+__device__ __forceinline__ unsigned ld_acquire(const unsigned *p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// All CTAs of the launch meet here: arrivals are counted in *arrive, and
+// this barrier completes when `target` arrivals have been counted.  Bounded:
+// false (and *status = kBatchWaitGrid) when the count does not arrive.  The
+// fences make the other CTAs' stores of the finished phase visible to this
+// CTA's later loads, TMA (async proxy) included.
+__device__ __forceinline__ bool grid_sync(unsigned *arrive, unsigned target, int *status, int *ok_sh) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        atomicAdd(arrive, 1u);
+        bool ok = true;
+        for (uint32_t n = 0; ld_acquire(arrive) < target; ++n) {
+            if (n >= kGridWaitCap) { ok = false; break; }
+            __nanosleep(1000);
+        }
+        __threadfence();
+        asm volatile("fence.proxy.async.global;" ::: "memory");
+        if (!ok) atomicExch(status, kBatchWaitGrid);
+        *ok_sh = ok;
+    }
+    __syncthreads();
+    return *ok_sh != 0;
+}
+
+template <bool FAST>
+__global__ void __launch_bounds__(NT, 2)
+k_batch_zpair(const PairModel *models, int nmodels, const int *first_item, int it0, int nsteps, unsigned *ctl,
+              unsigned barrier_ctas, int *status) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t bar_v[SV];
+    __shared__ __align__(8) uint64_t bar_s[SS];
+    __shared__ TmaBox boxes[kWarps][kMaxBoxesPerWarp];
+    __shared__ int item_sh, ok_sh;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < SV; ++s) mbar_init(&bar_v[s], 1);
+        for (int s = 0; s < SS; ++s) mbar_init(&bar_s[s], 1);
+        fence_barrier_init();
+    }
+    __syncthreads();
+    unsigned char *smem = align_smem(smem_raw);
+    uint32_t pv = 0, ps = 0;
+    const int total = first_item[nmodels];
+    unsigned phases = 0;
+    for (int k = 0; k < nsteps; ++k) {
+        for (int p = 0; p < 2; ++p) {
+            unsigned *ctr = ctl + 1 + 2 * k + p;
+            for (;;) {
+                if (threadIdx.x == 0) item_sh = (int)atomicAdd(ctr, 1u);
+                __syncthreads();
+                const int item = item_sh;
+                __syncthreads();
+                if (item >= total) break;
+                int mi = 0;
+                while (first_item[mi + 1] <= item) ++mi;
+                const PairModel &d = models[mi];
+                const int local = item - first_item[mi];
+                const int ntiles = d.g.ntx * d.g.nty;
+                const bool ok = p == 0 ? vel_pair<FAST>(d.vm, d.m, d.ph, d.g, d.sr, it0 + k, 0.0f, 1, local % ntiles,
+                                                        local / ntiles, smem, bar_v, boxes, pv)
+                                       : str_pair<FAST>(d.sm, d.m, d.ph, d.g, d.sr, it0 + k, 0.0f, 1, local % ntiles,
+                                                        local / ntiles, smem, bar_s, boxes, ps);
+                if (!ok) {
+                    if (threadIdx.x == 0) atomicExch(status, kBatchWaitTma);
+                    return;
+                }
+            }
+            ++phases;
+            if (!grid_sync(ctl, phases * barrier_ctas, status, &ok_sh)) return;
+        }
     }
 }
 
@@ -766,7 +888,34 @@ void launch(const Model &m, const Physics &ph, const SourceRec &sr, const ZGeom 
     if (ev) cudaEventRecord(ev[3], s);
 }
 
+constexpr int batch_smem() { return vel_smem() > str_smem() ? vel_smem() : str_smem(); }
+
 }  // namespace
+
+int zpair_batch_ctas(int device) {
+    int sms = 0, per = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return 0;
+    if (cudaFuncSetAttribute(k_batch_zpair<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, batch_smem()) !=
+            cudaSuccess ||
+        cudaFuncSetAttribute(k_batch_zpair<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, batch_smem()) !=
+            cudaSuccess)
+        return 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_batch_zpair<true>, NT, batch_smem()) != cudaSuccess)
+        return 0;
+    int per2 = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per2, k_batch_zpair<false>, NT, batch_smem()) != cudaSuccess)
+        return 0;
+    return sms * (per < per2 ? per : per2);
+}
+
+cudaError_t zpair_batch_run(const PairModel *models, int nmodels, const int *first_item, int it0, int nsteps,
+                            unsigned *ctl, int barrier_ctas, int ctas, bool fast, int *status, cudaStream_t s) {
+    unsigned target = (unsigned)barrier_ctas;
+    void *args[] = {(void *)&models, (void *)&nmodels, (void *)&first_item, (void *)&it0, (void *)&nsteps,
+                    (void *)&ctl, (void *)&target, (void *)&status};
+    const void *fn = fast ? (const void *)k_batch_zpair<true> : (const void *)k_batch_zpair<false>;
+    return cudaLaunchCooperativeKernel(fn, dim3(ctas), dim3(NT), args, batch_smem(), s);
+}
 
 cudaError_t zpair_prepare(const Model &m, VelMaps *vm, StrMaps *sm) {
     constexpr int ty = PY;

@@ -51,11 +51,37 @@ void zmarch_tiles(const Model &m, int cells, int *ntx, int *nty);
 cudaError_t zmarch_step(const Model &m, const Physics &ph, const SourceRec &sr, const ZGeom &g,
                         const VelMaps &vm, const StrMaps &sm, int it, float src_value, bool use_wavelet,
                         cudaStream_t s, cudaEvent_t *ev = nullptr);
+// One model of a persistent batch, in device memory (the kernel's TMA reads
+// its tensor maps from there: 64-byte alignment).  Its work items are the
+// (tile, z chunk) pairs of the paired tiling, tile fastest.
+struct alignas(64) PairModel {
+    VelMaps vm;
+    StrMaps sm;
+    Model m;
+    Physics ph;
+    ZGeom g;
+    SourceRec sr;       // it_dev null: the kernel passes the step index
+    int items;          // tiles x z chunks
+};
+// Status words of a persistent batch launch (device int): 1 a TMA wait gave
+// up (the model's own flag is set too), 2 a grid barrier wait gave up.
+constexpr int kBatchWaitTma = 1, kBatchWaitGrid = 2;
+
 // Paired tiling: tensor maps, tile counts and one step (velocity + stress).
 cudaError_t zpair_prepare(const Model &m, VelMaps *vm, StrMaps *sm);
 void zpair_tiles(const Model &m, int *ntx, int *nty);
 cudaError_t zpair_step(const Model &m, const Physics &ph, const SourceRec &sr, const ZGeom &g, const VelMaps &vm,
                        const StrMaps &sm, int it, float src_value, bool use_wavelet, cudaStream_t s,
                        cudaEvent_t *ev = nullptr);
+// Persistent batch: CTAs that fit at once on the device (cooperative launch),
+// and nsteps steps of all models in one launch.  first_item[nmodels + 1]:
+// prefix sums of the models' items; ctl: 1 + 2 * nsteps zeroed counters
+// (grid-barrier arrivals, then one work counter per step and phase); each
+// grid barrier waits for barrier_ctas arrivals (the launched CTAs unless a
+// caller asks otherwise), at most about a second, then the launch stops with
+// *status = kBatchWaitGrid.  All models FAST or all REF (fast).
+int zpair_batch_ctas(int device);
+cudaError_t zpair_batch_run(const PairModel *models, int nmodels, const int *first_item, int it0, int nsteps,
+                            unsigned *ctl, int barrier_ctas, int ctas, bool fast, int *status, cudaStream_t s);
 
 }  // namespace sgfd

@@ -133,6 +133,7 @@ def lib() -> ctypes.CDLL:
         "sgfd_batch_synchronize": (ctypes.c_int, [vp]),
         "sgfd_batch_stream": (vp, [vp]),
         "sgfd_batch_run_launches": (ctypes.c_int, [vp, i32]),
+        "sgfd_batch_set_persistent": (ctypes.c_int, [vp, i32, i32]),
         "sgfd_set_audit": (ctypes.c_int, [vp, i32, i32, i32]),
         "sgfd_get_audit": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_double)]),
         "sgfd_energy_noalloc": (ctypes.c_int, [vp, i32, i32, ctypes.POINTER(ctypes.c_double),
@@ -479,7 +480,8 @@ def checkpoint_checksum(payload: bytes) -> int:
 
 class Batch:
     """Several Solver models advanced together (sgfd_batch_*): one CUDA graph per
-    16 steps with every model's kernels in parallel branches."""
+    16 steps with every model's kernels in parallel branches, or (set_persistent)
+    one persistent launch per run over all models' work items."""
 
     def __init__(self, models):
         self.models = list(models)
@@ -496,6 +498,12 @@ class Batch:
 
     def run(self, it0: int, nsteps: int):
         self._check(lib().sgfd_batch_run(self.h, it0, nsteps))
+
+    def set_persistent(self, on: bool = True, barrier_ctas: int = 0):
+        """One cooperative launch per run over every model's (tile, z chunk)
+        work items, with a bounded grid barrier between the velocity and stress
+        phases (barrier_ctas: arrivals each barrier waits for, 0 = launched)."""
+        self._check(lib().sgfd_batch_set_persistent(self.h, 1 if on else 0, barrier_ctas))
 
     def synchronize(self):
         self._check(lib().sgfd_batch_synchronize(self.h))

@@ -48,6 +48,77 @@ def test_batch_equals_solo_runs(split):
             m.close()
 
 
+@pytest.mark.parametrize("split", [False, True], ids=["one_run", "split_runs"])
+def test_persistent_batch_equals_solo_runs(split):
+    """Persistent mode: one cooperative launch per run over every model's
+    (tile, z chunk) work items; every model ends bit for bit where it ends
+    alone, and a run is one launch."""
+    ws = _models()
+    solo, members = [], []
+    try:
+        for w in ws:
+            s = make_solver(w)
+            s.run(0, w.nt)
+            s.synchronize()
+            solo.append((s.traces(), [s.field(k) for k in range(9)]))
+            s.close()
+            members.append(make_solver(w))
+        with sgfd.Batch(members) as b:
+            b.set_persistent(True)
+            assert all(m.tile()[:2] == (64, 8) for m in members)
+            if split:
+                for it0, n in ((0, 20), (20, 1), (21, 24)):
+                    b.run(it0, n)
+            else:
+                b.run(0, 45)
+                assert b.run_launches(45) == 1
+            b.synchronize()
+            for m, (tr, fields) in zip(members, solo):
+                np.testing.assert_array_equal(m.traces(), tr)
+                for k in range(9):
+                    np.testing.assert_array_equal(m.field(k), fields[k], err_msg=sgfd.FIELD_NAMES[k])
+    finally:
+        for m in members:
+            m.close()
+
+
+def test_persistent_batch_grid_barrier_wait_is_bounded():
+    """A grid barrier that cannot complete (each barrier told to wait for more
+    arrivals than there are CTAs) gives up after about a second: the launch
+    ends, sgfd_batch_synchronize reports it, and the context stays usable —
+    the same batch then runs correctly."""
+    ws = _models()[:2]
+    members = [make_solver(w) for w in ws]
+    try:
+        with sgfd.Batch(members) as b:
+            b.set_persistent(True, barrier_ctas=1 << 20)
+            b.run(0, 3)
+            with pytest.raises(sgfd.SgfdError) as e:
+                b.synchronize()
+            assert "grid-barrier" in str(e.value)
+            for m in members:
+                m.reset()
+            b.set_persistent(True)
+            b.run(0, 10)
+            b.synchronize()
+            for w, m in zip(ws, members):
+                with make_solver(w) as s:
+                    s.run(0, 10)
+                    s.synchronize()
+                    np.testing.assert_array_equal(m.traces()[:, :10], s.traces()[:, :10])
+                    np.testing.assert_array_equal(m.field(sgfd.TXX), s.field(sgfd.TXX))
+    finally:
+        for m in members:
+            m.close()
+
+
+def test_persistent_batch_rejects_unsupported_models():
+    w = _models()[0]
+    with make_solver(w, kernel=sgfd.KERNEL_SIMPLE) as s, sgfd.Batch([s]) as b:
+        with pytest.raises(sgfd.SgfdError):
+            b.set_persistent(True)
+
+
 def test_batch_rejects_bad_input():
     w = _models()[0]
     with make_solver(w) as s:
