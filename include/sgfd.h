@@ -107,8 +107,9 @@ typedef enum sgfd_quirks {
  * +-65504), halving the wavefield bytes.  The scales are re-chosen after steps
  * 0, 1, 3, 7, 15, 31, 49 and then every 50 steps from the largest magnitude
  * each field wrote in that step, so that it is stored near 2^7.  16-bit storage
- * runs on the per-cell kernel family (SGFD_KERNEL_ZMARCH is rejected), and
- * the per-step audit (sgfd_set_audit) is not available with it. */
+ * runs on the z-marching kernels with 64 x 8 tiles (16-bit boxes staged by
+ * TMA) or, with SGFD_KERNEL_SIMPLE, on the per-cell kernels; both give the
+ * same bits.  The per-step audit (sgfd_set_audit) is not available with it. */
 typedef enum sgfd_storage {
     SGFD_STORE_F32 = 0,
     SGFD_STORE_BF16 = 1,

@@ -234,7 +234,7 @@ int sgfd_autotune(sgfd_solver *h, int32_t probe_steps, sgfd_tuning *out) {
     struct Cand { int kernel, cols, rows, zchunk; };
     std::vector<Cand> cands;
     if (h->dev_err) {
-        for (int shape = 0; shape < 3; ++shape)
+        for (int shape = h->storage == SGFD_STORE_F32 ? 0 : 2; shape < 3; ++shape)   // 16-bit: 64 x 8 only
             for (int zc : {0, 16, 32, 64})
                 if (zc == 0 || zc < h->m.nzc)
                     cands.push_back({SGFD_KERNEL_ZMARCH, shape == 2 ? kPairTileX : kZTileX, shape == 1 ? 16 : 8, zc});

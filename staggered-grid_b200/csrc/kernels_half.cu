@@ -342,7 +342,29 @@ cudaError_t step16(const Model &m, const Physics &ph, const SourceRec &sr, const
     return cudaGetLastError();
 }
 
+template <int ST>
+cudaError_t phases16(const Model &m, const Physics &ph, const SourceRec &sr, const HalfState &hs, int it,
+                     float src_value, bool use_wavelet, cudaStream_t s, int phase) {
+    if (phase == 0) {
+        if (sr.src >= 0) k_inject16<ST><<<1, 32, 0, s>>>(m, ph, sr, hs, it, src_value, use_wavelet ? 1 : 0);
+    } else if (phase == 1) {
+        if (sr.nrec > 0) k_record16<ST><<<(sr.nrec + 127) / 128, 128, 0, s>>>(m, sr, hs, it, 1);
+    } else {
+        if (sr.nrec > 0) k_record16<ST><<<(sr.nrec + 127) / 128, 128, 0, s>>>(m, sr, hs, it, 0);
+        k_rescale_choose<<<1, 32, 0, s>>>(sr, hs, it);
+        k_rescale_apply<ST><<<1184, 256, 0, s>>>(m, sr, hs, it, m.plane * m.nz);
+        k_rescale_commit<<<1, 32, 0, s>>>(sr, hs, it);
+    }
+    return cudaGetLastError();
+}
+
 }  // namespace
+
+cudaError_t half_phase(const Model &m, const Physics &ph, const SourceRec &sr, const HalfState &hs, int it,
+                       float src_value, bool use_wavelet, cudaStream_t s, int phase) {
+    return hs.storage == SGFD_STORE_BF16 ? phases16<SGFD_STORE_BF16>(m, ph, sr, hs, it, src_value, use_wavelet, s, phase)
+                                         : phases16<SGFD_STORE_F16>(m, ph, sr, hs, it, src_value, use_wavelet, s, phase);
+}
 
 cudaError_t half_step(const Model &m, const Physics &ph, const SourceRec &sr, const HalfState &hs, int it,
                       float src_value, bool use_wavelet, cudaStream_t s, cudaEvent_t *ev) {

@@ -814,6 +814,20 @@ bool make_box_map(CUtensorMap *map, const float *grid_origin, const Model &m, in
     return r == CUDA_SUCCESS;
 }
 
+bool make_box_map16(CUtensorMap *map, const uint16_t *grid_origin, const Model &m, int bx, int by) {
+    auto enc = get_encoder();
+    if (!enc) return false;
+    void *base = const_cast<uint16_t *>(grid_origin - kXOff);
+    cuuint64_t dims[3] = {(cuuint64_t)(m.nx + kXOff), (cuuint64_t)m.ny, (cuuint64_t)m.nz};
+    cuuint64_t strides[2] = {(cuuint64_t)m.px * 2, (cuuint64_t)m.plane * 2};
+    cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, 1};
+    cuuint32_t es[3] = {1, 1, 1};
+    CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_UINT16, 3, base, dims, strides, box, es,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
 bool zmarch_supported(const Model &m) {
     // Halo boxes start 8 cells left of the tile and 5 rows above: always inside
     // the padded array because the frame is 5 cells and kXOff is 27.  The

@@ -27,6 +27,10 @@
 
 #include <type_traits>
 
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include "../../include/sgfd.h"
 #include "cell_math.cuh"
 #include "zmarch.h"
 #include "zmarch_dev.cuh"
@@ -46,37 +50,45 @@ constexpr int SV = 3;            // velocity ring stages
 constexpr int SS = 2;            // stress ring stages
 
 constexpr int al128(int b) { return (b + 127) / 128 * 128; }
-constexpr int OB = al128(PX * PY * 4);   // one 64 x 8 FP32 box
+constexpr int OB = al128(PX * PY * 4);   // one 64 x 8 FP32 box (medium)
 
-// Shared-memory stage of the velocity update (byte offsets, 128-aligned boxes).
+// Shared-memory stage of the velocity update (byte offsets, 128-aligned
+// boxes); wavefield boxes hold ES-byte values (4: FP32, 2: 16-bit storage),
+// the buoyancy boxes FP32.
+template <int ES>
 struct VelP {
+    static constexpr int OBE = al128(PX * PY * ES);                // one 64 x 8 wavefield box
     static constexpr int SXX = 0;                                  // XW x PY        sigma_xx (x halo)
-    static constexpr int SYY = SXX + al128(XW * PY * 4);           // PX x (PY+10)   sigma_yy (y halo)
-    static constexpr int SXY = SYY + al128(PX * (PY + 10) * 4);    // XW x (PY+10)   sigma_xy (x, y halo)
-    static constexpr int SXZ = SXY + al128(XW * (PY + 10) * 4);    // XW x PY        sigma_xz (x halo)
-    static constexpr int SYZ = SXZ + al128(XW * PY * 4);           // PX x (PY+10)   sigma_yz (y halo)
-    static constexpr int B = SYZ + al128(PX * (PY + 10) * 4);      // BW x (PY+1)    buoyancy (x+1, y+1)
+    static constexpr int SYY = SXX + al128(XW * PY * ES);          // PX x (PY+10)   sigma_yy (y halo)
+    static constexpr int SXY = SYY + al128(PX * (PY + 10) * ES);   // XW x (PY+10)   sigma_xy (x, y halo)
+    static constexpr int SXZ = SXY + al128(XW * (PY + 10) * ES);   // XW x PY        sigma_xz (x halo)
+    static constexpr int SYZ = SXZ + al128(XW * PY * ES);          // PX x (PY+10)   sigma_yz (y halo)
+    static constexpr int B = SYZ + al128(PX * (PY + 10) * ES);     // BW x (PY+1)    buoyancy (x+1, y+1)
     static constexpr int LXZ = B + al128(BW * (PY + 1) * 4);       // sigma_xz at z+4
-    static constexpr int LYZ = LXZ + OB;                           // sigma_yz at z+4
-    static constexpr int LZZ = LYZ + OB;                           // sigma_zz at z+5
-    static constexpr int LB = LZZ + OB;                            // buoyancy at z+1
+    static constexpr int LYZ = LXZ + OBE;                          // sigma_yz at z+4
+    static constexpr int LZZ = LYZ + OBE;                          // sigma_zz at z+5
+    static constexpr int LB = LZZ + OBE;                           // buoyancy at z+1
     static constexpr int OV = LB + OB;                             // own vx, vy, vz at z
-    static constexpr int STAGE = OV + 3 * OB;
-    static constexpr uint32_t TXB = 4 * (2 * XW * PY + 2 * PX * (PY + 10) + XW * (PY + 10) + BW * (PY + 1) +
-                                         7 * PX * PY);
+    static constexpr int STAGE = OV + 3 * OBE;
+    static constexpr uint32_t TXB = ES * (2 * XW * PY + 2 * PX * (PY + 10) + XW * (PY + 10) + 6 * PX * PY) +
+                                    4 * (BW * (PY + 1) + PX * PY);
 };
 // Shared-memory stage of the stress update.
+template <int ES>
 struct StrP {
+    static constexpr int OBE = al128(PX * PY * ES);
     static constexpr int VX = 0;                                   // XW x (PY+10)  vx (x, y halo)
-    static constexpr int VY = VX + al128(XW * (PY + 10) * 4);
-    static constexpr int VZ = VY + al128(XW * (PY + 10) * 4);
-    static constexpr int LX = VZ + al128(XW * (PY + 10) * 4);      // vx at z+5
-    static constexpr int LY = LX + OB;                             // vy at z+5
-    static constexpr int LZ = LY + OB;                             // vz at z+4
-    static constexpr int OWN = LZ + OB;                            // txx..tyz, lambda, mu, mxy, mxz, myz at z
-    static constexpr int NOWN = 11;
-    static constexpr int STAGE = OWN + NOWN * OB;
-    static constexpr uint32_t TXB = 4 * (3 * XW * (PY + 10) + (3 + NOWN) * PX * PY);
+    static constexpr int VY = VX + al128(XW * (PY + 10) * ES);
+    static constexpr int VZ = VY + al128(XW * (PY + 10) * ES);
+    static constexpr int LX = VZ + al128(XW * (PY + 10) * ES);     // vx at z+5
+    static constexpr int LY = LX + OBE;                            // vy at z+5
+    static constexpr int LZ = LY + OBE;                            // vz at z+4
+    static constexpr int OWN = LZ + OBE;                           // txx..tyz at z
+    static constexpr int MED = OWN + 6 * OBE;                      // lambda, mu, mxy, mxz, myz at z
+    static constexpr int STAGE = MED + 5 * OB;
+    static constexpr uint32_t TXB = ES * (3 * XW * (PY + 10) + 9 * PX * PY) + 4 * 5 * PX * PY;
+    // byte offset of own-cell box q (0..5 stresses, 6..10 medium)
+    static constexpr uint32_t own(int q) { return q < 6 ? OWN + q * OBE : MED + (q - 6) * OB; }
 };
 
 struct PTile {
@@ -110,8 +122,9 @@ constexpr int kMaxBoxesPerWarp = 3;
 constexpr int kVelBoxes = 13;
 constexpr int kStrBoxes = 17;
 
+template <int ES>
 __device__ __forceinline__ TmaBox vel_box(const VelMaps &mp, const PTile &t, int q) {
-    using L = VelP;
+    using L = VelP<ES>;
     switch (q) {
     case 0: return {&mp.sxx, L::SXX, t.xd - 8, t.gy0, 0};
     case 1: return {&mp.syy, L::SYY, t.xd, t.gy0 - 5, 0};
@@ -124,13 +137,14 @@ __device__ __forceinline__ TmaBox vel_box(const VelMaps &mp, const PTile &t, int
     case 8: return {&mp.szz_c, L::LZZ, t.xd, t.gy0, 5};
     case 9: return {&mp.b_c, L::LB, t.xd, t.gy0, 1};
     case 10: return {&mp.own[0], L::OV, t.xd, t.gy0, 0};
-    case 11: return {&mp.own[1], L::OV + OB, t.xd, t.gy0, 0};
-    default: return {&mp.own[2], L::OV + 2 * OB, t.xd, t.gy0, 0};
+    case 11: return {&mp.own[1], L::OV + L::OBE, t.xd, t.gy0, 0};
+    default: return {&mp.own[2], L::OV + 2 * L::OBE, t.xd, t.gy0, 0};
     }
 }
 
+template <int ES>
 __device__ __forceinline__ TmaBox str_box(const StrMaps &mp, const PTile &t, int q) {
-    using L = StrP;
+    using L = StrP<ES>;
     switch (q) {
     case 0: return {&mp.vx, L::VX, t.xd - 8, t.gy0 - 5, 0};
     case 1: return {&mp.vy, L::VY, t.xd - 8, t.gy0 - 5, 0};
@@ -138,7 +152,7 @@ __device__ __forceinline__ TmaBox str_box(const StrMaps &mp, const PTile &t, int
     case 3: return {&mp.vx_c, L::LX, t.xd, t.gy0, 5};
     case 4: return {&mp.vy_c, L::LY, t.xd, t.gy0, 5};
     case 5: return {&mp.vz_c, L::LZ, t.xd, t.gy0, 4};
-    default: return {&mp.own[q - 6], L::OWN + (uint32_t)(q - 6) * OB, t.xd, t.gy0, 0};
+    default: return {&mp.own[q - 6], L::own(q - 6), t.xd, t.gy0, 0};
     }
 }
 
@@ -204,6 +218,95 @@ __device__ __forceinline__ T pick6(const T (&a)[6], int k) {
     return k == 0 ? a[0] : k == 1 ? a[1] : k == 2 ? a[2] : k == 3 ? a[3] : k == 4 ? a[4] : a[5];
 }
 
+__device__ __forceinline__ void st2(float *p, float2 v, bool both) {
+    if (both) *reinterpret_cast<float2 *>(p) = v;
+    else *p = v.x;
+}
+
+// Wavefield storage as the pair kernels see it.  FP32: the arrays as they
+// are.  BF16 / F16 (the 16-bit storage of kernels_half.cu): value h of field
+// g reads back as float(h) * 2^e_g and v is stored as RN16(v * 2^-e_g), F16
+// saturating at +-65504; the same roundings as kernels_half.cu and the oracle.
+template <int ST>
+struct Sto {
+    using E = float;
+    static constexpr int ES = 4;
+    __device__ static float2 pair(const E *p, float2) { return ld2(p); }
+    __device__ static float one(const E *p, float) { return *p; }
+    __device__ static void win(const E *row, float (&w)[12], float) { window(row, w); }
+    __device__ static void put2(E *p, float2 v, float2, bool both) { st2(p, v, both); }
+    __device__ static void put1(E *p, float v, float) { *p = v; }
+};
+template <int ST>
+struct Sto16 {
+    using E = uint16_t;
+    static constexpr int ES = 2;
+    __device__ static float h2f(uint32_t h) {
+        if (ST == SGFD_STORE_BF16) return __uint_as_float(h << 16);
+        return __half2float(__ushort_as_half((unsigned short)h));
+    }
+    __device__ static uint32_t f2h(float w) {
+        if (ST == SGFD_STORE_BF16) return __bfloat16_as_ushort(__float2bfloat16_rn(w));
+        return __half_as_ushort(__float2half_rn(fminf(fmaxf(w, -65504.0f), 65504.0f)));
+    }
+    __device__ static float2 pair(const E *p, float2 sc) {
+        const uint32_t u = *reinterpret_cast<const uint32_t *>(p);
+        return make_float2(h2f(u & 0xffffu) * sc.x, h2f(u >> 16) * sc.y);
+    }
+    __device__ static float one(const E *p, float sc) { return h2f(*p) * sc; }
+    __device__ static void win(const E *row, float (&w)[12], float sc) {
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            const float2 v = pair(row + 2 * k, make_float2(sc, sc));
+            w[2 * k] = v.x;
+            w[2 * k + 1] = v.y;
+        }
+    }
+    __device__ static void put2(E *p, float2 v, float2 inv, bool both) {
+        const float2 q = __fmul2_rn(v, inv);
+        if (both) *reinterpret_cast<uint32_t *>(p) = f2h(q.x) | (f2h(q.y) << 16);
+        else *p = (E)f2h(q.x);
+    }
+    __device__ static void put1(E *p, float v, float inv) { *p = (E)f2h(v * inv); }
+};
+template <> struct Sto<SGFD_STORE_BF16> : Sto16<SGFD_STORE_BF16> {};
+template <> struct Sto<SGFD_STORE_F16> : Sto16<SGFD_STORE_F16> {};
+
+// The wavefield arrays, split array and scales of either storage (read
+// where used: the pointers live in the kernel parameters, the 16-bit scales
+// in device memory, re-chosen between steps).
+template <int ST>
+struct Fields {
+    using E = typename Sto<ST>::E;
+    const Model &m;
+    const HalfState &hs;
+    __device__ Fields(const Model &m_, const HalfState &hs_) : m(m_), hs(hs_) {}
+    __device__ E *f(int k) const {
+        if constexpr (ST == SGFD_STORE_F32) return m.f[k];
+        else return hs.f[k];
+    }
+    __device__ E *split() const {
+        if constexpr (ST == SGFD_STORE_F32) return m.split;
+        else return hs.split;
+    }
+    __device__ float sc(int k) const {
+        if constexpr (ST == SGFD_STORE_F32) return 1.0f;
+        else return __ldg(hs.sc + k);
+    }
+    __device__ float inv(int k) const {
+        if constexpr (ST == SGFD_STORE_F32) return 1.0f;
+        else return __ldg(hs.inv + k);
+    }
+};
+
+// Largest |v| of the warp's active lanes into field g's running maximum (the
+// rescale steps of 16-bit storage, as kernels_half.cu notes them).
+__device__ __forceinline__ void note_max16(const HalfState &hs, int g, float v) {
+    const unsigned mask = __activemask();
+    const unsigned bits = __reduce_max_sync(mask, __float_as_uint(fabsf(v)));
+    if ((threadIdx.x & 31) == __ffs(mask) - 1) atomicMax(hs.amax + g, bits);
+}
+
 // Common per-thread state of both updates.
 struct PairCtx {
     int gx, gy;          // GRID coordinates of cell 0
@@ -230,10 +333,6 @@ __device__ __forceinline__ PairCtx pair_ctx(const Model &m, const PTile &t, int 
     return p;
 }
 
-__device__ __forceinline__ void st2(float *p, float2 v, bool both) {
-    if (both) *reinterpret_cast<float2 *>(p) = v;
-    else *p = v.x;
-}
 
 // ---------------------------------------------------------------------------
 // velocity update
@@ -244,20 +343,24 @@ __device__ __forceinline__ void st2(float *p, float2 v, bool both) {
 // the parity of the next wait of each stage and carries over between the
 // work items of a persistent caller.  Returns false when the block gave up
 // on a wait (after waiting, bounded, for its own copies still in flight).
-template <bool FAST>
+template <bool FAST, int ST>
 __device__ __forceinline__ bool vel_pair(const VelMaps &mp, const Model &m, const Physics &ph, const ZGeom &g,
-                                        const SourceRec &sr, int it_arg, float src_value, int use_wavelet, int tile,
-                                        int chunk, unsigned char *smem, uint64_t *bar,
+                                        const SourceRec &sr, const HalfState &hs, int it_arg, float src_value,
+                                        int use_wavelet, int tile, int chunk, unsigned char *smem, uint64_t *bar,
                                         TmaBox (*boxes)[kMaxBoxesPerWarp], uint32_t &pbits) {
-    using L = VelP;
+    using SA = Sto<ST>;
+    using E = typename SA::E;
+    using L = VelP<SA::ES>;
     constexpr int S = SV;
+    constexpr bool H = ST != SGFD_STORE_F32;   // 16-bit storage: source and receivers run as separate kernels
+    const Fields<ST> F(m, hs);
     const PTile t = make_ptile(m, g, tile, chunk);
     const int tid = threadIdx.x, lx = tid & 31, ly = tid >> 5, warp = ly;
     const TmaBox *mybox = boxes[warp];
     const int nbox = (kVelBoxes - warp + kWarps - 1) / kWarps;
     if (lx == 0) {
         fence_proxy_async();   // a persistent caller's previous item read these stages
-        for (int j = 0; j < nbox; ++j) boxes[warp][j] = vel_box(mp, t, warp + j * kWarps);
+        for (int j = 0; j < nbox; ++j) boxes[warp][j] = vel_box<SA::ES>(mp, t, warp + j * kWarps);
         for (int s = 0; s < S && t.zs + s < t.ze; ++s)
             issue(mybox, nbox, smem + s * L::STAGE, &bar[s], t.zs + s, warp, L::TXB);
     }
@@ -266,8 +369,9 @@ __device__ __forceinline__ bool vel_pair(const VelMaps &mp, const Model &m, cons
 
     const int it = step_index(sr, it_arg);
     const float inj = ph.inj_dt2 * ((use_wavelet && sr.wavelet) ? sr.wavelet[it] : src_value);
+    const bool track = H && rescale_step16(it);
     int sx = -1, sy = -1, sz = -1;
-    if (sr.src >= 0) {
+    if (!H && sr.src >= 0) {
         const int64_t r = sr.src;
         sz = (int)(r / m.plane);
         sy = (int)((r - (int64_t)sz * m.plane) / m.px);
@@ -281,10 +385,10 @@ __device__ __forceinline__ bool vel_pair(const VelMaps &mp, const Model &m, cons
     const int gz0 = t.zs + kHalo;
 #pragma unroll
     for (int k = 0; k < 9; ++k) {
-        qxz[k + 1] = ld2(m.f[7] + pc.col + (uint32_t)(gz0 - 5 + k) * PL);
-        qyz[k + 1] = ld2(m.f[8] + pc.col + (uint32_t)(gz0 - 5 + k) * PL);
-        float2 zz = ld2(m.f[5] + pc.col + (uint32_t)(gz0 - 4 + k) * PL);
-        if (pc.gy == sy && gz0 - 4 + k == sz) {
+        qxz[k + 1] = SA::pair(F.f(7) + pc.col + (uint32_t)(gz0 - 5 + k) * PL, bcast(F.sc(7)));
+        qyz[k + 1] = SA::pair(F.f(8) + pc.col + (uint32_t)(gz0 - 5 + k) * PL, bcast(F.sc(8)));
+        float2 zz = SA::pair(F.f(5) + pc.col + (uint32_t)(gz0 - 4 + k) * PL, bcast(F.sc(5)));
+        if (!H && pc.gy == sy && gz0 - 4 + k == sz) {
             if (pc.gx == sx) zz.x = zz.x + inj;
             if (pc.gx + 1 == sx) zz.y = zz.y + inj;
         }
@@ -292,14 +396,14 @@ __device__ __forceinline__ bool vel_pair(const VelMaps &mp, const Model &m, cons
     }
 
     // receivers of this tile, sorted by z: skip those below the chunk
-    int rp = g.rec_off[tile];
-    const int rend = g.rec_off[tile + 1];
+    int rp = H ? 0 : g.rec_off[tile];
+    const int rend = H ? 0 : g.rec_off[tile + 1];
     while (rp < rend && g.rec_list[rp].z < gz0) ++rp;
     int rz = rp < rend ? g.rec_list[rp].z : 0x7fffffff;
 
     bool failed = false, abort = false;
     int cz = t.zs;
-    const bool src_near = sr.src >= 0 && sy >= t.gy0 - 5 && sy < t.gy0 + PY + 5 && sx >= t.gx0 - 8 &&
+    const bool src_near = !H && sr.src >= 0 && sy >= t.gy0 - 5 && sy < t.gy0 + PY + 5 && sx >= t.gx0 - 8 &&
                           sx < t.gx0 + PX + 8;
     // One plane.  GEN selects the general path (PML cells, source, receivers);
     // every other tile-plane takes the packed interior path.  Returns false
@@ -315,7 +419,7 @@ __device__ __forceinline__ bool vel_pair(const VelMaps &mp, const Model &m, cons
         else failed = true;
 
         // source patch of the staged copies (uniform branch)
-        if (GEN && src_near && (gz == sz || gz + 5 == sz)) {
+        if constexpr (!H) if (GEN && src_near && (gz == sz || gz + 5 == sz)) {
             if (tid == 0) {
                 const int ox = sx - t.gx0, oy = sy - t.gy0;
                 if (gz == sz) {
@@ -332,14 +436,14 @@ __device__ __forceinline__ bool vel_pair(const VelMaps &mp, const Model &m, cons
             __syncthreads();
         }
 
-        const float *sxx = reinterpret_cast<const float *>(st + L::SXX);
-        const float *syy = reinterpret_cast<const float *>(st + L::SYY);
-        const float *sxy = reinterpret_cast<const float *>(st + L::SXY);
-        const float *sxz = reinterpret_cast<const float *>(st + L::SXZ);
-        const float *syz = reinterpret_cast<const float *>(st + L::SYZ);
+        const E *sxx = reinterpret_cast<const E *>(st + L::SXX);
+        const E *syy = reinterpret_cast<const E *>(st + L::SYY);
+        const E *sxy = reinterpret_cast<const E *>(st + L::SXY);
+        const E *sxz = reinterpret_cast<const E *>(st + L::SXZ);
+        const E *syz = reinterpret_cast<const E *>(st + L::SYZ);
         const float *bb = reinterpret_cast<const float *>(st + L::B);
-        const float *ov = reinterpret_cast<const float *>(st + L::OV);
-        constexpr int OVS = OB / 4;                 // floats between the own-velocity boxes
+        const E *ov = reinterpret_cast<const E *>(st + L::OV);
+        constexpr int OVS = L::OBE / SA::ES;        // values between the own-velocity boxes
         const int e = ly * PX + 2 * lx;             // 64 x 8 box index of cell 0
 
         // advance the z queues
@@ -349,26 +453,27 @@ __device__ __forceinline__ bool vel_pair(const VelMaps &mp, const Model &m, cons
             qyz[j] = qyz[j + 1];
             qzz[j] = qzz[j + 1];
         }
-        qxz[9] = ld2(reinterpret_cast<const float *>(st + L::LXZ) + e);
-        qyz[9] = ld2(reinterpret_cast<const float *>(st + L::LYZ) + e);
-        qzz[9] = ld2(reinterpret_cast<const float *>(st + L::LZZ) + e);
+        qxz[9] = SA::pair(reinterpret_cast<const E *>(st + L::LXZ) + e, bcast(F.sc(7)));
+        qyz[9] = SA::pair(reinterpret_cast<const E *>(st + L::LYZ) + e, bcast(F.sc(8)));
+        qzz[9] = SA::pair(reinterpret_cast<const E *>(st + L::LZZ) + e, bcast(F.sc(5)));
 
         if (pc.act0) {
             // x differences, per cell, from 12-value windows
             float w[12];
-            window(sxx + ly * XW + 2 * lx + 4, w);              // x offsets -4 .. 7 of cell 0
+            SA::win(sxx + ly * XW + 2 * lx + 4, w, F.sc(3));     // x offsets -4 .. 7 of cell 0
             const float2 xX = dFx<FAST>(ph, w, -4);
-            window(sxy + (ly + 5) * XW + 2 * lx + 2, w);        // -6 .. 5
+            SA::win(sxy + (ly + 5) * XW + 2 * lx + 2, w, F.sc(6));  // -6 .. 5
             const float2 yX = dBx<FAST>(ph, w, -6);
-            window(sxz + ly * XW + 2 * lx + 2, w);
+            SA::win(sxz + ly * XW + 2 * lx + 2, w, F.sc(7));
             const float2 zX = dBx<FAST>(ph, w, -6);
             // y and z differences, both cells at once
-            const float *cxy = sxy + (ly + 5) * XW + 2 * lx + 8;
-            const float *cyy = syy + (ly + 5) * PX + 2 * lx;
-            const float *cyz = syz + (ly + 5) * PX + 2 * lx;
-            const float2 xY = dB2p<FAST, 1>(ph, [&](int o) { return ld2(cxy + o * XW); });
-            const float2 yY = dF2p<FAST, 1>(ph, [&](int o) { return ld2(cyy + o * PX); });
-            const float2 zY = dB2p<FAST, 1>(ph, [&](int o) { return ld2(cyz + o * PX); });
+            const E *cxy = sxy + (ly + 5) * XW + 2 * lx + 8;
+            const E *cyy = syy + (ly + 5) * PX + 2 * lx;
+            const E *cyz = syz + (ly + 5) * PX + 2 * lx;
+            const float2 s6 = bcast(F.sc(6)), s4 = bcast(F.sc(4)), s8 = bcast(F.sc(8));
+            const float2 xY = dB2p<FAST, 1>(ph, [&](int o) { return SA::pair(cxy + o * XW, s6); });
+            const float2 yY = dF2p<FAST, 1>(ph, [&](int o) { return SA::pair(cyy + o * PX, s4); });
+            const float2 zY = dB2p<FAST, 1>(ph, [&](int o) { return SA::pair(cyz + o * PX, s8); });
             const float2 xZ = dB2p<FAST, 2>(ph, [&](int o) { return qxz[5 + o]; });
             const float2 yZ = dB2p<FAST, 2>(ph, [&](int o) { return qyz[5 + o]; });
             const float2 zZ = dF2p<FAST, 2>(ph, [&](int o) { return qzz[4 + o]; });
@@ -386,15 +491,21 @@ __device__ __forceinline__ bool vel_pair(const VelMaps &mp, const Model &m, cons
 
             const bool pml0 = (pc.kx0 | pc.ky | kz) != 0, pml1 = (pc.kx1 | pc.ky | kz) != 0;
             if (!(GEN && (t.xy_pml || kz != 0) && (pml0 || (pc.act1 && pml1)))) {
-                const float2 v0 = __ffma2_rn(__fmul2_rn(dt2, bx), __fadd2_rn(__fadd2_rn(xX, xY), xZ), ld2(ov + e));
-                const float2 v1 =
-                    __ffma2_rn(__fmul2_rn(dt2, by), __fadd2_rn(__fadd2_rn(yX, yY), yZ), ld2(ov + OVS + e));
-                const float2 v2 =
-                    __ffma2_rn(__fmul2_rn(dt2, bz), __fadd2_rn(__fadd2_rn(zX, zY), zZ), ld2(ov + 2 * OVS + e));
-                st2(m.f[0] + ci, v0, pc.act1);
-                st2(m.f[1] + ci, v1, pc.act1);
-                st2(m.f[2] + ci, v2, pc.act1);
-                if (GEN && gz == rz && it >= 0 && it < sr.nt) {
+                const float2 v0 = __ffma2_rn(__fmul2_rn(dt2, bx), __fadd2_rn(__fadd2_rn(xX, xY), xZ),
+                                             SA::pair(ov + e, bcast(F.sc(0))));
+                const float2 v1 = __ffma2_rn(__fmul2_rn(dt2, by), __fadd2_rn(__fadd2_rn(yX, yY), yZ),
+                                             SA::pair(ov + OVS + e, bcast(F.sc(1))));
+                const float2 v2 = __ffma2_rn(__fmul2_rn(dt2, bz), __fadd2_rn(__fadd2_rn(zX, zY), zZ),
+                                             SA::pair(ov + 2 * OVS + e, bcast(F.sc(2))));
+                SA::put2(F.f(0) + ci, v0, bcast(F.inv(0)), pc.act1);
+                SA::put2(F.f(1) + ci, v1, bcast(F.inv(1)), pc.act1);
+                SA::put2(F.f(2) + ci, v2, bcast(F.inv(2)), pc.act1);
+                if (track) {
+                    note_max16(hs, 0, fmaxf(fabsf(v0.x), pc.act1 ? fabsf(v0.y) : 0.0f));
+                    note_max16(hs, 1, fmaxf(fabsf(v1.x), pc.act1 ? fabsf(v1.y) : 0.0f));
+                    note_max16(hs, 2, fmaxf(fabsf(v2.x), pc.act1 ? fabsf(v2.y) : 0.0f));
+                }
+                if (!H && GEN && gz == rz && it >= 0 && it < sr.nt) {
                     for (int r = rp; r < rend && g.rec_list[r].z == gz; ++r) {
                         const int4 q = g.rec_list[r];
                         if (q.y == pc.gy && q.w <= 2 && (q.x == pc.gx || (pc.act1 && q.x == pc.gx + 1))) {
@@ -413,12 +524,12 @@ __device__ __forceinline__ bool vel_pair(const VelMaps &mp, const Model &m, cons
                     const uint32_t cc = ci + c;
                     float vnew[3];
                     if (!(kx | ky | kz)) {
-                        vnew[0] = __fmaf_rn(ph.dt * lane_of(bx, c),
-                                            (lane_of(xX, c) + lane_of(xY, c)) + lane_of(xZ, c), ov[e + c]);
-                        vnew[1] = __fmaf_rn(ph.dt * lane_of(by, c),
-                                            (lane_of(yX, c) + lane_of(yY, c)) + lane_of(yZ, c), ov[OVS + e + c]);
-                        vnew[2] = __fmaf_rn(ph.dt * lane_of(bz, c),
-                                            (lane_of(zX, c) + lane_of(zY, c)) + lane_of(zZ, c), ov[2 * OVS + e + c]);
+                        vnew[0] = __fmaf_rn(ph.dt * lane_of(bx, c), (lane_of(xX, c) + lane_of(xY, c)) + lane_of(xZ, c),
+                                            SA::one(ov + e + c, F.sc(0)));
+                        vnew[1] = __fmaf_rn(ph.dt * lane_of(by, c), (lane_of(yX, c) + lane_of(yY, c)) + lane_of(yZ, c),
+                                            SA::one(ov + OVS + e + c, F.sc(1)));
+                        vnew[2] = __fmaf_rn(ph.dt * lane_of(bz, c), (lane_of(zX, c) + lane_of(zY, c)) + lane_of(zZ, c),
+                                            SA::one(ov + 2 * OVS + e + c, F.sc(2)));
                     } else {
                         float mx = 1.f, px = 1.f, my = 1.f, py = 1.f, mz = 1.f, pz = 1.f;
                         {
@@ -432,29 +543,34 @@ __device__ __forceinline__ bool vel_pair(const VelMaps &mp, const Model &m, cons
                         const float bxc = lane_of(bx, c);
                         const float ax = ph.dt * bxc, ay = ph.dt * (ref ? bxc : lane_of(by, c)),
                                     az = ph.dt * (ref ? bxc : lane_of(bz, c));
-                        float *sp = m.split + pml_plane_index(m, c ? pc.pc1 : pc.pc0, cz);
+                        E *sp = F.split() + pml_plane_index(m, c ? pc.pc1 : pc.pc0, cz);
                         const uint32_t N = (uint32_t)m.npml;
-                        float a0, a1, a2;
-                        a0 = split_update<FAST>(sp[S_VXX * N], ax, lane_of(xX, c), kx, mx, px);
-                        a1 = split_update<FAST>(sp[S_VXY * N], ax, lane_of(xY, c), ky, my, py);
-                        a2 = split_update<FAST>(sp[S_VXZ * N], ax, lane_of(xZ, c), kz, mz, pz);
-                        sp[S_VXX * N] = a0; sp[S_VXY * N] = a1; sp[S_VXZ * N] = a2;
-                        vnew[0] = (a0 + a1) + a2;
-                        a0 = split_update<FAST>(sp[S_VYX * N], ay, lane_of(yX, c), kx, mx, px);
-                        a1 = split_update<FAST>(sp[S_VYY * N], ay, lane_of(yY, c), ky, my, py);
-                        a2 = split_update<FAST>(sp[S_VYZ * N], ay, lane_of(yZ, c), kz, mz, pz);
-                        sp[S_VYX * N] = a0; sp[S_VYY * N] = a1; sp[S_VYZ * N] = a2;
-                        vnew[1] = (a0 + a1) + a2;
-                        a0 = split_update<FAST>(sp[S_VZX * N], az, lane_of(zX, c), kx, mx, px);
-                        a1 = split_update<FAST>(sp[S_VZY * N], az, lane_of(zY, c), ky, my, py);
-                        a2 = split_update<FAST>(sp[S_VZZ * N], az, lane_of(zZ, c), kz, mz, pz);
-                        sp[S_VZX * N] = a0; sp[S_VZY * N] = a1; sp[S_VZZ * N] = a2;
-                        vnew[2] = (a0 + a1) + a2;
+                        const float dxyz[3][3] = {{lane_of(xX, c), lane_of(xY, c), lane_of(xZ, c)},
+                                                  {lane_of(yX, c), lane_of(yY, c), lane_of(yZ, c)},
+                                                  {lane_of(zX, c), lane_of(zY, c), lane_of(zZ, c)}};
+                        const float aq[3] = {ax, ay, az};
+                        const int kk[3] = {kx, ky, kz};
+                        const float mm[3] = {mx, my, mz}, pp[3] = {px, py, pz};
+#pragma unroll
+                        for (int q = 0; q < 3; ++q) {
+                            float part[3];
+#pragma unroll
+                            for (int a = 0; a < 3; ++a) {
+                                E *spk = sp + (3 * q + a) * N;   // split S_VXX + 3q + a, scale of field q
+                                part[a] = split_update<FAST>(SA::one(spk, F.sc(q)), aq[q], dxyz[q][a], kk[a], mm[a],
+                                                             pp[a]);
+                                if (track) note_max16(hs, q, part[a]);
+                                SA::put1(spk, part[a], F.inv(q));
+                            }
+                            vnew[q] = (part[0] + part[1]) + part[2];
+                        }
                     }
-                    m.f[0][cc] = vnew[0];
-                    m.f[1][cc] = vnew[1];
-                    m.f[2][cc] = vnew[2];
-                    if (gz == rz && it >= 0 && it < sr.nt) {
+#pragma unroll
+                    for (int q = 0; q < 3; ++q) {
+                        if (track) note_max16(hs, q, vnew[q]);
+                        SA::put1(F.f(q) + cc, vnew[q], F.inv(q));
+                    }
+                    if (!H && gz == rz && it >= 0 && it < sr.nt) {
                         for (int r = rp; r < rend && g.rec_list[r].z == gz; ++r) {
                             const int4 q = g.rec_list[r];
                             if (q.x == pc.gx + c && q.y == pc.gy && q.w <= 2)
@@ -513,20 +629,24 @@ __device__ __forceinline__ bool vel_pair(const VelMaps &mp, const Model &m, cons
 // the parity of the next wait of each stage and carries over between the
 // work items of a persistent caller.  Returns false when the block gave up
 // on a wait (after waiting, bounded, for its own copies still in flight).
-template <bool FAST>
+template <bool FAST, int ST>
 __device__ __forceinline__ bool str_pair(const StrMaps &mp, const Model &m, const Physics &ph, const ZGeom &g,
-                                        const SourceRec &sr, int it_arg, float src_value, int use_wavelet, int tile,
-                                        int chunk, unsigned char *smem, uint64_t *bar,
+                                        const SourceRec &sr, const HalfState &hs, int it_arg, float src_value,
+                                        int use_wavelet, int tile, int chunk, unsigned char *smem, uint64_t *bar,
                                         TmaBox (*boxes)[kMaxBoxesPerWarp], uint32_t &pbits) {
-    using L = StrP;
+    using SA = Sto<ST>;
+    using E = typename SA::E;
+    using L = StrP<SA::ES>;
     constexpr int S = SS;
+    constexpr bool H = ST != SGFD_STORE_F32;   // 16-bit storage: source and receivers run as separate kernels
+    const Fields<ST> F(m, hs);
     const PTile t = make_ptile(m, g, tile, chunk);
     const int tid = threadIdx.x, lx = tid & 31, ly = tid >> 5, warp = ly;
     const TmaBox *mybox = boxes[warp];
     const int nbox = (kStrBoxes - warp + kWarps - 1) / kWarps;
     if (lx == 0) {
         fence_proxy_async();
-        for (int j = 0; j < nbox; ++j) boxes[warp][j] = str_box(mp, t, warp + j * kWarps);
+        for (int j = 0; j < nbox; ++j) boxes[warp][j] = str_box<SA::ES>(mp, t, warp + j * kWarps);
         for (int s = 0; s < S && t.zs + s < t.ze; ++s)
             issue(mybox, nbox, smem + s * L::STAGE, &bar[s], t.zs + s, warp, L::TXB);
     }
@@ -535,7 +655,8 @@ __device__ __forceinline__ bool str_pair(const StrMaps &mp, const Model &m, cons
 
     const int it = step_index(sr, it_arg);
     const float inj = ph.inj_dt2 * ((use_wavelet && sr.wavelet) ? sr.wavelet[it] : src_value);
-    const int64_t src = sr.src;
+    const int64_t src = H ? -1 : sr.src;
+    const bool track = H && rescale_step16(it);
     const PairCtx pc = pair_ctx(m, t, lx, ly);
     const uint32_t PL = (uint32_t)m.plane;
 
@@ -544,13 +665,13 @@ __device__ __forceinline__ bool str_pair(const StrMaps &mp, const Model &m, cons
     const int gz0 = t.zs + kHalo;
 #pragma unroll
     for (int k = 0; k < 9; ++k) {
-        qx[k + 1] = ld2(m.f[0] + pc.col + (uint32_t)(gz0 - 4 + k) * PL);
-        qy[k + 1] = ld2(m.f[1] + pc.col + (uint32_t)(gz0 - 4 + k) * PL);
-        qz[k + 1] = ld2(m.f[2] + pc.col + (uint32_t)(gz0 - 5 + k) * PL);
+        qx[k + 1] = SA::pair(F.f(0) + pc.col + (uint32_t)(gz0 - 4 + k) * PL, bcast(F.sc(0)));
+        qy[k + 1] = SA::pair(F.f(1) + pc.col + (uint32_t)(gz0 - 4 + k) * PL, bcast(F.sc(1)));
+        qz[k + 1] = SA::pair(F.f(2) + pc.col + (uint32_t)(gz0 - 5 + k) * PL, bcast(F.sc(2)));
     }
 
-    int rp = g.rec_off[tile];
-    const int rend = g.rec_off[tile + 1];
+    int rp = H ? 0 : g.rec_off[tile];
+    const int rend = H ? 0 : g.rec_off[tile + 1];
     while (rp < rend && g.rec_list[rp].z < gz0) ++rp;
     int rz = rp < rend ? g.rec_list[rp].z : 0x7fffffff;
 
@@ -567,12 +688,14 @@ __device__ __forceinline__ bool str_pair(const StrMaps &mp, const Model &m, cons
         if (mbar_wait(&bar[s], (pbits >> s) & 1u)) pbits ^= 1u << s;
         else failed = true;
 
-        const float *svx = reinterpret_cast<const float *>(st + L::VX);
-        const float *svy = reinterpret_cast<const float *>(st + L::VY);
-        const float *svz = reinterpret_cast<const float *>(st + L::VZ);
-        // own-cell boxes: txx..tyz at q = 0..5, lambda 6, mu 7, shear moduli 8..10
-        const float *own = reinterpret_cast<const float *>(st + L::OWN);
-        constexpr int OS = OB / 4;
+        const E *svx = reinterpret_cast<const E *>(st + L::VX);
+        const E *svy = reinterpret_cast<const E *>(st + L::VY);
+        const E *svz = reinterpret_cast<const E *>(st + L::VZ);
+        // own-cell boxes: txx..tyz (wavefield values), then lambda, mu and the
+        // three shear moduli (FP32)
+        const E *own = reinterpret_cast<const E *>(st + L::OWN);
+        const float *med = reinterpret_cast<const float *>(st + L::MED);
+        constexpr int OS = L::OBE / SA::ES, MS = OB / 4;
         const int e = ly * PX + 2 * lx;
 
 #pragma unroll
@@ -581,49 +704,54 @@ __device__ __forceinline__ bool str_pair(const StrMaps &mp, const Model &m, cons
             qy[j] = qy[j + 1];
             qz[j] = qz[j + 1];
         }
-        qx[9] = ld2(reinterpret_cast<const float *>(st + L::LX) + e);
-        qy[9] = ld2(reinterpret_cast<const float *>(st + L::LY) + e);
-        qz[9] = ld2(reinterpret_cast<const float *>(st + L::LZ) + e);
+        qx[9] = SA::pair(reinterpret_cast<const E *>(st + L::LX) + e, bcast(F.sc(0)));
+        qy[9] = SA::pair(reinterpret_cast<const E *>(st + L::LY) + e, bcast(F.sc(1)));
+        qz[9] = SA::pair(reinterpret_cast<const E *>(st + L::LZ) + e, bcast(F.sc(2)));
 
         if (pc.act0) {
             float w[12];
-            window(svx + (ly + 5) * XW + 2 * lx + 2, w);        // x offsets -6 .. 5 of cell 0
+            SA::win(svx + (ly + 5) * XW + 2 * lx + 2, w, F.sc(0));  // x offsets -6 .. 5 of cell 0
             const float2 dXx = dBx<FAST>(ph, w, -6);
-            window(svy + (ly + 5) * XW + 2 * lx + 4, w);        // -4 .. 7
+            SA::win(svy + (ly + 5) * XW + 2 * lx + 4, w, F.sc(1));  // -4 .. 7
             const float2 xyX = dFx<FAST>(ph, w, -4);
-            window(svz + (ly + 5) * XW + 2 * lx + 4, w);
+            SA::win(svz + (ly + 5) * XW + 2 * lx + 4, w, F.sc(2));
             const float2 xzX = dFx<FAST>(ph, w, -4);
-            const float *cx_ = svx + (ly + 5) * XW + 2 * lx + 8;
-            const float *cy_ = svy + (ly + 5) * XW + 2 * lx + 8;
-            const float *cz_ = svz + (ly + 5) * XW + 2 * lx + 8;
-            const float2 dYy = dB2p<FAST, 1>(ph, [&](int o) { return ld2(cy_ + o * XW); });
-            const float2 xyY = dF2p<FAST, 1>(ph, [&](int o) { return ld2(cx_ + o * XW); });
-            const float2 yzY = dF2p<FAST, 1>(ph, [&](int o) { return ld2(cz_ + o * XW); });
+            const E *cx_ = svx + (ly + 5) * XW + 2 * lx + 8;
+            const E *cy_ = svy + (ly + 5) * XW + 2 * lx + 8;
+            const E *cz_ = svz + (ly + 5) * XW + 2 * lx + 8;
+            const float2 s0 = bcast(F.sc(0)), s1 = bcast(F.sc(1)), s2 = bcast(F.sc(2));
+            const float2 dYy = dB2p<FAST, 1>(ph, [&](int o) { return SA::pair(cy_ + o * XW, s1); });
+            const float2 xyY = dF2p<FAST, 1>(ph, [&](int o) { return SA::pair(cx_ + o * XW, s0); });
+            const float2 yzY = dF2p<FAST, 1>(ph, [&](int o) { return SA::pair(cz_ + o * XW, s2); });
             const float2 xzZ = dF2p<FAST, 2>(ph, [&](int o) { return qx[4 + o]; });
             const float2 yzZ = dF2p<FAST, 2>(ph, [&](int o) { return qy[4 + o]; });
             const float2 dZz = dB2p<FAST, 2>(ph, [&](int o) { return qz[5 + o]; });
 
-            const float2 l = ld2(own + 6 * OS + e), mu2 = ld2(own + 7 * OS + e);
+            const float2 l = ld2(med + e), mu2 = ld2(med + MS + e);
             const float2 l2m = __ffma2_rn(bcast(2.0f), mu2, l);
-            const float2 mxy = ld2(own + 8 * OS + e), mxz = ld2(own + 9 * OS + e), myz = ld2(own + 10 * OS + e);
+            const float2 mxy = ld2(med + 2 * MS + e), mxz = ld2(med + 3 * MS + e), myz = ld2(med + 4 * MS + e);
             const uint32_t ci = pc.col + (uint32_t)gz * PL;
             const float2 dt2 = bcast(ph.dt);
 
             const bool pml0 = (pc.kx0 | pc.ky | kz) != 0, pml1 = (pc.kx1 | pc.ky | kz) != 0;
             if (!(GEN && (t.xy_pml || kz != 0) && (pml0 || (pc.act1 && pml1)))) {
-                float2 o0 = ld2(own + e), o1 = ld2(own + OS + e), o2 = ld2(own + 2 * OS + e);
+                float2 o0 = SA::pair(own + e, bcast(F.sc(3))), o1 = SA::pair(own + OS + e, bcast(F.sc(4))),
+                       o2 = SA::pair(own + 2 * OS + e, bcast(F.sc(5)));
                 if (GEN && (int64_t)ci == src) { o0.x = o0.x + inj; o1.x = o1.x + inj; o2.x = o2.x + inj; }
                 if (GEN && (int64_t)ci + 1 == src) { o0.y = o0.y + inj; o1.y = o1.y + inj; o2.y = o2.y + inj; }
                 float2 sn[6];
                 sn[0] = __ffma2_rn(dt2, __ffma2_rn(l2m, dXx, __fmul2_rn(l, __fadd2_rn(dYy, dZz))), o0);
                 sn[1] = __ffma2_rn(dt2, __ffma2_rn(l2m, dYy, __fmul2_rn(l, __fadd2_rn(dXx, dZz))), o1);
                 sn[2] = __ffma2_rn(dt2, __ffma2_rn(l2m, dZz, __fmul2_rn(l, __fadd2_rn(dXx, dYy))), o2);
-                sn[3] = __ffma2_rn(__fmul2_rn(dt2, mxy), __fadd2_rn(xyY, xyX), ld2(own + 3 * OS + e));
-                sn[4] = __ffma2_rn(__fmul2_rn(dt2, mxz), __fadd2_rn(xzZ, xzX), ld2(own + 4 * OS + e));
-                sn[5] = __ffma2_rn(__fmul2_rn(dt2, myz), __fadd2_rn(yzZ, yzY), ld2(own + 5 * OS + e));
+                sn[3] = __ffma2_rn(__fmul2_rn(dt2, mxy), __fadd2_rn(xyY, xyX), SA::pair(own + 3 * OS + e, bcast(F.sc(6))));
+                sn[4] = __ffma2_rn(__fmul2_rn(dt2, mxz), __fadd2_rn(xzZ, xzX), SA::pair(own + 4 * OS + e, bcast(F.sc(7))));
+                sn[5] = __ffma2_rn(__fmul2_rn(dt2, myz), __fadd2_rn(yzZ, yzY), SA::pair(own + 5 * OS + e, bcast(F.sc(8))));
 #pragma unroll
-                for (int q = 0; q < 6; ++q) st2(m.f[3 + q] + ci, sn[q], pc.act1);
-                if (GEN && gz == rz && it >= 0 && it < sr.nt) {
+                for (int q = 0; q < 6; ++q) {
+                    SA::put2(F.f(3 + q) + ci, sn[q], bcast(F.inv(3 + q)), pc.act1);
+                    if (track) note_max16(hs, 3 + q, fmaxf(fabsf(sn[q].x), pc.act1 ? fabsf(sn[q].y) : 0.0f));
+                }
+                if (!H && GEN && gz == rz && it >= 0 && it < sr.nt) {
                     for (int r = rp; r < rend && g.rec_list[r].z == gz; ++r) {
                         const int4 q = g.rec_list[r];
                         if (q.y == pc.gy && q.w >= 3 && (q.x == pc.gx || (pc.act1 && q.x == pc.gx + 1)))
@@ -640,20 +768,28 @@ __device__ __forceinline__ bool str_pair(const StrMaps &mp, const Model &m, cons
                     const float dXxc = lane_of(dXx, c), dYyc = lane_of(dYy, c), dZzc = lane_of(dZz, c);
                     float snew[6];
                     if (!(kx | ky | kz)) {
-                        float o0 = own[e + c], o1 = own[OS + e + c], o2 = own[2 * OS + e + c];
+                        float o0 = SA::one(own + e + c, F.sc(3)), o1 = SA::one(own + OS + e + c, F.sc(4)),
+                              o2 = SA::one(own + 2 * OS + e + c, F.sc(5));
                         if ((int64_t)cc == src) { o0 = o0 + inj; o1 = o1 + inj; o2 = o2 + inj; }
                         snew[0] = __fmaf_rn(ph.dt, __fmaf_rn(l2mc, dXxc, lc * (dYyc + dZzc)), o0);
                         snew[1] = __fmaf_rn(ph.dt, __fmaf_rn(l2mc, dYyc, lc * (dXxc + dZzc)), o1);
                         snew[2] = __fmaf_rn(ph.dt, __fmaf_rn(l2mc, dZzc, lc * (dXxc + dYyc)), o2);
                         snew[3] = __fmaf_rn(ph.dt * lane_of(mxy, c), lane_of(xyY, c) + lane_of(xyX, c),
-                                            own[3 * OS + e + c]);
+                                            SA::one(own + 3 * OS + e + c, F.sc(6)));
                         snew[4] = __fmaf_rn(ph.dt * lane_of(mxz, c), lane_of(xzZ, c) + lane_of(xzX, c),
-                                            own[4 * OS + e + c]);
+                                            SA::one(own + 4 * OS + e + c, F.sc(7)));
                         snew[5] = __fmaf_rn(ph.dt * lane_of(myz, c), lane_of(yzZ, c) + lane_of(yzY, c),
-                                            own[5 * OS + e + c]);
+                                            SA::one(own + 5 * OS + e + c, F.sc(8)));
                     } else {
-                        float *sp = m.split + pml_plane_index(m, c ? pc.pc1 : pc.pc0, cz);
+                        E *sp = F.split() + pml_plane_index(m, c ? pc.pc1 : pc.pc0, cz);
                         const uint32_t N = (uint32_t)m.npml;
+                        // split k, in its field's scale (S_XXX.. -> txx.., two per shear stress)
+                        auto grp = [](int k) { return k < S_XYX ? 3 + (k - S_XXX) / 3 : 6 + (k - S_XYX) / 2; };
+                        auto rd = [&](int k) { return SA::one(sp + k * N, F.sc(grp(k))); };
+                        auto wr = [&](int k, float v) {
+                            if (track) note_max16(hs, grp(k), v);
+                            SA::put1(sp + k * N, v, F.inv(grp(k)));
+                        };
                         float mx = 1.f, px = 1.f, my = 1.f, py = 1.f, mz = 1.f, pz = 1.f;
                         {
                             const float v = damp_speed(ph, mu_c, m.b[cc], lc);
@@ -663,39 +799,42 @@ __device__ __forceinline__ bool str_pair(const StrMaps &mp, const Model &m, cons
                         }
                         const float dl = ph.dt * l2mc, dt = ph.dt;
                         float a0, a1, a2;
-                        a0 = split_update<FAST>(sp[S_XXX * N], dl, dXxc, kx, mx, px);
-                        a1 = split_update<FAST>(sp[S_XXY * N], dt, lc * dYyc, ky, my, py);
-                        a2 = split_update<FAST>(sp[S_XXZ * N], dt, lc * dZzc, kz, mz, pz);
-                        sp[S_XXX * N] = a0; sp[S_XXY * N] = a1; sp[S_XXZ * N] = a2;
+                        a0 = split_update<FAST>(rd(S_XXX), dl, dXxc, kx, mx, px);
+                        a1 = split_update<FAST>(rd(S_XXY), dt, lc * dYyc, ky, my, py);
+                        a2 = split_update<FAST>(rd(S_XXZ), dt, lc * dZzc, kz, mz, pz);
+                        wr(S_XXX, a0); wr(S_XXY, a1); wr(S_XXZ, a2);
                         snew[0] = (a0 + a1) + a2;
-                        a0 = split_update<FAST>(sp[S_YYX * N], dt, lc * dXxc, kx, mx, px);
-                        a1 = split_update<FAST>(sp[S_YYY * N], dl, dYyc, ky, my, py);
-                        a2 = split_update<FAST>(sp[S_YYZ * N], dt, lc * dZzc, kz, mz, pz);
-                        sp[S_YYX * N] = a0; sp[S_YYY * N] = a1; sp[S_YYZ * N] = a2;
+                        a0 = split_update<FAST>(rd(S_YYX), dt, lc * dXxc, kx, mx, px);
+                        a1 = split_update<FAST>(rd(S_YYY), dl, dYyc, ky, my, py);
+                        a2 = split_update<FAST>(rd(S_YYZ), dt, lc * dZzc, kz, mz, pz);
+                        wr(S_YYX, a0); wr(S_YYY, a1); wr(S_YYZ, a2);
                         snew[1] = (a0 + a1) + a2;
-                        a0 = split_update<FAST>(sp[S_ZZX * N], dt, lc * dXxc, kx, mx, px);
-                        a1 = split_update<FAST>(sp[S_ZZY * N], dt, lc * dYyc, ky, my, py);
-                        a2 = split_update<FAST>(sp[S_ZZZ * N], dl, dZzc, kz, mz, pz);
-                        sp[S_ZZX * N] = a0; sp[S_ZZY * N] = a1; sp[S_ZZZ * N] = a2;
+                        a0 = split_update<FAST>(rd(S_ZZX), dt, lc * dXxc, kx, mx, px);
+                        a1 = split_update<FAST>(rd(S_ZZY), dt, lc * dYyc, ky, my, py);
+                        a2 = split_update<FAST>(rd(S_ZZZ), dl, dZzc, kz, mz, pz);
+                        wr(S_ZZX, a0); wr(S_ZZY, a1); wr(S_ZZZ, a2);
                         snew[2] = (a0 + a1) + a2;
                         const float axy = dt * lane_of(mxy, c), axz = dt * lane_of(mxz, c),
                                     ayz = dt * lane_of(myz, c);
-                        a0 = split_update<FAST>(sp[S_XYX * N], axy, lane_of(xyX, c), kx, mx, px);
-                        a1 = split_update<FAST>(sp[S_XYY * N], axy, lane_of(xyY, c), ky, my, py);
-                        sp[S_XYX * N] = a0; sp[S_XYY * N] = a1;
+                        a0 = split_update<FAST>(rd(S_XYX), axy, lane_of(xyX, c), kx, mx, px);
+                        a1 = split_update<FAST>(rd(S_XYY), axy, lane_of(xyY, c), ky, my, py);
+                        wr(S_XYX, a0); wr(S_XYY, a1);
                         snew[3] = a0 + a1;
-                        a0 = split_update<FAST>(sp[S_XZX * N], axz, lane_of(xzX, c), kx, mx, px);
-                        a1 = split_update<FAST>(sp[S_XZZ * N], axz, lane_of(xzZ, c), kz, mz, pz);
-                        sp[S_XZX * N] = a0; sp[S_XZZ * N] = a1;
+                        a0 = split_update<FAST>(rd(S_XZX), axz, lane_of(xzX, c), kx, mx, px);
+                        a1 = split_update<FAST>(rd(S_XZZ), axz, lane_of(xzZ, c), kz, mz, pz);
+                        wr(S_XZX, a0); wr(S_XZZ, a1);
                         snew[4] = a0 + a1;
-                        a0 = split_update<FAST>(sp[S_YZY * N], ayz, lane_of(yzY, c), ky, my, py);
-                        a1 = split_update<FAST>(sp[S_YZZ * N], ayz, lane_of(yzZ, c), kz, mz, pz);
-                        sp[S_YZY * N] = a0; sp[S_YZZ * N] = a1;
+                        a0 = split_update<FAST>(rd(S_YZY), ayz, lane_of(yzY, c), ky, my, py);
+                        a1 = split_update<FAST>(rd(S_YZZ), ayz, lane_of(yzZ, c), kz, mz, pz);
+                        wr(S_YZY, a0); wr(S_YZZ, a1);
                         snew[5] = a0 + a1;
                     }
 #pragma unroll
-                    for (int q = 0; q < 6; ++q) m.f[3 + q][cc] = snew[q];
-                    if (gz == rz && it >= 0 && it < sr.nt) {
+                    for (int q = 0; q < 6; ++q) {
+                        if (track) note_max16(hs, 3 + q, snew[q]);
+                        SA::put1(F.f(3 + q) + cc, snew[q], F.inv(3 + q));
+                    }
+                    if (!H && gz == rz && it >= 0 && it < sr.nt) {
                         for (int r = rp; r < rend && g.rec_list[r].z == gz; ++r) {
                             const int4 q = g.rec_list[r];
                             if (q.x == pc.gx + c && q.y == pc.gy && q.w >= 3)
@@ -743,11 +882,11 @@ __device__ __forceinline__ bool str_pair(const StrMaps &mp, const Model &m, cons
 }
 
 // One launch per update: one CTA per (tile, z chunk).
-template <bool FAST>
+template <bool FAST, int ST>
 __global__ void __launch_bounds__(NT, 2)
 k_velocity_zpair(const __grid_constant__ VelMaps mp, const __grid_constant__ Model m, const __grid_constant__ Physics ph,
-                 const __grid_constant__ ZGeom g, const __grid_constant__ SourceRec sr, int it_arg, float src_value,
-                 int use_wavelet) {
+                 const __grid_constant__ ZGeom g, const __grid_constant__ SourceRec sr,
+                 const __grid_constant__ HalfState hs, int it_arg, float src_value, int use_wavelet) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t bar[SV];
     __shared__ TmaBox boxes[kWarps][kMaxBoxesPerWarp];
@@ -757,15 +896,15 @@ k_velocity_zpair(const __grid_constant__ VelMaps mp, const __grid_constant__ Mod
     }
     __syncthreads();
     uint32_t pbits = 0;
-    vel_pair<FAST>(mp, m, ph, g, sr, it_arg, src_value, use_wavelet, blockIdx.x, blockIdx.y, align_smem(smem_raw), bar,
-                   boxes, pbits);
+    vel_pair<FAST, ST>(mp, m, ph, g, sr, hs, it_arg, src_value, use_wavelet, blockIdx.x, blockIdx.y,
+                       align_smem(smem_raw), bar, boxes, pbits);
 }
 
-template <bool FAST>
+template <bool FAST, int ST>
 __global__ void __launch_bounds__(NT, 2)
 k_stress_zpair(const __grid_constant__ StrMaps mp, const __grid_constant__ Model m, const __grid_constant__ Physics ph,
-               const __grid_constant__ ZGeom g, const __grid_constant__ SourceRec sr, int it_arg, float src_value,
-               int use_wavelet) {
+               const __grid_constant__ ZGeom g, const __grid_constant__ SourceRec sr,
+               const __grid_constant__ HalfState hs, int it_arg, float src_value, int use_wavelet) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t bar[SS];
     __shared__ TmaBox boxes[kWarps][kMaxBoxesPerWarp];
@@ -775,8 +914,8 @@ k_stress_zpair(const __grid_constant__ StrMaps mp, const __grid_constant__ Model
     }
     __syncthreads();
     uint32_t pbits = 0;
-    str_pair<FAST>(mp, m, ph, g, sr, it_arg, src_value, use_wavelet, blockIdx.x, blockIdx.y, align_smem(smem_raw), bar,
-                   boxes, pbits);
+    str_pair<FAST, ST>(mp, m, ph, g, sr, hs, it_arg, src_value, use_wavelet, blockIdx.x, blockIdx.y,
+                       align_smem(smem_raw), bar, boxes, pbits);
 }
 
 // ---------------------------------------------------------------------------
@@ -848,10 +987,12 @@ k_batch_zpair(const PairModel *models, int nmodels, const int *first_item, int i
                 const PairModel &d = models[mi];
                 const int local = item - first_item[mi];
                 const int ntiles = d.g.ntx * d.g.nty;
-                const bool ok = p == 0 ? vel_pair<FAST>(d.vm, d.m, d.ph, d.g, d.sr, it0 + k, 0.0f, 1, local % ntiles,
-                                                        local / ntiles, smem, bar_v, boxes, pv)
-                                       : str_pair<FAST>(d.sm, d.m, d.ph, d.g, d.sr, it0 + k, 0.0f, 1, local % ntiles,
-                                                        local / ntiles, smem, bar_s, boxes, ps);
+                const HalfState no16{};
+                const bool ok =
+                    p == 0 ? vel_pair<FAST, SGFD_STORE_F32>(d.vm, d.m, d.ph, d.g, d.sr, no16, it0 + k, 0.0f, 1,
+                                                            local % ntiles, local / ntiles, smem, bar_v, boxes, pv)
+                           : str_pair<FAST, SGFD_STORE_F32>(d.sm, d.m, d.ph, d.g, d.sr, no16, it0 + k, 0.0f, 1,
+                                                            local % ntiles, local / ntiles, smem, bar_s, boxes, ps);
                 if (!ok) {
                     if (threadIdx.x == 0) atomicExch(status, kBatchWaitTma);
                     return;
@@ -863,32 +1004,52 @@ k_batch_zpair(const PairModel *models, int nmodels, const int *first_item, int i
     }
 }
 
-constexpr int vel_smem() { return SV * VelP::STAGE + 128; }
-constexpr int str_smem() { return SS * StrP::STAGE + 128; }
-static_assert(vel_smem() <= 113 * 1024 && str_smem() <= 113 * 1024, "two CTAs per SM");
+template <int ST>
+constexpr int vel_smem() { return SV * VelP<Sto<ST>::ES>::STAGE + 128; }
+template <int ST>
+constexpr int str_smem() { return SS * StrP<Sto<ST>::ES>::STAGE + 128; }
+static_assert(vel_smem<SGFD_STORE_F32>() <= 113 * 1024 && str_smem<SGFD_STORE_F32>() <= 113 * 1024,
+              "two CTAs per SM");
 
-template <bool FAST>
+template <bool FAST, int ST>
 cudaError_t set_attrs() {
-    cudaError_t e = cudaFuncSetAttribute(k_velocity_zpair<FAST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         vel_smem());
+    cudaError_t e = cudaFuncSetAttribute(k_velocity_zpair<FAST, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         vel_smem<ST>());
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_stress_zpair<FAST>, cudaFuncAttributeMaxDynamicSharedMemorySize, str_smem());
+        e = cudaFuncSetAttribute(k_stress_zpair<FAST, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 str_smem<ST>());
     return e;
 }
 
-template <bool FAST>
-void launch(const Model &m, const Physics &ph, const SourceRec &sr, const ZGeom &g, const VelMaps &vm,
-            const StrMaps &sm, int it, float src_value, int uw, cudaStream_t s, cudaEvent_t *ev) {
+template <bool FAST, int ST>
+void launch(const Model &m, const Physics &ph, const SourceRec &sr, const HalfState &hs, const ZGeom &g,
+            const VelMaps &vm, const StrMaps &sm, int it, float src_value, int uw, cudaStream_t s, cudaEvent_t *ev) {
     const dim3 grid(g.ntx * g.nty, g.nchunks);
     if (ev) cudaEventRecord(ev[0], s);
-    k_velocity_zpair<FAST><<<grid, NT, vel_smem(), s>>>(vm, m, ph, g, sr, it, src_value, uw);
+    k_velocity_zpair<FAST, ST><<<grid, NT, vel_smem<ST>(), s>>>(vm, m, ph, g, sr, hs, it, src_value, uw);
     if (ev) cudaEventRecord(ev[1], s);
+    if (ST != SGFD_STORE_F32) half_phase(m, ph, sr, hs, it, src_value, uw != 0, s, 1);
     if (ev) cudaEventRecord(ev[2], s);
-    k_stress_zpair<FAST><<<grid, NT, str_smem(), s>>>(sm, m, ph, g, sr, it, src_value, uw);
+    k_stress_zpair<FAST, ST><<<grid, NT, str_smem<ST>(), s>>>(sm, m, ph, g, sr, hs, it, src_value, uw);
     if (ev) cudaEventRecord(ev[3], s);
 }
 
-constexpr int batch_smem() { return vel_smem() > str_smem() ? vel_smem() : str_smem(); }
+template <int ST>
+cudaError_t launch_st(const Model &m, const Physics &ph, const SourceRec &sr, const HalfState &hs, const ZGeom &g,
+                      const VelMaps &vm, const StrMaps &sm, int it, float src_value, bool use_wavelet, cudaStream_t s,
+                      cudaEvent_t *ev) {
+    const int uw = use_wavelet ? 1 : 0;
+    if (ST != SGFD_STORE_F32) half_phase(m, ph, sr, hs, it, src_value, use_wavelet, s, 0);
+    if (ph.fast) launch<true, ST>(m, ph, sr, hs, g, vm, sm, it, src_value, uw, s, ev);
+    else launch<false, ST>(m, ph, sr, hs, g, vm, sm, it, src_value, uw, s, ev);
+    if (ST != SGFD_STORE_F32) half_phase(m, ph, sr, hs, it, src_value, use_wavelet, s, 2);
+    return cudaGetLastError();
+}
+
+constexpr int batch_smem() {
+    return vel_smem<SGFD_STORE_F32>() > str_smem<SGFD_STORE_F32>() ? vel_smem<SGFD_STORE_F32>()
+                                                                   : str_smem<SGFD_STORE_F32>();
+}
 
 }  // namespace
 
@@ -917,32 +1078,43 @@ cudaError_t zpair_batch_run(const PairModel *models, int nmodels, const int *fir
     return cudaLaunchCooperativeKernel(fn, dim3(ctas), dim3(NT), args, batch_smem(), s);
 }
 
-cudaError_t zpair_prepare(const Model &m, VelMaps *vm, StrMaps *sm) {
+cudaError_t zpair_prepare(const Model &m, const HalfState *hs, VelMaps *vm, StrMaps *sm) {
     constexpr int ty = PY;
     bool ok = true;
-    ok &= make_box_map(&vm->sxx, m.f[3], m, XW, ty);
-    ok &= make_box_map(&vm->syy, m.f[4], m, PX, ty + 10);
-    ok &= make_box_map(&vm->sxy, m.f[6], m, XW, ty + 10);
-    ok &= make_box_map(&vm->sxz, m.f[7], m, XW, ty);
-    ok &= make_box_map(&vm->syz, m.f[8], m, PX, ty + 10);
+    // wavefield maps: the FP32 arrays, or the 16-bit ones of the same layout
+    auto fm = [&](CUtensorMap *map, int k, int bx, int by) {
+        if (hs) return make_box_map16(map, hs->f[k], m, bx, by);
+        return make_box_map(map, m.f[k], m, bx, by);
+    };
+    ok &= fm(&vm->sxx, 3, XW, ty);
+    ok &= fm(&vm->syy, 4, PX, ty + 10);
+    ok &= fm(&vm->sxy, 6, XW, ty + 10);
+    ok &= fm(&vm->sxz, 7, XW, ty);
+    ok &= fm(&vm->syz, 8, PX, ty + 10);
     ok &= make_box_map(&vm->b, m.b, m, BW, ty + 1);
-    ok &= make_box_map(&vm->sxz_c, m.f[7], m, PX, ty);
-    ok &= make_box_map(&vm->syz_c, m.f[8], m, PX, ty);
-    ok &= make_box_map(&vm->szz_c, m.f[5], m, PX, ty);
+    ok &= fm(&vm->sxz_c, 7, PX, ty);
+    ok &= fm(&vm->syz_c, 8, PX, ty);
+    ok &= fm(&vm->szz_c, 5, PX, ty);
     ok &= make_box_map(&vm->b_c, m.b, m, PX, ty);
-    for (int q = 0; q < 3; ++q) ok &= make_box_map(&vm->own[q], m.f[q], m, PX, ty);
-    ok &= make_box_map(&sm->vx, m.f[0], m, XW, ty + 10);
-    ok &= make_box_map(&sm->vy, m.f[1], m, XW, ty + 10);
-    ok &= make_box_map(&sm->vz, m.f[2], m, XW, ty + 10);
-    ok &= make_box_map(&sm->vx_c, m.f[0], m, PX, ty);
-    ok &= make_box_map(&sm->vy_c, m.f[1], m, PX, ty);
-    ok &= make_box_map(&sm->vz_c, m.f[2], m, PX, ty);
-    const float *own[StrMaps::kOwn] = {m.f[3], m.f[4], m.f[5], m.f[6], m.f[7], m.f[8], m.lam, m.mu,
-                                       m.mxy, m.mxz, m.myz};
-    for (int q = 0; q < StrMaps::kOwn; ++q) ok &= make_box_map(&sm->own[q], own[q], m, PX, ty);
+    for (int q = 0; q < 3; ++q) ok &= fm(&vm->own[q], q, PX, ty);
+    ok &= fm(&sm->vx, 0, XW, ty + 10);
+    ok &= fm(&sm->vy, 1, XW, ty + 10);
+    ok &= fm(&sm->vz, 2, XW, ty + 10);
+    ok &= fm(&sm->vx_c, 0, PX, ty);
+    ok &= fm(&sm->vy_c, 1, PX, ty);
+    ok &= fm(&sm->vz_c, 2, PX, ty);
+    for (int q = 0; q < 6; ++q) ok &= fm(&sm->own[q], 3 + q, PX, ty);
+    const float *med[5] = {m.lam, m.mu, m.mxy, m.mxz, m.myz};
+    for (int q = 0; q < 5; ++q) ok &= make_box_map(&sm->own[6 + q], med[q], m, PX, ty);
     if (!ok) return cudaErrorInvalidValue;
-    cudaError_t e = set_attrs<false>();
-    if (e == cudaSuccess) e = set_attrs<true>();
+    if (!hs) {
+        cudaError_t e = set_attrs<false, SGFD_STORE_F32>();
+        return e == cudaSuccess ? set_attrs<true, SGFD_STORE_F32>() : e;
+    }
+    cudaError_t e = set_attrs<false, SGFD_STORE_BF16>();
+    if (e == cudaSuccess) e = set_attrs<true, SGFD_STORE_BF16>();
+    if (e == cudaSuccess) e = set_attrs<false, SGFD_STORE_F16>();
+    if (e == cudaSuccess) e = set_attrs<true, SGFD_STORE_F16>();
     return e;
 }
 
@@ -951,13 +1123,13 @@ void zpair_tiles(const Model &m, int *ntx, int *nty) {
     *nty = (m.nyc + PY - 1) / PY;
 }
 
-cudaError_t zpair_step(const Model &m, const Physics &ph, const SourceRec &sr, const ZGeom &g, const VelMaps &vm,
-                       const StrMaps &sm, int it, float src_value, bool use_wavelet, cudaStream_t s,
+cudaError_t zpair_step(const Model &m, const Physics &ph, const SourceRec &sr, const HalfState *hs, const ZGeom &g,
+                       const VelMaps &vm, const StrMaps &sm, int it, float src_value, bool use_wavelet, cudaStream_t s,
                        cudaEvent_t *ev) {
-    const int uw = use_wavelet ? 1 : 0;
-    if (ph.fast) launch<true>(m, ph, sr, g, vm, sm, it, src_value, uw, s, ev);
-    else launch<false>(m, ph, sr, g, vm, sm, it, src_value, uw, s, ev);
-    return cudaGetLastError();
+    if (!hs) return launch_st<SGFD_STORE_F32>(m, ph, sr, HalfState{}, g, vm, sm, it, src_value, use_wavelet, s, ev);
+    if (hs->storage == SGFD_STORE_BF16)
+        return launch_st<SGFD_STORE_BF16>(m, ph, sr, *hs, g, vm, sm, it, src_value, use_wavelet, s, ev);
+    return launch_st<SGFD_STORE_F16>(m, ph, sr, *hs, g, vm, sm, it, src_value, use_wavelet, s, ev);
 }
 
 }  // namespace sgfd

@@ -111,11 +111,12 @@ int get_scale_exponents(sgfd_solver *h, int *e) {
 
 cudaError_t dispatch_on(sgfd_solver *h, const SourceRec &sr, cudaStream_t s, int it, float value,
                         bool use_wavelet, cudaEvent_t *ev) {
-    cudaError_t e = h->storage != SGFD_STORE_F32
-                        ? half_step(h->m, h->ph, sr, h->hs, it, value, use_wavelet, s, ev)
-                    : h->kernel == SGFD_KERNEL_ZMARCH
-                        ? (h->zg.pair ? zpair_step(h->m, h->ph, sr, h->zg, h->vm, h->sm, it, value, use_wavelet, s, ev)
+    const bool h16 = h->storage != SGFD_STORE_F32;
+    cudaError_t e = h->kernel == SGFD_KERNEL_ZMARCH
+                        ? (h->zg.pair ? zpair_step(h->m, h->ph, sr, h16 ? &h->hs : nullptr, h->zg, h->vm, h->sm, it,
+                                                   value, use_wavelet, s, ev)
                                       : zmarch_step(h->m, h->ph, sr, h->zg, h->vm, h->sm, it, value, use_wavelet, s, ev))
+                    : h16 ? half_step(h->m, h->ph, sr, h->hs, it, value, use_wavelet, s, ev)
                         : simple_step(h->m, h->ph, sr, it, value, use_wavelet, s, ev);
     if (e == cudaSuccess && h->strip_n > 0)
         e = launch_strip(h->m, h->strip_w, h->strip_cells, h->strip_n, h->strip_buf, s);
@@ -404,8 +405,6 @@ int sgfd_create(const sgfd_config *cfg, sgfd_solver **out) {
         return fail(nullptr, SGFD_ERR_INVALID, "unknown quirks mode %d", c.quirks);
     if (c.storage != SGFD_STORE_F32 && c.storage != SGFD_STORE_BF16 && c.storage != SGFD_STORE_F16)
         return fail(nullptr, SGFD_ERR_UNSUPPORTED, "storage type %d is not built into this library", c.storage);
-    if (c.storage != SGFD_STORE_F32 && c.kernel == SGFD_KERNEL_ZMARCH)
-        return fail(nullptr, SGFD_ERR_UNSUPPORTED, "16-bit storage runs on the per-cell kernels only");
     if (c.kernel != SGFD_KERNEL_AUTO && c.kernel != SGFD_KERNEL_SIMPLE && c.kernel != SGFD_KERNEL_ZMARCH)
         return fail(nullptr, SGFD_ERR_UNSUPPORTED, "kernel family %d is not built into this library", c.kernel);
     const int64_t cells = (int64_t)c.nx * c.ny * c.nz;
@@ -501,11 +500,13 @@ int sgfd_create(const sgfd_config *cfg, sgfd_solver **out) {
         if (r) { g_error = h->err; sgfd_destroy(h); return r; }
     }
 
-    if (c.kernel != SGFD_KERNEL_SIMPLE && c.storage == SGFD_STORE_F32 && zmarch_supported(m)) {
+    if (c.kernel != SGFD_KERNEL_SIMPLE && zmarch_supported(m)) {
+        // FP32: 32 x 8 tiles; 16-bit storage: the paired tiling, the only one built for it
+        const bool h16 = c.storage != SGFD_STORE_F32;
         h->zg.cells = 1;
-        h->zg.pair = 0;
-        h->zg.tw = kZTileX;
-        e = zmarch_prepare(m, h->zg.cells, &h->vm, &h->sm);
+        h->zg.pair = h16 ? 1 : 0;
+        h->zg.tw = h16 ? kPairTileX : kZTileX;
+        e = h16 ? zpair_prepare(m, &h->hs, &h->vm, &h->sm) : zmarch_prepare(m, h->zg.cells, &h->vm, &h->sm);
         if (e == cudaSuccess) e = dev_malloc(h, &h->dev_err, sizeof(int));
         if (e == cudaSuccess) e = cudaMemset(h->dev_err, 0, sizeof(int));
         if (e != cudaSuccess) {
@@ -514,7 +515,8 @@ int sgfd_create(const sgfd_config *cfg, sgfd_solver **out) {
             return r;
         }
         h->kernel = SGFD_KERNEL_ZMARCH;
-        zmarch_tiles(m, h->zg.cells, &h->zg.ntx, &h->zg.nty);
+        if (h16) zpair_tiles(m, &h->zg.ntx, &h->zg.nty);
+        else zmarch_tiles(m, h->zg.cells, &h->zg.ntx, &h->zg.nty);
         h->zg.err = h->dev_err;
         set_zchunks(h);
         int r = upload_zrec(h, {});
@@ -766,10 +768,13 @@ int sgfd_set_tile(sgfd_solver *h, int32_t tile_cols, int32_t tile_rows, int32_t 
         return fail(h, SGFD_ERR_INVALID, "tiles are 32 x 8, 32 x 16 or 64 x 8");
     if (zchunk < 0) return fail(h, SGFD_ERR_INVALID, "negative chunk");
     if (!h->dev_err) return SGFD_OK;   // no z-marching kernels prepared: nothing to tile
+    if (h->storage != SGFD_STORE_F32 && !pair)
+        return fail(h, SGFD_ERR_UNSUPPORTED, "16-bit storage runs on 64 x 8 tiles only");
     SG_CUDA(h, cudaStreamSynchronize(h->stream), "synchronise before re-tiling");
     const int cells = tile_rows / 8;
     if (cells != h->zg.cells || (int)pair != h->zg.pair) {
-        cudaError_t e = pair ? zpair_prepare(h->m, &h->vm, &h->sm) : zmarch_prepare(h->m, cells, &h->vm, &h->sm);
+        cudaError_t e = pair ? zpair_prepare(h->m, h->storage != SGFD_STORE_F32 ? &h->hs : nullptr, &h->vm, &h->sm)
+                             : zmarch_prepare(h->m, cells, &h->vm, &h->sm);
         if (e != cudaSuccess) return cuda_fail(h, e, "z-march re-tiling");
         h->zg.cells = cells;
         h->zg.pair = pair ? 1 : 0;
@@ -1028,7 +1033,7 @@ int sgfd_device_allocations(const sgfd_solver *h, int64_t *count) {
 int sgfd_launches_per_step(const sgfd_solver *h) {
     if (!h) return -1;
     const int audit = (h->audit_every > 0 ? 2 : 0) + (h->strip_n > 0 ? 2 : 0);
-    if (h->storage != SGFD_STORE_F32) return half_launches_per_step(h->sr) + audit;
+    if (h->storage != SGFD_STORE_F32) return half_launches_per_step(h->sr) + audit;   // either family
     if (h->kernel == SGFD_KERNEL_ZMARCH) return 2 + audit;
     return simple_launches_per_step(h->sr) + audit;
 }

@@ -110,6 +110,14 @@ struct SourceRec {
 __device__ __forceinline__ int step_index(const SourceRec &sr, int it_arg) {
     return sr.it_dev ? it_arg + *sr.it_dev : it_arg;
 }
+// 16-bit storage: the steps after which the scales are re-chosen (it + 1 a
+// power of two up to kRescaleEvery, then every kRescaleEvery steps); their
+// updates note each field's largest written magnitude.
+__device__ __forceinline__ bool rescale_step16(int it) {
+    const int n = it + 1;
+    if (n <= 0) return false;
+    return (n <= kRescaleEvery && (n & (n - 1)) == 0) || n % kRescaleEvery == 0;
+}
 #endif
 
 __host__ __device__ inline int64_t pidx(const Model &m, int x, int y, int z) {
@@ -216,6 +224,11 @@ cudaError_t launch_energy_step(const Model &m, const Physics &ph, int region, do
 cudaError_t half_step(const Model &m, const Physics &ph, const SourceRec &sr, const HalfState &hs, int it,
                       float src_value, bool use_wavelet, cudaStream_t s, cudaEvent_t *ev = nullptr);
 int half_launches_per_step(const SourceRec &sr);
+// The 16-bit step's kernels around the two updates, for update kernels of
+// another family: phase 0 the source injection (before the velocity update),
+// 1 the velocity receivers, 2 the stress receivers and the rescale kernels.
+cudaError_t half_phase(const Model &m, const Physics &ph, const SourceRec &sr, const HalfState &hs, int it,
+                       float src_value, bool use_wavelet, cudaStream_t s, int phase);
 cudaError_t half_to_views(const Model &m, const HalfState &hs, cudaStream_t s);
 cudaError_t half_from_views(const Model &m, const HalfState &hs, cudaStream_t s);
 // *ctr = value, or *ctr += value when add is set.

@@ -42,8 +42,10 @@ struct ZGeom {
     int *err;               // device error flag (1: a bounded wait gave up)
 };
 
-// 3-D FP32 tensor map over one padded device array with a bx x by x 1 box.
+// 3-D FP32 tensor map over one padded device array with a bx x by x 1 box;
+// the same over a 16-bit array of the same layout.
 bool make_box_map(CUtensorMap *map, const float *grid_origin, const Model &m, int bx, int by);
+bool make_box_map16(CUtensorMap *map, const uint16_t *grid_origin, const Model &m, int bx, int by);
 
 bool zmarch_supported(const Model &m);
 cudaError_t zmarch_prepare(const Model &m, int cells, VelMaps *vm, StrMaps *sm);
@@ -68,10 +70,12 @@ struct alignas(64) PairModel {
 constexpr int kBatchWaitTma = 1, kBatchWaitGrid = 2;
 
 // Paired tiling: tensor maps, tile counts and one step (velocity + stress).
-cudaError_t zpair_prepare(const Model &m, VelMaps *vm, StrMaps *sm);
+// hs: null for FP32 storage, else the 16-bit storage state (the step then
+// also launches the 16-bit source, receiver and rescale kernels).
+cudaError_t zpair_prepare(const Model &m, const HalfState *hs, VelMaps *vm, StrMaps *sm);
 void zpair_tiles(const Model &m, int *ntx, int *nty);
-cudaError_t zpair_step(const Model &m, const Physics &ph, const SourceRec &sr, const ZGeom &g, const VelMaps &vm,
-                       const StrMaps &sm, int it, float src_value, bool use_wavelet, cudaStream_t s,
+cudaError_t zpair_step(const Model &m, const Physics &ph, const SourceRec &sr, const HalfState *hs, const ZGeom &g,
+                       const VelMaps &vm, const StrMaps &sm, int it, float src_value, bool use_wavelet, cudaStream_t s,
                        cudaEvent_t *ev = nullptr);
 // Persistent batch: CTAs that fit at once on the device (cooperative launch),
 // and nsteps steps of all models in one launch.  first_item[nmodels + 1]:
