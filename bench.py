@@ -60,7 +60,7 @@ def parse():
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", choices=["sgfd", "reference"], default="sgfd")
     p.add_argument("--workload", choices=["random344", "random472", "random216", "plain100", "reference_main",
-                                               "batch32", "learned256"],
+                                               "batch32", "learned256", "combined32"],
                    default="random344")
     p.add_argument("--no-autotune", action="store_true", help="batch32: keep the default launch shapes")
     p.add_argument("--batch-mode", choices=["persistent", "graph"], default="persistent",
@@ -275,7 +275,7 @@ def main():
         # CPU arm: rank 0 alone runs it, no process group is needed
         rank = int(os.environ.get("RANK", "0"))
         if rank == 0:
-            if args.workload == "batch32":
+            if args.workload in ("batch32", "combined32"):
                 import sgfd.workloads as wl
                 w = wl.layered_model(wl.batch_specs()[0])
                 w.name = "batch32 (sample: model 0, %s)" % w.name
@@ -284,7 +284,7 @@ def main():
                 run_reference_arm(args, build_workload(args.workload), 1, 0)
         return
     world, rank, local = dist_setup(args)
-    if args.workload == "batch32":
+    if args.workload in ("batch32", "combined32"):
         main_batch(args, world, rank, local)
         return
     if args.workload == "learned256":
@@ -539,12 +539,26 @@ def main_batch(args, world, rank, local):
     run over all models' work items (--batch-mode graph: 16-step graphs, one
     branch per model, autotuned launch shapes).  With N ranks the models are dealt out by computed cells (greedy,
     largest first); value = all ranks' cells x steps / slowest rank's time."""
+    import dataclasses
     import torch
     import sgfd
+    import sgfd.learned as L
     import sgfd.workloads as wl
     torch.cuda.set_device(local)
     K, W = args.steps, args.warmup
+    combined = args.workload == "combined32"
+    storage = args.storage if not (combined and args.storage == "f32") else "f16"
+    mode = args.batch_mode if storage == "f32" else "graph"      # the persistent kernel is FP32-only
+    arith = sgfd.ARITH_FAST if args.arith == "fast" else sgfd.ARITH_REF
     specs = wl.batch_specs()
+    gate = None
+    if combined:
+        # the learned strip is used only where its gate (calibration against the
+        # 20-cell PML) accepts it; otherwise every model keeps its PML
+        gate = L.gate(L.load_params(), nt=400, device=local)
+        if gate["boundary"] == "learned_strip":
+            specs = [dataclasses.replace(sp, pml=0, n_interior=sp.n_interior + 2 * L.WIDTH,
+                                         src=tuple(v - sp.pml + L.WIDTH for v in sp.src)) for sp in specs]
     cells_all = [sp.computed_cells() for sp in specs]
     mine = wl.balance(cells_all, world)[rank]
     models, media, tunings = [], [], []
@@ -553,12 +567,15 @@ def main_batch(args, world, rank, local):
         w = wl.layered_model(specs[i])
         nt = max(w.nt, W + K + 16)
         wav = np.resize(w.wavelet, nt).astype(np.float32)
-        s = sgfd.Solver(sgfd.default_config(**{**w.cfg, "device": local, "arith": sgfd.ARITH_FAST if args.arith == "fast" else sgfd.ARITH_REF}))
+        s = sgfd.Solver(sgfd.default_config(**{**w.cfg, "device": local, "arith": arith,
+                                               "storage": STORAGE[storage]}))
         s.set_medium(w.b, w.lam, w.mu)
         s.set_source(*w.src)
         s.set_receivers(w.rec_xyz, w.rec_comp, nt)
         s.set_wavelet(wav)
-        if not args.no_autotune and args.batch_mode == "graph":
+        if gate is not None and gate["boundary"] == "learned_strip":
+            s.set_learned_strip(L.WIDTH, L.load_params())
+        if not args.no_autotune and mode == "graph":
             t = s.autotune(3)
             tunings.append({"model": i, "kernel": "zmarch" if t.kernel == sgfd.KERNEL_ZMARCH else "simple",
                             "tile_rows": t.tile_rows, "zchunk": t.zchunk, "ms": round(t.ms_per_step, 4)})
@@ -568,7 +585,7 @@ def main_batch(args, world, rank, local):
         models.append(s)
         media.append((w.b, w.lam, w.mu, len(w.rec_comp)))
     batch = sgfd.Batch(models)
-    if args.batch_mode == "persistent":
+    if mode == "persistent":
         batch.set_persistent(True)
     stream = torch.cuda.ExternalStream(batch.stream())
     batch.run(0, W)
@@ -595,7 +612,8 @@ def main_batch(args, world, rank, local):
     total_cells = sum(cells_all)
     value = total_cells * K / (ms / 1e3) / 1e9
     peak, peak_kind = measured_peak()
-    alg = 120 * n_int + 276 * n_pml                 # this rank's bytes per step
+    bpc = BYTES if storage == "f32" else BYTES16
+    alg = (sum(v[0] for v in bpc.values()) * n_int + sum(v[1] for v in bpc.values()) * n_pml)   # this rank's bytes
     achieved = alg / (ms / K / 1e3) / 1e9
     roof = {"bound": "hbm", "kernel": "batch step (all models' velocity + stress kernels, overlapped)",
             "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
@@ -629,15 +647,28 @@ def main_batch(args, world, rank, local):
     result = {
         "metric": "Gcell-updates/s", "value": value, "unit": "Gcell/s", "n_gpus": world, "steps": K,
         "warmup": W, "ms_per_step": ms / K, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
-        "dtype": "f32", "data": "synthetic",
-        "config": {"workload": "batch32", "models": len(specs), "computed_cells": total_cells,
+        "dtype": "f32" if storage == "f32" else f"f32 arithmetic, {storage} storage", "data": "synthetic",
+        "config": {"workload": args.workload, "models": len(specs), "computed_cells": total_cells, "storage": storage,
                    "models_this_rank": len(mine), "interior_cells_rank0": n_int, "pml_cells_rank0": n_pml,
                    "arith": args.arith, "parallelism": f"replicas{world} (models dealt by cells)",
-                   "batch_mode": args.batch_mode,
+                   "batch_mode": mode,
                    "autotune": tunings or "off",
                    "l2": "inputs larger than L2 (%.1f GB of wavefields)" % (sum(cells_all) * 36 / 1e9)},
         "roofline": roof, "clocks": clk, "gpu_launches": launches, "e2e": e2e,
     }
+    if gate is not None:
+        result["gate"] = {k: gate[k] for k in ("boundary", "faces_accept", "steps", "learned_final_over_peak",
+                                               "pml_final_over_peak")}
+    if rank == 0 and world == 1 and not args.no_accuracy:
+        # the batch's smallest model alone, 300 steps, against the FP64 oracle
+        k0 = min(range(len(specs)), key=lambda k: cells_all[k])
+        sp = dataclasses.replace(specs[k0], nt=300)
+        wa = wl.layered_model(sp)
+        if gate is not None and gate["boundary"] == "learned_strip":
+            result["accuracy"] = {"note": "a learned-strip model has no FP64 oracle counterpart"}
+        else:
+            args_acc = argparse.Namespace(**{**vars(args), "storage": storage})
+            result["accuracy"] = accuracy_leg(wa, args_acc, local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         w0 = wl.layered_model(specs[0])
         rate, threads, secs = cpu_oracle_rate(w0, args.cpu_steps)
