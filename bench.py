@@ -237,7 +237,34 @@ def run_reference_arm(args, w, world, rank):
     ref_bin = os.path.join(ROOT, "oracle", "_ref", "ref_opt")
     if os.path.exists(ref_bin):
         line["gpu_reference"] = reference_gpu_program(ref_bin, w, steps=min(max(args.steps, 20), 200))
+    cpml = cpu_reference_program()
+    if cpml:
+        line["cpu_reference_program"] = cpml
     print(json.dumps(line), flush=True)
+
+
+def cpu_reference_program(steps: int = 8):
+    """The reference's own CPU program (3DCPUwithPML_3DArray_GridIncludePMLandOrder,
+    its split-field PML everywhere in the PML, 3-D arrays), built from its
+    sources by oracle/Makefile behind a timing harness, on its main.cpp's grid
+    (101^3 interior + 10-cell PML), single thread as shipped, flush-to-zero
+    off and on.  None if it was not built."""
+    exe = os.path.join(ROOT, "oracle", "_ref", "cpml_bench")
+    if not os.path.exists(exe):
+        return None
+    out = {}
+    with tempfile.TemporaryDirectory() as d:   # it writes its damping profiles to the working directory
+        for ftz in (0, 1):
+            r = subprocess.run([exe, "101", "10", str(steps), str(ftz)], cwd=d, capture_output=True, text=True,
+                               timeout=600)
+            if r.returncode != 0:
+                return {"error": r.stderr[-300:]}
+            tok = dict(t.split("=") for t in r.stdout.split() if t.startswith(("cells=", "steps=", "seconds=")))
+            out["ftz_on" if ftz else "ftz_off"] = int(tok["cells"]) * int(tok["steps"]) / float(tok["seconds"]) / 1e9
+    return {"value": out["ftz_off"], "unit": "Gcell/s", "cores": 1, "ftz_on": out["ftz_on"],
+            "sample": f"{steps} steps of the reference CPU program's own case (101^3 interior + 10-cell PML, "
+                      f"131^3 arrays) after 1 untimed step; its split fields cover the whole PML and its profile "
+                      f"uses a constant velocity, so it does more work per PML cell than the GPU program"}
 
 
 def write_case(path, w, nt):
@@ -315,6 +342,9 @@ def main():
             "value": rate, "unit": "Gcell/s", "cores": threads, "kind": "port",
             "sample": f"{args.cpu_steps} full time steps of {w.name} ({secs:.1f} s) after 1 untimed step; "
                       f"C++ oracle of the reference kernels, FP32, flush-to-zero, OpenMP {threads} threads"}
+        cpml = cpu_reference_program()
+        if cpml:
+            result["cpu_reference_program"] = cpml
     if rank == 0 and world == 1 and not args.no_accuracy:
         result["accuracy"] = accuracy_leg(w, args, local)
     # the other rounding mode on the same model, for comparison
