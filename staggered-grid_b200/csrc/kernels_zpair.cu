@@ -380,19 +380,22 @@ __device__ __forceinline__ bool vel_pair(const VelMaps &mp, const Model &m, cons
     const PairCtx pc = pair_ctx(m, t, lx, ly);
     const uint32_t PL = (uint32_t)m.plane;
 
-    // z queues (both cells): qxz, qyz hold z-5..z+4, qzz holds z-4..z+5 (filled 9 deep here)
-    float2 qxz[10], qyz[10], qzz[10];
+    // z queues (both cells), 11 deep: planes are taken two at a time, the
+    // even plane of a pair reads entries 0..9, the odd one 1..10, and the
+    // queues move by two after the odd plane.  qxz, qyz hold z-5..z+4 and qzz
+    // z-4..z+5 of the even plane; filled 9 deep here.
+    float2 qxz[11], qyz[11], qzz[11];
     const int gz0 = t.zs + kHalo;
 #pragma unroll
     for (int k = 0; k < 9; ++k) {
-        qxz[k + 1] = SA::pair(F.f(7) + pc.col + (uint32_t)(gz0 - 5 + k) * PL, bcast(F.sc(7)));
-        qyz[k + 1] = SA::pair(F.f(8) + pc.col + (uint32_t)(gz0 - 5 + k) * PL, bcast(F.sc(8)));
+        qxz[k] = SA::pair(F.f(7) + pc.col + (uint32_t)(gz0 - 5 + k) * PL, bcast(F.sc(7)));
+        qyz[k] = SA::pair(F.f(8) + pc.col + (uint32_t)(gz0 - 5 + k) * PL, bcast(F.sc(8)));
         float2 zz = SA::pair(F.f(5) + pc.col + (uint32_t)(gz0 - 4 + k) * PL, bcast(F.sc(5)));
         if (!H && pc.gy == sy && gz0 - 4 + k == sz) {
             if (pc.gx == sx) zz.x = zz.x + inj;
             if (pc.gx + 1 == sx) zz.y = zz.y + inj;
         }
-        qzz[k + 1] = zz;
+        qzz[k] = zz;
     }
 
     // receivers of this tile, sorted by z: skip those below the chunk
@@ -406,10 +409,12 @@ __device__ __forceinline__ bool vel_pair(const VelMaps &mp, const Model &m, cons
     const bool src_near = !H && sr.src >= 0 && sy >= t.gy0 - 5 && sy < t.gy0 + PY + 5 && sx >= t.gx0 - 8 &&
                           sx < t.gx0 + PX + 8;
     // One plane.  GEN selects the general path (PML cells, source, receivers);
-    // every other tile-plane takes the packed interior path.  Returns false
-    // when the block votes to abort.
-    auto plane = [&](auto gen_tag) -> bool {
+    // every other tile-plane takes the packed interior path.  ODD: the second
+    // plane of a pair (queue window one entry further).  Returns false when
+    // the block votes to abort.
+    auto plane = [&](auto gen_tag, auto odd_tag) -> bool {
         constexpr bool GEN = decltype(gen_tag)::value;
+        constexpr int Q = decltype(odd_tag)::value ? 1 : 0;
         const int s = stage;
         unsigned char *st = smem + s * L::STAGE;
         const int gz = cz + kHalo;
@@ -446,16 +451,10 @@ __device__ __forceinline__ bool vel_pair(const VelMaps &mp, const Model &m, cons
         constexpr int OVS = L::OBE / SA::ES;        // values between the own-velocity boxes
         const int e = ly * PX + 2 * lx;             // 64 x 8 box index of cell 0
 
-        // advance the z queues
-#pragma unroll
-        for (int j = 0; j < 9; ++j) {
-            qxz[j] = qxz[j + 1];
-            qyz[j] = qyz[j + 1];
-            qzz[j] = qzz[j + 1];
-        }
-        qxz[9] = SA::pair(reinterpret_cast<const E *>(st + L::LXZ) + e, bcast(F.sc(7)));
-        qyz[9] = SA::pair(reinterpret_cast<const E *>(st + L::LYZ) + e, bcast(F.sc(8)));
-        qzz[9] = SA::pair(reinterpret_cast<const E *>(st + L::LZZ) + e, bcast(F.sc(5)));
+        // the lead planes enter the z queues
+        qxz[9 + Q] = SA::pair(reinterpret_cast<const E *>(st + L::LXZ) + e, bcast(F.sc(7)));
+        qyz[9 + Q] = SA::pair(reinterpret_cast<const E *>(st + L::LYZ) + e, bcast(F.sc(8)));
+        qzz[9 + Q] = SA::pair(reinterpret_cast<const E *>(st + L::LZZ) + e, bcast(F.sc(5)));
 
         if (pc.act0) {
             // x differences, per cell, from 12-value windows
@@ -474,9 +473,9 @@ __device__ __forceinline__ bool vel_pair(const VelMaps &mp, const Model &m, cons
             const float2 xY = dB2p<FAST, 1>(ph, [&](int o) { return SA::pair(cxy + o * XW, s6); });
             const float2 yY = dF2p<FAST, 1>(ph, [&](int o) { return SA::pair(cyy + o * PX, s4); });
             const float2 zY = dB2p<FAST, 1>(ph, [&](int o) { return SA::pair(cyz + o * PX, s8); });
-            const float2 xZ = dB2p<FAST, 2>(ph, [&](int o) { return qxz[5 + o]; });
-            const float2 yZ = dB2p<FAST, 2>(ph, [&](int o) { return qyz[5 + o]; });
-            const float2 zZ = dF2p<FAST, 2>(ph, [&](int o) { return qzz[4 + o]; });
+            const float2 xZ = dB2p<FAST, 2>(ph, [&](int o) { return qxz[Q + 5 + o]; });
+            const float2 yZ = dB2p<FAST, 2>(ph, [&](int o) { return qyz[Q + 5 + o]; });
+            const float2 zZ = dF2p<FAST, 2>(ph, [&](int o) { return qzz[Q + 4 + o]; });
 
             const float2 b0 = ld2(bb + ly * BW + 2 * lx);
             const float2 bxp = make_float2(b0.y, bb[ly * BW + 2 * lx + 2]);
@@ -585,6 +584,14 @@ __device__ __forceinline__ bool vel_pair(const VelMaps &mp, const Model &m, cons
             while (rp < rend && g.rec_list[rp].z == gz) ++rp;
             rz = rp < rend ? g.rec_list[rp].z : 0x7fffffff;
         }
+        if constexpr (Q == 1) {   // after a pair of planes the queues move by two
+#pragma unroll
+            for (int j = 0; j < 9; ++j) {
+                qxz[j] = qxz[j + 2];
+                qyz[j] = qyz[j + 2];
+                qzz[j] = qzz[j + 2];
+            }
+        }
 
         // every thread is done with this stage: vote on aborts, then refill it
         if (__syncthreads_or(failed)) return false;
@@ -598,11 +605,15 @@ __device__ __forceinline__ bool vel_pair(const VelMaps &mp, const Model &m, cons
         if (++stage == S) stage = 0;
         return true;
     };
+    using T1 = std::true_type;
+    using T0 = std::false_type;
     for (; cz < t.ze; ++cz) {
         const int gzp = cz + kHalo;
         const bool gen = t.xy_pml || band(gzp, m.nz, m.pml) != 0 || (src_near && (gzp == sz || gzp + 5 == sz)) ||
                          gzp == rz;
-        if (!(gen ? plane(std::true_type{}) : plane(std::false_type{}))) {
+        const bool odd = ((cz - t.zs) & 1) != 0;
+        const bool ok = odd ? (gen ? plane(T1{}, T1{}) : plane(T0{}, T1{})) : (gen ? plane(T1{}, T0{}) : plane(T0{}, T0{}));
+        if (!ok) {
             abort = true;
             break;
         }
@@ -660,14 +671,16 @@ __device__ __forceinline__ bool str_pair(const StrMaps &mp, const Model &m, cons
     const PairCtx pc = pair_ctx(m, t, lx, ly);
     const uint32_t PL = (uint32_t)m.plane;
 
-    // z queues (both cells): qx, qy hold z-4..z+5 (vx, vy); qz holds z-5..z+4 (vz)
-    float2 qx[10], qy[10], qz[10];
+    // z queues (both cells), 11 deep and taken two planes at a time as in
+    // the velocity update: qx, qy hold z-4..z+5 (vx, vy), qz holds z-5..z+4
+    // (vz) of the even plane
+    float2 qx[11], qy[11], qz[11];
     const int gz0 = t.zs + kHalo;
 #pragma unroll
     for (int k = 0; k < 9; ++k) {
-        qx[k + 1] = SA::pair(F.f(0) + pc.col + (uint32_t)(gz0 - 4 + k) * PL, bcast(F.sc(0)));
-        qy[k + 1] = SA::pair(F.f(1) + pc.col + (uint32_t)(gz0 - 4 + k) * PL, bcast(F.sc(1)));
-        qz[k + 1] = SA::pair(F.f(2) + pc.col + (uint32_t)(gz0 - 5 + k) * PL, bcast(F.sc(2)));
+        qx[k] = SA::pair(F.f(0) + pc.col + (uint32_t)(gz0 - 4 + k) * PL, bcast(F.sc(0)));
+        qy[k] = SA::pair(F.f(1) + pc.col + (uint32_t)(gz0 - 4 + k) * PL, bcast(F.sc(1)));
+        qz[k] = SA::pair(F.f(2) + pc.col + (uint32_t)(gz0 - 5 + k) * PL, bcast(F.sc(2)));
     }
 
     int rp = H ? 0 : g.rec_off[tile];
@@ -678,8 +691,9 @@ __device__ __forceinline__ bool str_pair(const StrMaps &mp, const Model &m, cons
     bool failed = false, abort = false;
     int cz = t.zs;
     const int sz = src >= 0 ? (int)(src / m.plane) : -1;
-    auto plane = [&](auto gen_tag) -> bool {
+    auto plane = [&](auto gen_tag, auto odd_tag) -> bool {
         constexpr bool GEN = decltype(gen_tag)::value;
+        constexpr int Q = decltype(odd_tag)::value ? 1 : 0;
         const int s = stage;
         unsigned char *st = smem + s * L::STAGE;
         const int gz = cz + kHalo;
@@ -698,15 +712,9 @@ __device__ __forceinline__ bool str_pair(const StrMaps &mp, const Model &m, cons
         constexpr int OS = L::OBE / SA::ES, MS = OB / 4;
         const int e = ly * PX + 2 * lx;
 
-#pragma unroll
-        for (int j = 0; j < 9; ++j) {
-            qx[j] = qx[j + 1];
-            qy[j] = qy[j + 1];
-            qz[j] = qz[j + 1];
-        }
-        qx[9] = SA::pair(reinterpret_cast<const E *>(st + L::LX) + e, bcast(F.sc(0)));
-        qy[9] = SA::pair(reinterpret_cast<const E *>(st + L::LY) + e, bcast(F.sc(1)));
-        qz[9] = SA::pair(reinterpret_cast<const E *>(st + L::LZ) + e, bcast(F.sc(2)));
+        qx[9 + Q] = SA::pair(reinterpret_cast<const E *>(st + L::LX) + e, bcast(F.sc(0)));
+        qy[9 + Q] = SA::pair(reinterpret_cast<const E *>(st + L::LY) + e, bcast(F.sc(1)));
+        qz[9 + Q] = SA::pair(reinterpret_cast<const E *>(st + L::LZ) + e, bcast(F.sc(2)));
 
         if (pc.act0) {
             float w[12];
@@ -723,9 +731,9 @@ __device__ __forceinline__ bool str_pair(const StrMaps &mp, const Model &m, cons
             const float2 dYy = dB2p<FAST, 1>(ph, [&](int o) { return SA::pair(cy_ + o * XW, s1); });
             const float2 xyY = dF2p<FAST, 1>(ph, [&](int o) { return SA::pair(cx_ + o * XW, s0); });
             const float2 yzY = dF2p<FAST, 1>(ph, [&](int o) { return SA::pair(cz_ + o * XW, s2); });
-            const float2 xzZ = dF2p<FAST, 2>(ph, [&](int o) { return qx[4 + o]; });
-            const float2 yzZ = dF2p<FAST, 2>(ph, [&](int o) { return qy[4 + o]; });
-            const float2 dZz = dB2p<FAST, 2>(ph, [&](int o) { return qz[5 + o]; });
+            const float2 xzZ = dF2p<FAST, 2>(ph, [&](int o) { return qx[Q + 4 + o]; });
+            const float2 yzZ = dF2p<FAST, 2>(ph, [&](int o) { return qy[Q + 4 + o]; });
+            const float2 dZz = dB2p<FAST, 2>(ph, [&](int o) { return qz[Q + 5 + o]; });
 
             const float2 l = ld2(med + e), mu2 = ld2(med + MS + e);
             const float2 l2m = __ffma2_rn(bcast(2.0f), mu2, l);
@@ -848,6 +856,14 @@ __device__ __forceinline__ bool str_pair(const StrMaps &mp, const Model &m, cons
             while (rp < rend && g.rec_list[rp].z == gz) ++rp;
             rz = rp < rend ? g.rec_list[rp].z : 0x7fffffff;
         }
+        if constexpr (Q == 1) {
+#pragma unroll
+            for (int j = 0; j < 9; ++j) {
+                qx[j] = qx[j + 2];
+                qy[j] = qy[j + 2];
+                qz[j] = qz[j + 2];
+            }
+        }
 
         if (__syncthreads_or(failed)) return false;
         if (cz + S < t.ze) {
@@ -860,10 +876,14 @@ __device__ __forceinline__ bool str_pair(const StrMaps &mp, const Model &m, cons
         if (++stage == S) stage = 0;
         return true;
     };
+    using T1 = std::true_type;
+    using T0 = std::false_type;
     for (; cz < t.ze; ++cz) {
         const int gzp = cz + kHalo;
         const bool gen = t.xy_pml || band(gzp, m.nz, m.pml) != 0 || gzp == sz || gzp == rz;
-        if (!(gen ? plane(std::true_type{}) : plane(std::false_type{}))) {
+        const bool odd = ((cz - t.zs) & 1) != 0;
+        const bool ok = odd ? (gen ? plane(T1{}, T1{}) : plane(T0{}, T1{})) : (gen ? plane(T1{}, T0{}) : plane(T0{}, T0{}));
+        if (!ok) {
             abort = true;
             break;
         }
