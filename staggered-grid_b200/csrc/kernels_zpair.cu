@@ -231,30 +231,30 @@ template <int ST>
 struct Sto {
     using E = float;
     static constexpr int ES = 4;
-    __device__ static float2 pair(const E *p, float2) { return ld2(p); }
-    __device__ static float one(const E *p, float) { return *p; }
-    __device__ static void win(const E *row, float (&w)[12], float) { window(row, w); }
-    __device__ static void put2(E *p, float2 v, float2, bool both) { st2(p, v, both); }
-    __device__ static void put1(E *p, float v, float) { *p = v; }
+    __device__ __forceinline__ static float2 pair(const E *p, float2) { return ld2(p); }
+    __device__ __forceinline__ static float one(const E *p, float) { return *p; }
+    __device__ __forceinline__ static void win(const E *row, float (&w)[12], float) { window(row, w); }
+    __device__ __forceinline__ static void put2(E *p, float2 v, float2, bool both) { st2(p, v, both); }
+    __device__ __forceinline__ static void put1(E *p, float v, float) { *p = v; }
 };
 template <int ST>
 struct Sto16 {
     using E = uint16_t;
     static constexpr int ES = 2;
-    __device__ static float h2f(uint32_t h) {
+    __device__ __forceinline__ static float h2f(uint32_t h) {
         if (ST == SGFD_STORE_BF16) return __uint_as_float(h << 16);
         return __half2float(__ushort_as_half((unsigned short)h));
     }
-    __device__ static uint32_t f2h(float w) {
+    __device__ __forceinline__ static uint32_t f2h(float w) {
         if (ST == SGFD_STORE_BF16) return __bfloat16_as_ushort(__float2bfloat16_rn(w));
         return __half_as_ushort(__float2half_rn(fminf(fmaxf(w, -65504.0f), 65504.0f)));
     }
-    __device__ static float2 pair(const E *p, float2 sc) {
+    __device__ __forceinline__ static float2 pair(const E *p, float2 sc) {
         const uint32_t u = *reinterpret_cast<const uint32_t *>(p);
         return make_float2(h2f(u & 0xffffu) * sc.x, h2f(u >> 16) * sc.y);
     }
-    __device__ static float one(const E *p, float sc) { return h2f(*p) * sc; }
-    __device__ static void win(const E *row, float (&w)[12], float sc) {
+    __device__ __forceinline__ static float one(const E *p, float sc) { return h2f(*p) * sc; }
+    __device__ __forceinline__ static void win(const E *row, float (&w)[12], float sc) {
 #pragma unroll
         for (int k = 0; k < 6; ++k) {
             const float2 v = pair(row + 2 * k, make_float2(sc, sc));
@@ -262,12 +262,12 @@ struct Sto16 {
             w[2 * k + 1] = v.y;
         }
     }
-    __device__ static void put2(E *p, float2 v, float2 inv, bool both) {
+    __device__ __forceinline__ static void put2(E *p, float2 v, float2 inv, bool both) {
         const float2 q = __fmul2_rn(v, inv);
         if (both) *reinterpret_cast<uint32_t *>(p) = f2h(q.x) | (f2h(q.y) << 16);
         else *p = (E)f2h(q.x);
     }
-    __device__ static void put1(E *p, float v, float inv) { *p = (E)f2h(v * inv); }
+    __device__ __forceinline__ static void put1(E *p, float v, float inv) { *p = (E)f2h(v * inv); }
 };
 template <> struct Sto<SGFD_STORE_BF16> : Sto16<SGFD_STORE_BF16> {};
 template <> struct Sto<SGFD_STORE_F16> : Sto16<SGFD_STORE_F16> {};
@@ -280,20 +280,20 @@ struct Fields {
     using E = typename Sto<ST>::E;
     const Model &m;
     const HalfState &hs;
-    __device__ Fields(const Model &m_, const HalfState &hs_) : m(m_), hs(hs_) {}
-    __device__ E *f(int k) const {
+    __device__ __forceinline__ Fields(const Model &m_, const HalfState &hs_) : m(m_), hs(hs_) {}
+    __device__ __forceinline__ E *f(int k) const {
         if constexpr (ST == SGFD_STORE_F32) return m.f[k];
         else return hs.f[k];
     }
-    __device__ E *split() const {
+    __device__ __forceinline__ E *split() const {
         if constexpr (ST == SGFD_STORE_F32) return m.split;
         else return hs.split;
     }
-    __device__ float sc(int k) const {
+    __device__ __forceinline__ float sc(int k) const {
         if constexpr (ST == SGFD_STORE_F32) return 1.0f;
         else return __ldg(hs.sc + k);
     }
-    __device__ float inv(int k) const {
+    __device__ __forceinline__ float inv(int k) const {
         if constexpr (ST == SGFD_STORE_F32) return 1.0f;
         else return __ldg(hs.inv + k);
     }
@@ -530,10 +530,17 @@ __device__ __forceinline__ bool vel_pair(const VelMaps &mp, const Model &m, cons
                         vnew[2] = __fmaf_rn(ph.dt * lane_of(bz, c), (lane_of(zX, c) + lane_of(zY, c)) + lane_of(zZ, c),
                                             SA::one(ov + 2 * OVS + e + c, F.sc(2)));
                     } else {
+                        // every global load of the cell first: the split stores below could
+                        // alias them as far as the compiler knows, so loads after a store wait
+                        E *sp = F.split() + pml_plane_index(m, c ? pc.pc1 : pc.pc0, cz);
+                        const uint32_t N = (uint32_t)m.npml;
+                        float o[9];
+#pragma unroll
+                        for (int k = 0; k < 9; ++k) o[k] = SA::one(sp + k * N, F.sc(k / 3));
+                        const float mu_c = m.mu[cc], lam_c = ph.damping == 1 ? m.lam[cc] : 0.f;
                         float mx = 1.f, px = 1.f, my = 1.f, py = 1.f, mz = 1.f, pz = 1.f;
                         {
-                            const float v = damp_speed(ph, m.mu[cc], lane_of(b0, c),
-                                                       ph.damping == 1 ? m.lam[cc] : 0.f);
+                            const float v = damp_speed(ph, mu_c, lane_of(b0, c), lam_c);
                             if (kx) damp_factors<FAST>(ph, 0, ph.dx, kx, m.pml, v, mx, px);
                             if (ky) damp_factors<FAST>(ph, 1, ph.dy, ky, m.pml, v, my, py);
                             if (kz) damp_factors<FAST>(ph, 2, ph.dz, kz, m.pml, v, mz, pz);
@@ -542,8 +549,6 @@ __device__ __forceinline__ bool vel_pair(const VelMaps &mp, const Model &m, cons
                         const float bxc = lane_of(bx, c);
                         const float ax = ph.dt * bxc, ay = ph.dt * (ref ? bxc : lane_of(by, c)),
                                     az = ph.dt * (ref ? bxc : lane_of(bz, c));
-                        E *sp = F.split() + pml_plane_index(m, c ? pc.pc1 : pc.pc0, cz);
-                        const uint32_t N = (uint32_t)m.npml;
                         const float dxyz[3][3] = {{lane_of(xX, c), lane_of(xY, c), lane_of(xZ, c)},
                                                   {lane_of(yX, c), lane_of(yY, c), lane_of(yZ, c)},
                                                   {lane_of(zX, c), lane_of(zY, c), lane_of(zZ, c)}};
@@ -555,11 +560,10 @@ __device__ __forceinline__ bool vel_pair(const VelMaps &mp, const Model &m, cons
                             float part[3];
 #pragma unroll
                             for (int a = 0; a < 3; ++a) {
-                                E *spk = sp + (3 * q + a) * N;   // split S_VXX + 3q + a, scale of field q
-                                part[a] = split_update<FAST>(SA::one(spk, F.sc(q)), aq[q], dxyz[q][a], kk[a], mm[a],
-                                                             pp[a]);
+                                // split S_VXX + 3q + a, in the scale of field q
+                                part[a] = split_update<FAST>(o[3 * q + a], aq[q], dxyz[q][a], kk[a], mm[a], pp[a]);
                                 if (track) note_max16(hs, q, part[a]);
-                                SA::put1(spk, part[a], F.inv(q));
+                                SA::put1(sp + (3 * q + a) * N, part[a], F.inv(q));
                             }
                             vnew[q] = (part[0] + part[1]) + part[2];
                         }
@@ -793,14 +797,19 @@ __device__ __forceinline__ bool str_pair(const StrMaps &mp, const Model &m, cons
                         const uint32_t N = (uint32_t)m.npml;
                         // split k, in its field's scale (S_XXX.. -> txx.., two per shear stress)
                         auto grp = [](int k) { return k < S_XYX ? 3 + (k - S_XXX) / 3 : 6 + (k - S_XYX) / 2; };
-                        auto rd = [&](int k) { return SA::one(sp + k * N, F.sc(grp(k))); };
+                        // every global load of the cell first (the split stores could alias them)
+                        float o[15];
+#pragma unroll
+                        for (int k = 0; k < 15; ++k) o[k] = SA::one(sp + (S_XXX + k) * N, F.sc(grp(S_XXX + k)));
+                        const float b_c = m.b[cc];
+                        auto rd = [&](int k) { return o[k - S_XXX]; };
                         auto wr = [&](int k, float v) {
                             if (track) note_max16(hs, grp(k), v);
                             SA::put1(sp + k * N, v, F.inv(grp(k)));
                         };
                         float mx = 1.f, px = 1.f, my = 1.f, py = 1.f, mz = 1.f, pz = 1.f;
                         {
-                            const float v = damp_speed(ph, mu_c, m.b[cc], lc);
+                            const float v = damp_speed(ph, mu_c, b_c, lc);
                             if (kx) damp_factors<FAST>(ph, 0, ph.dx, kx, m.pml, v, mx, px);
                             if (ky) damp_factors<FAST>(ph, 1, ph.dy, ky, m.pml, v, my, py);
                             if (kz) damp_factors<FAST>(ph, 2, ph.dz, kz, m.pml, v, mz, pz);
