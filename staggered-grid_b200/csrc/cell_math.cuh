@@ -13,6 +13,8 @@
 //   split-field updates                      ElasticMacro.h:409-531
 #pragma once
 
+#include <type_traits>
+
 #include "sgfd_internal.h"
 
 namespace sgfd {
@@ -152,14 +154,41 @@ __device__ __forceinline__ float damp_speed(const Physics &ph, float mu, float b
     return 0.0f;
 }
 
+// The divisor of a damped split update as the updates take it: FAST the
+// correctly rounded reciprocal RN(1/p) (the update multiplies by it); REF a
+// 64-bit reciprocal of p within 2^-52 (relative), so that RN32(num * r) is
+// the correctly rounded num / p (recip64).
+template <bool FAST>
+using PDiv = typename std::conditional<FAST, float, double>::type;
+
+// 1/p in double precision within 2^-52 (relative): a single-precision
+// approximation refined by two Newton steps r += r (1 - p r), each squaring
+// the error (2^-21 -> 2^-42 -> below the steps' own rounding).  Then
+// RN32(num * r) = RN32(num / p) for every binary32 num, by the argument of
+// div_cell: the product lies within 2^-52 of num/p, every binary32 midpoint
+// more than 2^-50 away from it.  Divisors outside [2^-100, 2^100] (never a
+// damping divisor, which is at least 1) take a correctly rounded double
+// division instead.
+__device__ __forceinline__ double recip64(float p) {
+    const float ap = fabsf(p);
+    if (!(ap >= 0x1p-100f && ap <= 0x1p100f)) return __drcp_rn((double)p);
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(p));
+    const double pd = (double)p;
+    double r = (double)y;
+    double e = __fma_rn(-pd, r, 1.0);
+    r = __fma_rn(r, e, r);
+    e = __fma_rn(-pd, r, 1.0);
+    return __fma_rn(r, e, r);
+}
+
 // Damping factors of one damped axis at band distance k (1..pml):
 // m = 1 - q r^2 and p = 1 + q r^2 (ElasticMacro.h:26-27 inside
-// 1 -/+ 0.5*dt*DAMPING).  REF returns p; FAST returns RN(1/p) so the split
-// updates multiply instead of divide.  d_axis is dx, dy or dz; v is
-// damp_speed() of the cell.
+// 1 -/+ 0.5*dt*DAMPING), p in the form of PDiv.  d_axis is dx, dy or dz; v
+// is damp_speed() of the cell.
 template <bool FAST>
 __device__ __forceinline__ void damp_factors(const Physics &ph, int axis, float d_axis, int k, int pml, float v,
-                                             float &m, float &p) {
+                                             float &m, PDiv<FAST> &p) {
     float q;
     (void)d_axis;
     if (ph.damping == 0) {                    // SGFD_DAMP_REFGPU
@@ -177,17 +206,20 @@ __device__ __forceinline__ void damp_factors(const Physics &ph, int axis, float 
         pw = r * r;
     }
     m = __fmaf_rn(-q, pw, 1.0f);
-    p = __fmaf_rn(q, pw, 1.0f);
-    if (FAST) p = __frcp_rn(p);
+    const float pf = __fmaf_rn(q, pw, 1.0f);
+    if constexpr (FAST) p = __frcp_rn(pf);
+    else p = recip64(pf);
 }
 
-// One split-field update: (m*s + A*B)/p on a damped axis (FAST: times RN(1/p)),
-// s + A*B otherwise.
+// One split-field update: (m*s + A*B)/p on a damped axis (FAST: times RN(1/p);
+// REF: the correctly rounded quotient through the 64-bit reciprocal), s + A*B
+// otherwise.
 template <bool FAST>
-__device__ __forceinline__ float split_update(float s, float A, float B, bool damped, float m, float p) {
+__device__ __forceinline__ float split_update(float s, float A, float B, bool damped, float m, PDiv<FAST> p) {
     if (!damped) return __fmaf_rn(A, B, s);
     const float num = __fmaf_rn(m, s, A * B);
-    return FAST ? num * p : num / p;
+    if constexpr (FAST) return num * p;
+    else return __double2float_rn(__dmul_rn((double)num, p));
 }
 
 }  // namespace sgfd

@@ -122,7 +122,8 @@ __global__ void __launch_bounds__(kBX * kBY) k_velocity16(Model m, Physics ph, S
         if (track)
             for (int g = 0; g < 3; ++g) note_max(hs, g, vn[g]);
     } else {
-        float mx = 1.f, px = 1.f, my = 1.f, py = 1.f, mz = 1.f, pz = 1.f;
+        float mx = 1.f, my = 1.f, mz = 1.f;
+        PDiv<FAST> px = 1, py = 1, pz = 1;
         {
             const float v = damp_speed(ph, m.mu[ci], bb[0], m.lam[ci]);
             if (kx) damp_factors<FAST>(ph, 0, ph.dx, kx, m.pml, v, mx, px);
@@ -133,7 +134,8 @@ __global__ void __launch_bounds__(kBX * kBY) k_velocity16(Model m, Physics ph, S
         const float a[3] = {ph.dt * bx, ph.dt * (ref ? bx : by), ph.dt * (ref ? bx : bz)};
         const float d[3][3] = {{xX, xY, xZ}, {yX, yY, yZ}, {zX, zY, zZ}};
         const int kk[3] = {kx, ky, kz};
-        const float mm[3] = {mx, my, mz}, pp[3] = {px, py, pz};
+        const float mm[3] = {mx, my, mz};
+        const PDiv<FAST> pp[3] = {px, py, pz};
         const int64_t pi = pml_index(m, cx, cy, cz), N = m.npml;
         for (int q = 0; q < 3; ++q) {
             float part[3];
@@ -189,7 +191,8 @@ __global__ void __launch_bounds__(kBX * kBY) k_stress16(Model m, Physics ph, Sou
         sn[4] = __fmaf_rn(ph.dt * mxz, xzZ + xzX, S.get(7, ci));
         sn[5] = __fmaf_rn(ph.dt * myz, yzZ + yzY, S.get(8, ci));
     } else {
-        float mx = 1.f, px = 1.f, my = 1.f, py = 1.f, mz = 1.f, pz = 1.f;
+        float mx = 1.f, my = 1.f, mz = 1.f;
+        PDiv<FAST> px = 1, py = 1, pz = 1;
         {
             const float v = damp_speed(ph, m.mu[ci], m.b[ci], l);
             if (kx) damp_factors<FAST>(ph, 0, ph.dx, kx, m.pml, v, mx, px);

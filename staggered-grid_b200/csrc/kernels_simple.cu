@@ -60,7 +60,8 @@ __global__ void __launch_bounds__(kBX * kBY) k_velocity(Model m, Physics ph) {
         m.f[2][ci] = __fmaf_rn(ph.dt * bz, (zX + zY) + zZ, m.f[2][ci]);
         return;
     }
-    float mx = 1.f, px = 1.f, my = 1.f, py = 1.f, mz = 1.f, pz = 1.f;
+    float mx = 1.f, my = 1.f, mz = 1.f;
+        PDiv<FAST> px = 1, py = 1, pz = 1;
     {
         const float v = damp_speed(ph, m.mu[ci], bb[0], m.lam[ci]);
         if (kx) damp_factors<FAST>(ph, 0, ph.dx, kx, m.pml, v, mx, px);
@@ -128,7 +129,8 @@ __global__ void __launch_bounds__(kBX * kBY) k_stress(Model m, Physics ph) {
         m.f[8][ci] = __fmaf_rn(ph.dt * myz, yzZ + yzY, m.f[8][ci]);
         return;
     }
-    float mx = 1.f, px = 1.f, my = 1.f, py = 1.f, mz = 1.f, pz = 1.f;
+    float mx = 1.f, my = 1.f, mz = 1.f;
+        PDiv<FAST> px = 1, py = 1, pz = 1;
     {
         const float v = damp_speed(ph, mu0, m.b[ci], l);
         if (kx) damp_factors<FAST>(ph, 0, ph.dx, kx, m.pml, v, mx, px);

@@ -390,7 +390,8 @@ k_velocity_zmarch(const __grid_constant__ VelMaps mp, const __grid_constant__ Mo
                 vnew[1] = __fmaf_rn(ph.dt * by, (yX + yY) + yZ, ov[OVS + e]);
                 vnew[2] = __fmaf_rn(ph.dt * bz, (zX + zY) + zZ, ov[2 * OVS + e]);
             } else {
-                float mx = 1.f, px = 1.f, my = 1.f, py = 1.f, mz = 1.f, pz = 1.f;
+                float mx = 1.f, my = 1.f, mz = 1.f;
+        PDiv<FAST> px = 1, py = 1, pz = 1;
                 {
                     const float v = damp_speed(ph, mupre[c], b0, lampre[c]);
                     if (kx) damp_factors<FAST>(ph, 0, ph.dx, kx, m.pml, v, mx, px);
@@ -675,7 +676,8 @@ k_stress_zmarch(const __grid_constant__ StrMaps mp, const __grid_constant__ Mode
                 float o[15];
 #pragma unroll
                 for (int q = 0; q < 15; ++q) o[q] = sp[(S_XXX + q) * N];
-                float mx = 1.f, px = 1.f, my = 1.f, py = 1.f, mz = 1.f, pz = 1.f;
+                float mx = 1.f, my = 1.f, mz = 1.f;
+        PDiv<FAST> px = 1, py = 1, pz = 1;
                 {
                     const float v = damp_speed(ph, mu_c, m.b[ci], l);
                     if (kx) damp_factors<FAST>(ph, 0, ph.dx, kx, m.pml, v, mx, px);

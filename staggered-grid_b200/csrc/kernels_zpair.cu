@@ -538,7 +538,8 @@ __device__ __forceinline__ bool vel_pair(const VelMaps &mp, const Model &m, cons
 #pragma unroll
                         for (int k = 0; k < 9; ++k) o[k] = SA::one(sp + k * N, F.sc(k / 3));
                         const float mu_c = m.mu[cc], lam_c = ph.damping == 1 ? m.lam[cc] : 0.f;
-                        float mx = 1.f, px = 1.f, my = 1.f, py = 1.f, mz = 1.f, pz = 1.f;
+                        float mx = 1.f, my = 1.f, mz = 1.f;
+        PDiv<FAST> px = 1, py = 1, pz = 1;
                         {
                             const float v = damp_speed(ph, mu_c, lane_of(b0, c), lam_c);
                             if (kx) damp_factors<FAST>(ph, 0, ph.dx, kx, m.pml, v, mx, px);
@@ -554,7 +555,8 @@ __device__ __forceinline__ bool vel_pair(const VelMaps &mp, const Model &m, cons
                                                   {lane_of(zX, c), lane_of(zY, c), lane_of(zZ, c)}};
                         const float aq[3] = {ax, ay, az};
                         const int kk[3] = {kx, ky, kz};
-                        const float mm[3] = {mx, my, mz}, pp[3] = {px, py, pz};
+                        const float mm[3] = {mx, my, mz};
+        const PDiv<FAST> pp[3] = {px, py, pz};
 #pragma unroll
                         for (int q = 0; q < 3; ++q) {
                             float part[3];
@@ -807,7 +809,8 @@ __device__ __forceinline__ bool str_pair(const StrMaps &mp, const Model &m, cons
                             if (track) note_max16(hs, grp(k), v);
                             SA::put1(sp + k * N, v, F.inv(grp(k)));
                         };
-                        float mx = 1.f, px = 1.f, my = 1.f, py = 1.f, mz = 1.f, pz = 1.f;
+                        float mx = 1.f, my = 1.f, mz = 1.f;
+        PDiv<FAST> px = 1, py = 1, pz = 1;
                         {
                             const float v = damp_speed(ph, mu_c, b_c, lc);
                             if (kx) damp_factors<FAST>(ph, 0, ph.dx, kx, m.pml, v, mx, px);
