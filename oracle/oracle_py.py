@@ -58,6 +58,7 @@ def lib():
         L.sgo_run.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, dp]
         L.sgo_get_traces.argtypes = [ctypes.c_void_p, dp]
         L.sgo_get_field.argtypes = [ctypes.c_void_p, ctypes.c_int, dp]
+        L.sgo_set_field.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]
         L.sgo_round16.argtypes = [ctypes.c_int, fp, fp, ctypes.c_int64]
         L.sgo_scale_exponents.argtypes = [ctypes.c_void_p, ip]
         L.sgo_ricker_ref.restype = ctypes.c_float
@@ -160,6 +161,11 @@ class Oracle:
         out = np.zeros(self.shape, dtype=np.float64)
         lib().sgo_get_field(self.h, int(fid), _ptr(out, ctypes.c_double))
         return out
+
+    def set_field(self, fid: int, values):
+        a = np.ascontiguousarray(np.asarray(values, dtype=np.float32).reshape(self.shape))
+        if lib().sgo_set_field(self.h, int(fid), _ptr(a, ctypes.c_float)) != 0:
+            raise ValueError("bad field")
 
 
 # ---------------------------------------------------------------------------

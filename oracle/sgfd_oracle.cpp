@@ -644,6 +644,16 @@ int sgo_get_field(void *p, int field, double *out) {
     });
 }
 
+// Overwrite one wavefield from n float values (GRID, x fastest): initial
+// conditions, as sgfd_set_field does on the GPU.
+int sgo_set_field(void *p, int field, const float *in) {
+    return dispatch(static_cast<Handle *>(p), [&](auto &o) {
+        if (field < 0 || field > 8) return (int)SGFD_ERR_INVALID;
+        for (int64_t i = 0; i < o.n; ++i) o.f[field][i] = in[i];
+        return 0;
+    });
+}
+
 // The 16-bit roundings of the storage emulation, for checking against numpy.
 void sgo_round16(int storage, const float *in, float *out, int64_t n) {
     for (int64_t i = 0; i < n; ++i) out[i] = storage == SGFD_STORE_F16 ? rn_f16(in[i]) : rn_bf16(in[i]);
