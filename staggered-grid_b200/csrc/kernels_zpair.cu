@@ -280,7 +280,9 @@ struct Fields {
     using E = typename Sto<ST>::E;
     const Model &m;
     const HalfState &hs;
-    __device__ __forceinline__ Fields(const Model &m_, const HalfState &hs_) : m(m_), hs(hs_) {}
+    const float *scl;   // 16-bit: the 9 scales 2^e then the 9 inverses, staged in shared memory
+    __device__ __forceinline__ Fields(const Model &m_, const HalfState &hs_, const float *scl_)
+        : m(m_), hs(hs_), scl(scl_) {}
     __device__ __forceinline__ E *f(int k) const {
         if constexpr (ST == SGFD_STORE_F32) return m.f[k];
         else return hs.f[k];
@@ -291,11 +293,11 @@ struct Fields {
     }
     __device__ __forceinline__ float sc(int k) const {
         if constexpr (ST == SGFD_STORE_F32) return 1.0f;
-        else return __ldg(hs.sc + k);
+        else return scl[k];
     }
     __device__ __forceinline__ float inv(int k) const {
         if constexpr (ST == SGFD_STORE_F32) return 1.0f;
-        else return __ldg(hs.inv + k);
+        else return scl[9 + k];
     }
 };
 
@@ -353,7 +355,15 @@ __device__ __forceinline__ bool vel_pair(const VelMaps &mp, const Model &m, cons
     using L = VelP<SA::ES>;
     constexpr int S = SV;
     constexpr bool H = ST != SGFD_STORE_F32;   // 16-bit storage: source and receivers run as separate kernels
-    const Fields<ST> F(m, hs);
+    __shared__ float scl[18];   // 16-bit storage: this step's scales, read at every tap
+    if constexpr (ST != SGFD_STORE_F32) {
+        if (threadIdx.x < 9) {
+            scl[threadIdx.x] = hs.sc[threadIdx.x];
+            scl[9 + threadIdx.x] = hs.inv[threadIdx.x];
+        }
+        __syncthreads();
+    }
+    const Fields<ST> F(m, hs, scl);
     const PTile t = make_ptile(m, g, tile, chunk);
     const int tid = threadIdx.x, lx = tid & 31, ly = tid >> 5, warp = ly;
     const TmaBox *mybox = boxes[warp];
@@ -656,7 +666,15 @@ __device__ __forceinline__ bool str_pair(const StrMaps &mp, const Model &m, cons
     using L = StrP<SA::ES>;
     constexpr int S = SS;
     constexpr bool H = ST != SGFD_STORE_F32;   // 16-bit storage: source and receivers run as separate kernels
-    const Fields<ST> F(m, hs);
+    __shared__ float scl[18];   // 16-bit storage: this step's scales, read at every tap
+    if constexpr (ST != SGFD_STORE_F32) {
+        if (threadIdx.x < 9) {
+            scl[threadIdx.x] = hs.sc[threadIdx.x];
+            scl[9 + threadIdx.x] = hs.inv[threadIdx.x];
+        }
+        __syncthreads();
+    }
+    const Fields<ST> F(m, hs, scl);
     const PTile t = make_ptile(m, g, tile, chunk);
     const int tid = threadIdx.x, lx = tid & 31, ly = tid >> 5, warp = ly;
     const TmaBox *mybox = boxes[warp];
@@ -995,6 +1013,11 @@ k_batch_zpair(const PairModel *models, int nmodels, const int *first_item, int i
     __shared__ __align__(8) uint64_t bar_s[SS];
     __shared__ TmaBox boxes[kWarps][kMaxBoxesPerWarp];
     __shared__ int item_sh, ok_sh;
+    // the current model's physics and geometry, read in every plane's inner
+    // loops: a shared copy instead of loads from the descriptor array
+    __shared__ __align__(16) Physics ph_s;
+    __shared__ __align__(16) Model m_s;
+    int cur = -1;
     if (threadIdx.x == 0) {
         for (int s = 0; s < SV; ++s) mbar_init(&bar_v[s], 1);
         for (int s = 0; s < SS; ++s) mbar_init(&bar_s[s], 1);
@@ -1017,13 +1040,23 @@ k_batch_zpair(const PairModel *models, int nmodels, const int *first_item, int i
                 int mi = 0;
                 while (first_item[mi + 1] <= item) ++mi;
                 const PairModel &d = models[mi];
+                if (mi != cur) {   // every thread is past the previous item (the barriers above)
+                    const uint32_t *src = reinterpret_cast<const uint32_t *>(&d.ph);
+                    uint32_t *dst = reinterpret_cast<uint32_t *>(&ph_s);
+                    for (int i = threadIdx.x; i < (int)(sizeof(Physics) / 4); i += NT) dst[i] = src[i];
+                    src = reinterpret_cast<const uint32_t *>(&d.m);
+                    dst = reinterpret_cast<uint32_t *>(&m_s);
+                    for (int i = threadIdx.x; i < (int)(sizeof(Model) / 4); i += NT) dst[i] = src[i];
+                    __syncthreads();
+                    cur = mi;
+                }
                 const int local = item - first_item[mi];
                 const int ntiles = d.g.ntx * d.g.nty;
                 const HalfState no16{};
                 const bool ok =
-                    p == 0 ? vel_pair<FAST, SGFD_STORE_F32>(d.vm, d.m, d.ph, d.g, d.sr, no16, it0 + k, 0.0f, 1,
+                    p == 0 ? vel_pair<FAST, SGFD_STORE_F32>(d.vm, m_s, ph_s, d.g, d.sr, no16, it0 + k, 0.0f, 1,
                                                             local % ntiles, local / ntiles, smem, bar_v, boxes, pv)
-                           : str_pair<FAST, SGFD_STORE_F32>(d.sm, d.m, d.ph, d.g, d.sr, no16, it0 + k, 0.0f, 1,
+                           : str_pair<FAST, SGFD_STORE_F32>(d.sm, m_s, ph_s, d.g, d.sr, no16, it0 + k, 0.0f, 1,
                                                             local % ntiles, local / ntiles, smem, bar_s, boxes, ps);
                 if (!ok) {
                     if (threadIdx.x == 0) atomicExch(status, kBatchWaitTma);
