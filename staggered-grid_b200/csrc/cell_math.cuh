@@ -79,42 +79,6 @@ __device__ __forceinline__ float div_cell(const Physics &ph, int axis, float a) 
 #endif
 }
 
-// The cell size of `axis`.
-__device__ __forceinline__ float cell_size(const Physics &ph, int axis) {
-    return axis == 0 ? ph.dx : axis == 1 ? ph.dy : ph.dz;
-}
-
-// Whether Markstein's correction step cannot be trusted for dividend a:
-// a nonzero |a| below 2^-100 (its residual would fall below the normal range)
-// or an |a| from 2^100 up, infinities and NaNs included.  Zeros are fine (the
-// step returns them with their sign).
-__device__ __forceinline__ bool mk_unsafe(float a) {
-    const uint32_t b = __float_as_uint(a) & 0x7fffffffu;
-    return b != 0u && (b - 0x0d800000u) >= (0x71800000u - 0x0d800000u);
-}
-
-// REF quotients of two difference sums (lane 0 on axis a0, lane 1 on a1)
-// on FP32x2 by the single-precision correction step of div_cell:
-// q0 = RN(s y), t = RN(q0 d - s), q = RN(q0 - t y), y = RN(1/d).  Exact for
-// every s in [2^-100, 2^100] and for zeros when the host verified the step
-// for both divisors (ph.mdiv); `unsafe` collects the sums outside that
-// range, for which the caller recomputes with div_cell.
-__device__ __forceinline__ float2 mk_pair(const Physics &ph, float2 s, int a0, int a1, bool &unsafe) {
-    const float2 y = make_float2(ph.rd[a0], ph.rd[a1]);
-    const float2 d = make_float2(cell_size(ph, a0), cell_size(ph, a1));
-    const float2 q0 = __fmul2_rn(s, y);
-    const float2 t = __ffma2_rn(q0, d, make_float2(-s.x, -s.y));
-    unsafe = unsafe || mk_unsafe(s.x) || mk_unsafe(s.y);
-    return __ffma2_rn(make_float2(-t.x, -t.y), y, q0);
-}
-__device__ __forceinline__ float mk_one(const Physics &ph, float s, int axis, bool &unsafe) {
-    const float y = ph.rd[axis], d = cell_size(ph, axis);
-    const float q0 = __fmul_rn(s, y);
-    const float t = __fmaf_rn(q0, d, -s);
-    unsafe = unsafe || mk_unsafe(s);
-    return __fmaf_rn(-t, y, q0);
-}
-
 // A difference sum divided by the cell size of `axis` (REF), or as it is
 // (FAST sums are formed with the pre-divided coefficients).
 template <bool FAST>

@@ -201,7 +201,7 @@ __global__ void __launch_bounds__(kBX * kBY) k_stress16(Model m, Physics ph, Sou
         }
         const int64_t pi = pml_index(m, cx, cy, cz), N = m.npml;
         const float dl = ph.dt * l2m, dt = ph.dt;
-        auto upd = [&](int k, float A, float B, int kd, float mf, float pf) {
+        auto upd = [&](int k, float A, float B, int kd, float mf, PDiv<FAST> pf) {
             const float r = split_update<FAST>(S.sget(k, k * N + pi), A, B, kd, mf, pf);
             if (track) note_max(hs, split_group(k), r);
             S.sput(k, k * N + pi, r);

@@ -361,29 +361,10 @@ k_velocity_zmarch(const __grid_constant__ VelMaps mp, const __grid_constant__ Mo
                 const float2 xXyY = dpair(FAST ? ph.cp[3] : ph.cr,
                                           [&](int i) { return make_float2(rxx[1 + i], cyy[(1 + i) * W32]); },
                                           [&](int i) { return make_float2(rxx[-i], cyy[-i * W32]); });
-                if constexpr (FAST) {
-                    xX = xXyY.x; yY = xXyY.y; yX = yzX.x; zX = yzX.y;
-                    xY = xzY.x; zY = xzY.y; xZ = xyZ.x; yZ = xyZ.y;
-                    zZ = dF<FAST, 2>(ph, [&](int o) { return qzz[c][4 + o]; });
-                } else {
-                    // REF: the divisions by the cell sizes on FP32x2 (Markstein's
-                    // step) unless a sum in this warp is out of its range or the
-                    // step is not verified for these cell sizes; then div_cell
-                    const float szZ = dfwd(ph.c, [&](int o) { return qzz[c][4 + o]; });
-                    bool unsafe = ph.mdiv != 7;
-                    float2 q = mk_pair(ph, xXyY, 0, 1, unsafe); xX = q.x; yY = q.y;
-                    q = mk_pair(ph, yzX, 0, 0, unsafe); yX = q.x; zX = q.y;
-                    q = mk_pair(ph, xzY, 1, 1, unsafe); xY = q.x; zY = q.y;
-                    q = mk_pair(ph, xyZ, 2, 2, unsafe); xZ = q.x; yZ = q.y;
-                    zZ = mk_one(ph, szZ, 2, unsafe);
-                    if (__any_sync(__activemask(), unsafe)) {
-                        xX = div_cell(ph, 0, xXyY.x); yY = div_cell(ph, 1, xXyY.y);
-                        yX = div_cell(ph, 0, yzX.x); zX = div_cell(ph, 0, yzX.y);
-                        xY = div_cell(ph, 1, xzY.x); zY = div_cell(ph, 1, xzY.y);
-                        xZ = div_cell(ph, 2, xyZ.x); yZ = div_cell(ph, 2, xyZ.y);
-                        zZ = div_cell(ph, 2, szZ);
-                    }
-                }
+                xX = by_cell<FAST>(ph, 0, xXyY.x); yY = by_cell<FAST>(ph, 1, xXyY.y);
+                yX = by_cell<FAST>(ph, 0, yzX.x); zX = by_cell<FAST>(ph, 0, yzX.y);
+                xY = by_cell<FAST>(ph, 1, xzY.x); zY = by_cell<FAST>(ph, 1, xzY.y);
+                xZ = by_cell<FAST>(ph, 2, xyZ.x); yZ = by_cell<FAST>(ph, 2, xyZ.y);
             } else {
                 xX = dF<FAST, 0>(ph, [&](int o) { return rxx[o]; });
                 xY = CELLS == 2 ? xY2[c] : dB<FAST, 1>(ph, [&](int o) { return cxy[o * W48]; });
@@ -393,8 +374,8 @@ k_velocity_zmarch(const __grid_constant__ VelMaps mp, const __grid_constant__ Mo
                 yZ = dB<FAST, 2>(ph, [&](int o) { return qyz[c][5 + o]; });
                 zX = dB<FAST, 0>(ph, [&](int o) { return rxz[o]; });
                 zY = CELLS == 2 ? zY2[c] : dB<FAST, 1>(ph, [&](int o) { return cyz[o * W32]; });
-                zZ = dF<FAST, 2>(ph, [&](int o) { return qzz[c][4 + o]; });
             }
+            zZ = dF<FAST, 2>(ph, [&](int o) { return qzz[c][4 + o]; });
             const float b0 = bb[ly * W36 + lx];
             const float bx = (b0 + bb[ly * W36 + lx + 1]) / 2.0f;
             const float by = (b0 + bb[(ly + 1) * W36 + lx]) / 2.0f;
@@ -656,27 +637,10 @@ k_stress_zmarch(const __grid_constant__ StrMaps mp, const __grid_constant__ Mode
                 const float2 pN = dpair(FAST ? ph.cp[3] : ph.cr,
                                         [&](int i) { return make_float2(cx_[i], cy_[i * W48]); },
                                         [&](int i) { return make_float2(cx_[-1 - i], cy_[(-1 - i) * W48]); });
-                if constexpr (FAST) {
-                    xyX = pX.x; xzX = pX.y; xyY = pY.x; yzY = pY.y;
-                    xzZ = pZ.x; yzZ = pZ.y; dXx = pN.x; dYy = pN.y;
-                    dZz = dB<FAST, 2>(ph, [&](int o) { return qz[c][5 + o]; });
-                } else {
-                    // REF: as in the velocity update
-                    const float sZz = dbwd(ph.c, [&](int o) { return qz[c][5 + o]; });
-                    bool unsafe = ph.mdiv != 7;
-                    float2 q = mk_pair(ph, pX, 0, 0, unsafe); xyX = q.x; xzX = q.y;
-                    q = mk_pair(ph, pY, 1, 1, unsafe); xyY = q.x; yzY = q.y;
-                    q = mk_pair(ph, pZ, 2, 2, unsafe); xzZ = q.x; yzZ = q.y;
-                    q = mk_pair(ph, pN, 0, 1, unsafe); dXx = q.x; dYy = q.y;
-                    dZz = mk_one(ph, sZz, 2, unsafe);
-                    if (__any_sync(__activemask(), unsafe)) {
-                        xyX = div_cell(ph, 0, pX.x); xzX = div_cell(ph, 0, pX.y);
-                        xyY = div_cell(ph, 1, pY.x); yzY = div_cell(ph, 1, pY.y);
-                        xzZ = div_cell(ph, 2, pZ.x); yzZ = div_cell(ph, 2, pZ.y);
-                        dXx = div_cell(ph, 0, pN.x); dYy = div_cell(ph, 1, pN.y);
-                        dZz = div_cell(ph, 2, sZz);
-                    }
-                }
+                xyX = by_cell<FAST>(ph, 0, pX.x); xzX = by_cell<FAST>(ph, 0, pX.y);
+                xyY = by_cell<FAST>(ph, 1, pY.x); yzY = by_cell<FAST>(ph, 1, pY.y);
+                xzZ = by_cell<FAST>(ph, 2, pZ.x); yzZ = by_cell<FAST>(ph, 2, pZ.y);
+                dXx = by_cell<FAST>(ph, 0, pN.x); dYy = by_cell<FAST>(ph, 1, pN.y);
             } else {
                 dXx = dB<FAST, 0>(ph, [&](int o) { return cx_[o]; });
                 dYy = CELLS == 2 ? dYy2[c] : dB<FAST, 1>(ph, [&](int o) { return cy_[o * W48]; });
@@ -686,8 +650,8 @@ k_stress_zmarch(const __grid_constant__ StrMaps mp, const __grid_constant__ Mode
                 xzX = dF<FAST, 0>(ph, [&](int o) { return cz_[o]; });
                 yzZ = dF<FAST, 2>(ph, [&](int o) { return qy[c][4 + o]; });
                 yzY = CELLS == 2 ? yzY2[c] : dF<FAST, 1>(ph, [&](int o) { return cz_[o * W48]; });
-                dZz = dB<FAST, 2>(ph, [&](int o) { return qz[c][5 + o]; });
             }
+            dZz = dB<FAST, 2>(ph, [&](int o) { return qz[c][5 + o]; });
 
             const int e = ly * W32 + lx;
             const float l = own[6 * OS + e], mu_c = own[7 * OS + e];
