@@ -63,8 +63,8 @@ def parse():
                                                "batch32", "learned256", "combined32"],
                    default="random344")
     p.add_argument("--no-autotune", action="store_true", help="batch32: keep the default launch shapes")
-    p.add_argument("--batch-mode", choices=["persistent", "graph"], default="persistent",
-                   help="batch32: one persistent launch per run, or graph replays with one branch per model")
+    p.add_argument("--batch-mode", choices=["persistent", "graph"], default="graph",
+                   help="batch32: graph replays with one branch per model (faster here), or one persistent launch per run")
     p.add_argument("--kernel", choices=["auto", "simple", "zmarch"], default="auto")
     p.add_argument("--tile", choices=["default", "32x8", "32x16", "64x8"], default="default",
                    help="z-marching tile shape (default: the library's choice)")
@@ -569,9 +569,9 @@ def main_learned(args, world, rank, local):
 def main_batch(args, world, rank, local):
     """The batched configuration: 32 layered models of uneven size (359 M
     computed cells in all), each with its own source and 128 receivers,
-    advanced together by sgfd_batch_run: by default one persistent launch per
-    run over all models' work items (--batch-mode graph: 16-step graphs, one
-    branch per model, autotuned launch shapes).  With N ranks the models are dealt out by computed cells (greedy,
+    advanced together by sgfd_batch_run: by default 16-step graphs with one
+    branch per model and autotuned launch shapes (--batch-mode persistent: one
+    persistent launch per run over all models' work items).  With N ranks the models are dealt out by computed cells (greedy,
     largest first); value = all ranks' cells x steps / slowest rank's time."""
     import dataclasses
     import torch
