@@ -41,12 +41,12 @@ sys.path.insert(0, os.path.join(ROOT, "staggered-grid_b200"))
 # 6 stresses.  Sum per step: 120 B interior, 276 B PML.
 BYTES = {"velocity": (52, 112), "stress": (68, 164)}
 # DRAM traffic / algorithmic bytes per kernel, from ncu (dram__bytes_read.sum +
-# dram__bytes_write.sum) on the 216^3 + 20 PML cube of the same kernels; the
+# dram__bytes_write.sum) on the 216^3 + 20 PML cube of the same kernels (REF); the
 # 394^3 workload is too large for a multi-metric capture, so its traffic is
 # reported as its algorithmic bytes times this ratio.
-TRAFFIC_RATIO = {"velocity": 1.18, "stress": 1.31}
-TRAFFIC_SOURCE = ("ncu dram bytes / algorithmic bytes of the z-march kernels on the 216^3 + 20 PML cube, "
-                  "times this launch's algorithmic bytes")
+TRAFFIC_RATIO = {"velocity": 1.19, "stress": 1.33}
+TRAFFIC_SOURCE = ("ncu dram bytes / algorithmic bytes of the z-march kernels (REF rounding) on the 216^3 + 20 PML "
+                  "cube, times this launch's algorithmic bytes")
 # 16-bit storage: fields and splits 2 B, medium 4 B (per step 66 B interior, 144 B PML).
 BYTES16 = {"velocity": (28, 58), "stress": (38, 86)}
 STORAGE = {"f32": 0, "bf16": 1, "f16": 2}
