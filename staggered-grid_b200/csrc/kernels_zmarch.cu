@@ -57,14 +57,16 @@ constexpr int W48 = 48, W32 = 32, W36 = 36;
 constexpr int al128(int b) { return (b + 127) / 128 * 128; }
 
 // Shared-memory stage layout of the velocity update (bytes, 128-aligned boxes).
+// Arrays that arrive in one 4-D copy are adjacent (sigma_xx, sigma_xz;
+// sigma_yy, sigma_yz; the two lead planes at z+4; vx, vy, vz).
 template <int TY>
 struct VelL {
     static constexpr int SXX = 0;                                  // 48 x TY       sigma_xx (x halo)
-    static constexpr int SYY = SXX + al128(W48 * TY * 4);          // 32 x (TY+10)  sigma_yy (y halo)
-    static constexpr int SXY = SYY + al128(W32 * (TY + 10) * 4);   // 48 x (TY+10)  sigma_xy (x, y halo)
-    static constexpr int SXZ = SXY + al128(W48 * (TY + 10) * 4);   // 48 x TY       sigma_xz (x halo)
-    static constexpr int SYZ = SXZ + al128(W48 * TY * 4);          // 32 x (TY+10)  sigma_yz (y halo)
-    static constexpr int B = SYZ + al128(W32 * (TY + 10) * 4);     // 36 x (TY+1)   buoyancy (x+1, y+1)
+    static constexpr int SXZ = SXX + W48 * TY * 4;                 // 48 x TY       sigma_xz (x halo)
+    static constexpr int SYY = SXZ + al128(W48 * TY * 4);          // 32 x (TY+10)  sigma_yy (y halo)
+    static constexpr int SYZ = SYY + W32 * (TY + 10) * 4;          // 32 x (TY+10)  sigma_yz (y halo)
+    static constexpr int SXY = SYZ + al128(W32 * (TY + 10) * 4);   // 48 x (TY+10)  sigma_xy (x, y halo)
+    static constexpr int B = SXY + al128(W48 * (TY + 10) * 4);     // 36 x (TY+1)   buoyancy (x+1, y+1)
     static constexpr int LXZ = B + al128(W36 * (TY + 1) * 4);      // 32 x TY       sigma_xz at z+4
     static constexpr int LYZ = LXZ + al128(W32 * TY * 4);          // 32 x TY       sigma_yz at z+4
     static constexpr int LZZ = LYZ + al128(W32 * TY * 4);          // 32 x TY       sigma_zz at z+5
@@ -73,6 +75,8 @@ struct VelL {
     static constexpr int STAGE = OV + 3 * al128(W32 * TY * 4);
     static constexpr uint32_t TXB = 4 * (2 * W48 * TY + 2 * W32 * (TY + 10) + W48 * (TY + 10) +
                                          W36 * (TY + 1) + 7 * W32 * TY);
+    static_assert(W48 * TY * 4 % 128 == 0 && W32 * (TY + 10) * 4 % 128 == 0 && W32 * TY * 4 % 128 == 0,
+                  "arrays of one copy must be contiguous and 128-byte aligned");
 };
 // Shared-memory stage layout of the stress update.
 template <int TY>
@@ -89,6 +93,8 @@ struct StrL {
     static constexpr int NOWN = 11;
     static constexpr int STAGE = OWN + NOWN * al128(W32 * TY * 4);
     static constexpr uint32_t TXB = 4 * (3 * W48 * (TY + 10) + (3 + NOWN) * W32 * TY);
+    static_assert(W48 * (TY + 10) * 4 % 128 == 0 && W32 * TY * 4 % 128 == 0,
+                  "arrays of one copy must be contiguous and 128-byte aligned");
 };
 
 struct Tile {
@@ -120,10 +126,11 @@ __device__ __forceinline__ Tile make_tile(const Model &m, const ZGeom &g) {
 
 constexpr int kWarps = NT / 32;
 
-// One TMA box of a stage: tensor map, destination offset in the stage, x and
-// y of its origin and its plane relative to the staged plane.  Each warp's
-// boxes are worked out once per CTA and kept in shared memory, so that the
-// per-plane issue is a few loads and the copies themselves.
+// One TMA box of a stage: 4-D tensor map (its first array at w = 0),
+// destination offset in the stage, x and y of its origin and its plane
+// relative to the staged plane.  Each warp's boxes are worked out once per
+// CTA and kept in shared memory, so that the per-plane issue is a few loads
+// and the copies themselves.
 struct TmaBox {
     const CUtensorMap *map;
     uint32_t off;
@@ -132,30 +139,24 @@ struct TmaBox {
 constexpr int kMaxBoxesPerWarp = 3;
 
 __device__ __forceinline__ void issue_boxes(const TmaBox *b, int n, unsigned char *st, uint64_t *bar, int gz) {
-    for (int j = 0; j < n; ++j) tma3(st + b[j].off, b[j].map, b[j].x, b[j].y, gz + b[j].dz, bar);
+    for (int j = 0; j < n; ++j) tma4(st + b[j].off, b[j].map, b[j].x, b[j].y, gz + b[j].dz, 0, bar);
 }
-constexpr int kVelBoxes = 13;
-constexpr int kStrBoxes = 17;
+constexpr int kVelBoxes = 8;
+constexpr int kStrBoxes = 4;
 
 // Box q of the velocity stage.
 template <int TY>
-__device__ __forceinline__ TmaBox vel_box(const VelMaps &mp, const Tile &t, int q) {
+__device__ __forceinline__ TmaBox vel_box(const ZMaps &mp, const Tile &t, int q) {
     using L = VelL<TY>;
-    constexpr uint32_t OB = al128(W32 * TY * 4);
     switch (q) {
-    case 0: return {&mp.sxx, L::SXX, t.xd - 8, t.gy0, 0};
-    case 1: return {&mp.syy, L::SYY, t.xd, t.gy0 - 5, 0};
-    case 2: return {&mp.sxy, L::SXY, t.xd - 8, t.gy0 - 5, 0};
-    case 3: return {&mp.sxz, L::SXZ, t.xd - 8, t.gy0, 0};
-    case 4: return {&mp.syz, L::SYZ, t.xd, t.gy0 - 5, 0};
-    case 5: return {&mp.b, L::B, t.xd, t.gy0, 0};
-    case 6: return {&mp.sxz_c, L::LXZ, t.xd, t.gy0, 4};
-    case 7: return {&mp.syz_c, L::LYZ, t.xd, t.gy0, 4};
-    case 8: return {&mp.szz_c, L::LZZ, t.xd, t.gy0, 5};
-    case 9: return {&mp.b_c, L::LB, t.xd, t.gy0, 1};
-    case 10: return {&mp.own[0], L::OV, t.xd, t.gy0, 0};
-    case 11: return {&mp.own[1], L::OV + OB, t.xd, t.gy0, 0};
-    default: return {&mp.own[2], L::OV + 2 * OB, t.xd, t.gy0, 0};
+    case 0: return {&mp.v_sxx_sxz, L::SXX, t.xd - 8, t.gy0, 0};
+    case 1: return {&mp.v_syy_syz, L::SYY, t.xd, t.gy0 - 5, 0};
+    case 2: return {&mp.v_sxy, L::SXY, t.xd - 8, t.gy0 - 5, 0};
+    case 3: return {&mp.v_b, L::B, t.xd, t.gy0, 0};
+    case 4: return {&mp.v_lead_xz_yz, L::LXZ, t.xd, t.gy0, 4};
+    case 5: return {&mp.v_lead_zz, L::LZZ, t.xd, t.gy0, 5};
+    case 6: return {&mp.v_lead_b, L::LB, t.xd, t.gy0, 1};
+    default: return {&mp.v_own, L::OV, t.xd, t.gy0, 0};
     }
 }
 
@@ -172,7 +173,7 @@ __device__ __forceinline__ void vel_issue(const TmaBox *b, int n, unsigned char 
 
 template <bool FAST, int CELLS>
 __global__ void __launch_bounds__(NT, 3)
-k_velocity_zmarch(const __grid_constant__ VelMaps mp, const __grid_constant__ Model m, const __grid_constant__ Physics ph,
+k_velocity_zmarch(const __grid_constant__ ZMaps mp, const __grid_constant__ Model m, const __grid_constant__ Physics ph,
                   const __grid_constant__ ZGeom g, const __grid_constant__ SourceRec sr, int it_arg,
                   float src_value, int use_wavelet) {
     constexpr int TY = 8 * CELLS;
@@ -473,17 +474,13 @@ k_velocity_zmarch(const __grid_constant__ VelMaps mp, const __grid_constant__ Mo
 
 // Box q of the stress stage.
 template <int TY>
-__device__ __forceinline__ TmaBox str_box(const StrMaps &mp, const Tile &t, int q) {
+__device__ __forceinline__ TmaBox str_box(const ZMaps &mp, const Tile &t, int q) {
     using L = StrL<TY>;
-    constexpr uint32_t OB = al128(W32 * TY * 4);
     switch (q) {
-    case 0: return {&mp.vx, L::VX, t.xd - 8, t.gy0 - 5, 0};
-    case 1: return {&mp.vy, L::VY, t.xd - 8, t.gy0 - 5, 0};
-    case 2: return {&mp.vz, L::VZ, t.xd - 8, t.gy0 - 5, 0};
-    case 3: return {&mp.vx_c, L::LX, t.xd, t.gy0, 5};
-    case 4: return {&mp.vy_c, L::LY, t.xd, t.gy0, 5};
-    case 5: return {&mp.vz_c, L::LZ, t.xd, t.gy0, 4};
-    default: return {&mp.own[q - 6], L::OWN + (uint32_t)(q - 6) * OB, t.xd, t.gy0, 0};
+    case 0: return {&mp.s_v, L::VX, t.xd - 8, t.gy0 - 5, 0};
+    case 1: return {&mp.s_lead_xy, L::LX, t.xd, t.gy0, 5};
+    case 2: return {&mp.s_lead_z, L::LZ, t.xd, t.gy0, 4};
+    default: return {&mp.s_own, L::OWN, t.xd, t.gy0, 0};
     }
 }
 
@@ -496,7 +493,7 @@ __device__ __forceinline__ void str_issue(const TmaBox *b, int n, unsigned char 
 
 template <bool FAST, int CELLS>
 __global__ void __launch_bounds__(NT, 3)
-k_stress_zmarch(const __grid_constant__ StrMaps mp, const __grid_constant__ Model m, const __grid_constant__ Physics ph,
+k_stress_zmarch(const __grid_constant__ ZMaps mp, const __grid_constant__ Model m, const __grid_constant__ Physics ph,
                   const __grid_constant__ ZGeom g, const __grid_constant__ SourceRec sr, int it_arg,
                 float src_value, int use_wavelet) {
     constexpr int TY = 8 * CELLS;
@@ -788,14 +785,14 @@ cudaError_t set_attrs() {
 }
 
 template <bool FAST, int CELLS>
-void launch(const Model &m, const Physics &ph, const SourceRec &sr, const ZGeom &g, const VelMaps &vm,
-            const StrMaps &sm, int it, float src_value, int uw, cudaStream_t s, cudaEvent_t *ev) {
+void launch(const Model &m, const Physics &ph, const SourceRec &sr, const ZGeom &g, const ZMaps &zm, int it,
+            float src_value, int uw, cudaStream_t s, cudaEvent_t *ev) {
     const dim3 grid(g.ntx * g.nty, g.nchunks);
     if (ev) cudaEventRecord(ev[0], s);
-    k_velocity_zmarch<FAST, CELLS><<<grid, NT, vel_smem<CELLS>(), s>>>(vm, m, ph, g, sr, it, src_value, uw);
+    k_velocity_zmarch<FAST, CELLS><<<grid, NT, vel_smem<CELLS>(), s>>>(zm, m, ph, g, sr, it, src_value, uw);
     if (ev) cudaEventRecord(ev[1], s);
     if (ev) cudaEventRecord(ev[2], s);
-    k_stress_zmarch<FAST, CELLS><<<grid, NT, str_smem<CELLS>(), s>>>(sm, m, ph, g, sr, it, src_value, uw);
+    k_stress_zmarch<FAST, CELLS><<<grid, NT, str_smem<CELLS>(), s>>>(zm, m, ph, g, sr, it, src_value, uw);
     if (ev) cudaEventRecord(ev[3], s);
 }
 
@@ -833,35 +830,51 @@ bool make_box_map16(CUtensorMap *map, const uint16_t *grid_origin, const Model &
 bool zmarch_supported(const Model &m) {
     // Halo boxes start 8 cells left of the tile and 5 rows above: always inside
     // the padded array because the frame is 5 cells and kXOff is 27.  The
-    // kernels address cells and PML cells with 32-bit offsets
-    const bool small = m.plane * (int64_t)m.nz < ((int64_t)1 << 31) && m.npml < ((int64_t)1 << 31);
+    // kernels address cells and PML split values with 32-bit offsets: cell
+    // offsets below 2^31, split offsets (component * npml + PML cell) below 2^32
+    const bool small = m.plane * (int64_t)m.nz < ((int64_t)1 << 31) &&
+                       (int64_t)kNumSplit * m.npml <= ((int64_t)1 << 32);
     return small && m.nxc >= 1 && m.nyc >= 1 && m.nzc >= 1 && get_encoder() != nullptr;
 }
 
-cudaError_t zmarch_prepare(const Model &m, int cells, VelMaps *vm, StrMaps *sm) {
+// 4-D FP32 tensor map over `count` arrays of the pool, `stride` bytes apart,
+// the first at `first`, with a bx x by x 1 x count box.
+bool make_pool_map(CUtensorMap *map, const float *first, const Model &m, size_t stride, int count, int bx, int by) {
+    auto enc = get_encoder();
+    if (!enc) return false;
+    void *base = const_cast<float *>(first - kXOff);
+    cuuint64_t dims[4] = {(cuuint64_t)(m.nx + kXOff), (cuuint64_t)m.ny, (cuuint64_t)m.nz, (cuuint64_t)count};
+    cuuint64_t strides[3] = {(cuuint64_t)m.px * 4, (cuuint64_t)m.plane * 4, (cuuint64_t)stride};
+    cuuint32_t box[4] = {(cuuint32_t)bx, (cuuint32_t)by, 1, (cuuint32_t)count};
+    cuuint32_t es[4] = {1, 1, 1, 1};
+    CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, base, dims, strides, box, es,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
+cudaError_t zmarch_prepare(const Model &m, int cells, size_t st, ZMaps *zm) {
     if (cells != 1 && cells != 2) return cudaErrorInvalidValue;
+    // the pool order the merged copies rely on: vx..tyz, lambda, mu, mxy, mxz, myz
+    auto at = [&](int k) { return reinterpret_cast<const float *>(reinterpret_cast<const char *>(m.f[0]) + k * st); };
+    const float *order[14] = {m.f[0], m.f[1], m.f[2], m.f[3], m.f[4], m.f[5], m.f[6], m.f[7],
+                              m.f[8], m.lam, m.mu, m.mxy, m.mxz, m.myz};
+    for (int k = 0; k < 14; ++k)
+        if (order[k] != at(k)) return cudaErrorInvalidValue;
     const int ty = 8 * cells;
     bool ok = true;
-    ok &= make_box_map(&vm->sxx, m.f[3], m, W48, ty);
-    ok &= make_box_map(&vm->syy, m.f[4], m, W32, ty + 10);
-    ok &= make_box_map(&vm->sxy, m.f[6], m, W48, ty + 10);
-    ok &= make_box_map(&vm->sxz, m.f[7], m, W48, ty);
-    ok &= make_box_map(&vm->syz, m.f[8], m, W32, ty + 10);
-    ok &= make_box_map(&vm->b, m.b, m, W36, ty + 1);
-    ok &= make_box_map(&vm->sxz_c, m.f[7], m, W32, ty);
-    ok &= make_box_map(&vm->syz_c, m.f[8], m, W32, ty);
-    ok &= make_box_map(&vm->szz_c, m.f[5], m, W32, ty);
-    ok &= make_box_map(&vm->b_c, m.b, m, W32, ty);
-    for (int q = 0; q < 3; ++q) ok &= make_box_map(&vm->own[q], m.f[q], m, W32, ty);
-    ok &= make_box_map(&sm->vx, m.f[0], m, W48, ty + 10);
-    ok &= make_box_map(&sm->vy, m.f[1], m, W48, ty + 10);
-    ok &= make_box_map(&sm->vz, m.f[2], m, W48, ty + 10);
-    ok &= make_box_map(&sm->vx_c, m.f[0], m, W32, ty);
-    ok &= make_box_map(&sm->vy_c, m.f[1], m, W32, ty);
-    ok &= make_box_map(&sm->vz_c, m.f[2], m, W32, ty);
-    const float *own[StrMaps::kOwn] = {m.f[3], m.f[4], m.f[5], m.f[6], m.f[7], m.f[8], m.lam, m.mu,
-                                       m.mxy, m.mxz, m.myz};
-    for (int q = 0; q < StrMaps::kOwn; ++q) ok &= make_box_map(&sm->own[q], own[q], m, W32, ty);
+    ok &= make_pool_map(&zm->v_sxx_sxz, m.f[3], m, 4 * st, 2, W48, ty);        // sigma_xx, sigma_xz
+    ok &= make_pool_map(&zm->v_syy_syz, m.f[4], m, 4 * st, 2, W32, ty + 10);   // sigma_yy, sigma_yz
+    ok &= make_pool_map(&zm->v_sxy, m.f[6], m, st, 1, W48, ty + 10);
+    ok &= make_pool_map(&zm->v_b, m.b, m, st, 1, W36, ty + 1);
+    ok &= make_pool_map(&zm->v_lead_xz_yz, m.f[7], m, st, 2, W32, ty);
+    ok &= make_pool_map(&zm->v_lead_zz, m.f[5], m, st, 1, W32, ty);
+    ok &= make_pool_map(&zm->v_lead_b, m.b, m, st, 1, W32, ty);
+    ok &= make_pool_map(&zm->v_own, m.f[0], m, st, 3, W32, ty);
+    ok &= make_pool_map(&zm->s_v, m.f[0], m, st, 3, W48, ty + 10);
+    ok &= make_pool_map(&zm->s_lead_xy, m.f[0], m, st, 2, W32, ty);
+    ok &= make_pool_map(&zm->s_lead_z, m.f[2], m, st, 1, W32, ty);
+    ok &= make_pool_map(&zm->s_own, m.f[3], m, st, StrL<8>::NOWN, W32, ty);
     if (!ok) return cudaErrorInvalidValue;
     cudaError_t e = cells == 1 ? set_attrs<false, 1>() : set_attrs<false, 2>();
     if (e == cudaSuccess) e = cells == 1 ? set_attrs<true, 1>() : set_attrs<true, 2>();
@@ -873,16 +886,15 @@ void zmarch_tiles(const Model &m, int cells, int *ntx, int *nty) {
     *nty = (m.nyc + 8 * cells - 1) / (8 * cells);
 }
 
-cudaError_t zmarch_step(const Model &m, const Physics &ph, const SourceRec &sr, const ZGeom &g,
-                        const VelMaps &vm, const StrMaps &sm, int it, float src_value, bool use_wavelet,
-                        cudaStream_t s, cudaEvent_t *ev) {
+cudaError_t zmarch_step(const Model &m, const Physics &ph, const SourceRec &sr, const ZGeom &g, const ZMaps &zm,
+                        int it, float src_value, bool use_wavelet, cudaStream_t s, cudaEvent_t *ev) {
     const int uw = use_wavelet ? 1 : 0;
     if (ph.fast) {
-        if (g.cells == 1) launch<true, 1>(m, ph, sr, g, vm, sm, it, src_value, uw, s, ev);
-        else launch<true, 2>(m, ph, sr, g, vm, sm, it, src_value, uw, s, ev);
+        if (g.cells == 1) launch<true, 1>(m, ph, sr, g, zm, it, src_value, uw, s, ev);
+        else launch<true, 2>(m, ph, sr, g, zm, it, src_value, uw, s, ev);
     } else {
-        if (g.cells == 1) launch<false, 1>(m, ph, sr, g, vm, sm, it, src_value, uw, s, ev);
-        else launch<false, 2>(m, ph, sr, g, vm, sm, it, src_value, uw, s, ev);
+        if (g.cells == 1) launch<false, 1>(m, ph, sr, g, zm, it, src_value, uw, s, ev);
+        else launch<false, 2>(m, ph, sr, g, zm, it, src_value, uw, s, ev);
     }
     return cudaGetLastError();
 }

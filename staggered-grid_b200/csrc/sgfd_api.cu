@@ -115,7 +115,7 @@ cudaError_t dispatch_on(sgfd_solver *h, const SourceRec &sr, cudaStream_t s, int
     cudaError_t e = h->kernel == SGFD_KERNEL_ZMARCH
                         ? (h->zg.pair ? zpair_step(h->m, h->ph, sr, h16 ? &h->hs : nullptr, h->zg, h->vm, h->sm, it,
                                                    value, use_wavelet, s, ev)
-                                      : zmarch_step(h->m, h->ph, sr, h->zg, h->vm, h->sm, it, value, use_wavelet, s, ev))
+                                      : zmarch_step(h->m, h->ph, sr, h->zg, h->zm, it, value, use_wavelet, s, ev))
                     : h16 ? half_step(h->m, h->ph, sr, h->hs, it, value, use_wavelet, s, ev)
                         : simple_step(h->m, h->ph, sr, it, value, use_wavelet, s, ev);
     if (e == cudaSuccess && h->strip_n > 0)
@@ -144,6 +144,7 @@ void graph_key(const sgfd_solver *h, GraphKey *k) {
     std::memcpy(static_cast<void *>(&k->zg), &h->zg, sizeof h->zg);
     std::memcpy(static_cast<void *>(&k->vm), &h->vm, sizeof h->vm);
     std::memcpy(static_cast<void *>(&k->sm), &h->sm, sizeof h->sm);
+    std::memcpy(static_cast<void *>(&k->zm), &h->zm, sizeof h->zm);
     k->kernel = h->kernel;
     k->audit_every = h->audit_every;
     k->audit_region = h->audit_region;
@@ -451,14 +452,16 @@ int sgfd_create(const sgfd_config *cfg, sgfd_solver **out) {
         return r;
     }
     auto arr = [&](int k) { return reinterpret_cast<float *>(h->field_pool + k * arr_bytes) + kXOff; };
+    // txx..tyz, lambda, mu and the shear moduli consecutive: the z-march
+    // stress update stages a cell's 11 own values with one copy
     for (int k = 0; k < 9; ++k) m.f[k] = arr(k);
-    m.b = arr(9);
-    m.lam = arr(10);
-    m.mu = arr(11);
-    m.rmu = arr(12);
-    m.mxy = arr(13);
-    m.mxz = arr(14);
-    m.myz = arr(15);
+    m.lam = arr(9);
+    m.mu = arr(10);
+    m.mxy = arr(11);
+    m.mxz = arr(12);
+    m.myz = arr(13);
+    m.b = arr(14);
+    m.rmu = arr(15);
     m.split = h->split;
     e = cudaMemsetAsync(h->field_pool, 0, pool_bytes, h->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(h->split, 0, (size_t)kNumSplit * m.npml * sizeof(float), h->stream);
@@ -507,7 +510,7 @@ int sgfd_create(const sgfd_config *cfg, sgfd_solver **out) {
         h->zg.cells = 1;
         h->zg.pair = h16 ? 1 : 0;
         h->zg.tw = h16 ? kPairTileX : kZTileX;
-        e = h16 ? zpair_prepare(m, &h->hs, &h->vm, &h->sm) : zmarch_prepare(m, h->zg.cells, &h->vm, &h->sm);
+        e = h16 ? zpair_prepare(m, &h->hs, &h->vm, &h->sm) : zmarch_prepare(m, h->zg.cells, arr_bytes, &h->zm);
         if (e == cudaSuccess) e = dev_malloc(h, &h->dev_err, sizeof(int));
         if (e == cudaSuccess) e = cudaMemset(h->dev_err, 0, sizeof(int));
         if (e != cudaSuccess) {
@@ -775,7 +778,7 @@ int sgfd_set_tile(sgfd_solver *h, int32_t tile_cols, int32_t tile_rows, int32_t 
     const int cells = tile_rows / 8;
     if (cells != h->zg.cells || (int)pair != h->zg.pair) {
         cudaError_t e = pair ? zpair_prepare(h->m, h->storage != SGFD_STORE_F32 ? &h->hs : nullptr, &h->vm, &h->sm)
-                             : zmarch_prepare(h->m, cells, &h->vm, &h->sm);
+                             : zmarch_prepare(h->m, cells, array_bytes(h->m), &h->zm);
         if (e != cudaSuccess) return cuda_fail(h, e, "z-march re-tiling");
         h->zg.cells = cells;
         h->zg.pair = pair ? 1 : 0;

@@ -20,6 +20,7 @@ struct GraphKey {
     ZGeom zg;
     VelMaps vm;
     StrMaps sm;
+    ZMaps zm;
     int kernel;
     int audit_every, audit_region, audit_count;
     double *audit_hist, *audit;
@@ -39,7 +40,7 @@ struct sgfd_solver {
     int device = 0;
     cudaStream_t stream = nullptr;
     cudaStream_t own_stream = nullptr;
-    char *field_pool = nullptr;   // 9 fields + b, lambda, mu, 1/mu, 3 shear moduli
+    char *field_pool = nullptr;   // 9 fields, lambda, mu, 3 shear moduli, b, 1/mu
     float *split = nullptr;
     int4 *rec = nullptr;
     float *traces = nullptr;
@@ -47,7 +48,8 @@ struct sgfd_solver {
     int wavelet_nt = 0;
     bool medium_set = false;
     int kernel = SGFD_KERNEL_SIMPLE;
-    // z-marching family
+    // z-marching family: single-cell maps (zm) or paired maps (vm, sm)
+    sgfd::ZMaps zm{};
     sgfd::VelMaps vm{};
     sgfd::StrMaps sm{};
     sgfd::ZGeom zg{};

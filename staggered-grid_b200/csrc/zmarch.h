@@ -13,14 +13,31 @@ constexpr int kZTileX = 32;
 // Paired tiling (kernels_zpair.cu): tiles 64 x 8, two x-adjacent cells per thread.
 constexpr int kPairTileX = 64;
 
-// TMA descriptors of the velocity update: x/y-halo boxes of the current plane
-// and 32 x 16 centre boxes of the planes that feed the z register queues.
+// TMA descriptors of the single-cell z-march kernels: 4-D maps over the array
+// pool (x, y, z, array), so that arrays one update reads with the same box
+// shape at the same plane arrive in one copy (one box per map and plane).
+// Arrays of one map are evenly spaced in the pool; the stress update's own
+// cell arrays (txx..tyz, lambda, mu, mxy, mxz, myz) are 11 consecutive ones.
+struct ZMaps {
+    // velocity update, plane z: sigma_xx + sigma_xz (48 x TY), sigma_yy +
+    // sigma_yz (32 x TY+10), sigma_xy (48 x TY+10), buoyancy (36 x TY+1);
+    // lead planes: sigma_xz + sigma_yz at z+4, sigma_zz at z+5, buoyancy at
+    // z+1; own vx, vy, vz (32 x TY each)
+    CUtensorMap v_sxx_sxz, v_syy_syz, v_sxy, v_b, v_lead_xz_yz, v_lead_zz, v_lead_b, v_own;
+    // stress update: vx, vy, vz (48 x TY+10); lead vx + vy at z+5, vz at z+4;
+    // own txx..myz (11 arrays, 32 x TY each)
+    CUtensorMap s_v, s_lead_xy, s_lead_z, s_own;
+};
+
+// TMA descriptors of the paired velocity update (kernels_zpair.cu): x/y-halo
+// boxes of the current plane and centre boxes of the planes that feed the z
+// register queues.
 struct VelMaps {
     CUtensorMap sxx, syy, sxy, sxz, syz, b;      // current plane
     CUtensorMap sxz_c, syz_c, szz_c, b_c;        // lead planes (centre boxes)
     CUtensorMap own[3];                          // own-cell vx, vy, vz (centre boxes)
 };
-// TMA descriptors of the stress update.
+// TMA descriptors of the paired stress update.
 struct StrMaps {
     CUtensorMap vx, vy, vz;                      // current plane
     CUtensorMap vx_c, vy_c, vz_c;                // lead planes
@@ -47,12 +64,14 @@ struct ZGeom {
 bool make_box_map(CUtensorMap *map, const float *grid_origin, const Model &m, int bx, int by);
 bool make_box_map16(CUtensorMap *map, const uint16_t *grid_origin, const Model &m, int bx, int by);
 
+// zmarch_prepare: the maps of the single-cell family over the model's array
+// pool, whose arrays are array_stride bytes apart in the order the stress
+// update reads them (cudaErrorInvalidValue when the pointers are otherwise).
 bool zmarch_supported(const Model &m);
-cudaError_t zmarch_prepare(const Model &m, int cells, VelMaps *vm, StrMaps *sm);
+cudaError_t zmarch_prepare(const Model &m, int cells, size_t array_stride, ZMaps *zm);
 void zmarch_tiles(const Model &m, int cells, int *ntx, int *nty);
-cudaError_t zmarch_step(const Model &m, const Physics &ph, const SourceRec &sr, const ZGeom &g,
-                        const VelMaps &vm, const StrMaps &sm, int it, float src_value, bool use_wavelet,
-                        cudaStream_t s, cudaEvent_t *ev = nullptr);
+cudaError_t zmarch_step(const Model &m, const Physics &ph, const SourceRec &sr, const ZGeom &g, const ZMaps &zm,
+                        int it, float src_value, bool use_wavelet, cudaStream_t s, cudaEvent_t *ev = nullptr);
 // One model of a persistent batch, in device memory (the kernel's TMA reads
 // its tensor maps from there: 64-byte alignment).  Its work items are the
 // (tile, z chunk) pairs of the paired tiling, tile fastest.

@@ -48,6 +48,14 @@ __device__ __forceinline__ void tma3(void *dst, const CUtensorMap *map, int x, i
         : "memory");
 }
 
+// 4-D tiled load: box at (x, y, z, w) of the map into dst.
+__device__ __forceinline__ void tma4(void *dst, const CUtensorMap *map, int x, int y, int z, int w, uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];"
+        ::"r"(sptr(dst)), "l"(map), "r"(x), "r"(y), "r"(z), "r"(w), "r"(sptr(bar))
+        : "memory");
+}
+
 // Wait (bounded) for the stages still in flight before an early exit:
 // planes [from, issued_end) of a ring of S stages started at plane zs.
 template <int S>
