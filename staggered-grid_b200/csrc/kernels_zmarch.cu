@@ -543,16 +543,18 @@ k_stress_zmarch(const __grid_constant__ ZMaps mp, const __grid_constant__ Model 
         pcol[c] = pml_column(m, min(t.cx0 + lx, m.nxc - 1), min(t.cy0 + lyc[c], m.nyc - 1));
     }
 
-    // z queues: qx, qy hold z-4..z+5 (vx, vy); qz holds z-5..z+4 (vz)
-    float qx[CELLS][10], qy[CELLS][10], qz[CELLS][10];
+    // z queues, 11 deep, planes in pairs as in the velocity update: before the
+    // first plane of a pair at z, qx and qy (vx, vy) hold z-4..z+4 and qz (vz)
+    // z-5..z+3 in slots 0..8
+    float qx[CELLS][11], qy[CELLS][11], qz[CELLS][11];
     const int gz0 = t.zs + kHalo;
 #pragma unroll
     for (int c = 0; c < CELLS; ++c) {
 #pragma unroll
         for (int k = 0; k < 9; ++k) {
-            qx[c][k + 1] = m.f[0][col[c] + (uint32_t)(gz0 - 4 + k) * PL];
-            qy[c][k + 1] = m.f[1][col[c] + (uint32_t)(gz0 - 4 + k) * PL];
-            qz[c][k + 1] = m.f[2][col[c] + (uint32_t)(gz0 - 5 + k) * PL];
+            qx[c][k] = m.f[0][col[c] + (uint32_t)(gz0 - 4 + k) * PL];
+            qy[c][k] = m.f[1][col[c] + (uint32_t)(gz0 - 4 + k) * PL];
+            qz[c][k] = m.f[2][col[c] + (uint32_t)(gz0 - 5 + k) * PL];
         }
     }
 
@@ -565,20 +567,16 @@ k_stress_zmarch(const __grid_constant__ ZMaps mp, const __grid_constant__ Model 
     int cz = t.zs;
     int sz = -1;
     if (src >= 0) sz = (int)(src / m.plane);
-    // One plane.  GEN selects the general path (PML cells, source, receivers);
-    // the interior-only path is used for every other tile-plane.  Returns
-    // false when the block votes to abort.
-    auto plane = [&](auto gen_tag) -> bool {
+    // One plane, as in the velocity update (GEN: general path; P: place in
+    // the pair).  Returns false when the block votes to abort.
+    auto plane = [&](auto gen_tag, auto p_tag) -> bool {
         constexpr bool GEN = decltype(gen_tag)::value;
+        constexpr int P = decltype(p_tag)::value;
         const int s = stage;
         unsigned char *st = smem + s * L::STAGE;
         const int gz = cz + kHalo;
         const int kz = band(gz, m.nz, m.pml);
         const bool plane_pml = GEN && (t.xy_pml || kz != 0);
-
-
-        // PML cells: splits and the buoyancy of the damping, loaded before the
-        // stage wait so that their latency overlaps the wait and the stencil
 
         if (!mbar_wait(&bar[s], parity)) failed = true;
 
@@ -604,15 +602,9 @@ k_stress_zmarch(const __grid_constant__ ZMaps mp, const __grid_constant__ Model 
 #pragma unroll
         for (int c = 0; c < CELLS; ++c) {
             const int ly = lyc[c];
-#pragma unroll
-            for (int j = 0; j < 9; ++j) {
-                qx[c][j] = qx[c][j + 1];
-                qy[c][j] = qy[c][j + 1];
-                qz[c][j] = qz[c][j + 1];
-            }
-            qx[c][9] = llx[ly * W32 + lx];
-            qy[c][9] = lly[ly * W32 + lx];
-            qz[c][9] = llz[ly * W32 + lx];
+            qx[c][9 + P] = llx[ly * W32 + lx];
+            qy[c][9 + P] = lly[ly * W32 + lx];
+            qz[c][9 + P] = llz[ly * W32 + lx];
             if (!act[c]) continue;
 
             const float *cx_ = svx + (ly + 5) * W48 + lx + 8;
@@ -629,8 +621,8 @@ k_stress_zmarch(const __grid_constant__ ZMaps mp, const __grid_constant__ Model 
                                         [&](int i) { return make_float2(cx_[(1 + i) * W48], cz_[(1 + i) * W48]); },
                                         [&](int i) { return make_float2(cx_[-i * W48], cz_[-i * W48]); });
                 const float2 pZ = dpair(FAST ? ph.cp[2] : ph.cr,
-                                        [&](int i) { return make_float2(qx[c][5 + i], qy[c][5 + i]); },
-                                        [&](int i) { return make_float2(qx[c][4 - i], qy[c][4 - i]); });
+                                        [&](int i) { return make_float2(qx[c][P + 5 + i], qy[c][P + 5 + i]); },
+                                        [&](int i) { return make_float2(qx[c][P + 4 - i], qy[c][P + 4 - i]); });
                 const float2 pN = dpair(FAST ? ph.cp[3] : ph.cr,
                                         [&](int i) { return make_float2(cx_[i], cy_[i * W48]); },
                                         [&](int i) { return make_float2(cx_[-1 - i], cy_[(-1 - i) * W48]); });
@@ -643,12 +635,12 @@ k_stress_zmarch(const __grid_constant__ ZMaps mp, const __grid_constant__ Model 
                 dYy = CELLS == 2 ? dYy2[c] : dB<FAST, 1>(ph, [&](int o) { return cy_[o * W48]; });
                 xyY = CELLS == 2 ? xyY2[c] : dF<FAST, 1>(ph, [&](int o) { return cx_[o * W48]; });
                 xyX = dF<FAST, 0>(ph, [&](int o) { return cy_[o]; });
-                xzZ = dF<FAST, 2>(ph, [&](int o) { return qx[c][4 + o]; });
+                xzZ = dF<FAST, 2>(ph, [&](int o) { return qx[c][P + 4 + o]; });
                 xzX = dF<FAST, 0>(ph, [&](int o) { return cz_[o]; });
-                yzZ = dF<FAST, 2>(ph, [&](int o) { return qy[c][4 + o]; });
+                yzZ = dF<FAST, 2>(ph, [&](int o) { return qy[c][P + 4 + o]; });
                 yzY = CELLS == 2 ? yzY2[c] : dF<FAST, 1>(ph, [&](int o) { return cz_[o * W48]; });
             }
-            dZz = dB<FAST, 2>(ph, [&](int o) { return qz[c][5 + o]; });
+            dZz = dB<FAST, 2>(ph, [&](int o) { return qz[c][P + 5 + o]; });
 
             const int e = ly * W32 + lx;
             const float l = own[6 * OS + e], mu_c = own[7 * OS + e];
@@ -743,12 +735,24 @@ k_stress_zmarch(const __grid_constant__ ZMaps mp, const __grid_constant__ Model 
         }
         return true;
     };
-    for (; cz < t.ze; ++cz) {
+    auto run = [&](auto p_tag) -> bool {
         const int gzp = cz + kHalo;
         const bool gen = t.xy_pml || band(gzp, m.nz, m.pml) != 0 || gzp == sz || gzp == rz;
-        if (!(gen ? plane(std::true_type{}) : plane(std::false_type{}))) {
-            abort = true;
-            break;
+        return gen ? plane(std::true_type{}, p_tag) : plane(std::false_type{}, p_tag);
+    };
+    while (cz < t.ze) {
+        if (!run(std::integral_constant<int, 0>{})) { abort = true; break; }
+        if (++cz == t.ze) break;
+        if (!run(std::integral_constant<int, 1>{})) { abort = true; break; }
+        ++cz;
+#pragma unroll
+        for (int c = 0; c < CELLS; ++c) {
+#pragma unroll
+            for (int j = 0; j < 9; ++j) {
+                qx[c][j] = qx[c][j + 2];
+                qy[c][j] = qy[c][j + 2];
+                qz[c][j] = qz[c][j + 2];
+            }
         }
     }
     if (abort && tid == 0) {
