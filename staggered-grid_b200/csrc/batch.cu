@@ -12,7 +12,7 @@
 // cooperative launch runs all steps of all models instead: its CTAs take the
 // models' (tile, z chunk) work items from a global counter, velocity phase
 // then stress phase, with a bounded grid barrier between the phases
-// (kernels_zpair.cu, k_batch_zpair).
+// (kernels_zmarch.cu, k_batch_zmarch; the models run the 32 x 8 tiling).
 #include <algorithm>
 #include <cstdarg>
 #include <cstdio>
@@ -40,7 +40,7 @@ struct sgfd_batch {
     bool pfast = false;
     int barrier_ctas = 0;                 // 0: as many as launched
     int ctas = 0;                         // CTAs that fit at once
-    PairModel *pdesc = nullptr;           // device copies of the models' descriptors
+    ZModel *pdesc = nullptr;              // device copies of the models' descriptors
     int *pfirst = nullptr;                // prefix sums of the models' work items
     unsigned *pctl = nullptr;             // barrier arrivals + work counters
     int pctl_steps = 0;
@@ -118,7 +118,7 @@ int capture(sgfd_batch *b) {
     return SGFD_OK;
 }
 
-// Whether a model can run in a persistent batch (paired z-march tiling).
+// Whether a model can run in a persistent batch (single-cell z-march tiling).
 const char *persistent_blocker(const sgfd_solver *h) {
     if (h->storage != SGFD_STORE_F32) return "16-bit storage";
     if (!h->dev_err) return "no z-marching kernels on this grid";
@@ -137,13 +137,12 @@ int build_descriptors(sgfd_batch *b) {
         current = std::memcmp(&k, &b->pkeys[i], sizeof k) == 0;
     }
     if (current) return SGFD_OK;
-    std::vector<PairModel> d(n);
+    std::vector<ZModel> d(n);
     std::vector<int> first(n + 1, 0);
     for (int i = 0; i < n; ++i) {
         const sgfd_solver *h = b->models[i];
         std::memset(static_cast<void *>(&d[i]), 0, sizeof d[i]);
-        d[i].vm = h->vm;
-        d[i].sm = h->sm;
+        d[i].zm = h->zm;
         d[i].m = h->m;
         d[i].ph = h->ph;
         d[i].g = h->zg;
@@ -153,12 +152,12 @@ int build_descriptors(sgfd_batch *b) {
         first[i + 1] = first[i] + d[i].items;
     }
     if (!b->pdesc) {
-        BATCH_CUDA(b, cudaMalloc(&b->pdesc, (size_t)n * sizeof(PairModel)), "batch descriptors");
+        BATCH_CUDA(b, cudaMalloc(&b->pdesc, (size_t)n * sizeof(ZModel)), "batch descriptors");
         BATCH_CUDA(b, cudaMalloc(&b->pfirst, (size_t)(n + 1) * sizeof(int)), "batch descriptors");
         BATCH_CUDA(b, cudaMalloc(&b->pstatus, sizeof(int)), "batch status");
         BATCH_CUDA(b, cudaMemset(b->pstatus, 0, sizeof(int)), "batch status");
     }
-    BATCH_CUDA(b, cudaMemcpy(b->pdesc, d.data(), (size_t)n * sizeof(PairModel), cudaMemcpyHostToDevice),
+    BATCH_CUDA(b, cudaMemcpy(b->pdesc, d.data(), (size_t)n * sizeof(ZModel), cudaMemcpyHostToDevice),
                "batch descriptors");
     BATCH_CUDA(b, cudaMemcpy(b->pfirst, first.data(), (size_t)(n + 1) * sizeof(int), cudaMemcpyHostToDevice),
                "batch descriptors");
@@ -172,7 +171,8 @@ int run_persistent(sgfd_batch *b, int it0, int nsteps) {
     for (size_t i = 0; i < b->models.size(); ++i) {
         const char *why = persistent_blocker(b->models[i]);
         if (why) return bfail(b, SGFD_ERR_STATE, "model %zu cannot run persistently: %s", i, why);
-        if (b->models[i]->zg.pair != 1 || (bool)b->models[i]->ph.fast != b->pfast)
+        const sgfd_solver *h = b->models[i];
+        if (h->zg.pair != 0 || h->zg.cells != 1 || (bool)h->ph.fast != b->pfast)
             return bfail(b, SGFD_ERR_STATE, "model %zu changed tiling or rounding since sgfd_batch_set_persistent", i);
     }
     int r = build_descriptors(b);
@@ -187,8 +187,8 @@ int run_persistent(sgfd_batch *b, int it0, int nsteps) {
     BATCH_CUDA(b, cudaMemsetAsync(b->pctl, 0, (size_t)(1 + 2 * nsteps) * sizeof(unsigned), b->stream),
                "batch counters");
     const int bar = b->barrier_ctas > 0 ? b->barrier_ctas : b->ctas;
-    BATCH_CUDA(b, zpair_batch_run(b->pdesc, (int)b->models.size(), b->pfirst, it0, nsteps, b->pctl, bar, b->ctas,
-                                  b->pfast, b->pstatus, b->stream),
+    BATCH_CUDA(b, zmarch_batch_run(b->pdesc, (int)b->models.size(), b->pfirst, it0, nsteps, b->pctl, bar, b->ctas,
+                                   b->pfast, b->pstatus, b->stream),
                "persistent batch launch");
     return SGFD_OK;
 }
@@ -211,11 +211,11 @@ int sgfd_batch_set_persistent(sgfd_batch *b, int32_t on, int32_t barrier_ctas) {
         if ((bool)b->models[i]->ph.fast != (bool)b->models[0]->ph.fast)
             return bfail(b, SGFD_ERR_UNSUPPORTED, "models %zu and 0 differ in rounding mode", i);
     }
-    b->ctas = zpair_batch_ctas(b->device);
+    b->ctas = zmarch_batch_ctas(b->device);
     if (b->ctas <= 0) return bfail(b, SGFD_ERR_UNSUPPORTED, "the persistent batch kernel does not fit this device");
     for (size_t i = 0; i < b->models.size(); ++i) {
         sgfd_solver *h = b->models[i];
-        if (h->zg.pair != 1 && sgfd_set_tile(h, kPairTileX, 8, h->zchunk_req) != SGFD_OK)
+        if ((h->zg.pair != 0 || h->zg.cells != 1) && sgfd_set_tile(h, kZTileX, 8, h->zchunk_req) != SGFD_OK)
             return bfail(b, SGFD_ERR_CUDA, "model %zu: %s", i, h->err.c_str());
     }
     b->pfast = b->models[0]->ph.fast != 0;

@@ -106,15 +106,14 @@ struct Tile {
 };
 
 template <int TY>
-__device__ __forceinline__ Tile make_tile(const Model &m, const ZGeom &g) {
+__device__ __forceinline__ Tile make_tile(const Model &m, const ZGeom &g, int tile, int chunk) {
     Tile t;
-    const int tile = blockIdx.x;
     t.cx0 = (tile % g.ntx) * TX;
     t.cy0 = (tile / g.ntx) * TY;
     t.gx0 = t.cx0 + kHalo;
     t.gy0 = t.cy0 + kHalo;
     t.xd = t.gx0 + kXOff;
-    t.zs = blockIdx.y * g.zc;
+    t.zs = chunk * g.zc;
     t.ze = min(t.zs + g.zc, m.nzc);
     t.xy_pml = t.cx0 < m.pml || t.cx0 + TX > m.nxc - m.pml || t.cy0 < m.pml || t.cy0 + TY > m.nyc - m.pml;
     return t;
@@ -171,35 +170,34 @@ __device__ __forceinline__ void vel_issue(const TmaBox *b, int n, unsigned char 
     issue_boxes(b, n, st, bar, cz + kHalo);
 }
 
-template <bool FAST, int CELLS>
-__global__ void __launch_bounds__(NT, 3)
-k_velocity_zmarch(const __grid_constant__ ZMaps mp, const __grid_constant__ Model m, const __grid_constant__ Physics ph,
-                  const __grid_constant__ ZGeom g, const __grid_constant__ SourceRec sr, int it_arg,
-                  float src_value, int use_wavelet) {
+// The velocity update of one work item: the tile `tile` (x fastest) over z
+// chunk `chunk`.  smem: the stage ring; bar: its S initialised mbarriers,
+// whose phase parities pbits carries from item to item (bit s: the parity
+// the next wait on stage s expects); boxes: per-warp TMA box scratch.
+// Returns false after a bounded wait gave up (g.err set, copies drained).
+// MANY: the CTA runs several items (persistent batch); a single-item launch
+// keeps one parity for the whole ring and skips the fences a previous item needs.
+template <bool FAST, int CELLS, bool MANY>
+__device__ __forceinline__ bool vel_item(const ZMaps &mp, const Model &m, const Physics &ph, const ZGeom &g,
+                                         const SourceRec &sr, int it_arg, float src_value, int use_wavelet, int tile,
+                                         int chunk, unsigned char *smem, uint64_t *bar,
+                                         TmaBox (*boxes)[kMaxBoxesPerWarp], uint32_t &pbits) {
     constexpr int TY = 8 * CELLS;
     using L = VelL<TY>;
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    unsigned char *smem = align_smem(smem_raw);
-    __shared__ __align__(8) uint64_t bar[S];
-    const Tile t = make_tile<TY>(m, g);
+    const Tile t = make_tile<TY>(m, g, tile, chunk);
     const int tid = threadIdx.x, lx = tid & 31, ty = tid >> 5;
-    if (tid == 0) {
-        for (int s = 0; s < S; ++s) mbar_init(&bar[s], 1);
-        fence_barrier_init();
-    }
-    __syncthreads();
     const int warp = tid >> 5;
-    __shared__ TmaBox boxes[kWarps][kMaxBoxesPerWarp];
     const TmaBox *mybox = boxes[warp];
     const int nbox = (kVelBoxes - warp + kWarps - 1) / kWarps;
     if (lx == 0) {
         for (int j = 0; j < nbox; ++j) boxes[warp][j] = vel_box<TY>(mp, t, warp + j * kWarps);
+        if (MANY) fence_proxy_async();   // a previous item's stages were read through the generic proxy
         for (int s = 0; s < S && t.zs + s < t.ze; ++s)
             vel_issue<TY>(mybox, nbox, smem + s * L::STAGE, &bar[s], t.zs + s, warp);
     }
     int issued_end = min(t.zs + S, t.ze);   // planes [zs, issued_end) issued
-    int stage = 0;                          // stage of plane cz, and the parity of its barrier
-    uint32_t parity = 0;
+    int stage = 0;                          // stage of plane cz
+    uint32_t parity = 0;                    // single item: the parity of every stage's next wait
 
     const int it = step_index(sr, it_arg);
     const float inj = ph.inj_dt2 * ((use_wavelet && sr.wavelet) ? sr.wavelet[it] : src_value);
@@ -245,8 +243,8 @@ k_velocity_zmarch(const __grid_constant__ ZMaps mp, const __grid_constant__ Mode
     }
 
     // receivers of this tile, sorted by z: skip those below the chunk
-    int rp = g.rec_off[blockIdx.x];
-    const int rend = g.rec_off[blockIdx.x + 1];
+    int rp = g.rec_off[tile];
+    const int rend = g.rec_off[tile + 1];
     while (rp < rend && g.rec_list[rp].z < gz0) ++rp;
     int rz = rp < rend ? g.rec_list[rp].z : 0x7fffffff;   // z of the next receiver
 
@@ -284,7 +282,7 @@ k_velocity_zmarch(const __grid_constant__ ZMaps mp, const __grid_constant__ Mode
             }
         }
 
-        if (!mbar_wait(&bar[s], parity)) failed = true;
+        if (!mbar_wait(&bar[s], MANY ? (pbits >> s) & 1u : parity)) failed = true;
 
         // source patch of the staged copies (uniform branch)
         if (GEN && src_near && (gz == sz || gz + 5 == sz)) {
@@ -448,9 +446,10 @@ k_velocity_zmarch(const __grid_constant__ ZMaps mp, const __grid_constant__ Mode
             }
             issued_end = cz + S + 1;
         }
+        if (MANY) pbits ^= 1u << s;
         if (++stage == S) {
             stage = 0;
-            parity ^= 1u;
+            if (!MANY) parity ^= 1u;
         }
         return true;
     };
@@ -464,8 +463,28 @@ k_velocity_zmarch(const __grid_constant__ ZMaps mp, const __grid_constant__ Mode
     }
     if (abort && tid == 0) {
         atomicExch(g.err, 1);
-        drain<S>(bar, issued_end, cz, t.zs);
+        if (MANY) drain_bits<S>(bar, issued_end, cz, t.zs, pbits);
+        else drain<S>(bar, issued_end, cz, t.zs);
     }
+    return !abort;
+}
+
+template <bool FAST, int CELLS>
+__global__ void __launch_bounds__(NT, 3)
+k_velocity_zmarch(const __grid_constant__ ZMaps mp, const __grid_constant__ Model m, const __grid_constant__ Physics ph,
+                  const __grid_constant__ ZGeom g, const __grid_constant__ SourceRec sr, int it_arg,
+                  float src_value, int use_wavelet) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t bar[S];
+    __shared__ TmaBox boxes[kWarps][kMaxBoxesPerWarp];
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < S; ++s) mbar_init(&bar[s], 1);
+        fence_barrier_init();
+    }
+    __syncthreads();
+    uint32_t pbits = 0;
+    vel_item<FAST, CELLS, false>(mp, m, ph, g, sr, it_arg, src_value, use_wavelet, blockIdx.x, blockIdx.y,
+                          align_smem(smem_raw), bar, boxes, pbits);
 }
 
 // ---------------------------------------------------------------------------
@@ -491,35 +510,28 @@ __device__ __forceinline__ void str_issue(const TmaBox *b, int n, unsigned char 
     issue_boxes(b, n, st, bar, cz + kHalo);
 }
 
-template <bool FAST, int CELLS>
-__global__ void __launch_bounds__(NT, 3)
-k_stress_zmarch(const __grid_constant__ ZMaps mp, const __grid_constant__ Model m, const __grid_constant__ Physics ph,
-                  const __grid_constant__ ZGeom g, const __grid_constant__ SourceRec sr, int it_arg,
-                float src_value, int use_wavelet) {
+// The stress update of one work item, as vel_item.
+template <bool FAST, int CELLS, bool MANY>
+__device__ __forceinline__ bool str_item(const ZMaps &mp, const Model &m, const Physics &ph, const ZGeom &g,
+                                         const SourceRec &sr, int it_arg, float src_value, int use_wavelet, int tile,
+                                         int chunk, unsigned char *smem, uint64_t *bar,
+                                         TmaBox (*boxes)[kMaxBoxesPerWarp], uint32_t &pbits) {
     constexpr int TY = 8 * CELLS;
     using L = StrL<TY>;
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    unsigned char *smem = align_smem(smem_raw);
-    __shared__ __align__(8) uint64_t bar[S];
-    const Tile t = make_tile<TY>(m, g);
+    const Tile t = make_tile<TY>(m, g, tile, chunk);
     const int tid = threadIdx.x, lx = tid & 31, ty = tid >> 5;
-    if (tid == 0) {
-        for (int s = 0; s < S; ++s) mbar_init(&bar[s], 1);
-        fence_barrier_init();
-    }
-    __syncthreads();
     const int warp = tid >> 5;
-    __shared__ TmaBox boxes[kWarps][kMaxBoxesPerWarp];
     const TmaBox *mybox = boxes[warp];
     const int nbox = (kStrBoxes - warp + kWarps - 1) / kWarps;
     if (lx == 0) {
         for (int j = 0; j < nbox; ++j) boxes[warp][j] = str_box<TY>(mp, t, warp + j * kWarps);
+        if (MANY) fence_proxy_async();   // a previous item's stages were read through the generic proxy
         for (int s = 0; s < S && t.zs + s < t.ze; ++s)
             str_issue<TY>(mybox, nbox, smem + s * L::STAGE, &bar[s], t.zs + s, warp);
     }
     int issued_end = min(t.zs + S, t.ze);   // planes [zs, issued_end) issued
-    int stage = 0;                          // stage of plane cz, and the parity of its barrier
-    uint32_t parity = 0;
+    int stage = 0;                          // stage of plane cz
+    uint32_t parity = 0;                    // single item: the parity of every stage's next wait
 
     const int it = step_index(sr, it_arg);
     const float inj = ph.inj_dt2 * ((use_wavelet && sr.wavelet) ? sr.wavelet[it] : src_value);
@@ -558,8 +570,8 @@ k_stress_zmarch(const __grid_constant__ ZMaps mp, const __grid_constant__ Model 
         }
     }
 
-    int rp = g.rec_off[blockIdx.x];
-    const int rend = g.rec_off[blockIdx.x + 1];
+    int rp = g.rec_off[tile];
+    const int rend = g.rec_off[tile + 1];
     while (rp < rend && g.rec_list[rp].z < gz0) ++rp;
     int rz = rp < rend ? g.rec_list[rp].z : 0x7fffffff;
 
@@ -578,7 +590,7 @@ k_stress_zmarch(const __grid_constant__ ZMaps mp, const __grid_constant__ Model 
         const int kz = band(gz, m.nz, m.pml);
         const bool plane_pml = GEN && (t.xy_pml || kz != 0);
 
-        if (!mbar_wait(&bar[s], parity)) failed = true;
+        if (!mbar_wait(&bar[s], MANY ? (pbits >> s) & 1u : parity)) failed = true;
 
         const float *svx = reinterpret_cast<const float *>(st + L::VX);
         const float *svy = reinterpret_cast<const float *>(st + L::VY);
@@ -729,9 +741,10 @@ k_stress_zmarch(const __grid_constant__ ZMaps mp, const __grid_constant__ Model 
             }
             issued_end = cz + S + 1;
         }
+        if (MANY) pbits ^= 1u << s;
         if (++stage == S) {
             stage = 0;
-            parity ^= 1u;
+            if (!MANY) parity ^= 1u;
         }
         return true;
     };
@@ -757,8 +770,28 @@ k_stress_zmarch(const __grid_constant__ ZMaps mp, const __grid_constant__ Model 
     }
     if (abort && tid == 0) {
         atomicExch(g.err, 1);
-        drain<S>(bar, issued_end, cz, t.zs);
+        if (MANY) drain_bits<S>(bar, issued_end, cz, t.zs, pbits);
+        else drain<S>(bar, issued_end, cz, t.zs);
     }
+    return !abort;
+}
+
+template <bool FAST, int CELLS>
+__global__ void __launch_bounds__(NT, 3)
+k_stress_zmarch(const __grid_constant__ ZMaps mp, const __grid_constant__ Model m, const __grid_constant__ Physics ph,
+                const __grid_constant__ ZGeom g, const __grid_constant__ SourceRec sr, int it_arg,
+                float src_value, int use_wavelet) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t bar[S];
+    __shared__ TmaBox boxes[kWarps][kMaxBoxesPerWarp];
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < S; ++s) mbar_init(&bar[s], 1);
+        fence_barrier_init();
+    }
+    __syncthreads();
+    uint32_t pbits = 0;
+    str_item<FAST, CELLS, false>(mp, m, ph, g, sr, it_arg, src_value, use_wavelet, blockIdx.x, blockIdx.y,
+                          align_smem(smem_raw), bar, boxes, pbits);
 }
 
 PFN_cuTensorMapEncodeTiled_v12000 get_encoder() {
@@ -786,6 +819,96 @@ cudaError_t set_attrs() {
         e = cudaFuncSetAttribute(k_stress_zmarch<FAST, CELLS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  str_smem<CELLS>());
     return e;
+}
+
+// ---------------------------------------------------------------------------
+// persistent batch: every model's (tile, z chunk) work items of the 32 x 8
+// tiling, the velocity phase then the stress phase of each step, a bounded
+// grid barrier after each phase
+// ---------------------------------------------------------------------------
+
+constexpr int batch_smem() { return vel_smem<1>() > str_smem<1>() ? vel_smem<1>() : str_smem<1>(); }
+
+// The two updates as called functions, so that each is register-allocated on
+// its own rather than inlined side by side into the persistent loop.
+template <bool FAST>
+__device__ __noinline__ bool vel_item_call(const ZMaps &mp, const Model &m, const Physics &ph, const ZGeom &g,
+                                           const SourceRec &sr, int it, int tile, int chunk, unsigned char *smem,
+                                           uint64_t *bar, TmaBox (*boxes)[kMaxBoxesPerWarp], uint32_t &pbits) {
+    return vel_item<FAST, 1, true>(mp, m, ph, g, sr, it, 0.0f, 1, tile, chunk, smem, bar, boxes, pbits);
+}
+template <bool FAST>
+__device__ __noinline__ bool str_item_call(const ZMaps &mp, const Model &m, const Physics &ph, const ZGeom &g,
+                                           const SourceRec &sr, int it, int tile, int chunk, unsigned char *smem,
+                                           uint64_t *bar, TmaBox (*boxes)[kMaxBoxesPerWarp], uint32_t &pbits) {
+    return str_item<FAST, 1, true>(mp, m, ph, g, sr, it, 0.0f, 1, tile, chunk, smem, bar, boxes, pbits);
+}
+
+// Two CTAs per SM: the 128 registers a thread then has keep both called
+// updates nearly free of spills (at three CTAs the stress update, whose
+// physics and geometry come from shared memory here, spills 0.5 KB).
+template <bool FAST>
+__global__ void __launch_bounds__(NT, 2)
+k_batch_zmarch(const ZModel *models, int nmodels, const int *first_item, int it0, int nsteps, unsigned *ctl,
+               unsigned barrier_ctas, int *status) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t bar_v[S];
+    __shared__ __align__(8) uint64_t bar_s[S];
+    __shared__ TmaBox boxes[kWarps][kMaxBoxesPerWarp];
+    __shared__ int item_sh, ok_sh;
+    // the current model's physics and geometry, read in every plane's inner
+    // loops: a shared copy instead of loads from the descriptor array
+    __shared__ __align__(16) Physics ph_s;
+    __shared__ __align__(16) Model m_s;
+    int cur = -1;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < S; ++s) mbar_init(&bar_v[s], 1);
+        for (int s = 0; s < S; ++s) mbar_init(&bar_s[s], 1);
+        fence_barrier_init();
+    }
+    __syncthreads();
+    unsigned char *smem = align_smem(smem_raw);
+    uint32_t pv = 0, ps = 0;
+    const int total = first_item[nmodels];
+    unsigned phases = 0;
+    for (int k = 0; k < nsteps; ++k) {
+        for (int p = 0; p < 2; ++p) {
+            unsigned *ctr = ctl + 1 + 2 * k + p;
+            for (;;) {
+                if (threadIdx.x == 0) item_sh = (int)atomicAdd(ctr, 1u);
+                __syncthreads();
+                const int item = item_sh;
+                __syncthreads();
+                if (item >= total) break;
+                int mi = 0;
+                while (first_item[mi + 1] <= item) ++mi;
+                const ZModel &d = models[mi];
+                if (mi != cur) {   // every thread is past the previous item (the barriers above)
+                    const uint32_t *src = reinterpret_cast<const uint32_t *>(&d.ph);
+                    uint32_t *dst = reinterpret_cast<uint32_t *>(&ph_s);
+                    for (int i = threadIdx.x; i < (int)(sizeof(Physics) / 4); i += NT) dst[i] = src[i];
+                    src = reinterpret_cast<const uint32_t *>(&d.m);
+                    dst = reinterpret_cast<uint32_t *>(&m_s);
+                    for (int i = threadIdx.x; i < (int)(sizeof(Model) / 4); i += NT) dst[i] = src[i];
+                    __syncthreads();
+                    cur = mi;
+                }
+                const int local = item - first_item[mi];
+                const int ntiles = d.g.ntx * d.g.nty;
+                const bool ok =
+                    p == 0 ? vel_item_call<FAST>(d.zm, m_s, ph_s, d.g, d.sr, it0 + k, local % ntiles, local / ntiles,
+                                                 smem, bar_v, boxes, pv)
+                           : str_item_call<FAST>(d.zm, m_s, ph_s, d.g, d.sr, it0 + k, local % ntiles, local / ntiles,
+                                                 smem, bar_s, boxes, ps);
+                if (!ok) {
+                    if (threadIdx.x == 0) atomicExch(status, kBatchWaitTma);
+                    return;
+                }
+            }
+            ++phases;
+            if (!grid_sync(ctl, phases * barrier_ctas, status, kBatchWaitGrid, &ok_sh)) return;
+        }
+    }
 }
 
 template <bool FAST, int CELLS>
@@ -901,6 +1024,29 @@ cudaError_t zmarch_step(const Model &m, const Physics &ph, const SourceRec &sr, 
         else launch<false, 2>(m, ph, sr, g, zm, it, src_value, uw, s, ev);
     }
     return cudaGetLastError();
+}
+
+int zmarch_batch_ctas(int device) {
+    int sms = 0, per = 0, per2 = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return 0;
+    if (cudaFuncSetAttribute(k_batch_zmarch<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, batch_smem()) !=
+            cudaSuccess ||
+        cudaFuncSetAttribute(k_batch_zmarch<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, batch_smem()) !=
+            cudaSuccess)
+        return 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_batch_zmarch<true>, NT, batch_smem()) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per2, k_batch_zmarch<false>, NT, batch_smem()) != cudaSuccess)
+        return 0;
+    return sms * (per < per2 ? per : per2);
+}
+
+cudaError_t zmarch_batch_run(const ZModel *models, int nmodels, const int *first_item, int it0, int nsteps,
+                             unsigned *ctl, int barrier_ctas, int ctas, bool fast, int *status, cudaStream_t s) {
+    unsigned target = (unsigned)barrier_ctas;
+    void *args[] = {(void *)&models, (void *)&nmodels, (void *)&first_item, (void *)&it0, (void *)&nsteps,
+                    (void *)&ctl, (void *)&target, (void *)&status};
+    const void *fn = fast ? (const void *)k_batch_zmarch<true> : (const void *)k_batch_zmarch<false>;
+    return cudaLaunchCooperativeKernel(fn, dim3(ctas), dim3(NT), args, batch_smem(), s);
 }
 
 }  // namespace sgfd

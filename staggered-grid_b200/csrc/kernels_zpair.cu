@@ -968,107 +968,6 @@ k_stress_zpair(const __grid_constant__ StrMaps mp, const __grid_constant__ Model
                        align_smem(smem_raw), bar, boxes, pbits);
 }
 
-// ---------------------------------------------------------------------------
-// persistent batch: every model's work items, both updates, nsteps steps
-// ---------------------------------------------------------------------------
-
-constexpr uint32_t kGridWaitCap = 1u << 20;   // polls of about 1 us: a grid barrier gives up after ~1 s
-
-__device__ __forceinline__ unsigned ld_acquire(const unsigned *p) {
-    unsigned v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-
-// All CTAs of the launch meet here: arrivals are counted in *arrive, and
-// this barrier completes when `target` arrivals have been counted.  Bounded:
-// false (and *status = kBatchWaitGrid) when the count does not arrive.  The
-// fences make the other CTAs' stores of the finished phase visible to this
-// CTA's later loads, TMA (async proxy) included.
-__device__ __forceinline__ bool grid_sync(unsigned *arrive, unsigned target, int *status, int *ok_sh) {
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        atomicAdd(arrive, 1u);
-        bool ok = true;
-        for (uint32_t n = 0; ld_acquire(arrive) < target; ++n) {
-            if (n >= kGridWaitCap) { ok = false; break; }
-            __nanosleep(1000);
-        }
-        __threadfence();
-        asm volatile("fence.proxy.async.global;" ::: "memory");
-        if (!ok) atomicExch(status, kBatchWaitGrid);
-        *ok_sh = ok;
-    }
-    __syncthreads();
-    return *ok_sh != 0;
-}
-
-template <bool FAST>
-__global__ void __launch_bounds__(NT, 2)
-k_batch_zpair(const PairModel *models, int nmodels, const int *first_item, int it0, int nsteps, unsigned *ctl,
-              unsigned barrier_ctas, int *status) {
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    __shared__ __align__(8) uint64_t bar_v[SV];
-    __shared__ __align__(8) uint64_t bar_s[SS];
-    __shared__ TmaBox boxes[kWarps][kMaxBoxesPerWarp];
-    __shared__ int item_sh, ok_sh;
-    // the current model's physics and geometry, read in every plane's inner
-    // loops: a shared copy instead of loads from the descriptor array
-    __shared__ __align__(16) Physics ph_s;
-    __shared__ __align__(16) Model m_s;
-    int cur = -1;
-    if (threadIdx.x == 0) {
-        for (int s = 0; s < SV; ++s) mbar_init(&bar_v[s], 1);
-        for (int s = 0; s < SS; ++s) mbar_init(&bar_s[s], 1);
-        fence_barrier_init();
-    }
-    __syncthreads();
-    unsigned char *smem = align_smem(smem_raw);
-    uint32_t pv = 0, ps = 0;
-    const int total = first_item[nmodels];
-    unsigned phases = 0;
-    for (int k = 0; k < nsteps; ++k) {
-        for (int p = 0; p < 2; ++p) {
-            unsigned *ctr = ctl + 1 + 2 * k + p;
-            for (;;) {
-                if (threadIdx.x == 0) item_sh = (int)atomicAdd(ctr, 1u);
-                __syncthreads();
-                const int item = item_sh;
-                __syncthreads();
-                if (item >= total) break;
-                int mi = 0;
-                while (first_item[mi + 1] <= item) ++mi;
-                const PairModel &d = models[mi];
-                if (mi != cur) {   // every thread is past the previous item (the barriers above)
-                    const uint32_t *src = reinterpret_cast<const uint32_t *>(&d.ph);
-                    uint32_t *dst = reinterpret_cast<uint32_t *>(&ph_s);
-                    for (int i = threadIdx.x; i < (int)(sizeof(Physics) / 4); i += NT) dst[i] = src[i];
-                    src = reinterpret_cast<const uint32_t *>(&d.m);
-                    dst = reinterpret_cast<uint32_t *>(&m_s);
-                    for (int i = threadIdx.x; i < (int)(sizeof(Model) / 4); i += NT) dst[i] = src[i];
-                    __syncthreads();
-                    cur = mi;
-                }
-                const int local = item - first_item[mi];
-                const int ntiles = d.g.ntx * d.g.nty;
-                const HalfState no16{};
-                const bool ok =
-                    p == 0 ? vel_pair<FAST, SGFD_STORE_F32>(d.vm, m_s, ph_s, d.g, d.sr, no16, it0 + k, 0.0f, 1,
-                                                            local % ntiles, local / ntiles, smem, bar_v, boxes, pv)
-                           : str_pair<FAST, SGFD_STORE_F32>(d.sm, m_s, ph_s, d.g, d.sr, no16, it0 + k, 0.0f, 1,
-                                                            local % ntiles, local / ntiles, smem, bar_s, boxes, ps);
-                if (!ok) {
-                    if (threadIdx.x == 0) atomicExch(status, kBatchWaitTma);
-                    return;
-                }
-            }
-            ++phases;
-            if (!grid_sync(ctl, phases * barrier_ctas, status, &ok_sh)) return;
-        }
-    }
-}
-
 template <int ST>
 constexpr int vel_smem() { return SV * VelP<Sto<ST>::ES>::STAGE + 128; }
 template <int ST>
@@ -1111,37 +1010,7 @@ cudaError_t launch_st(const Model &m, const Physics &ph, const SourceRec &sr, co
     return cudaGetLastError();
 }
 
-constexpr int batch_smem() {
-    return vel_smem<SGFD_STORE_F32>() > str_smem<SGFD_STORE_F32>() ? vel_smem<SGFD_STORE_F32>()
-                                                                   : str_smem<SGFD_STORE_F32>();
-}
-
 }  // namespace
-
-int zpair_batch_ctas(int device) {
-    int sms = 0, per = 0;
-    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) return 0;
-    if (cudaFuncSetAttribute(k_batch_zpair<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, batch_smem()) !=
-            cudaSuccess ||
-        cudaFuncSetAttribute(k_batch_zpair<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, batch_smem()) !=
-            cudaSuccess)
-        return 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_batch_zpair<true>, NT, batch_smem()) != cudaSuccess)
-        return 0;
-    int per2 = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per2, k_batch_zpair<false>, NT, batch_smem()) != cudaSuccess)
-        return 0;
-    return sms * (per < per2 ? per : per2);
-}
-
-cudaError_t zpair_batch_run(const PairModel *models, int nmodels, const int *first_item, int it0, int nsteps,
-                            unsigned *ctl, int barrier_ctas, int ctas, bool fast, int *status, cudaStream_t s) {
-    unsigned target = (unsigned)barrier_ctas;
-    void *args[] = {(void *)&models, (void *)&nmodels, (void *)&first_item, (void *)&it0, (void *)&nsteps,
-                    (void *)&ctl, (void *)&target, (void *)&status};
-    const void *fn = fast ? (const void *)k_batch_zpair<true> : (const void *)k_batch_zpair<false>;
-    return cudaLaunchCooperativeKernel(fn, dim3(ctas), dim3(NT), args, batch_smem(), s);
-}
 
 cudaError_t zpair_prepare(const Model &m, const HalfState *hs, VelMaps *vm, StrMaps *sm) {
     constexpr int ty = PY;

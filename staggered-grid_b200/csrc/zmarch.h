@@ -74,10 +74,9 @@ cudaError_t zmarch_step(const Model &m, const Physics &ph, const SourceRec &sr, 
                         int it, float src_value, bool use_wavelet, cudaStream_t s, cudaEvent_t *ev = nullptr);
 // One model of a persistent batch, in device memory (the kernel's TMA reads
 // its tensor maps from there: 64-byte alignment).  Its work items are the
-// (tile, z chunk) pairs of the paired tiling, tile fastest.
-struct alignas(64) PairModel {
-    VelMaps vm;
-    StrMaps sm;
+// (tile, z chunk) pairs of the single-cell 32 x 8 tiling, tile fastest.
+struct alignas(64) ZModel {
+    ZMaps zm;
     Model m;
     Physics ph;
     ZGeom g;
@@ -88,6 +87,17 @@ struct alignas(64) PairModel {
 // up (the model's own flag is set too), 2 a grid barrier wait gave up.
 constexpr int kBatchWaitTma = 1, kBatchWaitGrid = 2;
 
+// Persistent batch: CTAs that fit at once on the device (cooperative launch),
+// and nsteps steps of all models in one launch.  first_item[nmodels + 1]:
+// prefix sums of the models' items; ctl: 1 + 2 * nsteps zeroed counters
+// (grid-barrier arrivals, then one work counter per step and phase); each
+// grid barrier waits for barrier_ctas arrivals (the launched CTAs unless a
+// caller asks otherwise), at most about a second, then the launch stops with
+// *status = kBatchWaitGrid.  All models FAST or all REF (fast).
+int zmarch_batch_ctas(int device);
+cudaError_t zmarch_batch_run(const ZModel *models, int nmodels, const int *first_item, int it0, int nsteps,
+                             unsigned *ctl, int barrier_ctas, int ctas, bool fast, int *status, cudaStream_t s);
+
 // Paired tiling: tensor maps, tile counts and one step (velocity + stress).
 // hs: null for FP32 storage, else the 16-bit storage state (the step then
 // also launches the 16-bit source, receiver and rescale kernels).
@@ -96,15 +106,5 @@ void zpair_tiles(const Model &m, int *ntx, int *nty);
 cudaError_t zpair_step(const Model &m, const Physics &ph, const SourceRec &sr, const HalfState *hs, const ZGeom &g,
                        const VelMaps &vm, const StrMaps &sm, int it, float src_value, bool use_wavelet, cudaStream_t s,
                        cudaEvent_t *ev = nullptr);
-// Persistent batch: CTAs that fit at once on the device (cooperative launch),
-// and nsteps steps of all models in one launch.  first_item[nmodels + 1]:
-// prefix sums of the models' items; ctl: 1 + 2 * nsteps zeroed counters
-// (grid-barrier arrivals, then one work counter per step and phase); each
-// grid barrier waits for barrier_ctas arrivals (the launched CTAs unless a
-// caller asks otherwise), at most about a second, then the launch stops with
-// *status = kBatchWaitGrid.  All models FAST or all REF (fast).
-int zpair_batch_ctas(int device);
-cudaError_t zpair_batch_run(const PairModel *models, int nmodels, const int *first_item, int it0, int nsteps,
-                            unsigned *ctl, int barrier_ctas, int ctas, bool fast, int *status, cudaStream_t s);
 
 }  // namespace sgfd

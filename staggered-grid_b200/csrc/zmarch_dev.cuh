@@ -1,6 +1,7 @@
 // zmarch_dev.cuh — device helpers shared by the z-marching kernel families
 // (kernels_zmarch.cu, kernels_zpair.cu): mbarrier waits with an iteration
-// cap, TMA tiled loads (no multicast) and shared-memory alignment.
+// cap, TMA tiled loads (no multicast), shared-memory alignment and the
+// bounded grid barrier of the persistent batch kernel.
 #pragma once
 
 #include <cuda.h>
@@ -61,6 +62,50 @@ __device__ __forceinline__ void tma4(void *dst, const CUtensorMap *map, int x, i
 template <int S>
 __device__ void drain(uint64_t *bar, int issued_end, int from, int zs) {
     for (int j = from; j < issued_end; ++j) mbar_wait(&bar[(j - zs) % S], (uint32_t)(((j - zs) / S) & 1));
+}
+
+// The same for a ring whose barriers carry their phase parities in pbits
+// (bit s: the parity the next wait on stage s expects); planes [from,
+// issued_end) are pending, at most one per stage.
+template <int S>
+__device__ void drain_bits(uint64_t *bar, int issued_end, int from, int zs, uint32_t pbits) {
+    for (int j = from; j < issued_end; ++j) {
+        const int s = (j - zs) % S;
+        mbar_wait(&bar[s], (pbits >> s) & 1u);
+    }
+}
+
+constexpr uint32_t kGridWaitCap = 1u << 20;   // polls of about 1 us: a grid barrier gives up after ~1 s
+
+__device__ __forceinline__ unsigned ld_acquire(const unsigned *p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// All CTAs of a cooperative launch meet here: arrivals are counted in
+// *arrive, and the barrier completes when `target` arrivals have been
+// counted.  Bounded: false (and *status = fail_code) when the count does not
+// arrive.  The fences make the other CTAs' stores of the finished phase
+// visible to this CTA's later loads, TMA (async proxy) included.
+__device__ __forceinline__ bool grid_sync(unsigned *arrive, unsigned target, int *status, int fail_code,
+                                          int *ok_sh) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        atomicAdd(arrive, 1u);
+        bool ok = true;
+        for (uint32_t n = 0; ld_acquire(arrive) < target; ++n) {
+            if (n >= kGridWaitCap) { ok = false; break; }
+            __nanosleep(1000);
+        }
+        __threadfence();
+        asm volatile("fence.proxy.async.global;" ::: "memory");
+        if (!ok) atomicExch(status, fail_code);
+        *ok_sh = ok;
+    }
+    __syncthreads();
+    return *ok_sh != 0;
 }
 
 // 128-byte aligned start inside the dynamic shared array.  The offset is

@@ -65,7 +65,7 @@ def test_persistent_batch_equals_solo_runs(split):
             members.append(make_solver(w))
         with sgfd.Batch(members) as b:
             b.set_persistent(True)
-            assert all(m.tile()[:2] == (64, 8) for m in members)
+            assert all(m.tile()[:2] == (32, 8) for m in members)
             if split:
                 for it0, n in ((0, 20), (20, 1), (21, 24)):
                     b.run(it0, n)
