@@ -44,7 +44,7 @@ BYTES = {"velocity": (52, 112), "stress": (68, 164)}
 # dram__bytes_write.sum) on the 216^3 + 20 PML cube of the same kernels (REF); the
 # 394^3 workload is too large for a multi-metric capture, so its traffic is
 # reported as its algorithmic bytes times this ratio.
-TRAFFIC_RATIO = {"velocity": 1.19, "stress": 1.33}
+TRAFFIC_RATIO = {"velocity": 1.18, "stress": 1.32}
 TRAFFIC_SOURCE = ("ncu dram bytes / algorithmic bytes of the z-march kernels (REF rounding) on the 216^3 + 20 PML "
                   "cube, times this launch's algorithmic bytes")
 # 16-bit storage: fields and splits 2 B, medium 4 B (per step 66 B interior, 144 B PML).
@@ -59,8 +59,8 @@ def parse():
     p.add_argument("--steps", type=int, default=100)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", choices=["sgfd", "reference"], default="sgfd")
-    p.add_argument("--workload", choices=["random344", "random472", "random216", "plain100", "reference_main",
-                                               "batch32", "learned256", "combined32"],
+    p.add_argument("--workload", choices=["random344", "random472", "random216", "interior512", "interior256",
+                                               "plain100", "reference_main", "batch32", "learned256", "combined32"],
                    default="random344")
     p.add_argument("--no-autotune", action="store_true", help="batch32: keep the default launch shapes")
     p.add_argument("--batch-mode", choices=["persistent", "graph"], default="graph",
@@ -91,6 +91,11 @@ def build_workload(name):
                               src_computed=(256, 256, 40))
     if name == "random216":            # a smaller cube of the same kind, for ncu captures
         return wl.random_cube(n_interior=216, pml=20, nt=2000, src_computed=(128, 128, 40))
+    # no PML (zero frame): the interior-cell rate alone, 512^3 and, for ncu captures, 256^3 computed
+    if name == "interior512":
+        return wl.random_cube(n_interior=512, pml=0, nt=2000, src_computed=(256, 256, 40))
+    if name == "interior256":
+        return wl.random_cube(n_interior=256, pml=0, nt=2000, src_computed=(128, 128, 40))
     if name == "plain100":
         return wl.plain_cube(n_interior=100, pml=20, nt=500)
     return wl.reference_case(nt=1500)

@@ -304,12 +304,12 @@ int sgfd_batch_run(sgfd_batch *b, int32_t it0, int32_t nsteps);
 int sgfd_batch_synchronize(sgfd_batch *b);
 /* Persistent mode (on != 0): each sgfd_batch_run becomes ONE cooperative
  * launch that runs all its steps for all models.  The CTAs that fit on the
- * GPU at once take the models' (tile, z chunk) work items, 64 x 8 tiles, from
+ * GPU at once take the models' (tile, z chunk) work items, 32 x 8 tiles, from
  * a global counter, velocity phase and stress phase in turn, with a grid
  * barrier between phases.  Results are bit-identical to the models' own
  * runs.  Requires FP32 storage, z-marching kernels, no learned strip and no
  * per-step audit on every model, and one rounding mode for all.  The models
- * are switched to the 64 x 8 tiling.  Every wait is bounded: a grid barrier
+ * are switched to the 32 x 8 tiling.  Every wait is bounded: a grid barrier
  * that does not complete within about a second ends the launch, and
  * sgfd_batch_synchronize reports SGFD_ERR_CUDA.  barrier_ctas = 0 waits for
  * the CTAs launched; another value sets the number of arrivals each barrier
