@@ -234,10 +234,12 @@ int sgfd_autotune(sgfd_solver *h, int32_t probe_steps, sgfd_tuning *out) {
     struct Cand { int kernel, cols, rows, zchunk; };
     std::vector<Cand> cands;
     if (h->dev_err) {
-        for (int shape = h->storage == SGFD_STORE_F32 ? 0 : 2; shape < 3; ++shape)   // 16-bit: 64 x 8 only
+        for (int shape = 0; shape < 3; ++shape) {
+            if (shape == 1 && h->storage != SGFD_STORE_F32) continue;   // 16-bit: 32 x 8 and 64 x 8
             for (int zc : {0, 16, 32, 64})
                 if (zc == 0 || zc < h->m.nzc)
                     cands.push_back({SGFD_KERNEL_ZMARCH, shape == 2 ? kPairTileX : kZTileX, shape == 1 ? 16 : 8, zc});
+        }
     }
     cands.push_back({SGFD_KERNEL_SIMPLE, 0, 8, 0});
     cudaEvent_t e0, e1;

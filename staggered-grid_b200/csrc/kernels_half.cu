@@ -264,18 +264,35 @@ template <int ST>
 __global__ void k_rescale_apply(Model m, SourceRec sr, HalfState hs, int it_arg, int64_t n_grid) {
     if (!rescale_step(step_index(sr, it_arg))) return;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x, t0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    // every stored value h of p[0, n) becomes RN16(float(h) * f): eight at a
+    // time through 16-byte accesses, the unaligned head and the tail one by one
+    auto rescale = [&](uint16_t *p, int64_t n, float f) {
+        const int64_t head = ((16 - (int64_t)(reinterpret_cast<uintptr_t>(p) & 15)) & 15) / 2;
+        const int64_t h = head < n ? head : n;
+        const int64_t n8 = (n - h) / 8;
+        for (int64_t i = t0; i < h; i += stride) p[i] = f2h<ST>(h2f<ST>(p[i]) * f);
+        uint4 *q = reinterpret_cast<uint4 *>(p + h);
+        for (int64_t i = t0; i < n8; i += stride) {
+            uint4 v = q[i];
+            uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const uint32_t lo = f2h<ST>(h2f<ST>(w[j] & 0xffffu) * f);
+                const uint32_t hi = f2h<ST>(h2f<ST>(w[j] >> 16) * f);
+                w[j] = lo | (hi << 16);
+            }
+            q[i] = make_uint4(w[0], w[1], w[2], w[3]);
+        }
+        for (int64_t i = h + 8 * n8 + t0; i < n; i += stride) p[i] = f2h<ST>(h2f<ST>(p[i]) * f);
+    };
     for (int g = 0; g < 9; ++g) {
         if (hs.e_new[g] == hs.e[g]) continue;
-        const float f = ldexpf(1.0f, hs.e[g] - hs.e_new[g]);
-        uint16_t *p = hs.f[g] - kXOff;   // the whole padded array (padding stays zero)
-        for (int64_t i = t0; i < n_grid; i += stride) p[i] = f2h<ST>(h2f<ST>(p[i]) * f);
+        rescale(hs.f[g] - kXOff, n_grid, ldexpf(1.0f, hs.e[g] - hs.e_new[g]));   // the whole padded array
     }
     for (int k = 0; k < kNumSplit; ++k) {
         const int g = split_group(k);
         if (hs.e_new[g] == hs.e[g]) continue;
-        const float f = ldexpf(1.0f, hs.e[g] - hs.e_new[g]);
-        uint16_t *p = hs.split + (int64_t)k * m.npml;
-        for (int64_t i = t0; i < m.npml; i += stride) p[i] = f2h<ST>(h2f<ST>(p[i]) * f);
+        rescale(hs.split + (int64_t)k * m.npml, m.npml, ldexpf(1.0f, hs.e[g] - hs.e_new[g]));
     }
 }
 

@@ -42,6 +42,7 @@
 #include <type_traits>
 
 #include "cell_math.cuh"
+#include "store16.cuh"
 #include "zmarch.h"
 #include "zmarch_dev.cuh"
 
@@ -57,43 +58,46 @@ constexpr int W48 = 48, W32 = 32, W36 = 36;
 constexpr int al128(int b) { return (b + 127) / 128 * 128; }
 
 // Shared-memory stage layout of the velocity update (bytes, 128-aligned boxes).
-// Arrays that arrive in one 4-D copy are adjacent (sigma_xx, sigma_xz;
-// sigma_yy, sigma_yz; the two lead planes at z+4; vx, vy, vz).
-template <int TY>
+// Wavefield boxes hold ES-byte values (4: FP32, 2: 16-bit storage), the
+// buoyancy boxes FP32.  Arrays that arrive in one 4-D copy are adjacent
+// (sigma_xx, sigma_xz; sigma_yy, sigma_yz; the two lead planes at z+4; vx,
+// vy, vz).
+template <int TY, int ES = 4>
 struct VelL {
     static constexpr int SXX = 0;                                  // 48 x TY       sigma_xx (x halo)
-    static constexpr int SXZ = SXX + W48 * TY * 4;                 // 48 x TY       sigma_xz (x halo)
-    static constexpr int SYY = SXZ + al128(W48 * TY * 4);          // 32 x (TY+10)  sigma_yy (y halo)
-    static constexpr int SYZ = SYY + W32 * (TY + 10) * 4;          // 32 x (TY+10)  sigma_yz (y halo)
-    static constexpr int SXY = SYZ + al128(W32 * (TY + 10) * 4);   // 48 x (TY+10)  sigma_xy (x, y halo)
-    static constexpr int B = SXY + al128(W48 * (TY + 10) * 4);     // 36 x (TY+1)   buoyancy (x+1, y+1)
+    static constexpr int SXZ = SXX + W48 * TY * ES;                // 48 x TY       sigma_xz (x halo)
+    static constexpr int SYY = SXZ + al128(W48 * TY * ES);         // 32 x (TY+10)  sigma_yy (y halo)
+    static constexpr int SYZ = SYY + W32 * (TY + 10) * ES;         // 32 x (TY+10)  sigma_yz (y halo)
+    static constexpr int SXY = SYZ + al128(W32 * (TY + 10) * ES);  // 48 x (TY+10)  sigma_xy (x, y halo)
+    static constexpr int B = SXY + al128(W48 * (TY + 10) * ES);    // 36 x (TY+1)   buoyancy (x+1, y+1)
     static constexpr int LXZ = B + al128(W36 * (TY + 1) * 4);      // 32 x TY       sigma_xz at z+4
-    static constexpr int LYZ = LXZ + al128(W32 * TY * 4);          // 32 x TY       sigma_yz at z+4
-    static constexpr int LZZ = LYZ + al128(W32 * TY * 4);          // 32 x TY       sigma_zz at z+5
-    static constexpr int LB = LZZ + al128(W32 * TY * 4);           // 32 x TY       buoyancy at z+1
+    static constexpr int LYZ = LXZ + al128(W32 * TY * ES);         // 32 x TY       sigma_yz at z+4
+    static constexpr int LZZ = LYZ + al128(W32 * TY * ES);         // 32 x TY       sigma_zz at z+5
+    static constexpr int LB = LZZ + al128(W32 * TY * ES);          // 32 x TY       buoyancy at z+1
     static constexpr int OV = LB + al128(W32 * TY * 4);            // 3 x 32 x TY   own vx, vy, vz at z
-    static constexpr int STAGE = OV + 3 * al128(W32 * TY * 4);
-    static constexpr uint32_t TXB = 4 * (2 * W48 * TY + 2 * W32 * (TY + 10) + W48 * (TY + 10) +
-                                         W36 * (TY + 1) + 7 * W32 * TY);
-    static_assert(W48 * TY * 4 % 128 == 0 && W32 * (TY + 10) * 4 % 128 == 0 && W32 * TY * 4 % 128 == 0,
+    static constexpr int STAGE = OV + 3 * al128(W32 * TY * ES);
+    static constexpr uint32_t TXB = ES * (2 * W48 * TY + 2 * W32 * (TY + 10) + W48 * (TY + 10) + 6 * W32 * TY) +
+                                    4 * (W36 * (TY + 1) + W32 * TY);
+    static_assert(W48 * TY * ES % 128 == 0 && W32 * (TY + 10) * ES % 128 == 0 && W32 * TY * ES % 128 == 0,
                   "arrays of one copy must be contiguous and 128-byte aligned");
 };
-// Shared-memory stage layout of the stress update.
-template <int TY>
+// Shared-memory stage layout of the stress update (ES as above; the medium
+// boxes FP32).
+template <int TY, int ES = 4>
 struct StrL {
     static constexpr int VX = 0;                                   // 48 x (TY+10)  vx (x, y halo)
-    static constexpr int VY = VX + al128(W48 * (TY + 10) * 4);     // 48 x (TY+10)  vy
-    static constexpr int VZ = VY + al128(W48 * (TY + 10) * 4);     // 48 x (TY+10)  vz
-    static constexpr int LX = VZ + al128(W48 * (TY + 10) * 4);     // 32 x TY       vx at z+5
-    static constexpr int LY = LX + al128(W32 * TY * 4);            // 32 x TY       vy at z+5
-    static constexpr int LZ = LY + al128(W32 * TY * 4);            // 32 x TY       vz at z+4
-    // own-cell data at z, 32 x TY each: txx tyy tzz txy txz tyz, lambda, mu,
-    // the shear moduli of txy, txz, tyz
-    static constexpr int OWN = LZ + al128(W32 * TY * 4);
-    static constexpr int NOWN = 11;
-    static constexpr int STAGE = OWN + NOWN * al128(W32 * TY * 4);
-    static constexpr uint32_t TXB = 4 * (3 * W48 * (TY + 10) + (3 + NOWN) * W32 * TY);
-    static_assert(W48 * (TY + 10) * 4 % 128 == 0 && W32 * TY * 4 % 128 == 0,
+    static constexpr int VY = VX + W48 * (TY + 10) * ES;           // 48 x (TY+10)  vy
+    static constexpr int VZ = VY + W48 * (TY + 10) * ES;           // 48 x (TY+10)  vz
+    static constexpr int LX = al128(VZ + W48 * (TY + 10) * ES);    // 32 x TY       vx at z+5
+    static constexpr int LY = LX + W32 * TY * ES;                  // 32 x TY       vy at z+5
+    static constexpr int LZ = LY + al128(W32 * TY * ES);           // 32 x TY       vz at z+4
+    // own-cell data at z, 32 x TY each: txx tyy tzz txy txz tyz, then the
+    // medium: lambda, mu, the shear moduli of txy, txz, tyz
+    static constexpr int OWN = LZ + al128(W32 * TY * ES);
+    static constexpr int MED = OWN + 6 * W32 * TY * ES;
+    static constexpr int STAGE = MED + 5 * W32 * TY * 4;
+    static constexpr uint32_t TXB = ES * (3 * W48 * (TY + 10) + 9 * W32 * TY) + 4 * 5 * W32 * TY;
+    static_assert(W32 * TY * ES % 128 == 0 && (ES == 2 || W48 * (TY + 10) * ES % 128 == 0),
                   "arrays of one copy must be contiguous and 128-byte aligned");
 };
 
@@ -141,12 +145,28 @@ __device__ __forceinline__ void issue_boxes(const TmaBox *b, int n, unsigned cha
     for (int j = 0; j < n; ++j) tma4(st + b[j].off, b[j].map, b[j].x, b[j].y, gz + b[j].dz, 0, bar);
 }
 constexpr int kVelBoxes = 8;
-constexpr int kStrBoxes = 4;
+constexpr int kStrBoxes = 4;      // FP32: the 11 own-cell arrays in one copy
+constexpr int kStrBoxes16 = 5;    // 16-bit storage: the 6 stresses and the FP32 medium separately
 
-// Box q of the velocity stage.
-template <int TY>
+// 16-bit storage: n stored values of field box `src` (stage) as FP32 values
+// float(h) * sc in `dst` (the work buffer, laid out as an FP32 stage) — the
+// read-back of every tap, done once per staged value.
+template <int ST, int N>
+__device__ __forceinline__ void widen(const unsigned char *src, unsigned char *dst, float sc) {
+    static_assert(N % 2 == 0, "pairs of values");
+    const uint32_t *s2 = reinterpret_cast<const uint32_t *>(src);
+    float2 *d2 = reinterpret_cast<float2 *>(dst);
+#pragma unroll
+    for (int i = threadIdx.x; i < N / 2; i += NT) {
+        const uint32_t u = s2[i];
+        d2[i] = make_float2(H16<ST>::h2f(u & 0xffffu) * sc, H16<ST>::h2f(u >> 16) * sc);
+    }
+}
+
+// Box q of the velocity stage (ES: bytes per stored wavefield value).
+template <int TY, int ES>
 __device__ __forceinline__ TmaBox vel_box(const ZMaps &mp, const Tile &t, int q) {
-    using L = VelL<TY>;
+    using L = VelL<TY, ES>;
     switch (q) {
     case 0: return {&mp.v_sxx_sxz, L::SXX, t.xd - 8, t.gy0, 0};
     case 1: return {&mp.v_syy_syz, L::SYY, t.xd, t.gy0 - 5, 0};
@@ -164,9 +184,9 @@ __device__ __forceinline__ TmaBox vel_box(const ZMaps &mp, const Tile &t, int q)
 // warp).  Thread 0 also arms the stage's barrier with all of the stage's
 // bytes; the barrier's phase cannot complete before that arrival, whichever
 // copy lands first.
-template <int TY>
+template <int TY, int ES>
 __device__ __forceinline__ void vel_issue(const TmaBox *b, int n, unsigned char *st, uint64_t *bar, int cz, int warp) {
-    if (warp == 0) mbar_expect_tx(bar, VelL<TY>::TXB);
+    if (warp == 0) mbar_expect_tx(bar, VelL<TY, ES>::TXB);
     issue_boxes(b, n, st, bar, cz + kHalo);
 }
 
@@ -177,23 +197,53 @@ __device__ __forceinline__ void vel_issue(const TmaBox *b, int n, unsigned char 
 // Returns false after a bounded wait gave up (g.err set, copies drained).
 // MANY: the CTA runs several items (persistent batch); a single-item launch
 // keeps one parity for the whole ring and skips the fences a previous item needs.
-template <bool FAST, int CELLS, bool MANY>
+// ST: wavefield storage.  16-bit storage (32 x 8 tiles): the copies bring
+// 16-bit field boxes, which each plane widens once into an FP32 work buffer
+// after the ring (float(h) * 2^e, the read-back of kernels_half.cu and the
+// oracle) for the unchanged FP32 arithmetic; stores round to 16 bits; the
+// source and the receivers run as the 16-bit family's own kernels.
+template <bool FAST, int CELLS, bool MANY, int ST = SGFD_STORE_F32>
 __device__ __forceinline__ bool vel_item(const ZMaps &mp, const Model &m, const Physics &ph, const ZGeom &g,
                                          const SourceRec &sr, int it_arg, float src_value, int use_wavelet, int tile,
                                          int chunk, unsigned char *smem, uint64_t *bar,
-                                         TmaBox (*boxes)[kMaxBoxesPerWarp], uint32_t &pbits) {
+                                         TmaBox (*boxes)[kMaxBoxesPerWarp], uint32_t &pbits,
+                                         const HalfState &hs = HalfState{}) {
     constexpr int TY = 8 * CELLS;
-    using L = VelL<TY>;
+    constexpr bool H = ST != SGFD_STORE_F32;
+    static_assert(!H || CELLS == 1, "16-bit storage runs on 32 x 8 tiles");
+    constexpr int ES = H ? 2 : 4;
+    using L = VelL<TY>;          // FP32 layout: the stage itself, or the 16-bit storage's work buffer
+    using LS = VelL<TY, ES>;     // the stage as the copies fill it
+    __shared__ float scl[18];    // 16-bit storage: this step's scales 2^e, then 2^-e
+    __shared__ unsigned smax[9]; // 16-bit storage, rescale steps: this CTA's largest written magnitudes
+    if constexpr (H) {
+        if (threadIdx.x < 9) {
+            scl[threadIdx.x] = hs.sc[threadIdx.x];
+            scl[9 + threadIdx.x] = hs.inv[threadIdx.x];
+            smax[threadIdx.x] = 0u;
+        }
+        __syncthreads();
+    }
+    unsigned char *work = smem + S * LS::STAGE;   // 16-bit storage only
+    // stored value k of field (or split group) g, read back as FP32
+    auto ld = [&](auto *p, int g) -> float {
+        if constexpr (H) return H16<ST>::h2f(*p) * scl[g];
+        else return *p;
+    };
+    auto put = [&](auto *p, int g, float v) {
+        if constexpr (H) *p = (uint16_t)H16<ST>::f2h(v * scl[9 + g]);
+        else *p = v;
+    };
     const Tile t = make_tile<TY>(m, g, tile, chunk);
     const int tid = threadIdx.x, lx = tid & 31, ty = tid >> 5;
     const int warp = tid >> 5;
     const TmaBox *mybox = boxes[warp];
     const int nbox = (kVelBoxes - warp + kWarps - 1) / kWarps;
     if (lx == 0) {
-        for (int j = 0; j < nbox; ++j) boxes[warp][j] = vel_box<TY>(mp, t, warp + j * kWarps);
+        for (int j = 0; j < nbox; ++j) boxes[warp][j] = vel_box<TY, ES>(mp, t, warp + j * kWarps);
         if (MANY) fence_proxy_async();   // a previous item's stages were read through the generic proxy
         for (int s = 0; s < S && t.zs + s < t.ze; ++s)
-            vel_issue<TY>(mybox, nbox, smem + s * L::STAGE, &bar[s], t.zs + s, warp);
+            vel_issue<TY, ES>(mybox, nbox, smem + s * LS::STAGE, &bar[s], t.zs + s, warp);
     }
     int issued_end = min(t.zs + S, t.ze);   // planes [zs, issued_end) issued
     int stage = 0;                          // stage of plane cz
@@ -201,13 +251,22 @@ __device__ __forceinline__ bool vel_item(const ZMaps &mp, const Model &m, const 
 
     const int it = step_index(sr, it_arg);
     const float inj = ph.inj_dt2 * ((use_wavelet && sr.wavelet) ? sr.wavelet[it] : src_value);
+    [[maybe_unused]] const bool track = H && rescale_step16(it);   // 16-bit: note the written maxima
     int sx = -1, sy = -1, sz = -1;
-    if (sr.src >= 0) {
+    if (!H && sr.src >= 0) {
         const int64_t r = sr.src;
         sz = (int)(r / m.plane);
         sy = (int)((r - (int64_t)sz * m.plane) / m.px);
         sx = (int)(r - (int64_t)sz * m.plane - (int64_t)sy * m.px);
     }
+    [[maybe_unused]] auto fld = [&](int k) {
+        if constexpr (H) return hs.f[k];
+        else return m.f[k];
+    };
+    [[maybe_unused]] auto spl = [&]() {
+        if constexpr (H) return hs.split;
+        else return m.split;
+    };
 
     const int gx = t.gx0 + lx;
     const int kx = band(gx, m.nx, m.pml);
@@ -234,23 +293,23 @@ __device__ __forceinline__ bool vel_item(const ZMaps &mp, const Model &m, const 
     for (int c = 0; c < CELLS; ++c) {
 #pragma unroll
         for (int k = 0; k < 9; ++k) {
-            qxz[c][k + 1] = m.f[7][col[c] + (uint32_t)(gz0 - 5 + k) * PL];
-            qyz[c][k + 1] = m.f[8][col[c] + (uint32_t)(gz0 - 5 + k) * PL];
-            float zz = m.f[5][col[c] + (uint32_t)(gz0 - 4 + k) * PL];
+            qxz[c][k + 1] = ld(fld(7) + col[c] + (uint32_t)(gz0 - 5 + k) * PL, 7);
+            qyz[c][k + 1] = ld(fld(8) + col[c] + (uint32_t)(gz0 - 5 + k) * PL, 8);
+            float zz = ld(fld(5) + col[c] + (uint32_t)(gz0 - 4 + k) * PL, 5);
             if (gx == sx && gyc[c] == sy && gz0 - 4 + k == sz) zz = zz + inj;
             qzz[c][k + 1] = zz;
         }
     }
 
     // receivers of this tile, sorted by z: skip those below the chunk
-    int rp = g.rec_off[tile];
-    const int rend = g.rec_off[tile + 1];
+    int rp = H ? 0 : g.rec_off[tile];
+    const int rend = H ? 0 : g.rec_off[tile + 1];
     while (rp < rend && g.rec_list[rp].z < gz0) ++rp;
     int rz = rp < rend ? g.rec_list[rp].z : 0x7fffffff;   // z of the next receiver
 
     bool failed = false, abort = false;
     int cz = t.zs;
-    const bool src_near = sr.src >= 0 && sy >= t.gy0 - 5 && sy < t.gy0 + TY + 5 && sx >= t.gx0 - 8 &&
+    const bool src_near = !H && sr.src >= 0 && sy >= t.gy0 - 5 && sy < t.gy0 + TY + 5 && sx >= t.gx0 - 8 &&
                           sx < t.gx0 + TX + 8;
     // One plane.  GEN selects the general path (PML cells, source, receivers);
     // the interior-only path is used for every other tile-plane.  Returns
@@ -258,7 +317,7 @@ __device__ __forceinline__ bool vel_item(const ZMaps &mp, const Model &m, const 
     auto plane = [&](auto gen_tag) -> bool {
         constexpr bool GEN = decltype(gen_tag)::value;
         const int s = stage;
-        unsigned char *st = smem + s * L::STAGE;
+        unsigned char *st = smem + s * LS::STAGE;
         const int gz = cz + kHalo;
         const int kz = band(gz, m.nz, m.pml);
         const bool plane_pml = GEN && (t.xy_pml || kz != 0);
@@ -273,9 +332,9 @@ __device__ __forceinline__ bool vel_item(const ZMaps &mp, const Model &m, const 
             for (int c = 0; c < CELLS; ++c) {
                 if (act[c] && (kx | kyc[c] | kz)) {
                     const uint32_t ci = col[c] + (uint32_t)gz * PL;
-                    const float *sp = m.split + pml_plane_index(m, pcol[c], cz);
+                    const auto *sp = spl() + pml_plane_index(m, pcol[c], cz);
 #pragma unroll
-                    for (int q = 0; q < 9; ++q) opre[c][q] = sp[q * N];
+                    for (int q = 0; q < 9; ++q) opre[c][q] = ld(sp + q * N, q / 3);   // split q: field q / 3
                     mupre[c] = m.mu[ci];
                     lampre[c] = ph.damping == 1 ? m.lam[ci] : 0.f;
                 }
@@ -283,6 +342,24 @@ __device__ __forceinline__ bool vel_item(const ZMaps &mp, const Model &m, const 
         }
 
         if (!mbar_wait(&bar[s], MANY ? (pbits >> s) & 1u : parity)) failed = true;
+        // the FP32 view of the stage's wavefield boxes
+        const unsigned char *wk = st;
+        if constexpr (H) {
+            widen<ST, W48 * TY>(st + LS::SXX, work + L::SXX, scl[3]);
+            widen<ST, W48 * TY>(st + LS::SXZ, work + L::SXZ, scl[7]);
+            widen<ST, W32 * (TY + 10)>(st + LS::SYY, work + L::SYY, scl[4]);
+            widen<ST, W32 * (TY + 10)>(st + LS::SYZ, work + L::SYZ, scl[8]);
+            widen<ST, W48 * (TY + 10)>(st + LS::SXY, work + L::SXY, scl[6]);
+            widen<ST, W32 * TY>(st + LS::LXZ, work + L::LXZ, scl[7]);
+            widen<ST, W32 * TY>(st + LS::LYZ, work + L::LYZ, scl[8]);
+            widen<ST, W32 * TY>(st + LS::LZZ, work + L::LZZ, scl[5]);
+#pragma unroll
+            for (int q = 0; q < 3; ++q)
+                widen<ST, W32 * TY>(st + LS::OV + q * al128(W32 * TY * ES), work + L::OV + q * al128(W32 * TY * 4),
+                                    scl[q]);
+            __syncthreads();
+            wk = work;
+        }
 
         // source patch of the staged copies (uniform branch)
         if (GEN && src_near && (gz == sz || gz + 5 == sz)) {
@@ -302,17 +379,17 @@ __device__ __forceinline__ bool vel_item(const ZMaps &mp, const Model &m, const 
             __syncthreads();
         }
 
-        const float *sxx = reinterpret_cast<const float *>(st + L::SXX);
-        const float *syy = reinterpret_cast<const float *>(st + L::SYY);
-        const float *sxy = reinterpret_cast<const float *>(st + L::SXY);
-        const float *sxz = reinterpret_cast<const float *>(st + L::SXZ);
-        const float *syz = reinterpret_cast<const float *>(st + L::SYZ);
-        const float *bb = reinterpret_cast<const float *>(st + L::B);
-        const float *lxz = reinterpret_cast<const float *>(st + L::LXZ);
-        const float *lyz = reinterpret_cast<const float *>(st + L::LYZ);
-        const float *lzz = reinterpret_cast<const float *>(st + L::LZZ);
-        const float *lb = reinterpret_cast<const float *>(st + L::LB);
-        const float *ov = reinterpret_cast<const float *>(st + L::OV);
+        const float *sxx = reinterpret_cast<const float *>(wk + L::SXX);
+        const float *syy = reinterpret_cast<const float *>(wk + L::SYY);
+        const float *sxy = reinterpret_cast<const float *>(wk + L::SXY);
+        const float *sxz = reinterpret_cast<const float *>(wk + L::SXZ);
+        const float *syz = reinterpret_cast<const float *>(wk + L::SYZ);
+        const float *bb = reinterpret_cast<const float *>(st + LS::B);
+        const float *lxz = reinterpret_cast<const float *>(wk + L::LXZ);
+        const float *lyz = reinterpret_cast<const float *>(wk + L::LYZ);
+        const float *lzz = reinterpret_cast<const float *>(wk + L::LZZ);
+        const float *lb = reinterpret_cast<const float *>(st + LS::LB);
+        const float *ov = reinterpret_cast<const float *>(wk + L::OV);
         constexpr int OVS = al128(W32 * TY * 4) / 4;   // floats between the own-velocity boxes
 
         // y differences of vertically adjacent cells share their windows
@@ -399,31 +476,45 @@ __device__ __forceinline__ bool vel_item(const ZMaps &mp, const Model &m, const 
                 }
                 const bool ref = ph.quirks == 0;
                 const float ax = ph.dt * bx, ay = ph.dt * (ref ? bx : by), az = ph.dt * (ref ? bx : bz);
-                float *sp = m.split + pml_plane_index(m, pcol[c], cz);
+                auto *sp = spl() + pml_plane_index(m, pcol[c], cz);
                 const uint32_t N = (uint32_t)m.npml;
                 const float *o = opre[c];
+                // split k belongs to field k / 3 (its scale with 16-bit storage)
+                auto sput = [&](int k, float v) {
+                    if constexpr (H) {
+                        if (track) note_max16s(smax, k / 3, v);
+                    }
+                    put(sp + k * N, k / 3, v);
+                };
                 float a0, a1, a2;
                 a0 = split_update<FAST>(o[S_VXX], ax, xX, kx, mx, px);
                 a1 = split_update<FAST>(o[S_VXY], ax, xY, ky, my, py);
                 a2 = split_update<FAST>(o[S_VXZ], ax, xZ, kz, mz, pz);
-                sp[S_VXX * N] = a0; sp[S_VXY * N] = a1; sp[S_VXZ * N] = a2;
+                sput(S_VXX, a0); sput(S_VXY, a1); sput(S_VXZ, a2);
                 vnew[0] = (a0 + a1) + a2;
                 a0 = split_update<FAST>(o[S_VYX], ay, yX, kx, mx, px);
                 a1 = split_update<FAST>(o[S_VYY], ay, yY, ky, my, py);
                 a2 = split_update<FAST>(o[S_VYZ], ay, yZ, kz, mz, pz);
-                sp[S_VYX * N] = a0; sp[S_VYY * N] = a1; sp[S_VYZ * N] = a2;
+                sput(S_VYX, a0); sput(S_VYY, a1); sput(S_VYZ, a2);
                 vnew[1] = (a0 + a1) + a2;
                 a0 = split_update<FAST>(o[S_VZX], az, zX, kx, mx, px);
                 a1 = split_update<FAST>(o[S_VZY], az, zY, ky, my, py);
                 a2 = split_update<FAST>(o[S_VZZ], az, zZ, kz, mz, pz);
-                sp[S_VZX * N] = a0; sp[S_VZY * N] = a1; sp[S_VZZ * N] = a2;
+                sput(S_VZX, a0); sput(S_VZY, a1); sput(S_VZZ, a2);
                 vnew[2] = (a0 + a1) + a2;
             }
-            m.f[0][ci] = vnew[0];
-            m.f[1][ci] = vnew[1];
-            m.f[2][ci] = vnew[2];
+            if constexpr (H) {
+                if (track) {
+                    note_max16s(smax, 0, vnew[0]);
+                    note_max16s(smax, 1, vnew[1]);
+                    note_max16s(smax, 2, vnew[2]);
+                }
+            }
+            put(fld(0) + ci, 0, vnew[0]);
+            put(fld(1) + ci, 1, vnew[1]);
+            put(fld(2) + ci, 2, vnew[2]);
             // receivers of velocity components at this cell (list sorted by z)
-            if (GEN && gz == rz && it >= 0 && it < sr.nt) {
+            if (GEN && !H && gz == rz && it >= 0 && it < sr.nt) {
                 for (int r = rp; r < rend && g.rec_list[r].z == gz; ++r) {
                     const int4 q = g.rec_list[r];
                     if (q.x == gx && q.y == gyc[c] && q.w <= 2)
@@ -442,7 +533,7 @@ __device__ __forceinline__ bool vel_item(const ZMaps &mp, const Model &m, const 
         if (cz + S < t.ze) {
             if (lx == 0) {
                 fence_proxy_async();
-                vel_issue<TY>(mybox, nbox, st, &bar[s], cz + S, warp);
+                vel_issue<TY, ES>(mybox, nbox, st, &bar[s], cz + S, warp);
             }
             issued_end = cz + S + 1;
         }
@@ -465,6 +556,12 @@ __device__ __forceinline__ bool vel_item(const ZMaps &mp, const Model &m, const 
         atomicExch(g.err, 1);
         if (MANY) drain_bits<S>(bar, issued_end, cz, t.zs, pbits);
         else drain<S>(bar, issued_end, cz, t.zs);
+    }
+    if constexpr (H) {
+        if (track) {
+            __syncthreads();
+            flush_max16(hs, smax);
+        }
     }
     return !abort;
 }
@@ -491,43 +588,78 @@ k_velocity_zmarch(const __grid_constant__ ZMaps mp, const __grid_constant__ Mode
 // stress update
 // ---------------------------------------------------------------------------
 
-// Box q of the stress stage.
-template <int TY>
+// Box q of the stress stage (ES as vel_box; FP32: the 11 own-cell arrays
+// in one copy, 16-bit: the 6 stored stresses, then the FP32 medium).
+template <int TY, int ES>
 __device__ __forceinline__ TmaBox str_box(const ZMaps &mp, const Tile &t, int q) {
-    using L = StrL<TY>;
+    using L = StrL<TY, ES>;
     switch (q) {
     case 0: return {&mp.s_v, L::VX, t.xd - 8, t.gy0 - 5, 0};
     case 1: return {&mp.s_lead_xy, L::LX, t.xd, t.gy0, 5};
     case 2: return {&mp.s_lead_z, L::LZ, t.xd, t.gy0, 4};
-    default: return {&mp.s_own, L::OWN, t.xd, t.gy0, 0};
+    case 3: return {&mp.s_own, L::OWN, t.xd, t.gy0, 0};
+    default: return {&mp.s_med, L::MED, t.xd, t.gy0, 0};
     }
 }
 
 // Stage the stress inputs of computed plane cz, as vel_issue.
-template <int TY>
+template <int TY, int ES>
 __device__ __forceinline__ void str_issue(const TmaBox *b, int n, unsigned char *st, uint64_t *bar, int cz, int warp) {
-    if (warp == 0) mbar_expect_tx(bar, StrL<TY>::TXB);
+    if (warp == 0) mbar_expect_tx(bar, StrL<TY, ES>::TXB);
     issue_boxes(b, n, st, bar, cz + kHalo);
 }
 
-// The stress update of one work item, as vel_item.
-template <bool FAST, int CELLS, bool MANY>
+// The stress update of one work item, as vel_item (ST: storage, as there).
+template <bool FAST, int CELLS, bool MANY, int ST = SGFD_STORE_F32>
 __device__ __forceinline__ bool str_item(const ZMaps &mp, const Model &m, const Physics &ph, const ZGeom &g,
                                          const SourceRec &sr, int it_arg, float src_value, int use_wavelet, int tile,
                                          int chunk, unsigned char *smem, uint64_t *bar,
-                                         TmaBox (*boxes)[kMaxBoxesPerWarp], uint32_t &pbits) {
+                                         TmaBox (*boxes)[kMaxBoxesPerWarp], uint32_t &pbits,
+                                         const HalfState &hs = HalfState{}) {
     constexpr int TY = 8 * CELLS;
-    using L = StrL<TY>;
+    constexpr bool H = ST != SGFD_STORE_F32;
+    static_assert(!H || CELLS == 1, "16-bit storage runs on 32 x 8 tiles");
+    constexpr int ES = H ? 2 : 4;
+    using L = StrL<TY>;          // FP32 layout: the stage itself, or the 16-bit storage's work buffer
+    using LS = StrL<TY, ES>;     // the stage as the copies fill it
+    __shared__ float scl[18];    // 16-bit storage: this step's scales 2^e, then 2^-e
+    __shared__ unsigned smax[9]; // 16-bit storage, rescale steps: this CTA's largest written magnitudes
+    if constexpr (H) {
+        if (threadIdx.x < 9) {
+            scl[threadIdx.x] = hs.sc[threadIdx.x];
+            scl[9 + threadIdx.x] = hs.inv[threadIdx.x];
+            smax[threadIdx.x] = 0u;
+        }
+        __syncthreads();
+    }
+    unsigned char *work = smem + S * LS::STAGE;   // 16-bit storage only
+    auto ld = [&](auto *p, int g) -> float {
+        if constexpr (H) return H16<ST>::h2f(*p) * scl[g];
+        else return *p;
+    };
+    auto put = [&](auto *p, int g, float v) {
+        if constexpr (H) *p = (uint16_t)H16<ST>::f2h(v * scl[9 + g]);
+        else *p = v;
+    };
+    [[maybe_unused]] auto fld = [&](int k) {
+        if constexpr (H) return hs.f[k];
+        else return m.f[k];
+    };
+    [[maybe_unused]] auto spl = [&]() {
+        if constexpr (H) return hs.split;
+        else return m.split;
+    };
     const Tile t = make_tile<TY>(m, g, tile, chunk);
     const int tid = threadIdx.x, lx = tid & 31, ty = tid >> 5;
     const int warp = tid >> 5;
     const TmaBox *mybox = boxes[warp];
-    const int nbox = (kStrBoxes - warp + kWarps - 1) / kWarps;
+    constexpr int NB = H ? kStrBoxes16 : kStrBoxes;
+    const int nbox = (NB - warp + kWarps - 1) / kWarps;
     if (lx == 0) {
-        for (int j = 0; j < nbox; ++j) boxes[warp][j] = str_box<TY>(mp, t, warp + j * kWarps);
+        for (int j = 0; j < nbox; ++j) boxes[warp][j] = str_box<TY, ES>(mp, t, warp + j * kWarps);
         if (MANY) fence_proxy_async();   // a previous item's stages were read through the generic proxy
         for (int s = 0; s < S && t.zs + s < t.ze; ++s)
-            str_issue<TY>(mybox, nbox, smem + s * L::STAGE, &bar[s], t.zs + s, warp);
+            str_issue<TY, ES>(mybox, nbox, smem + s * LS::STAGE, &bar[s], t.zs + s, warp);
     }
     int issued_end = min(t.zs + S, t.ze);   // planes [zs, issued_end) issued
     int stage = 0;                          // stage of plane cz
@@ -535,7 +667,8 @@ __device__ __forceinline__ bool str_item(const ZMaps &mp, const Model &m, const 
 
     const int it = step_index(sr, it_arg);
     const float inj = ph.inj_dt2 * ((use_wavelet && sr.wavelet) ? sr.wavelet[it] : src_value);
-    const int64_t src = sr.src;
+    [[maybe_unused]] const bool track = H && rescale_step16(it);   // 16-bit: note the written maxima
+    const int64_t src = H ? -1 : sr.src;
 
     const int gx = t.gx0 + lx;
     const int kx = band(gx, m.nx, m.pml);
@@ -564,14 +697,14 @@ __device__ __forceinline__ bool str_item(const ZMaps &mp, const Model &m, const 
     for (int c = 0; c < CELLS; ++c) {
 #pragma unroll
         for (int k = 0; k < 9; ++k) {
-            qx[c][k] = m.f[0][col[c] + (uint32_t)(gz0 - 4 + k) * PL];
-            qy[c][k] = m.f[1][col[c] + (uint32_t)(gz0 - 4 + k) * PL];
-            qz[c][k] = m.f[2][col[c] + (uint32_t)(gz0 - 5 + k) * PL];
+            qx[c][k] = ld(fld(0) + col[c] + (uint32_t)(gz0 - 4 + k) * PL, 0);
+            qy[c][k] = ld(fld(1) + col[c] + (uint32_t)(gz0 - 4 + k) * PL, 1);
+            qz[c][k] = ld(fld(2) + col[c] + (uint32_t)(gz0 - 5 + k) * PL, 2);
         }
     }
 
-    int rp = g.rec_off[tile];
-    const int rend = g.rec_off[tile + 1];
+    int rp = H ? 0 : g.rec_off[tile];
+    const int rend = H ? 0 : g.rec_off[tile + 1];
     while (rp < rend && g.rec_list[rp].z < gz0) ++rp;
     int rz = rp < rend ? g.rec_list[rp].z : 0x7fffffff;
 
@@ -585,21 +718,37 @@ __device__ __forceinline__ bool str_item(const ZMaps &mp, const Model &m, const 
         constexpr bool GEN = decltype(gen_tag)::value;
         constexpr int P = decltype(p_tag)::value;
         const int s = stage;
-        unsigned char *st = smem + s * L::STAGE;
+        unsigned char *st = smem + s * LS::STAGE;
         const int gz = cz + kHalo;
         const int kz = band(gz, m.nz, m.pml);
         const bool plane_pml = GEN && (t.xy_pml || kz != 0);
 
         if (!mbar_wait(&bar[s], MANY ? (pbits >> s) & 1u : parity)) failed = true;
+        // the FP32 view of the stage's wavefield boxes
+        const unsigned char *wk = st;
+        if constexpr (H) {
+            widen<ST, W48 * (TY + 10)>(st + LS::VX, work + L::VX, scl[0]);
+            widen<ST, W48 * (TY + 10)>(st + LS::VY, work + L::VY, scl[1]);
+            widen<ST, W48 * (TY + 10)>(st + LS::VZ, work + L::VZ, scl[2]);
+            widen<ST, W32 * TY>(st + LS::LX, work + L::LX, scl[0]);
+            widen<ST, W32 * TY>(st + LS::LY, work + L::LY, scl[1]);
+            widen<ST, W32 * TY>(st + LS::LZ, work + L::LZ, scl[2]);
+#pragma unroll
+            for (int q = 0; q < 6; ++q)
+                widen<ST, W32 * TY>(st + LS::OWN + q * W32 * TY * ES, work + L::OWN + q * W32 * TY * 4, scl[3 + q]);
+            __syncthreads();
+            wk = work;
+        }
 
-        const float *svx = reinterpret_cast<const float *>(st + L::VX);
-        const float *svy = reinterpret_cast<const float *>(st + L::VY);
-        const float *svz = reinterpret_cast<const float *>(st + L::VZ);
-        const float *llx = reinterpret_cast<const float *>(st + L::LX);
-        const float *lly = reinterpret_cast<const float *>(st + L::LY);
-        const float *llz = reinterpret_cast<const float *>(st + L::LZ);
-        // own-cell boxes: txx..tyz at q = 0..5, lambda 6, mu 7, shear moduli 8..10
-        const float *own = reinterpret_cast<const float *>(st + L::OWN);
+        const float *svx = reinterpret_cast<const float *>(wk + L::VX);
+        const float *svy = reinterpret_cast<const float *>(wk + L::VY);
+        const float *svz = reinterpret_cast<const float *>(wk + L::VZ);
+        const float *llx = reinterpret_cast<const float *>(wk + L::LX);
+        const float *lly = reinterpret_cast<const float *>(wk + L::LY);
+        const float *llz = reinterpret_cast<const float *>(wk + L::LZ);
+        // own-cell boxes: txx..tyz at q = 0..5; the medium: lambda, mu, shear moduli 0..4
+        const float *own = reinterpret_cast<const float *>(wk + L::OWN);
+        const float *med = reinterpret_cast<const float *>(st + LS::MED);
         constexpr int OS = al128(W32 * TY * 4) / 4;
 
         [[maybe_unused]] float dYy2[2] = {0.f, 0.f}, xyY2[2] = {0.f, 0.f}, yzY2[2] = {0.f, 0.f};
@@ -655,9 +804,9 @@ __device__ __forceinline__ bool str_item(const ZMaps &mp, const Model &m, const 
             dZz = dB<FAST, 2>(ph, [&](int o) { return qz[c][P + 5 + o]; });
 
             const int e = ly * W32 + lx;
-            const float l = own[6 * OS + e], mu_c = own[7 * OS + e];
+            const float l = med[e], mu_c = med[OS + e];
             const float l2m = __fmaf_rn(2.0f, mu_c, l);
-            const float mxy = own[8 * OS + e], mxz = own[9 * OS + e], myz = own[10 * OS + e];
+            const float mxy = med[2 * OS + e], mxz = med[3 * OS + e], myz = med[4 * OS + e];
 
             const uint32_t ci = col[c] + (uint32_t)gz * PL;
             const int ky = kyc[c];
@@ -672,11 +821,19 @@ __device__ __forceinline__ bool str_item(const ZMaps &mp, const Model &m, const 
                 snew[4] = __fmaf_rn(ph.dt * mxz, xzZ + xzX, own[4 * OS + e]);
                 snew[5] = __fmaf_rn(ph.dt * myz, yzZ + yzY, own[5 * OS + e]);
             } else {
-                float *sp = m.split + pml_plane_index(m, pcol[c], cz);
+                auto *sp = spl() + pml_plane_index(m, pcol[c], cz);
                 const uint32_t N = (uint32_t)m.npml;
+                // split S_XXX + k belongs to field txx..tyz (its scale with 16-bit storage)
+                auto grp = [](int k) { return k < 9 ? 3 + k / 3 : 6 + (k - 9) / 2; };
+                auto sput = [&](int k, float v) {
+                    if constexpr (H) {
+                        if (track) note_max16s(smax, grp(k - S_XXX), v);
+                    }
+                    put(sp + k * N, grp(k - S_XXX), v);
+                };
                 float o[15];
 #pragma unroll
-                for (int q = 0; q < 15; ++q) o[q] = sp[(S_XXX + q) * N];
+                for (int q = 0; q < 15; ++q) o[q] = ld(sp + (S_XXX + q) * N, grp(q));
                 float mx = 1.f, my = 1.f, mz = 1.f;
         PDiv<FAST> px = 1, py = 1, pz = 1;
                 {
@@ -690,35 +847,40 @@ __device__ __forceinline__ bool str_item(const ZMaps &mp, const Model &m, const 
                 a0 = split_update<FAST>(o[S_XXX - S_XXX], dl, dXx, kx, mx, px);
                 a1 = split_update<FAST>(o[S_XXY - S_XXX], dt, l * dYy, ky, my, py);
                 a2 = split_update<FAST>(o[S_XXZ - S_XXX], dt, l * dZz, kz, mz, pz);
-                sp[S_XXX * N] = a0; sp[S_XXY * N] = a1; sp[S_XXZ * N] = a2;
+                sput(S_XXX, a0); sput(S_XXY, a1); sput(S_XXZ, a2);
                 snew[0] = (a0 + a1) + a2;
                 a0 = split_update<FAST>(o[S_YYX - S_XXX], dt, l * dXx, kx, mx, px);
                 a1 = split_update<FAST>(o[S_YYY - S_XXX], dl, dYy, ky, my, py);
                 a2 = split_update<FAST>(o[S_YYZ - S_XXX], dt, l * dZz, kz, mz, pz);
-                sp[S_YYX * N] = a0; sp[S_YYY * N] = a1; sp[S_YYZ * N] = a2;
+                sput(S_YYX, a0); sput(S_YYY, a1); sput(S_YYZ, a2);
                 snew[1] = (a0 + a1) + a2;
                 a0 = split_update<FAST>(o[S_ZZX - S_XXX], dt, l * dXx, kx, mx, px);
                 a1 = split_update<FAST>(o[S_ZZY - S_XXX], dt, l * dYy, ky, my, py);
                 a2 = split_update<FAST>(o[S_ZZZ - S_XXX], dl, dZz, kz, mz, pz);
-                sp[S_ZZX * N] = a0; sp[S_ZZY * N] = a1; sp[S_ZZZ * N] = a2;
+                sput(S_ZZX, a0); sput(S_ZZY, a1); sput(S_ZZZ, a2);
                 snew[2] = (a0 + a1) + a2;
                 const float axy = dt * mxy, axz = dt * mxz, ayz = dt * myz;
                 a0 = split_update<FAST>(o[S_XYX - S_XXX], axy, xyX, kx, mx, px);
                 a1 = split_update<FAST>(o[S_XYY - S_XXX], axy, xyY, ky, my, py);
-                sp[S_XYX * N] = a0; sp[S_XYY * N] = a1;
+                sput(S_XYX, a0); sput(S_XYY, a1);
                 snew[3] = a0 + a1;
                 a0 = split_update<FAST>(o[S_XZX - S_XXX], axz, xzX, kx, mx, px);
                 a1 = split_update<FAST>(o[S_XZZ - S_XXX], axz, xzZ, kz, mz, pz);
-                sp[S_XZX * N] = a0; sp[S_XZZ * N] = a1;
+                sput(S_XZX, a0); sput(S_XZZ, a1);
                 snew[4] = a0 + a1;
                 a0 = split_update<FAST>(o[S_YZY - S_XXX], ayz, yzY, ky, my, py);
                 a1 = split_update<FAST>(o[S_YZZ - S_XXX], ayz, yzZ, kz, mz, pz);
-                sp[S_YZY * N] = a0; sp[S_YZZ * N] = a1;
+                sput(S_YZY, a0); sput(S_YZZ, a1);
                 snew[5] = a0 + a1;
             }
 #pragma unroll
-            for (int q = 0; q < 6; ++q) m.f[3 + q][ci] = snew[q];
-            if (GEN && gz == rz && it >= 0 && it < sr.nt) {
+            for (int q = 0; q < 6; ++q) {
+                if constexpr (H) {
+                    if (track) note_max16s(smax, 3 + q, snew[q]);
+                }
+                put(fld(3 + q) + ci, 3 + q, snew[q]);
+            }
+            if (GEN && !H && gz == rz && it >= 0 && it < sr.nt) {
                 for (int r = rp; r < rend && g.rec_list[r].z == gz; ++r) {
                     const int4 q = g.rec_list[r];
                     if (q.x == gx && q.y == gyc[c] && q.w >= 3)
@@ -737,7 +899,7 @@ __device__ __forceinline__ bool str_item(const ZMaps &mp, const Model &m, const 
         if (cz + S < t.ze) {
             if (lx == 0) {
                 fence_proxy_async();
-                str_issue<TY>(mybox, nbox, st, &bar[s], cz + S, warp);
+                str_issue<TY, ES>(mybox, nbox, st, &bar[s], cz + S, warp);
             }
             issued_end = cz + S + 1;
         }
@@ -773,6 +935,12 @@ __device__ __forceinline__ bool str_item(const ZMaps &mp, const Model &m, const 
         if (MANY) drain_bits<S>(bar, issued_end, cz, t.zs, pbits);
         else drain<S>(bar, issued_end, cz, t.zs);
     }
+    if constexpr (H) {
+        if (track) {
+            __syncthreads();
+            flush_max16(hs, smax);
+        }
+    }
     return !abort;
 }
 
@@ -792,6 +960,42 @@ k_stress_zmarch(const __grid_constant__ ZMaps mp, const __grid_constant__ Model 
     uint32_t pbits = 0;
     str_item<FAST, CELLS, false>(mp, m, ph, g, sr, it_arg, src_value, use_wavelet, blockIdx.x, blockIdx.y,
                           align_smem(smem_raw), bar, boxes, pbits);
+}
+
+// 16-bit wavefield storage (ST = SGFD_STORE_BF16 / _F16), 32 x 8 tiles.
+template <bool FAST, int ST>
+__global__ void __launch_bounds__(NT, 3)
+k_velocity_zmarch16(const __grid_constant__ ZMaps mp, const __grid_constant__ Model m,
+                    const __grid_constant__ Physics ph, const __grid_constant__ ZGeom g,
+                    const __grid_constant__ SourceRec sr, const __grid_constant__ HalfState hs, int it_arg) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t bar[S];
+    __shared__ TmaBox boxes[kWarps][kMaxBoxesPerWarp];
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < S; ++s) mbar_init(&bar[s], 1);
+        fence_barrier_init();
+    }
+    __syncthreads();
+    uint32_t pbits = 0;
+    vel_item<FAST, 1, false, ST>(mp, m, ph, g, sr, it_arg, 0.0f, 0, blockIdx.x, blockIdx.y, align_smem(smem_raw), bar,
+                                 boxes, pbits, hs);
+}
+template <bool FAST, int ST>
+__global__ void __launch_bounds__(NT, 3)
+k_stress_zmarch16(const __grid_constant__ ZMaps mp, const __grid_constant__ Model m,
+                  const __grid_constant__ Physics ph, const __grid_constant__ ZGeom g,
+                  const __grid_constant__ SourceRec sr, const __grid_constant__ HalfState hs, int it_arg) {
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t bar[S];
+    __shared__ TmaBox boxes[kWarps][kMaxBoxesPerWarp];
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < S; ++s) mbar_init(&bar[s], 1);
+        fence_barrier_init();
+    }
+    __syncthreads();
+    uint32_t pbits = 0;
+    str_item<FAST, 1, false, ST>(mp, m, ph, g, sr, it_arg, 0.0f, 0, blockIdx.x, blockIdx.y, align_smem(smem_raw), bar,
+                                 boxes, pbits, hs);
 }
 
 PFN_cuTensorMapEncodeTiled_v12000 get_encoder() {
@@ -818,6 +1022,22 @@ cudaError_t set_attrs() {
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_stress_zmarch<FAST, CELLS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  str_smem<CELLS>());
+    return e;
+}
+
+// 16-bit storage: the ring of 16-bit stages, then the FP32 work buffer.
+constexpr int vel_smem16() { return S * VelL<8, 2>::STAGE + VelL<8>::STAGE + 128; }
+constexpr int str_smem16() { return S * StrL<8, 2>::STAGE + StrL<8>::STAGE + 128; }
+static_assert(3 * (vel_smem16() + 1024) <= 228 * 1024 && 3 * (str_smem16() + 1024) <= 228 * 1024,
+              "three CTAs per SM");
+
+template <bool FAST, int ST>
+cudaError_t set_attrs16() {
+    cudaError_t e = cudaFuncSetAttribute(k_velocity_zmarch16<FAST, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         vel_smem16());
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_stress_zmarch16<FAST, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 str_smem16());
     return e;
 }
 
@@ -911,6 +1131,24 @@ k_batch_zmarch(const ZModel *models, int nmodels, const int *first_item, int it0
     }
 }
 
+// One step with 16-bit storage: the source injection before the velocity
+// update, the velocity receivers after it, the stress receivers and the
+// rescale after the stress update (kernels_half.cu, half_phase).
+template <bool FAST, int ST>
+void launch16(const Model &m, const Physics &ph, const SourceRec &sr, const HalfState &hs, const ZGeom &g,
+              const ZMaps &zm, int it, float src_value, bool uw, cudaStream_t s, cudaEvent_t *ev) {
+    const dim3 grid(g.ntx * g.nty, g.nchunks);
+    half_phase(m, ph, sr, hs, it, src_value, uw, s, 0);
+    if (ev) cudaEventRecord(ev[0], s);
+    k_velocity_zmarch16<FAST, ST><<<grid, NT, vel_smem16(), s>>>(zm, m, ph, g, sr, hs, it);
+    if (ev) cudaEventRecord(ev[1], s);
+    half_phase(m, ph, sr, hs, it, src_value, uw, s, 1);
+    if (ev) cudaEventRecord(ev[2], s);
+    k_stress_zmarch16<FAST, ST><<<grid, NT, str_smem16(), s>>>(zm, m, ph, g, sr, hs, it);
+    if (ev) cudaEventRecord(ev[3], s);
+    half_phase(m, ph, sr, hs, it, src_value, uw, s, 2);
+}
+
 template <bool FAST, int CELLS>
 void launch(const Model &m, const Physics &ph, const SourceRec &sr, const ZGeom &g, const ZMaps &zm, int it,
             float src_value, int uw, cudaStream_t s, cudaEvent_t *ev) {
@@ -980,8 +1218,56 @@ bool make_pool_map(CUtensorMap *map, const float *first, const Model &m, size_t 
     return r == CUDA_SUCCESS;
 }
 
-cudaError_t zmarch_prepare(const Model &m, int cells, size_t st, ZMaps *zm) {
+// The same over 16-bit arrays of the same layout.
+bool make_pool_map16(CUtensorMap *map, const uint16_t *first, const Model &m, size_t stride, int count, int bx,
+                     int by) {
+    auto enc = get_encoder();
+    if (!enc) return false;
+    void *base = const_cast<uint16_t *>(first - kXOff);
+    cuuint64_t dims[4] = {(cuuint64_t)(m.nx + kXOff), (cuuint64_t)m.ny, (cuuint64_t)m.nz, (cuuint64_t)count};
+    cuuint64_t strides[3] = {(cuuint64_t)m.px * 2, (cuuint64_t)m.plane * 2, (cuuint64_t)stride};
+    cuuint32_t box[4] = {(cuuint32_t)bx, (cuuint32_t)by, 1, (cuuint32_t)count};
+    cuuint32_t es[4] = {1, 1, 1, 1};
+    CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_UINT16, 4, base, dims, strides, box, es,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
+cudaError_t zmarch_prepare(const Model &m, int cells, size_t st, ZMaps *zm, const HalfState *hs, size_t st16) {
     if (cells != 1 && cells != 2) return cudaErrorInvalidValue;
+    if (hs) {
+        // 16-bit storage: the stored wavefields (evenly spaced 16-bit arrays) and the FP32 medium
+        if (cells != 1) return cudaErrorInvalidValue;
+        for (int k = 0; k < 9; ++k)
+            if (hs->f[k] != reinterpret_cast<const uint16_t *>(reinterpret_cast<const char *>(hs->f[0]) + k * st16))
+                return cudaErrorInvalidValue;
+        const float *med[5] = {m.lam, m.mu, m.mxy, m.mxz, m.myz};
+        for (int k = 0; k < 5; ++k)
+            if (med[k] != reinterpret_cast<const float *>(reinterpret_cast<const char *>(m.lam) + k * st))
+                return cudaErrorInvalidValue;
+        const int ty = 8;
+        bool ok = true;
+        ok &= make_pool_map16(&zm->v_sxx_sxz, hs->f[3], m, 4 * st16, 2, W48, ty);
+        ok &= make_pool_map16(&zm->v_syy_syz, hs->f[4], m, 4 * st16, 2, W32, ty + 10);
+        ok &= make_pool_map16(&zm->v_sxy, hs->f[6], m, st16, 1, W48, ty + 10);
+        ok &= make_pool_map(&zm->v_b, m.b, m, st, 1, W36, ty + 1);
+        ok &= make_pool_map16(&zm->v_lead_xz_yz, hs->f[7], m, st16, 2, W32, ty);
+        ok &= make_pool_map16(&zm->v_lead_zz, hs->f[5], m, st16, 1, W32, ty);
+        ok &= make_pool_map(&zm->v_lead_b, m.b, m, st, 1, W32, ty);
+        ok &= make_pool_map16(&zm->v_own, hs->f[0], m, st16, 3, W32, ty);
+        ok &= make_pool_map16(&zm->s_v, hs->f[0], m, st16, 3, W48, ty + 10);
+        ok &= make_pool_map16(&zm->s_lead_xy, hs->f[0], m, st16, 2, W32, ty);
+        ok &= make_pool_map16(&zm->s_lead_z, hs->f[2], m, st16, 1, W32, ty);
+        ok &= make_pool_map16(&zm->s_own, hs->f[3], m, st16, 6, W32, ty);
+        ok &= make_pool_map(&zm->s_med, m.lam, m, st, 5, W32, ty);
+        if (!ok) return cudaErrorInvalidValue;
+        cudaError_t e = set_attrs16<false, SGFD_STORE_BF16>();
+        if (e == cudaSuccess) e = set_attrs16<true, SGFD_STORE_BF16>();
+        if (e == cudaSuccess) e = set_attrs16<false, SGFD_STORE_F16>();
+        if (e == cudaSuccess) e = set_attrs16<true, SGFD_STORE_F16>();
+        return e;
+    }
     // the pool order the merged copies rely on: vx..tyz, lambda, mu, mxy, mxz, myz
     auto at = [&](int k) { return reinterpret_cast<const float *>(reinterpret_cast<const char *>(m.f[0]) + k * st); };
     const float *order[14] = {m.f[0], m.f[1], m.f[2], m.f[3], m.f[4], m.f[5], m.f[6], m.f[7],
@@ -1001,7 +1287,8 @@ cudaError_t zmarch_prepare(const Model &m, int cells, size_t st, ZMaps *zm) {
     ok &= make_pool_map(&zm->s_v, m.f[0], m, st, 3, W48, ty + 10);
     ok &= make_pool_map(&zm->s_lead_xy, m.f[0], m, st, 2, W32, ty);
     ok &= make_pool_map(&zm->s_lead_z, m.f[2], m, st, 1, W32, ty);
-    ok &= make_pool_map(&zm->s_own, m.f[3], m, st, StrL<8>::NOWN, W32, ty);
+    ok &= make_pool_map(&zm->s_own, m.f[3], m, st, 11, W32, ty);
+    zm->s_med = zm->s_own;   // unused by FP32 storage (its own-cell copy brings the medium too)
     if (!ok) return cudaErrorInvalidValue;
     cudaError_t e = cells == 1 ? set_attrs<false, 1>() : set_attrs<false, 2>();
     if (e == cudaSuccess) e = cells == 1 ? set_attrs<true, 1>() : set_attrs<true, 2>();
@@ -1014,7 +1301,18 @@ void zmarch_tiles(const Model &m, int cells, int *ntx, int *nty) {
 }
 
 cudaError_t zmarch_step(const Model &m, const Physics &ph, const SourceRec &sr, const ZGeom &g, const ZMaps &zm,
-                        int it, float src_value, bool use_wavelet, cudaStream_t s, cudaEvent_t *ev) {
+                        int it, float src_value, bool use_wavelet, cudaStream_t s, cudaEvent_t *ev,
+                        const HalfState *hs) {
+    if (hs) {
+        if (hs->storage == SGFD_STORE_BF16) {
+            if (ph.fast) launch16<true, SGFD_STORE_BF16>(m, ph, sr, *hs, g, zm, it, src_value, use_wavelet, s, ev);
+            else launch16<false, SGFD_STORE_BF16>(m, ph, sr, *hs, g, zm, it, src_value, use_wavelet, s, ev);
+        } else {
+            if (ph.fast) launch16<true, SGFD_STORE_F16>(m, ph, sr, *hs, g, zm, it, src_value, use_wavelet, s, ev);
+            else launch16<false, SGFD_STORE_F16>(m, ph, sr, *hs, g, zm, it, src_value, use_wavelet, s, ev);
+        }
+        return cudaGetLastError();
+    }
     const int uw = use_wavelet ? 1 : 0;
     if (ph.fast) {
         if (g.cells == 1) launch<true, 1>(m, ph, sr, g, zm, it, src_value, uw, s, ev);

@@ -32,6 +32,7 @@
 
 #include "../../include/sgfd.h"
 #include "cell_math.cuh"
+#include "store16.cuh"
 #include "zmarch.h"
 #include "zmarch_dev.cuh"
 
@@ -241,14 +242,8 @@ template <int ST>
 struct Sto16 {
     using E = uint16_t;
     static constexpr int ES = 2;
-    __device__ __forceinline__ static float h2f(uint32_t h) {
-        if (ST == SGFD_STORE_BF16) return __uint_as_float(h << 16);
-        return __half2float(__ushort_as_half((unsigned short)h));
-    }
-    __device__ __forceinline__ static uint32_t f2h(float w) {
-        if (ST == SGFD_STORE_BF16) return __bfloat16_as_ushort(__float2bfloat16_rn(w));
-        return __half_as_ushort(__float2half_rn(fminf(fmaxf(w, -65504.0f), 65504.0f)));
-    }
+    __device__ __forceinline__ static float h2f(uint32_t h) { return H16<ST>::h2f(h); }
+    __device__ __forceinline__ static uint32_t f2h(float w) { return H16<ST>::f2h(w); }
     __device__ __forceinline__ static float2 pair(const E *p, float2 sc) {
         const uint32_t u = *reinterpret_cast<const uint32_t *>(p);
         return make_float2(h2f(u & 0xffffu) * sc.x, h2f(u >> 16) * sc.y);
@@ -301,13 +296,6 @@ struct Fields {
     }
 };
 
-// Largest |v| of the warp's active lanes into field g's running maximum (the
-// rescale steps of 16-bit storage, as kernels_half.cu notes them).
-__device__ __forceinline__ void note_max16(const HalfState &hs, int g, float v) {
-    const unsigned mask = __activemask();
-    const unsigned bits = __reduce_max_sync(mask, __float_as_uint(fabsf(v)));
-    if ((threadIdx.x & 31) == __ffs(mask) - 1) atomicMax(hs.amax + g, bits);
-}
 
 // Common per-thread state of both updates.
 struct PairCtx {

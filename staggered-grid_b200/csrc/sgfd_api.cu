@@ -109,13 +109,20 @@ int get_scale_exponents(sgfd_solver *h, int *e) {
     return SGFD_OK;
 }
 
+// Bytes between consecutive 16-bit wavefield arrays (0 with FP32 storage).
+size_t stride16(const sgfd_solver *h) {
+    if (h->storage == SGFD_STORE_F32) return 0;
+    return (size_t)(reinterpret_cast<const char *>(h->hs.f[1]) - reinterpret_cast<const char *>(h->hs.f[0]));
+}
+
 cudaError_t dispatch_on(sgfd_solver *h, const SourceRec &sr, cudaStream_t s, int it, float value,
                         bool use_wavelet, cudaEvent_t *ev) {
     const bool h16 = h->storage != SGFD_STORE_F32;
     cudaError_t e = h->kernel == SGFD_KERNEL_ZMARCH
                         ? (h->zg.pair ? zpair_step(h->m, h->ph, sr, h16 ? &h->hs : nullptr, h->zg, h->vm, h->sm, it,
                                                    value, use_wavelet, s, ev)
-                                      : zmarch_step(h->m, h->ph, sr, h->zg, h->zm, it, value, use_wavelet, s, ev))
+                                      : zmarch_step(h->m, h->ph, sr, h->zg, h->zm, it, value, use_wavelet, s, ev,
+                                                    h16 ? &h->hs : nullptr))
                     : h16 ? half_step(h->m, h->ph, sr, h->hs, it, value, use_wavelet, s, ev)
                         : simple_step(h->m, h->ph, sr, it, value, use_wavelet, s, ev);
     if (e == cudaSuccess && h->strip_n > 0)
@@ -505,12 +512,12 @@ int sgfd_create(const sgfd_config *cfg, sgfd_solver **out) {
     }
 
     if (c.kernel != SGFD_KERNEL_SIMPLE && zmarch_supported(m)) {
-        // FP32: 32 x 8 tiles; 16-bit storage: the paired tiling, the only one built for it
+        // 32 x 8 tiles, with either storage (16-bit storage also runs on the paired 64 x 8 tiling)
         const bool h16 = c.storage != SGFD_STORE_F32;
         h->zg.cells = 1;
-        h->zg.pair = h16 ? 1 : 0;
-        h->zg.tw = h16 ? kPairTileX : kZTileX;
-        e = h16 ? zpair_prepare(m, &h->hs, &h->vm, &h->sm) : zmarch_prepare(m, h->zg.cells, arr_bytes, &h->zm);
+        h->zg.pair = 0;
+        h->zg.tw = kZTileX;
+        e = zmarch_prepare(m, h->zg.cells, arr_bytes, &h->zm, h16 ? &h->hs : nullptr, stride16(h));
         if (e == cudaSuccess) e = dev_malloc(h, &h->dev_err, sizeof(int));
         if (e == cudaSuccess) e = cudaMemset(h->dev_err, 0, sizeof(int));
         if (e != cudaSuccess) {
@@ -519,8 +526,7 @@ int sgfd_create(const sgfd_config *cfg, sgfd_solver **out) {
             return r;
         }
         h->kernel = SGFD_KERNEL_ZMARCH;
-        if (h16) zpair_tiles(m, &h->zg.ntx, &h->zg.nty);
-        else zmarch_tiles(m, h->zg.cells, &h->zg.ntx, &h->zg.nty);
+        zmarch_tiles(m, h->zg.cells, &h->zg.ntx, &h->zg.nty);
         h->zg.err = h->dev_err;
         set_zchunks(h);
         int r = upload_zrec(h, {});
@@ -772,13 +778,15 @@ int sgfd_set_tile(sgfd_solver *h, int32_t tile_cols, int32_t tile_rows, int32_t 
         return fail(h, SGFD_ERR_INVALID, "tiles are 32 x 8, 32 x 16 or 64 x 8");
     if (zchunk < 0) return fail(h, SGFD_ERR_INVALID, "negative chunk");
     if (!h->dev_err) return SGFD_OK;   // no z-marching kernels prepared: nothing to tile
-    if (h->storage != SGFD_STORE_F32 && !pair)
-        return fail(h, SGFD_ERR_UNSUPPORTED, "16-bit storage runs on 64 x 8 tiles only");
+    const bool h16 = h->storage != SGFD_STORE_F32;
+    if (h16 && !pair && tile_rows != 8)
+        return fail(h, SGFD_ERR_UNSUPPORTED, "16-bit storage runs on 32 x 8 or 64 x 8 tiles");
     SG_CUDA(h, cudaStreamSynchronize(h->stream), "synchronise before re-tiling");
     const int cells = tile_rows / 8;
     if (cells != h->zg.cells || (int)pair != h->zg.pair) {
-        cudaError_t e = pair ? zpair_prepare(h->m, h->storage != SGFD_STORE_F32 ? &h->hs : nullptr, &h->vm, &h->sm)
-                             : zmarch_prepare(h->m, cells, array_bytes(h->m), &h->zm);
+        cudaError_t e = pair ? zpair_prepare(h->m, h16 ? &h->hs : nullptr, &h->vm, &h->sm)
+                             : zmarch_prepare(h->m, cells, array_bytes(h->m), &h->zm, h16 ? &h->hs : nullptr,
+                                              stride16(h));
         if (e != cudaSuccess) return cuda_fail(h, e, "z-march re-tiling");
         h->zg.cells = cells;
         h->zg.pair = pair ? 1 : 0;

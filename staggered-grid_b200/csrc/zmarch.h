@@ -25,8 +25,9 @@ struct ZMaps {
     // z+1; own vx, vy, vz (32 x TY each)
     CUtensorMap v_sxx_sxz, v_syy_syz, v_sxy, v_b, v_lead_xz_yz, v_lead_zz, v_lead_b, v_own;
     // stress update: vx, vy, vz (48 x TY+10); lead vx + vy at z+5, vz at z+4;
-    // own txx..myz (11 arrays, 32 x TY each)
-    CUtensorMap s_v, s_lead_xy, s_lead_z, s_own;
+    // own txx..myz (11 arrays, 32 x TY each; with 16-bit storage the 6
+    // stored stresses in s_own and the FP32 lambda..myz in s_med)
+    CUtensorMap s_v, s_lead_xy, s_lead_z, s_own, s_med;
 };
 
 // TMA descriptors of the paired velocity update (kernels_zpair.cu): x/y-halo
@@ -66,12 +67,17 @@ bool make_box_map16(CUtensorMap *map, const uint16_t *grid_origin, const Model &
 
 // zmarch_prepare: the maps of the single-cell family over the model's array
 // pool, whose arrays are array_stride bytes apart in the order the stress
-// update reads them (cudaErrorInvalidValue when the pointers are otherwise).
+// update reads them (cudaErrorInvalidValue when the pointers are otherwise);
+// with hs (16-bit storage, cells = 1), the wavefield maps cover the 16-bit
+// arrays, stride16 bytes apart.  zmarch_step: one step (velocity + stress);
+// with hs also the 16-bit source, receiver and rescale kernels.
 bool zmarch_supported(const Model &m);
-cudaError_t zmarch_prepare(const Model &m, int cells, size_t array_stride, ZMaps *zm);
+cudaError_t zmarch_prepare(const Model &m, int cells, size_t array_stride, ZMaps *zm, const HalfState *hs = nullptr,
+                           size_t stride16 = 0);
 void zmarch_tiles(const Model &m, int cells, int *ntx, int *nty);
 cudaError_t zmarch_step(const Model &m, const Physics &ph, const SourceRec &sr, const ZGeom &g, const ZMaps &zm,
-                        int it, float src_value, bool use_wavelet, cudaStream_t s, cudaEvent_t *ev = nullptr);
+                        int it, float src_value, bool use_wavelet, cudaStream_t s, cudaEvent_t *ev = nullptr,
+                        const HalfState *hs = nullptr);
 // One model of a persistent batch, in device memory (the kernel's TMA reads
 // its tensor maps from there: 64-byte alignment).  Its work items are the
 // (tile, z chunk) pairs of the single-cell 32 x 8 tiling, tile fastest.

@@ -21,22 +21,27 @@ def _case(storage, **kw):
     return w
 
 
-FAMILIES = [("zmarch", sgfd.KERNEL_AUTO, 0), ("zmarch_chunk6", sgfd.KERNEL_AUTO, 6), ("simple", sgfd.KERNEL_SIMPLE, 0)]
+# (name, kernel family, tile columns (0: the default 32 x 8), z chunk)
+FAMILIES = [("zmarch", sgfd.KERNEL_AUTO, 0, 0), ("zmarch_chunk6", sgfd.KERNEL_AUTO, 32, 6),
+            ("zmarch_pairs", sgfd.KERNEL_AUTO, 64, 0), ("zmarch_pairs_chunk6", sgfd.KERNEL_AUTO, 64, 6),
+            ("simple", sgfd.KERNEL_SIMPLE, 0, 0)]
 
 
 @pytest.mark.parametrize("family", FAMILIES, ids=[f[0] for f in FAMILIES])
 @pytest.mark.parametrize("arith", [sgfd.ARITH_REF, sgfd.ARITH_FAST], ids=["ref", "fast"])
 @pytest.mark.parametrize("store", STORES, ids=[s[1] for s in STORES])
 def test_bit_exact_vs_oracle_emulation(store, arith, family):
-    """The z-marching kernels (64 x 8 tiles, 16-bit boxes staged by TMA) and
-    the per-cell kernels both equal the oracle's emulation bit for bit."""
+    """The z-marching kernels (32 x 8 tiles: 16-bit boxes staged by TMA and
+    widened once per plane; 64 x 8 tiles: read back per tap) and the per-cell
+    kernels all equal the oracle's emulation bit for bit."""
     w = _case(store[0], nt=110, nrec=36)    # scales re-chosen after steps 0, 1, 3, 7, 15, 31, 49, 99
     w.cfg["arith"] = arith
     o = run_oracle(w)
     with make_solver(w, kernel=family[1]) as s:
         assert s.kernel_name() == family[0].split("_")[0]
         if family[2]:
-            s.set_tile(64, 8, family[2])
+            s.set_tile(family[2], 8, family[3])
+        assert s.tile()[0] in ((family[2] or 32),) or family[1] == sgfd.KERNEL_SIMPLE
         s.run(0, w.nt)
         s.synchronize()
         np.testing.assert_array_equal(s.traces(), o.traces().astype(np.float32))
@@ -83,15 +88,18 @@ def test_16_bit_error_against_fp64():
     assert errs["f16"] < errs["bf16"]
 
 
+@pytest.mark.parametrize("cols", [32, 64], ids=["32x8", "64x8"])
 @pytest.mark.parametrize("store", STORES, ids=[s[1] for s in STORES])
-def test_16_bit_zmarch_large_interior_matches_oracle(store):
-    """A case with interior-only tile-planes and several z chunks: the packed
-    interior path of the 16-bit kernels equals the oracle's emulation too."""
+def test_16_bit_zmarch_large_interior_matches_oracle(store, cols):
+    """A case with interior-only tile-planes and several z chunks: the
+    interior paths of both 16-bit tilings equal the oracle's emulation too."""
     w = wl.small_random_case(nx=150, ny=60, nz=70, pml=4, nt=60, nrec=30)
     w.cfg["storage"] = store[0]
     o = run_oracle(w)
     with make_solver(w) as s:
-        assert s.kernel_name() == "zmarch" and s.tile()[:2] == (64, 8)
+        assert s.kernel_name() == "zmarch" and s.tile()[:2] == (32, 8)
+        s.set_tile(cols, 8, 0)
+        assert s.tile()[:2] == (cols, 8)
         s.run(0, w.nt)
         np.testing.assert_array_equal(s.traces(), o.traces().astype(np.float32))
         for fid in (sgfd.VX, sgfd.TXX, sgfd.TYZ):
@@ -103,7 +111,7 @@ def test_16_bit_handles_reject_what_needs_fp32():
     with make_solver(w, kernel=sgfd.KERNEL_ZMARCH) as z:
         assert z.kernel_name() == "zmarch"
         with pytest.raises(sgfd.SgfdError) as e:
-            z.set_tile(32, 8)                       # 16-bit boxes only on the paired tiling
+            z.set_tile(32, 16)                      # 16-bit boxes on 32 x 8 and 64 x 8 tiles only
         assert e.value.code == sgfd.ERR_UNSUPPORTED
     with make_solver(w, kernel=sgfd.KERNEL_SIMPLE) as s:
         with pytest.raises(sgfd.SgfdError) as e:
