@@ -107,9 +107,10 @@ typedef enum sgfd_quirks {
  * +-65504), halving the wavefield bytes.  The scales are re-chosen after steps
  * 0, 1, 3, 7, 15, 31, 49 and then every 50 steps from the largest magnitude
  * each field wrote in that step, so that it is stored near 2^7.  16-bit storage
- * runs on the z-marching kernels with 64 x 8 tiles (16-bit boxes staged by
- * TMA) or, with SGFD_KERNEL_SIMPLE, on the per-cell kernels; both give the
- * same bits.  The per-step audit (sgfd_set_audit) is not available with it. */
+ * runs on the z-marching kernels with 32 x 8 tiles (16-bit boxes staged by
+ * TMA and widened once per plane; 64 x 8 tiles through sgfd_set_tile) or,
+ * with SGFD_KERNEL_SIMPLE, on the per-cell kernels; all give the same bits.
+ * The per-step audit (sgfd_set_audit) is not available with it. */
 typedef enum sgfd_storage {
     SGFD_STORE_F32 = 0,
     SGFD_STORE_BF16 = 1,
@@ -260,7 +261,8 @@ int sgfd_set_tiling(sgfd_solver *h, int32_t tile_rows, int32_t zchunk);
 /* z-marching kernels: tile shape and planes per z chunk (0 = automatic).
  * 32 x 8 and 32 x 16: one or two y-adjacent cells per thread; 64 x 8: two
  * x-adjacent cells per thread, differences and updates of the pair on packed
- * FP32x2.  Results do not depend on the tiling (bit-identical). */
+ * FP32x2.  16-bit storage: 32 x 8 or 64 x 8.  Results do not depend on the
+ * tiling (bit-identical). */
 int sgfd_set_tile(sgfd_solver *h, int32_t tile_cols, int32_t tile_rows, int32_t zchunk);
 /* The z-marching tile shape and z chunk in use (zeros for the simple family). */
 int sgfd_get_tile(const sgfd_solver *h, int32_t *tile_cols, int32_t *tile_rows, int32_t *zchunk);
