@@ -344,10 +344,12 @@ __device__ __forceinline__ bool vel_pair(const VelMaps &mp, const Model &m, cons
     constexpr int S = SV;
     constexpr bool H = ST != SGFD_STORE_F32;   // 16-bit storage: source and receivers run as separate kernels
     __shared__ float scl[18];   // 16-bit storage: this step's scales, read at every tap
+    __shared__ unsigned smax[9];   // 16-bit storage, rescale steps: this CTA's largest written magnitudes
     if constexpr (ST != SGFD_STORE_F32) {
         if (threadIdx.x < 9) {
             scl[threadIdx.x] = hs.sc[threadIdx.x];
             scl[9 + threadIdx.x] = hs.inv[threadIdx.x];
+            smax[threadIdx.x] = 0u;
         }
         __syncthreads();
     }
@@ -498,9 +500,9 @@ __device__ __forceinline__ bool vel_pair(const VelMaps &mp, const Model &m, cons
                 SA::put2(F.f(1) + ci, v1, bcast(F.inv(1)), pc.act1);
                 SA::put2(F.f(2) + ci, v2, bcast(F.inv(2)), pc.act1);
                 if (track) {
-                    note_max16(hs, 0, fmaxf(fabsf(v0.x), pc.act1 ? fabsf(v0.y) : 0.0f));
-                    note_max16(hs, 1, fmaxf(fabsf(v1.x), pc.act1 ? fabsf(v1.y) : 0.0f));
-                    note_max16(hs, 2, fmaxf(fabsf(v2.x), pc.act1 ? fabsf(v2.y) : 0.0f));
+                    note_max16s(smax, 0, fmaxf(fabsf(v0.x), pc.act1 ? fabsf(v0.y) : 0.0f));
+                    note_max16s(smax, 1, fmaxf(fabsf(v1.x), pc.act1 ? fabsf(v1.y) : 0.0f));
+                    note_max16s(smax, 2, fmaxf(fabsf(v2.x), pc.act1 ? fabsf(v2.y) : 0.0f));
                 }
                 if (!H && GEN && gz == rz && it >= 0 && it < sr.nt) {
                     for (int r = rp; r < rend && g.rec_list[r].z == gz; ++r) {
@@ -562,7 +564,7 @@ __device__ __forceinline__ bool vel_pair(const VelMaps &mp, const Model &m, cons
                             for (int a = 0; a < 3; ++a) {
                                 // split S_VXX + 3q + a, in the scale of field q
                                 part[a] = split_update<FAST>(o[3 * q + a], aq[q], dxyz[q][a], kk[a], mm[a], pp[a]);
-                                if (track) note_max16(hs, q, part[a]);
+                                if (track) note_max16s(smax, q, part[a]);
                                 SA::put1(sp + (3 * q + a) * N, part[a], F.inv(q));
                             }
                             vnew[q] = (part[0] + part[1]) + part[2];
@@ -570,7 +572,7 @@ __device__ __forceinline__ bool vel_pair(const VelMaps &mp, const Model &m, cons
                     }
 #pragma unroll
                     for (int q = 0; q < 3; ++q) {
-                        if (track) note_max16(hs, q, vnew[q]);
+                        if (track) note_max16s(smax, q, vnew[q]);
                         SA::put1(F.f(q) + cc, vnew[q], F.inv(q));
                     }
                     if (!H && gz == rz && it >= 0 && it < sr.nt) {
@@ -632,6 +634,12 @@ __device__ __forceinline__ bool vel_pair(const VelMaps &mp, const Model &m, cons
             pbits ^= 1u << q;
         }
     }
+    if constexpr (H) {
+        if (track) {
+            __syncthreads();
+            flush_max16(hs, smax);
+        }
+    }
     return !abort;
 }
 
@@ -655,10 +663,12 @@ __device__ __forceinline__ bool str_pair(const StrMaps &mp, const Model &m, cons
     constexpr int S = SS;
     constexpr bool H = ST != SGFD_STORE_F32;   // 16-bit storage: source and receivers run as separate kernels
     __shared__ float scl[18];   // 16-bit storage: this step's scales, read at every tap
+    __shared__ unsigned smax[9];   // 16-bit storage, rescale steps: this CTA's largest written magnitudes
     if constexpr (ST != SGFD_STORE_F32) {
         if (threadIdx.x < 9) {
             scl[threadIdx.x] = hs.sc[threadIdx.x];
             scl[9 + threadIdx.x] = hs.inv[threadIdx.x];
+            smax[threadIdx.x] = 0u;
         }
         __syncthreads();
     }
@@ -769,7 +779,7 @@ __device__ __forceinline__ bool str_pair(const StrMaps &mp, const Model &m, cons
 #pragma unroll
                 for (int q = 0; q < 6; ++q) {
                     SA::put2(F.f(3 + q) + ci, sn[q], bcast(F.inv(3 + q)), pc.act1);
-                    if (track) note_max16(hs, 3 + q, fmaxf(fabsf(sn[q].x), pc.act1 ? fabsf(sn[q].y) : 0.0f));
+                    if (track) note_max16s(smax, 3 + q, fmaxf(fabsf(sn[q].x), pc.act1 ? fabsf(sn[q].y) : 0.0f));
                 }
                 if (!H && GEN && gz == rz && it >= 0 && it < sr.nt) {
                     for (int r = rp; r < rend && g.rec_list[r].z == gz; ++r) {
@@ -812,7 +822,7 @@ __device__ __forceinline__ bool str_pair(const StrMaps &mp, const Model &m, cons
                         const float b_c = m.b[cc];
                         auto rd = [&](int k) { return o[k - S_XXX]; };
                         auto wr = [&](int k, float v) {
-                            if (track) note_max16(hs, grp(k), v);
+                            if (track) note_max16s(smax, grp(k), v);
                             SA::put1(sp + k * N, v, F.inv(grp(k)));
                         };
                         float mx = 1.f, my = 1.f, mz = 1.f;
@@ -857,7 +867,7 @@ __device__ __forceinline__ bool str_pair(const StrMaps &mp, const Model &m, cons
                     }
 #pragma unroll
                     for (int q = 0; q < 6; ++q) {
-                        if (track) note_max16(hs, 3 + q, snew[q]);
+                        if (track) note_max16s(smax, 3 + q, snew[q]);
                         SA::put1(F.f(3 + q) + cc, snew[q], F.inv(3 + q));
                     }
                     if (!H && gz == rz && it >= 0 && it < sr.nt) {
@@ -914,6 +924,12 @@ __device__ __forceinline__ bool str_pair(const StrMaps &mp, const Model &m, cons
             const int q = (j - t.zs) % S;
             mbar_wait(&bar[q], (pbits >> q) & 1u);
             pbits ^= 1u << q;
+        }
+    }
+    if constexpr (H) {
+        if (track) {
+            __syncthreads();
+            flush_max16(hs, smax);
         }
     }
     return !abort;
