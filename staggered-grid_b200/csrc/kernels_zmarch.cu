@@ -1,31 +1,37 @@
 // kernels_zmarch.cu — the "zmarch" kernel family: 2.5-D z-marching velocity
-// and stress updates for sm_100a.
+// and stress updates for sm_100a, and the persistent batch kernel built from
+// the same per-tile bodies.
 //
 // Work decomposition.  A CTA of 256 threads owns a 32 x TY tile of computed
 // cells in the xy plane (TY = 8 * CELLS, each thread owning CELLS vertically
 // adjacent cells, whose y differences share one window of staged values) and
-// marches along z over a chunk of planes.
+// marches along z over a chunk of planes (a work item: vel_item / str_item).
 //
 // Data movement per plane z (all HBM traffic is TMA or coalesced 128-byte rows):
-//   * TMA (cp.async.bulk.tensor.3d, no multicast) stages
+//   * TMA (cp.async.bulk.tensor.4d over the array pool, no multicast) stages
 //     the xy boxes the x/y derivatives need — tile plus its 5-cell halo on the
 //     sides a field is differentiated along — and the "lead" planes that feed
 //     the z register queues, and the cell's own read-modify-write data, into
 //     a 3-stage shared-memory ring guarded by one mbarrier per stage (expect-tx
-//     bytes, parity wait with an iteration cap); lane 0 of each warp issues a
-//     share of a stage's boxes so that no warp carries the issue alone.
-//     A stage is refilled with plane z + 3 as soon as plane z is done, so
-//     every load has two plane-iterations to land.
-//   * Each thread keeps the 10 z-taps of the fields it differentiates along z
-//     in a register queue (sigma_xz, sigma_yz, sigma_zz for the velocity
-//     update; vx, vy, vz for the stress update), shifted by one per plane.
+//     bytes, parity wait with an iteration cap).  Arrays read with the same
+//     box at the same plane come in one copy (the 4th map dimension walks the
+//     arrays): 8 copies per velocity plane, 4 per stress plane; lane 0 of warp
+//     w issues copy w.  A stage is refilled with plane z + 3 as soon as plane
+//     z is done, so every load has two plane-iterations to land.
+//   * Each thread keeps the z-taps of the fields it differentiates along z in
+//     register queues (sigma_xz, sigma_yz, sigma_zz for the velocity update,
+//     10 deep, shifted by one per plane; vx, vy, vz for the stress update, 11
+//     deep, planes taken in pairs and the queues moved by two per pair).
 //   * The velocity update loads the PML split fields of its cell into
 //     registers before the plane's TMA wait; the stress update, which needs
 //     15 of them, loads them where they are used, so that it fits the 80
 //     registers per thread of three resident CTAs per SM.
+//   * 16-bit wavefield storage (ST = BF16 / F16, 32 x 8 tiles): the field
+//     boxes arrive as 16-bit values and are widened once per plane into an
+//     FP32 work buffer (float(h) * 2^e) before the same FP32 arithmetic.
 // Every row starts at a 128-byte boundary (the device arrays are shifted by
 // kXOff), so x-halo boxes start 8 cells left of the tile (48 wide), centre
-// boxes are exactly 32 wide, and every TMA x coordinate is a multiple of 4.
+// boxes are exactly 32 wide, and every TMA x coordinate is a multiple of 8.
 // One block barrier per plane separates the reads of a stage from its refill
 // and carries the abort vote of the bounded waits.
 //
@@ -34,7 +40,8 @@
 // The source (dt*dt*s(it) on txx, tyy, tzz, OPT/ElasticWaveEquation.cu:206-221)
 // is applied to the staged copies the velocity update reads and to the old
 // value the stress update accumulates onto, which reproduces the reference's
-// store-then-read order exactly; receivers are written from registers.
+// store-then-read order exactly; receivers are written from registers (with
+// 16-bit storage both run as the 16-bit family's own kernels).
 // Arithmetic per cell is the same sequence as kernels_simple.cu and the oracle.
 #include <cuda.h>
 #include <cudaTypedefs.h>
