@@ -136,7 +136,7 @@ __global__ void __launch_bounds__(kBX * kBY) k_velocity16(Model m, Physics ph, S
         const int kk[3] = {kx, ky, kz};
         const float mm[3] = {mx, my, mz};
         const PDiv<FAST> pp[3] = {px, py, pz};
-        const int64_t pi = pml_index(m, cx, cy, cz), N = m.npml;
+        const int64_t pi = split_base(pml_index(m, cx, cy, cz)), N = kSplitBlock;
         for (int q = 0; q < 3; ++q) {
             float part[3];
             for (int ax = 0; ax < 3; ++ax) {
@@ -199,7 +199,7 @@ __global__ void __launch_bounds__(kBX * kBY) k_stress16(Model m, Physics ph, Sou
             if (ky) damp_factors<FAST>(ph, 1, ph.dy, ky, m.pml, v, my, py);
             if (kz) damp_factors<FAST>(ph, 2, ph.dz, kz, m.pml, v, mz, pz);
         }
-        const int64_t pi = pml_index(m, cx, cy, cz), N = m.npml;
+        const int64_t pi = split_base(pml_index(m, cx, cy, cz)), N = kSplitBlock;
         const float dl = ph.dt * l2m, dt = ph.dt;
         auto upd = [&](int k, float A, float B, int kd, float mf, PDiv<FAST> pf) {
             const float r = split_update<FAST>(S.sget(k, k * N + pi), A, B, kd, mf, pf);
@@ -289,10 +289,24 @@ __global__ void k_rescale_apply(Model m, SourceRec sr, HalfState hs, int it_arg,
         if (hs.e_new[g] == hs.e[g]) continue;
         rescale(hs.f[g] - kXOff, n_grid, ldexpf(1.0f, hs.e[g] - hs.e_new[g]));   // the whole padded array
     }
-    for (int k = 0; k < kNumSplit; ++k) {
-        const int g = split_group(k);
-        if (hs.e_new[g] == hs.e[g]) continue;
-        rescale(hs.split + (int64_t)k * m.npml, m.npml, ldexpf(1.0f, hs.e[g] - hs.e_new[g]));
+    // the blocked splits: eight values of one split per 16-byte access
+    {
+        const int64_t n8 = split_elems(m.npml) / 8;
+        uint4 *q = reinterpret_cast<uint4 *>(hs.split);
+        for (int64_t i = t0; i < n8; i += stride) {
+            const int g = split_group(split_of(8 * i));
+            if (hs.e_new[g] == hs.e[g]) continue;
+            const float f = ldexpf(1.0f, hs.e[g] - hs.e_new[g]);
+            uint4 v = q[i];
+            uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const uint32_t lo = f2h<ST>(h2f<ST>(w[j] & 0xffffu) * f);
+                const uint32_t hi = f2h<ST>(h2f<ST>(w[j] >> 16) * f);
+                w[j] = lo | (hi << 16);
+            }
+            q[i] = make_uint4(w[0], w[1], w[2], w[3]);
+        }
     }
 }
 
@@ -316,11 +330,8 @@ __global__ void k_to_views(Model m, HalfState hs, int64_t n_grid) {
         const float sc = hs.sc[g];
         for (int64_t i = t0; i < n_grid; i += stride) q[i] = h2f<ST>(p[i]) * sc;
     }
-    for (int k = 0; k < kNumSplit; ++k) {
-        const float sc = hs.sc[split_group(k)];
-        for (int64_t i = t0; i < m.npml; i += stride)
-            m.split[(int64_t)k * m.npml + i] = h2f<ST>(hs.split[(int64_t)k * m.npml + i]) * sc;
-    }
+    const int64_t ns = split_elems(m.npml);
+    for (int64_t j = t0; j < ns; j += stride) m.split[j] = h2f<ST>(hs.split[j]) * hs.sc[split_group(split_of(j))];
 }
 
 // Stored values from the FP32 copies (after a checkpoint load).
@@ -333,11 +344,8 @@ __global__ void k_from_views(Model m, HalfState hs, int64_t n_grid) {
         const float inv = hs.inv[g];
         for (int64_t i = t0; i < n_grid; i += stride) p[i] = f2h<ST>(q[i] * inv);
     }
-    for (int k = 0; k < kNumSplit; ++k) {
-        const float inv = hs.inv[split_group(k)];
-        for (int64_t i = t0; i < m.npml; i += stride)
-            hs.split[(int64_t)k * m.npml + i] = f2h<ST>(m.split[(int64_t)k * m.npml + i] * inv);
-    }
+    const int64_t ns = split_elems(m.npml);
+    for (int64_t j = t0; j < ns; j += stride) hs.split[j] = f2h<ST>(m.split[j] * hs.inv[split_group(split_of(j))]);
 }
 
 template <int ST>

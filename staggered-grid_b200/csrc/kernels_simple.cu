@@ -71,8 +71,8 @@ __global__ void __launch_bounds__(kBX * kBY) k_velocity(Model m, Physics ph) {
     const bool ref = ph.quirks == 0;   // REF: x-averaged buoyancy for all components
     const float ax = ph.dt * bx, ay = ph.dt * (ref ? bx : by), az = ph.dt * (ref ? bx : bz);
     const int64_t pi = pml_index(m, cx, cy, cz);
-    float *sp = m.split + pi;
-    const int64_t N = m.npml;
+    float *sp = m.split + split_base(pi);
+    const int64_t N = kSplitBlock;   // split k at sp[k * N]
     float a0, a1, a2;
     a0 = sp[S_VXX * N] = split_update<FAST>(sp[S_VXX * N], ax, xX, kx, mx, px);
     a1 = sp[S_VXY * N] = split_update<FAST>(sp[S_VXY * N], ax, xY, ky, my, py);
@@ -138,8 +138,8 @@ __global__ void __launch_bounds__(kBX * kBY) k_stress(Model m, Physics ph) {
         if (kz) damp_factors<FAST>(ph, 2, ph.dz, kz, m.pml, v, mz, pz);
     }
     const int64_t pi = pml_index(m, cx, cy, cz);
-    float *sp = m.split + pi;
-    const int64_t N = m.npml;
+    float *sp = m.split + split_base(pi);
+    const int64_t N = kSplitBlock;   // split k at sp[k * N]
     const float dl = ph.dt * l2m, dt = ph.dt;
     float a0, a1, a2;
     a0 = sp[S_XXX * N] = split_update<FAST>(sp[S_XXX * N], dl, dXx, kx, mx, px);

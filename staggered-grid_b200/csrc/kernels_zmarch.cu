@@ -334,14 +334,13 @@ __device__ __forceinline__ bool vel_item(const ZMaps &mp, const Model &m, const 
         // stage wait so that their latency overlaps the wait and the stencil
         float opre[CELLS][9], mupre[CELLS], lampre[CELLS];
         if (plane_pml) {
-            const uint32_t N = (uint32_t)m.npml;
 #pragma unroll
             for (int c = 0; c < CELLS; ++c) {
                 if (act[c] && (kx | kyc[c] | kz)) {
                     const uint32_t ci = col[c] + (uint32_t)gz * PL;
-                    const auto *sp = spl() + pml_plane_index(m, pcol[c], cz);
+                    const auto *sp = spl() + split_base32(pml_plane_index(m, pcol[c], cz));
 #pragma unroll
-                    for (int q = 0; q < 9; ++q) opre[c][q] = ld(sp + q * N, q / 3);   // split q: field q / 3
+                    for (int q = 0; q < 9; ++q) opre[c][q] = ld(sp + q * kSplitBlock, q / 3);   // split q: field q / 3
                     mupre[c] = m.mu[ci];
                     lampre[c] = ph.damping == 1 ? m.lam[ci] : 0.f;
                 }
@@ -483,8 +482,8 @@ __device__ __forceinline__ bool vel_item(const ZMaps &mp, const Model &m, const 
                 }
                 const bool ref = ph.quirks == 0;
                 const float ax = ph.dt * bx, ay = ph.dt * (ref ? bx : by), az = ph.dt * (ref ? bx : bz);
-                auto *sp = spl() + pml_plane_index(m, pcol[c], cz);
-                const uint32_t N = (uint32_t)m.npml;
+                auto *sp = spl() + split_base32(pml_plane_index(m, pcol[c], cz));
+                constexpr uint32_t N = kSplitBlock;   // split k at sp[k * N]
                 const float *o = opre[c];
                 // split k belongs to field k / 3 (its scale with 16-bit storage)
                 auto sput = [&](int k, float v) {
@@ -828,8 +827,8 @@ __device__ __forceinline__ bool str_item(const ZMaps &mp, const Model &m, const 
                 snew[4] = __fmaf_rn(ph.dt * mxz, xzZ + xzX, own[4 * OS + e]);
                 snew[5] = __fmaf_rn(ph.dt * myz, yzZ + yzY, own[5 * OS + e]);
             } else {
-                auto *sp = spl() + pml_plane_index(m, pcol[c], cz);
-                const uint32_t N = (uint32_t)m.npml;
+                auto *sp = spl() + split_base32(pml_plane_index(m, pcol[c], cz));
+                constexpr uint32_t N = kSplitBlock;   // split k at sp[k * N]
                 // split S_XXX + k belongs to field txx..tyz (its scale with 16-bit storage)
                 auto grp = [](int k) { return k < 9 ? 3 + k / 3 : 6 + (k - 9) / 2; };
                 auto sput = [&](int k, float v) {
@@ -1203,9 +1202,8 @@ bool zmarch_supported(const Model &m) {
     // Halo boxes start 8 cells left of the tile and 5 rows above: always inside
     // the padded array because the frame is 5 cells and kXOff is 27.  The
     // kernels address cells and PML split values with 32-bit offsets: cell
-    // offsets below 2^31, split offsets (component * npml + PML cell) below 2^32
-    const bool small = m.plane * (int64_t)m.nz < ((int64_t)1 << 31) &&
-                       (int64_t)kNumSplit * m.npml <= ((int64_t)1 << 32);
+    // offsets below 2^31, split offsets (the blocked split array) below 2^32
+    const bool small = m.plane * (int64_t)m.nz < ((int64_t)1 << 31) && split_elems(m.npml) <= ((int64_t)1 << 32);
     return small && m.nxc >= 1 && m.nyc >= 1 && m.nzc >= 1 && get_encoder() != nullptr;
 }
 

@@ -532,8 +532,8 @@ __device__ __forceinline__ bool vel_pair(const VelMaps &mp, const Model &m, cons
                     } else {
                         // every global load of the cell first: the split stores below could
                         // alias them as far as the compiler knows, so loads after a store wait
-                        E *sp = F.split() + pml_plane_index(m, c ? pc.pc1 : pc.pc0, cz);
-                        const uint32_t N = (uint32_t)m.npml;
+                        E *sp = F.split() + split_base32(pml_plane_index(m, c ? pc.pc1 : pc.pc0, cz));
+                        const uint32_t N = kSplitBlock;   // split k at sp[k * N]
                         float o[9];
 #pragma unroll
                         for (int k = 0; k < 9; ++k) o[k] = SA::one(sp + k * N, F.sc(k / 3));
@@ -811,8 +811,8 @@ __device__ __forceinline__ bool str_pair(const StrMaps &mp, const Model &m, cons
                         snew[5] = __fmaf_rn(ph.dt * lane_of(myz, c), lane_of(yzZ, c) + lane_of(yzY, c),
                                             SA::one(own + 5 * OS + e + c, F.sc(8)));
                     } else {
-                        E *sp = F.split() + pml_plane_index(m, c ? pc.pc1 : pc.pc0, cz);
-                        const uint32_t N = (uint32_t)m.npml;
+                        E *sp = F.split() + split_base32(pml_plane_index(m, c ? pc.pc1 : pc.pc0, cz));
+                        const uint32_t N = kSplitBlock;   // split k at sp[k * N]
                         // split k, in its field's scale (S_XXX.. -> txx.., two per shear stress)
                         auto grp = [](int k) { return k < S_XYX ? 3 + (k - S_XXX) / 3 : 6 + (k - S_XYX) / 2; };
                         // every global load of the cell first (the split stores could alias them)

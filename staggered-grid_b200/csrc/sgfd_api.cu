@@ -450,11 +450,11 @@ int sgfd_create(const sgfd_config *cfg, sgfd_solver **out) {
     const size_t arr_bytes = array_bytes(m);
     const size_t pool_bytes = arr_bytes * 16;
     e = dev_malloc(h, &h->field_pool, pool_bytes);
-    if (e == cudaSuccess) e = dev_malloc(h, &h->split, (size_t)kNumSplit * m.npml * sizeof(float));
+    if (e == cudaSuccess) e = dev_malloc(h, &h->split, (size_t)split_elems(m.npml) * sizeof(float));
     if (e != cudaSuccess) {
         cudaGetLastError();
         int r = fail(nullptr, SGFD_ERR_ALLOC, "device allocation of %.2f GB failed",
-                     (pool_bytes + (double)kNumSplit * m.npml * 4) / 1e9);
+                     (pool_bytes + (double)split_elems(m.npml) * 4) / 1e9);
         sgfd_destroy(h);
         return r;
     }
@@ -471,7 +471,7 @@ int sgfd_create(const sgfd_config *cfg, sgfd_solver **out) {
     m.rmu = arr(15);
     m.split = h->split;
     e = cudaMemsetAsync(h->field_pool, 0, pool_bytes, h->stream);
-    if (e == cudaSuccess) e = cudaMemsetAsync(h->split, 0, (size_t)kNumSplit * m.npml * sizeof(float), h->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(h->split, 0, (size_t)split_elems(m.npml) * sizeof(float), h->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
     if (e != cudaSuccess) {
         int r = cuda_fail(nullptr, e, "zeroing device state");
@@ -487,7 +487,7 @@ int sgfd_create(const sgfd_config *cfg, sgfd_solver **out) {
     if (c.storage != SGFD_STORE_F32) {
         h->storage = c.storage;
         const size_t a16 = round_up((size_t)m.plane * m.nz * 2, 256);
-        const size_t s16 = round_up((size_t)kNumSplit * m.npml * 2, 256);
+        const size_t s16 = round_up((size_t)split_elems(m.npml) * 2, 256);
         e = dev_malloc(h, &h->h16_pool, a16 * 9 + s16);
         if (e == cudaSuccess) e = dev_malloc(h, &h->hstate, 64 * sizeof(int));
         if (e == cudaSuccess) e = cudaMemsetAsync(h->h16_pool, 0, a16 * 9 + s16, h->stream);
@@ -819,7 +819,7 @@ int sgfd_reset(sgfd_solver *h) {
     const Model &m = h->m;
     const size_t arr_bytes = array_bytes(m);
     SG_CUDA(h, cudaMemsetAsync(h->field_pool, 0, arr_bytes * 9, h->stream), "reset fields");
-    SG_CUDA(h, cudaMemsetAsync(h->split, 0, (size_t)kNumSplit * m.npml * sizeof(float), h->stream), "reset splits");
+    SG_CUDA(h, cudaMemsetAsync(h->split, 0, (size_t)split_elems(m.npml) * sizeof(float), h->stream), "reset splits");
     if (h->traces)
         SG_CUDA(h, cudaMemsetAsync(h->traces, 0, (size_t)h->sr.nrec * h->sr.nt * sizeof(float), h->stream), "reset traces");
     if (h->audit_hist)
@@ -827,7 +827,7 @@ int sgfd_reset(sgfd_solver *h) {
                 "reset audit history");
     if (h->h16_pool) {
         const size_t a16 = round_up((size_t)m.plane * m.nz * 2, 256);
-        const size_t s16 = round_up((size_t)kNumSplit * m.npml * 2, 256);
+        const size_t s16 = round_up((size_t)split_elems(m.npml) * 2, 256);
         SG_CUDA(h, cudaMemsetAsync(h->h16_pool, 0, a16 * 9 + s16, h->stream), "reset 16-bit fields");
         const int r = reset_scales(h);
         if (r) return r;

@@ -10,11 +10,13 @@
 //     computed cells of every 32-wide tile start on a 128-byte boundary.
 //     Model::f[k] etc. point at GRID (0,0,0); the allocation starts kXOff
 //     floats earlier.  index(ix, iy, iz) = ix + iy*px + iz*px*ny.
-//   * PML split fields: a compact array of the PML cells only, 24 splits as
-//     structure-of-arrays, split k of PML cell c at split[k*npml + c].  PML
-//     cells are enumerated plane by plane (z slowest), and within a plane row
-//     by row, x fastest, so a warp reading consecutive x reads consecutive
-//     addresses (pml_index()).  The reference keeps 26 region arrays of
+//   * PML split fields: a compact array of the PML cells only.  PML cells
+//     are enumerated plane by plane (z slowest), and within a plane row by
+//     row, x fastest (pml_index()); blocks of 32 consecutive cells hold their
+//     24 splits as 24 rows of 32 values, split k of cell c at
+//     split[split_base(c) + 32*k] (split_base()).  A warp reading consecutive
+//     x reads one 128-byte row per split, and a cell's 24 splits sit at fixed
+//     offsets from one address.  The reference keeps 26 region arrays of
 //     (len+1)^3 each (OPT/ElasticWaveEquation.cu:34-41).
 #pragma once
 
@@ -76,7 +78,7 @@ struct Model {
     // staggered shear moduli of the txy, txz, tyz updates: harmonic means of
     // four mu (ElasticMacro.h:110-119), computed once per medium upload
     const float *mxy, *mxz, *myz;
-    float *split;        // kNumSplit * npml
+    float *split;        // split_elems(npml) values, blocked (split_base)
 };
 
 // 16-bit wavefield storage (kernels_half.cu): fields and splits as 16-bit
@@ -86,7 +88,7 @@ constexpr int kRescaleEvery = 50;   // scales re-chosen every 50 steps (after st
 constexpr int kScaleHead = 8;       // largest stored magnitude put in [2^7, 2^8)
 struct HalfState {
     uint16_t *f[9];      // same layout (pitch, offset) as Model::f
-    uint16_t *split;     // kNumSplit * npml
+    uint16_t *split;     // split_elems(npml) values, blocked as Model::split
     int *e, *e_new;      // scale exponents (9 each)
     float *sc, *inv;     // 2^e, 2^-e
     unsigned *amax;      // largest |value| written on a rescale step (float bits)
@@ -151,6 +153,22 @@ __host__ __device__ inline int64_t pml_index(const Model &m, int cx, int cy, int
     }
     return base + (int64_t)p * m.nxc + (int64_t)(m.nyc - 2 * p) * 2 * p + (int64_t)(cy - (m.nyc - p)) * m.nxc + cx;
 }
+
+// Split storage: blocks of kSplitBlock PML cells (consecutive compact
+// indices), each block kNumSplit rows of kSplitBlock values; split k of PML
+// cell c at split_base(c) + k * kSplitBlock.
+constexpr int kSplitBlock = 32;
+__host__ __device__ inline int64_t split_base(int64_t c) {
+    return (c / kSplitBlock) * (int64_t)(kNumSplit * kSplitBlock) + c % kSplitBlock;
+}
+__host__ __device__ inline uint32_t split_base32(uint32_t c) {
+    return (c / kSplitBlock) * (uint32_t)(kNumSplit * kSplitBlock) + c % kSplitBlock;
+}
+// Values the split array holds (the last block padded), and the split of value j.
+__host__ __device__ inline int64_t split_elems(int64_t npml) {
+    return (npml + kSplitBlock - 1) / kSplitBlock * (int64_t)(kNumSplit * kSplitBlock);
+}
+__host__ __device__ inline int split_of(int64_t j) { return (int)((j / kSplitBlock) % kNumSplit); }
 
 // pml_index() split in two for kernels that march along z: a per-column
 // offset (in full PML planes and in ring planes) and a per-plane base.  32-bit

@@ -9,12 +9,14 @@
 // receivers and wavelet are the caller's inputs and are set again before a
 // resume.
 //
-// Format (little-endian), version 1:
+// Format (little-endian), version 2:
 //   header, 128 bytes: see CkptHeader below;
 //   payload: 9 fields of nx*ny*nz float32 (x fastest, in SGFD_VX..SGFD_TYZ
-//   order), then 24 split arrays of npml float32 in the library's compact PML
-//   order (split-major; cells ordered as sgfd's pml_index), then the traces,
-//   nt*nrec float32 time-major.
+//   order), then the 24 PML splits as the library holds them: PML cells in
+//   sgfd's pml_index order, in blocks of 32 cells, each block 24 rows of 32
+//   float32 (split k of cell c at (c / 32) * 768 + 32 k + c % 32; the last
+//   block zero-padded), then the traces, nt*nrec float32 time-major.
+//   (Version 1 stored the splits split-major, 24 arrays of npml values.)
 // The header's checksum covers the payload (4-lane FNV-1a over 64-bit words).
 #include <cstdio>
 #include <cstring>
@@ -29,7 +31,7 @@ using namespace sgfd;
 namespace {
 
 constexpr char kMagic[8] = {'S', 'G', 'F', 'D', 'C', 'K', 'P', '1'};
-constexpr uint32_t kVersion = 1;
+constexpr uint32_t kVersion = 2;
 constexpr size_t kStage = size_t(32) << 20;   // pinned staging chunk
 
 struct CkptHeader {
@@ -123,7 +125,7 @@ std::vector<Region> payload_regions(sgfd_solver *h) {
     for (int k = 0; k < SGFD_NFIELDS; ++k)
         r.push_back({reinterpret_cast<char *>(m.f[k]), (size_t)m.px * 4, (size_t)m.nx * 4, (size_t)m.ny * m.nz});
     if (m.npml > 0) {
-        const size_t b = (size_t)kNumSplit * m.npml * 4;
+        const size_t b = (size_t)split_elems(m.npml) * 4;
         r.push_back({reinterpret_cast<char *>(h->split), b, b, 1});
     }
     if (h->traces && h->sr.nrec > 0) {

@@ -81,8 +81,10 @@ def test_ricker_matches_oracle_bitwise():
 def test_pml_index_is_a_bijection(tmp_path):
     """Host-compiles the device layout helpers of csrc/sgfd_internal.h and checks
     that pml_index() maps the PML cells one-to-one onto [0, npml) for uneven
-    sizes, and that the per-column/per-plane split the z-marching kernels use
-    gives the same index."""
+    sizes, that the per-column/per-plane split the z-marching kernels use
+    gives the same index, and that the blocked split storage (split k of cell
+    c at split_base(c) + 32 k) gives every (cell, split) its own value inside
+    split_elems(npml), in 64-bit and 32-bit form."""
     src = tmp_path / "t.cpp"
     src.write_text(r'''
 #include "sgfd_internal.h"
@@ -108,6 +110,13 @@ int main() {
     }
     if (cnt != m.npml) { std::printf("count %lld vs %lld\n", (long long)cnt, (long long)m.npml); return 1; }
     for (auto h : hit) if (h != 1) { std::printf("not bijective\n"); return 1; }
+    std::vector<unsigned char> used(split_elems(m.npml), 0);
+    for (int64_t c = 0; c < m.npml; ++c)
+      for (int k = 0; k < kNumSplit; ++k) {
+        const int64_t j = split_base(c) + (int64_t)k * kSplitBlock;
+        if (j < 0 || j >= (int64_t)used.size() || used[j]++) { std::printf("split slot %lld\n", (long long)j); return 1; }
+        if ((int64_t)split_base32((uint32_t)c) != split_base(c) || split_of(j) != k) { std::printf("split forms\n"); return 1; }
+      }
   }
   std::puts("ok"); return 0;
 }
