@@ -79,6 +79,9 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-steps", type=int, default=6, help="steps of the CPU sample")
+    p.add_argument("--slabs", type=int, default=0,
+                   help="one model cut into z-slabs with halo exchange: this many slabs on one GPU, or with "
+                        "N > 1 one slab per rank (NCCL send/recv between neighbours)")
     return p.parse_args()
 
 
@@ -320,6 +323,9 @@ def main():
                 run_reference_arm(args, build_workload(args.workload), 1, 0)
         return
     world, rank, local = dist_setup(args)
+    if args.slabs:
+        main_slabs(args, world, rank, local)
+        return
     if args.workload in ("batch32", "combined32"):
         main_batch(args, world, rank, local)
         return
@@ -374,6 +380,78 @@ def main():
             "clocks": b["clocks"], "gpu_launches": b["launches"]}
         if rank == 0 and world == 1 and not args.no_accuracy:
             result["random472"]["accuracy"] = accuracy_leg(big, args, local)
+    if rank == 0:
+        print(json.dumps(result), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def main_slabs(args, world, rank, local):
+    """One model cut along z: args.slabs slabs on this GPU (world 1), or one
+    slab per rank (world > 1; total work fixed, "strong" scaling).  Each step
+    trades the 5 planes beside every cut twice (sgfd.slabs); timed with CUDA
+    events on the stream all slab work runs on, max over ranks."""
+    import torch
+    import sgfd
+    import sgfd.slabs as sl
+    w = build_workload(args.workload)
+    torch.cuda.set_device(local)
+    K, W = args.steps, args.warmup
+    nslabs = world if world > 1 else args.slabs
+    arith = sgfd.ARITH_FAST if args.arith == "fast" else sgfd.ARITH_REF
+    cfg = sgfd.default_config(**{**w.cfg, "device": local, "arith": arith})
+    cuts = sl.plan_cuts(cfg.nz, nslabs, src_z=w.src[2])
+    nt = max(w.nt, W + K + 4)
+    wav = np.resize(w.wavelet, nt).astype(np.float32)
+    if world > 1:
+        m = sl.DistributedSlab(cfg, cuts, rank, world, local)
+        handles = [m.s]
+    else:
+        m = sl.SlabModel(cfg, cuts)
+        handles = m.slabs
+    m.set_medium(w.b, w.lam, w.mu)
+    m.set_source(*w.src)
+    m.set_receivers(w.rec_xyz, w.rec_comp, nt)
+    m.run(0, W, wav)
+    torch.cuda.synchronize()
+    n_int = sum(h.cell_counts()[0] for h in handles)
+    n_pml = sum(h.cell_counts()[1] for h in handles)
+    stream = torch.cuda.current_stream()
+    clocks = ClockSampler(None)
+    clocks.start()
+    barrier(world)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    m.run(W, K, wav)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    clk = clocks.stop()
+    ms = max_over_ranks(e0.elapsed_time(e1), world)
+    cells = w.computed_cells()
+    value = cells * K / (ms / 1e3) / 1e9
+    peak, peak_kind = measured_peak()
+    # algorithmic bytes of this GPU's cells (all slabs on one GPU, this rank's slab otherwise)
+    alg = (sum(v[0] for v in BYTES.values()) * n_int + sum(v[1] for v in BYTES.values()) * n_pml)
+    halo = 2 * 2 * (nslabs - 1) * handles[0].halo_bytes()   # bytes crossing cuts per step, both directions
+    result = {
+        "metric": "Gcell-updates/s", "value": value, "unit": "Gcell/s", "n_gpus": world, "steps": K, "warmup": W,
+        "ms_per_step": ms / K, "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": f"{w.name} in {nslabs} z-slabs", "grid": [cfg.nx, cfg.ny, cfg.nz],
+                   "cuts": cuts, "computed_cells": cells, "arith": args.arith,
+                   "parallelism": f"zslab{nslabs}" + ("" if world > 1 else " on one GPU"),
+                   "halo_bytes_per_step": halo if world > 1 else 0,
+                   "l2": "inputs larger than L2 (9 wavefields of %.0f MB each)" % (cfg.nx * cfg.ny * cfg.nz * 4 / 1e6)},
+        "roofline": {"bound": "hbm", "kernel": "step (all slabs' kernels and halo copies)",
+                     "achieved": alg / (ms / K / 1e3) / 1e9, "peak": peak,
+                     "unit": "GB/s", "frac": alg / (ms / K / 1e3) / 1e9 / peak,
+                     "peak_source": peak_kind, "traffic": None},
+        "clocks": clk, "gpu_launches": K * 2 * len(handles),
+        "e2e": None,
+    }
     if rank == 0:
         print(json.dumps(result), flush=True)
     if world > 1:

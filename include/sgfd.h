@@ -148,7 +148,10 @@ typedef struct sgfd_config {
     int32_t kernel;           /* sgfd_kernel */
     int32_t device;           /* CUDA device ordinal */
     int32_t arith;            /* sgfd_arith */
-    int32_t reserved[7];      /* must be zero */
+    int32_t nz_total;         /* 0: the handle is a whole model; else the GRID z extent of the
+                                 whole model this handle is a z-slab of (see sgfd_halo_pack) */
+    int32_t z_offset;         /* z-slab: computed planes of the whole model below the slab */
+    int32_t reserved[5];      /* must be zero */
 } sgfd_config;
 
 typedef struct sgfd_solver sgfd_solver;
@@ -266,6 +269,45 @@ int sgfd_set_tiling(sgfd_solver *h, int32_t tile_rows, int32_t zchunk);
 int sgfd_set_tile(sgfd_solver *h, int32_t tile_cols, int32_t tile_rows, int32_t zchunk);
 /* The z-marching tile shape and z chunk in use (zeros for the simple family). */
 int sgfd_get_tile(const sgfd_solver *h, int32_t *tile_cols, int32_t *tile_rows, int32_t *zchunk);
+
+/* ---- z-slabs: one model split along z over several handles, on one GPU or
+ * one handle per GPU (no counterpart in the reference, whose model must fit
+ * one GPU and whose 32-bit `memsize` caps it at 2^29 cells:
+ * OPT/ElasticWaveEquation.cu:20,143) ----
+ * A handle created with nz_total != 0 holds computed planes [z_offset,
+ * z_offset + nz - 10) of a model whose GRID has nz_total planes; every slab of
+ * the model has the same nx, ny, pml and physics.  The PML is the whole
+ * model's: z bands only where the slab reaches the model's z ends, damping
+ * distances and the compact split order counted in the whole model.  At a cut
+ * between two slabs, each slab's 5 frame planes hold its neighbour's values
+ * (the reach of the 10th-order z differences): before every velocity update
+ * the neighbour's txz, tyz, tzz (SGFD_HALO_STRESS), before every stress update
+ * its vx, vy, vz (SGFD_HALO_VELOCITY).  sgfd_halo_pack copies the slab's own 5
+ * computed planes beside a cut (3 fields, sgfd_halo_bytes in all) to a DEVICE
+ * buffer; sgfd_halo_unpack writes a received buffer into the 5 frame planes
+ * on that side.  The caller moves the buffer to the neighbour: a device copy
+ * between slabs on one GPU, NCCL send/recv or a peer copy between GPUs.  Both
+ * are ordered on the handle's stream.  A step of the whole model is then, per
+ * slab: exchange STRESS, sgfd_step_phase(VELOCITY), exchange VELOCITY,
+ * sgfd_step_phase(STRESS), and the slabs together give the whole model's
+ * results bit for bit.  Each slab is given the whole model's medium on its
+ * GRID planes (frame planes included), the receivers that lie in its planes,
+ * and the source if it lies there; the source must lie 5 or more computed
+ * planes from every cut (its injection is not part of the exchanged planes).
+ * Slabs have FP32 storage, the z-marching kernels with 32-column tiles or the simple kernels,
+ * no learned strip and no per-step audit. */
+#define SGFD_HALO_LOW 0        /* the cut below the slab (smaller z) */
+#define SGFD_HALO_HIGH 1       /* the cut above it */
+#define SGFD_HALO_STRESS 0     /* txz, tyz, tzz: exchanged before the velocity update */
+#define SGFD_HALO_VELOCITY 1   /* vx, vy, vz: exchanged before the stress update */
+#define SGFD_PHASE_VELOCITY 0  /* source injection, velocity update, velocity receivers */
+#define SGFD_PHASE_STRESS 1    /* stress update, stress receivers */
+int sgfd_halo_bytes(const sgfd_solver *h, int64_t *bytes);
+int sgfd_halo_pack(sgfd_solver *h, int32_t side, int32_t kind, void *dst);
+int sgfd_halo_unpack(sgfd_solver *h, int32_t side, int32_t kind, const void *src);
+/* Half of sgfd_step: SGFD_PHASE_VELOCITY then SGFD_PHASE_STRESS with the same
+ * it and source value is one step.  Any handle (whole model or slab). */
+int sgfd_step_phase(sgfd_solver *h, int32_t it, float source_value, int32_t phase);
 
 /* ---- autotuning and batches (no counterpart in the reference, which runs
  * one model with a fixed launch shape: OPT/main.cu's GPUDim) ---- */

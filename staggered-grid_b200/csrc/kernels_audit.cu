@@ -66,7 +66,7 @@ __global__ void __launch_bounds__(kAuditThreads) k_energy_partial(Model m, int r
     for (int r = blockIdx.x * (kAuditThreads / 32) + (threadIdx.x >> 5); r < rows; r += warps) {
         const int cz = r / m.nyc, cy = r - cz * m.nyc;
         const int y = cy + kHalo, z = cz + kHalo;
-        const bool yz_pml = band(y, m.ny, m.pml) != 0 || band(z, m.nz, m.pml) != 0;
+        const bool yz_pml = band(y, m.ny, m.pml) != 0 || bandz(m, z) != 0;
         for (int cx = lane; cx < m.nxc; cx += 32) {
             const int x = cx + kHalo;
             const bool in_pml = yz_pml || band(x, m.nx, m.pml) != 0;

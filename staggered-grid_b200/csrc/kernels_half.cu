@@ -113,7 +113,7 @@ __global__ void __launch_bounds__(kBX * kBY) k_velocity16(Model m, Physics ph, S
     const float zY = dB<FAST, 1>(ph, [&](int o) { return S.tap(8, syz, o * SY); });
     const float zZ = dF<FAST, 2>(ph, [&](int o) { return S.tap(5, szz, o * SZ); });
 
-    const int kx = band(x, m.nx, m.pml), ky = band(y, m.ny, m.pml), kz = band(z, m.nz, m.pml);
+    const int kx = band(x, m.nx, m.pml), ky = band(y, m.ny, m.pml), kz = bandz(m, z);
     float vn[3];
     if (!(kx | ky | kz)) {
         vn[0] = __fmaf_rn(ph.dt * bx, (xX + xY) + xZ, S.get(0, ci));
@@ -181,7 +181,7 @@ __global__ void __launch_bounds__(kBX * kBY) k_stress16(Model m, Physics ph, Sou
     const float l2m = __fmaf_rn(2.0f, m.mu[ci], l);
     const float mxy = m.mxy[ci], mxz = m.mxz[ci], myz = m.myz[ci];
 
-    const int kx = band(x, m.nx, m.pml), ky = band(y, m.ny, m.pml), kz = band(z, m.nz, m.pml);
+    const int kx = band(x, m.nx, m.pml), ky = band(y, m.ny, m.pml), kz = bandz(m, z);
     float sn[6];
     if (!(kx | ky | kz)) {
         sn[0] = __fmaf_rn(ph.dt, __fmaf_rn(l2m, dXx, l * (dYy + dZz)), S.get(3, ci));

@@ -53,7 +53,7 @@ __global__ void __launch_bounds__(kBX * kBY) k_velocity(Model m, Physics ph) {
     const float zY = dB<FAST, 1>(ph, [&](int o) { return __ldg(syz + o * SY); });
     const float zZ = dF<FAST, 2>(ph, [&](int o) { return __ldg(szz + o * SZ); });
 
-    const int kx = band(x, m.nx, m.pml), ky = band(y, m.ny, m.pml), kz = band(z, m.nz, m.pml);
+    const int kx = band(x, m.nx, m.pml), ky = band(y, m.ny, m.pml), kz = bandz(m, z);
     if (!(kx | ky | kz)) {
         m.f[0][ci] = __fmaf_rn(ph.dt * bx, (xX + xY) + xZ, m.f[0][ci]);
         m.f[1][ci] = __fmaf_rn(ph.dt * by, (yX + yY) + yZ, m.f[1][ci]);
@@ -119,7 +119,7 @@ __global__ void __launch_bounds__(kBX * kBY) k_stress(Model m, Physics ph) {
     const float mxz = hmean<FAST>(r[0], r[1], r[SZ], ref ? r[1 + SY] : r[1 + SZ]);
     const float myz = hmean<FAST>(r[0], r[SY], r[SZ], r[SY + SZ]);
 
-    const int kx = band(x, m.nx, m.pml), ky = band(y, m.ny, m.pml), kz = band(z, m.nz, m.pml);
+    const int kx = band(x, m.nx, m.pml), ky = band(y, m.ny, m.pml), kz = bandz(m, z);
     if (!(kx | ky | kz)) {
         m.f[3][ci] = __fmaf_rn(ph.dt, __fmaf_rn(l2m, dXx, l * (dYy + dZz)), m.f[3][ci]);
         m.f[4][ci] = __fmaf_rn(ph.dt, __fmaf_rn(l2m, dYy, l * (dXx + dZz)), m.f[4][ci]);
@@ -223,20 +223,24 @@ int simple_launches_per_step(const SourceRec &sr) {
 }
 
 cudaError_t simple_step(const Model &m, const Physics &ph, const SourceRec &sr,
-                        int it, float src_value, bool use_wavelet, cudaStream_t s, cudaEvent_t *ev) {
-    if (sr.src >= 0) k_inject<<<1, 32, 0, s>>>(m, ph, sr, it, src_value, use_wavelet ? 1 : 0);
+                        int it, float src_value, bool use_wavelet, cudaStream_t s, cudaEvent_t *ev, int phases) {
     const dim3 block(kBX, kBY);
     const dim3 grid((m.nxc + kBX - 1) / kBX, (m.nyc + kBY - 1) / kBY, m.nzc);
-    if (ev) cudaEventRecord(ev[0], s);
-    if (ph.fast) k_velocity<true><<<grid, block, 0, s>>>(m, ph);
-    else k_velocity<false><<<grid, block, 0, s>>>(m, ph);
-    if (ev) cudaEventRecord(ev[1], s);
-    if (sr.nrec > 0) k_record<<<(sr.nrec + 127) / 128, 128, 0, s>>>(m, sr, it, 1);
-    if (ev) cudaEventRecord(ev[2], s);
-    if (ph.fast) k_stress<true><<<grid, block, 0, s>>>(m, ph);
-    else k_stress<false><<<grid, block, 0, s>>>(m, ph);
-    if (ev) cudaEventRecord(ev[3], s);
-    if (sr.nrec > 0) k_record<<<(sr.nrec + 127) / 128, 128, 0, s>>>(m, sr, it, 0);
+    if (phases & 1) {
+        if (sr.src >= 0) k_inject<<<1, 32, 0, s>>>(m, ph, sr, it, src_value, use_wavelet ? 1 : 0);
+        if (ev) cudaEventRecord(ev[0], s);
+        if (ph.fast) k_velocity<true><<<grid, block, 0, s>>>(m, ph);
+        else k_velocity<false><<<grid, block, 0, s>>>(m, ph);
+        if (ev) cudaEventRecord(ev[1], s);
+        if (sr.nrec > 0) k_record<<<(sr.nrec + 127) / 128, 128, 0, s>>>(m, sr, it, 1);
+    }
+    if (phases & 2) {
+        if (ev) cudaEventRecord(ev[2], s);
+        if (ph.fast) k_stress<true><<<grid, block, 0, s>>>(m, ph);
+        else k_stress<false><<<grid, block, 0, s>>>(m, ph);
+        if (ev) cudaEventRecord(ev[3], s);
+        if (sr.nrec > 0) k_record<<<(sr.nrec + 127) / 128, 128, 0, s>>>(m, sr, it, 0);
+    }
     return cudaGetLastError();
 }
 

@@ -318,6 +318,23 @@ __device__ __forceinline__ bool vel_item(const ZMaps &mp, const Model &m, const 
     int cz = t.zs;
     const bool src_near = !H && sr.src >= 0 && sy >= t.gy0 - 5 && sy < t.gy0 + TY + 5 && sx >= t.gx0 - 8 &&
                           sx < t.gx0 + TX + 8;
+    // The PML cells' splits and damping medium into L2 two planes ahead of
+    // their plain loads (32 x 8 tiles: a warp's cells are one row).
+    auto prefetch = [&](int pz) {
+        if constexpr (CELLS == 1) {
+            if (pz >= t.ze) return;
+            const int kzp = bandz(m, pz + kHalo);
+            if (!t.xy_pml && kzp == 0) return;
+            const bool p = act[0] && (kx | kyc[0] | kzp);
+            if (prefetch_split_rows(spl(), p, pml_plane_index(m, pcol[0], pz), 0, kNumVelSplit, lx) && lx == 0) {
+                const uint32_t r = col[0] + (uint32_t)(pz + kHalo) * PL;
+                l2_prefetch(m.mu + r, TX * 4);
+                if (ph.damping == 1) l2_prefetch(m.lam + r, TX * 4);
+            }
+        }
+    };
+    prefetch(t.zs);
+    prefetch(t.zs + 1);
     // One plane.  GEN selects the general path (PML cells, source, receivers);
     // the interior-only path is used for every other tile-plane.  Returns
     // false when the block votes to abort.
@@ -326,7 +343,7 @@ __device__ __forceinline__ bool vel_item(const ZMaps &mp, const Model &m, const 
         const int s = stage;
         unsigned char *st = smem + s * LS::STAGE;
         const int gz = cz + kHalo;
-        const int kz = band(gz, m.nz, m.pml);
+        const int kz = bandz(m, gz);
         const bool plane_pml = GEN && (t.xy_pml || kz != 0);
 
 
@@ -552,7 +569,8 @@ __device__ __forceinline__ bool vel_item(const ZMaps &mp, const Model &m, const 
     };
     for (; cz < t.ze; ++cz) {
         const int gzp = cz + kHalo;
-        const bool gen = t.xy_pml || band(gzp, m.nz, m.pml) != 0 || (src_near && (gzp == sz || gzp + 5 == sz)) || gzp == rz;
+        const bool gen = t.xy_pml || bandz(m, gzp) != 0 || (src_near && (gzp == sz || gzp + 5 == sz)) || gzp == rz;
+        prefetch(cz + 2);
         if (!(gen ? plane(std::true_type{}) : plane(std::false_type{}))) {
             abort = true;
             break;
@@ -718,6 +736,21 @@ __device__ __forceinline__ bool str_item(const ZMaps &mp, const Model &m, const 
     int cz = t.zs;
     int sz = -1;
     if (src >= 0) sz = (int)(src / m.plane);
+    // The PML cells' splits and buoyancy, loaded by plain loads after the
+    // stencil, are brought into L2 two planes ahead (32 x 8 tiles: a warp's
+    // cells are one row): their loads then wait on L2 rather than on HBM.
+    auto prefetch = [&](int pz) {
+        if constexpr (CELLS == 1) {
+            if (pz >= t.ze) return;
+            const int kzp = bandz(m, pz + kHalo);
+            if (!t.xy_pml && kzp == 0) return;
+            const bool p = act[0] && (kx | kyc[0] | kzp);
+            if (prefetch_split_rows(spl(), p, pml_plane_index(m, pcol[0], pz), S_XXX, kNumSplit, lx) && lx == 0)
+                l2_prefetch(m.b + col[0] + (uint32_t)(pz + kHalo) * PL, TX * 4);
+        }
+    };
+    prefetch(t.zs);
+    prefetch(t.zs + 1);
     // One plane, as in the velocity update (GEN: general path; P: place in
     // the pair).  Returns false when the block votes to abort.
     auto plane = [&](auto gen_tag, auto p_tag) -> bool {
@@ -726,7 +759,7 @@ __device__ __forceinline__ bool str_item(const ZMaps &mp, const Model &m, const 
         const int s = stage;
         unsigned char *st = smem + s * LS::STAGE;
         const int gz = cz + kHalo;
-        const int kz = band(gz, m.nz, m.pml);
+        const int kz = bandz(m, gz);
         const bool plane_pml = GEN && (t.xy_pml || kz != 0);
 
         if (!mbar_wait(&bar[s], MANY ? (pbits >> s) & 1u : parity)) failed = true;
@@ -918,7 +951,8 @@ __device__ __forceinline__ bool str_item(const ZMaps &mp, const Model &m, const 
     };
     auto run = [&](auto p_tag) -> bool {
         const int gzp = cz + kHalo;
-        const bool gen = t.xy_pml || band(gzp, m.nz, m.pml) != 0 || gzp == sz || gzp == rz;
+        const bool gen = t.xy_pml || bandz(m, gzp) != 0 || gzp == sz || gzp == rz;
+        prefetch(cz + 2);
         return gen ? plane(std::true_type{}, p_tag) : plane(std::false_type{}, p_tag);
     };
     while (cz < t.ze) {
@@ -1157,14 +1191,18 @@ void launch16(const Model &m, const Physics &ph, const SourceRec &sr, const Half
 
 template <bool FAST, int CELLS>
 void launch(const Model &m, const Physics &ph, const SourceRec &sr, const ZGeom &g, const ZMaps &zm, int it,
-            float src_value, int uw, cudaStream_t s, cudaEvent_t *ev) {
+            float src_value, int uw, cudaStream_t s, cudaEvent_t *ev, int phases) {
     const dim3 grid(g.ntx * g.nty, g.nchunks);
-    if (ev) cudaEventRecord(ev[0], s);
-    k_velocity_zmarch<FAST, CELLS><<<grid, NT, vel_smem<CELLS>(), s>>>(zm, m, ph, g, sr, it, src_value, uw);
-    if (ev) cudaEventRecord(ev[1], s);
-    if (ev) cudaEventRecord(ev[2], s);
-    k_stress_zmarch<FAST, CELLS><<<grid, NT, str_smem<CELLS>(), s>>>(zm, m, ph, g, sr, it, src_value, uw);
-    if (ev) cudaEventRecord(ev[3], s);
+    if (phases & 1) {
+        if (ev) cudaEventRecord(ev[0], s);
+        k_velocity_zmarch<FAST, CELLS><<<grid, NT, vel_smem<CELLS>(), s>>>(zm, m, ph, g, sr, it, src_value, uw);
+        if (ev) cudaEventRecord(ev[1], s);
+    }
+    if (phases & 2) {
+        if (ev) cudaEventRecord(ev[2], s);
+        k_stress_zmarch<FAST, CELLS><<<grid, NT, str_smem<CELLS>(), s>>>(zm, m, ph, g, sr, it, src_value, uw);
+        if (ev) cudaEventRecord(ev[3], s);
+    }
 }
 
 }  // namespace
@@ -1307,7 +1345,7 @@ void zmarch_tiles(const Model &m, int cells, int *ntx, int *nty) {
 
 cudaError_t zmarch_step(const Model &m, const Physics &ph, const SourceRec &sr, const ZGeom &g, const ZMaps &zm,
                         int it, float src_value, bool use_wavelet, cudaStream_t s, cudaEvent_t *ev,
-                        const HalfState *hs) {
+                        const HalfState *hs, int phases) {
     if (hs) {
         if (hs->storage == SGFD_STORE_BF16) {
             if (ph.fast) launch16<true, SGFD_STORE_BF16>(m, ph, sr, *hs, g, zm, it, src_value, use_wavelet, s, ev);
@@ -1320,11 +1358,11 @@ cudaError_t zmarch_step(const Model &m, const Physics &ph, const SourceRec &sr, 
     }
     const int uw = use_wavelet ? 1 : 0;
     if (ph.fast) {
-        if (g.cells == 1) launch<true, 1>(m, ph, sr, g, zm, it, src_value, uw, s, ev);
-        else launch<true, 2>(m, ph, sr, g, zm, it, src_value, uw, s, ev);
+        if (g.cells == 1) launch<true, 1>(m, ph, sr, g, zm, it, src_value, uw, s, ev, phases);
+        else launch<true, 2>(m, ph, sr, g, zm, it, src_value, uw, s, ev, phases);
     } else {
-        if (g.cells == 1) launch<false, 1>(m, ph, sr, g, zm, it, src_value, uw, s, ev);
-        else launch<false, 2>(m, ph, sr, g, zm, it, src_value, uw, s, ev);
+        if (g.cells == 1) launch<false, 1>(m, ph, sr, g, zm, it, src_value, uw, s, ev, phases);
+        else launch<false, 2>(m, ph, sr, g, zm, it, src_value, uw, s, ev, phases);
     }
     return cudaGetLastError();
 }

@@ -418,7 +418,7 @@ __device__ __forceinline__ bool vel_pair(const VelMaps &mp, const Model &m, cons
         const int s = stage;
         unsigned char *st = smem + s * L::STAGE;
         const int gz = cz + kHalo;
-        const int kz = band(gz, m.nz, m.pml);
+        const int kz = bandz(m, gz);
 
         if (mbar_wait(&bar[s], (pbits >> s) & 1u)) pbits ^= 1u << s;
         else failed = true;
@@ -615,7 +615,7 @@ __device__ __forceinline__ bool vel_pair(const VelMaps &mp, const Model &m, cons
     using T0 = std::false_type;
     for (; cz < t.ze; ++cz) {
         const int gzp = cz + kHalo;
-        const bool gen = t.xy_pml || band(gzp, m.nz, m.pml) != 0 || (src_near && (gzp == sz || gzp + 5 == sz)) ||
+        const bool gen = t.xy_pml || bandz(m, gzp) != 0 || (src_near && (gzp == sz || gzp + 5 == sz)) ||
                          gzp == rz;
         const bool odd = ((cz - t.zs) & 1) != 0;
         const bool ok = odd ? (gen ? plane(T1{}, T1{}) : plane(T0{}, T1{})) : (gen ? plane(T1{}, T0{}) : plane(T0{}, T0{}));
@@ -719,7 +719,7 @@ __device__ __forceinline__ bool str_pair(const StrMaps &mp, const Model &m, cons
         const int s = stage;
         unsigned char *st = smem + s * L::STAGE;
         const int gz = cz + kHalo;
-        const int kz = band(gz, m.nz, m.pml);
+        const int kz = bandz(m, gz);
 
         if (mbar_wait(&bar[s], (pbits >> s) & 1u)) pbits ^= 1u << s;
         else failed = true;
@@ -908,7 +908,7 @@ __device__ __forceinline__ bool str_pair(const StrMaps &mp, const Model &m, cons
     using T0 = std::false_type;
     for (; cz < t.ze; ++cz) {
         const int gzp = cz + kHalo;
-        const bool gen = t.xy_pml || band(gzp, m.nz, m.pml) != 0 || gzp == sz || gzp == rz;
+        const bool gen = t.xy_pml || bandz(m, gzp) != 0 || gzp == sz || gzp == rz;
         const bool odd = ((cz - t.zs) & 1) != 0;
         const bool ok = odd ? (gen ? plane(T1{}, T1{}) : plane(T0{}, T1{})) : (gen ? plane(T1{}, T0{}) : plane(T0{}, T0{}));
         if (!ok) {

@@ -944,6 +944,7 @@ int sgfd_set_learned_strip(sgfd_solver *h, int32_t width, const float *params) {
     int r = check_handle(h);
     if (r) return r;
     if (width < 0) return fail(h, SGFD_ERR_INVALID, "negative strip width");
+    if (width > 0 && h->cfg.nz_total != 0) return fail(h, SGFD_ERR_UNSUPPORTED, "a z-slab takes no learned strip");
     SG_CUDA(h, cudaStreamSynchronize(h->stream), "synchronise before changing the strip");
     cudaFree(h->strip_cells);
     cudaFree(h->strip_buf);

@@ -393,13 +393,29 @@ int sgfd_create(const sgfd_config *cfg, sgfd_solver **out) {
     if (!cfg || !out) return fail(nullptr, SGFD_ERR_INVALID, "null config or output pointer");
     *out = nullptr;
     const sgfd_config &c = *cfg;
-    for (int i = 0; i < 7; ++i)
+    for (int i = 0; i < 5; ++i)
         if (c.reserved[i] != 0) return fail(nullptr, SGFD_ERR_INVALID, "reserved config fields must be zero");
+    const bool slab = c.nz_total != 0;
+    if (slab) {
+        // the whole model must be a valid model; the slab needs its own 5 computed planes beside each cut
+        const int need_z = 2 * (kHalo + c.pml) + 1;
+        if (c.nz_total < need_z)
+            return fail(nullptr, SGFD_ERR_INVALID, "nz_total %d too small for pml %d (needs >= %d)", c.nz_total,
+                        c.pml, need_z);
+        if (c.nz < 3 * kHalo || c.z_offset < 0 || (int64_t)c.z_offset + c.nz - 2 * kHalo > c.nz_total - 2 * kHalo)
+            return fail(nullptr, SGFD_ERR_INVALID,
+                        "z-slab of %d GRID planes at computed offset %d does not fit a model of %d GRID planes "
+                        "(a slab needs >= %d computed planes)", c.nz, c.z_offset, c.nz_total, kHalo);
+        if (c.storage != SGFD_STORE_F32)
+            return fail(nullptr, SGFD_ERR_UNSUPPORTED, "z-slabs need FP32 storage");
+    } else if (c.z_offset != 0) {
+        return fail(nullptr, SGFD_ERR_INVALID, "z_offset needs nz_total");
+    }
     if (c.arith != SGFD_ARITH_REF && c.arith != SGFD_ARITH_FAST)
         return fail(nullptr, SGFD_ERR_INVALID, "unknown arithmetic mode %d", c.arith);
     if (c.pml < 0) return fail(nullptr, SGFD_ERR_INVALID, "pml must be >= 0 (got %d)", c.pml);
     const int need = 2 * (kHalo + c.pml) + 1;
-    if (c.nx < need || c.ny < need || c.nz < need)
+    if (c.nx < need || c.ny < need || (!slab && c.nz < need))
         return fail(nullptr, SGFD_ERR_INVALID, "grid %dx%dx%d too small for pml %d (each axis needs >= %d)",
                     c.nx, c.ny, c.nz, c.pml, need);
     if (!finite_pos(c.dt) || !finite_pos(c.dx) || !finite_pos(c.dy) || !finite_pos(c.dz))
@@ -446,7 +462,10 @@ int sgfd_create(const sgfd_config *cfg, sgfd_solver **out) {
     m.pml = c.pml;
     m.nxc = c.nx - 2 * kHalo; m.nyc = c.ny - 2 * kHalo; m.nzc = c.nz - 2 * kHalo;
     m.plane = (int64_t)m.px * m.ny;
-    m.npml = pml_count(m.nxc, m.nyc, m.nzc, m.pml);
+    m.zoff = slab ? c.z_offset : 0;
+    m.nzcg = slab ? c.nz_total - 2 * kHalo : m.nzc;
+    m.pbase = pml_before(m.nxc, m.nyc, m.nzcg, m.pml, m.zoff);
+    m.npml = pml_before(m.nxc, m.nyc, m.nzcg, m.pml, m.zoff + m.nzc) - m.pbase;
     const size_t arr_bytes = array_bytes(m);
     const size_t pool_bytes = arr_bytes * 16;
     e = dev_malloc(h, &h->field_pool, pool_bytes);
@@ -718,6 +737,68 @@ int sgfd_run(sgfd_solver *h, int32_t it0, int32_t nsteps, int32_t use_graph) {
         if (r) return r;
     }
     return SGFD_OK;
+}
+
+int sgfd_step_phase(sgfd_solver *h, int32_t it, float source_value, int32_t phase) {
+    int r = check_handle(h);
+    if (r) return r;
+    if (!h->medium_set) return fail(h, SGFD_ERR_STATE, "sgfd_set_medium must come before stepping");
+    if (phase != SGFD_PHASE_VELOCITY && phase != SGFD_PHASE_STRESS)
+        return fail(h, SGFD_ERR_INVALID, "unknown phase %d", phase);
+    if (h->storage != SGFD_STORE_F32 || (h->kernel == SGFD_KERNEL_ZMARCH && h->zg.pair))
+        return fail(h, SGFD_ERR_UNSUPPORTED,
+                    "half steps need FP32 storage and the simple kernels or 32-column z-march tiles");
+    if (h->strip_n > 0 || h->audit_every > 0)
+        return fail(h, SGFD_ERR_UNSUPPORTED, "half steps run neither a learned strip nor a per-step audit");
+    const int phases = phase == SGFD_PHASE_VELOCITY ? 1 : 2;
+    const cudaError_t e =
+        h->kernel == SGFD_KERNEL_ZMARCH
+            ? zmarch_step(h->m, h->ph, h->sr, h->zg, h->zm, it, source_value, false, h->stream, nullptr, nullptr,
+                          phases)
+            : simple_step(h->m, h->ph, h->sr, it, source_value, false, h->stream, nullptr, phases);
+    if (e != cudaSuccess) return cuda_fail(h, e, "half-step launch");
+    return SGFD_OK;
+}
+
+int sgfd_halo_bytes(const sgfd_solver *h, int64_t *bytes) {
+    if (!h || !bytes) return fail(nullptr, SGFD_ERR_INVALID, "null handle or output pointer");
+    *bytes = 3 * (int64_t)kHalo * h->m.plane * (int64_t)sizeof(float);
+    return SGFD_OK;
+}
+
+namespace {
+
+// The three fields of one halo kind, 5 padded GRID planes each, between the
+// slab and buf: pack reads the slab's own computed planes beside the cut,
+// unpack writes its frame planes there.  The 5 planes of a field are one
+// contiguous range of its padded array.
+int halo_copy(sgfd_solver *h, int32_t side, int32_t kind, void *buf, bool pack) {
+    int r = check_handle(h);
+    if (r) return r;
+    if (!buf) return fail(h, SGFD_ERR_INVALID, "null halo buffer");
+    if (side != SGFD_HALO_LOW && side != SGFD_HALO_HIGH) return fail(h, SGFD_ERR_INVALID, "bad halo side %d", side);
+    if (kind != SGFD_HALO_STRESS && kind != SGFD_HALO_VELOCITY)
+        return fail(h, SGFD_ERR_INVALID, "bad halo kind %d", kind);
+    if (h->storage != SGFD_STORE_F32) return fail(h, SGFD_ERR_UNSUPPORTED, "halo exchange needs FP32 storage");
+    static const int fields[2][3] = {{SGFD_TXZ, SGFD_TYZ, SGFD_TZZ}, {SGFD_VX, SGFD_VY, SGFD_VZ}};
+    const Model &m = h->m;
+    const int z0 = side == SGFD_HALO_LOW ? (pack ? kHalo : 0) : (pack ? m.nz - 2 * kHalo : m.nz - kHalo);
+    const size_t n = (size_t)kHalo * (size_t)m.plane;
+    for (int k = 0; k < 3; ++k) {
+        float *f = m.f[fields[kind][k]] - kXOff + (int64_t)z0 * m.plane;   // padded array origin, plane z0
+        float *b = static_cast<float *>(buf) + k * n;
+        SG_CUDA(h, cudaMemcpyAsync(pack ? b : f, pack ? f : b, n * sizeof(float), cudaMemcpyDeviceToDevice,
+                                   h->stream), "halo copy");
+    }
+    return SGFD_OK;
+}
+
+}  // namespace
+
+int sgfd_halo_pack(sgfd_solver *h, int32_t side, int32_t kind, void *dst) { return halo_copy(h, side, kind, dst, true); }
+
+int sgfd_halo_unpack(sgfd_solver *h, int32_t side, int32_t kind, const void *src) {
+    return halo_copy(h, side, kind, const_cast<void *>(src), false);
 }
 
 int sgfd_prepare_run(sgfd_solver *h) {

@@ -79,6 +79,13 @@ struct Model {
     // four mu (ElasticMacro.h:110-119), computed once per medium upload
     const float *mxy, *mxz, *myz;
     float *split;        // split_elems(npml) values, blocked (split_base)
+    // z-slab of a larger model (sgfd_config.nz_total != 0): the whole model's
+    // computed planes below this slab, the whole model's computed z extent,
+    // and the whole model's compact index of the slab's first PML cell.  The
+    // PML bands and the compact PML order are the whole model's.  A model on
+    // its own: 0, nzc, 0.
+    int zoff, nzcg;
+    int64_t pbase;
 };
 
 // 16-bit wavefield storage (kernels_half.cu): fields and splits as 16-bit
@@ -135,16 +142,25 @@ __host__ __device__ inline int band(int i, int n, int pml) {
     return 0;
 }
 
-// Compact index of a PML cell given computed coordinates (cx, cy, cz).
+// Band distance along z of GRID plane gz, counted in the whole model's planes
+// (a z-slab's PML is the whole model's).
+__host__ __device__ inline int bandz(const Model &m, int gz) {
+    return band(gz + m.zoff, m.nzcg + 2 * kHalo, m.pml);
+}
+
+// Compact index of a PML cell given computed coordinates (cx, cy, cz), in
+// the model's own split array (a z-slab's part of the whole model's order).
 __host__ __device__ inline int64_t pml_index(const Model &m, int cx, int cy, int cz) {
     const int p = m.pml;
     const int64_t full = (int64_t)m.nxc * m.nyc;
     const int64_t ring = (int64_t)2 * p * m.nxc + (int64_t)(m.nyc - 2 * p) * 2 * p;
+    const int z = cz + m.zoff;
     int64_t base;
     bool full_plane;
-    if (cz < p) { base = cz * full; full_plane = true; }
-    else if (cz < m.nzc - p) { base = p * full + (int64_t)(cz - p) * ring; full_plane = false; }
-    else { base = p * full + (int64_t)(m.nzc - 2 * p) * ring + (int64_t)(cz - (m.nzc - p)) * full; full_plane = true; }
+    if (z < p) { base = z * full; full_plane = true; }
+    else if (z < m.nzcg - p) { base = p * full + (int64_t)(z - p) * ring; full_plane = false; }
+    else { base = p * full + (int64_t)(m.nzcg - 2 * p) * ring + (int64_t)(z - (m.nzcg - p)) * full; full_plane = true; }
+    base -= m.pbase;
     if (full_plane) return base + (int64_t)cy * m.nxc + cx;
     if (cy < p) return base + (int64_t)cy * m.nxc + cx;
     if (cy < m.nyc - p) {
@@ -187,15 +203,19 @@ __host__ __device__ inline PmlColumn pml_column(const Model &m, int cx, int cy) 
     else c.ring_off = (uint32_t)(p * m.nxc + (m.nyc - 2 * p) * 2 * p + (cy - (m.nyc - p)) * m.nxc + cx);
     return c;
 }
-// Index of the PML cell of column c in computed plane cz.
+// Index of the PML cell of column c in computed plane cz.  Modulo 2^32: a
+// z-slab's whole-model index may wrap, its difference with pbase (the
+// slab's own index, below 2^32) does not.
 __host__ __device__ inline uint32_t pml_plane_index(const Model &m, const PmlColumn &c, int cz) {
     const uint32_t p = (uint32_t)m.pml;
     const uint32_t full = (uint32_t)m.nxc * (uint32_t)m.nyc;
     const uint32_t ring = 2u * p * (uint32_t)m.nxc + (uint32_t)(m.nyc - 2 * m.pml) * 2u * p;
-    const uint32_t z = (uint32_t)cz;
-    if (cz < m.pml) return z * full + c.full_off;
-    if (cz < m.nzc - m.pml) return p * full + (z - p) * ring + c.ring_off;
-    return p * full + (uint32_t)(m.nzc - 2 * m.pml) * ring + (z - (uint32_t)(m.nzc - m.pml)) * full + c.full_off;
+    const int zi = cz + m.zoff;
+    const uint32_t z = (uint32_t)zi, pb = (uint32_t)m.pbase;
+    if (zi < m.pml) return z * full + c.full_off - pb;
+    if (zi < m.nzcg - m.pml) return p * full + (z - p) * ring + c.ring_off - pb;
+    return p * full + (uint32_t)(m.nzcg - 2 * m.pml) * ring + (z - (uint32_t)(m.nzcg - m.pml)) * full + c.full_off -
+           pb;
 }
 
 __host__ inline int64_t pml_count(int nxc, int nyc, int nzc, int p) {
@@ -203,15 +223,26 @@ __host__ inline int64_t pml_count(int nxc, int nyc, int nzc, int p) {
     const int64_t ring = (int64_t)2 * p * nxc + (int64_t)(nyc - 2 * p) * 2 * p;
     return 2 * p * full + (int64_t)(nzc - 2 * p) * ring;
 }
+// PML cells in computed planes [0, z) of a model of nzc computed planes
+// (where a z-slab starting at plane z starts in the compact order).
+__host__ inline int64_t pml_before(int nxc, int nyc, int nzc, int p, int z) {
+    const int64_t full = (int64_t)nxc * nyc;
+    const int64_t ring = (int64_t)2 * p * nxc + (int64_t)(nyc - 2 * p) * 2 * p;
+    const int lo = z < p ? z : p;
+    const int mid = z - p < 0 ? 0 : (z - p < nzc - 2 * p ? z - p : nzc - 2 * p);
+    const int hi = z - (nzc - p) < 0 ? 0 : z - (nzc - p);
+    return (int64_t)(lo + hi) * full + (int64_t)mid * ring;
+}
 
 // ---- kernel family entry points (host side) -------------------------------
 
 // "simple": one thread per computed cell.
 // ev (optional, 4 events): recorded before/after the velocity kernel and
-// before/after the stress kernel.
+// before/after the stress kernel.  phases: bit 0 the source injection, the
+// velocity update and its receivers, bit 1 the stress update and its receivers.
 cudaError_t simple_step(const Model &m, const Physics &ph, const SourceRec &sr,
                         int it, float src_value, bool use_wavelet, cudaStream_t s,
-                        cudaEvent_t *ev = nullptr);
+                        cudaEvent_t *ev = nullptr, int phases = 3);
 int simple_launches_per_step(const SourceRec &sr);
 
 // medium post-processing: rmu = 1/mu over the padded arrays, then the three

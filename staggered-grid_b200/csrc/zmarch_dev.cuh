@@ -8,6 +8,8 @@
 
 #include <cstdint>
 
+#include "sgfd_internal.h"
+
 namespace sgfd {
 namespace zdev {
 
@@ -55,6 +57,29 @@ __device__ __forceinline__ void tma4(void *dst, const CUtensorMap *map, int x, i
         "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];"
         ::"r"(sptr(dst)), "l"(map), "r"(x), "r"(y), "r"(z), "r"(w), "r"(sptr(bar))
         : "memory");
+}
+
+// Bring [p, p + bytes) into L2 (p 16-byte aligned, bytes a multiple of 16).
+// A hint: it returns no data and completes on no barrier.
+__device__ __forceinline__ void l2_prefetch(const void *p, uint32_t bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
+
+// Warp-wide, all lanes: for the lanes whose cell is a PML cell (pml) with
+// compact index idx, bring rows [k0, k1) of every split block those cells
+// lie in into L2 (one bulk prefetch per block, from lanes 0, 1, ...).
+// Returns whether any lane's cell is a PML cell.
+template <class T>
+__device__ __forceinline__ bool prefetch_split_rows(const T *split, bool pml, uint32_t idx, int k0, int k1,
+                                                    int lane) {
+    const uint32_t lo = __reduce_min_sync(0xffffffffu, pml ? idx : 0xffffffffu);
+    if (lo == 0xffffffffu) return false;
+    const uint32_t hi = __reduce_max_sync(0xffffffffu, pml ? idx : 0u);
+    const uint32_t b0 = lo / kSplitBlock;
+    if ((uint32_t)lane <= hi / kSplitBlock - b0)
+        l2_prefetch(split + (size_t)(b0 + lane) * (kNumSplit * kSplitBlock) + k0 * kSplitBlock,
+                    (uint32_t)((k1 - k0) * kSplitBlock * sizeof(T)));
+    return true;
 }
 
 // Wait (bounded) for the stages still in flight before an early exit:

@@ -35,6 +35,9 @@ STORE_F32, STORE_BF16, STORE_F16 = range(3)
 KERNEL_AUTO, KERNEL_SIMPLE, KERNEL_ZMARCH = range(3)
 ARITH_REF, ARITH_FAST = range(2)
 REGION_COMPUTED, REGION_INTERIOR, REGION_PML = range(3)
+HALO_LOW, HALO_HIGH = range(2)             # the cut below / above a z-slab
+HALO_STRESS, HALO_VELOCITY = range(2)      # txz, tyz, tzz / vx, vy, vz
+PHASE_VELOCITY, PHASE_STRESS = range(2)
 
 # sgfd_status
 OK, ERR_INVALID, ERR_ALLOC, ERR_CUDA, ERR_STATE, ERR_UNSUPPORTED, ERR_NO_DEVICE, ERR_NONFINITE = range(8)
@@ -51,7 +54,8 @@ class Config(ctypes.Structure):
         ("coef", ctypes.c_float * 5),
         ("damping", ctypes.c_int32), ("damping_R", ctypes.c_float), ("damping_vconst", ctypes.c_float),
         ("quirks", ctypes.c_int32), ("storage", ctypes.c_int32), ("kernel", ctypes.c_int32),
-        ("device", ctypes.c_int32), ("arith", ctypes.c_int32), ("reserved", ctypes.c_int32 * 7),
+        ("device", ctypes.c_int32), ("arith", ctypes.c_int32), ("nz_total", ctypes.c_int32),
+        ("z_offset", ctypes.c_int32), ("reserved", ctypes.c_int32 * 5),
     ]
 
 
@@ -96,6 +100,10 @@ def lib() -> ctypes.CDLL:
         "sgfd_set_receivers": (ctypes.c_int, [vp, i32, ip, ip, i32]),
         "sgfd_set_wavelet": (ctypes.c_int, [vp, i32, fp]),
         "sgfd_step": (ctypes.c_int, [vp, i32, ctypes.c_float]),
+        "sgfd_step_phase": (ctypes.c_int, [vp, i32, ctypes.c_float, i32]),
+        "sgfd_halo_bytes": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_int64)]),
+        "sgfd_halo_pack": (ctypes.c_int, [vp, i32, i32, vp]),
+        "sgfd_halo_unpack": (ctypes.c_int, [vp, i32, i32, vp]),
         "sgfd_run": (ctypes.c_int, [vp, i32, i32, i32]),
         "sgfd_synchronize": (ctypes.c_int, [vp]),
         "sgfd_reset": (ctypes.c_int, [vp]),
@@ -259,6 +267,25 @@ class Solver:
 
     def step(self, it: int, value: float):
         self._check(lib().sgfd_step(self.h, it, value))
+
+    def step_phase(self, it: int, value: float, phase: int):
+        """Half a step: PHASE_VELOCITY (source, velocity update, velocity
+        receivers) or PHASE_STRESS (stress update, stress receivers)."""
+        self._check(lib().sgfd_step_phase(self.h, it, value, phase))
+
+    def halo_bytes(self) -> int:
+        """Bytes of one halo buffer of a z-slab (3 fields x 5 padded planes)."""
+        n = ctypes.c_int64()
+        self._check(lib().sgfd_halo_bytes(self.h, ctypes.byref(n)))
+        return n.value
+
+    def halo_pack(self, side: int, kind: int, dst_ptr: int):
+        """The slab's own 5 planes beside cut `side` to the device buffer at dst_ptr."""
+        self._check(lib().sgfd_halo_pack(self.h, side, kind, dst_ptr))
+
+    def halo_unpack(self, side: int, kind: int, src_ptr: int):
+        """A received device buffer into the slab's 5 frame planes on `side`."""
+        self._check(lib().sgfd_halo_unpack(self.h, side, kind, src_ptr))
 
     def run(self, it0: int, nsteps: int, graph: bool = True):
         self._check(lib().sgfd_run(self.h, it0, nsteps, 1 if graph else 0))

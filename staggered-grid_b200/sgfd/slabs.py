@@ -1,0 +1,314 @@
+"""z-slabs: one model split along z over several solver handles.
+
+The reference runs one model on one GPU and caps it at 2^29 cells with a
+32-bit `memsize` (3DGPUwithPML_1DArraySingleGPU_optimization/
+ElasticWaveEquation.cu:20,143).  Here a model of GRID nx x ny x nz_total is
+cut along z into slabs of whole computed planes; each slab is an sgfd handle
+(sgfd_config.nz_total / z_offset) that keeps the whole model's PML bands and
+compact split order.  At every cut the two slabs trade the 5 planes next to it
+(the reach of the 10th-order z differences) twice per step:
+
+    for every slab: exchange txz, tyz, tzz  (HALO_STRESS)
+                    velocity half step      (PHASE_VELOCITY)
+                    exchange vx, vy, vz     (HALO_VELOCITY)
+                    stress half step        (PHASE_STRESS)
+
+which gives the whole model's results bit for bit (the updates of a cell read
+only its 10-cell neighbourhood, and every value a slab reads at its frame is
+the neighbour's value of the same half step).
+
+Two forms share the plan and the step sequence:
+  * SlabModel — all slabs in one process on one GPU, halos moved by device
+    copies on one stream;
+  * DistributedSlab — one slab per rank (one process per GPU, torch.distributed
+    over NCCL), halos moved by send/recv to the ranks above and below
+    (exchange_remote, also run on CPU tensors over gloo by the tests).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import (Config, Solver, HALO_LOW, HALO_HIGH, HALO_STRESS, HALO_VELOCITY, PHASE_VELOCITY, PHASE_STRESS)
+
+HALO = 5            # planes exchanged at a cut (the reference `order`)
+MIN_PLANES = HALO   # computed planes a slab needs to fill its neighbour's frame
+
+
+def plan_cuts(nz_total: int, nslabs: int, src_z: int | None = None, weights=None) -> list[tuple[int, int]]:
+    """Computed-plane ranges (z_offset, planes) of nslabs slabs of a model with
+    nz_total GRID planes, in z order, sized in proportion to `weights` (equal by
+    default; e.g. the free memory of each slab's GPU).  A source at GRID plane
+    src_z must lie 5 or more planes from every cut, because its injection is
+    applied inside the owning slab only: a cut that lands closer is moved past
+    it."""
+    nzc = nz_total - 2 * HALO
+    if nslabs < 1:
+        raise ValueError("nslabs must be >= 1")
+    if nzc < nslabs * MIN_PLANES:
+        raise ValueError(f"{nzc} computed planes cannot make {nslabs} slabs of >= {MIN_PLANES} planes")
+    w = np.ones(nslabs) if weights is None else np.asarray(weights, dtype=np.float64)
+    if len(w) != nslabs or np.any(w <= 0):
+        raise ValueError("one positive weight per slab")
+    cuts = [int(round(nzc * float(np.sum(w[:k])) / float(np.sum(w)))) for k in range(1, nslabs)]
+    if src_z is not None:
+        zs = src_z - HALO
+        for k, c in enumerate(cuts):
+            if c - HALO <= zs < c + HALO:
+                lo = cuts[k - 1] if k > 0 else 0
+                hi = cuts[k + 1] if k + 1 < len(cuts) else nzc
+                options = [zs - HALO, zs + HALO + 1]   # the source HALO planes above / below the cut
+                ok = [o for o in options if o - lo >= MIN_PLANES and hi - o >= MIN_PLANES]
+                if not ok:
+                    raise ValueError(f"no cut near plane {c} keeps the source plane {src_z} {HALO} planes away")
+                cuts[k] = min(ok, key=lambda o: abs(o - c))
+    edges = [0] + cuts + [nzc]
+    out = [(edges[k], edges[k + 1] - edges[k]) for k in range(nslabs)]
+    if any(n < MIN_PLANES for _, n in out):
+        raise ValueError(f"slab sizes {[n for _, n in out]}: each needs >= {MIN_PLANES} planes")
+    return out
+
+
+def slab_config(cfg: Config, z_offset: int, planes: int, device: int | None = None) -> Config:
+    """The handle configuration of one slab of the whole model `cfg`."""
+    c = Config.from_buffer_copy(cfg)
+    c.nz_total = cfg.nz
+    c.z_offset = z_offset
+    c.nz = planes + 2 * HALO
+    if device is not None:
+        c.device = device
+    return c
+
+
+def split_receivers(cuts, xyz, comp):
+    """Receivers per slab: (indices into the whole list, slab-local xyz, comp)."""
+    xyz = np.asarray(xyz, dtype=np.int32).reshape(-1, 3)
+    comp = np.asarray(comp, dtype=np.int32).reshape(-1)
+    cz = xyz[:, 2] - HALO
+    out = []
+    for z0, n in cuts:
+        idx = np.nonzero((cz >= z0) & (cz < z0 + n))[0]
+        local = xyz[idx].copy()
+        local[:, 2] -= z0
+        out.append((idx, local, comp[idx]))
+    return out
+
+
+def source_slab(cuts, z: int) -> int:
+    """Index of the slab holding GRID plane z (a computed plane)."""
+    cz = z - HALO
+    for k, (z0, n) in enumerate(cuts):
+        if z0 <= cz < z0 + n:
+            return k
+    raise ValueError(f"plane {z} is not a computed plane")
+
+
+def check_source(cuts, z: int):
+    cz = z - HALO
+    for z0, _ in cuts[1:]:
+        if z0 - HALO <= cz < z0 + HALO:
+            raise ValueError(f"source plane {z} lies within {HALO} planes of the cut at computed plane {z0}")
+
+
+def exchange_remote(send_lo, send_hi, recv_lo, recv_hi, rank: int, world: int, group=None):
+    """Trade halo buffers with the ranks below (rank - 1) and above (rank + 1):
+    send_lo goes down and arrives as that rank's recv_hi, send_hi goes up and
+    arrives as its recv_lo.  Tensors on the backend's device (CUDA over NCCL,
+    CPU over gloo); every rank posts its sends and receives together."""
+    import torch.distributed as dist
+    ops = []
+    if rank > 0:
+        ops.append(dist.P2POp(dist.isend, send_lo, rank - 1, group))
+        ops.append(dist.P2POp(dist.irecv, recv_lo, rank - 1, group))
+    if rank < world - 1:
+        ops.append(dist.P2POp(dist.isend, send_hi, rank + 1, group))
+        ops.append(dist.P2POp(dist.irecv, recv_hi, rank + 1, group))
+    if ops:
+        for w in dist.batch_isend_irecv(ops):
+            w.wait()
+
+
+class _Slabs:
+    """What both forms share: the plan, the per-slab inputs and the step."""
+
+    def __init__(self, cfg: Config, cuts):
+        self.cfg = cfg
+        self.cuts = list(cuts)
+        self.nx, self.ny, self.nz = cfg.nx, cfg.ny, cfg.nz
+        self.src_slab = -1
+        self.rec_parts = None
+        self.nrec = 0
+        self.nt = 0
+
+    # GRID planes of slab k in the whole model: [z0, z0 + planes + 10)
+    def _grid_planes(self, k):
+        z0, n = self.cuts[k]
+        return z0, z0 + n + 2 * HALO
+
+
+class SlabModel(_Slabs):
+    """All slabs of one model in this process, on one GPU (cfg.device): they
+    share that device's current stream, and halos move by device copies
+    between the slabs' buffers.  Slabs on several GPUs: DistributedSlab."""
+
+    def __init__(self, cfg: Config, cuts):
+        super().__init__(cfg, cuts)
+        import torch
+        devs = [cfg.device] * len(self.cuts)
+        self.devices = devs
+        self.slabs = []
+        self.bufs = []          # per slab: (buffer of its LOW side, buffer of its HIGH side)
+        self._torch = torch
+        try:
+            for (z0, n), d in zip(self.cuts, devs):
+                s = Solver(slab_config(cfg, z0, n, d))
+                s.set_stream(torch.cuda.current_stream(d).cuda_stream)
+                nbytes = s.halo_bytes()
+                self.bufs.append(tuple(torch.empty(nbytes // 4, dtype=torch.float32, device=f"cuda:{d}")
+                                       for _ in range(2)))
+                self.slabs.append(s)
+        except Exception:
+            self.close()
+            raise
+
+    def close(self):
+        for s in self.slabs:
+            s.close()
+        self.slabs = []
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def set_medium(self, b, lam, mu):
+        arrs = [np.asarray(a, dtype=np.float32).reshape(self.nz, self.ny, self.nx) for a in (b, lam, mu)]
+        for k, s in enumerate(self.slabs):
+            g0, g1 = self._grid_planes(k)
+            s.set_medium(*[a[g0:g1] for a in arrs])
+
+    def set_source(self, x: int, y: int, z: int):
+        check_source(self.cuts, z)
+        self.src_slab = source_slab(self.cuts, z)
+        self.slabs[self.src_slab].set_source(x, y, z - self.cuts[self.src_slab][0])
+
+    def set_receivers(self, xyz, comp, nt: int):
+        self.rec_parts = split_receivers(self.cuts, xyz, comp)
+        for s, (idx, local, c) in zip(self.slabs, self.rec_parts):
+            s.set_receivers(local, c, nt)
+        self.nrec = len(np.asarray(comp).reshape(-1))
+        self.nt = nt
+
+    def _exchange(self, kind: int):
+        last = len(self.slabs) - 1
+        for k, s in enumerate(self.slabs):
+            if k > 0:
+                s.halo_pack(HALO_LOW, kind, self.bufs[k][0].data_ptr())
+            if k < last:
+                s.halo_pack(HALO_HIGH, kind, self.bufs[k][1].data_ptr())
+        for k, s in enumerate(self.slabs):
+            if k > 0:
+                s.halo_unpack(HALO_LOW, kind, self.bufs[k - 1][1].data_ptr())
+            if k < last:
+                s.halo_unpack(HALO_HIGH, kind, self.bufs[k + 1][0].data_ptr())
+
+    def step(self, it: int, value: float):
+        """One step of the whole model (reference propagate())."""
+        self._exchange(HALO_STRESS)
+        for s in self.slabs:
+            s.step_phase(it, value, PHASE_VELOCITY)
+        self._exchange(HALO_VELOCITY)
+        for s in self.slabs:
+            s.step_phase(it, value, PHASE_STRESS)
+
+    def run(self, it0: int, nsteps: int, wavelet):
+        for it in range(it0, it0 + nsteps):
+            self.step(it, float(wavelet[it]))
+
+    def synchronize(self):
+        for s in self.slabs:
+            s.synchronize()
+
+    def traces(self) -> np.ndarray:
+        out = np.zeros((self.nrec, self.nt), dtype=np.float32)
+        for s, (idx, _, _) in zip(self.slabs, self.rec_parts or []):
+            if len(idx):
+                out[idx] = s.traces()
+        return out
+
+    def field(self, fid: int) -> np.ndarray:
+        """One wavefield of the whole model (GRID, frame planes zero)."""
+        out = np.zeros((self.nz, self.ny, self.nx), dtype=np.float32)
+        for k, s in enumerate(self.slabs):
+            z0, n = self.cuts[k]
+            out[HALO + z0:HALO + z0 + n] = s.field(fid)[HALO:HALO + n]
+        return out
+
+
+class DistributedSlab(_Slabs):
+    """This rank's slab of a model cut into world_size slabs (slab r on rank r,
+    its GPU the current device), halos traded with the ranks above and below
+    by exchange_remote over the default process group (NCCL)."""
+
+    def __init__(self, cfg: Config, cuts, rank: int, world: int, device: int):
+        super().__init__(cfg, cuts)
+        import torch
+        if len(self.cuts) != world:
+            raise ValueError("one slab per rank")
+        self.rank, self.world = rank, world
+        z0, n = self.cuts[rank]
+        self.s = Solver(slab_config(cfg, z0, n, device))
+        self.s.set_stream(torch.cuda.current_stream(device).cuda_stream)
+        nf = self.s.halo_bytes() // 4
+        dev = f"cuda:{device}"
+        self.send = [torch.empty(nf, dtype=torch.float32, device=dev) for _ in range(2)]
+        self.recv = [torch.empty(nf, dtype=torch.float32, device=dev) for _ in range(2)]
+
+    def close(self):
+        self.s.close()
+
+    def set_medium(self, b, lam, mu):
+        g0, g1 = self._grid_planes(self.rank)
+        self.s.set_medium(*[np.asarray(a, dtype=np.float32).reshape(self.nz, self.ny, self.nx)[g0:g1]
+                            for a in (b, lam, mu)])
+
+    def set_source(self, x: int, y: int, z: int):
+        check_source(self.cuts, z)
+        self.src_slab = source_slab(self.cuts, z)
+        if self.src_slab == self.rank:
+            self.s.set_source(x, y, z - self.cuts[self.rank][0])
+
+    def set_receivers(self, xyz, comp, nt: int):
+        self.rec_parts = split_receivers(self.cuts, xyz, comp)
+        idx, local, c = self.rec_parts[self.rank]
+        self.s.set_receivers(local, c, nt)
+        self.nrec = len(idx)
+        self.nt = nt
+
+    def _exchange(self, kind: int):
+        if self.rank > 0:
+            self.s.halo_pack(HALO_LOW, kind, self.send[0].data_ptr())
+        if self.rank < self.world - 1:
+            self.s.halo_pack(HALO_HIGH, kind, self.send[1].data_ptr())
+        exchange_remote(self.send[0], self.send[1], self.recv[0], self.recv[1], self.rank, self.world)
+        if self.rank > 0:
+            self.s.halo_unpack(HALO_LOW, kind, self.recv[0].data_ptr())
+        if self.rank < self.world - 1:
+            self.s.halo_unpack(HALO_HIGH, kind, self.recv[1].data_ptr())
+
+    def step(self, it: int, value: float):
+        self._exchange(HALO_STRESS)
+        self.s.step_phase(it, value, PHASE_VELOCITY)
+        self._exchange(HALO_VELOCITY)
+        self.s.step_phase(it, value, PHASE_STRESS)
+
+    def run(self, it0: int, nsteps: int, wavelet):
+        for it in range(it0, it0 + nsteps):
+            self.step(it, float(wavelet[it]))
+
+    def synchronize(self):
+        self.s.synchronize()
+
+    def traces(self) -> np.ndarray:
+        """This rank's receivers (rows in the order of rec_parts[rank][0])."""
+        return self.s.traces()

@@ -84,7 +84,9 @@ def test_pml_index_is_a_bijection(tmp_path):
     sizes, that the per-column/per-plane split the z-marching kernels use
     gives the same index, and that the blocked split storage (split k of cell
     c at split_base(c) + 32 k) gives every (cell, split) its own value inside
-    split_elems(npml), in 64-bit and 32-bit form."""
+    split_elems(npml), in 64-bit and 32-bit form.  Then cuts each model into
+    z-slabs: a slab's z bands, compact indices (whole-model index minus the
+    slab's base, in both forms) and PML count agree with the whole model's."""
     src = tmp_path / "t.cpp"
     src.write_text(r'''
 #include "sgfd_internal.h"
@@ -96,10 +98,13 @@ int main() {
   for (auto &s : sizes) {
     Model m{}; m.nx=s[0]; m.ny=s[1]; m.nz=s[2]; m.pml=s[3];
     m.nxc=m.nx-10; m.nyc=m.ny-10; m.nzc=m.nz-10; m.px=m.nx; m.plane=(int64_t)m.px*m.ny;
+    m.nzcg = m.nzc;
     m.npml = pml_count(m.nxc, m.nyc, m.nzc, m.pml);
+    if (pml_before(m.nxc, m.nyc, m.nzc, m.pml, m.nzc) != m.npml) { std::printf("pml_before\n"); return 1; }
     std::vector<int> hit(m.npml, 0); int64_t cnt = 0;
     for (int z=5; z<m.nz-5; ++z) for (int y=5; y<m.ny-5; ++y) for (int x=5; x<m.nx-5; ++x) {
-      int kx=band(x,m.nx,m.pml), ky=band(y,m.ny,m.pml), kz=band(z,m.nz,m.pml);
+      int kx=band(x,m.nx,m.pml), ky=band(y,m.ny,m.pml), kz=bandz(m,z);
+      if (kz != band(z,m.nz,m.pml)) { std::printf("bandz\n"); return 1; }
       if (!(kx|ky|kz)) continue;
       if (kx<0||kx>m.pml||ky<0||ky>m.pml||kz<0||kz>m.pml) { std::printf("bad band\n"); return 1; }
       int64_t i = pml_index(m, x-5, y-5, z-5);
@@ -117,6 +122,31 @@ int main() {
         if (j < 0 || j >= (int64_t)used.size() || used[j]++) { std::printf("split slot %lld\n", (long long)j); return 1; }
         if ((int64_t)split_base32((uint32_t)c) != split_base(c) || split_of(j) != k) { std::printf("split forms\n"); return 1; }
       }
+    // z-slabs at uneven cuts (1-plane slabs included)
+    const int nzc = m.nzc;
+    const int cutsets[3][3] = {{nzc / 3, 2 * nzc / 3, nzc}, {1, nzc - 1, nzc}, {m.pml, m.pml + 1, nzc}};
+    for (auto &cs : cutsets) {
+      int64_t total = 0; int z0 = 0;
+      for (int e : cs) {
+        if (e <= z0) continue;
+        Model q = m; q.nz = (e - z0) + 10; q.nzc = e - z0; q.zoff = z0; q.nzcg = nzc;
+        q.pbase = pml_before(m.nxc, m.nyc, nzc, m.pml, z0);
+        q.npml = pml_before(m.nxc, m.nyc, nzc, m.pml, e) - q.pbase;
+        int64_t c2 = 0;
+        for (int z=5; z<q.nz-5; ++z) for (int y=5; y<m.ny-5; ++y) for (int x=5; x<m.nx-5; ++x) {
+          const int kz = bandz(q, z);
+          if (kz != band(z + z0, m.nz, m.pml)) { std::printf("slab band\n"); return 1; }
+          if (!(band(x,m.nx,m.pml) | band(y,m.ny,m.pml) | kz)) continue;
+          const int64_t i = pml_index(q, x-5, y-5, z-5);
+          if (i != pml_index(m, x-5, y-5, z-5+z0) - q.pbase || i < 0 || i >= q.npml) { std::printf("slab index\n"); return 1; }
+          if (pml_plane_index(q, pml_column(q, x-5, y-5), z-5) != (uint32_t)i) { std::printf("slab plane index\n"); return 1; }
+          ++c2;
+        }
+        if (c2 != q.npml) { std::printf("slab count\n"); return 1; }
+        total += q.npml; z0 = e;
+      }
+      if (total != m.npml) { std::printf("slab total\n"); return 1; }
+    }
   }
   std::puts("ok"); return 0;
 }

@@ -1,0 +1,93 @@
+"""z-slabs on one GPU: the model cut along z into 2 or 3 handles that trade
+5-plane halos between the half steps gives the whole model's traces and
+final wavefields BIT FOR BIT (the whole-model run is itself pinned bit for bit
+to the oracle by test_gpu_parity.py).  Cases cover a cut moved away from the
+source, a slab lying entirely inside the bottom z-PML band, slabs crossing the
+band edges, several z chunks per slab, both kernel families and both rounding
+modes."""
+import numpy as np
+import pytest
+
+from helpers import make_solver
+import sgfd
+import sgfd.slabs as sl
+import sgfd.workloads as wl
+
+pytestmark = pytest.mark.gpu
+
+CASES = [
+    # (id, small_random_case arguments, slabs or explicit cuts, kernel, z chunk, arith, source override)
+    ("two_zmarch_ref", dict(), 2, sgfd.KERNEL_ZMARCH, 0, sgfd.ARITH_REF, None),
+    ("three_simple_fast", dict(quirks=sgfd.QUIRKS_FIXED, damping=sgfd.DAMP_LOGR), 3, sgfd.KERNEL_SIMPLE, 0,
+     sgfd.ARITH_FAST, None),
+    ("pml_slab_zmarch_chunk7", dict(nx=40, ny=34, nz=60, pml=6, nt=50), [(0, 5), (5, 20), (25, 25)],
+     sgfd.KERNEL_ZMARCH, 7, sgfd.ARITH_REF, (21, 18, 45)),
+    ("three_zmarch_fast_logr", dict(nx=45, ny=38, nz=70, pml=8, nt=40, damping=sgfd.DAMP_LOGR,
+                                    quirks=sgfd.QUIRKS_FIXED), 3, sgfd.KERNEL_ZMARCH, 0, sgfd.ARITH_FAST, None),
+]
+
+
+@pytest.mark.parametrize("case", CASES, ids=[c[0] for c in CASES])
+def test_slabs_equal_whole_model(case):
+    _, kw, slabs, kernel, zchunk, arith, src = case
+    w = wl.small_random_case(**kw)
+    w.cfg["arith"] = arith
+    if src is not None:
+        w.src = src
+    cuts = sl.plan_cuts(w.cfg["nz"], slabs, src_z=w.src[2]) if isinstance(slabs, int) else slabs
+    with make_solver(w, kernel=kernel) as s:
+        if zchunk:
+            s.set_zchunk(zchunk)
+        s.run(0, w.nt)
+        s.synchronize()
+        want_tr = s.traces()
+        want = [s.field(f) for f in range(9)]
+    cfg = sgfd.default_config(**{**w.cfg, "kernel": kernel})
+    with sl.SlabModel(cfg, cuts) as m:
+        assert [sb.kernel_name() for sb in m.slabs] == [("zmarch" if kernel == sgfd.KERNEL_ZMARCH else "simple")] * len(cuts)
+        if zchunk:
+            for sb in m.slabs:
+                sb.set_zchunk(zchunk)
+        m.set_medium(w.b, w.lam, w.mu)
+        m.set_source(*w.src)
+        m.set_receivers(w.rec_xyz, w.rec_comp, w.nt)
+        m.run(0, w.nt, w.wavelet)
+        m.synchronize()
+        tr = m.traces()
+        assert np.abs(want_tr).max() > 0
+        np.testing.assert_array_equal(tr, want_tr)
+        for f in range(9):
+            np.testing.assert_array_equal(m.field(f), want[f], err_msg=sgfd.FIELD_NAMES[f])
+
+
+def test_slab_cell_counts_add_up():
+    """The slabs' PML cells (counted in the whole model's bands) add up to the whole model's."""
+    w = wl.small_random_case(nx=40, ny=34, nz=60, pml=6, nt=4)
+    cuts = [(0, 5), (5, 20), (25, 25)]
+    cfg = sgfd.default_config(**w.cfg)
+    with make_solver(w) as s:
+        n_int, n_pml = s.cell_counts()
+    with sl.SlabModel(cfg, cuts) as m:
+        counts = [sb.cell_counts() for sb in m.slabs]
+    assert sum(c[0] for c in counts) == n_int
+    assert sum(c[1] for c in counts) == n_pml
+    assert counts[0][0] == 0                      # the first slab lies inside the bottom z band
+
+
+def test_slab_configuration_errors():
+    w = wl.small_random_case(nt=4)
+    cfg = sgfd.default_config(**w.cfg)
+    bad = [dict(nz_total=cfg.nz, z_offset=0, nz=14),                   # 4 computed planes: too thin
+           dict(nz_total=cfg.nz, z_offset=cfg.nz - 10 - 4, nz=15),     # runs past the model's top
+           dict(nz_total=0, z_offset=3),                               # offset without a whole model
+           dict(nz_total=cfg.nz, z_offset=0, nz=20, storage=sgfd.STORE_F16)]
+    for kw in bad:
+        c = sgfd.default_config(**{**w.cfg, **kw})
+        with pytest.raises(sgfd.SgfdError):
+            sgfd.Solver(c)
+    c = sl.slab_config(cfg, 0, 20)
+    with sgfd.Solver(c) as s:
+        px = (cfg.nx + 27 + 31) // 32 * 32                         # padded row pitch
+        assert s.halo_bytes() == 3 * 5 * px * cfg.ny * 4
+        with pytest.raises(sgfd.SgfdError):
+            s.set_learned_strip(6, np.zeros(sgfd.lib().sgfd_mlp_param_count(), np.float32))
