@@ -417,7 +417,7 @@ def main_slabs(args, world, rank, local):
     torch.cuda.synchronize()
     n_int = sum(h.cell_counts()[0] for h in handles)
     n_pml = sum(h.cell_counts()[1] for h in handles)
-    stream = torch.cuda.current_stream()
+    stream = m.stream                     # every slab's work runs on it
     clocks = ClockSampler(None)
     clocks.start()
     barrier(world)

@@ -25,7 +25,9 @@
 //   * The velocity update loads the PML split fields of its cell into
 //     registers before the plane's TMA wait; the stress update, which needs
 //     15 of them, loads them where they are used, so that it fits the 80
-//     registers per thread of three resident CTAs per SM.
+//     registers per thread of three resident CTAs per SM, and brings them
+//     (and the buoyancy of the damping) into L2 two planes ahead: one bulk
+//     prefetch of the 15 stress rows per 32-cell split block.
 //   * 16-bit wavefield storage (ST = BF16 / F16, 32 x 8 tiles): the field
 //     boxes arrive as 16-bit values and are widened once per plane into an
 //     FP32 work buffer (float(h) * 2^e) before the same FP32 arithmetic.
@@ -318,23 +320,6 @@ __device__ __forceinline__ bool vel_item(const ZMaps &mp, const Model &m, const 
     int cz = t.zs;
     const bool src_near = !H && sr.src >= 0 && sy >= t.gy0 - 5 && sy < t.gy0 + TY + 5 && sx >= t.gx0 - 8 &&
                           sx < t.gx0 + TX + 8;
-    // The PML cells' splits and damping medium into L2 two planes ahead of
-    // their plain loads (32 x 8 tiles: a warp's cells are one row).
-    auto prefetch = [&](int pz) {
-        if constexpr (CELLS == 1) {
-            if (pz >= t.ze) return;
-            const int kzp = bandz(m, pz + kHalo);
-            if (!t.xy_pml && kzp == 0) return;
-            const bool p = act[0] && (kx | kyc[0] | kzp);
-            if (prefetch_split_rows(spl(), p, pml_plane_index(m, pcol[0], pz), 0, kNumVelSplit, lx) && lx == 0) {
-                const uint32_t r = col[0] + (uint32_t)(pz + kHalo) * PL;
-                l2_prefetch(m.mu + r, TX * 4);
-                if (ph.damping == 1) l2_prefetch(m.lam + r, TX * 4);
-            }
-        }
-    };
-    prefetch(t.zs);
-    prefetch(t.zs + 1);
     // One plane.  GEN selects the general path (PML cells, source, receivers);
     // the interior-only path is used for every other tile-plane.  Returns
     // false when the block votes to abort.
@@ -570,7 +555,6 @@ __device__ __forceinline__ bool vel_item(const ZMaps &mp, const Model &m, const 
     for (; cz < t.ze; ++cz) {
         const int gzp = cz + kHalo;
         const bool gen = t.xy_pml || bandz(m, gzp) != 0 || (src_near && (gzp == sz || gzp + 5 == sz)) || gzp == rz;
-        prefetch(cz + 2);
         if (!(gen ? plane(std::true_type{}) : plane(std::false_type{}))) {
             abort = true;
             break;

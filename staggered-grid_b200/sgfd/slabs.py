@@ -157,14 +157,17 @@ class SlabModel(_Slabs):
         self.devices = devs
         self.slabs = []
         self.bufs = []          # per slab: (buffer of its LOW side, buffer of its HIGH side)
-        self._torch = torch
+        # one stream for every slab (a null stream would give each handle its own): the packs, copies,
+        # unpacks and half steps of all slabs are ordered on it
+        self.stream = torch.cuda.Stream(device=cfg.device)
         try:
             for (z0, n), d in zip(self.cuts, devs):
                 s = Solver(slab_config(cfg, z0, n, d))
-                s.set_stream(torch.cuda.current_stream(d).cuda_stream)
+                s.set_stream(self.stream.cuda_stream)
                 nbytes = s.halo_bytes()
-                self.bufs.append(tuple(torch.empty(nbytes // 4, dtype=torch.float32, device=f"cuda:{d}")
-                                       for _ in range(2)))
+                with torch.cuda.stream(self.stream):   # the buffers belong to the stream that uses them
+                    self.bufs.append(tuple(torch.empty(nbytes // 4, dtype=torch.float32, device=f"cuda:{d}")
+                                           for _ in range(2)))
                 self.slabs.append(s)
         except Exception:
             self.close()
@@ -258,11 +261,14 @@ class DistributedSlab(_Slabs):
         self.rank, self.world = rank, world
         z0, n = self.cuts[rank]
         self.s = Solver(slab_config(cfg, z0, n, device))
-        self.s.set_stream(torch.cuda.current_stream(device).cuda_stream)
+        # the slab's work and the exchanges' send/recv are ordered on this stream
+        self.stream = torch.cuda.Stream(device=device)
+        self.s.set_stream(self.stream.cuda_stream)
         nf = self.s.halo_bytes() // 4
         dev = f"cuda:{device}"
-        self.send = [torch.empty(nf, dtype=torch.float32, device=dev) for _ in range(2)]
-        self.recv = [torch.empty(nf, dtype=torch.float32, device=dev) for _ in range(2)]
+        with torch.cuda.stream(self.stream):
+            self.send = [torch.empty(nf, dtype=torch.float32, device=dev) for _ in range(2)]
+            self.recv = [torch.empty(nf, dtype=torch.float32, device=dev) for _ in range(2)]
 
     def close(self):
         self.s.close()
@@ -290,7 +296,9 @@ class DistributedSlab(_Slabs):
             self.s.halo_pack(HALO_LOW, kind, self.send[0].data_ptr())
         if self.rank < self.world - 1:
             self.s.halo_pack(HALO_HIGH, kind, self.send[1].data_ptr())
-        exchange_remote(self.send[0], self.send[1], self.recv[0], self.recv[1], self.rank, self.world)
+        import torch
+        with torch.cuda.stream(self.stream):   # NCCL orders its send/recv after, and before, this stream's work
+            exchange_remote(self.send[0], self.send[1], self.recv[0], self.recv[1], self.rank, self.world)
         if self.rank > 0:
             self.s.halo_unpack(HALO_LOW, kind, self.recv[0].data_ptr())
         if self.rank < self.world - 1:
