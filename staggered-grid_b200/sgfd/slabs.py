@@ -147,7 +147,7 @@ class _Slabs:
 
 class SlabModel(_Slabs):
     """All slabs of one model in this process, on one GPU (cfg.device): they
-    share that device's current stream, and halos move by device copies
+    share one stream of their own (`stream`), and halos move by device copies
     between the slabs' buffers.  Slabs on several GPUs: DistributedSlab."""
 
     def __init__(self, cfg: Config, cuts):
