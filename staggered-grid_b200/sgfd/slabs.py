@@ -251,7 +251,10 @@ class SlabModel(_Slabs):
 class DistributedSlab(_Slabs):
     """This rank's slab of a model cut into world_size slabs (slab r on rank r,
     its GPU the current device), halos traded with the ranks above and below
-    by exchange_remote over the default process group (NCCL)."""
+    by exchange_remote over the default process group: NCCL moves the device
+    buffers themselves; a host backend (gloo) gets them staged through host
+    memory, which lets several ranks share one GPU, since no kernel then waits
+    on another process (the host does, in its receive)."""
 
     def __init__(self, cfg: Config, cuts, rank: int, world: int, device: int):
         super().__init__(cfg, cuts)
@@ -297,8 +300,18 @@ class DistributedSlab(_Slabs):
         if self.rank < self.world - 1:
             self.s.halo_pack(HALO_HIGH, kind, self.send[1].data_ptr())
         import torch
-        with torch.cuda.stream(self.stream):   # NCCL orders its send/recv after, and before, this stream's work
-            exchange_remote(self.send[0], self.send[1], self.recv[0], self.recv[1], self.rank, self.world)
+        import torch.distributed as dist
+        if dist.get_backend() == "nccl":
+            with torch.cuda.stream(self.stream):   # NCCL orders its send/recv after, and before, this stream's work
+                exchange_remote(self.send[0], self.send[1], self.recv[0], self.recv[1], self.rank, self.world)
+        else:
+            with torch.cuda.stream(self.stream):   # device -> host after the packs (a synchronous copy)
+                hs = [t.to("cpu") for t in self.send]
+            hr = [torch.empty_like(t) for t in hs]
+            exchange_remote(hs[0], hs[1], hr[0], hr[1], self.rank, self.world)
+            with torch.cuda.stream(self.stream):   # host -> device before the unpacks
+                for d, h in zip(self.recv, hr):
+                    d.copy_(h)
         if self.rank > 0:
             self.s.halo_unpack(HALO_LOW, kind, self.recv[0].data_ptr())
         if self.rank < self.world - 1:
@@ -320,3 +333,9 @@ class DistributedSlab(_Slabs):
     def traces(self) -> np.ndarray:
         """This rank's receivers (rows in the order of rec_parts[rank][0])."""
         return self.s.traces()
+
+    def own_planes(self, fid: int) -> tuple[int, np.ndarray]:
+        """(first computed plane, the slab's computed planes of one wavefield):
+        this rank's part of the whole model's field."""
+        z0, n = self.cuts[self.rank]
+        return z0, self.s.field(fid)[HALO:HALO + n]
