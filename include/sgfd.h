@@ -290,7 +290,8 @@ int sgfd_get_tile(const sgfd_solver *h, int32_t *tile_cols, int32_t *tile_rows, 
  * are ordered on the handle's stream.  A step of the whole model is then, per
  * slab: exchange STRESS, sgfd_step_phase(VELOCITY), exchange VELOCITY,
  * sgfd_step_phase(STRESS), and the slabs together give the whole model's
- * results bit for bit.  Each slab is given the whole model's medium on its
+ * results bit for bit (sgfd_step_phase_part splits each half step so that
+ * its inner part runs while the halos travel).  Each slab is given the whole model's medium on its
  * GRID planes (frame planes included), the receivers that lie in its planes,
  * and the source if it lies there; the source must lie 5 or more computed
  * planes from every cut (its injection is not part of the exchanged planes).
@@ -308,6 +309,16 @@ int sgfd_halo_unpack(sgfd_solver *h, int32_t side, int32_t kind, const void *src
 /* Half of sgfd_step: SGFD_PHASE_VELOCITY then SGFD_PHASE_STRESS with the same
  * it and source value is one step.  Any handle (whole model or slab). */
 int sgfd_step_phase(sgfd_solver *h, int32_t it, float source_value, int32_t phase);
+/* Part of a half step, to overlap a slab's halo exchange with its own work.
+ * SGFD_PART_INNER updates the planes 5 or more computed planes from both ends
+ * of the handle's planes (z chunks of the z-marching kernels, planes of the
+ * simple ones): they read no frame plane, so they may run while the halos are
+ * in flight.  SGFD_PART_OUTER updates the rest, after the unpack.  Run INNER
+ * before OUTER (the simple kernels inject the source with INNER and record
+ * the receivers with OUTER); INNER | OUTER is sgfd_step_phase. */
+#define SGFD_PART_INNER 1
+#define SGFD_PART_OUTER 2
+int sgfd_step_phase_part(sgfd_solver *h, int32_t it, float source_value, int32_t phase, int32_t parts);
 
 /* ---- autotuning and batches (no counterpart in the reference, which runs
  * one model with a fixed launch shape: OPT/main.cu's GPUDim) ---- */

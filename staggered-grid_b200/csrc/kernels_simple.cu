@@ -7,6 +7,8 @@
 // the 26 region split arrays replaced by the compact PML array.  It serves as
 // the correctness baseline for the z-marching family and as the fallback for
 // grids the z-marching kernels do not tile.
+#include <algorithm>
+
 #include "cell_math.cuh"
 
 namespace sgfd {
@@ -28,10 +30,10 @@ __global__ void k_inject(Model m, Physics ph, SourceRec sr, int it_arg, float va
 
 // Velocity update of one cell (ElasticWaveEquation.cu:234-526, ElasticMacro.h:409-458).
 template <bool FAST>
-__global__ void __launch_bounds__(kBX * kBY) k_velocity(Model m, Physics ph) {
+__global__ void __launch_bounds__(kBX * kBY) k_velocity(Model m, Physics ph, int z0) {
     const int cx = blockIdx.x * kBX + threadIdx.x;
     const int cy = blockIdx.y * kBY + threadIdx.y;
-    const int cz = blockIdx.z;
+    const int cz = blockIdx.z + z0;   // computed planes [z0, z0 + gridDim.z)
     if (cx >= m.nxc || cy >= m.nyc) return;
     const int x = cx + kHalo, y = cy + kHalo, z = cz + kHalo;
     const int64_t ci = pidx(m, x, y, z);
@@ -90,10 +92,10 @@ __global__ void __launch_bounds__(kBX * kBY) k_velocity(Model m, Physics ph) {
 
 // Stress update of one cell (ElasticWaveEquation.cu:528-841, ElasticMacro.h:460-531).
 template <bool FAST>
-__global__ void __launch_bounds__(kBX * kBY) k_stress(Model m, Physics ph) {
+__global__ void __launch_bounds__(kBX * kBY) k_stress(Model m, Physics ph, int z0) {
     const int cx = blockIdx.x * kBX + threadIdx.x;
     const int cy = blockIdx.y * kBY + threadIdx.y;
-    const int cz = blockIdx.z;
+    const int cz = blockIdx.z + z0;   // computed planes [z0, z0 + gridDim.z)
     if (cx >= m.nxc || cy >= m.nyc) return;
     const int x = cx + kHalo, y = cy + kHalo, z = cz + kHalo;
     const int64_t ci = pidx(m, x, y, z);
@@ -223,23 +225,42 @@ int simple_launches_per_step(const SourceRec &sr) {
 }
 
 cudaError_t simple_step(const Model &m, const Physics &ph, const SourceRec &sr,
-                        int it, float src_value, bool use_wavelet, cudaStream_t s, cudaEvent_t *ev, int phases) {
+                        int it, float src_value, bool use_wavelet, cudaStream_t s, cudaEvent_t *ev, int phases,
+                        int parts) {
     const dim3 block(kBX, kBY);
-    const dim3 grid((m.nxc + kBX - 1) / kBX, (m.nyc + kBY - 1) / kBY, m.nzc);
+    // plane ranges of the selected parts: inner [5, nzc - 5), outer the planes below and above it
+    const int i0 = std::min(kHalo, m.nzc), i1 = std::max(i0, m.nzc - kHalo);
+    int range[3][2], nr = 0;
+    if (parts == (kPartInner | kPartOuter)) {   // the whole half step: one launch
+        range[0][0] = 0; range[0][1] = m.nzc; nr = 1;
+    } else {
+        if (parts & kPartOuter) { range[nr][0] = 0; range[nr][1] = i0; ++nr; }
+        if (parts & kPartInner) { range[nr][0] = i0; range[nr][1] = i1; ++nr; }
+        if (parts & kPartOuter) { range[nr][0] = i1; range[nr][1] = m.nzc; ++nr; }
+    }
+    auto each = [&](auto fn) {
+        for (int r = 0; r < nr; ++r)
+            if (range[r][1] > range[r][0])
+                fn(dim3((m.nxc + kBX - 1) / kBX, (m.nyc + kBY - 1) / kBY, range[r][1] - range[r][0]), range[r][0]);
+    };
     if (phases & 1) {
-        if (sr.src >= 0) k_inject<<<1, 32, 0, s>>>(m, ph, sr, it, src_value, use_wavelet ? 1 : 0);
+        if ((parts & kPartInner) && sr.src >= 0) k_inject<<<1, 32, 0, s>>>(m, ph, sr, it, src_value, use_wavelet ? 1 : 0);
         if (ev) cudaEventRecord(ev[0], s);
-        if (ph.fast) k_velocity<true><<<grid, block, 0, s>>>(m, ph);
-        else k_velocity<false><<<grid, block, 0, s>>>(m, ph);
+        each([&](dim3 grid, int z0) {
+            if (ph.fast) k_velocity<true><<<grid, block, 0, s>>>(m, ph, z0);
+            else k_velocity<false><<<grid, block, 0, s>>>(m, ph, z0);
+        });
         if (ev) cudaEventRecord(ev[1], s);
-        if (sr.nrec > 0) k_record<<<(sr.nrec + 127) / 128, 128, 0, s>>>(m, sr, it, 1);
+        if ((parts & kPartOuter) && sr.nrec > 0) k_record<<<(sr.nrec + 127) / 128, 128, 0, s>>>(m, sr, it, 1);
     }
     if (phases & 2) {
         if (ev) cudaEventRecord(ev[2], s);
-        if (ph.fast) k_stress<true><<<grid, block, 0, s>>>(m, ph);
-        else k_stress<false><<<grid, block, 0, s>>>(m, ph);
+        each([&](dim3 grid, int z0) {
+            if (ph.fast) k_stress<true><<<grid, block, 0, s>>>(m, ph, z0);
+            else k_stress<false><<<grid, block, 0, s>>>(m, ph, z0);
+        });
         if (ev) cudaEventRecord(ev[3], s);
-        if (sr.nrec > 0) k_record<<<(sr.nrec + 127) / 128, 128, 0, s>>>(m, sr, it, 0);
+        if ((parts & kPartOuter) && sr.nrec > 0) k_record<<<(sr.nrec + 127) / 128, 128, 0, s>>>(m, sr, it, 0);
     }
     return cudaGetLastError();
 }

@@ -48,6 +48,7 @@
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
+#include <algorithm>
 #include <type_traits>
 
 #include "cell_math.cuh"
@@ -588,7 +589,7 @@ k_velocity_zmarch(const __grid_constant__ ZMaps mp, const __grid_constant__ Mode
     }
     __syncthreads();
     uint32_t pbits = 0;
-    vel_item<FAST, CELLS, false>(mp, m, ph, g, sr, it_arg, src_value, use_wavelet, blockIdx.x, blockIdx.y,
+    vel_item<FAST, CELLS, false>(mp, m, ph, g, sr, it_arg, src_value, use_wavelet, blockIdx.x, blockIdx.y + g.c0,
                           align_smem(smem_raw), bar, boxes, pbits);
 }
 
@@ -982,7 +983,7 @@ k_stress_zmarch(const __grid_constant__ ZMaps mp, const __grid_constant__ Model 
     }
     __syncthreads();
     uint32_t pbits = 0;
-    str_item<FAST, CELLS, false>(mp, m, ph, g, sr, it_arg, src_value, use_wavelet, blockIdx.x, blockIdx.y,
+    str_item<FAST, CELLS, false>(mp, m, ph, g, sr, it_arg, src_value, use_wavelet, blockIdx.x, blockIdx.y + g.c0,
                           align_smem(smem_raw), bar, boxes, pbits);
 }
 
@@ -1001,7 +1002,7 @@ k_velocity_zmarch16(const __grid_constant__ ZMaps mp, const __grid_constant__ Mo
     }
     __syncthreads();
     uint32_t pbits = 0;
-    vel_item<FAST, 1, false, ST>(mp, m, ph, g, sr, it_arg, 0.0f, 0, blockIdx.x, blockIdx.y, align_smem(smem_raw), bar,
+    vel_item<FAST, 1, false, ST>(mp, m, ph, g, sr, it_arg, 0.0f, 0, blockIdx.x, blockIdx.y + g.c0, align_smem(smem_raw), bar,
                                  boxes, pbits, hs);
 }
 template <bool FAST, int ST>
@@ -1018,7 +1019,7 @@ k_stress_zmarch16(const __grid_constant__ ZMaps mp, const __grid_constant__ Mode
     }
     __syncthreads();
     uint32_t pbits = 0;
-    str_item<FAST, 1, false, ST>(mp, m, ph, g, sr, it_arg, 0.0f, 0, blockIdx.x, blockIdx.y, align_smem(smem_raw), bar,
+    str_item<FAST, 1, false, ST>(mp, m, ph, g, sr, it_arg, 0.0f, 0, blockIdx.x, blockIdx.y + g.c0, align_smem(smem_raw), bar,
                                  boxes, pbits, hs);
 }
 
@@ -1175,16 +1176,39 @@ void launch16(const Model &m, const Physics &ph, const SourceRec &sr, const Half
 
 template <bool FAST, int CELLS>
 void launch(const Model &m, const Physics &ph, const SourceRec &sr, const ZGeom &g, const ZMaps &zm, int it,
-            float src_value, int uw, cudaStream_t s, cudaEvent_t *ev, int phases) {
-    const dim3 grid(g.ntx * g.nty, g.nchunks);
+            float src_value, int uw, cudaStream_t s, cudaEvent_t *ev, int phases, int parts) {
+    // chunk ranges of the selected parts: inner chunks [c_in0, c_in1) lie 5 or
+    // more planes from both ends (they read no frame plane), outer chunks the rest
+    const int c_in0 = std::min(g.nchunks, (kHalo + g.zc - 1) / g.zc);
+    const int c_in1 = std::max(c_in0, m.nzc >= kHalo ? (m.nzc - kHalo) / g.zc : 0);
+    int range[3][2], nr = 0;
+    if (parts == (kPartInner | kPartOuter)) {   // the whole half step: one launch
+        range[0][0] = 0; range[0][1] = g.nchunks; nr = 1;
+    } else {
+        if (parts & kPartOuter) { range[nr][0] = 0; range[nr][1] = c_in0; ++nr; }
+        if (parts & kPartInner) { range[nr][0] = c_in0; range[nr][1] = c_in1; ++nr; }
+        if (parts & kPartOuter) { range[nr][0] = c_in1; range[nr][1] = g.nchunks; ++nr; }
+    }
+    auto each = [&](auto fn) {
+        for (int r = 0; r < nr; ++r) {
+            if (range[r][1] <= range[r][0]) continue;
+            ZGeom gr = g;
+            gr.c0 = range[r][0];
+            fn(dim3(g.ntx * g.nty, range[r][1] - range[r][0]), gr);
+        }
+    };
     if (phases & 1) {
         if (ev) cudaEventRecord(ev[0], s);
-        k_velocity_zmarch<FAST, CELLS><<<grid, NT, vel_smem<CELLS>(), s>>>(zm, m, ph, g, sr, it, src_value, uw);
+        each([&](dim3 grid, const ZGeom &gr) {
+            k_velocity_zmarch<FAST, CELLS><<<grid, NT, vel_smem<CELLS>(), s>>>(zm, m, ph, gr, sr, it, src_value, uw);
+        });
         if (ev) cudaEventRecord(ev[1], s);
     }
     if (phases & 2) {
         if (ev) cudaEventRecord(ev[2], s);
-        k_stress_zmarch<FAST, CELLS><<<grid, NT, str_smem<CELLS>(), s>>>(zm, m, ph, g, sr, it, src_value, uw);
+        each([&](dim3 grid, const ZGeom &gr) {
+            k_stress_zmarch<FAST, CELLS><<<grid, NT, str_smem<CELLS>(), s>>>(zm, m, ph, gr, sr, it, src_value, uw);
+        });
         if (ev) cudaEventRecord(ev[3], s);
     }
 }
@@ -1329,7 +1353,7 @@ void zmarch_tiles(const Model &m, int cells, int *ntx, int *nty) {
 
 cudaError_t zmarch_step(const Model &m, const Physics &ph, const SourceRec &sr, const ZGeom &g, const ZMaps &zm,
                         int it, float src_value, bool use_wavelet, cudaStream_t s, cudaEvent_t *ev,
-                        const HalfState *hs, int phases) {
+                        const HalfState *hs, int phases, int parts) {
     if (hs) {
         if (hs->storage == SGFD_STORE_BF16) {
             if (ph.fast) launch16<true, SGFD_STORE_BF16>(m, ph, sr, *hs, g, zm, it, src_value, use_wavelet, s, ev);
@@ -1342,11 +1366,11 @@ cudaError_t zmarch_step(const Model &m, const Physics &ph, const SourceRec &sr, 
     }
     const int uw = use_wavelet ? 1 : 0;
     if (ph.fast) {
-        if (g.cells == 1) launch<true, 1>(m, ph, sr, g, zm, it, src_value, uw, s, ev, phases);
-        else launch<true, 2>(m, ph, sr, g, zm, it, src_value, uw, s, ev, phases);
+        if (g.cells == 1) launch<true, 1>(m, ph, sr, g, zm, it, src_value, uw, s, ev, phases, parts);
+        else launch<true, 2>(m, ph, sr, g, zm, it, src_value, uw, s, ev, phases, parts);
     } else {
-        if (g.cells == 1) launch<false, 1>(m, ph, sr, g, zm, it, src_value, uw, s, ev, phases);
-        else launch<false, 2>(m, ph, sr, g, zm, it, src_value, uw, s, ev, phases);
+        if (g.cells == 1) launch<false, 1>(m, ph, sr, g, zm, it, src_value, uw, s, ev, phases, parts);
+        else launch<false, 2>(m, ph, sr, g, zm, it, src_value, uw, s, ev, phases, parts);
     }
     return cudaGetLastError();
 }

@@ -950,7 +950,7 @@ k_velocity_zpair(const __grid_constant__ VelMaps mp, const __grid_constant__ Mod
     }
     __syncthreads();
     uint32_t pbits = 0;
-    vel_pair<FAST, ST>(mp, m, ph, g, sr, hs, it_arg, src_value, use_wavelet, blockIdx.x, blockIdx.y,
+    vel_pair<FAST, ST>(mp, m, ph, g, sr, hs, it_arg, src_value, use_wavelet, blockIdx.x, blockIdx.y + g.c0,
                        align_smem(smem_raw), bar, boxes, pbits);
 }
 
@@ -968,7 +968,7 @@ k_stress_zpair(const __grid_constant__ StrMaps mp, const __grid_constant__ Model
     }
     __syncthreads();
     uint32_t pbits = 0;
-    str_pair<FAST, ST>(mp, m, ph, g, sr, hs, it_arg, src_value, use_wavelet, blockIdx.x, blockIdx.y,
+    str_pair<FAST, ST>(mp, m, ph, g, sr, hs, it_arg, src_value, use_wavelet, blockIdx.x, blockIdx.y + g.c0,
                        align_smem(smem_raw), bar, boxes, pbits);
 }
 

@@ -740,11 +740,17 @@ int sgfd_run(sgfd_solver *h, int32_t it0, int32_t nsteps, int32_t use_graph) {
 }
 
 int sgfd_step_phase(sgfd_solver *h, int32_t it, float source_value, int32_t phase) {
+    return sgfd_step_phase_part(h, it, source_value, phase, SGFD_PART_INNER | SGFD_PART_OUTER);
+}
+
+int sgfd_step_phase_part(sgfd_solver *h, int32_t it, float source_value, int32_t phase, int32_t parts) {
     int r = check_handle(h);
     if (r) return r;
     if (!h->medium_set) return fail(h, SGFD_ERR_STATE, "sgfd_set_medium must come before stepping");
     if (phase != SGFD_PHASE_VELOCITY && phase != SGFD_PHASE_STRESS)
         return fail(h, SGFD_ERR_INVALID, "unknown phase %d", phase);
+    if (parts < 1 || parts > (SGFD_PART_INNER | SGFD_PART_OUTER))
+        return fail(h, SGFD_ERR_INVALID, "bad part mask %d", parts);
     if (h->storage != SGFD_STORE_F32 || (h->kernel == SGFD_KERNEL_ZMARCH && h->zg.pair))
         return fail(h, SGFD_ERR_UNSUPPORTED,
                     "half steps need FP32 storage and the simple kernels or 32-column z-march tiles");
@@ -754,8 +760,8 @@ int sgfd_step_phase(sgfd_solver *h, int32_t it, float source_value, int32_t phas
     const cudaError_t e =
         h->kernel == SGFD_KERNEL_ZMARCH
             ? zmarch_step(h->m, h->ph, h->sr, h->zg, h->zm, it, source_value, false, h->stream, nullptr, nullptr,
-                          phases)
-            : simple_step(h->m, h->ph, h->sr, it, source_value, false, h->stream, nullptr, phases);
+                          phases, parts)
+            : simple_step(h->m, h->ph, h->sr, it, source_value, false, h->stream, nullptr, phases, parts);
     if (e != cudaSuccess) return cuda_fail(h, e, "half-step launch");
     return SGFD_OK;
 }

@@ -234,15 +234,23 @@ __host__ inline int64_t pml_before(int nxc, int nyc, int nzc, int p, int z) {
     return (int64_t)(lo + hi) * full + (int64_t)mid * ring;
 }
 
+// Parts of a half step, so that a z-slab can overlap its halo exchange with
+// its own work: kPartInner the planes whose updates read no frame plane
+// (5 or more computed planes from both ends of the model's planes),
+// kPartOuter the others.  Run inner before outer (the simple family injects
+// the source with the inner part and records receivers with the outer one).
+constexpr int kPartInner = 1, kPartOuter = 2;
+
 // ---- kernel family entry points (host side) -------------------------------
 
 // "simple": one thread per computed cell.
 // ev (optional, 4 events): recorded before/after the velocity kernel and
 // before/after the stress kernel.  phases: bit 0 the source injection, the
-// velocity update and its receivers, bit 1 the stress update and its receivers.
+// velocity update and its receivers, bit 1 the stress update and its
+// receivers; parts: kPartInner / kPartOuter planes (both: all).
 cudaError_t simple_step(const Model &m, const Physics &ph, const SourceRec &sr,
                         int it, float src_value, bool use_wavelet, cudaStream_t s,
-                        cudaEvent_t *ev = nullptr, int phases = 3);
+                        cudaEvent_t *ev = nullptr, int phases = 3, int parts = 3);
 int simple_launches_per_step(const SourceRec &sr);
 
 // medium post-processing: rmu = 1/mu over the padded arrays, then the three

@@ -54,6 +54,7 @@ struct ZGeom {
     int cells;
     int ntx, nty;
     int zc, nchunks;
+    int c0;                 // first z chunk of this launch (blockIdx.y = chunk - c0); 0 for a whole half step
     const int *rec_off;     // ntx*nty + 1 offsets into rec_list / rec_idx
     const int4 *rec_list;   // GRID x, y, z, component
     const int *rec_idx;     // receiver index (trace column)
@@ -71,14 +72,16 @@ bool make_box_map16(CUtensorMap *map, const uint16_t *grid_origin, const Model &
 // with hs (16-bit storage, cells = 1), the wavefield maps cover the 16-bit
 // arrays, stride16 bytes apart.  zmarch_step: one step (velocity + stress);
 // with hs also the 16-bit source, receiver and rescale kernels.  phases
-// (FP32 storage): bit 0 the velocity update, bit 1 the stress update.
+// (FP32 storage): bit 0 the velocity update, bit 1 the stress update; parts
+// (FP32 storage): kPartInner the z chunks whose planes read no frame plane,
+// kPartOuter the others.
 bool zmarch_supported(const Model &m);
 cudaError_t zmarch_prepare(const Model &m, int cells, size_t array_stride, ZMaps *zm, const HalfState *hs = nullptr,
                            size_t stride16 = 0);
 void zmarch_tiles(const Model &m, int cells, int *ntx, int *nty);
 cudaError_t zmarch_step(const Model &m, const Physics &ph, const SourceRec &sr, const ZGeom &g, const ZMaps &zm,
                         int it, float src_value, bool use_wavelet, cudaStream_t s, cudaEvent_t *ev = nullptr,
-                        const HalfState *hs = nullptr, int phases = 3);
+                        const HalfState *hs = nullptr, int phases = 3, int parts = 3);
 // One model of a persistent batch, in device memory (the kernel's TMA reads
 // its tensor maps from there: 64-byte alignment).  Its work items are the
 // (tile, z chunk) pairs of the single-cell 32 x 8 tiling, tile fastest.

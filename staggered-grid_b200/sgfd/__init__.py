@@ -38,6 +38,7 @@ REGION_COMPUTED, REGION_INTERIOR, REGION_PML = range(3)
 HALO_LOW, HALO_HIGH = range(2)             # the cut below / above a z-slab
 HALO_STRESS, HALO_VELOCITY = range(2)      # txz, tyz, tzz / vx, vy, vz
 PHASE_VELOCITY, PHASE_STRESS = range(2)
+PART_INNER, PART_OUTER = 1, 2              # planes that read no frame plane / the rest
 
 # sgfd_status
 OK, ERR_INVALID, ERR_ALLOC, ERR_CUDA, ERR_STATE, ERR_UNSUPPORTED, ERR_NO_DEVICE, ERR_NONFINITE = range(8)
@@ -101,6 +102,7 @@ def lib() -> ctypes.CDLL:
         "sgfd_set_wavelet": (ctypes.c_int, [vp, i32, fp]),
         "sgfd_step": (ctypes.c_int, [vp, i32, ctypes.c_float]),
         "sgfd_step_phase": (ctypes.c_int, [vp, i32, ctypes.c_float, i32]),
+        "sgfd_step_phase_part": (ctypes.c_int, [vp, i32, ctypes.c_float, i32, i32]),
         "sgfd_halo_bytes": (ctypes.c_int, [vp, ctypes.POINTER(ctypes.c_int64)]),
         "sgfd_halo_pack": (ctypes.c_int, [vp, i32, i32, vp]),
         "sgfd_halo_unpack": (ctypes.c_int, [vp, i32, i32, vp]),
@@ -268,10 +270,11 @@ class Solver:
     def step(self, it: int, value: float):
         self._check(lib().sgfd_step(self.h, it, value))
 
-    def step_phase(self, it: int, value: float, phase: int):
+    def step_phase(self, it: int, value: float, phase: int, parts: int = PART_INNER | PART_OUTER):
         """Half a step: PHASE_VELOCITY (source, velocity update, velocity
-        receivers) or PHASE_STRESS (stress update, stress receivers)."""
-        self._check(lib().sgfd_step_phase(self.h, it, value, phase))
+        receivers) or PHASE_STRESS (stress update, stress receivers); parts
+        PART_INNER (planes that read no frame plane) then PART_OUTER split it."""
+        self._check(lib().sgfd_step_phase_part(self.h, it, value, phase, parts))
 
     def halo_bytes(self) -> int:
         """Bytes of one halo buffer of a z-slab (3 fields x 5 padded planes)."""

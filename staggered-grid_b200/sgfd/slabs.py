@@ -15,11 +15,14 @@ compact split order.  At every cut the two slabs trade the 5 planes next to it
 
 which gives the whole model's results bit for bit (the updates of a cell read
 only its 10-cell neighbourhood, and every value a slab reads at its frame is
-the neighbour's value of the same half step).
+the neighbour's value of the same half step).  Each exchange overlaps the
+inner part of the half step after it (PART_INNER: the planes 5 or more planes
+from the slab's ends, which read no frame plane); the outer part runs once
+the halos are unpacked.
 
 Two forms share the plan and the step sequence:
-  * SlabModel — all slabs in one process on one GPU, halos moved by device
-    copies on one stream;
+  * SlabModel — all slabs in one process on one GPU, a stream each, halos
+    moved by device copies ordered by events;
   * DistributedSlab — one slab per rank (one process per GPU, torch.distributed
     over NCCL), halos moved by send/recv to the ranks above and below
     (exchange_remote, also run on CPU tensors over gloo by the tests).
@@ -28,7 +31,8 @@ from __future__ import annotations
 
 import numpy as np
 
-from . import (Config, Solver, HALO_LOW, HALO_HIGH, HALO_STRESS, HALO_VELOCITY, PHASE_VELOCITY, PHASE_STRESS)
+from . import (Config, Solver, HALO_LOW, HALO_HIGH, HALO_STRESS, HALO_VELOCITY, PHASE_VELOCITY, PHASE_STRESS,
+               PART_INNER, PART_OUTER)
 
 HALO = 5            # planes exchanged at a cut (the reference `order`)
 MIN_PLANES = HALO   # computed planes a slab needs to fill its neighbour's frame
@@ -146,28 +150,36 @@ class _Slabs:
 
 
 class SlabModel(_Slabs):
-    """All slabs of one model in this process, on one GPU (cfg.device): they
-    share one stream of their own (`stream`), and halos move by device copies
-    between the slabs' buffers.  Slabs on several GPUs: DistributedSlab."""
+    """All slabs of one model in this process, on one GPU (cfg.device).  Each
+    slab runs on a stream of its own, so one slab's halo copies and kernels
+    overlap another's; events order what must be ordered: a slab unpacks its
+    neighbours' planes after they packed them, and packs again only after
+    both neighbours unpacked the previous buffer.  `run` starts after, and
+    ends before, the work queued on `stream`.  Slabs on several GPUs:
+    DistributedSlab."""
 
     def __init__(self, cfg: Config, cuts):
         super().__init__(cfg, cuts)
         import torch
-        devs = [cfg.device] * len(self.cuts)
-        self.devices = devs
+        self._torch = torch
+        d = cfg.device
         self.slabs = []
-        self.bufs = []          # per slab: (buffer of its LOW side, buffer of its HIGH side)
-        # one stream for every slab (a null stream would give each handle its own): the packs, copies,
-        # unpacks and half steps of all slabs are ordered on it
-        self.stream = torch.cuda.Stream(device=cfg.device)
+        # per halo kind and slab: (buffer of its LOW side, buffer of its HIGH side), and the events
+        # after the slab packed them and after it unpacked its neighbours' buffers
+        self.bufs = [[], []]
+        self.stream = torch.cuda.Stream(device=d)                 # joins every slab's stream around a run
+        self.streams = [torch.cuda.Stream(device=d) for _ in self.cuts]
+        self.packed = [[torch.cuda.Event() for _ in self.cuts] for _ in range(2)]
+        self.unpacked = [[torch.cuda.Event() for _ in self.cuts] for _ in range(2)]
         try:
-            for (z0, n), d in zip(self.cuts, devs):
+            for (z0, n), st in zip(self.cuts, self.streams):
                 s = Solver(slab_config(cfg, z0, n, d))
-                s.set_stream(self.stream.cuda_stream)
+                s.set_stream(st.cuda_stream)
                 nbytes = s.halo_bytes()
-                with torch.cuda.stream(self.stream):   # the buffers belong to the stream that uses them
-                    self.bufs.append(tuple(torch.empty(nbytes // 4, dtype=torch.float32, device=f"cuda:{d}")
-                                           for _ in range(2)))
+                with torch.cuda.stream(st):
+                    for kind in (HALO_STRESS, HALO_VELOCITY):
+                        self.bufs[kind].append(tuple(torch.empty(nbytes // 4, dtype=torch.float32,
+                                                                 device=f"cuda:{d}") for _ in range(2)))
                 self.slabs.append(s)
         except Exception:
             self.close()
@@ -202,31 +214,56 @@ class SlabModel(_Slabs):
         self.nrec = len(np.asarray(comp).reshape(-1))
         self.nt = nt
 
-    def _exchange(self, kind: int):
+    def _pack(self, kind: int):
         last = len(self.slabs) - 1
+        bufs, packed, unpacked = self.bufs[kind], self.packed[kind], self.unpacked[kind]
         for k, s in enumerate(self.slabs):
+            st = self.streams[k]
+            for j in (k - 1, k + 1):          # the neighbours have unpacked this slab's previous buffers
+                if 0 <= j <= last:
+                    st.wait_event(unpacked[j])
             if k > 0:
-                s.halo_pack(HALO_LOW, kind, self.bufs[k][0].data_ptr())
+                s.halo_pack(HALO_LOW, kind, bufs[k][0].data_ptr())
             if k < last:
-                s.halo_pack(HALO_HIGH, kind, self.bufs[k][1].data_ptr())
+                s.halo_pack(HALO_HIGH, kind, bufs[k][1].data_ptr())
+            packed[k].record(st)
+
+    def _unpack(self, kind: int):
+        last = len(self.slabs) - 1
+        bufs, packed, unpacked = self.bufs[kind], self.packed[kind], self.unpacked[kind]
         for k, s in enumerate(self.slabs):
+            st = self.streams[k]
             if k > 0:
-                s.halo_unpack(HALO_LOW, kind, self.bufs[k - 1][1].data_ptr())
+                st.wait_event(packed[k - 1])
+                s.halo_unpack(HALO_LOW, kind, bufs[k - 1][1].data_ptr())
             if k < last:
-                s.halo_unpack(HALO_HIGH, kind, self.bufs[k + 1][0].data_ptr())
+                st.wait_event(packed[k + 1])
+                s.halo_unpack(HALO_HIGH, kind, bufs[k + 1][0].data_ptr())
+            unpacked[k].record(st)
 
     def step(self, it: int, value: float):
-        """One step of the whole model (reference propagate())."""
-        self._exchange(HALO_STRESS)
-        for s in self.slabs:
-            s.step_phase(it, value, PHASE_VELOCITY)
-        self._exchange(HALO_VELOCITY)
-        for s in self.slabs:
-            s.step_phase(it, value, PHASE_STRESS)
+        """One step of the whole model (reference propagate()): each slab packs,
+        runs the inner part of the half step, unpacks its neighbours' planes
+        once they are packed, then runs the outer part."""
+        for kind, phase in ((HALO_STRESS, PHASE_VELOCITY), (HALO_VELOCITY, PHASE_STRESS)):
+            self._pack(kind)
+            for s in self.slabs:
+                s.step_phase(it, value, phase, PART_INNER)
+            self._unpack(kind)
+            for s in self.slabs:
+                s.step_phase(it, value, phase, PART_OUTER)
 
     def run(self, it0: int, nsteps: int, wavelet):
+        start = self._torch.cuda.Event()
+        start.record(self.stream)
+        for st in self.streams:
+            st.wait_event(start)
         for it in range(it0, it0 + nsteps):
             self.step(it, float(wavelet[it]))
+        for st in self.streams:
+            done = self._torch.cuda.Event()
+            done.record(st)
+            self.stream.wait_event(done)
 
     def synchronize(self):
         for s in self.slabs:
@@ -294,34 +331,50 @@ class DistributedSlab(_Slabs):
         self.nrec = len(idx)
         self.nt = nt
 
-    def _exchange(self, kind: int):
+    def _exchange_start(self, kind: int):
+        """Pack this slab's planes beside its cuts and start the transfers;
+        returns what _exchange_finish waits for."""
+        import torch
+        import torch.distributed as dist
         if self.rank > 0:
             self.s.halo_pack(HALO_LOW, kind, self.send[0].data_ptr())
         if self.rank < self.world - 1:
             self.s.halo_pack(HALO_HIGH, kind, self.send[1].data_ptr())
-        import torch
-        import torch.distributed as dist
-        if dist.get_backend() == "nccl":
-            with torch.cuda.stream(self.stream):   # NCCL orders its send/recv after, and before, this stream's work
-                exchange_remote(self.send[0], self.send[1], self.recv[0], self.recv[1], self.rank, self.world)
-        else:
-            with torch.cuda.stream(self.stream):   # device -> host after the packs (a synchronous copy)
+        if dist.get_backend() != "nccl":
+            # a host backend: device -> host after the packs, the send/recv on the host, host -> device
+            with torch.cuda.stream(self.stream):
                 hs = [t.to("cpu") for t in self.send]
             hr = [torch.empty_like(t) for t in hs]
             exchange_remote(hs[0], hs[1], hr[0], hr[1], self.rank, self.world)
-            with torch.cuda.stream(self.stream):   # host -> device before the unpacks
+            with torch.cuda.stream(self.stream):
                 for d, h in zip(self.recv, hr):
                     d.copy_(h)
+            return []
+        ops = []
+        for side, peer in ((0, self.rank - 1), (1, self.rank + 1)):
+            if 0 <= peer < self.world:
+                ops += [dist.P2POp(dist.isend, self.send[side], peer), dist.P2POp(dist.irecv, self.recv[side], peer)]
+        with torch.cuda.stream(self.stream):   # NCCL starts after this stream's packs
+            return dist.batch_isend_irecv(ops) if ops else []
+
+    def _exchange_finish(self, kind: int, works):
+        import torch
+        with torch.cuda.stream(self.stream):   # this stream waits for the transfers
+            for w in works:
+                w.wait()
         if self.rank > 0:
             self.s.halo_unpack(HALO_LOW, kind, self.recv[0].data_ptr())
         if self.rank < self.world - 1:
             self.s.halo_unpack(HALO_HIGH, kind, self.recv[1].data_ptr())
 
     def step(self, it: int, value: float):
-        self._exchange(HALO_STRESS)
-        self.s.step_phase(it, value, PHASE_VELOCITY)
-        self._exchange(HALO_VELOCITY)
-        self.s.step_phase(it, value, PHASE_STRESS)
+        """One step of the whole model: per half step, the transfers run while
+        the slab's inner part is computed, the outer part after the unpack."""
+        for kind, phase in ((HALO_STRESS, PHASE_VELOCITY), (HALO_VELOCITY, PHASE_STRESS)):
+            works = self._exchange_start(kind)
+            self.s.step_phase(it, value, phase, PART_INNER)
+            self._exchange_finish(kind, works)
+            self.s.step_phase(it, value, phase, PART_OUTER)
 
     def run(self, it0: int, nsteps: int, wavelet):
         for it in range(it0, it0 + nsteps):

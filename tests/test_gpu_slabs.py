@@ -155,3 +155,30 @@ def test_distributed_slabs_on_one_gpu(world, kernel):
         for f, (z0, a) in enumerate(planes):
             np.testing.assert_array_equal(a, want[f][5 + z0:5 + z0 + a.shape[0]], err_msg=sgfd.FIELD_NAMES[f])
     assert covered == len(w.rec_comp) and np.abs(want_tr).max() > 0
+
+
+@pytest.mark.parametrize("kernel,zchunk", [(sgfd.KERNEL_ZMARCH, 0), (sgfd.KERNEL_ZMARCH, 7), (sgfd.KERNEL_ZMARCH, 3),
+                                           (sgfd.KERNEL_SIMPLE, 0)], ids=["zmarch", "zmarch_chunk7", "zmarch_chunk3",
+                                                                          "simple"])
+def test_half_step_parts_equal_steps(kernel, zchunk):
+    """A whole model stepped as velocity inner, velocity outer, stress inner,
+    stress outer (the slabs' overlapped order) equals sgfd_run bit for bit."""
+    w = wl.small_random_case(nx=39, ny=35, nz=44, pml=5, nt=30)
+    outs = []
+    for split in (False, True):
+        with make_solver(w, kernel=kernel) as s:
+            if zchunk:
+                s.set_zchunk(zchunk)
+            if split:
+                for it in range(w.nt):
+                    for phase in (sgfd.PHASE_VELOCITY, sgfd.PHASE_STRESS):
+                        s.step_phase(it, float(w.wavelet[it]), phase, sgfd.PART_INNER)
+                        s.step_phase(it, float(w.wavelet[it]), phase, sgfd.PART_OUTER)
+            else:
+                s.run(0, w.nt)
+            s.synchronize()
+            outs.append((s.traces(), [s.field(f) for f in range(9)]))
+    np.testing.assert_array_equal(outs[1][0], outs[0][0])
+    for f in range(9):
+        np.testing.assert_array_equal(outs[1][1][f], outs[0][1][f], err_msg=sgfd.FIELD_NAMES[f])
+    assert np.abs(outs[0][0]).max() > 0
