@@ -460,8 +460,8 @@ int sgfd_get_audit(sgfd_solver *h, double *out);
  * handle is created with the same configuration, given the same inputs, then
  * loads the checkpoint and continues with step it_next.  Layout: a 128-byte
  * header (magic "SGFDCKP1", version 1, grid, pml, receivers x steps, it_next,
- * physics, payload size, 64-bit checksum, storage type and the 16-bit field
- * scales), then the payload: 9 x nx*ny*nz
+ * physics, payload size, 64-bit checksum, storage type, the 16-bit field
+ * scales and, for a z-slab, its place in the whole model), then the payload: 9 x nx*ny*nz
  * float32 fields (x fastest), 24 x npml float32 splits, nt x nrec float32
  * traces (time-major).  Loading checks the grid, physics and checksum; a
  * checksum or length failure zeroes the state (as sgfd_reset) and returns

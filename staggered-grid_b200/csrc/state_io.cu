@@ -47,7 +47,9 @@ struct CkptHeader {
     uint64_t checksum;
     int8_t scale_e[9];   // 16-bit storage: exponents of the field scales (0 for FP32)
     uint8_t storage;     // sgfd_storage of the payload's values
-    uint8_t pad[128 - 8 - 8 - 16 - 12 - 12 - 16 - 24 - 10];
+    uint8_t pad0[2];
+    int32_t nz_total, z_offset;   // z-slab: the whole model's GRID nz and the slab's offset (0, 0: whole model)
+    uint8_t pad[128 - 8 - 8 - 16 - 12 - 12 - 16 - 24 - 10 - 2 - 8];
 };
 static_assert(sizeof(CkptHeader) == 128, "checkpoint header is 128 bytes");
 
@@ -154,6 +156,8 @@ void fill_header(sgfd_solver *h, int32_t it_next, CkptHeader *hd) {
     hd->npml = h->m.npml;
     hd->payload_bytes = payload_bytes(h);
     hd->storage = (uint8_t)h->storage;
+    hd->nz_total = c.nz_total;
+    hd->z_offset = c.z_offset;
 }
 
 // Regions move through the staging chunk as whole rows where a row fits
@@ -221,6 +225,9 @@ int load_state(sgfd_solver *h, Stream &in, int32_t *it_next) {
     if (hd.nx != want.nx || hd.ny != want.ny || hd.nz != want.nz || hd.pml != want.pml || hd.npml != want.npml)
         return fail(h, SGFD_ERR_INVALID, "checkpoint grid %dx%dx%d pml %d does not match the solver's %dx%dx%d pml %d",
                     hd.nx, hd.ny, hd.nz, hd.pml, want.nx, want.ny, want.nz, want.pml);
+    if (hd.nz_total != want.nz_total || hd.z_offset != want.z_offset)
+        return fail(h, SGFD_ERR_INVALID, "checkpoint of the z-slab at plane %d of %d planes, the solver is at %d of %d",
+                    hd.z_offset, hd.nz_total, want.z_offset, want.nz_total);
     if (hd.nrec != want.nrec || hd.nt != want.nt)
         return fail(h, SGFD_ERR_INVALID, "checkpoint holds %d receivers x %d steps, the solver %d x %d",
                     hd.nrec, hd.nt, want.nrec, want.nt);

@@ -472,7 +472,7 @@ class Solver:
 
 
 CHECKPOINT_MAGIC = b"SGFDCKP1"
-_CKPT_HEADER = struct.Struct("<8sII4i3i3i4fqQQ9bB22x")
+_CKPT_HEADER = struct.Struct("<8sII4i3i3i4fqQQ9bB2x2i12x")
 
 
 def checkpoint_header(data: bytes) -> dict:
@@ -487,6 +487,7 @@ def checkpoint_header(data: bytes) -> dict:
     d = dict(zip(keys, v[:20]))
     d["scale_exponents"] = list(v[20:29])
     d["storage"] = v[29]
+    d["nz_total"], d["z_offset"] = v[30], v[31]
     return d
 
 
