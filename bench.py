@@ -387,6 +387,21 @@ def main():
         dist.destroy_process_group()
 
 
+def _part_launches(h, has_source: bool) -> int:
+    """Kernel launches of one step of a slab run as inner and outer parts."""
+    nzc = h.cfg.nz - 10
+    cols, rows, zc = h.tile()
+    if zc:                                # z-marching: chunk ranges [0, i0), [i0, i1), [i1, nchunks)
+        nch = (nzc + zc - 1) // zc
+        i0 = min(nch, (5 + zc - 1) // zc)
+        i1 = max(i0, (nzc - 5) // zc)
+        return 2 * sum(1 for a, b in ((0, i0), (i0, i1), (i1, nch)) if b > a)
+    i0 = min(5, nzc)                      # simple kernels: plane ranges, plus source and receivers
+    i1 = max(i0, nzc - 5)
+    n = 2 * sum(1 for a, b in ((0, i0), (i0, i1), (i1, nzc)) if b > a)
+    return n + (1 if has_source else 0) + (2 if h.nrec else 0)
+
+
 def main_slabs(args, world, rank, local):
     """One model cut along z: args.slabs slabs on this GPU (world 1), or one
     slab per rank (world > 1; total work fixed, "strong" scaling).  Each step
@@ -449,7 +464,9 @@ def main_slabs(args, world, rank, local):
                      "achieved": alg / (ms / K / 1e3) / 1e9, "peak": peak,
                      "unit": "GB/s", "frac": alg / (ms / K / 1e3) / 1e9 / peak,
                      "peak_source": peak_kind, "traffic": None},
-        "clocks": clk, "gpu_launches": K * 2 * len(handles),
+        "clocks": clk,
+        "gpu_launches": K * sum(_part_launches(h, (rank if world > 1 else k) == m.src_slab)
+                                for k, h in enumerate(handles)),
         "e2e": None,
     }
     if rank == 0:
