@@ -7,8 +7,6 @@
 // the 26 region split arrays replaced by the compact PML array.  It serves as
 // the correctness baseline for the z-marching family and as the fallback for
 // grids the z-marching kernels do not tile.
-#include <algorithm>
-
 #include "cell_math.cuh"
 
 namespace sgfd {
@@ -229,15 +227,8 @@ cudaError_t simple_step(const Model &m, const Physics &ph, const SourceRec &sr,
                         int parts) {
     const dim3 block(kBX, kBY);
     // plane ranges of the selected parts: inner [5, nzc - 5), outer the planes below and above it
-    const int i0 = std::min(kHalo, m.nzc), i1 = std::max(i0, m.nzc - kHalo);
-    int range[3][2], nr = 0;
-    if (parts == (kPartInner | kPartOuter)) {   // the whole half step: one launch
-        range[0][0] = 0; range[0][1] = m.nzc; nr = 1;
-    } else {
-        if (parts & kPartOuter) { range[nr][0] = 0; range[nr][1] = i0; ++nr; }
-        if (parts & kPartInner) { range[nr][0] = i0; range[nr][1] = i1; ++nr; }
-        if (parts & kPartOuter) { range[nr][0] = i1; range[nr][1] = m.nzc; ++nr; }
-    }
+    int range[3][2];
+    const int nr = part_ranges(m.nzc, 1, m.nzc, parts, range);
     auto each = [&](auto fn) {
         for (int r = 0; r < nr; ++r)
             if (range[r][1] > range[r][0])

@@ -48,7 +48,6 @@
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
-#include <algorithm>
 #include <type_traits>
 
 #include "cell_math.cuh"
@@ -1177,18 +1176,10 @@ void launch16(const Model &m, const Physics &ph, const SourceRec &sr, const Half
 template <bool FAST, int CELLS>
 void launch(const Model &m, const Physics &ph, const SourceRec &sr, const ZGeom &g, const ZMaps &zm, int it,
             float src_value, int uw, cudaStream_t s, cudaEvent_t *ev, int phases, int parts) {
-    // chunk ranges of the selected parts: inner chunks [c_in0, c_in1) lie 5 or
-    // more planes from both ends (they read no frame plane), outer chunks the rest
-    const int c_in0 = std::min(g.nchunks, (kHalo + g.zc - 1) / g.zc);
-    const int c_in1 = std::max(c_in0, m.nzc >= kHalo ? (m.nzc - kHalo) / g.zc : 0);
-    int range[3][2], nr = 0;
-    if (parts == (kPartInner | kPartOuter)) {   // the whole half step: one launch
-        range[0][0] = 0; range[0][1] = g.nchunks; nr = 1;
-    } else {
-        if (parts & kPartOuter) { range[nr][0] = 0; range[nr][1] = c_in0; ++nr; }
-        if (parts & kPartInner) { range[nr][0] = c_in0; range[nr][1] = c_in1; ++nr; }
-        if (parts & kPartOuter) { range[nr][0] = c_in1; range[nr][1] = g.nchunks; ++nr; }
-    }
+    // chunk ranges of the selected parts: inner chunks lie 5 or more planes
+    // from both ends (they read no frame plane), outer chunks are the rest
+    int range[3][2];
+    const int nr = part_ranges(m.nzc, g.zc, g.nchunks, parts, range);
     auto each = [&](auto fn) {
         for (int r = 0; r < nr; ++r) {
             if (range[r][1] <= range[r][0]) continue;

@@ -241,6 +241,25 @@ __host__ inline int64_t pml_before(int nxc, int nyc, int nzc, int p, int z) {
 // the source with the inner part and records receivers with the outer one).
 constexpr int kPartInner = 1, kPartOuter = 2;
 
+// The units a part covers, for a model of nzc computed planes cut into n
+// units of `size` planes (z chunks; planes: size 1): up to three ranges
+// [r[i][0], r[i][1]), possibly empty, in z order; returns their count.  A
+// unit is inner when its planes lie 5 or more planes from both ends; the
+// whole half step (both parts) is one range.
+__host__ __device__ inline int part_ranges(int nzc, int size, int n, int parts, int (*r)[2]) {
+    if (parts == (kPartInner | kPartOuter)) {
+        r[0][0] = 0; r[0][1] = n;
+        return 1;
+    }
+    const int a = (kHalo + size - 1) / size, i0 = a < n ? a : n;   // first inner unit
+    const int b = nzc >= kHalo ? (nzc - kHalo) / size : 0, i1 = b > i0 ? b : i0;   // end of the inner units
+    int k = 0;
+    if (parts & kPartOuter) { r[k][0] = 0; r[k][1] = i0; ++k; }
+    if (parts & kPartInner) { r[k][0] = i0; r[k][1] = i1; ++k; }
+    if (parts & kPartOuter) { r[k][0] = i1; r[k][1] = n; ++k; }
+    return k;
+}
+
 // ---- kernel family entry points (host side) -------------------------------
 
 // "simple": one thread per computed cell.

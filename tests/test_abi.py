@@ -161,6 +161,57 @@ int main() {
     assert r.returncode == 0 and r.stdout.strip() == "ok", r.stdout
 
 
+def test_half_step_parts_cover_every_unit_once(tmp_path):
+    """Host-compiles part_ranges() of csrc/sgfd_internal.h, which splits a half
+    step into the units (z chunks, or planes) a z-slab runs while its halos
+    travel and the rest: for every plane count and unit size, the inner and
+    outer parts together cover each unit exactly once, an inner unit's planes
+    lie 5 or more planes from both ends (its updates read no frame plane),
+    every outer unit has a plane closer than that, and the whole half step
+    is one range."""
+    src = tmp_path / "p.cpp"
+    src.write_text(r'''
+#include "sgfd_internal.h"
+#include <cstdio>
+#include <vector>
+using namespace sgfd;
+int main() {
+  for (int nzc = 1; nzc <= 130; ++nzc)
+    for (int size = 1; size <= 60; ++size) {
+      const int n = (nzc + size - 1) / size;
+      int r[3][2];
+      if (part_ranges(nzc, size, n, kPartInner | kPartOuter, r) != 1 || r[0][0] != 0 || r[0][1] != n) {
+        std::printf("whole %d %d\n", nzc, size); return 1;
+      }
+      std::vector<int> seen(n, 0);
+      for (int part : {kPartInner, kPartOuter}) {
+        const int k = part_ranges(nzc, size, n, part, r);
+        int prev = 0;
+        for (int i = 0; i < k; ++i) {
+          if (r[i][0] < prev || r[i][1] < r[i][0] || r[i][1] > n) { std::printf("order %d %d\n", nzc, size); return 1; }
+          prev = r[i][1];
+          for (int u = r[i][0]; u < r[i][1]; ++u) {
+            const int zs = u * size, ze = (u + 1) * size < nzc ? (u + 1) * size : nzc;
+            const bool inner = zs >= kHalo && ze <= nzc - kHalo;
+            if (inner != (part == kPartInner)) { std::printf("unit %d of %d %d\n", u, nzc, size); return 1; }
+            seen[u]++;
+          }
+        }
+      }
+      for (int u = 0; u < n; ++u) if (seen[u] != 1) { std::printf("cover %d %d\n", nzc, size); return 1; }
+    }
+  std::puts("ok"); return 0;
+}
+''')
+    exe = tmp_path / "p"
+    inc = os.path.join(ROOT, "staggered-grid_b200", "csrc")
+    r = subprocess.run(["g++", "-std=c++17", "-O1", f"-I{inc}", "-I/usr/local/cuda/include", str(src), "-o", str(exe)],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    r = subprocess.run([str(exe)], capture_output=True, text=True)
+    assert r.returncode == 0 and r.stdout.strip() == "ok", r.stdout
+
+
 def test_strip_tiles_cover_the_strip_once(tmp_path):
     """Host-compiles csrc/strip_tiles.h and checks the learned strip's tiling
     for uneven sizes and widths: every strip cell in exactly one tile, no
