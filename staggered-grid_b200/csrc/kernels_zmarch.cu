@@ -26,7 +26,7 @@
 //     registers before the plane's TMA wait; the stress update, which needs
 //     15 of them, loads them where they are used, so that it fits the 80
 //     registers per thread of three resident CTAs per SM, and brings them
-//     (and the buoyancy of the damping) into L2 two planes ahead: one bulk
+//     (and the buoyancy of the damping) into L2 one plane ahead: one bulk
 //     prefetch of the 15 stress rows per 32-cell split block.
 //   * 16-bit wavefield storage (ST = BF16 / F16, 32 x 8 tiles): the field
 //     boxes arrive as 16-bit values and are widened once per plane into an
@@ -721,8 +721,10 @@ __device__ __forceinline__ bool str_item(const ZMaps &mp, const Model &m, const 
     int sz = -1;
     if (src >= 0) sz = (int)(src / m.plane);
     // The PML cells' splits and buoyancy, loaded by plain loads after the
-    // stencil, are brought into L2 two planes ahead (32 x 8 tiles: a warp's
-    // cells are one row): their loads then wait on L2 rather than on HBM.
+    // stencil, are brought into L2 one plane ahead, while the plane before
+    // them is computed (32 x 8 tiles: a warp's cells are one row): their
+    // loads then wait on L2 rather than on HBM.  Two and three planes ahead
+    // measured slower.
     auto prefetch = [&](int pz) {
         if constexpr (CELLS == 1) {
             if (pz >= t.ze) return;
@@ -734,7 +736,7 @@ __device__ __forceinline__ bool str_item(const ZMaps &mp, const Model &m, const 
         }
     };
     prefetch(t.zs);
-    prefetch(t.zs + 1);
+
     // One plane, as in the velocity update (GEN: general path; P: place in
     // the pair).  Returns false when the block votes to abort.
     auto plane = [&](auto gen_tag, auto p_tag) -> bool {
@@ -936,7 +938,7 @@ __device__ __forceinline__ bool str_item(const ZMaps &mp, const Model &m, const 
     auto run = [&](auto p_tag) -> bool {
         const int gzp = cz + kHalo;
         const bool gen = t.xy_pml || bandz(m, gzp) != 0 || gzp == sz || gzp == rz;
-        prefetch(cz + 2);
+        prefetch(cz + 1);
         return gen ? plane(std::true_type{}, p_tag) : plane(std::false_type{}, p_tag);
     };
     while (cz < t.ze) {
