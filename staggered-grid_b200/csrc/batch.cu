@@ -357,6 +357,7 @@ void sgfd_batch_destroy(sgfd_batch *b) {
 const char *sgfd_batch_last_error(const sgfd_batch *b) { return b ? b->err.c_str() : ""; }
 
 int sgfd_batch_run(sgfd_batch *b, int32_t it0, int32_t nsteps) {
+    TraceRange trace("sgfd_batch_run");
     if (!b) return fail(nullptr, SGFD_ERR_INVALID, "null batch");
     BATCH_CUDA(b, cudaSetDevice(b->device), "cudaSetDevice");
     if (nsteps < 0 || it0 < 0 || (int64_t)it0 + nsteps > INT32_MAX) return bfail(b, SGFD_ERR_INVALID, "bad step range");

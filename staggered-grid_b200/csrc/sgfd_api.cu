@@ -628,6 +628,7 @@ static int upload_medium(sgfd_solver *h, const float *b, const float *l, const f
 }
 
 int sgfd_set_medium(sgfd_solver *h, const float *b, const float *l, const float *mu) {
+    TraceRange trace("sgfd_set_medium");
     return upload_medium(h, b, l, mu, cudaMemcpyHostToDevice);
 }
 
@@ -708,6 +709,7 @@ int sgfd_set_wavelet(sgfd_solver *h, int32_t nt, const float *values) {
 }
 
 int sgfd_step(sgfd_solver *h, int32_t it, float source_value) {
+    TraceRange trace("sgfd_step");
     int r = check_handle(h);
     if (r) return r;
     if (!h->medium_set) return fail(h, SGFD_ERR_STATE, "sgfd_set_medium must come before stepping");
@@ -715,6 +717,7 @@ int sgfd_step(sgfd_solver *h, int32_t it, float source_value) {
 }
 
 int sgfd_run(sgfd_solver *h, int32_t it0, int32_t nsteps, int32_t use_graph) {
+    TraceRange trace("sgfd_run");
     int r = check_handle(h);
     if (r) return r;
     if (!h->medium_set) return fail(h, SGFD_ERR_STATE, "sgfd_set_medium must come before stepping");
@@ -744,6 +747,7 @@ int sgfd_step_phase(sgfd_solver *h, int32_t it, float source_value, int32_t phas
 }
 
 int sgfd_step_phase_part(sgfd_solver *h, int32_t it, float source_value, int32_t phase, int32_t parts) {
+    TraceRange trace("sgfd_step_phase_part");
     int r = check_handle(h);
     if (r) return r;
     if (!h->medium_set) return fail(h, SGFD_ERR_STATE, "sgfd_set_medium must come before stepping");
@@ -779,6 +783,7 @@ namespace {
 // unpack writes its frame planes there.  The 5 planes of a field are one
 // contiguous range of its padded array.
 int halo_copy(sgfd_solver *h, int32_t side, int32_t kind, void *buf, bool pack) {
+    TraceRange trace("sgfd_halo");
     int r = check_handle(h);
     if (r) return r;
     if (!buf) return fail(h, SGFD_ERR_INVALID, "null halo buffer");

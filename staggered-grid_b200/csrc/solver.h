@@ -5,6 +5,8 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/sgfd.h"
 #include "sgfd_internal.h"
 #include "zmarch.h"
@@ -30,6 +32,17 @@ struct GraphKey {
 };
 // Steps per captured graph; sgfd_run launches the remainder directly.
 constexpr int kGraphSteps = 16;
+
+// A named range on the host timeline of the calling thread, from here to the
+// end of the scope: what a profiler (Nsight Systems, Nsight Compute's
+// --nvtx filters) shows around the launches of a call.  Without a profiler
+// attached the calls return at once.
+struct TraceRange {
+    explicit TraceRange(const char *name) { nvtxRangePushA(name); }
+    ~TraceRange() { nvtxRangePop(); }
+    TraceRange(const TraceRange &) = delete;
+    TraceRange &operator=(const TraceRange &) = delete;
+};
 }  // namespace sgfd
 
 struct sgfd_solver {

@@ -263,3 +263,19 @@ int main() {
     assert r.returncode == 0, r.stderr
     r = subprocess.run([str(exe)], capture_output=True, text=True)
     assert r.returncode == 0 and r.stdout.strip() == "ok", r.stdout
+
+
+def test_entry_points_reject_a_null_handle():
+    """Without a handle the stepping, halo and medium calls return
+    SGFD_ERR_INVALID instead of touching a device (their profiler trace
+    ranges open and close on the host all the same)."""
+    L = sgfd.lib()
+    assert L.sgfd_run(None, 0, 1, 0) == sgfd.ERR_INVALID
+    assert L.sgfd_step(None, 0, 0.0) == sgfd.ERR_INVALID
+    assert L.sgfd_step_phase(None, 0, 0.0, sgfd.PHASE_VELOCITY) == sgfd.ERR_INVALID
+    assert L.sgfd_step_phase_part(None, 0, 0.0, sgfd.PHASE_STRESS, sgfd.PART_INNER) == sgfd.ERR_INVALID
+    assert L.sgfd_halo_pack(None, sgfd.HALO_LOW, sgfd.HALO_STRESS, None) == sgfd.ERR_INVALID
+    assert L.sgfd_halo_unpack(None, sgfd.HALO_HIGH, sgfd.HALO_VELOCITY, None) == sgfd.ERR_INVALID
+    n = ctypes.c_int64(-1)
+    assert L.sgfd_halo_bytes(None, ctypes.byref(n)) == sgfd.ERR_INVALID
+    assert L.sgfd_set_medium(None, None, None, None) == sgfd.ERR_INVALID
