@@ -9,8 +9,10 @@ cells x steps / device seconds), whole job over all ranks.
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl sgfd|reference]
 
 With N > 1 (torchrun) every rank advances its own independent replica of the
-model on its own GPU ("replicas only": the path has no exchange step), so
-scaling is weak.  `--impl reference` times the reference algorithm's CPU
+model on its own GPU (no exchange step), so scaling is weak.  `--slabs N`
+instead cuts the one model into z-slabs that trade 5-plane halos every half
+step: N slabs on one GPU, or one slab per rank under torchrun (NCCL
+send/recv; total work fixed, strong scaling).  `--impl reference` times the reference algorithm's CPU
 implementation (this project's oracle port, all host threads) on rank 0 and
 also reports the reference's own GPU program (compiled from its sources under
 oracle/_ref/) timed on this GPU.
